@@ -1,0 +1,275 @@
+"""Benchmark of the cloud-rendering hot path on B200.
+
+Workload (one step = one frame): the neural form of the renderer (render type
+MRPNN) on a 512^3 seeded Perlin-fBm cloud with its full mip pyramid, at
+1920 x 1080, 1 primary sample per pixel, fp32 network (Xavier weights from
+seed 1), extinction scale 64, albedo 0.99, g = 0.857, one seeded directional
+light, camera at distance 2.5 with a 40 degree field of view. Synthetic
+inputs; the volume is generated on the GPU before timing.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Multi-GPU runs are independent replicas (each rank renders its own frames;
+no collective on the data path); `value` is the frames of all ranks divided by
+the slowest rank's device time. `--impl reference` times the CPU
+restatement of the reference path (the oracle, OpenMP on all host cores) on
+a bounded sample of rows of the same frame.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "frames/s at 1080p, neural vs delta-tracking at matched RMSE vs 16k-spp oracle"
+WIDTH, HEIGHT, RES = 1920, 1080, 512
+FLOP_PER_PIXEL = 97072  # 48,536 MAC of the network per active pixel and albedo channel
+WORKLOAD = ("neural (MRPNN) render 1920x1080, 1 spp, 512^3 Perlin-fBm cloud (6 oct, f0 4, lac 2, gain 0.5, "
+            "thr 0.45, radial falloff), fp32 network, Xavier(seed 1) weights, alpha 64, albedo 0.99, g 0.857")
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d["hbm_gbs"], d["bf16_tflops"], "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples every 200 ms during the timed region."""
+
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.flush()
+        rows = [l.split(",") for l in open(self.f.name).read().strip().splitlines() if l.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_reference(args, rank):
+    """CPU restatement (oracle) of the reference path on the host cores."""
+    if rank != 0:
+        return
+    from internship_b200 import scenes, xavier_weights, builtin_stencil
+    from oracle import orc
+    threads = orc.nthreads()
+    dens = orc.cloud(RES, 7)
+    md, mips, _ = orc.build_mips(dens)
+    p = scenes.cloud_scene_params(WIDTH, HEIGHT)
+    L = np.array([p.light_dir.x, p.light_dir.y, p.light_dir.z], np.float32)
+    tr = orc.build_tr(mips, p.alpha, L)
+    lut = orc.build_hglut(p.g, p.seed)
+    w, st = xavier_weights(1), builtin_stencil()
+    rows_per_step = 16
+    rows = np.linspace(0, HEIGHT - 1, rows_per_step * (args.steps + args.warmup)).astype(int)
+    times = []
+    for k in range(args.warmup + args.steps):
+        sel = rows[k::args.warmup + args.steps]
+        t0 = time.perf_counter()
+        for r in sel:
+            orc.render_neural(dens, md, mips, tr, lut, w, st, p, int(r), int(r) + 1)
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            times.append(dt)
+    t = float(np.sum(times))
+    frames = args.steps * rows_per_step / HEIGHT
+    fps = frames / t
+    line = {"metric": METRIC, "value": fps, "unit": "frames/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "parallelism": "host cores (OpenMP)"},
+            "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": threads, "kind": "port",
+                             "sample": "%d of %d rows per step, rows spread over the frame" % (rows_per_step, HEIGHT)},
+            "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_sample(v, dens_dev, p, w, st):
+    """Bounded sample of the same frame on the oracle (all host cores)."""
+    from internship_b200 import _lib
+    from oracle import orc
+    dens = dens_dev.cpu().numpy()
+    mips = np.concatenate([v.read(_lib.READ_MIP, k) for k in range(9)])
+    tr = np.concatenate([v.read(_lib.READ_TR, k) for k in range(8)])
+    lut = v.read(_lib.READ_HGLUT)
+    rows = np.linspace(0, HEIGHT - 1, 24).astype(int)
+    t0 = time.perf_counter()
+    for r in rows:
+        orc.render_neural(dens, v.max_density, mips, tr, lut, w, st, p, int(r), int(r) + 1)
+    dt = time.perf_counter() - t0
+    fps = (len(rows) / HEIGHT) / dt
+    return {"value": fps, "unit": "frames/s", "cores": orc.nthreads(), "kind": "port",
+            "sample": "%d of %d rows of one frame (oracle, OpenMP)" % (len(rows), HEIGHT)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    torch.cuda.set_device(local)
+    import internship_b200 as mr
+    from internship_b200 import _lib, scenes
+    L = _lib.load()
+    stream = torch.cuda.current_stream().cuda_stream
+    sp = C.c_void_p(stream)
+
+    # -- inputs: cloud generated on the device, tables built, network uploaded
+    dens = torch.empty(RES ** 3, device="cuda", dtype=torch.float32)
+    scenes.generate_cloud_device(RES, 7, dens.data_ptr(), sp)
+    v = mr.VolumeRender(RES)
+    _lib.check(L.mr_volume_set_data_device(v.handle, C.c_void_p(dens.data_ptr()), dens.numel(), sp))
+    _lib.check(L.mr_volume_update(v.handle, sp))
+    md = C.c_float()
+    _lib.check(L.mr_volume_max_density(v.handle, C.byref(md)))
+    v.max_density = md.value
+    w, st = mr.xavier_weights(1), mr.builtin_stencil()
+    v.SetWeights(w, st)
+    net = v.network.handle
+    p = scenes.cloud_scene_params(WIDTH, HEIGHT, seed=rank)
+    out = torch.empty(WIDTH * HEIGHT * 3, device="cuda", dtype=torch.float32)
+    flush = torch.empty(256 * 1024 * 1024 // 4, device="cuda", dtype=torch.float32)
+
+    def render(step):
+        p.sample_offset = step
+        _lib.check(L.mr_render(v.handle, net, C.byref(p), C.c_void_p(out.data_ptr()), sp))
+
+    for k in range(args.warmup):
+        render(k)
+    torch.cuda.synchronize()
+    L.mr_volume_stage_times(v.handle, (C.c_double * 8)(), (C.c_int32 * 8)(), 8)  # reset
+    _lib.check(L.mr_volume_set_timing(v.handle, 1))
+
+    # -- device-timed steps (L2 flushed between steps, outside the events)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(torch.cuda.current_device())
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        evs[k][0].record()
+        render(args.warmup + k)
+        evs[k][1].record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = float(sum(a.elapsed_time(b) for a, b in evs))
+    stage_ms = (C.c_double * 8)()
+    stage_n = (C.c_int32 * 8)()
+    _lib.check(L.mr_volume_stage_times(v.handle, stage_ms, stage_n, 8))
+    _lib.check(L.mr_volume_set_timing(v.handle, 0))
+    cnt = (C.c_uint64 * 4)()
+    _lib.check(L.mr_volume_counters(v.handle, cnt))
+    active = int(cnt[3])
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    fps = world * args.steps / (ms / 1000.0)
+
+    # -- end to end through the public API: render + D2H of the frame to pinned memory
+    host = torch.empty(WIDTH * HEIGHT * 3, dtype=torch.float32, pin_memory=True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(args.steps):
+        render(1000 + k)
+        host.copy_(out, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_fps = world * args.steps / (e2e_ms / 1000.0)
+
+    hbm, bf16, src = peaks()
+    pred_ms = stage_ms[2] / max(1, stage_n[2])
+    achieved = FLOP_PER_PIXEL * (active / max(1, args.steps)) / (pred_ms / 1000.0) / 1e12
+    roofline = {"bound": "tensor", "kernel": "k_nn_predict_simt (gather + fp32 network)", "achieved": achieved,
+                "peak": bf16, "unit": "TFLOP/s", "frac": achieved / bf16, "peak_source": src,
+                "traffic": None}
+    line = {"metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "frame": "%dx%d" % (WIDTH, HEIGHT), "volume": "%d^3" % RES,
+                       "l2": "flushed between steps (256 MiB write outside the timed events)",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "e2e": {"value": e2e_fps, "unit": "frames/s", "h2d_bytes_per_step": C.sizeof(_lib.RenderParams),
+                    "d2h_bytes_per_step": WIDTH * HEIGHT * 3 * 4},
+            "gpu_launches": int(sum(stage_n[i] for i in range(8))),
+            "roofline": roofline, "clocks": clk,
+            "stages_ms_per_step": {"nn_trace": stage_ms[1] / max(1, stage_n[1]),
+                                   "nn_gather_network": stage_ms[2] / max(1, stage_n[2])},
+            "active_pixels_per_frame": active / max(1, args.steps)}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample(v, dens, p, w, st)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    v.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,183 @@
+/*
+ * mrpnn_b200.h - C ABI of the B200-native MRPNN cloud renderer.
+ *
+ * Plain pointers, sizes and POD structs only. Every entry point returns an
+ * int status (mr_status); mr_last_error() gives the message of the last
+ * failure on the calling thread. Device pointers are CUDA device memory on
+ * the current device; `stream` is a cudaStream_t passed as void* (NULL = the
+ * legacy default stream).
+ *
+ * Each entry point names the reference interface it replaces
+ * (paths relative to the reference project).
+ */
+#ifndef MRPNN_B200_H
+#define MRPNN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct { float x, y, z; } mr_float3;
+
+typedef enum {
+  MR_OK = 0,
+  MR_ERR_ARG = 1,         /* invalid argument (size, pointer, range) */
+  MR_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+  MR_ERR_TIMEOUT = 3,     /* mr_sync watchdog expired */
+  MR_ERR_LOOP_CAP = 4,    /* a device loop hit its iteration cap and reported it */
+  MR_ERR_STATE = 5,       /* call made in the wrong state (e.g. render before update) */
+  MR_ERR_NOMEM = 6,       /* device allocation failed */
+  MR_ERR_UNSUPPORTED = 7  /* feature not built into this library */
+} mr_status;
+
+/* core/volume.hpp:88-90 VolumeRender::RenderType (RPNN's weights are not in
+ * the reference tree and it is not supported here). */
+typedef enum { MR_RT_PT = 0, MR_RT_RPNN = 1, MR_RT_MRPNN = 2 } mr_render_type;
+
+/* Arithmetic of the radiance-predictor MLP. */
+typedef enum { MR_PREC_FP32 = 0, MR_PREC_BF16 = 1, MR_PREC_FP8 = 2 } mr_precision;
+
+/* What mr_volume_read copies back. */
+typedef enum {
+  MR_READ_DENSITY = 0,   /* res^3, x-major */
+  MR_READ_MIP = 1,       /* level k: (256>>k)^3 */
+  MR_READ_VARIANCE = 2,  /* level k: (256>>k)^3 */
+  MR_READ_TR = 3,        /* level k: (128>>k)^3 */
+  MR_READ_HGLUT = 4      /* 512 x 512, index i + j*512 (i: cos bin, j: cone-angle bin) */
+} mr_read_what;
+
+typedef struct mr_volume mr_volume;
+typedef struct mr_network mr_network;
+
+/* One render request. Mirrors the arguments of VolumeRender::Render
+ * (core/volume.hpp:141) plus the device-side settings the reference keeps in
+ * __device__ globals (core/render.cuh:9-17): scatter_rate, tr_scale,
+ * enviroment_exp. */
+typedef struct {
+  int32_t width, height;
+  mr_float3 ori;          /* camera position; forward = normalize(-ori) */
+  mr_float3 up, right;    /* screen half-extent vectors (tan(fov/2) scaled) */
+  mr_float3 light_dir;    /* direction towards the light (normalised inside) */
+  mr_float3 light_color;
+  float alpha;            /* extinction scale */
+  float g;                /* Henyey-Greenstein asymmetry */
+  mr_float3 scatter_rate; /* per-channel albedo (SetScatterRate) */
+  float tr_scale;         /* NEE step scale (SetTrScale), normally 1 */
+  mr_float3 env_color;    /* radiance of escaped rays (constant environment), 0 = black */
+  int32_t max_bounces;    /* multiScatter */
+  int32_t spp;            /* samples per pixel (PT); neural renders 1 primary sample per pass */
+  uint32_t seed;          /* Philox key */
+  uint32_t sample_offset; /* index of the first sample (progressive accumulation) */
+  int32_t render_type;    /* mr_render_type */
+  int32_t precision;      /* mr_precision (MRPNN only) */
+} mr_render_params;
+
+/* Library version string. */
+const char* mr_version(void);
+/* Message of the last failed call on this thread ("" if none). */
+const char* mr_last_error(void);
+
+/* ---- volume (replaces VolumeRender: core/volume.hpp:45-146) ---------------- */
+
+/* VolumeRender(int resolution) + MallocMemory (core/volume.cu:748-773,831-833). */
+int mr_volume_create(int32_t resolution, mr_volume** out);
+/* ~VolumeRender (core/volume.cu:913-936). */
+int mr_volume_destroy(mr_volume* v);
+/* SetDatas / SetData (core/volume.cu:938-944): host array, index (x*res+y)*res+z. */
+int mr_volume_set_data(mr_volume* v, const float* host_data, size_t count);
+/* Same, from device memory, stream-ordered. */
+int mr_volume_set_data_device(mr_volume* v, const float* dev_data, size_t count, void* stream);
+/* Update() (core/volume.cu:1203-1316): global majorant, density mip pyramid
+ * 256^3..1^3 and its 2x2x2 variance pyramid. */
+int mr_volume_update(mr_volume* v, void* stream);
+/* Update_TR(lightDir, alpha) (core/volume.cu:1346-1424): light-transmittance
+ * pyramid 128^3..1^3. Skipped when light and alpha are unchanged. */
+int mr_volume_update_tr(mr_volume* v, mr_float3 light_dir, float alpha, void* stream);
+/* UpdateHGLut(g) (core/volume.cu:1161-1183): 512x512 cone-averaged HG table.
+ * Skipped when g and seed are unchanged. */
+int mr_volume_update_hglut(mr_volume* v, float g, uint32_t seed, void* stream);
+/* VolumeRender::max_density after mr_volume_update. */
+int mr_volume_max_density(const mr_volume* v, float* out);
+int mr_volume_resolution(const mr_volume* v, int32_t* out);
+/* Copy one level of a volume-side table back to the host (synchronous). */
+int mr_volume_read(const mr_volume* v, int32_t what, int32_t level, float* host_out, size_t count);
+
+/* ---- network (replaces the NNWeight.cuh constants: core/NNWeight.cuh) ------ */
+
+/* Upload MR_WEIGHT_TOTAL fp32 weights in the blob layout of mrpnn_weights.h.
+ * `stencil_xyz` is 160 x 3 floats of stencil directions (the tables of
+ * core/vector.cu:77-172); NULL selects the library's built-in stencil. */
+int mr_network_create(const float* host_weights, size_t count, const float* stencil_xyz,
+                      mr_network** out);
+int mr_network_destroy(mr_network* net);
+
+/* The library's built-in 160-point stencil (used when mr_network_create gets
+ * NULL): 480 floats. */
+int mr_builtin_stencil(float* host_out, size_t count);
+/* Xavier-uniform initial weights for the blob layout (zero biases), from
+ * Philox with the given seed: MR_WEIGHT_TOTAL floats. */
+int mr_weights_xavier(uint32_t seed, float* host_out, size_t count);
+
+/* ---- rendering ------------------------------------------------------------- */
+
+/* VolumeRender::Render(int2 size, ...) (core/volume.cu:410-467) into caller
+ * device memory: dev_rgb = width*height*3 fp32, row-major, mean radiance over
+ * the samples. PT = delta tracking; MRPNN = neural form (network required;
+ * call mr_volume_update_tr / _hglut first or let the call do it). */
+int mr_render(mr_volume* v, const mr_network* net, const mr_render_params* p, float* dev_rgb,
+              void* stream);
+/* Same, synchronous, into host memory (the reference returns vector<float3>). */
+int mr_render_host(mr_volume* v, const mr_network* net, const mr_render_params* p, float* host_rgb);
+/* Delta tracking with FP64 accumulation: adds this call's per-pixel radiance
+ * sums and sums of squares (width*height*3 doubles each, caller-zeroed) so
+ * that many calls build a high-spp reference image. */
+int mr_render_accumulate_f64(mr_volume* v, const mr_render_params* p, double* dev_sum,
+                             double* dev_sumsq, void* stream);
+
+/* RadiancePredict network body (core/radiancePredict.cu:370-485) on n
+ * descriptors: dev_desc = n x 576 fp32 ([density 192 | transmittance 192 |
+ * phase 192], log-encoded as the reference does), dev_aux = n x 5 fp32
+ * (g, gamma, srp.x, srp.y, srp.z), dev_out = n x 3 fp32. */
+int mr_radiance_predict(const mr_network* net, int32_t precision, const float* dev_desc,
+                        const float* dev_aux, int32_t n, float* dev_out, void* stream);
+
+/* Descriptor gather (core/radiancePredict.cu:319-368) for n points:
+ * dev_pos n x 3, dev_frame n x 12 (XMain, YMain, ZMain, LXMain), writes
+ * dev_desc n x 576 and dev_aux n x 5 (g, gamma, srp) for the given alpha, g,
+ * scatter_rate. Volume tables must be up to date. */
+int mr_gather_descriptors(const mr_volume* v, const mr_network* net, const float* dev_pos,
+                          const float* dev_frame, int32_t n, float alpha, float g,
+                          mr_float3 scatter_rate, float* dev_desc, float* dev_aux, void* stream);
+
+/* Seeded procedural cloud (benchmark / training input): Perlin fBm with
+ * `octaves` octaves from `base_freq`, lacunarity and gain, normalised to
+ * [0,1], thresholded at `threshold` and shaped by a radial falloff; res^3
+ * fp32 into dev_out, index (x*res+y)*res+z. */
+int mr_generate_cloud(int32_t res, uint32_t seed, int32_t octaves, float base_freq, float lacunarity,
+                      float gain, float threshold, float* dev_out, void* stream);
+/* The 256-entry noise permutation the cloud generator uses for `seed`. */
+int mr_cloud_permutation(uint32_t seed, int32_t* host_out256);
+
+/* Wait for `stream` with a watchdog: MR_ERR_TIMEOUT after timeout_ms. */
+int mr_sync(void* stream, int32_t timeout_ms);
+
+/* Per-stage CUDA-event timing of this volume's kernels (off by default).
+ * Stages: 0 delta tracking, 1 neural trace, 2 neural gather+network,
+ * 3 TR build, 4 HG table build, 5 pyramid build. mr_volume_stage_times waits
+ * for the device, returns the summed milliseconds and launch counts of the
+ * first n stages since the last query, and resets them. */
+int mr_volume_set_timing(mr_volume* v, int32_t enable);
+int mr_volume_stage_times(mr_volume* v, double* host_ms, int32_t* host_launches, int32_t n);
+
+/* Counters of the last render on this volume: [0] density fetches, [1] paths,
+ * [2] loop-cap hits, [3] active neural pixels. */
+int mr_volume_counters(const mr_volume* v, uint64_t* host_out4);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MRPNN_B200_H */

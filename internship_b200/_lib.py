@@ -1,0 +1,102 @@
+"""ctypes binding of libmrpnn_b200.so (the C ABI in include/mrpnn_b200.h).
+
+The library is loaded from this package directory only; a missing or stale
+build raises immediately -- there is no fallback implementation.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmrpnn_b200.so")
+
+MR_OK, MR_ERR_ARG, MR_ERR_CUDA, MR_ERR_TIMEOUT, MR_ERR_LOOP_CAP, MR_ERR_STATE, MR_ERR_NOMEM, MR_ERR_UNSUPPORTED = range(8)
+RT_PT, RT_RPNN, RT_MRPNN = 0, 1, 2
+PREC_FP32, PREC_BF16, PREC_FP8 = 0, 1, 2
+READ_DENSITY, READ_MIP, READ_VARIANCE, READ_TR, READ_HGLUT = range(5)
+WEIGHT_TOTAL = 49673
+
+# Every symbol include/mrpnn_b200.h declares (checked by the CPU tests).
+EXPORTS = [
+    "mr_version", "mr_last_error", "mr_volume_create", "mr_volume_destroy", "mr_volume_set_data",
+    "mr_volume_set_data_device", "mr_volume_update", "mr_volume_update_tr", "mr_volume_update_hglut",
+    "mr_volume_max_density", "mr_volume_resolution", "mr_volume_read", "mr_network_create",
+    "mr_network_destroy", "mr_builtin_stencil", "mr_weights_xavier", "mr_render", "mr_render_host",
+    "mr_render_accumulate_f64", "mr_radiance_predict", "mr_gather_descriptors", "mr_sync",
+    "mr_volume_counters", "mr_generate_cloud", "mr_cloud_permutation",
+    "mr_volume_set_timing", "mr_volume_stage_times",
+]
+
+
+class Float3(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float), ("z", C.c_float)]
+
+
+class RenderParams(C.Structure):
+    """mr_render_params."""
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32),
+                ("ori", Float3), ("up", Float3), ("right", Float3),
+                ("light_dir", Float3), ("light_color", Float3),
+                ("alpha", C.c_float), ("g", C.c_float), ("scatter_rate", Float3),
+                ("tr_scale", C.c_float), ("env_color", Float3),
+                ("max_bounces", C.c_int32), ("spp", C.c_int32),
+                ("seed", C.c_uint32), ("sample_offset", C.c_uint32),
+                ("render_type", C.c_int32), ("precision", C.c_int32)]
+
+
+class MRError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("mrpnn error %d: %s" % (code, msg))
+        self.code = code
+
+
+_lib = None
+
+
+def f3(v):
+    return Float3(float(v[0]), float(v[1]), float(v[2]))
+
+
+def load():
+    """Load the library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libmrpnn_b200.so is not built; run internship_b200.build.build()")
+    L = C.CDLL(LIB_PATH)
+    vp, sz, i32, u32, fp = C.c_void_p, C.c_size_t, C.c_int32, C.c_uint32, C.c_float
+    L.mr_version.restype = C.c_char_p
+    L.mr_last_error.restype = C.c_char_p
+    L.mr_volume_create.argtypes = [i32, C.POINTER(vp)]
+    L.mr_volume_destroy.argtypes = [vp]
+    L.mr_volume_set_data.argtypes = [vp, vp, sz]
+    L.mr_volume_set_data_device.argtypes = [vp, vp, sz, vp]
+    L.mr_volume_update.argtypes = [vp, vp]
+    L.mr_volume_update_tr.argtypes = [vp, Float3, fp, vp]
+    L.mr_volume_update_hglut.argtypes = [vp, fp, u32, vp]
+    L.mr_volume_max_density.argtypes = [vp, C.POINTER(fp)]
+    L.mr_volume_resolution.argtypes = [vp, C.POINTER(i32)]
+    L.mr_volume_read.argtypes = [vp, i32, i32, vp, sz]
+    L.mr_network_create.argtypes = [vp, sz, vp, C.POINTER(vp)]
+    L.mr_network_destroy.argtypes = [vp]
+    L.mr_builtin_stencil.argtypes = [vp, sz]
+    L.mr_weights_xavier.argtypes = [u32, vp, sz]
+    L.mr_render.argtypes = [vp, vp, C.POINTER(RenderParams), vp, vp]
+    L.mr_render_host.argtypes = [vp, vp, C.POINTER(RenderParams), vp]
+    L.mr_render_accumulate_f64.argtypes = [vp, C.POINTER(RenderParams), vp, vp, vp]
+    L.mr_radiance_predict.argtypes = [vp, i32, vp, vp, i32, vp, vp]
+    L.mr_gather_descriptors.argtypes = [vp, vp, vp, vp, i32, fp, fp, Float3, vp, vp, vp]
+    L.mr_sync.argtypes = [vp, i32]
+    L.mr_volume_counters.argtypes = [vp, vp]
+    L.mr_generate_cloud.argtypes = [i32, u32, i32, fp, fp, fp, fp, vp, vp]
+    L.mr_cloud_permutation.argtypes = [u32, vp]
+    L.mr_volume_set_timing.argtypes = [vp, i32]
+    L.mr_volume_stage_times.argtypes = [vp, vp, vp, i32]
+    _lib = L
+    return L
+
+
+def check(rc):
+    if rc != MR_OK:
+        raise MRError(rc, load().mr_last_error().decode())
+    return rc

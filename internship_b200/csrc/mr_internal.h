@@ -1,0 +1,92 @@
+// Host-side internals shared by the library's translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/mrpnn_b200.h"
+#include "../../include/mrpnn_weights.h"
+#include "mr_device.cuh"
+
+namespace mr {
+
+// Counters kept per volume on the device ([0] density fetches, [1] paths,
+// [2] loop-cap hits, [3] active neural pixels, [4..7] scratch).
+constexpr int kCounters = 8;
+
+// Optional per-stage CUDA-event timing (mr_volume_set_timing).
+enum Stage { ST_PT = 0, ST_NN_TRACE = 1, ST_NN_PREDICT = 2, ST_TR = 3, ST_LUT = 4, ST_MIPS = 5, ST_COUNT = 8 };
+struct StageTimer {
+  bool on = false;
+  std::vector<cudaEvent_t> ev[ST_COUNT];  // begin/end pairs
+  void mark(int st, cudaStream_t s) {
+    if (!on) return;
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    cudaEventRecord(e, s);
+    ev[st].push_back(e);
+  }
+};
+
+struct Volume {
+  int res = 0;
+  int device = 0;
+  float* density = nullptr;  // res^3
+  float* mips = nullptr;     // kMipTotal
+  float* var = nullptr;      // kMipTotal
+  float* tr = nullptr;       // kTrTotal
+  float* lut = nullptr;      // 512 x 512
+  float* d_max = nullptr;    // device majorant (one float)
+  unsigned long long* d_counters = nullptr;
+  float max_density = 0.00001f;
+  bool data_set = false;
+  bool mips_valid = false;
+  bool tr_valid = false;
+  F3 tr_light{0, 0, 0};
+  float tr_alpha = 0;
+  bool lut_valid = false;
+  float lut_g = 0;
+  uint32_t lut_seed = 0;
+  StageTimer timer;
+  // Per-render scratch owned by the volume (grown on demand).
+  void* scratch = nullptr;
+  size_t scratch_bytes = 0;
+};
+
+struct Network {
+  float* w = nullptr;        // MR_WEIGHT_TOTAL fp32, blob layout
+  float* stencil = nullptr;  // 160 x 3
+  void* packed = nullptr;    // tensor-core operand images (bf16/fp8), see mr_mlp_tc.cu
+  size_t packed_bytes = 0;
+  float h_stencil[MR_STENCIL_POINTS * 3];
+};
+
+// Error reporting: thread-local message, returns the code.
+int set_error(int code, const char* fmt, ...);
+int cuda_error(cudaError_t e, const char* what);
+void clear_error();
+
+#define MR_CUDA(call)                                   \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) return ::mr::cuda_error(e_, #call); \
+  } while (0)
+
+inline F3 to_f3(const mr_float3& a) { return F3{a.x, a.y, a.z}; }
+
+// Grows v->scratch to at least `bytes` (stream-ordered free of the old block).
+int ensure_scratch(Volume* v, size_t bytes, cudaStream_t s);
+
+// Kernels launched from several translation units.
+int launch_update_tr(Volume* v, F3 L, float alpha, cudaStream_t s);
+int launch_update_lut(Volume* v, float g, uint32_t seed, cudaStream_t s);
+int sm_count();
+
+}  // namespace mr
+
+struct mr_volume { mr::Volume v; };
+struct mr_network { mr::Network n; };

@@ -1,0 +1,362 @@
+// Neural render (render type MRPNN), fp32: NNPredict<MRPNN> of
+// core/render.cuh:469-523 split into two stream-ordered kernels.
+//  1. k_nn_trace: per pixel, camera ray + first Woodcock collision
+//     (GetSamplePoint), the two random frames (GetMatrixFromNormal) and the
+//     single-scatter NEE term Tr*HG; active pixels are compacted into a record
+//     list with warp-aggregated atomics, inactive ones get the environment.
+//  2. k_nn_predict_simt: per active record, the 192-point multi-scale
+//     descriptor gather (core/radiancePredict.cu:319-368) and the network body.
+#include "mr_internal.h"
+#include "mr_net_simt.cuh"
+#include "mr_track.cuh"
+
+namespace mr {
+
+struct Tables {
+  const float* __restrict__ mips;
+  const float* __restrict__ tr;
+  const float* __restrict__ lut;
+};
+
+__constant__ unsigned c_mip_off[9] = {0u, 16777216u, 18874368u, 19136512u, 19169280u, 19173376u, 19173888u,
+                                      19173952u, 19173960u};
+__constant__ unsigned c_tr_off[8] = {0u, 2097152u, 2359296u, 2392064u, 2396160u, 2396672u, 2396736u, 2396744u};
+
+__device__ __forceinline__ float mip_density(const Tables& t, int mip, F3 p) {
+  return tri_border(t.mips + c_mip_off[mip], 256 >> mip, p + 0.5f);
+}
+__device__ __forceinline__ float mip_tr(const Tables& t, int mip, F3 p) {
+  return tri_clamp(t.tr + c_tr_off[mip], 128 >> mip, p + 0.5f);
+}
+// ShadowTerm_TRTex (core/renderResources.cu:121-139), light colour 1.
+__device__ __forceinline__ float shadow_tr(const Tables& t, F3 p, F3 L, int mip) {
+  if (p.x < -0.5f || p.y < -0.5f || p.z < -0.5f || p.x > 0.5f || p.y > 0.5f || p.z > 0.5f) {
+    float off = ray_box_offset(p, L);
+    if (off >= 0) return mip_tr(t, mip, p + L * off);
+    return 1.0f;
+  }
+  return mip_tr(t, mip, p);
+}
+
+struct Frame { F3 X, Y, Z, LX; };
+
+// Descriptor gather for one point (core/radiancePredict.cu:319-359).
+__device__ __forceinline__ void gather_point(const Tables& t, const float* __restrict__ stencil, F3 pos, F3 L,
+                                             const Frame& f, float alpha, float g, float* xv, float* xs,
+                                             float* xh) {
+  const float kLutAngle = 3.1415926535f * 60.0f / 180.0f;
+#pragma unroll 1
+  for (int i = 0; i < 192; ++i) {
+    StencilInfo si = stencil_info(i);
+    F3 p;
+    if (si.type >= 4) {
+      float sx = __ldg(stencil + 3 * i), sy = __ldg(stencil + 3 * i + 1), sz = __ldg(stencil + 3 * i + 2);
+      p = pos + ((f.X * sx + f.Y * sy + f.Z * sz) * si.offset);
+    } else {
+      p = pos + L * si.offset;
+    }
+    int mip = si.mip;
+    xv[i] = logf(1.0f + alpha * mip_density(t, mip, p) / 64.0f);
+    if (si.localindex == 0) {
+      xh[i] = logf(hg_phase(dot(f.X, L), g) + 1.0f);
+    } else {
+      F3 md = normalize(p - pos);
+      float radius = (float)(1 << mip) / 256.0f;
+      float angle = atanf(0.5f * radius / si.offset);
+      float c1 = dot(f.X, md), c2 = dot(f.LX, md);
+      float u1 = c1 * 0.5f + 0.5f, u2 = c2 * 0.5f + 0.5f;
+      float v = angle / kLutAngle;
+      float h0 = bilinear_clamp(t.lut, kLut, kLut, u1, v);
+      float h1 = bilinear_clamp(t.lut, kLut, kLut, u2, v);
+      xh[i] = logf(h0 * h1 + 1.0f);
+    }
+    xs[i] = shadow_tr(t, p, f.LX, max(mip - 1, 0));
+  }
+}
+
+// GetMatrixFromNormal (core/render.cuh:355-369), rejection capped at 64 tries.
+__device__ __forceinline__ void frame_from(Rng& rng, F3 v1, F3& a, F3& b, F3& c) {
+  v1 = normalize(v1);
+  for (int tries = 0; tries < 64; ++tries) {
+    float ex = rng.next();
+    float ey = rng.next();
+    F3 r = uniform_sphere(ex, ey);
+    if (fabsf(dot(r, v1)) < 0.01f) continue;
+    F3 v2 = normalize(cross(v1, r));
+    a = v1; b = v2; c = cross(v2, v1);
+    return;
+  }
+  F3 r = fabsf(v1.x) < 0.5f ? f3(1, 0, 0) : f3(0, 1, 0);
+  F3 v2 = normalize(cross(v1, r));
+  a = v1; b = v2; c = cross(v2, v1);
+}
+
+// Active-pixel record written by the trace kernel (SoA for coalescing).
+struct Records {
+  int* pix;        // n
+  float* pos;      // 3n
+  float* frame;    // 12n: X, Y, Z, LX
+  float* trph;     // n
+  unsigned* count; // 1
+};
+
+struct NNTraceArgs {
+  Medium m;
+  PathScene sc;
+  CameraModel cam;
+  uint32_t seed, frame_index;
+  float* out;
+  Records rec;
+  unsigned long long* counters;
+};
+
+// Warp-aggregated slot allocation in a 32-bit counter.
+__device__ __forceinline__ unsigned claim_slot(unsigned* counter) {
+  unsigned mask = __activemask();
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(mask) - 1;
+  unsigned base = 0;
+  if (lane == leader) base = atomicAdd(counter, (unsigned)__popc(mask));
+  base = __shfl_sync(mask, base, leader);
+  return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+__global__ void __launch_bounds__(128) k_nn_trace(NNTraceArgs a) {
+  int pix = blockIdx.x * blockDim.x + threadIdx.x;
+  int npx = a.cam.width * a.cam.height;
+  TrackStats st{0, 0};
+  unsigned act = 0;
+  if (pix < npx) {
+    int row = pix / a.cam.width, col = pix - row * a.cam.width;
+    Rng rng;
+    rng.init(a.seed, (uint32_t)pix, a.frame_index, TAG_NN);
+    float jx = rng.next(), jy = rng.next();
+    F3 dir = camera_dir(a.cam, row, col, jx, jy);
+    // GetSamplePoint (core/render.cuh:174-198)
+    bool active = false;
+    F3 pos = f3(0, 0, 0);
+    float dis = ray_box_offset(a.cam.ori, dir);
+    if (dis >= 0) {
+      F3 sp = a.cam.ori + dir * dis;
+      float maxd = ray_box_distance(sp, dir);
+      F3 p0, p1;
+      active = next_vertex(a.m, rng, a.sc.alpha, 0.0f, sp, dir, maxd, p0, p1, st);
+      if (active) pos = p0;
+    }
+    Frame f;
+    F3 ly, lz;
+    frame_from(rng, dir, f.X, f.Y, f.Z);
+    frame_from(rng, a.sc.L, f.LX, ly, lz);
+    if (!active) {
+      a.out[3 * (size_t)pix + 0] = fmaxf(a.sc.env.x, 0.0f);
+      a.out[3 * (size_t)pix + 1] = fmaxf(a.sc.env.y, 0.0f);
+      a.out[3 * (size_t)pix + 2] = fmaxf(a.sc.env.z, 0.0f);
+    } else {
+      float d2 = ray_box_distance(pos, f.LX);
+      float ph = hg_phase(dot(f.X, f.LX), a.sc.g);
+      float tr = transmittance(a.m, rng, pos, f.LX, d2, a.sc.alpha, st) * ph;
+      unsigned k = claim_slot(a.rec.count);
+      a.rec.pix[k] = pix;
+      a.rec.pos[3 * (size_t)k + 0] = pos.x;
+      a.rec.pos[3 * (size_t)k + 1] = pos.y;
+      a.rec.pos[3 * (size_t)k + 2] = pos.z;
+      float* fr = a.rec.frame + 12 * (size_t)k;
+      fr[0] = f.X.x; fr[1] = f.X.y; fr[2] = f.X.z;
+      fr[3] = f.Y.x; fr[4] = f.Y.y; fr[5] = f.Y.z;
+      fr[6] = f.Z.x; fr[7] = f.Z.y; fr[8] = f.Z.z;
+      fr[9] = f.LX.x; fr[10] = f.LX.y; fr[11] = f.LX.z;
+      a.rec.trph[k] = tr;
+      act = 1;
+    }
+  }
+  unsigned fsum = st.fetches, csum = st.caps;
+  for (int o = 16; o; o >>= 1) {
+    fsum += __shfl_xor_sync(0xffffffffu, fsum, o);
+    csum += __shfl_xor_sync(0xffffffffu, csum, o);
+    act += __shfl_xor_sync(0xffffffffu, act, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(a.counters + 0, (unsigned long long)fsum);
+    if (csum) atomicAdd(a.counters + 2, (unsigned long long)csum);
+    atomicAdd(a.counters + 3, (unsigned long long)act);
+  }
+}
+
+struct NNPredictArgs {
+  Tables t;
+  const float* __restrict__ w;
+  const float* __restrict__ stencil;
+  Records rec;
+  int capacity;
+  F3 L, light_color, scatter;
+  float alpha, g;
+  float* out;
+};
+
+inline __device__ Frame load_frame(const float* fr) {
+  Frame f;
+  f.X = f3(fr[0], fr[1], fr[2]);
+  f.Y = f3(fr[3], fr[4], fr[5]);
+  f.Z = f3(fr[6], fr[7], fr[8]);
+  f.LX = f3(fr[9], fr[10], fr[11]);
+  return f;
+}
+
+// Gather + per-thread network, one active record per thread.
+__global__ void __launch_bounds__(64) k_nn_predict_simt(NNPredictArgs a) {
+  unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned n = min(*a.rec.count, (unsigned)a.capacity);
+  if (k >= n) return;
+  NetSIMT s;
+  F3 pos = f3(a.rec.pos[3 * (size_t)k], a.rec.pos[3 * (size_t)k + 1], a.rec.pos[3 * (size_t)k + 2]);
+  Frame f = load_frame(a.rec.frame + 12 * (size_t)k);
+  gather_point(a.t, a.stencil, pos, a.L, f, a.alpha, a.g, s.xv, s.xs, s.xh);
+  F3 sr = a.scatter / 1.001f;
+  float gamma = acosf(dot(f.X, f.LX));
+  n_trunks(s, a.w, a.g, gamma);
+  F3 pred = n_heads(s, a.w, srp_of(sr));
+  pred = pred + a.rec.trph[k];
+  F3 o = vmax((pred * a.light_color) * a.scatter, f3(0, 0, 0));
+  int pix = a.rec.pix[k];
+  a.out[3 * (size_t)pix + 0] = o.x;
+  a.out[3 * (size_t)pix + 1] = o.y;
+  a.out[3 * (size_t)pix + 2] = o.z;
+}
+
+// Gather only, for explicit points and frames (test / training entry).
+__global__ void k_gather(Tables t, const float* __restrict__ stencil, const float* __restrict__ pos,
+                         const float* __restrict__ frame, int n, F3 L, float alpha, float g, F3 srp,
+                         float* __restrict__ desc, float* __restrict__ aux) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  float xv[192], xs[192], xh[192];
+  Frame f = load_frame(frame + 12 * (size_t)k);
+  gather_point(t, stencil, f3(pos[3 * k], pos[3 * k + 1], pos[3 * k + 2]), L, f, alpha, g, xv, xs, xh);
+  float* d = desc + 576 * (size_t)k;
+  for (int i = 0; i < 192; ++i) { d[i] = xv[i]; d[192 + i] = xs[i]; d[384 + i] = xh[i]; }
+  float* ax = aux + 5 * (size_t)k;
+  ax[0] = g;
+  ax[1] = acosf(dot(f.X, f.LX));
+  ax[2] = srp.x; ax[3] = srp.y; ax[4] = srp.z;
+}
+
+// Network only on descriptors (desc n x 576, aux n x 5).
+__global__ void __launch_bounds__(64) k_predict_simt(const float* __restrict__ w, const float* __restrict__ desc,
+                                                     const float* __restrict__ aux, int n, float* __restrict__ out) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  NetSIMT s;
+  const float* d = desc + 576 * (size_t)k;
+  for (int i = 0; i < 192; ++i) { s.xv[i] = d[i]; s.xs[i] = d[192 + i]; s.xh[i] = d[384 + i]; }
+  const float* ax = aux + 5 * (size_t)k;
+  n_trunks(s, w, ax[0], ax[1]);
+  F3 r = n_heads(s, w, f3(ax[2], ax[3], ax[4]));
+  out[3 * (size_t)k + 0] = r.x;
+  out[3 * (size_t)k + 1] = r.y;
+  out[3 * (size_t)k + 2] = r.z;
+}
+
+extern int check_params(const mr_render_params* p);
+extern CameraModel make_camera(const mr_render_params* p);
+extern PathScene make_path_scene(const mr_render_params* p);
+
+static size_t records_bytes(size_t n) { return n * (sizeof(int) + 16 * sizeof(float)) + 256; }
+
+static Records carve_records(void* base, size_t n) {
+  char* p = (char*)base;
+  Records r;
+  r.count = (unsigned*)p; p += 256;
+  r.pix = (int*)p; p += n * sizeof(int);
+  r.pos = (float*)p; p += 3 * n * sizeof(float);
+  r.frame = (float*)p; p += 12 * n * sizeof(float);
+  r.trph = (float*)p;
+  return r;
+}
+
+int render_neural(Volume* v, const Network* net, const mr_render_params* p, float* dev_rgb, cudaStream_t s) {
+  if (!net) return set_error(MR_ERR_ARG, "MRPNN render needs a network (mr_network_create)");
+  if (!v->data_set) return set_error(MR_ERR_STATE, "render before mr_volume_set_data");
+  if (!v->mips_valid) return set_error(MR_ERR_STATE, "render before mr_volume_update");
+  if (p->precision != MR_PREC_FP32) return set_error(MR_ERR_UNSUPPORTED, "precision %d not built", p->precision);
+  F3 L = normalize(to_f3(p->light_dir));
+  // UpdateHGLut / Update_TR on demand (core/volume.cu:434-437).
+  if (!v->lut_valid || v->lut_g != p->g || v->lut_seed != p->seed) {
+    int rc = launch_update_lut(v, p->g, p->seed, s);
+    if (rc) return rc;
+  }
+  if (!v->tr_valid || L.x != v->tr_light.x || L.y != v->tr_light.y || L.z != v->tr_light.z || p->alpha != v->tr_alpha) {
+    int rc = launch_update_tr(v, L, p->alpha, s);
+    if (rc) return rc;
+  }
+  size_t npx = (size_t)p->width * p->height;
+  int rc = ensure_scratch(v, records_bytes(npx), s);
+  if (rc) return rc;
+  Records rec = carve_records(v->scratch, npx);
+  MR_CUDA(cudaMemsetAsync(v->d_counters, 0, kCounters * sizeof(unsigned long long), s));
+  MR_CUDA(cudaMemsetAsync(rec.count, 0, sizeof(unsigned), s));
+  NNTraceArgs ta;
+  ta.m = Medium{v->density, v->res, v->max_density, p->tr_scale};
+  ta.sc = make_path_scene(p);
+  ta.cam = make_camera(p);
+  ta.seed = p->seed;
+  ta.frame_index = p->sample_offset;
+  ta.out = dev_rgb;
+  ta.rec = rec;
+  ta.counters = v->d_counters;
+  v->timer.mark(ST_NN_TRACE, s);
+  k_nn_trace<<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(ta);
+  v->timer.mark(ST_NN_TRACE, s);
+  MR_CUDA(cudaGetLastError());
+  NNPredictArgs pa;
+  pa.t = Tables{v->mips, v->tr, v->lut};
+  pa.w = net->w;
+  pa.stencil = net->stencil;
+  pa.rec = rec;
+  pa.capacity = (int)npx;
+  pa.L = L;
+  pa.light_color = to_f3(p->light_color);
+  pa.scatter = to_f3(p->scatter_rate);
+  pa.alpha = p->alpha;
+  pa.g = p->g;
+  pa.out = dev_rgb;
+  v->timer.mark(ST_NN_PREDICT, s);
+  k_nn_predict_simt<<<(unsigned)((npx + 63) / 64), 64, 0, s>>>(pa);
+  v->timer.mark(ST_NN_PREDICT, s);
+  MR_CUDA(cudaGetLastError());
+  return MR_OK;
+}
+
+}  // namespace mr
+
+using namespace mr;
+
+extern "C" int mr_gather_descriptors(const mr_volume* h, const mr_network* nh, const float* dev_pos,
+                                     const float* dev_frame, int32_t n, float alpha, float g,
+                                     mr_float3 scatter_rate, float* dev_desc, float* dev_aux, void* stream) {
+  clear_error();
+  if (!h || !nh || !dev_pos || !dev_frame || !dev_desc || !dev_aux)
+    return set_error(MR_ERR_ARG, "mr_gather_descriptors: NULL argument");
+  if (n < 0) return set_error(MR_ERR_ARG, "n < 0");
+  if (n == 0) return MR_OK;
+  const Volume* v = &h->v;
+  if (!v->mips_valid || !v->tr_valid || !v->lut_valid)
+    return set_error(MR_ERR_STATE, "gather needs mr_volume_update, _update_tr and _update_hglut first");
+  F3 sr = to_f3(scatter_rate) / 1.001f;
+  k_gather<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(Tables{v->mips, v->tr, v->lut}, nh->n.stencil,
+                                                            dev_pos, dev_frame, n, v->tr_light, alpha, g,
+                                                            srp_of(sr), dev_desc, dev_aux);
+  MR_CUDA(cudaGetLastError());
+  return MR_OK;
+}
+
+extern "C" int mr_radiance_predict(const mr_network* nh, int32_t precision, const float* dev_desc,
+                                   const float* dev_aux, int32_t n, float* dev_out, void* stream) {
+  clear_error();
+  if (!nh || !dev_desc || !dev_aux || !dev_out) return set_error(MR_ERR_ARG, "mr_radiance_predict: NULL argument");
+  if (n < 0) return set_error(MR_ERR_ARG, "n < 0");
+  if (n == 0) return MR_OK;
+  if (precision != MR_PREC_FP32) return set_error(MR_ERR_UNSUPPORTED, "precision %d not built", precision);
+  k_predict_simt<<<(n + 63) / 64, 64, 0, (cudaStream_t)stream>>>(nh->n.w, dev_desc, dev_aux, n, dev_out);
+  MR_CUDA(cudaGetLastError());
+  return MR_OK;
+}

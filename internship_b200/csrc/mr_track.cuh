@@ -1,0 +1,140 @@
+// Woodcock delta tracking on a raw fp32 density grid: free flight, NEE
+// transmittance and the path estimator (core/render.cuh:93-258).
+#pragma once
+#include "mr_device.cuh"
+
+namespace mr {
+
+struct Medium {
+  const float* __restrict__ density;  // res^3, x-major
+  int res;
+  float max_density;  // global majorant (before alpha)
+  float tr_scale;
+};
+
+struct TrackStats {
+  unsigned fetches;
+  unsigned caps;
+};
+
+__device__ __forceinline__ float fetch_density(const Medium& m, F3 pos, TrackStats& st) {
+  ++st.fetches;
+  return tri_border(m.density, m.res, pos + 0.5f);
+}
+
+// DeterminateNextVertex (core/render.cuh:138-172).
+__device__ __forceinline__ bool next_vertex(const Medium& m, Rng& rng, float alpha, float g, F3 pos, F3 dir,
+                                            float dis, F3& npos, F3& ndir, TrackStats& st) {
+  float smax = m.max_density * alpha;
+  float t = 0;
+  int loop = 0;
+  bool capped = true;
+  while (loop++ < 10000) {
+    float rk = rng.next();
+    t -= logf(1 - rk) / smax;
+    if (t > dis) { npos = f3(0, 0, 0); ndir = f3(0, 0, 0); return false; }
+    rk = rng.next();
+    float d = fetch_density(m, pos + (dir * t), st);
+    float s = d * alpha;
+    if (s / smax > rk) { capped = false; break; }
+    if (d < 0) t -= d;
+  }
+  if (capped) ++st.caps;
+  float e0 = rng.next();
+  float e1 = rng.next();
+  ndir = hg_sample_dir(e0, e1, dir, g);
+  npos = (dir * t) + pos;
+  return true;
+}
+
+// Tr (core/render.cuh:93-136): ratio tracking while tr > 0.5, then delta tracking.
+__device__ __forceinline__ float transmittance(const Medium& m, Rng& rng, F3 pos, F3 dir, float dis, float alpha,
+                                               TrackStats& st) {
+  float smax = m.max_density * alpha;
+  float tr = 1, t = 0;
+  int loop = 0;
+  while (loop++ < 10000 && tr > 0.5f) {
+    float rk = rng.next();
+    t -= logf(1 - rk) / smax * m.tr_scale;
+    if (t > dis) break;
+    float d = fetch_density(m, pos + (dir * t), st);
+    float s = d * alpha;
+    tr *= 1 - fmaxf(0.0f, s / smax);
+    if (d < 0) t -= d;
+  }
+  while (loop++ < 10000 && tr > 0.001f) {
+    float rk = rng.next();
+    t -= logf(1 - rk) / smax * m.tr_scale;
+    if (t > dis) break;
+    float d = fetch_density(m, pos + (dir * t), st);
+    float s = d * alpha;
+    if (rng.next() < fmaxf(0.0f, s / smax)) { tr = 0; break; }
+    if (d < 0) t -= d;
+  }
+  if (loop > 10000) ++st.caps;
+  return tr;
+}
+
+struct PathScene {
+  F3 L;            // normalized light direction
+  F3 light_color;
+  F3 scatter;      // albedo per channel
+  F3 env;          // radiance of escaped rays
+  float alpha, g;
+  int max_bounces;
+};
+
+// CalculateRadiance (core/render.cuh:200-258), one sample.
+__device__ __forceinline__ F3 path_radiance(const Medium& m, const PathScene& sc, Rng& rng, F3 ori, F3 dir,
+                                            float* first_t, TrackStats& st) {
+  dir = normalize(dir);
+  float t = -1;
+  float dis = ray_box_offset(ori, dir);
+  if (dis < 0) { *first_t = t; return sc.env; }
+  F3 res = f3(0, 0, 0);
+  F3 pos = ori + dir * dis;
+  F3 rd = dir;
+  F3 rate = f3(1, 1, 1);
+  for (int s = 0; s < sc.max_bounces; ++s) {
+    F3 np, nd;
+    float maxd = ray_box_distance(pos, rd);
+    bool hit = next_vertex(m, rng, sc.alpha, sc.g, pos, rd, maxd, np, nd, st);
+    if (!hit) { res = res + sc.env * rate; break; }
+    if (s == 0) t = length(ori - np);
+    pos = np;
+    rate = rate * sc.scatter;
+    maxd = ray_box_distance(pos, sc.L);
+    float ph = hg_phase(dot(rd, sc.L), sc.g);
+    res = res + (sc.light_color * rate) * (transmittance(m, rng, pos, sc.L, maxd, sc.alpha, st) * ph);
+    rd = nd;
+  }
+  *first_t = t;
+  return res;
+}
+
+struct CameraModel {
+  F3 ori, fwd, up, right;
+  int width, height;
+};
+
+// Camera ray of pixel (row, col) (core/volume.cu:155-163, row-major W x H).
+__device__ __forceinline__ F3 camera_dir(const CameraModel& c, int row, int col, float jx, float jy) {
+  float u = 1.0f - ((float)col + jx) / (float)c.width;
+  float v = 1.0f - ((float)row + jy) / (float)c.height;
+  F3 d = c.fwd + (c.right * (u * 2 - 1)) + (c.up * (v * 2 - 1));
+  return normalize(d);
+}
+
+// Warp-aggregated claim of one work item per calling lane.
+__device__ __forceinline__ unsigned long long claim_work(unsigned long long* counter) {
+  unsigned mask = __activemask();
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(mask) - 1;
+  unsigned lt = mask & ((1u << lane) - 1u);
+  unsigned long long base = 0;
+  if (lane == leader) base = atomicAdd(counter, (unsigned long long)__popc(mask));
+  base = __shfl_sync(mask, base, leader);
+  return base + __popc(lt);
+}
+
+}  // namespace mr

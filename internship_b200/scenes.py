@@ -1,0 +1,111 @@
+"""Benchmark and test scenes (synthetic, seeded).
+
+sphere_scene  : 128^3 solid sphere (centre 0.5, radius 0.25, density 1),
+                extinction scale 64, albedo 0.99, HG g = 0.857, one unit
+                directional light with a seeded direction, camera at distance
+                2.5 looking at the centre with a 40 degree field of view,
+                256 x 256, 64 spp, up to 512 bounces, Philox seed 0.
+cloud_scene   : 512^3 seeded Perlin-fBm cloud (6 octaves, base frequency 4,
+                lacunarity 2, gain 0.5, threshold 0.45, radial falloff) with
+                the sphere scene's light, medium and camera at 1920 x 1080.
+"""
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import RenderParams, check, f3
+
+M0, M1, W0, W1 = 0xD2511F53, 0xCD9E8D57, 0x9E3779B9, 0xBB67AE85
+
+
+def philox4x32_10(ctr, key):
+    """Philox4x32-10 (Salmon et al., SC'11) on python ints."""
+    c = [int(x) & 0xFFFFFFFF for x in ctr]
+    k0, k1 = int(key[0]) & 0xFFFFFFFF, int(key[1]) & 0xFFFFFFFF
+    for r in range(10):
+        if r:
+            k0, k1 = (k0 + W0) & 0xFFFFFFFF, (k1 + W1) & 0xFFFFFFFF
+        p0, p1 = M0 * c[0], M1 * c[2]
+        c = [((p1 >> 32) ^ c[1] ^ k0) & 0xFFFFFFFF, p1 & 0xFFFFFFFF, ((p0 >> 32) ^ c[3] ^ k1) & 0xFFFFFFFF,
+             p0 & 0xFFFFFFFF]
+    return c
+
+
+def u01(x):
+    return ((x >> 9) + 0.5) * 1.1920928955078125e-7
+
+
+def seeded_light(seed=0):
+    """Uniform direction on the sphere from Philox(seed; 0, 0, 0, 8)."""
+    w = philox4x32_10([0, 0, 0, 8], [seed, 0])
+    ex, ey = u01(w[0]), u01(w[1])
+    phi = 2 * math.pi * ex
+    ct = 1 - 2 * ey
+    st = math.sqrt(max(0.0, 1 - ct * ct))
+    return (st * math.cos(phi), st * math.sin(phi), ct)
+
+
+def camera_vectors(position, fov_deg):
+    """Camera::SetPosition (core/camera.cu:173-189), right/up scaled by
+    tan(fov/2) as VolumeRender::Render expects."""
+    ori = np.asarray(position, np.float64)
+    fwd = -ori / np.linalg.norm(ori)
+    right = np.cross([0.0, 1.0, 0.0], fwd)
+    right /= np.linalg.norm(right)
+    up = np.cross(fwd, right)
+    s = math.tan(math.radians(fov_deg) / 2)
+    return tuple(ori), tuple(up * s), tuple(right * s)
+
+
+def sphere_density(res=128):
+    i = (np.arange(res) + 0.5) / res
+    x, y, z = np.meshgrid(i, i, i, indexing="ij")
+    d = np.sqrt((x - 0.5) ** 2 + (y - 0.5) ** 2 + (z - 0.5) ** 2)
+    return (d < 0.25).astype(np.float32)
+
+
+CAMERA_DIR = np.array([1.0, 0.55, 0.8]) / np.linalg.norm([1.0, 0.55, 0.8])
+
+
+def make_params(width, height, spp=1, rt=_lib.RT_PT, bounces=512, seed=0, alpha=64.0, g=0.857, albedo=0.99,
+                distance=2.5, fov=40.0, sample_offset=0, precision=_lib.PREC_FP32, light_seed=0):
+    ori, up, right = camera_vectors(CAMERA_DIR * distance, fov)
+    p = RenderParams()
+    p.width, p.height = width, height
+    p.ori, p.up, p.right = f3(ori), f3(up), f3(right)
+    p.light_dir = f3(seeded_light(light_seed))
+    p.light_color = f3((1.0, 1.0, 1.0))
+    p.alpha, p.g = alpha, g
+    p.scatter_rate = f3((albedo, albedo, albedo))
+    p.tr_scale = 1.0
+    p.env_color = f3((0.0, 0.0, 0.0))
+    p.max_bounces, p.spp = bounces, spp
+    p.seed, p.sample_offset = seed, sample_offset
+    p.render_type, p.precision = rt, precision
+    return p
+
+
+def sphere_scene(width=256, height=256, spp=64, **kw):
+    return sphere_density(128), make_params(width, height, spp, **kw)
+
+
+CLOUD_ARGS = dict(octaves=6, base_freq=4.0, lacunarity=2.0, gain=0.5, threshold=0.45)
+
+
+def generate_cloud_device(res, seed, dev_ptr, stream=None, **over):
+    a = dict(CLOUD_ARGS, **over)
+    check(_lib.load().mr_generate_cloud(res, seed, a["octaves"], a["base_freq"], a["lacunarity"], a["gain"],
+                                        a["threshold"], C.c_void_p(dev_ptr), stream))
+
+
+def cloud_permutation(seed):
+    out = np.zeros(256, np.int32)
+    check(_lib.load().mr_cloud_permutation(seed, out.ctypes.data))
+    return out
+
+
+def cloud_scene_params(width=1920, height=1080, **kw):
+    kw.setdefault("rt", _lib.RT_MRPNN)
+    return make_params(width, height, 1, **kw)

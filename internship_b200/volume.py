@@ -1,0 +1,302 @@
+"""Python mirror of the reference's host API for the cloud-rendering path.
+
+`VolumeRender` and `Camera` keep the names, argument order and meaning of
+core/volume.hpp:45-146 and core/camera.hpp:10-41; every call goes through the
+C ABI of libmrpnn_b200.so. Images are numpy arrays (H, W, 3) float32,
+row-major, top row first.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import MRError, RenderParams, check, f3
+
+PT, RPNN, MRPNN = _lib.RT_PT, _lib.RT_RPNN, _lib.RT_MRPNN
+
+
+def builtin_stencil():
+    out = np.zeros(480, np.float32)
+    check(_lib.load().mr_builtin_stencil(out.ctypes.data, out.size))
+    return out
+
+
+def xavier_weights(seed=1):
+    """Xavier-uniform initial weights in the NNWeight.cuh blob layout."""
+    out = np.zeros(_lib.WEIGHT_TOTAL, np.float32)
+    check(_lib.load().mr_weights_xavier(seed, out.ctypes.data, out.size))
+    return out
+
+
+class Network:
+    """Radiance-predictor weights on the device (the NNWeight.cuh arrays)."""
+
+    def __init__(self, weights, stencil=None):
+        w = np.ascontiguousarray(weights, np.float32).ravel()
+        st = None if stencil is None else np.ascontiguousarray(stencil, np.float32).ravel()
+        if st is not None and st.size != 480:
+            raise ValueError("stencil must have 160 x 3 values")
+        h = C.c_void_p()
+        check(_lib.load().mr_network_create(w.ctypes.data, w.size, None if st is None else st.ctypes.data,
+                                            C.byref(h)))
+        self.handle = h
+        self.weights = w
+
+    def close(self):
+        if self.handle:
+            _lib.load().mr_network_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class VolumeRender:
+    """core/volume.hpp:45-146 on the B200 library."""
+
+    PT, RPNN, MRPNN = PT, RPNN, MRPNN
+
+    def __init__(self, resolution):
+        self.resolution = int(resolution)
+        h = C.c_void_p()
+        check(_lib.load().mr_volume_create(self.resolution, C.byref(h)))
+        self.handle = h
+        self.datas = np.zeros((self.resolution,) * 3, np.float32)
+        self.max_density = 0.00001
+        self.scatter_rate = (1.001, 1.001, 1.001)  # core/render.cuh:16 default
+        self.tr_scale = 1.0
+        self.exposure = 1.0
+        self.env_color = (0.0, 0.0, 0.0)
+        self.network = None
+        self.seed = 0
+
+    # -- data -------------------------------------------------------------
+    def SetData(self, x, y, z, value):
+        self.datas[x, y, z] = value
+
+    def SetDatas(self, func_or_array):
+        """Fill from an array (res^3, x-major) or func(x, y, z, u, v, w)
+        evaluated on the grid with u = (x+0.5)/res (core/omp.cpp:4-18)."""
+        r = self.resolution
+        if callable(func_or_array):
+            i = np.arange(r)
+            x, y, z = np.meshgrid(i, i, i, indexing="ij")
+            u, v, w = (x + 0.5) / r, (y + 0.5) / r, (z + 0.5) / r
+            self.datas = np.asarray(func_or_array(x, y, z, u, v, w), np.float32).reshape(r, r, r)
+        else:
+            a = np.asarray(func_or_array, np.float32)
+            if a.size != r ** 3:
+                raise ValueError("expected %d values" % r ** 3)
+            self.datas = a.reshape(r, r, r).copy()
+
+    def Update(self):
+        L = _lib.load()
+        d = np.ascontiguousarray(self.datas, np.float32)
+        check(L.mr_volume_set_data(self.handle, d.ctypes.data, d.size))
+        check(L.mr_volume_update(self.handle, None))
+        md = C.c_float()
+        check(L.mr_volume_max_density(self.handle, C.byref(md)))
+        self.max_density = md.value
+
+    def Update_TR(self, lightDir, alpha=64.0):
+        check(_lib.load().mr_volume_update_tr(self.handle, f3(lightDir), float(alpha), None))
+
+    def UpdateHGLut(self, g):
+        check(_lib.load().mr_volume_update_hglut(self.handle, float(g), self.seed, None))
+
+    # -- settings (device globals of the reference become render params) ----
+    def SetScatterRate(self, rate):
+        self.scatter_rate = (rate,) * 3 if np.isscalar(rate) else tuple(float(r) for r in rate)
+
+    def SetTrScale(self, scale):
+        self.tr_scale = float(scale)
+
+    def SetExposure(self, exp):
+        self.exposure = float(exp)
+
+    def SetEnvColor(self, color):
+        self.env_color = tuple(float(c) for c in color)
+
+    def SetWeights(self, weights, stencil=None):
+        if self.network is not None:
+            self.network.close()
+        self.network = Network(weights, stencil)
+
+    def SetSeed(self, seed):
+        self.seed = int(seed)
+
+    # -- queries ------------------------------------------------------------
+    def read(self, what, level=0):
+        L = _lib.load()
+        if what == _lib.READ_DENSITY:
+            n = self.resolution ** 3
+        elif what in (_lib.READ_MIP, _lib.READ_VARIANCE):
+            n = (256 >> level) ** 3
+        elif what == _lib.READ_TR:
+            n = (128 >> level) ** 3
+        else:
+            n = 512 * 512
+        out = np.zeros(n, np.float32)
+        check(L.mr_volume_read(self.handle, what, level, out.ctypes.data, n))
+        return out
+
+    def params(self, size, ori, up, right, lightDir, rt=PT, g=0.857, alpha=1.0, lightColor=(1, 1, 1),
+               multiScatter=512, sampleNum=1024, sample_offset=0, precision=_lib.PREC_FP32):
+        p = RenderParams()
+        p.width, p.height = int(size[0]), int(size[1])
+        p.ori, p.up, p.right = f3(ori), f3(up), f3(right)
+        p.light_dir, p.light_color = f3(lightDir), f3(lightColor)
+        p.alpha, p.g = float(alpha), float(g)
+        p.scatter_rate = f3(self.scatter_rate)
+        p.tr_scale = self.tr_scale
+        p.env_color = f3(self.env_color)
+        p.max_bounces, p.spp = int(multiScatter), int(sampleNum)
+        p.seed, p.sample_offset = self.seed, int(sample_offset)
+        p.render_type, p.precision = int(rt), int(precision)
+        return p
+
+    def Render(self, size, ori, up, right, lightDir, rt=PT, g=0.857, alpha=1.0, lightColor=(1, 1, 1),
+               multiScatter=512, sampleNum=1024, precision=_lib.PREC_FP32):
+        """core/volume.cu:410-467: returns the mean radiance image (H, W, 3).
+        Neural renders average `sampleNum` primary samples."""
+        L = _lib.load()
+        w, h = int(size[0]), int(size[1])
+        out = np.zeros((h, w, 3), np.float32)
+        net = self.network.handle if self.network is not None else None
+        if rt == PT:
+            p = self.params(size, ori, up, right, lightDir, rt, g, alpha, lightColor, multiScatter, sampleNum,
+                            precision=precision)
+            check(L.mr_render_host(self.handle, net, C.byref(p), out.ctypes.data))
+            return out
+        acc = np.zeros_like(out, np.float64)
+        for s in range(sampleNum):
+            p = self.params(size, ori, up, right, lightDir, rt, g, alpha, lightColor, multiScatter, 1,
+                            sample_offset=s, precision=precision)
+            check(L.mr_render_host(self.handle, net, C.byref(p), out.ctypes.data))
+            acc += out
+        return (acc / sampleNum).astype(np.float32)
+
+    def close(self):
+        if self.handle:
+            _lib.load().mr_volume_destroy(self.handle)
+            self.handle = None
+        if self.network is not None:
+            self.network.close()
+            self.network = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---- tone mapping and image output (core/camera.cu:10-160) --------------------
+_SRGB_2_AP0 = np.array([[0.4397010, 0.3829780, 0.1773350], [0.0897923, 0.8134230, 0.0967616],
+                        [0.0175440, 0.1115440, 0.8707040]], np.float64)
+_AP0_2_AP1 = np.array([[1.4514393161, -0.2365107469, -0.2149285693], [-0.0765537734, 1.1762296998, -0.0996759264],
+                       [0.0083161484, -0.0060324498, 0.9977163014]], np.float64)
+_AP1_2_XYZ = np.array([[0.6624541811, 0.1340042065, 0.1561876870], [0.2722287168, 0.6740817658, 0.0536895174],
+                       [-0.0055746495, 0.0040607335, 1.0103391003]], np.float64)
+_XYZ_2_AP1 = np.array([[1.6410233797, -0.3248032942, -0.2364246952], [-0.6636628587, 1.6153315917, 0.0167563477],
+                       [0.0117218943, -0.0082844420, 0.9883948585]], np.float64)
+_D60_2_D65 = np.array([[0.98722400, -0.00611327, 0.0159533], [-0.00759836, 1.00186000, 0.0053302],
+                       [0.00307257, -0.00509595, 1.0816800]], np.float64)
+_XYZ_2_709 = np.array([[3.2409699419, -1.5373831776, -0.4986107603], [-0.9692436363, 1.8759675015, 0.0415550574],
+                       [0.0556300797, -0.2039769589, 1.0569715142]], np.float64)
+_AP1_Y = np.array([0.272229, 0.674082, 0.0536895])
+
+
+def tone_gamma(c):
+    return np.power(np.maximum(c, 0), 1.0 / 2.2)
+
+
+def tone_none(c):
+    return c
+
+
+def tone_aces(c):
+    """ACES RRT+ODT fit with dim-surround and desaturation steps
+    (core/camera.cu:74-160 / core/render.cuh:640-732), on (..., 3) arrays."""
+    c = np.asarray(c, np.float64)
+    acescg = c @ (_AP0_2_AP1 @ _SRGB_2_AP0).T
+    y = acescg @ _AP1_Y
+    acescg = y[..., None] * (1 - 0.96) + acescg * 0.96
+    x = acescg
+    post = (x * (x * 278.5085 + 10.7772)) / (x * (x * 293.6045 + 88.7122) + 80.6889)
+    xyz = post @ _AP1_2_XYZ.T
+    div = np.maximum(xyz.sum(-1), 1e-4)
+    xx, yy = xyz[..., 0] / div, xyz[..., 1] / div
+    Y = np.minimum(np.maximum(xyz[..., 1], 0.0), 65504.0) ** 0.9811
+    m = Y / np.maximum(yy, 1e-4)
+    xyz = np.stack([xx * m, Y, (1.0 - xx - yy) * m], -1)
+    lin = xyz @ _XYZ_2_AP1.T
+    y = lin @ _AP1_Y
+    lin = y[..., None] * (1 - 0.93) + lin * 0.93
+    out = lin @ (_XYZ_2_709 @ _D60_2_D65 @ _AP1_2_XYZ).T
+    return np.power(np.maximum(out, 0), 1.0 / 2.2).astype(np.float32)
+
+
+def save_bmp(path, rgb8):
+    """32-bit top-down BMP (core/camera.cu:10-64); `path` gets ".bmp" appended."""
+    h, w, _ = rgb8.shape
+    bgra = np.empty((h, w, 4), np.uint8)
+    bgra[..., 0], bgra[..., 1], bgra[..., 2], bgra[..., 3] = rgb8[..., 2], rgb8[..., 1], rgb8[..., 0], 255
+    header = bytearray(54)
+    header[0:2] = b"BM"
+    header[2:6] = int(w * h * 4 + 54).to_bytes(4, "little")
+    header[10] = 0x36
+    header[14] = 0x28
+    header[18:22] = int(w).to_bytes(4, "little", signed=True)
+    header[22:26] = int(-h).to_bytes(4, "little", signed=True)
+    header[26] = 1
+    header[28] = 32
+    header[34:38] = int(w * h * 4).to_bytes(4, "little")
+    with open(path + ".bmp", "wb") as f:
+        f.write(bytes(header))
+        f.write(bgra.tobytes())
+
+
+class Camera:
+    """core/camera.hpp:10-41: position on a sphere around the volume, 90 degree
+    field of view (unit right/up) unless `fov_deg` is given."""
+
+    def __init__(self, volume, name="test camera", position=(0.75, 0.75, 0.75), resolution=512, fov_deg=90.0):
+        self.volume = volume
+        self.name = name
+        self.resolution = int(resolution)
+        self.fov_deg = float(fov_deg)
+        self.SetPosition(position)
+
+    def SetPosition(self, position):
+        ori = np.asarray(position, np.float64)
+        fwd = -ori / np.linalg.norm(ori)
+        right = np.cross([0.0, 1.0, 0.0], fwd)
+        right /= np.linalg.norm(right)
+        up = np.cross(fwd, right)
+        if ori[0] == 0 and ori[2] == 0:  # core/camera.cu:178-188
+            right = np.array([1.0, 0, 0])
+            up = np.array([0, 0, 1.0]) if ori[1] > 0 else np.array([0, 0, -1.0])
+        self.ori, self.forward, self.right, self.up = ori, fwd, right, up
+
+    def GetPosition(self):
+        return self.ori
+
+    def _scaled(self):
+        s = np.tan(np.radians(self.fov_deg) / 2)
+        return self.up * s, self.right * s
+
+    def Render(self, lightDir, lightColor=(1, 1, 1), alpha=1.0, multiScatter=1, g=0.0, sampleNum=1, rt=PT):
+        up, right = self._scaled()
+        return self.volume.Render((self.resolution, self.resolution), self.ori, up, right, lightDir, rt, g, alpha,
+                                  lightColor, multiScatter, sampleNum)
+
+    def RenderToFile(self, path, lightDir, lightColor=(1, 1, 1), alpha=1.0, multiScatter=1, g=0.0, sampleNum=1,
+                     tone=tone_aces, rt=PT, exp=1.0):
+        img = self.Render(lightDir, lightColor, alpha, multiScatter, g, sampleNum, rt)
+        t = np.clip(tone(img * exp), 0.0, 1.0)
+        save_bmp(path, (t * 255).astype(np.uint8))
+        return img

@@ -1,0 +1,875 @@
+// CPU oracle for the MRPNN cloud-rendering path - TEST INFRASTRUCTURE ONLY.
+//
+// A plain C++17 restatement of the reference's algorithm (citations are
+// paths relative to the reference project). Only the tests, the smoke check
+// and the CPU-baseline leg of bench.py load this library; the product never
+// does. The random-number source is Philox4x32-10 with the stream layout the
+// CUDA kernels use, so oracle and kernels follow the same paths.
+#include "mr_oracle_math.hpp"
+
+#include <omp.h>
+
+#include <atomic>
+#include <vector>
+
+#include "../include/mrpnn_b200.h"
+#include "../include/mrpnn_weights.h"
+
+using namespace orc;
+
+namespace {
+
+// ---- samplers -------------------------------------------------------------
+// core/volume.cu:675-703 trilinear with zero border; normalized coordinates
+// with texel centres at (i+0.5)/res (the cudaFilterModeLinear convention).
+inline float tap_border(const float* d, int res, int x, int y, int z) {
+  if (x < 0 || y < 0 || z < 0 || x >= res || y >= res || z >= res) return 0.0f;
+  return d[((size_t)x * res + y) * res + z];
+}
+inline float tri_border(const float* d, int res, V3 uv) {
+  float px = uv.x * res - 0.5f, py = uv.y * res - 0.5f, pz = uv.z * res - 0.5f;
+  float fx = std::floor(px), fy = std::floor(py), fz = std::floor(pz);
+  int x = (int)fx, y = (int)fy, z = (int)fz;
+  float wx = px - fx, wy = py - fy, wz = pz - fz;
+  float c000 = tap_border(d, res, x, y, z), c001 = tap_border(d, res, x, y, z + 1);
+  float c010 = tap_border(d, res, x, y + 1, z), c011 = tap_border(d, res, x, y + 1, z + 1);
+  float c100 = tap_border(d, res, x + 1, y, z), c101 = tap_border(d, res, x + 1, y, z + 1);
+  float c110 = tap_border(d, res, x + 1, y + 1, z), c111 = tap_border(d, res, x + 1, y + 1, z + 1);
+  return lerp(lerp(lerp(c000, c001, wz), lerp(c010, c011, wz), wy),
+              lerp(lerp(c100, c101, wz), lerp(c110, c111, wz), wy), wx);
+}
+// Clamp-to-edge addressing (the TR tables are bound with cudaAddressModeClamp,
+// core/volume.cu:1412-1417; host reader SampleClamp :704-722).
+inline float tap_clamp(const float* d, int res, int x, int y, int z) {
+  x = std::max(std::min(x, res - 1), 0);
+  y = std::max(std::min(y, res - 1), 0);
+  z = std::max(std::min(z, res - 1), 0);
+  return d[((size_t)x * res + y) * res + z];
+}
+inline float tri_clamp(const float* d, int res, V3 uv) {
+  float px = uv.x * res - 0.5f, py = uv.y * res - 0.5f, pz = uv.z * res - 0.5f;
+  float fx = std::floor(px), fy = std::floor(py), fz = std::floor(pz);
+  int x = (int)fx, y = (int)fy, z = (int)fz;
+  float wx = px - fx, wy = py - fy, wz = pz - fz;
+  float c000 = tap_clamp(d, res, x, y, z), c001 = tap_clamp(d, res, x, y, z + 1);
+  float c010 = tap_clamp(d, res, x, y + 1, z), c011 = tap_clamp(d, res, x, y + 1, z + 1);
+  float c100 = tap_clamp(d, res, x + 1, y, z), c101 = tap_clamp(d, res, x + 1, y, z + 1);
+  float c110 = tap_clamp(d, res, x + 1, y + 1, z), c111 = tap_clamp(d, res, x + 1, y + 1, z + 1);
+  return lerp(lerp(lerp(c000, c001, wz), lerp(c010, c011, wz), wy),
+              lerp(lerp(c100, c101, wz), lerp(c110, c111, wz), wy), wx);
+}
+// 2-D bilinear, clamp addressing, lut[i + j*W] (u -> i, v -> j).
+inline float bilinear_clamp(const float* d, int w, int h, float u, float v) {
+  float px = u * w - 0.5f, py = v * h - 0.5f;
+  float fx = std::floor(px), fy = std::floor(py);
+  int x = (int)fx, y = (int)fy;
+  float wx = px - fx, wy = py - fy;
+  int x0 = std::max(std::min(x, w - 1), 0), x1 = std::max(std::min(x + 1, w - 1), 0);
+  int y0 = std::max(std::min(y, h - 1), 0), y1 = std::max(std::min(y + 1, h - 1), 0);
+  float a = lerp(d[x0 + y0 * w], d[x1 + y0 * w], wx);
+  float b = lerp(d[x0 + y1 * w], d[x1 + y1 * w], wx);
+  return lerp(a, b, wy);
+}
+
+inline size_t mip_offset(int k) { size_t o = 0; for (int j = 0; j < k; ++j) { size_t r = 256 >> j; o += r * r * r; } return o; }
+inline size_t tr_offset(int k) { size_t o = 0; for (int j = 0; j < k; ++j) { size_t r = 128 >> j; o += r * r * r; } return o; }
+
+struct Vol {
+  const float* density; int res; float max_density;
+  const float* mips;  // concatenated levels 0..8
+  const float* tr;    // concatenated levels 0..7
+  const float* lut;   // 512 x 512
+};
+
+struct Scene {
+  float alpha, g, tr_scale;
+  V3 scatter, light_dir, light_color, env;
+  int max_bounces;
+};
+
+inline V3 f3(const mr_float3& a) { return v3(a.x, a.y, a.z); }
+
+// ---- delta tracking ---------------------------------------------------------
+struct Tracker {
+  const Vol& vol;
+  const Scene& sc;
+  uint64_t fetches = 0;
+  uint64_t caps = 0;
+  float density(V3 pos) { ++fetches; return tri_border(vol.density, vol.res, pos + 0.5f); }
+
+  // core/render.cuh:138-172 DeterminateNextVertex (Woodcock free flight).
+  bool next_vertex(Rng& rng, float alpha, float g, V3 pos, V3 dir, float dis, V3& npos, V3& ndir) {
+    float smax = vol.max_density * alpha;
+    float t = 0;
+    int loop = 0;
+    bool capped = true;
+    while (loop++ < 10000) {
+      float rk = rng.next();
+      t -= std::log(1 - rk) / smax;
+      if (t > dis) { npos = v3(0, 0, 0); ndir = v3(0, 0, 0); return false; }
+      rk = rng.next();
+      float d = density(pos + (dir * t));
+      float s = d * alpha;
+      if (s / smax > rk) { capped = false; break; }
+      if (d < 0) t -= d;
+    }
+    if (capped) ++caps;
+    float e0 = rng.next();
+    float e1 = rng.next();
+    ndir = hg_sample_dir(e0, e1, dir, g);
+    npos = (dir * t) + pos;
+    return true;
+  }
+
+  // core/render.cuh:93-136 Tr: ratio tracking while tr > 0.5, then delta tracking.
+  float transmittance(Rng& rng, V3 pos, V3 dir, float dis, float alpha) {
+    float smax = vol.max_density * alpha;
+    float tr = 1, t = 0;
+    int loop = 0;
+    while (loop++ < 10000 && tr > 0.5f) {
+      float rk = rng.next();
+      t -= std::log(1 - rk) / smax * sc.tr_scale;
+      if (t > dis) break;
+      float d = density(pos + (dir * t));
+      float s = d * alpha;
+      tr *= 1 - std::max(0.0f, s / smax);
+      if (d < 0) t -= d;
+    }
+    while (loop++ < 10000 && tr > 0.001f) {
+      float rk = rng.next();
+      t -= std::log(1 - rk) / smax * sc.tr_scale;
+      if (t > dis) break;
+      float d = density(pos + (dir * t));
+      float s = d * alpha;
+      if (rng.next() < std::max(0.0f, s / smax)) { tr = 0; break; }
+      if (d < 0) t -= d;
+    }
+    if (loop > 10000) ++caps;
+    return tr;
+  }
+
+  // core/render.cuh:200-258 CalculateRadiance (one sample). Returns radiance;
+  // *first_t = distance to the first scattering vertex or -1.
+  V3 radiance(Rng& rng, V3 ori, V3 dir, float* first_t) {
+    dir = normalize(dir);
+    V3 L = normalize(sc.light_dir);
+    float t = -1;
+    float dis = ray_box_offset(ori, dir);
+    if (dis < 0) { *first_t = t; return sc.env; }
+    V3 res = v3(0, 0, 0);
+    V3 pos = ori + dir * dis;
+    V3 rd = dir;
+    V3 rate = v3(1, 1, 1);
+    for (int s = 0; s < sc.max_bounces; ++s) {
+      V3 np, nd;
+      float maxd = ray_box_distance(pos, rd);
+      bool hit = next_vertex(rng, sc.alpha, sc.g, pos, rd, maxd, np, nd);
+      if (!hit) { res = res + sc.env * rate; break; }
+      if (s == 0) t = length(ori - np);
+      pos = np;
+      rate = rate * sc.scatter;
+      maxd = ray_box_distance(pos, L);
+      float ph = hg_phase(dot(rd, L), sc.g);
+      res = res + (sc.light_color * rate) * (transmittance(rng, pos, L, maxd, sc.alpha) * ph);
+      rd = nd;
+    }
+    *first_t = t;
+    return res;
+  }
+};
+
+// Camera ray of pixel (row, col): core/volume.cu:155-163 with the row-major
+// W x H indexing this build defines (u from the column, v from the row).
+inline V3 camera_dir(const mr_render_params& p, int row, int col, float jx, float jy) {
+  float u = 1.0f - ((float)col + jx) / (float)p.width;
+  float v = 1.0f - ((float)row + jy) / (float)p.height;
+  V3 fwd = normalize(-f3(p.ori));
+  V3 d = fwd + (f3(p.right) * (u * 2 - 1)) + (f3(p.up) * (v * 2 - 1));
+  return normalize(d);
+}
+
+Scene make_scene(const mr_render_params& p) {
+  Scene s;
+  s.alpha = p.alpha; s.g = p.g; s.tr_scale = p.tr_scale;
+  s.scatter = f3(p.scatter_rate); s.light_dir = f3(p.light_dir);
+  s.light_color = f3(p.light_color); s.env = f3(p.env_color);
+  s.max_bounces = p.max_bounces;
+  return s;
+}
+
+// ---- network (core/radiancePredict.cu:11-238, 240-294, 370-485) -------------
+struct Net {
+  const float* w[MR_W_COUNT];
+  explicit Net(const float* blob) {
+    size_t off = 0;
+#define MR_BIND(name, n) w[MR_W_##name] = blob + off; off += (n);
+    MR_WEIGHT_LIST(MR_BIND)
+#undef MR_BIND
+  }
+};
+
+inline float relu(float x) { return x >= 0.0f ? x : 0.0f; }
+// AVGMAX (radiancePredict.cu:21-33)
+inline void avgmax(const float* in, float* out, int len, int at, int wa, int wm) {
+  float s = 0.0f, m = -10000.0f;
+  for (int i = 0; i < len; ++i) { s += in[at + i]; m = std::max(m, in[at + i]); }
+  out[wa] = s / (float)len;
+  out[wm] = m;
+}
+// LinearReLU_Unbias (:58-72)
+inline void lin_relu_nobias(const float* in, float* out, int from, int to, int ra, int wa, const float* W) {
+  for (int i = 0; i < to; ++i) {
+    float acc = 0.0f;
+    for (int j = 0; j < from; ++j) acc += in[j + ra] * W[j + i * from];
+    out[i + wa] = relu(acc);
+  }
+}
+// LinearSm_Unbias (:74-86)
+inline void lin_sigmoid_nobias(const float* in, float* out, int from, int to, int ra, int wa, const float* W) {
+  for (int i = 0; i < to; ++i) {
+    float acc = 0.0f;
+    for (int j = 0; j < from; ++j) acc += in[j + ra] * W[j + i * from];
+    out[i + wa] = 1.0f / (1.0f + std::exp(-acc));
+  }
+}
+// LinearReLU (:41-56): bias added after the sum.
+inline void lin_relu_bias_last(const float* in, float* out, int from, int to, int ra, int wa, const float* W, const float* B) {
+  for (int i = 0; i < to; ++i) {
+    float acc = 0.0f;
+    for (int j = 0; j < from; ++j) acc += in[j + ra] * W[j + i * from];
+    acc += B[i];
+    out[i + wa] = relu(acc);
+  }
+}
+// LinearReLU<Size> / LinearReLU_SFL<From,To> (:129-224): bias first, then the
+// products in ascending input order.
+inline void lin_relu(const float* in, float* out, int from, int to, int ra, int wa, const float* W, const float* B) {
+  for (int i = 0; i < to; ++i) {
+    float acc = B[i];
+    for (int j = 0; j < from; ++j) acc += in[j + ra] * W[j + i * from];
+    out[i + wa] = relu(acc);
+  }
+}
+
+struct NetState {
+  float xv[192], xs[192], xh[192];
+  float a[160], b[160], c[160], a2[160], b2[160], c2[160];
+  float pool[75], sew[16], sep[6], tmp[8], comb[128];
+};
+
+enum { POOL = 36, P_DI = 24, DI = 160 };
+
+// SE / SERES block (macros at radiancePredict.cu:240-279). last < 0 = SE.
+void se_block(NetState& s, const Net& n, int last, int from, int to, int size, int pid,
+              int sew0, int sew1, int ww, int trw, int hgw) {
+  avgmax(s.xv, s.pool, size, from, pid + 0, POOL + pid + 0);
+  avgmax(s.xs, s.pool, size, from, pid + 1, POOL + pid + 1);
+  avgmax(s.xh, s.pool, size, from, pid + 2, POOL + pid + 2);
+  for (int i = 0; i < 3; ++i) { s.tmp[i] = s.pool[pid + i]; s.tmp[3 + i] = s.pool[POOL + pid + i]; }
+  lin_relu_nobias(s.tmp, s.sew, 8, 8, 0, 0, n.w[sew0]);
+  lin_sigmoid_nobias(s.sew, s.sep, 8, 3, 0, 0, n.w[sew1]);
+  const float* srcs[3] = {s.xv, s.xs, s.xh};
+  float* xs[3] = {s.a, s.b, s.c};
+  float* ys[3] = {s.a2, s.b2, s.c2};
+  int wid[3] = {ww, trw, hgw};
+  for (int br = 0; br < 3; ++br) {
+    for (int i = 0; i < size; ++i) xs[br][to + i] = srcs[br][from + i];
+    for (int i = 0; i < size; ++i) xs[br][to + i] *= s.sep[br];
+    if (last >= 0)
+      for (int i = 0; i < size; ++i) xs[br][to + i] = xs[br][to + i] + ys[br][last + i];
+    lin_relu(xs[br], ys[br], size, size, to, to, n.w[wid[br]], n.w[wid[br] + 1]);
+  }
+}
+void add3(NetState& s, int from, int to, int size) {
+  for (int i = 0; i < size; ++i) {
+    s.a2[to + i] = s.a2[to + i] + s.xv[from + i];
+    s.b2[to + i] = s.b2[to + i] + s.xs[from + i];
+    s.c2[to + i] = s.c2[to + i] + s.xh[from + i];
+  }
+}
+void rep3(NetState& s, int from, int to, int size) {
+  std::memmove(s.a2 + from, s.a2 + to, size * sizeof(float));
+  std::memcpy(s.a2 + to, s.xv + to, size * sizeof(float));
+  std::memmove(s.b2 + from, s.b2 + to, size * sizeof(float));
+  std::memcpy(s.b2 + to, s.xs + to, size * sizeof(float));
+  std::memmove(s.c2 + from, s.c2 + to, size * sizeof(float));
+  std::memcpy(s.c2 + to, s.xh + to, size * sizeof(float));
+}
+
+#define W_(name) MR_W_##name
+
+// Head SC(p) (radiancePredict.cu:439-473) for one albedo channel.
+float head(NetState& s, const Net& n, float srp_channel) {
+  s.pool[POOL + POOL + 2] = srp_channel;
+  std::memcpy(s.a, s.comb, 120 * sizeof(float));
+  lin_relu_bias_last(s.pool, s.a, 3, 8, POOL + POOL, 120, n.w[W_(LGGSW)], n.w[W_(LGGSB)]);
+  lin_relu_nobias(s.pool, s.sew, 75, 16, 0, 0, n.w[W_(LSEFin1W)]);
+  lin_sigmoid_nobias(s.sew, s.sep, 16, 6, 0, 0, n.w[W_(LSEFin2W)]);
+  for (int i = 0; i < 32; ++i) s.a[i] *= s.sep[0];
+  for (int i = 0; i < 32; ++i) s.a[32 + i] *= s.sep[1];
+  for (int i = 0; i < 32; ++i) s.a[64 + i] *= s.sep[2];
+  for (int i = 0; i < 8; ++i) s.a[96 + i] *= s.sep[3];
+  for (int i = 0; i < 8; ++i) s.a[104 + i] *= s.sep[4];
+  for (int i = 0; i < 8; ++i) s.a[112 + i] *= s.sep[5];
+  lin_relu(s.a, s.b, 128, 128, 0, 0, n.w[W_(LC0W)], n.w[W_(LC0B)]);
+  lin_relu(s.b, s.a, 128, 64, 0, 0, n.w[W_(LC1W)], n.w[W_(LC1B)]);
+  lin_relu(s.a, s.b, 64, 32, 0, 0, n.w[W_(LC2W)], n.w[W_(LC2B)]);
+  lin_relu(s.b, s.a, 32, 16, 0, 0, n.w[W_(LXW)], n.w[W_(LXB)]);
+  const int lx[12] = {W_(LX0W), W_(LX1W), W_(LX2W), W_(LX3W), W_(LX4W), W_(LX5W),
+                      W_(LX6W), W_(LX7W), W_(LX8W), W_(LX9W), W_(LX10W), W_(LX11W)};
+  for (int r = 0; r < 6; ++r) {
+    lin_relu(s.a, s.b, 16, 16, 0, 0, n.w[lx[2 * r]], n.w[lx[2 * r] + 1]);
+    lin_relu(s.b, s.c, 16, 16, 0, 0, n.w[lx[2 * r + 1]], n.w[lx[2 * r + 1] + 1]);
+    for (int i = 0; i < 16; ++i) s.a[i] = s.a[i] + s.c[i];
+  }
+  lin_relu_bias_last(s.a, s.b, 16, 1, 0, 0, n.w[W_(LX12W)], n.w[W_(LX12B)]);
+  return s.b[0];
+}
+
+// Trunks of RadiancePredict (radiancePredict.cu:385-437): fills s.comb and
+// s.pool from the gathered arrays in s.xv/xs/xh.
+void trunks(NetState& s, const Net& n, float g, float gamma) {
+  s.tmp[6] = g;
+  s.tmp[7] = gamma;
+  s.pool[POOL + POOL] = g;
+  s.pool[POOL + POOL + 1] = gamma;
+  // main trunk (:396-421)
+  se_block(s, n, -1, 0, 0, 8, 0, W_(LSE01W), W_(LSE02W), W_(L01W), W_(L_Tr01W), W_(L_Hg01W));
+  add3(s, 0, 0, 8);
+  se_block(s, n, 0, 8, 8, 8, 3, W_(LSE11W), W_(LSE12W), W_(L11W), W_(L_Tr11W), W_(L_Hg11W));
+  rep3(s, 0, 8, 8);
+  se_block(s, n, 0, 16, 16, 16, 6, W_(LSE21W), W_(LSE22W), W_(L21W), W_(L_Tr21W), W_(L_Hg21W));
+  add3(s, 16, 16, 16);
+  se_block(s, n, 16, 32, 32, 16, 9, W_(LSE31W), W_(LSE32W), W_(L31W), W_(L_Tr31W), W_(L_Hg31W));
+  add3(s, 32, 32, 16);
+  se_block(s, n, 32, 48, 48, 16, 12, W_(LSE41W), W_(LSE42W), W_(L41W), W_(L_Tr41W), W_(L_Hg41W));
+  rep3(s, 32, 48, 16);
+  se_block(s, n, 32, 64, 64, 32, 15, W_(LSE51W), W_(LSE52W), W_(L51W), W_(L_Tr51W), W_(L_Hg51W));
+  add3(s, 64, 64, 32);
+  se_block(s, n, 64, 96, 96, 32, 18, W_(LSE61W), W_(LSE62W), W_(L61W), W_(L_Tr61W), W_(L_Hg61W));
+  add3(s, 96, 96, 32);
+  se_block(s, n, 96, 128, 128, 32, 21, W_(LSE71W), W_(LSE72W), W_(L71W), W_(L_Tr71W), W_(L_Hg71W));
+  add3(s, 128, 128, 32);
+  lin_relu(s.a2, s.comb, 32, 32, 128, 0, n.w[W_(L81W)], n.w[W_(L81B)]);
+  lin_relu(s.b2, s.comb, 32, 32, 128, 32, n.w[W_(L_Tr81W)], n.w[W_(L_Tr81B)]);
+  lin_relu(s.c2, s.comb, 32, 32, 128, 64, n.w[W_(L_Hg81W)], n.w[W_(L_Hg81B)]);
+  // light-direction trunk (:424-437)
+  se_block(s, n, -1, DI + 0, 0, 8, P_DI + 0, W_(LDSE01W), W_(LDSE02W), W_(LD01W), W_(LD_Tr01W), W_(LD_Hg01W));
+  add3(s, DI + 0, 0, 8);
+  se_block(s, n, 0, DI + 8, 8, 8, P_DI + 3, W_(LDSE11W), W_(LDSE12W), W_(LD11W), W_(LD_Tr11W), W_(LD_Hg11W));
+  add3(s, DI + 8, 8, 8);
+  se_block(s, n, 8, DI + 16, 16, 8, P_DI + 6, W_(LDSE21W), W_(LDSE22W), W_(LD21W), W_(LD_Tr21W), W_(LD_Hg21W));
+  add3(s, DI + 16, 16, 8);
+  se_block(s, n, 16, DI + 24, 24, 8, P_DI + 9, W_(LDSE31W), W_(LDSE32W), W_(LD31W), W_(LD_Tr31W), W_(LD_Hg31W));
+  add3(s, DI + 24, 24, 8);
+  lin_relu(s.a2, s.comb, 8, 8, 24, 96, n.w[W_(LD41W)], n.w[W_(LD41B)]);
+  lin_relu(s.b2, s.comb, 8, 8, 24, 104, n.w[W_(LD_Tr41W)], n.w[W_(LD_Tr41B)]);
+  lin_relu(s.c2, s.comb, 8, 8, 24, 112, n.w[W_(LD_Hg41W)], n.w[W_(LD_Hg41B)]);
+}
+
+// Heads per distinct albedo channel and the output transform (:475-485).
+// srp = scatterrate^4; channels with equal srp share one head evaluation
+// (x^4 is monotonic on albedos >= 0, so this is the reference's rate test).
+V3 heads(NetState& s, const Net& n, V3 srp) {
+  float X = head(s, n, srp.x), Y, Z;
+  if (srp.y == srp.x) Y = X; else Y = head(s, n, srp.y);
+  if (srp.z == srp.x) Z = X;
+  else if (srp.z == srp.y) Z = Y;
+  else Z = head(s, n, srp.z);
+  return v3(std::max(std::exp(X) - 1.0f, 0.0f) * srp.x, std::max(std::exp(Y) - 1.0f, 0.0f) * srp.y,
+            std::max(std::exp(Z) - 1.0f, 0.0f) * srp.z);
+}
+
+inline V3 srp_of(V3 sr) {
+  return v3((sr.x * sr.x) * (sr.x * sr.x), (sr.y * sr.y) * (sr.y * sr.y), (sr.z * sr.z) * (sr.z * sr.z));
+}
+
+// Network body of RadiancePredict given the gathered arrays;
+// scatterrate = scatter_rate/1.001.
+V3 network(NetState& s, const Net& n, float g, float gamma, V3 scatterrate) {
+  trunks(s, n, g, gamma);
+  return heads(s, n, srp_of(scatterrate));
+}
+
+// ---- descriptor gather (radiancePredict.cu:319-359, renderResources.cu:42-139)
+struct Frame { V3 X, Y, Z, LX; };
+
+inline float mip_density(const Vol& vol, int mip, V3 pos) {
+  return tri_border(vol.mips + mip_offset(mip), 256 >> mip, pos + 0.5f);
+}
+inline float mip_tr(const Vol& vol, int mip, V3 pos) {
+  return tri_clamp(vol.tr + tr_offset(mip), 128 >> mip, pos + 0.5f);
+}
+// ShadowTerm_TRTex (renderResources.cu:121-139), light colour 1.
+inline float shadow_tr(const Vol& vol, V3 p, V3 L, int mip) {
+  if (p.x < -0.5f || p.y < -0.5f || p.z < -0.5f || p.x > 0.5f || p.y > 0.5f || p.z > 0.5f) {
+    float off = ray_box_offset(p, L);
+    if (off >= 0) return mip_tr(vol, mip, p + L * off);
+    return 1.0f;
+  }
+  return mip_tr(vol, mip, p);
+}
+
+void gather(NetState& s, const Vol& vol, const float* stencil, V3 pos, V3 L, const Frame& f,
+            float alpha, float g) {
+  const float kLutAngle = 3.1415926535f * 60.0f / 180.0f;
+  int ri = 0;
+  for (int i = 0; i < 192; ++i) {
+    StencilInfo si = stencil_info(i);
+    float layer = (float)si.mip + 0.1f;
+    V3 p;
+    if (si.type >= 4) {
+      const float* sp = stencil + 3 * ri;
+      ++ri;
+      p = pos + ((f.X * sp[0] + f.Y * sp[1] + f.Z * sp[2]) * si.offset);
+    } else {
+      p = pos + L * si.offset;
+    }
+    int mip = (int)layer;
+    s.xv[i] = std::log(1.0f + alpha * mip_density(vol, mip, p) / 64.0f);
+    if (si.localindex == 0) {
+      s.xh[i] = std::log(hg_phase(dot(f.X, L), g) + 1.0f);
+    } else {
+      V3 md = normalize(p - pos);
+      float radius = (float)(1 << mip) / 256.0f;
+      float angle = std::atan(0.5f * radius / si.offset);
+      float c1 = dot(f.X, md), c2 = dot(f.LX, md);
+      float u1 = c1 * 0.5f + 0.5f, u2 = c2 * 0.5f + 0.5f;
+      float v = angle / kLutAngle;
+      float h0 = bilinear_clamp(vol.lut, 512, 512, u1, v);
+      float h1 = bilinear_clamp(vol.lut, 512, 512, u2, v);
+      s.xh[i] = std::log(h0 * h1 + 1.0f);
+    }
+    s.xs[i] = shadow_tr(vol, p, f.LX, std::max(mip - 1, 0));
+  }
+}
+
+// GetMatrixFromNormal (core/render.cuh:355-369), rejection capped at 64 tries.
+void frame_from(Rng& rng, V3 v1, V3& a, V3& b, V3& c) {
+  v1 = normalize(v1);
+  for (int tries = 0; tries < 64; ++tries) {
+    float ex = rng.next();
+    float ey = rng.next();
+    V3 r = uniform_sphere(ex, ey);
+    if (std::fabs(dot(r, v1)) < 0.01f) continue;
+    V3 v2 = normalize(cross(v1, r));
+    a = v1; b = v2; c = cross(v2, v1);
+    return;
+  }
+  V3 r = std::fabs(v1.x) < 0.5f ? v3(1, 0, 0) : v3(0, 1, 0);
+  V3 v2 = normalize(cross(v1, r));
+  a = v1; b = v2; c = cross(v2, v1);
+}
+
+// NNPredict<MRPNN> for one pixel (core/render.cuh:469-523) without the warp
+// ballot (per-pixel results are identical). Returns radiance; *hit_t set.
+V3 neural_pixel(Tracker& tk, const Net& net, const float* stencil, Rng& rng, V3 ori, V3 dir, float* hit_t) {
+  const Scene& sc = tk.sc;
+  dir = normalize(dir);
+  V3 L = normalize(sc.light_dir);
+  // GetSamplePoint (:174-198)
+  bool active = false;
+  V3 pos = v3(0, 0, 0);
+  float dis = ray_box_offset(ori, dir);
+  if (dis >= 0) {
+    V3 sp = ori + dir * dis;
+    float maxd = ray_box_distance(sp, dir);
+    V3 p0, p1;
+    active = tk.next_vertex(rng, sc.alpha, 0.0f, sp, dir, maxd, p0, p1);
+    if (active) pos = p0;
+  }
+  Frame f;
+  V3 ly, lz;
+  frame_from(rng, dir, f.X, f.Y, f.Z);
+  frame_from(rng, L, f.LX, ly, lz);
+  if (!active) { *hit_t = -1; return sc.env; }
+  NetState s;
+  gather(s, tk.vol, stencil, pos, L, f, sc.alpha, sc.g);
+  V3 scatterrate = sc.scatter / 1.001f;
+  float gamma = std::acos(dot(f.X, f.LX));
+  V3 pred = network(s, net, sc.g, gamma, scatterrate);
+  float d2 = ray_box_distance(pos, f.LX);
+  float ph = hg_phase(dot(f.X, f.LX), sc.g);
+  float tr = tk.transmittance(rng, pos, f.LX, d2, sc.alpha) * ph;
+  pred = pred + tr;
+  *hit_t = length(ori - pos);
+  return (pred * sc.light_color) * sc.scatter;
+}
+
+inline float u01_tag(uint32_t seed, uint32_t a, uint32_t b, uint32_t tag) {
+  Rng r(seed, a, b, tag);
+  return r.next();
+}
+
+}  // namespace
+
+// =============================================================================
+// C ABI (ctypes)
+// =============================================================================
+extern "C" {
+
+void orc_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
+  philox4x32_10(ctr, key[0], key[1], out);
+}
+void orc_uniforms(uint32_t seed, uint32_t a, uint32_t b, uint32_t tag, int n, float* out) {
+  Rng r(seed, a, b, tag);
+  for (int i = 0; i < n; ++i) out[i] = r.next();
+}
+float orc_hg(float c, float g) { return hg_phase(c, g); }
+float orc_hg_sample_cos(float s, float g) { return hg_sample_cos(s, g); }
+void orc_hg_sample_dir(float e0, float e1, const float* v, float g, float* out) {
+  V3 r = hg_sample_dir(e0, e1, v3(v[0], v[1], v[2]), g);
+  out[0] = r.x; out[1] = r.y; out[2] = r.z;
+}
+float orc_ray_box_offset(const float* p, const float* d) { return ray_box_offset(v3(p[0], p[1], p[2]), v3(d[0], d[1], d[2])); }
+float orc_ray_box_distance(const float* p, const float* d) { return ray_box_distance(v3(p[0], p[1], p[2]), v3(d[0], d[1], d[2])); }
+void orc_stencil_info(int i, float* offset, int* mip, int* type, int* localindex) {
+  StencilInfo s = stencil_info(i);
+  *offset = s.offset; *mip = s.mip; *type = s.type; *localindex = s.localindex;
+}
+float orc_sample_border(const float* d, int res, const float* uv) { return tri_border(d, res, v3(uv[0], uv[1], uv[2])); }
+float orc_sample_clamp(const float* d, int res, const float* uv) { return tri_clamp(d, res, v3(uv[0], uv[1], uv[2])); }
+float orc_sample_lut(const float* lut, float u, float v) { return bilinear_clamp(lut, 512, 512, u, v); }
+
+// Update(): intended mip/variance pyramid (core/volume.cu:1228-1287, :775-827).
+// mip0 = trilinear resample (zero border, negatives clamped) to 256^3;
+// mip k+1 = 2x2x2 mean of mip k; var k+1 = max(0, E[x^2] - E[x]^2); var0 = 0.
+// Returns the global majorant max(1e-5, max density) (:1219-1224).
+float orc_build_mips(const float* density, int res, float* mips, float* var, int nthreads) {
+  float md = 0.00001f;
+  size_t n = (size_t)res * res * res;
+  for (size_t i = 0; i < n; ++i) md = std::max(md, density[i]);
+  std::vector<float> clamped(n);
+  for (size_t i = 0; i < n; ++i) clamped[i] = std::max(0.0f, density[i]);
+  float* m0 = mips;
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+  for (int x = 0; x < 256; ++x)
+    for (int y = 0; y < 256; ++y)
+      for (int z = 0; z < 256; ++z) {
+        V3 uv = v3(((float)x + 0.5f) / 256.0f, ((float)y + 0.5f) / 256.0f, ((float)z + 0.5f) / 256.0f);
+        m0[((size_t)x * 256 + y) * 256 + z] = tri_border(clamped.data(), res, uv);
+      }
+  std::memset(var, 0, sizeof(float) * 256 * 256 * 256);
+  for (int k = 0; k < 8; ++k) {
+    int r = 256 >> k, nr = r >> 1;
+    const float* src = mips + mip_offset(k);
+    float* dm = mips + mip_offset(k + 1);
+    float* dv = var + mip_offset(k + 1);
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (int x = 0; x < nr; ++x)
+      for (int y = 0; y < nr; ++y)
+        for (int z = 0; z < nr; ++z) {
+          float s = 0.0f, s2 = 0.0f;
+          for (int dx = 0; dx < 2; ++dx)
+            for (int dy = 0; dy < 2; ++dy)
+              for (int dz = 0; dz < 2; ++dz) {
+                float v = src[((size_t)(2 * x + dx) * r + (2 * y + dy)) * r + (2 * z + dz)];
+                s += v;
+                s2 += v * v;
+              }
+          float mean = s / 8.0f;
+          float variance = s2 / 8.0f - mean * mean;
+          size_t o = ((size_t)x * nr + y) * nr + z;
+          dm[o] = mean;
+          dv[o] = std::max(0.0f, variance);
+        }
+  }
+  return md;
+}
+
+// Fill_TR (core/volume.cu:1320-1345) for all 8 levels: level k (res 128>>k)
+// marches 128 steps towards the light through mip k+1 with alpha/1.73^(k+1).
+void orc_build_tr(const float* mips, float alpha, const float* light, float* tr, int nthreads) {
+  V3 L = normalize(v3(light[0], light[1], light[2]));
+  for (int k = 0; k < 8; ++k) {
+    int r = 128 >> k;
+    const float* src = mips + mip_offset(k + 1);
+    float* dst = tr + tr_offset(k);
+    float a = alpha / std::pow(1.73f, (float)k + 1.0f);
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (int x = 0; x < r; ++x)
+      for (int y = 0; y < r; ++y)
+        for (int z = 0; z < r; ++z) {
+          V3 uv = v3(((float)x + 0.5f) / (float)r, ((float)y + 0.5f) / (float)r, ((float)z + 0.5f) / (float)r);
+          V3 o = uv - 0.5f;
+          float dis = ray_box_distance(o, L);
+          float step = dis / 128.0f;
+          V3 lp = o;
+          float sum = 0.0f;
+          for (int i = 0; i < 128; ++i) {
+            lp = lp + L * step;
+            sum = sum + tri_border(src, r, lp + 0.5f);
+          }
+          dst[((size_t)x * r + y) * r + z] = std::exp(-sum * a * step);
+        }
+  }
+}
+
+// Radical inverse in base b (unscrambled), clamped below 1.
+static float radical_inverse(uint32_t base, uint32_t a) {
+  const float inv_base = 1.0f / (float)base;
+  uint32_t rev = 0;
+  float inv_bn = 1.0f;
+  while (a) {
+    uint32_t next = a / base;
+    uint32_t digit = a - next * base;
+    rev = rev * base + digit;
+    inv_bn *= inv_base;
+    a = next;
+  }
+  return std::min((float)rev * inv_bn, 0.99999994f);
+}
+static inline float fracf(float f) { return f - (float)(long)f; }
+
+// Fill_Hg (core/volume.cu:1082-1160): lut[i + j*512] = average of HG over a
+// ball of radius tan(angle_j) centred on direction cos_i at unit distance,
+// 1024 Halton samples (dims 2,3,5 and 11) mixing HG-sampled chords and
+// uniform ball points; per-texel Cranley-Patterson offset from Philox.
+void orc_build_hglut(float g, uint32_t seed, float* lut, int nthreads) {
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+  for (int j = 0; j < 512; ++j)
+    for (int i = 0; i < 512; ++i) {
+      float costheta = (((float)i + 0.5f) / 512.0f) * 2.0f - 1.0f;
+      float aa = ((float)j + 0.5f) / 512.0f;
+      float angle = aa * 3.1415926535f * 60.0f / 180.0f;
+      float bn = u01_tag(seed, (uint32_t)(i + j * 512), 0, TAG_LUT);
+      float hg = 0.0f;
+      float R = std::tan(angle);
+      V3 view = v3(1, 0, 0);
+      V3 D = v3(costheta, std::sqrt(1.0f - costheta * costheta), 0.0f);
+      float mis = 0.0f;
+      {
+        float p = R * R - 1 + D.x * D.x;
+        if (p > 0) {
+          float sdotl = g > 0 ? D.x : -D.x;
+          float w = std::sqrt(p);
+          float d0 = std::max(0.0f, sdotl - w) / R;
+          float d1 = (sdotl + w) / R;
+          float d = d1 * d1 * d1 - d0 * d0 * d0;
+          mis = (d1 > d0) ? d : 0.0f;
+        }
+        mis = std::min(std::max(mis, 1e-8f), 1.0f);
+        float a = std::fabs(g);
+        a = a < 0.6f ? 0.0f : (a < 0.7f ? (a - 0.6f) * 9.0f : (std::pow((a - 0.7f) / 0.3f, 0.05f) * 0.1f + 0.9f));
+        mis = 1.0f - 1.0f / (1.0f + a * mis / (1.0f - a));
+      }
+      for (int k = 0; k < 1024; ++k) {
+        if (fracf(radical_inverse(11, k) + bn) < mis) {
+          float r0 = fracf(radical_inverse(2, k) + bn), r1 = fracf(radical_inverse(3, k) + bn);
+          V3 l = hg_sample_dir(r0, r1, view, g);
+          float sdotl = dot(D, l);
+          float p = R * R - 1 + sdotl * sdotl;
+          if (p <= 0) continue;
+          float w = std::sqrt(p);
+          float d0 = sdotl - w;
+          float d1 = (sdotl + w) / R;
+          d0 = std::max(0.0f, d0) / R;
+          float d = d1 * d1 * d1 - d0 * d0 * d0;
+          hg += std::max(0.0f, d / 4);
+        } else {
+          float r0 = fracf(radical_inverse(2, k) + bn), r1 = fracf(radical_inverse(3, k) + bn);
+          float r2 = fracf(radical_inverse(5, k) + bn);
+          float theta = r0 * 2.0f * 3.1415926535f;
+          float phi = std::acos(2.0f * r1 - 1.0f);
+          float rr = std::cbrt(r2);
+          float x = R * rr * std::sin(phi) * std::cos(theta);
+          float y = R * rr * std::sin(phi) * std::sin(theta);
+          float z = R * rr * std::cos(phi);
+          V3 rp = v3(x, y, z) + D;
+          hg += hg_phase(dot(normalize(rp), view), g);
+        }
+      }
+      lut[i + j * 512] = hg / 1024.0f;
+    }
+}
+
+// Delta-tracking render (VolumeRender::Render, rt = PT). Pixel (row, col),
+// sample s uses Philox stream (seed; row*W+col, sample_offset+s, ., TAG_PT):
+// draws 0,1 jitter, then the path. Writes per-pixel sums and sums of squares
+// of the radiance (W*H*3 each, fp64). Rows [row0, row1) only.
+void orc_render_pt(const float* density, int res, float max_density, const mr_render_params* p,
+                   int row0, int row1, double* sum, double* sumsq, uint64_t* counters, int nthreads) {
+  Vol vol{density, res, max_density, nullptr, nullptr, nullptr};
+  Scene sc = make_scene(*p);
+  std::atomic<uint64_t> fetches{0}, caps{0};
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+  for (int row = row0; row < row1; ++row) {
+    Tracker tk{vol, sc};
+    for (int col = 0; col < p->width; ++col) {
+      size_t pix = (size_t)row * p->width + col;
+      double acc[3] = {0, 0, 0}, acc2[3] = {0, 0, 0};
+      for (int s = 0; s < p->spp; ++s) {
+        Rng rng(p->seed, (uint32_t)pix, p->sample_offset + (uint32_t)s, TAG_PT);
+        float jx = rng.next(), jy = rng.next();
+        V3 dir = camera_dir(*p, row, col, jx, jy);
+        float t;
+        V3 L = tk.radiance(rng, f3(p->ori), dir, &t);
+        L = vmax(L, v3(0, 0, 0));
+        acc[0] += L.x; acc[1] += L.y; acc[2] += L.z;
+        acc2[0] += (double)L.x * L.x; acc2[1] += (double)L.y * L.y; acc2[2] += (double)L.z * L.z;
+      }
+      for (int c = 0; c < 3; ++c) {
+        sum[pix * 3 + c] = acc[c];
+        if (sumsq) sumsq[pix * 3 + c] = acc2[c];
+      }
+    }
+    fetches += tk.fetches;
+    caps += tk.caps;
+  }
+  if (counters) { counters[0] = fetches.load(); counters[1] = caps.load(); }
+}
+
+// Neural render (rt = MRPNN), one primary sample per pixel with stream
+// (seed; pixel, sample_offset, ., TAG_NN): draws 0,1 jitter, then
+// GetSamplePoint, two frames, and the single-scatter Tr.
+void orc_render_neural(const float* density, int res, float max_density, const float* mips,
+                       const float* tr, const float* lut, const float* weights, const float* stencil,
+                       const mr_render_params* p, int row0, int row1, float* out_rgb, int nthreads) {
+  Vol vol{density, res, max_density, mips, tr, lut};
+  Scene sc = make_scene(*p);
+  Net net(weights);
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+  for (int row = row0; row < row1; ++row) {
+    Tracker tk{vol, sc};
+    for (int col = 0; col < p->width; ++col) {
+      size_t pix = (size_t)row * p->width + col;
+      Rng rng(p->seed, (uint32_t)pix, p->sample_offset, TAG_NN);
+      float jx = rng.next(), jy = rng.next();
+      V3 dir = camera_dir(*p, row, col, jx, jy);
+      float t;
+      V3 L = neural_pixel(tk, net, stencil, rng, f3(p->ori), dir, &t);
+      L = vmax(L, v3(0, 0, 0));
+      out_rgb[pix * 3 + 0] = L.x; out_rgb[pix * 3 + 1] = L.y; out_rgb[pix * 3 + 2] = L.z;
+    }
+  }
+}
+
+// Gather + network for n points with explicit frames (bypasses the RNG):
+// pos n x 3, frame n x 12 (X, Y, Z, LX). Writes desc n x 576, aux n x 5 and,
+// if out != NULL, the network output n x 3.
+void orc_gather(const float* mips, const float* tr, const float* lut, const float* stencil,
+                const float* pos, const float* frame, int n, float alpha, float g,
+                const float* scatter_rate, const float* light_dir, float* desc, float* aux) {
+  Vol vol{nullptr, 0, 0, mips, tr, lut};
+  V3 L = normalize(v3(light_dir[0], light_dir[1], light_dir[2]));
+  V3 sr = v3(scatter_rate[0], scatter_rate[1], scatter_rate[2]) / 1.001f;
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < n; ++k) {
+    NetState s;
+    const float* fr = frame + 12 * k;
+    Frame f{v3(fr[0], fr[1], fr[2]), v3(fr[3], fr[4], fr[5]), v3(fr[6], fr[7], fr[8]), v3(fr[9], fr[10], fr[11])};
+    gather(s, vol, stencil, v3(pos[3 * k], pos[3 * k + 1], pos[3 * k + 2]), L, f, alpha, g);
+    std::memcpy(desc + 576 * k, s.xv, 192 * sizeof(float));
+    std::memcpy(desc + 576 * k + 192, s.xs, 192 * sizeof(float));
+    std::memcpy(desc + 576 * k + 384, s.xh, 192 * sizeof(float));
+    float* ax = aux + 5 * k;
+    ax[0] = g;
+    ax[1] = std::acos(dot(f.X, f.LX));
+    V3 srp = srp_of(sr);
+    ax[2] = srp.x; ax[3] = srp.y; ax[4] = srp.z;
+  }
+}
+
+// Network body on n descriptors (desc n x 576, aux n x 5 = g, gamma, srp.xyz).
+void orc_predict(const float* weights, const float* desc, const float* aux, int n, float* out) {
+  Net net(weights);
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < n; ++k) {
+    NetState s;
+    std::memcpy(s.xv, desc + 576 * k, 192 * sizeof(float));
+    std::memcpy(s.xs, desc + 576 * k + 192, 192 * sizeof(float));
+    std::memcpy(s.xh, desc + 576 * k + 384, 192 * sizeof(float));
+    const float* ax = aux + 5 * k;
+    trunks(s, net, ax[0], ax[1]);
+    V3 r = heads(s, net, v3(ax[2], ax[3], ax[4]));
+    out[3 * k + 0] = r.x; out[3 * k + 1] = r.y; out[3 * k + 2] = r.z;
+  }
+}
+
+// Procedural cloud (same definition as oracle/cloud_np.py): Perlin improved
+// noise fBm, normalised, thresholded, radial falloff; perm = 256 entries.
+static inline float orc_fade(float t) { return t * t * t * (t * (t * 6.0f - 15.0f) + 10.0f); }
+static inline float orc_grad(int h, float x, float y, float z) {
+  h &= 15;
+  float u = h < 8 ? x : y;
+  float v = h < 4 ? y : (h == 12 || h == 14 ? x : z);
+  return ((h & 1) ? -u : u) + ((h & 2) ? -v : v);
+}
+static float orc_perlin(const int* P, float x, float y, float z) {
+  float fx = std::floor(x), fy = std::floor(y), fz = std::floor(z);
+  int X = (int)fx & 255, Y = (int)fy & 255, Z = (int)fz & 255;
+  x -= fx; y -= fy; z -= fz;
+  float u = orc_fade(x), v = orc_fade(y), w = orc_fade(z);
+  int A = P[X] + Y, AA = P[A] + Z, AB = P[A + 1] + Z, B = P[X + 1] + Y, BA = P[B] + Z, BB = P[B + 1] + Z;
+  return lerp(lerp(lerp(orc_grad(P[AA], x, y, z), orc_grad(P[BA], x - 1, y, z), u),
+                   lerp(orc_grad(P[AB], x, y - 1, z), orc_grad(P[BB], x - 1, y - 1, z), u), v),
+              lerp(lerp(orc_grad(P[AA + 1], x, y, z - 1), orc_grad(P[BA + 1], x - 1, y, z - 1), u),
+                   lerp(orc_grad(P[AB + 1], x, y - 1, z - 1), orc_grad(P[BB + 1], x - 1, y - 1, z - 1), u), v),
+              w);
+}
+void orc_cloud(int res, const int* perm256, int octaves, float f0, float lac, float gain, float thr, float* out,
+               int nthreads) {
+  int P[512];
+  for (int i = 0; i < 512; ++i) P[i] = perm256[i & 255];
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+  for (int x = 0; x < res; ++x)
+    for (int y = 0; y < res; ++y)
+      for (int z = 0; z < res; ++z) {
+        float px = ((float)x + 0.5f) / res, py = ((float)y + 0.5f) / res, pz = ((float)z + 0.5f) / res;
+        float sum = 0.0f, norm = 0.0f, amp = 1.0f, f = f0;
+        for (int o = 0; o < octaves; ++o) {
+          sum += amp * orc_perlin(P, px * f, py * f, pz * f);
+          norm += amp;
+          amp *= gain;
+          f *= lac;
+        }
+        float nv = 0.5f + 0.5f * sum / norm;
+        float dx = px - 0.5f, dy = py - 0.5f, dz = pz - 0.5f;
+        float r2 = 4.0f * (dx * dx + dy * dy + dz * dz);
+        out[((size_t)x * res + y) * res + z] = std::max(0.0f, nv - thr) / (1.0f - thr) * std::max(0.0f, 1.0f - r2);
+      }
+}
+
+// Training label GetSample (core/render.cuh:276-315): multiple-scattering
+// radiance at pos along view dir, light L; stream (seed; k, sample, ., TAG_LABEL).
+void orc_get_samples(const float* density, int res, float max_density, const float* pos,
+                     const float* dir, const float* light, const float* alpha, const float* g,
+                     const float* scatter, int n, int max_bounces, int spp, uint32_t seed,
+                     double* out, int nthreads) {
+  Vol vol{density, res, max_density, nullptr, nullptr, nullptr};
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+  for (int k = 0; k < n; ++k) {
+    Scene sc;
+    sc.alpha = alpha[k]; sc.g = g[k]; sc.tr_scale = 1.0f;
+    sc.scatter = v3(scatter[k], scatter[k], scatter[k]);
+    sc.light_dir = v3(light[3 * k], light[3 * k + 1], light[3 * k + 2]);
+    sc.light_color = v3(1, 1, 1); sc.env = v3(0, 0, 0); sc.max_bounces = max_bounces;
+    Tracker tk{vol, sc};
+    V3 L = normalize(sc.light_dir);
+    V3 d0 = v3(dir[3 * k], dir[3 * k + 1], dir[3 * k + 2]);
+    double acc = 0.0;
+    for (int s = 0; s < spp; ++s) {
+      Rng rng(seed, (uint32_t)k, (uint32_t)s, TAG_LABEL);
+      V3 sp = v3(pos[3 * k], pos[3 * k + 1], pos[3 * k + 2]);
+      float e0 = rng.next(), e1 = rng.next();
+      V3 rd = hg_sample_dir(e0, e1, d0, sc.g);
+      float rate = 1.0f;
+      float res_acc = 0.0f;
+      for (int b = 0; b < max_bounces; ++b) {
+        V3 np, nd;
+        float dis = ray_box_distance(sp, rd);
+        if (!tk.next_vertex(rng, sc.alpha, sc.g, sp, rd, dis, np, nd)) break;
+        sp = np;
+        rate = rate * 1.001f * scatter[k];
+        dis = ray_box_distance(sp, L);
+        float ph = hg_phase(dot(rd, L), sc.g);
+        res_acc = res_acc + rate * (tk.transmittance(rng, sp, L, dis, sc.alpha) * ph);
+        rd = nd;
+      }
+      acc += res_acc;
+    }
+    out[k] = acc / spp;
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,119 @@
+"""ctypes bindings of the reference harness libraries in oracle/_ref/ --
+test infrastructure only. Both libraries run the reference's own device code
+on the GPU; they exist only where oracle.build.build_reference() ran."""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_SO = os.path.join(HERE, "_ref", "libref_mrpnn.so")
+INJ_SO = os.path.join(HERE, "_ref", "libref_net_inj.so")
+
+f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+
+
+def available():
+    return os.path.exists(REF_SO) and os.path.exists(INJ_SO)
+
+
+class Ref:
+    """The reference renderer (core/render.cuh, core/radiancePredict.cu)."""
+
+    def __init__(self):
+        L = C.CDLL(REF_SO)
+        L.ref_setup.argtypes = [f32p, C.c_int, C.c_float, f32p, f32p, f32p, f32p, f32p, C.c_float]
+        L.ref_render.argtypes = [C.c_int, C.c_int, C.c_int, f32p, f32p, f32p, f32p, f32p, C.c_float, C.c_int,
+                                 C.c_float, C.c_int, f64p, f64p]
+        L.ref_predict_frames.argtypes = [C.c_int, f32p, f32p, f32p, C.c_float, C.c_float, f32p, f32p]
+        L.ref_load_weights.argtypes = [f32p, C.c_long]
+        L.ref_read_weights.argtypes = [f32p, C.c_long]
+        L.ref_read_stencil.argtypes = [f32p]
+        self.L = L
+
+    def setup(self, density, max_density, mips, tr, lut, env=(0, 0, 0), scatter=(0.99,) * 3, tr_scale=1.0):
+        d = np.ascontiguousarray(density, np.float32).ravel()
+        res = round(d.size ** (1 / 3))
+        rc = self.L.ref_setup(d, res, float(max_density), np.ascontiguousarray(mips, np.float32),
+                              np.ascontiguousarray(tr, np.float32), np.ascontiguousarray(lut, np.float32),
+                              np.asarray(env, np.float32), np.asarray(scatter, np.float32), float(tr_scale))
+        assert rc == 0, "ref_setup failed"
+
+    def render(self, mode, w, h, ori, up, right, light, light_color, alpha, bounces, g, spp):
+        s = np.zeros(w * h * 3, np.float64)
+        s2 = np.zeros(w * h * 3, np.float64)
+        a = lambda v: np.asarray(v, np.float32)
+        rc = self.L.ref_render(mode, w, h, a(ori), a(up), a(right), a(light), a(light_color), float(alpha),
+                               int(bounces), float(g), int(spp), s, s2)
+        assert rc == 0, "ref_render failed"
+        return s, s2
+
+    def predict_frames(self, pos, frame, light, alpha, g, scatterrate):
+        n = len(pos)
+        out = np.zeros(3 * n, np.float32)
+        rc = self.L.ref_predict_frames(n, np.ascontiguousarray(pos, np.float32).ravel(),
+                                       np.ascontiguousarray(frame, np.float32).ravel(), np.asarray(light, np.float32),
+                                       float(alpha), float(g), np.asarray(scatterrate, np.float32), out)
+        assert rc == 0
+        return out.reshape(n, 3)
+
+    def load_weights(self, blob):
+        assert self.L.ref_load_weights(np.ascontiguousarray(blob, np.float32), blob.size) == 0
+
+    def read_weights(self):
+        out = np.zeros(49673, np.float32)
+        assert self.L.ref_read_weights(out, out.size) == 0
+        return out
+
+    def read_stencil(self):
+        out = np.zeros(480, np.float32)
+        assert self.L.ref_read_stencil(out) == 0
+        return out
+
+
+class RefNet:
+    """The reference network on injected descriptor values (ref_inject.cu)."""
+
+    def __init__(self):
+        L = C.CDLL(INJ_SO)
+        L.ref_inject_predict.argtypes = [C.c_int, f32p, f32p, f32p, C.c_float, f32p, f32p]
+        L.ref_load_weights.argtypes = [f32p, C.c_long]
+        L.ref_read_weights.argtypes = [f32p, C.c_long]
+        self.L = L
+
+    def load_weights(self, blob):
+        assert self.L.ref_load_weights(np.ascontiguousarray(blob, np.float32), blob.size) == 0
+
+    def read_weights(self):
+        out = np.zeros(49673, np.float32)
+        assert self.L.ref_read_weights(out, out.size) == 0
+        return out
+
+    def predict(self, raw, frame, light, g, scatterrate):
+        n = len(raw)
+        out = np.zeros(3 * n, np.float32)
+        rc = self.L.ref_inject_predict(n, np.ascontiguousarray(raw, np.float32).ravel(),
+                                       np.ascontiguousarray(frame, np.float32).ravel(), np.asarray(light, np.float32),
+                                       float(g), np.asarray(scatterrate, np.float32), out)
+        assert rc == 0
+        return out.reshape(n, 3)
+
+
+def raw_to_desc(raw, frame, light, g):
+    """The descriptor the reference network sees for injected raw values
+    (ref_inject.cu): density log(1+rho), transmittance as is, phase
+    log(HG0+1) for i >= 1 and log(HG(X.L, g)+1) for i = 0."""
+    raw = np.asarray(raw, np.float32)
+    desc = np.empty_like(raw)
+    desc[:, :192] = np.log(np.float32(1) + raw[:, :192])
+    desc[:, 192:384] = raw[:, 192:384]
+    desc[:, 385:576] = np.log(raw[:, 385:576] + np.float32(1))
+    X = np.asarray(frame, np.float32)[:, 0:3]
+    L = np.asarray(light, np.float32)
+    c = (X * L).sum(1, dtype=np.float32)
+    g2 = np.float32(g) * np.float32(g)
+    d = np.float32(1) + g2 - np.float32(2) * np.float32(g) * c
+    hg = ((np.float32(1) - g2) / (d * np.sqrt(d))) * np.float32(0.25)
+    desc[:, 384] = np.log(hg + np.float32(1))
+    return desc
