@@ -161,6 +161,16 @@ int mr_generate_cloud(int32_t res, uint32_t seed, int32_t octaves, float base_fr
 /* The 256-entry noise permutation the cloud generator uses for `seed`. */
 int mr_cloud_permutation(uint32_t seed, int32_t* host_out256);
 
+/* Self-test of the tensor-core tile path (no reference counterpart): one
+ * 128 x n x k BF16 product D = A * B^T through the same shared-memory and
+ * instruction descriptors as the network kernel. host_a 128 x k and host_b
+ * n x k are BF16 bit patterns, row-major; host_d receives 128 x n fp32.
+ * Shapes (n, k): (16,16) (32,32) (16,32) (32,64) (64,128) (128,128). */
+int mr_tc_selftest(int32_t n, int32_t k, const uint16_t* host_a, const uint16_t* host_b, float* host_d);
+/* Error word of the tensor-core network kernel of `net` (an mbarrier wait
+ * that timed out): MR_ERR_TIMEOUT if set; `reset` clears it. */
+int mr_network_check(const mr_network* net, int32_t reset);
+
 /* Wait for `stream` with a watchdog: MR_ERR_TIMEOUT after timeout_ms. */
 int mr_sync(void* stream, int32_t timeout_ms);
 

@@ -23,7 +23,7 @@ EXPORTS = [
     "mr_network_destroy", "mr_builtin_stencil", "mr_weights_xavier", "mr_render", "mr_render_host",
     "mr_render_accumulate_f64", "mr_radiance_predict", "mr_gather_descriptors", "mr_sync",
     "mr_volume_counters", "mr_generate_cloud", "mr_cloud_permutation",
-    "mr_volume_set_timing", "mr_volume_stage_times",
+    "mr_volume_set_timing", "mr_volume_stage_times", "mr_tc_selftest", "mr_network_check",
 ]
 
 
@@ -92,6 +92,8 @@ def load():
     L.mr_cloud_permutation.argtypes = [u32, vp]
     L.mr_volume_set_timing.argtypes = [vp, i32]
     L.mr_volume_stage_times.argtypes = [vp, vp, vp, i32]
+    L.mr_tc_selftest.argtypes = [i32, i32, vp, vp, vp]
+    L.mr_network_check.argtypes = [vp, i32]
     _lib = L
     return L
 

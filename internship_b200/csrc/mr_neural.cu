@@ -256,6 +256,29 @@ __global__ void __launch_bounds__(64) k_predict_simt(const float* __restrict__ w
   out[3 * (size_t)k + 2] = r.z;
 }
 
+// Gather for the compacted records (tensor-core path): desc / aux rows k.
+__global__ void __launch_bounds__(128) k_gather_records(Tables t, const float* __restrict__ stencil, Records rec,
+                                                        int capacity, F3 L, float alpha, float g, F3 srp,
+                                                        float* __restrict__ desc, float* __restrict__ aux) {
+  unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned n = min(*rec.count, (unsigned)capacity);
+  if (k >= n) return;
+  float xv[192], xs[192], xh[192];
+  F3 pos = f3(rec.pos[3 * (size_t)k], rec.pos[3 * (size_t)k + 1], rec.pos[3 * (size_t)k + 2]);
+  Frame f = load_frame(rec.frame + 12 * (size_t)k);
+  gather_point(t, stencil, pos, L, f, alpha, g, xv, xs, xh);
+  float* d = desc + 576 * (size_t)k;
+  for (int i = 0; i < 192; ++i) { d[i] = xv[i]; d[192 + i] = xs[i]; d[384 + i] = xh[i]; }
+  float* ax = aux + 5 * (size_t)k;
+  ax[0] = g;
+  ax[1] = acosf(dot(f.X, f.LX));
+  ax[2] = srp.x; ax[3] = srp.y; ax[4] = srp.z;
+}
+
+int launch_mlp_tc(const Network* net, const float* desc, const float* aux, int n, float* out, const int* pix,
+                  const float* trph, const unsigned* count, F3 light_color, F3 scatter, cudaStream_t s);
+int mlp_tc_error(const Network* net, bool reset);
+
 extern int check_params(const mr_render_params* p);
 extern CameraModel make_camera(const mr_render_params* p);
 extern PathScene make_path_scene(const mr_render_params* p);
@@ -277,7 +300,8 @@ int render_neural(Volume* v, const Network* net, const mr_render_params* p, floa
   if (!net) return set_error(MR_ERR_ARG, "MRPNN render needs a network (mr_network_create)");
   if (!v->data_set) return set_error(MR_ERR_STATE, "render before mr_volume_set_data");
   if (!v->mips_valid) return set_error(MR_ERR_STATE, "render before mr_volume_update");
-  if (p->precision != MR_PREC_FP32) return set_error(MR_ERR_UNSUPPORTED, "precision %d not built", p->precision);
+  if (p->precision != MR_PREC_FP32 && p->precision != MR_PREC_BF16)
+    return set_error(MR_ERR_UNSUPPORTED, "precision %d not built", p->precision);
   F3 L = normalize(to_f3(p->light_dir));
   // UpdateHGLut / Update_TR on demand (core/volume.cu:434-437).
   if (!v->lut_valid || v->lut_g != p->g || v->lut_seed != p->seed) {
@@ -289,9 +313,15 @@ int render_neural(Volume* v, const Network* net, const mr_render_params* p, floa
     if (rc) return rc;
   }
   size_t npx = (size_t)p->width * p->height;
-  int rc = ensure_scratch(v, records_bytes(npx), s);
+  const bool tc = p->precision == MR_PREC_BF16;
+  // records, then (tensor-core path) descriptor rows and aux rows
+  size_t rbytes = (records_bytes(npx) + 255) / 256 * 256;
+  size_t need = rbytes + (tc ? npx * (576 + 5) * sizeof(float) + 256 : 0);
+  int rc = ensure_scratch(v, need, s);
   if (rc) return rc;
   Records rec = carve_records(v->scratch, npx);
+  float* desc = (float*)((char*)v->scratch + rbytes);
+  float* aux = desc + npx * 576;
   MR_CUDA(cudaMemsetAsync(v->d_counters, 0, kCounters * sizeof(unsigned long long), s));
   MR_CUDA(cudaMemsetAsync(rec.count, 0, sizeof(unsigned), s));
   NNTraceArgs ta;
@@ -307,6 +337,19 @@ int render_neural(Volume* v, const Network* net, const mr_render_params* p, floa
   k_nn_trace<<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(ta);
   v->timer.mark(ST_NN_TRACE, s);
   MR_CUDA(cudaGetLastError());
+  if (tc) {
+    F3 sr = to_f3(p->scatter_rate) / 1.001f;
+    v->timer.mark(ST_NN_PREDICT, s);
+    k_gather_records<<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(Tables{v->mips, v->tr, v->lut}, net->stencil, rec,
+                                                                   (int)npx, L, p->alpha, p->g, srp_of(sr), desc, aux);
+    v->timer.mark(ST_NN_PREDICT, s);
+    MR_CUDA(cudaGetLastError());
+    v->timer.mark(ST_NN_MLP, s);
+    rc = launch_mlp_tc(net, desc, aux, (int)npx, dev_rgb, rec.pix, rec.trph, rec.count, to_f3(p->light_color),
+                       to_f3(p->scatter_rate), s);
+    v->timer.mark(ST_NN_MLP, s);
+    return rc;
+  }
   NNPredictArgs pa;
   pa.t = Tables{v->mips, v->tr, v->lut};
   pa.w = net->w;
@@ -355,6 +398,9 @@ extern "C" int mr_radiance_predict(const mr_network* nh, int32_t precision, cons
   if (!nh || !dev_desc || !dev_aux || !dev_out) return set_error(MR_ERR_ARG, "mr_radiance_predict: NULL argument");
   if (n < 0) return set_error(MR_ERR_ARG, "n < 0");
   if (n == 0) return MR_OK;
+  if (precision == MR_PREC_BF16)
+    return launch_mlp_tc(&nh->n, dev_desc, dev_aux, n, dev_out, nullptr, nullptr, nullptr, f3(1, 1, 1), f3(1, 1, 1),
+                         (cudaStream_t)stream);
   if (precision != MR_PREC_FP32) return set_error(MR_ERR_UNSUPPORTED, "precision %d not built", precision);
   k_predict_simt<<<(n + 63) / 64, 64, 0, (cudaStream_t)stream>>>(nh->n.w, dev_desc, dev_aux, n, dev_out);
   MR_CUDA(cudaGetLastError());

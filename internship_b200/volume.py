@@ -21,10 +21,21 @@ def builtin_stencil():
     return out
 
 
-def xavier_weights(seed=1):
-    """Xavier-uniform initial weights in the NNWeight.cuh blob layout."""
+def xavier_weights(seed=1, bias_range=None):
+    """Xavier-uniform initial weights in the NNWeight.cuh blob layout (zero
+    biases). With bias_range=(lo, hi) the biases are drawn uniformly from it
+    (numpy generator seeded with `seed`), which keeps every ReLU of a random
+    network active."""
     out = np.zeros(_lib.WEIGHT_TOTAL, np.float32)
     check(_lib.load().mr_weights_xavier(seed, out.ctypes.data, out.size))
+    if bias_range is not None:
+        from .weights import layout
+        rng = np.random.default_rng(seed)
+        off = 0
+        for name, n in layout():
+            if name.endswith("B"):
+                out[off:off + n] = rng.uniform(bias_range[0], bias_range[1], n)
+            off += n
     return out
 
 

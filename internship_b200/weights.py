@@ -65,6 +65,21 @@ def load_stencil_source(path):
     return np.array(pts, np.float32).ravel()
 
 
+def active_random_weights(seed=1):
+    """Random network whose every ReLU, the last one included, is active on
+    non-negative descriptors: Xavier(seed) weights, biases uniform in
+    [0, 0.1], and the final 16->1 layer's weights made non-negative. Useful
+    for parity tests, where all-zero outputs would prove nothing."""
+    from .volume import xavier_weights
+    w = xavier_weights(seed, bias_range=(0.0, 0.1))
+    off = 0
+    for name, n in layout():
+        if name == "LX12W":
+            w[off:off + n] = np.abs(w[off:off + n])
+        off += n
+    return w
+
+
 def save_blob(path, weights, stencil=None):
     w = np.ascontiguousarray(weights, np.float32).ravel()
     st = np.zeros(480, np.float32) if stencil is None else np.ascontiguousarray(stencil, np.float32).ravel()

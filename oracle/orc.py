@@ -58,10 +58,10 @@ def lib():
         L.orc_build_mips.restype = C.c_float
         L.orc_build_tr.argtypes = [f32p, C.c_float, f32p, f32p, C.c_int]
         L.orc_build_hglut.argtypes = [C.c_float, C.c_uint32, f32p, C.c_int]
-        L.orc_render_pt.argtypes = [f32p, C.c_int, C.c_float, C.POINTER(RenderParams), C.c_int,
+        L.orc_render_pt.argtypes = [f32p, C.c_int, C.c_float, C.c_void_p, C.c_int,
                                     C.c_int, f64p, f64p, u64p, C.c_int]
         L.orc_render_neural.argtypes = [f32p, C.c_int, C.c_float, f32p, f32p, f32p, f32p, f32p,
-                                        C.POINTER(RenderParams), C.c_int, C.c_int, f32p, C.c_int]
+                                        C.c_void_p, C.c_int, C.c_int, f32p, C.c_int]
         L.orc_gather.argtypes = [f32p, f32p, f32p, f32p, f32p, f32p, C.c_int, C.c_float,
                                  C.c_float, f32p, f32p, f32p, f32p]
         L.orc_predict.argtypes = [f32p, f32p, f32p, C.c_int, f32p]
@@ -129,7 +129,7 @@ def render_pt(density, max_density, params, row0=0, row1=None):
     s = np.zeros(n, np.float64)
     s2 = np.zeros(n, np.float64)
     cnt = np.zeros(2, np.uint64)
-    lib().orc_render_pt(density.ravel(), res, float(max_density), C.byref(params), row0,
+    lib().orc_render_pt(density.ravel(), res, float(max_density), C.addressof(params), row0,
                         params.height if row1 is None else row1, s, s2, cnt, nthreads())
     return s, s2, cnt
 
@@ -139,7 +139,7 @@ def render_neural(density, max_density, mips, tr, lut, weights, stencil, params,
     res = round(density.size ** (1 / 3))
     out = np.zeros(params.width * params.height * 3, np.float32)
     lib().orc_render_neural(density.ravel(), res, float(max_density), _a(mips), _a(tr), _a(lut),
-                            _a(weights), _a(stencil), C.byref(params), row0,
+                            _a(weights), _a(stencil), C.addressof(params), row0,
                             params.height if row1 is None else row1, out, nthreads())
     return out
 

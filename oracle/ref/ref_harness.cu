@@ -153,7 +153,7 @@ extern "C" {
 // Bind the volume tables: density res^3, mips (9 concatenated levels
 // 256^3..1^3), tr (8 levels 128^3..1^3), lut 512x512, constant environment.
 int ref_setup(const float* density, int res, float max_density, const float* mips, const float* tr,
-              const float* lut, const float* env, const float* scatter_rate, float tr_scale_) {
+              const float* lut, const float* env, const float* albedo, float tr_scale_) {
   cudaTextureObject_t o;
   if (make_tex3(density, res, cudaAddressModeBorder, &o)) return 1;
   if (set_ref(_DensityVolume, o)) return 1;
@@ -195,7 +195,7 @@ int ref_setup(const float* density, int res, float max_density, const float* mip
     return 1;
   if (set_ref(_HDRI, g_env)) return 1;
   float one = 1.0f, ior = -1.0f;
-  float3 sr = F3(scatter_rate);
+  float3 sr = F3(albedo);
   CK(cudaMemcpyToSymbol(maxDensity, &max_density, sizeof(float)));
   CK(cudaMemcpyToSymbol(Resolution, &res, sizeof(int)));
   CK(cudaMemcpyToSymbol(tr_scale, &tr_scale_, sizeof(float)));

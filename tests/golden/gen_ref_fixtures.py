@@ -8,16 +8,17 @@ inputs generated here from fixed seeds and the reference's outputs; no
 reference data (weights, tables) is stored.
 
 ref_network.npz  -- the reference network (core/radiancePredict.cu:370-485)
-                    on 256 injected descriptors, with Xavier(seed 1) weights
-                    (out_xavier) and with its compiled-in weights (out_refw).
+                    on 256 injected descriptors, with random weights (weights.active_random_weights(1),
+                    out_xavier) and with its compiled-in
+                    weights (out_refw).
 ref_pt_sphere.npz -- the reference delta tracker (CalculateRadiance) on the
                     sphere scene at 32x32, 2048 spp: per-pixel sums and sums
                     of squares.
 ref_gather.npz   -- RadiancePredict with the reference's texture gather, on
                     200 points of the sphere scene with explicit frames, with
-                    Xavier(seed 1) weights and the reference's stencil.
+                    the reference's compiled-in weights and stencil.
 ref_nn_sphere.npz -- NNPredict<MRPNN> on the sphere scene at 32x32, 1024
-                    passes, Xavier(seed 1) weights: per-pixel sums / squares.
+                    passes, the reference's weights: per-pixel sums / squares.
 """
 import os
 import sys
@@ -47,7 +48,8 @@ def rand_frames(rng, n, light):
 def main(out):
     os.makedirs(out, exist_ok=True)
     rng = np.random.default_rng(20261203)
-    wx = xavier_weights(1)
+    from internship_b200.weights import active_random_weights
+    wx = active_random_weights(1)
 
     # -- network on injected descriptors --------------------------------------------
     net = ref_py.RefNet()
@@ -95,7 +97,7 @@ def main(out):
     m = 200
     pos = rng.uniform(-0.3, 0.3, (m, 3)).astype(np.float32)
     fr = rand_frames(rng, m, L)
-    ref.load_weights(wx)
+    ref.load_weights(ref_w)
     outg = ref.predict_frames(pos, fr, L, p.alpha, p.g, scatterrate)
     np.savez_compressed(os.path.join(out, "ref_gather.npz"), pos=pos, frames=fr, light=L, alpha=np.float32(p.alpha),
                         g=np.float32(p.g), scatterrate=scatterrate, out=outg)

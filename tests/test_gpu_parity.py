@@ -50,7 +50,9 @@ def test_volume_build_matches_oracle(mr):
         assert v.max_density == pytest.approx(md)
         gm, gv = _mips_from(v)
         np.testing.assert_allclose(gm, mips, rtol=2e-6, atol=2e-6)
-        np.testing.assert_allclose(gv, var, rtol=1e-4, atol=2e-6)
+        # E[x^2]-E[x]^2 cancels: 1-ulp differences of the means (FMA contraction
+        # in the resample) show up at ~ulp(max x^2) absolute.
+        np.testing.assert_allclose(gv, var, rtol=1e-4, atol=4e-6 * max(1.0, float(dens.max()) ** 2))
         L = np.array([0.3, -0.8, 0.5], np.float32)
         L /= np.linalg.norm(L)
         v.Update_TR(L, 64.0)
@@ -129,6 +131,13 @@ def test_fp64_accumulation_matches(mr, torch):
     v.close()
 
 
+def _test_weights(mr):
+    """Xavier(seed 1) weights with biases in [0, 0.1], so that every ReLU is
+    active and the outputs are not trivially zero."""
+    from internship_b200.weights import active_random_weights
+    return active_random_weights(1)
+
+
 def _frames(rng, n, L):
     fr = np.zeros((n, 12), np.float32)
     for k in range(n):
@@ -149,7 +158,7 @@ def test_gather_and_predict_match_oracle(mr, torch):
     L /= np.linalg.norm(L)
     v.Update_TR(L, p.alpha)
     v.UpdateHGLut(p.g)
-    w = mr.xavier_weights(1)
+    w = _test_weights(mr)
     st = mr.builtin_stencil()
     net = mr.Network(w, st)
     rng = np.random.default_rng(3)
@@ -172,6 +181,7 @@ def test_gather_and_predict_match_oracle(mr, torch):
     np.testing.assert_allclose(desc.cpu().numpy(), rdesc, rtol=1e-4, atol=2e-5)
     np.testing.assert_allclose(aux.cpu().numpy(), raux, rtol=1e-5, atol=1e-6)
     rout = orc.predict(w, desc.cpu().numpy(), aux.cpu().numpy())
+    assert (rout > 0).mean() > 0.9
     np.testing.assert_allclose(out.cpu().numpy(), rout, rtol=1e-4, atol=1e-6)
     net.close()
     v.close()
@@ -181,7 +191,7 @@ def test_neural_render_matches_oracle(mr):
     from internship_b200 import _lib, scenes
     dens = scenes.sphere_density(128)
     v = _volume(mr, dens)
-    w = mr.xavier_weights(1)
+    w = _test_weights(mr)
     st = mr.builtin_stencil()
     v.SetWeights(w, st)
     p = scenes.make_params(24, 24, 1, rt=_lib.RT_MRPNN)
@@ -241,7 +251,7 @@ def test_predict_matches_reference_network(mr, torch):
     L /= np.linalg.norm(L)
     fr = _frames(rng, n, L)
     sr = np.array([0.9, 0.95, 0.99], np.float32) / np.float32(1.001)
-    for w in (mr.xavier_weights(1), refw):
+    for w in (_test_weights(mr), refw):
         rn.load_weights(w)
         ref = rn.predict(raw, fr, L, 0.857, sr)
         desc = ref_py.raw_to_desc(raw, fr, L, 0.857)

@@ -1,0 +1,137 @@
+"""GPU tests of the tcgen05 tensor-core network path (BF16 operands, FP32
+accumulation) against plain matrix products and the FP32 oracle network."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import orc, ref_py
+
+pytestmark = pytest.mark.gpu
+
+
+def _bf16_bits(x):
+    u = np.asarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) >> 16
+    return u.astype(np.uint16)
+
+
+def _bf16_value(bits):
+    return (bits.astype(np.uint32) << 16).view(np.float32)
+
+
+@pytest.mark.parametrize("n,k", [(16, 16), (32, 32), (16, 32), (32, 64), (64, 128), (128, 128)])
+def test_tile_product_matches_matmul(n, k):
+    from internship_b200 import _lib
+    rng = np.random.default_rng(n * 1000 + k)
+    a = _bf16_bits(rng.uniform(-1, 1, (128, k)))
+    b = _bf16_bits(rng.uniform(-1, 1, (n, k)))
+    d = np.zeros((128, n), np.float32)
+    _lib.check(_lib.load().mr_tc_selftest(n, k, a.ctypes.data, b.ctypes.data, d.ctypes.data))
+    ref = _bf16_value(a).astype(np.float64) @ _bf16_value(b).astype(np.float64).T
+    np.testing.assert_allclose(d, ref, rtol=1e-5, atol=1e-5 * k)
+
+
+def _predict(mr, w, desc, aux, precision):
+    import torch
+    from internship_b200 import _lib
+    net = mr.Network(w)
+    n = len(desc)
+    dd = torch.from_numpy(np.ascontiguousarray(desc)).cuda()
+    da = torch.from_numpy(np.ascontiguousarray(aux)).cuda()
+    out = torch.empty(n, 3, device="cuda")
+    _lib.check(_lib.load().mr_radiance_predict(net.handle, precision, C.c_void_p(dd.data_ptr()),
+                                               C.c_void_p(da.data_ptr()), n, C.c_void_p(out.data_ptr()), None))
+    torch.cuda.synchronize()
+    _lib.check(_lib.load().mr_network_check(net.handle, 1))
+    net.close()
+    return out.cpu().numpy()
+
+
+def _descriptors(n, seed):
+    rng = np.random.default_rng(seed)
+    desc = np.zeros((n, 576), np.float32)
+    desc[:, :192] = np.log1p(rng.uniform(0, 2, (n, 192)) * (rng.uniform(size=(n, 192)) > 0.3))
+    desc[:, 192:384] = rng.uniform(0, 1, (n, 192))
+    desc[:, 384:] = np.log1p(rng.uniform(0, 3, (n, 192)))
+    aux = np.zeros((n, 5), np.float32)
+    aux[:, 0] = 0.857
+    aux[:, 1] = rng.uniform(0, np.pi, n)
+    aux[:, 2:5] = np.float32((0.99 / 1.001) ** 4)
+    return desc, aux
+
+
+def _compare(bf, ref):
+    # compare the network's pre-exponential output X = log(1 + out/srp)
+    srp = np.float32((0.99 / 1.001) ** 4)
+    xb, xr = np.log1p(bf / srp), np.log1p(ref / srp)
+    return np.abs(xb - xr)
+
+
+def test_bf16_network_matches_fp32_oracle():
+    import internship_b200 as mr
+    from internship_b200 import _lib
+    from internship_b200.weights import active_random_weights
+    w = active_random_weights(1)
+    desc, aux = _descriptors(1000, 4)  # 7 full tiles + a partial one
+    ref = orc.predict(w, desc, aux)
+    bf = _predict(mr, w, desc, aux, _lib.PREC_BF16)
+    fp = _predict(mr, w, desc, aux, _lib.PREC_FP32)
+    np.testing.assert_allclose(fp, ref, rtol=1e-4, atol=1e-6)
+    err = _compare(bf, ref)
+    assert np.median(err) < 0.02, np.median(err)
+    assert np.quantile(err, 0.99) < 0.1, np.quantile(err, 0.99)
+
+
+def test_bf16_network_three_albedo_channels():
+    import internship_b200 as mr
+    from internship_b200 import _lib
+    from internship_b200.weights import active_random_weights
+    w = active_random_weights(1)
+    desc, aux = _descriptors(300, 5)
+    sr = np.array([0.9, 0.95, 0.99], np.float32) / np.float32(1.001)
+    aux[:, 2:5] = (sr * sr) * (sr * sr)
+    ref = orc.predict(w, desc, aux)
+    bf = _predict(mr, w, desc, aux, _lib.PREC_BF16)
+    x_b = np.log1p(bf / aux[:, 2:5])
+    x_r = np.log1p(ref / aux[:, 2:5])
+    assert np.median(np.abs(x_b - x_r)) < 0.02
+    # the three channels are distinct heads
+    assert not np.allclose(ref[:, 0], ref[:, 2])
+
+
+@pytest.mark.skipif(not ref_py.available(), reason="oracle/_ref not built")
+def test_bf16_network_with_reference_weights():
+    import internship_b200 as mr
+    from internship_b200 import _lib
+    w = ref_py.RefNet().read_weights()
+    desc, aux = _descriptors(512, 6)
+    ref = orc.predict(w, desc, aux)
+    bf = _predict(mr, w, desc, aux, _lib.PREC_BF16)
+    rel = np.abs(bf - ref) / (np.abs(ref) + 1e-2)
+    assert np.median(rel) < 0.03, np.median(rel)
+    assert np.quantile(rel, 0.99) < 0.2
+
+
+def test_bf16_neural_render_close_to_fp32():
+    import internship_b200 as mr
+    from internship_b200 import _lib, scenes
+    from internship_b200.weights import active_random_weights
+    dens = scenes.sphere_density(128)
+    v = mr.VolumeRender(128)
+    v.SetDatas(dens)
+    v.Update()
+    v.SetWeights(active_random_weights(1), mr.builtin_stencil())
+    out = {}
+    for prec in (_lib.PREC_FP32, _lib.PREC_BF16):
+        p = scenes.make_params(64, 64, 1, rt=_lib.RT_MRPNN, precision=prec)
+        img = np.zeros(64 * 64 * 3, np.float32)
+        _lib.check(_lib.load().mr_render_host(v.handle, v.network.handle, C.byref(p), img.ctypes.data))
+        out[prec] = img
+    a, b = out[_lib.PREC_FP32], out[_lib.PREC_BF16]
+    active = a > 0
+    assert active.mean() > 0.05
+    rel = np.abs(np.log1p(b[active]) - np.log1p(a[active]))
+    assert np.median(rel) < 0.05
+    assert ((a == 0) == (b == 0)).all()
+    v.close()
