@@ -142,7 +142,7 @@ def cpu_baseline_sample(v, dens_dev, p, w, st):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -218,13 +218,40 @@ def main():
     _lib.check(L.mr_volume_set_timing(v.handle, 0))
     cnt = (C.c_uint64 * 4)()
     _lib.check(L.mr_volume_counters(v.handle, cnt))
-    active = int(cnt[3])
+    active = int(cnt[3])  # the counters cover the last frame
+    fetches = int(cnt[0])
     if dist is not None:
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
         dist.barrier()
     fps = world * args.steps / (ms / 1000.0)
+
+    # -- the same frames with the BF16 tensor-core network (precision sweep leg)
+    p.precision = _lib.PREC_BF16
+    for k in range(args.warmup):
+        render(2000 + k)
+    torch.cuda.synchronize()
+    L.mr_volume_stage_times(v.handle, (C.c_double * 8)(), (C.c_int32 * 8)(), 8)
+    _lib.check(L.mr_volume_set_timing(v.handle, 1))
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        evs[k][0].record()
+        render(3000 + k)
+        evs[k][1].record()
+    torch.cuda.synchronize()
+    bf_ms = float(sum(a.elapsed_time(b) for a, b in evs))
+    bf_stage = (C.c_double * 8)()
+    bf_n = (C.c_int32 * 8)()
+    _lib.check(L.mr_volume_stage_times(v.handle, bf_stage, bf_n, 8))
+    _lib.check(L.mr_volume_set_timing(v.handle, 0))
+    _lib.check(L.mr_network_check(net, 1))
+    _lib.check(L.mr_volume_counters(v.handle, cnt))
+    bf_active = int(cnt[3])  # counters cover the last frame
+    mlp_ms = bf_stage[6] / max(1, bf_n[6])
+    bf_tflops = FLOP_PER_PIXEL * bf_active / (mlp_ms / 1000.0) / 1e12
+    p.precision = _lib.PREC_FP32
 
     # -- end to end through the public API: render + D2H of the frame to pinned memory
     host = torch.empty(WIDTH * HEIGHT * 3, dtype=torch.float32, pin_memory=True)
@@ -244,11 +271,28 @@ def main():
     e2e_fps = world * args.steps / (e2e_ms / 1000.0)
 
     hbm, bf16, src = peaks()
-    pred_ms = stage_ms[2] / max(1, stage_n[2])
-    achieved = FLOP_PER_PIXEL * (active / max(1, args.steps)) / (pred_ms / 1000.0) / 1e12
-    roofline = {"bound": "tensor", "kernel": "k_nn_predict_simt (gather + fp32 network)", "achieved": achieved,
-                "peak": bf16, "unit": "TFLOP/s", "frac": achieved / bf16, "peak_source": src,
-                "traffic": None}
+    per = lambda i: stage_ms[i] / max(1, stage_n[i])
+    trace_ms, gather_ms, mlp_ms32 = per(1), per(2), per(6)
+    # algorithmic bytes: trace = density fetches x 32 B (8 fp32 texels);
+    # gather = 192 + 192 trilinear fetches x 32 B + 383 bilinear x 16 B + the
+    # 581 fp32 descriptor values written, per active pixel.
+    trace_bytes = fetches * 32.0
+    gather_bytes = active * (384 * 32 + 383 * 16 + 581 * 4)
+    stages = {
+        "nn_trace": {"bound": "hbm", "kernel": "k_nn_trace", "ms": trace_ms,
+                     "achieved": trace_bytes / (trace_ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s"},
+        "nn_gather": {"bound": "hbm", "kernel": "k_gather_fm", "ms": gather_ms,
+                      "achieved": gather_bytes / (gather_ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s"},
+        "nn_network": {"bound": "tensor", "kernel": "k_mlp_simt (fp32 network, CUDA cores)", "ms": mlp_ms32,
+                       "achieved": FLOP_PER_PIXEL * active / (mlp_ms32 / 1e3) / 1e12, "peak": bf16,
+                       "unit": "TFLOP/s"},
+    }
+    for s_ in stages.values():
+        s_["frac"] = s_["achieved"] / s_["peak"]
+        s_["peak_source"] = src
+        s_["traffic"] = None
+    dom = max(stages, key=lambda k: stages[k]["ms"])
+    roofline = dict(stages[dom], stage=dom)
     line = {"metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
@@ -259,9 +303,16 @@ def main():
                     "d2h_bytes_per_step": WIDTH * HEIGHT * 3 * 4},
             "gpu_launches": int(sum(stage_n[i] for i in range(8))),
             "roofline": roofline, "clocks": clk,
-            "stages_ms_per_step": {"nn_trace": stage_ms[1] / max(1, stage_n[1]),
-                                   "nn_gather_network": stage_ms[2] / max(1, stage_n[2])},
-            "active_pixels_per_frame": active / max(1, args.steps)}
+            "stage_rooflines": stages,
+            "active_pixels_per_frame": active,
+            "density_fetches_per_frame": fetches,
+            "bf16": {"value": world * args.steps / (bf_ms / 1000.0), "unit": "frames/s",
+                     "ms_per_step": bf_ms / args.steps,
+                     "stages_ms_per_step": {"nn_trace": bf_stage[1] / max(1, bf_n[1]),
+                                            "nn_gather": bf_stage[2] / max(1, bf_n[2]), "nn_network_tc": mlp_ms},
+                     "roofline": {"bound": "tensor", "kernel": "k_mlp_tc (tcgen05 BF16 network)",
+                                  "achieved": bf_tflops, "peak": bf16, "unit": "TFLOP/s", "frac": bf_tflops / bf16,
+                                  "peak_source": src, "traffic": None}}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(v, dens, p, w, st)
     if rank == 0:

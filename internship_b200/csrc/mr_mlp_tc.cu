@@ -193,7 +193,8 @@ __device__ __forceinline__ float sigm(float x) { return 1.0f / (1.0f + expf(-x))
 struct TcArgs {
   const uint8_t* __restrict__ wpack;  // kWBytes packed bf16 image
   const float* __restrict__ w;        // fp32 blob (biases, SE and small layers)
-  const float* __restrict__ desc;     // n x 576
+  const float* __restrict__ desc;     // row k feature i at desc[k*rs + i*fs]
+  long long rs, fs, ars, afs;         // descriptor / aux strides
   const float* __restrict__ aux;      // n x 5
   int n;
   float* out;                         // n x 3, or image when pix != null
@@ -202,6 +203,14 @@ struct TcArgs {
   const unsigned* __restrict__ count; // compose mode: number of records (device)
   F3 light_color, scatter;
   int* err;                           // set on a wait timeout
+};
+
+// One descriptor row: feature i at p[i*fs] (fs = 1 row-major, fs = capacity
+// feature-major).
+struct DIn {
+  const float* __restrict__ p;
+  long long fs;
+  __device__ __forceinline__ float operator[](int i) const { return __ldg(p + i * fs); }
 };
 
 struct GroupCtx {
@@ -255,7 +264,7 @@ __device__ __forceinline__ void epi_relu(const GroupCtx& c, int col, const float
 // width S on the descriptor row d, pooling into the SEFin1 accumulators.
 // MODE: 0 = SE, then ADD3; 1 = SERES, then ADD3; 2 = SERES, then REP3.
 template <int S, int MODE>
-__device__ __forceinline__ void trunk_block(GroupCtx& c, const float* __restrict__ d, const float* __restrict__ w,
+__device__ __forceinline__ void trunk_block(GroupCtx& c, const DIn& d, const float* __restrict__ w,
                                             int from, int pid, int sew0, int sew1, int layer0, float g, float gamma,
                                             float (&y)[3][32], float* fin) {
   constexpr int KP = S < 16 ? 16 : S;
@@ -266,7 +275,7 @@ __device__ __forceinline__ void trunk_block(GroupCtx& c, const float* __restrict
     float s = 0.0f, m = -10000.0f;
 #pragma unroll
     for (int i = 0; i < S; ++i) {
-      float v = __ldg(d + br * 192 + from + i);
+      float v = d[br * 192 + from + i];
       s += v;
       m = fmaxf(m, v);
     }
@@ -311,7 +320,7 @@ __device__ __forceinline__ void trunk_block(GroupCtx& c, const float* __restrict
     for (int i = 0; i < KP; ++i) {
       float v = 0.0f;
       if (i < S) {
-        v = __ldg(d + br * 192 + from + i) * gate[br];
+        v = d[br * 192 + from + i] * gate[br];
         if (MODE != 0) v = v + y[br][i];
       }
       x[i] = v;
@@ -331,7 +340,7 @@ __device__ __forceinline__ void trunk_block(GroupCtx& c, const float* __restrict
     epi_relu<S>(c, 32 * br, w + kTcBias(layer0 + br), yn);
 #pragma unroll
     for (int i = 0; i < S; ++i) {
-      float s = __ldg(d + br * 192 + from + i);
+      float s = d[br * 192 + from + i];
       if (MODE == 2) {
         y[br][i] = yn[i];
         y[br][S + i] = s;
@@ -424,7 +433,7 @@ __device__ __forceinline__ void head_input(GroupCtx& c, const float* __restrict_
 
 // Light-direction trunk block (width 8).
 template <int MODE>
-__device__ __forceinline__ void di_block(GroupCtx& c, const float* __restrict__ d, const float* __restrict__ w,
+__device__ __forceinline__ void di_block(GroupCtx& c, const DIn& d, const float* __restrict__ w,
                                          int blk, float g, float gamma, float (&y)[3][32], float* fin) {
   const int sew0[4] = {WOFF(LDSE01W), WOFF(LDSE11W), WOFF(LDSE21W), WOFF(LDSE31W)};
   const int sew1[4] = {WOFF(LDSE02W), WOFF(LDSE12W), WOFF(LDSE22W), WOFF(LDSE32W)};
@@ -475,10 +484,10 @@ __global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(TcArgs a) {
     if (tile * 128 >= n) break;  // group-uniform exit
     const int row = tile * 128 + t;
     const int kk = row < n ? row : n - 1;
-    const float* d = a.desc + (size_t)576 * kk;
-    const float gg = __ldg(a.aux + 5 * (size_t)kk), gamma = __ldg(a.aux + 5 * (size_t)kk + 1);
-    float srp[3] = {__ldg(a.aux + 5 * (size_t)kk + 2), __ldg(a.aux + 5 * (size_t)kk + 3),
-                    __ldg(a.aux + 5 * (size_t)kk + 4)};
+    const DIn d{a.desc + (long long)kk * a.rs, a.fs};
+    const float* ax = a.aux + (long long)kk * a.ars;
+    const float gg = __ldg(ax), gamma = __ldg(ax + a.afs);
+    float srp[3] = {__ldg(ax + 2 * a.afs), __ldg(ax + 3 * a.afs), __ldg(ax + 4 * a.afs)};
     float fin[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) fin[j] = 0.0f;
@@ -668,8 +677,9 @@ void free_packed(Network* n) {
 
 // Launch the tensor-core network. pix/trph/count != null selects compose
 // mode (out = image). The error word lives after the packed image.
-int launch_mlp_tc(const Network* net, const float* desc, const float* aux, int n, float* out, const int* pix,
-                  const float* trph, const unsigned* count, F3 light_color, F3 scatter, cudaStream_t s) {
+int launch_mlp_tc(const Network* net, const float* desc, const float* aux, long long rs, long long fs,
+                  long long ars, long long afs, int n, float* out, const int* pix, const float* trph,
+                  const unsigned* count, F3 light_color, F3 scatter, cudaStream_t s) {
   static bool attr = false;
   if (!attr) {
     MR_CUDA(cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
@@ -680,6 +690,10 @@ int launch_mlp_tc(const Network* net, const float* desc, const float* aux, int n
   a.w = net->w;
   a.desc = desc;
   a.aux = aux;
+  a.rs = rs;
+  a.fs = fs;
+  a.ars = ars;
+  a.afs = afs;
   a.n = n;
   a.out = out;
   a.pix = pix;

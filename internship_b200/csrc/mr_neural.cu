@@ -40,6 +40,44 @@ __device__ __forceinline__ float shadow_tr(const Tables& t, F3 p, F3 L, int mip)
 
 struct Frame { F3 X, Y, Z, LX; };
 
+// Descriptor gather for one point (core/radiancePredict.cu:319-359); each
+// stencil point's three values go to sink(i, density, transmittance, phase).
+template <class Sink>
+__device__ __forceinline__ void gather_sink(const Tables& t, const float* __restrict__ stencil, F3 pos, F3 L,
+                                            const Frame& f, float alpha, float g, Sink sink) {
+  const float kLutAngle = 3.1415926535f * 60.0f / 180.0f;
+  const float hg0 = logf(hg_phase(dot(f.X, L), g) + 1.0f);
+#pragma unroll 2
+  for (int i = 0; i < 192; ++i) {
+    StencilInfo si = stencil_info(i);
+    F3 p;
+    if (si.type >= 4) {
+      float sx = __ldg(stencil + 3 * i), sy = __ldg(stencil + 3 * i + 1), sz = __ldg(stencil + 3 * i + 2);
+      p = pos + ((f.X * sx + f.Y * sy + f.Z * sz) * si.offset);
+    } else {
+      p = pos + L * si.offset;
+    }
+    int mip = si.mip;
+    float xv = logf(1.0f + alpha * mip_density(t, mip, p) / 64.0f);
+    float xh;
+    if (si.localindex == 0) {
+      xh = hg0;
+    } else {
+      F3 md = normalize(p - pos);
+      float radius = (float)(1 << mip) / 256.0f;
+      float angle = atanf(0.5f * radius / si.offset);
+      float c1 = dot(f.X, md), c2 = dot(f.LX, md);
+      float u1 = c1 * 0.5f + 0.5f, u2 = c2 * 0.5f + 0.5f;
+      float v = angle / kLutAngle;
+      float h0 = bilinear_clamp(t.lut, kLut, kLut, u1, v);
+      float h1 = bilinear_clamp(t.lut, kLut, kLut, u2, v);
+      xh = logf(h0 * h1 + 1.0f);
+    }
+    float xs = shadow_tr(t, p, f.LX, max(mip - 1, 0));
+    sink(i, xv, xs, xh);
+  }
+}
+
 // Descriptor gather for one point (core/radiancePredict.cu:319-359).
 __device__ __forceinline__ void gather_point(const Tables& t, const float* __restrict__ stencil, F3 pos, F3 L,
                                              const Frame& f, float alpha, float g, float* xv, float* xs,
@@ -256,27 +294,37 @@ __global__ void __launch_bounds__(64) k_predict_simt(const float* __restrict__ w
   out[3 * (size_t)k + 2] = r.z;
 }
 
-// Gather for the compacted records (tensor-core path): desc / aux rows k.
-__global__ void __launch_bounds__(128) k_gather_records(Tables t, const float* __restrict__ stencil, Records rec,
-                                                        int capacity, F3 L, float alpha, float g, F3 srp,
-                                                        float* __restrict__ desc, float* __restrict__ aux) {
+// Gather for the compacted records, feature-major: feature i of record k at
+// desc[i*cap + k] (aux likewise), so that a warp's stores and the network's
+// loads of one feature are single coalesced transactions.
+__global__ void __launch_bounds__(128) k_gather_fm(Tables t, const float* __restrict__ stencil, Records rec,
+                                                   int cap, F3 L, float alpha, float g, F3 srp,
+                                                   float* __restrict__ desc, float* __restrict__ aux) {
   unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned n = min(*rec.count, (unsigned)capacity);
+  unsigned n = min(*rec.count, (unsigned)cap);
   if (k >= n) return;
-  float xv[192], xs[192], xh[192];
   F3 pos = f3(rec.pos[3 * (size_t)k], rec.pos[3 * (size_t)k + 1], rec.pos[3 * (size_t)k + 2]);
   Frame f = load_frame(rec.frame + 12 * (size_t)k);
-  gather_point(t, stencil, pos, L, f, alpha, g, xv, xs, xh);
-  float* d = desc + 576 * (size_t)k;
-  for (int i = 0; i < 192; ++i) { d[i] = xv[i]; d[192 + i] = xs[i]; d[384 + i] = xh[i]; }
-  float* ax = aux + 5 * (size_t)k;
-  ax[0] = g;
-  ax[1] = acosf(dot(f.X, f.LX));
-  ax[2] = srp.x; ax[3] = srp.y; ax[4] = srp.z;
+  float* d = desc + k;
+  const size_t c = (size_t)cap;
+  gather_sink(t, stencil, pos, L, f, alpha, g, [&](int i, float xv, float xs, float xh) {
+    d[i * c] = xv;
+    d[(192 + i) * c] = xs;
+    d[(384 + i) * c] = xh;
+  });
+  aux[k] = g;
+  aux[c + k] = acosf(dot(f.X, f.LX));
+  aux[2 * c + k] = srp.x;
+  aux[3 * c + k] = srp.y;
+  aux[4 * c + k] = srp.z;
 }
 
-int launch_mlp_tc(const Network* net, const float* desc, const float* aux, int n, float* out, const int* pix,
-                  const float* trph, const unsigned* count, F3 light_color, F3 scatter, cudaStream_t s);
+int launch_mlp_tc(const Network* net, const float* desc, const float* aux, long long rs, long long fs,
+                  long long ars, long long afs, int n, float* out, const int* pix, const float* trph,
+                  const unsigned* count, F3 light_color, F3 scatter, cudaStream_t s);
+int launch_mlp_simt(const Network* net, const float* desc, const float* aux, long long rs, long long fs,
+                    long long ars, long long afs, int n, const unsigned* count, float* out, const int* pix,
+                    const float* trph, F3 light_color, F3 scatter, cudaStream_t s);
 int mlp_tc_error(const Network* net, bool reset);
 
 extern int check_params(const mr_render_params* p);
@@ -314,9 +362,9 @@ int render_neural(Volume* v, const Network* net, const mr_render_params* p, floa
   }
   size_t npx = (size_t)p->width * p->height;
   const bool tc = p->precision == MR_PREC_BF16;
-  // records, then (tensor-core path) descriptor rows and aux rows
+  // records, then the feature-major descriptor and aux columns
   size_t rbytes = (records_bytes(npx) + 255) / 256 * 256;
-  size_t need = rbytes + (tc ? npx * (576 + 5) * sizeof(float) + 256 : 0);
+  size_t need = rbytes + npx * (576 + 5) * sizeof(float) + 256;
   int rc = ensure_scratch(v, need, s);
   if (rc) return rc;
   Records rec = carve_records(v->scratch, npx);
@@ -337,36 +385,22 @@ int render_neural(Volume* v, const Network* net, const mr_render_params* p, floa
   k_nn_trace<<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(ta);
   v->timer.mark(ST_NN_TRACE, s);
   MR_CUDA(cudaGetLastError());
-  if (tc) {
-    F3 sr = to_f3(p->scatter_rate) / 1.001f;
-    v->timer.mark(ST_NN_PREDICT, s);
-    k_gather_records<<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(Tables{v->mips, v->tr, v->lut}, net->stencil, rec,
-                                                                   (int)npx, L, p->alpha, p->g, srp_of(sr), desc, aux);
-    v->timer.mark(ST_NN_PREDICT, s);
-    MR_CUDA(cudaGetLastError());
-    v->timer.mark(ST_NN_MLP, s);
-    rc = launch_mlp_tc(net, desc, aux, (int)npx, dev_rgb, rec.pix, rec.trph, rec.count, to_f3(p->light_color),
-                       to_f3(p->scatter_rate), s);
-    v->timer.mark(ST_NN_MLP, s);
-    return rc;
-  }
-  NNPredictArgs pa;
-  pa.t = Tables{v->mips, v->tr, v->lut};
-  pa.w = net->w;
-  pa.stencil = net->stencil;
-  pa.rec = rec;
-  pa.capacity = (int)npx;
-  pa.L = L;
-  pa.light_color = to_f3(p->light_color);
-  pa.scatter = to_f3(p->scatter_rate);
-  pa.alpha = p->alpha;
-  pa.g = p->g;
-  pa.out = dev_rgb;
+  F3 sr = to_f3(p->scatter_rate) / 1.001f;
   v->timer.mark(ST_NN_PREDICT, s);
-  k_nn_predict_simt<<<(unsigned)((npx + 63) / 64), 64, 0, s>>>(pa);
+  k_gather_fm<<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(Tables{v->mips, v->tr, v->lut}, net->stencil, rec,
+                                                            (int)npx, L, p->alpha, p->g, srp_of(sr), desc, aux);
   v->timer.mark(ST_NN_PREDICT, s);
   MR_CUDA(cudaGetLastError());
-  return MR_OK;
+  const long long cap = (long long)npx;
+  v->timer.mark(ST_NN_MLP, s);
+  if (tc)
+    rc = launch_mlp_tc(net, desc, aux, 1, cap, 1, cap, (int)npx, dev_rgb, rec.pix, rec.trph, rec.count,
+                       to_f3(p->light_color), to_f3(p->scatter_rate), s);
+  else
+    rc = launch_mlp_simt(net, desc, aux, 1, cap, 1, cap, (int)npx, rec.count, dev_rgb, rec.pix, rec.trph,
+                         to_f3(p->light_color), to_f3(p->scatter_rate), s);
+  v->timer.mark(ST_NN_MLP, s);
+  return rc;
 }
 
 }  // namespace mr
@@ -399,10 +433,9 @@ extern "C" int mr_radiance_predict(const mr_network* nh, int32_t precision, cons
   if (n < 0) return set_error(MR_ERR_ARG, "n < 0");
   if (n == 0) return MR_OK;
   if (precision == MR_PREC_BF16)
-    return launch_mlp_tc(&nh->n, dev_desc, dev_aux, n, dev_out, nullptr, nullptr, nullptr, f3(1, 1, 1), f3(1, 1, 1),
-                         (cudaStream_t)stream);
+    return launch_mlp_tc(&nh->n, dev_desc, dev_aux, 576, 1, 5, 1, n, dev_out, nullptr, nullptr, nullptr, f3(1, 1, 1),
+                         f3(1, 1, 1), (cudaStream_t)stream);
   if (precision != MR_PREC_FP32) return set_error(MR_ERR_UNSUPPORTED, "precision %d not built", precision);
-  k_predict_simt<<<(n + 63) / 64, 64, 0, (cudaStream_t)stream>>>(nh->n.w, dev_desc, dev_aux, n, dev_out);
-  MR_CUDA(cudaGetLastError());
-  return MR_OK;
+  return launch_mlp_simt(&nh->n, dev_desc, dev_aux, 576, 1, 5, 1, n, nullptr, dev_out, nullptr, nullptr, f3(1, 1, 1),
+                         f3(1, 1, 1), (cudaStream_t)stream);
 }
