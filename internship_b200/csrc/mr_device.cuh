@@ -88,6 +88,11 @@ __host__ __device__ __forceinline__ F3 uniform_sphere(float ex, float ey) {
   return {st * cp, st * sp, ct};
 }
 
+// srp = scatterrate^4 per channel (core/radiancePredict.cu:388).
+__host__ __device__ __forceinline__ F3 srp_of(F3 sr) {
+  return f3((sr.x * sr.x) * (sr.x * sr.x), (sr.y * sr.y) * (sr.y * sr.y), (sr.z * sr.z) * (sr.z * sr.z));
+}
+
 // ---- Philox4x32-10 (Salmon et al., SC'11) -------------------------------------
 __host__ __device__ __forceinline__ void philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
                                                        uint32_t k0, uint32_t k1, uint32_t out[4]) {

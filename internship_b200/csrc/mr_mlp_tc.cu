@@ -11,8 +11,9 @@
 // The packed BF16 weight image (canonical K-major, no swizzle: 8x16-byte core
 // matrices, row groups SBO apart, K halves LBO = 128 B apart) is loaded into
 // shared memory once per CTA and shared by the groups. Each group owns a
-// 24 KB trunk A region (3 branch tiles of 128 x 32), a 32 KB head A region
-// (128 x 128), 128 TMEM columns and an mbarrier signalled by tcgen05.commit.
+// 32 KB A region (three 128 x 32 branch tiles in the trunks, one 128 x 128
+// tile in the head), 128 TMEM columns and an mbarrier signalled by
+// tcgen05.commit.
 // Only the elected thread 0 of a group issues MMAs. Every wait is bounded.
 #include <cuda_bf16.h>
 
@@ -65,12 +66,16 @@ __constant__ TcTables c_tc = make_tc_tables();
 __device__ __forceinline__ int tc_offset_dev(int i) { return c_tc.woff[i]; }
 __device__ __forceinline__ int kTcBias(int i) { return c_tc.boff[i]; }
 
-constexpr int kGroups = 2;
+constexpr int kGroups = 3;
 constexpr int kTrunkBytes = 3 * 128 * 32 * 2;  // 24 KB
 constexpr int kHeadBytes = 128 * 128 * 2;      // 32 KB
-constexpr int kGroupBytes = kTrunkBytes + kHeadBytes;
+// The trunk tiles and the head tile of a group share one region: every
+// layer's MMA has completed (mbarrier) before its epilogue overwrites it.
+constexpr int kGroupBytes = kHeadBytes;
+static_assert(kTrunkBytes <= kHeadBytes, "trunk tiles alias the head tile");
 constexpr int kSmemBytes = kWBytes + kGroups * kGroupBytes + 64 * kGroups + 16;
-constexpr int kTmemCols = 256;  // 128 per group
+constexpr int kTmemCols = 512;  // 128 per group (power of two allocation)
+static_assert(128 * kGroups <= kTmemCols, "tensor memory budget");
 static_assert(kSmemBytes <= 232448, "shared memory budget");
 
 // Byte offset of element (row, k) of a K-major tile with KP columns.
@@ -160,6 +165,19 @@ __device__ __forceinline__ void store_row(uint8_t* tile, int row, const float* x
     q.z = pack_bf16(x[8 * kg + 4], x[8 * kg + 5]);
     q.w = pack_bf16(x[8 * kg + 6], x[8 * kg + 7]);
     *reinterpret_cast<uint4*>(tile + canon_off(row, 8 * kg, KP)) = q;
+  }
+}
+// N columns starting at column k0 (a multiple of 8) of row `row`.
+template <int KP, int N>
+__device__ __forceinline__ void store_cols(uint8_t* tile, int row, int k0, const float* x) {
+#pragma unroll
+  for (int kg = 0; kg < N / 8; ++kg) {
+    uint4 q;
+    q.x = pack_bf16(x[8 * kg + 0], x[8 * kg + 1]);
+    q.y = pack_bf16(x[8 * kg + 2], x[8 * kg + 3]);
+    q.z = pack_bf16(x[8 * kg + 4], x[8 * kg + 5]);
+    q.w = pack_bf16(x[8 * kg + 6], x[8 * kg + 7]);
+    *reinterpret_cast<uint4*>(tile + canon_off(row, k0 + 8 * kg, KP)) = q;
   }
 }
 template <int KP>
@@ -264,7 +282,7 @@ __device__ __forceinline__ void epi_relu(const GroupCtx& c, int col, const float
 // width S on the descriptor row d, pooling into the SEFin1 accumulators.
 // MODE: 0 = SE, then ADD3; 1 = SERES, then ADD3; 2 = SERES, then REP3.
 template <int S, int MODE>
-__device__ __forceinline__ void trunk_block(GroupCtx& c, const DIn& d, const float* __restrict__ w,
+__device__ __noinline__ void trunk_block(GroupCtx& c, const DIn& d, const float* __restrict__ w,
                                             int from, int pid, int sew0, int sew1, int layer0, float g, float gamma,
                                             float (&y)[3][32], float* fin) {
   constexpr int KP = S < 16 ? 16 : S;
@@ -353,19 +371,23 @@ __device__ __forceinline__ void trunk_block(GroupCtx& c, const DIn& d, const flo
 
 // Head SC(p) (radiancePredict.cu:439-473) for one albedo channel; the
 // gated 128-wide input is already in c.head (bf16). Returns the output X.
-__device__ __forceinline__ float head_chain(GroupCtx& c, const float* __restrict__ w) {
+__device__ __noinline__ float head_chain(GroupCtx& c, const float* __restrict__ w) {
   const uint32_t hb = smem_u32(c.head), tb = smem_u32(c.trunk), wb = smem_u32(c.wsm);
-  float v[128];
-  // LC0 128 -> 128
+  float v[32];
+  // LC0 128 -> 128, read back and re-stored 32 columns at a time
   mma_round(c, [&]() { issue_layer<128, 128>(c.tmem, hb, wb + tc_offset(TC_LC0)); });
-#pragma unroll
-  for (int h = 0; h < 4; ++h) epi_relu<32>(c, 32 * h, w + WOFF(LC0B) + 32 * h, v + 32 * h);
-  store_row<128>(c.head, c.t, v);
+#pragma unroll 1
+  for (int h = 0; h < 4; ++h) {
+    epi_relu<32>(c, 32 * h, w + WOFF(LC0B) + 32 * h, v);
+    store_cols<128, 32>(c.head, c.t, 32 * h, v);
+  }
   // LC1 128 -> 64
   mma_round(c, [&]() { issue_layer<64, 128>(c.tmem, hb, wb + tc_offset(TC_LC1)); });
-  epi_relu<32>(c, 0, w + WOFF(LC1B), v);
-  epi_relu<32>(c, 32, w + WOFF(LC1B) + 32, v + 32);
-  store_row<64>(c.trunk, c.t, v);
+#pragma unroll 1
+  for (int h = 0; h < 2; ++h) {
+    epi_relu<32>(c, 32 * h, w + WOFF(LC1B) + 32 * h, v);
+    store_cols<64, 32>(c.trunk, c.t, 32 * h, v);
+  }
   // LC2 64 -> 32
   mma_round(c, [&]() { issue_layer<32, 64>(c.tmem, tb, wb + tc_offset(TC_LC2)); });
   epi_relu<32>(c, 0, w + WOFF(LC2B), v);
@@ -396,19 +418,18 @@ __device__ __forceinline__ float head_chain(GroupCtx& c, const float* __restrict
 }
 
 // Builds the gated head input for albedo channel value srp into c.head.
-__device__ __forceinline__ void head_input(GroupCtx& c, const float* __restrict__ w, const float* comb_raw,
+__device__ __noinline__ void head_input(GroupCtx& c, const float* __restrict__ w, const float* comb_raw,
                                            const float* fin, float g, float gamma, float srp) {
   // pool[72..74] = g, gamma, srp: LGGS (3 -> 8, bias last) and LSEFin1's last columns
-  float x[128];
-#pragma unroll
-  for (int i = 0; i < 120; ++i) x[i] = comb_raw[i];
+  float x8[8];
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     float a = g * __ldg(w + WOFF(LGGSW) + 3 * i) + gamma * __ldg(w + WOFF(LGGSW) + 3 * i + 1) +
               srp * __ldg(w + WOFF(LGGSW) + 3 * i + 2);
     a += __ldg(w + WOFF(LGGSB) + i);
-    x[120 + i] = a >= 0.0f ? a : 0.0f;
+    x8[i] = a >= 0.0f ? a : 0.0f;
   }
+  store_cols<128, 8>(c.head, c.t, 120, x8);
   float sew[16];
   const float* f1 = w + WOFF(LSEFin1W);
 #pragma unroll
@@ -424,11 +445,15 @@ __device__ __forceinline__ void head_input(GroupCtx& c, const float* __restrict_
     for (int j = 0; j < 16; ++j) a += sew[j] * __ldg(w + WOFF(LSEFin2W) + j + i * 16);
     sep[i] = sigm(a);
   }
+  // gated comb, 8 columns at a time: segments [0,32) [32,64) [64,96) use
+  // gates 0..2, [96,104) [104,112) [112,120) gates 3..5
+#pragma unroll 1
+  for (int g8 = 0; g8 < 15; ++g8) {
+    const float s = sep[g8 < 12 ? g8 / 4 : g8 - 9];
 #pragma unroll
-  for (int i = 0; i < 32; ++i) { x[i] *= sep[0]; x[32 + i] *= sep[1]; x[64 + i] *= sep[2]; }
-#pragma unroll
-  for (int i = 0; i < 8; ++i) { x[96 + i] *= sep[3]; x[104 + i] *= sep[4]; x[112 + i] *= sep[5]; }
-  store_row<128>(c.head, c.t, x);
+    for (int i = 0; i < 8; ++i) x8[i] = comb_raw[8 * g8 + i] * s;
+    store_cols<128, 8>(c.head, c.t, 8 * g8, x8);
+  }
 }
 
 // Light-direction trunk block (width 8).
@@ -466,7 +491,7 @@ __global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(TcArgs a) {
 
   GroupCtx c;
   c.trunk = gbase + g * kGroupBytes;
-  c.head = c.trunk + kTrunkBytes;
+  c.head = c.trunk;
   c.tmem = *tmem_holder + (uint32_t)(128 * g);
   c.tlane = (uint32_t)(32 * (warp & 3)) << 16;
   c.mbar = smem_u32(mbars + g);
@@ -492,7 +517,12 @@ __global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(TcArgs a) {
 #pragma unroll
     for (int j = 0; j < 16; ++j) fin[j] = 0.0f;
     float y[3][32];
-    float comb[120];
+    // comb (the head input before gating) lives in local memory through an
+    // opaque offset; it is written in chunks and read once per head.
+    float comb_store[120];
+    int zero = 0;
+    asm volatile("" : "+r"(zero));
+    float* comb = comb_store + zero;
     // main trunk (radiancePredict.cu:396-421)
     trunk_block<8, 0>(c, d, w, 0, 0, WOFF(LSE01W), WOFF(LSE02W), TC_MAIN + 0, gg, gamma, y, fin);
     trunk_block<8, 2>(c, d, w, 8, 3, WOFF(LSE11W), WOFF(LSE12W), TC_MAIN + 3, gg, gamma, y, fin);

@@ -7,7 +7,7 @@
 //  2. k_nn_predict_simt: per active record, the 192-point multi-scale
 //     descriptor gather (core/radiancePredict.cu:319-368) and the network body.
 #include "mr_internal.h"
-#include "mr_net_simt.cuh"
+#include "mr_net_layout.cuh"
 #include "mr_track.cuh"
 
 namespace mr {
@@ -39,78 +39,6 @@ __device__ __forceinline__ float shadow_tr(const Tables& t, F3 p, F3 L, int mip)
 }
 
 struct Frame { F3 X, Y, Z, LX; };
-
-// Descriptor gather for one point (core/radiancePredict.cu:319-359); each
-// stencil point's three values go to sink(i, density, transmittance, phase).
-template <class Sink>
-__device__ __forceinline__ void gather_sink(const Tables& t, const float* __restrict__ stencil, F3 pos, F3 L,
-                                            const Frame& f, float alpha, float g, Sink sink) {
-  const float kLutAngle = 3.1415926535f * 60.0f / 180.0f;
-  const float hg0 = logf(hg_phase(dot(f.X, L), g) + 1.0f);
-#pragma unroll 2
-  for (int i = 0; i < 192; ++i) {
-    StencilInfo si = stencil_info(i);
-    F3 p;
-    if (si.type >= 4) {
-      float sx = __ldg(stencil + 3 * i), sy = __ldg(stencil + 3 * i + 1), sz = __ldg(stencil + 3 * i + 2);
-      p = pos + ((f.X * sx + f.Y * sy + f.Z * sz) * si.offset);
-    } else {
-      p = pos + L * si.offset;
-    }
-    int mip = si.mip;
-    float xv = logf(1.0f + alpha * mip_density(t, mip, p) / 64.0f);
-    float xh;
-    if (si.localindex == 0) {
-      xh = hg0;
-    } else {
-      F3 md = normalize(p - pos);
-      float radius = (float)(1 << mip) / 256.0f;
-      float angle = atanf(0.5f * radius / si.offset);
-      float c1 = dot(f.X, md), c2 = dot(f.LX, md);
-      float u1 = c1 * 0.5f + 0.5f, u2 = c2 * 0.5f + 0.5f;
-      float v = angle / kLutAngle;
-      float h0 = bilinear_clamp(t.lut, kLut, kLut, u1, v);
-      float h1 = bilinear_clamp(t.lut, kLut, kLut, u2, v);
-      xh = logf(h0 * h1 + 1.0f);
-    }
-    float xs = shadow_tr(t, p, f.LX, max(mip - 1, 0));
-    sink(i, xv, xs, xh);
-  }
-}
-
-// Descriptor gather for one point (core/radiancePredict.cu:319-359).
-__device__ __forceinline__ void gather_point(const Tables& t, const float* __restrict__ stencil, F3 pos, F3 L,
-                                             const Frame& f, float alpha, float g, float* xv, float* xs,
-                                             float* xh) {
-  const float kLutAngle = 3.1415926535f * 60.0f / 180.0f;
-#pragma unroll 1
-  for (int i = 0; i < 192; ++i) {
-    StencilInfo si = stencil_info(i);
-    F3 p;
-    if (si.type >= 4) {
-      float sx = __ldg(stencil + 3 * i), sy = __ldg(stencil + 3 * i + 1), sz = __ldg(stencil + 3 * i + 2);
-      p = pos + ((f.X * sx + f.Y * sy + f.Z * sz) * si.offset);
-    } else {
-      p = pos + L * si.offset;
-    }
-    int mip = si.mip;
-    xv[i] = logf(1.0f + alpha * mip_density(t, mip, p) / 64.0f);
-    if (si.localindex == 0) {
-      xh[i] = logf(hg_phase(dot(f.X, L), g) + 1.0f);
-    } else {
-      F3 md = normalize(p - pos);
-      float radius = (float)(1 << mip) / 256.0f;
-      float angle = atanf(0.5f * radius / si.offset);
-      float c1 = dot(f.X, md), c2 = dot(f.LX, md);
-      float u1 = c1 * 0.5f + 0.5f, u2 = c2 * 0.5f + 0.5f;
-      float v = angle / kLutAngle;
-      float h0 = bilinear_clamp(t.lut, kLut, kLut, u1, v);
-      float h1 = bilinear_clamp(t.lut, kLut, kLut, u2, v);
-      xh[i] = logf(h0 * h1 + 1.0f);
-    }
-    xs[i] = shadow_tr(t, p, f.LX, max(mip - 1, 0));
-  }
-}
 
 // GetMatrixFromNormal (core/render.cuh:355-369), rejection capped at 64 tries.
 __device__ __forceinline__ void frame_from(Rng& rng, F3 v1, F3& a, F3& b, F3& c) {
@@ -220,17 +148,6 @@ __global__ void __launch_bounds__(128) k_nn_trace(NNTraceArgs a) {
   }
 }
 
-struct NNPredictArgs {
-  Tables t;
-  const float* __restrict__ w;
-  const float* __restrict__ stencil;
-  Records rec;
-  int capacity;
-  F3 L, light_color, scatter;
-  float alpha, g;
-  float* out;
-};
-
 inline __device__ Frame load_frame(const float* fr) {
   Frame f;
   f.X = f3(fr[0], fr[1], fr[2]);
@@ -240,25 +157,151 @@ inline __device__ Frame load_frame(const float* fr) {
   return f;
 }
 
-// Gather + per-thread network, one active record per thread.
-__global__ void __launch_bounds__(64) k_nn_predict_simt(NNPredictArgs a) {
-  unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned n = min(*a.rec.count, (unsigned)a.capacity);
-  if (k >= n) return;
-  NetSIMT s;
-  F3 pos = f3(a.rec.pos[3 * (size_t)k], a.rec.pos[3 * (size_t)k + 1], a.rec.pos[3 * (size_t)k + 2]);
-  Frame f = load_frame(a.rec.frame + 12 * (size_t)k);
-  gather_point(a.t, a.stencil, pos, a.L, f, a.alpha, a.g, s.xv, s.xs, s.xh);
-  F3 sr = a.scatter / 1.001f;
-  float gamma = acosf(dot(f.X, f.LX));
-  n_trunks(s, a.w, a.g, gamma);
-  F3 pred = n_heads(s, a.w, srp_of(sr));
-  pred = pred + a.rec.trph[k];
-  F3 o = vmax((pred * a.light_color) * a.scatter, f3(0, 0, 0));
-  int pix = a.rec.pix[k];
-  a.out[3 * (size_t)pix + 0] = o.x;
-  a.out[3 * (size_t)pix + 1] = o.y;
-  a.out[3 * (size_t)pix + 2] = o.z;
+
+// ---- specialised gather ---------------------------------------------------------
+// The 192 stencil points fall into 12 segments of constant mip level and
+// offset (core/vector.cu:299-400). Per segment, the level's resolution and
+// table base are compile-time constants and the HG-table row v (from the cone
+// angle) is computed once. For a sphere point p - pos = off * (X s.x + Y s.y
+// + Z s.z) with an orthonormal frame, so the cone cosines are
+// dot(X, md) = s.x/|s| and dot(LX, md) = (LX.X s.x + LX.Y s.y + LX.Z s.z)/|s|;
+// for a light-direction point md = L. Same arithmetic as gather_sink up to
+// rounding.
+template <int RES>
+__device__ __forceinline__ float tri_border_c(const float* __restrict__ d, F3 uv) {
+  float px = uv.x * RES - 0.5f, py = uv.y * RES - 0.5f, pz = uv.z * RES - 0.5f;
+  float fx = floorf(px), fy = floorf(py), fz = floorf(pz);
+  int x = (int)fx, y = (int)fy, z = (int)fz;
+  float wx = px - fx, wy = py - fy, wz = pz - fz;
+  bool x0 = (unsigned)x < (unsigned)RES, x1 = (unsigned)(x + 1) < (unsigned)RES;
+  bool y0 = (unsigned)y < (unsigned)RES, y1 = (unsigned)(y + 1) < (unsigned)RES;
+  bool z0 = (unsigned)z < (unsigned)RES, z1 = (unsigned)(z + 1) < (unsigned)RES;
+  const float* b = d + (x * RES + y) * RES + z;  // 32-bit index: RES^3 < 2^31
+  float c000 = (x0 && y0 && z0) ? __ldg(b) : 0.0f;
+  float c001 = (x0 && y0 && z1) ? __ldg(b + 1) : 0.0f;
+  float c010 = (x0 && y1 && z0) ? __ldg(b + RES) : 0.0f;
+  float c011 = (x0 && y1 && z1) ? __ldg(b + RES + 1) : 0.0f;
+  float c100 = (x1 && y0 && z0) ? __ldg(b + RES * RES) : 0.0f;
+  float c101 = (x1 && y0 && z1) ? __ldg(b + RES * RES + 1) : 0.0f;
+  float c110 = (x1 && y1 && z0) ? __ldg(b + RES * RES + RES) : 0.0f;
+  float c111 = (x1 && y1 && z1) ? __ldg(b + RES * RES + RES + 1) : 0.0f;
+  return lerpf(lerpf(lerpf(c000, c001, wz), lerpf(c010, c011, wz), wy),
+               lerpf(lerpf(c100, c101, wz), lerpf(c110, c111, wz), wy), wx);
+}
+template <int RES>
+__device__ __forceinline__ float tri_clamp_c(const float* __restrict__ d, F3 uv) {
+  float px = uv.x * RES - 0.5f, py = uv.y * RES - 0.5f, pz = uv.z * RES - 0.5f;
+  float fx = floorf(px), fy = floorf(py), fz = floorf(pz);
+  int x = (int)fx, y = (int)fy, z = (int)fz;
+  float wx = px - fx, wy = py - fy, wz = pz - fz;
+  int xa = min(max(x, 0), RES - 1), xb = min(max(x + 1, 0), RES - 1);
+  int ya = min(max(y, 0), RES - 1), yb = min(max(y + 1, 0), RES - 1);
+  int za = min(max(z, 0), RES - 1), zb = min(max(z + 1, 0), RES - 1);
+  const int ra = xa * RES * RES, rb = xb * RES * RES, sa = ya * RES, sb = yb * RES;
+  float c000 = __ldg(d + ra + sa + za), c001 = __ldg(d + ra + sa + zb);
+  float c010 = __ldg(d + ra + sb + za), c011 = __ldg(d + ra + sb + zb);
+  float c100 = __ldg(d + rb + sa + za), c101 = __ldg(d + rb + sa + zb);
+  float c110 = __ldg(d + rb + sb + za), c111 = __ldg(d + rb + sb + zb);
+  return lerpf(lerpf(lerpf(c000, c001, wz), lerpf(c010, c011, wz), wy),
+               lerpf(lerpf(c100, c101, wz), lerpf(c110, c111, wz), wy), wx);
+}
+
+struct PixelGather {
+  F3 pos, L, X, Y, Z, LX;
+  float lx, ly, lz;   // LX in the (X, Y, Z) frame
+  float cXL, cLXL;    // cone cosines of the light-direction points
+  float alpha, hg0;
+};
+
+constexpr unsigned kMipOff[9] = {0u, 16777216u, 18874368u, 19136512u, 19169280u, 19173376u, 19173888u, 19173952u,
+                                 19173960u};
+constexpr unsigned kTrOff[8] = {0u, 2097152u, 2359296u, 2392064u, 2396160u, 2396672u, 2396736u, 2396744u};
+
+// Stencil points [I0, I1) at mip level MIP, offset `off`; SPHERE selects the
+// rotated-stencil points (else the points along the light direction).
+template <int MIP, bool SPHERE, int I0, int I1, class Sink>
+__device__ __forceinline__ void gather_seg(const Tables& t, const float* __restrict__ stencil, const PixelGather& q,
+                                           float off, Sink& sink) {
+  constexpr int R = 256 >> MIP;
+  constexpr int TL = MIP > 0 ? MIP - 1 : 0;
+  constexpr int RT = 128 >> TL;
+  const float* mb = t.mips + kMipOff[MIP];
+  const float* tb = t.tr + kTrOff[TL];
+  const float radius = (float)(1 << MIP) / 256.0f;
+  const float vrow = atanf(0.5f * radius / off) / (3.1415926535f * 60.0f / 180.0f);
+#pragma unroll 2
+  for (int i = I0; i < I1; ++i) {
+    F3 p;
+    float c1, c2;
+    if (SPHERE) {
+      const float sx = __ldg(stencil + 3 * i), sy = __ldg(stencil + 3 * i + 1), sz = __ldg(stencil + 3 * i + 2);
+      p = q.pos + ((q.X * sx + q.Y * sy + q.Z * sz) * off);
+      const float inv = rsqrtf(sx * sx + sy * sy + sz * sz);
+      c1 = sx * inv;
+      c2 = (q.lx * sx + q.ly * sy + q.lz * sz) * inv;
+    } else {
+      p = q.pos + q.L * off;
+      c1 = q.cXL;
+      c2 = q.cLXL;
+    }
+    const float xv = __logf(1.0f + q.alpha * tri_border_c<R>(mb, p + 0.5f) / 64.0f);
+    float xh;
+    if (SPHERE && MIP == 0 && I0 == 0 && i == 0) {
+      xh = q.hg0;
+    } else {
+      const float h0 = bilinear_clamp(t.lut, kLut, kLut, c1 * 0.5f + 0.5f, vrow);
+      const float h1 = bilinear_clamp(t.lut, kLut, kLut, c2 * 0.5f + 0.5f, vrow);
+      xh = __logf(h0 * h1 + 1.0f);
+    }
+    float xs;
+    if (p.x < -0.5f || p.y < -0.5f || p.z < -0.5f || p.x > 0.5f || p.y > 0.5f || p.z > 0.5f) {
+      const float o2 = ray_box_offset(p, q.LX);
+      xs = o2 >= 0 ? tri_clamp_c<RT>(tb, p + q.LX * o2 + 0.5f) : 1.0f;
+    } else {
+      xs = tri_clamp_c<RT>(tb, p + 0.5f);
+    }
+    sink(i, xv, xs, xh);
+  }
+}
+
+template <class Sink>
+__device__ __forceinline__ void gather_fast(const Tables& t, const float* __restrict__ stencil, F3 pos, F3 L,
+                                            const Frame& f, float alpha, float g, Sink sink) {
+  PixelGather q;
+  q.pos = pos; q.L = L; q.X = f.X; q.Y = f.Y; q.Z = f.Z; q.LX = f.LX;
+  q.lx = dot(f.LX, f.X); q.ly = dot(f.LX, f.Y); q.lz = dot(f.LX, f.Z);
+  q.cXL = dot(f.X, L);
+  q.cLXL = dot(f.LX, L);
+  q.alpha = alpha;
+  q.hg0 = __logf(hg_phase(dot(f.X, L), g) + 1.0f);
+  const float ms = 0.6f;
+  gather_seg<0, true, 0, 8>(t, stencil, q, 1.0f / 256.0f * lerpf(ms, 1.0f, 1.0f), sink);
+  gather_seg<1, true, 8, 16>(t, stencil, q, 2.5f / 256.0f * lerpf(ms, 1.0f, 0.8f), sink);
+  gather_seg<2, true, 16, 32>(t, stencil, q, 5.5f / 256.0f * lerpf(ms, 1.0f, 0.6f), sink);
+  gather_seg<3, true, 32, 48>(t, stencil, q, 11.5f / 256.0f * lerpf(ms, 1.0f, 0.4f), sink);
+  gather_seg<4, true, 48, 64>(t, stencil, q, 23.5f / 256.0f * lerpf(ms, 1.0f, 0.2f), sink);
+  gather_seg<5, true, 64, 96>(t, stencil, q, 47.5f / 256.0f * ms, sink);
+  gather_seg<6, true, 96, 128>(t, stencil, q, 95.5f / 256.0f * ms, sink);
+  gather_seg<7, true, 128, 160>(t, stencil, q, 191.5f / 256.0f * ms, sink);
+  // light-direction points: offsets vary per point, so one loop per segment
+  // with the offset computed as in the stencil layout
+#pragma unroll 1
+  for (int s = 0; s < 4; ++s) {
+    for (int j = 0; j < 8; ++j) {
+      const int i = 160 + 8 * s + j;
+      const StencilInfo si = stencil_info(i);
+      const F3 p = pos + L * si.offset;
+      const int mip = si.mip;
+      const float xv = __logf(1.0f + alpha * mip_density(t, mip, p) / 64.0f);
+      const float radius = (float)(1 << mip) / 256.0f;
+      const float v = atanf(0.5f * radius / si.offset) / (3.1415926535f * 60.0f / 180.0f);
+      const float h0 = bilinear_clamp(t.lut, kLut, kLut, q.cXL * 0.5f + 0.5f, v);
+      const float h1 = bilinear_clamp(t.lut, kLut, kLut, q.cLXL * 0.5f + 0.5f, v);
+      const float xh = __logf(h0 * h1 + 1.0f);
+      const float xs = shadow_tr(t, p, f.LX, max(mip - 1, 0));
+      sink(i, xv, xs, xh);
+    }
+  }
 }
 
 // Gather only, for explicit points and frames (test / training entry).
@@ -267,31 +310,18 @@ __global__ void k_gather(Tables t, const float* __restrict__ stencil, const floa
                          float* __restrict__ desc, float* __restrict__ aux) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
-  float xv[192], xs[192], xh[192];
   Frame f = load_frame(frame + 12 * (size_t)k);
-  gather_point(t, stencil, f3(pos[3 * k], pos[3 * k + 1], pos[3 * k + 2]), L, f, alpha, g, xv, xs, xh);
   float* d = desc + 576 * (size_t)k;
-  for (int i = 0; i < 192; ++i) { d[i] = xv[i]; d[192 + i] = xs[i]; d[384 + i] = xh[i]; }
+  auto sink = [&](int i, float xv, float xs, float xh) {
+    d[i] = xv;
+    d[192 + i] = xs;
+    d[384 + i] = xh;
+  };
+  gather_fast(t, stencil, f3(pos[3 * k], pos[3 * k + 1], pos[3 * k + 2]), L, f, alpha, g, sink);
   float* ax = aux + 5 * (size_t)k;
   ax[0] = g;
   ax[1] = acosf(dot(f.X, f.LX));
   ax[2] = srp.x; ax[3] = srp.y; ax[4] = srp.z;
-}
-
-// Network only on descriptors (desc n x 576, aux n x 5).
-__global__ void __launch_bounds__(64) k_predict_simt(const float* __restrict__ w, const float* __restrict__ desc,
-                                                     const float* __restrict__ aux, int n, float* __restrict__ out) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  NetSIMT s;
-  const float* d = desc + 576 * (size_t)k;
-  for (int i = 0; i < 192; ++i) { s.xv[i] = d[i]; s.xs[i] = d[192 + i]; s.xh[i] = d[384 + i]; }
-  const float* ax = aux + 5 * (size_t)k;
-  n_trunks(s, w, ax[0], ax[1]);
-  F3 r = n_heads(s, w, f3(ax[2], ax[3], ax[4]));
-  out[3 * (size_t)k + 0] = r.x;
-  out[3 * (size_t)k + 1] = r.y;
-  out[3 * (size_t)k + 2] = r.z;
 }
 
 // Gather for the compacted records, feature-major: feature i of record k at
@@ -307,11 +337,12 @@ __global__ void __launch_bounds__(128) k_gather_fm(Tables t, const float* __rest
   Frame f = load_frame(rec.frame + 12 * (size_t)k);
   float* d = desc + k;
   const size_t c = (size_t)cap;
-  gather_sink(t, stencil, pos, L, f, alpha, g, [&](int i, float xv, float xs, float xh) {
+  auto sink = [&](int i, float xv, float xs, float xh) {
     d[i * c] = xv;
     d[(192 + i) * c] = xs;
     d[(384 + i) * c] = xh;
-  });
+  };
+  gather_fast(t, stencil, pos, L, f, alpha, g, sink);
   aux[k] = g;
   aux[c + k] = acosf(dot(f.X, f.LX));
   aux[2 * c + k] = srp.x;
