@@ -192,66 +192,55 @@ def main():
         p.sample_offset = step
         _lib.check(L.mr_render(v.handle, net, C.byref(p), C.c_void_p(out.data_ptr()), sp))
 
-    for k in range(args.warmup):
-        render(k)
-    torch.cuda.synchronize()
-    L.mr_volume_stage_times(v.handle, (C.c_double * 8)(), (C.c_int32 * 8)(), 8)  # reset
-    _lib.check(L.mr_volume_set_timing(v.handle, 1))
+    def leg(precision, sampler, base):
+        """Time args.steps frames (L2 flushed between steps, outside the events)
+        with per-stage events inside the library; returns the max-over-ranks
+        device time, per-stage means and the last frame's counters."""
+        p.precision, p.sampler = precision, sampler
+        for k in range(args.warmup):
+            render(base + k)
+        torch.cuda.synchronize()
+        L.mr_volume_stage_times(v.handle, (C.c_double * 8)(), (C.c_int32 * 8)(), 8)  # reset
+        _lib.check(L.mr_volume_set_timing(v.handle, 1))
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps)]
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            evs[k][0].record()
+            render(base + 100 + k)
+            evs[k][1].record()
+        torch.cuda.synchronize()
+        ms = float(sum(a.elapsed_time(b) for a, b in evs))
+        st_ms = (C.c_double * 8)()
+        st_n = (C.c_int32 * 8)()
+        _lib.check(L.mr_volume_stage_times(v.handle, st_ms, st_n, 8))
+        _lib.check(L.mr_volume_set_timing(v.handle, 0))
+        _lib.check(L.mr_network_check(net, 1))
+        cnt = (C.c_uint64 * 4)()
+        _lib.check(L.mr_volume_counters(v.handle, cnt))
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+            dist.barrier()
+        per = [st_ms[i] / max(1, st_n[i]) for i in range(8)]
+        return {"ms": ms, "stage": per, "launches": int(sum(st_n[i] for i in range(8))),
+                "active": int(cnt[3]), "fetches": int(cnt[0])}
 
-    # -- device-timed steps (L2 flushed between steps, outside the events)
-    if dist is not None:
-        dist.barrier()
-    torch.cuda.synchronize()
+    # fp32 network, exact sampler: the headline configuration
     clocks = ClockSampler(torch.cuda.current_device())
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    for k in range(args.steps):
-        flush.fill_(float(k))
-        evs[k][0].record()
-        render(args.warmup + k)
-        evs[k][1].record()
-    torch.cuda.synchronize()
+    head = leg(_lib.PREC_FP32, _lib.SAMPLER_EXACT, 0)
     clk = clocks.stop()
-    ms = float(sum(a.elapsed_time(b) for a, b in evs))
-    stage_ms = (C.c_double * 8)()
-    stage_n = (C.c_int32 * 8)()
-    _lib.check(L.mr_volume_stage_times(v.handle, stage_ms, stage_n, 8))
-    _lib.check(L.mr_volume_set_timing(v.handle, 0))
-    cnt = (C.c_uint64 * 4)()
-    _lib.check(L.mr_volume_counters(v.handle, cnt))
-    active = int(cnt[3])  # the counters cover the last frame
-    fetches = int(cnt[0])
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
+    ms, active, fetches = head["ms"], head["active"], head["fetches"]
     fps = world * args.steps / (ms / 1000.0)
-
-    # -- the same frames with the BF16 tensor-core network (precision sweep leg)
-    p.precision = _lib.PREC_BF16
-    for k in range(args.warmup):
-        render(2000 + k)
-    torch.cuda.synchronize()
-    L.mr_volume_stage_times(v.handle, (C.c_double * 8)(), (C.c_int32 * 8)(), 8)
-    _lib.check(L.mr_volume_set_timing(v.handle, 1))
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    for k in range(args.steps):
-        flush.fill_(float(k))
-        evs[k][0].record()
-        render(3000 + k)
-        evs[k][1].record()
-    torch.cuda.synchronize()
-    bf_ms = float(sum(a.elapsed_time(b) for a, b in evs))
-    bf_stage = (C.c_double * 8)()
-    bf_n = (C.c_int32 * 8)()
-    _lib.check(L.mr_volume_stage_times(v.handle, bf_stage, bf_n, 8))
-    _lib.check(L.mr_volume_set_timing(v.handle, 0))
-    _lib.check(L.mr_network_check(net, 1))
-    _lib.check(L.mr_volume_counters(v.handle, cnt))
-    bf_active = int(cnt[3])  # counters cover the last frame
-    mlp_ms = bf_stage[6] / max(1, bf_n[6])
-    bf_tflops = FLOP_PER_PIXEL * bf_active / (mlp_ms / 1000.0) / 1e12
-    p.precision = _lib.PREC_FP32
+    # the same frames with texture-unit sampling and with the BF16 tensor-core network
+    legs = {"fp32_texture": leg(_lib.PREC_FP32, _lib.SAMPLER_TEXTURE, 1000),
+            "bf16_exact": leg(_lib.PREC_BF16, _lib.SAMPLER_EXACT, 2000),
+            "bf16_texture": leg(_lib.PREC_BF16, _lib.SAMPLER_TEXTURE, 3000)}
+    p.precision, p.sampler = _lib.PREC_FP32, _lib.SAMPLER_EXACT
 
     # -- end to end through the public API: render + D2H of the frame to pinned memory
     host = torch.empty(WIDTH * HEIGHT * 3, dtype=torch.float32, pin_memory=True)
@@ -259,7 +248,7 @@ def main():
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for k in range(args.steps):
-        render(1000 + k)
+        render(5000 + k)
         host.copy_(out, non_blocking=True)
     e1.record()
     torch.cuda.synchronize()
@@ -271,8 +260,7 @@ def main():
     e2e_fps = world * args.steps / (e2e_ms / 1000.0)
 
     hbm, bf16, src = peaks()
-    per = lambda i: stage_ms[i] / max(1, stage_n[i])
-    trace_ms, gather_ms, mlp_ms32 = per(1), per(2), per(6)
+    trace_ms, gather_ms, mlp_ms32 = head["stage"][1], head["stage"][2], head["stage"][6]
     # algorithmic bytes: trace = density fetches x 32 B (8 fp32 texels);
     # gather = 192 + 192 trilinear fetches x 32 B + 383 bilinear x 16 B + the
     # 581 fp32 descriptor values written, per active pixel.
@@ -281,7 +269,7 @@ def main():
     stages = {
         "nn_trace": {"bound": "hbm", "kernel": "k_nn_trace", "ms": trace_ms,
                      "achieved": trace_bytes / (trace_ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s"},
-        "nn_gather": {"bound": "hbm", "kernel": "k_gather_fm", "ms": gather_ms,
+        "nn_gather": {"bound": "hbm", "kernel": "k_gather_fm<false> (exact sampler)", "ms": gather_ms,
                       "achieved": gather_bytes / (gather_ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s"},
         "nn_network": {"bound": "tensor", "kernel": "k_mlp_simt (fp32 network, CUDA cores)", "ms": mlp_ms32,
                        "achieved": FLOP_PER_PIXEL * active / (mlp_ms32 / 1e3) / 1e12, "peak": bf16,
@@ -293,26 +281,35 @@ def main():
         s_["traffic"] = None
     dom = max(stages, key=lambda k: stages[k]["ms"])
     roofline = dict(stages[dom], stage=dom)
+    variants = {}
+    for name, lg in legs.items():
+        g_ms, m_ms = lg["stage"][2], lg["stage"][6]
+        tc = name.startswith("bf16")
+        tf = FLOP_PER_PIXEL * lg["active"] / (m_ms / 1e3) / 1e12
+        variants[name] = {
+            "value": world * args.steps / (lg["ms"] / 1000.0), "unit": "frames/s", "ms_per_step": lg["ms"] / args.steps,
+            "stages_ms_per_step": {"nn_trace": lg["stage"][1], "nn_gather": g_ms, "nn_network": m_ms},
+            "gather": {"bound": "hbm", "achieved": lg["active"] * (384 * 32 + 383 * 16 + 581 * 4) / (g_ms / 1e3) / 1e9,
+                       "peak": hbm, "unit": "GB/s"},
+            "network": {"bound": "tensor",
+                        "kernel": "k_mlp_tc (tcgen05 BF16 network)" if tc else "k_mlp_simt (fp32 network, CUDA cores)",
+                        "achieved": tf, "peak": bf16, "unit": "TFLOP/s", "frac": tf / bf16, "peak_source": src},
+        }
     line = {"metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "frame": "%dx%d" % (WIDTH, HEIGHT), "volume": "%d^3" % RES,
+                       "sampler": "exact fp32 trilinear",
                        "l2": "flushed between steps (256 MiB write outside the timed events)",
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "e2e": {"value": e2e_fps, "unit": "frames/s", "h2d_bytes_per_step": C.sizeof(_lib.RenderParams),
                     "d2h_bytes_per_step": WIDTH * HEIGHT * 3 * 4},
-            "gpu_launches": int(sum(stage_n[i] for i in range(8))),
+            "gpu_launches": head["launches"],
             "roofline": roofline, "clocks": clk,
             "stage_rooflines": stages,
             "active_pixels_per_frame": active,
             "density_fetches_per_frame": fetches,
-            "bf16": {"value": world * args.steps / (bf_ms / 1000.0), "unit": "frames/s",
-                     "ms_per_step": bf_ms / args.steps,
-                     "stages_ms_per_step": {"nn_trace": bf_stage[1] / max(1, bf_n[1]),
-                                            "nn_gather": bf_stage[2] / max(1, bf_n[2]), "nn_network_tc": mlp_ms},
-                     "roofline": {"bound": "tensor", "kernel": "k_mlp_tc (tcgen05 BF16 network)",
-                                  "achieved": bf_tflops, "peak": bf16, "unit": "TFLOP/s", "frac": bf_tflops / bf16,
-                                  "peak_source": src, "traffic": None}}}
+            "variants": variants}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(v, dens, p, w, st)
     if rank == 0:

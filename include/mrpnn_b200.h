@@ -73,7 +73,15 @@ typedef struct {
   uint32_t sample_offset; /* index of the first sample (progressive accumulation) */
   int32_t render_type;    /* mr_render_type */
   int32_t precision;      /* mr_precision (MRPNN only) */
+  int32_t sampler;        /* mr_sampler for the descriptor gather (MRPNN only) */
 } mr_render_params;
+
+/* How the neural gather samples the mip / transmittance / HG tables.
+ * EXACT: fp32 trilinear in software (bit-stable, the oracle's arithmetic).
+ * TEXTURE: the texture units' linear filter, as the reference samples its
+ * texture references (core/volume.cu:1289-1298): 8-bit interpolation
+ * weights, several times fewer instructions per sample. */
+typedef enum { MR_SAMPLER_EXACT = 0, MR_SAMPLER_TEXTURE = 1 } mr_sampler;
 
 /* Library version string. */
 const char* mr_version(void);
@@ -175,8 +183,9 @@ int mr_network_check(const mr_network* net, int32_t reset);
 int mr_sync(void* stream, int32_t timeout_ms);
 
 /* Per-stage CUDA-event timing of this volume's kernels (off by default).
- * Stages: 0 delta tracking, 1 neural trace, 2 neural gather+network,
- * 3 TR build, 4 HG table build, 5 pyramid build. mr_volume_stage_times waits
+ * Stages: 0 delta tracking, 1 neural trace, 2 neural descriptor gather,
+ * 3 TR build, 4 HG table build, 5 pyramid build, 6 neural network (MLP).
+ * mr_volume_stage_times waits
  * for the device, returns the summed milliseconds and launch counts of the
  * first n stages since the last query, and resets them. */
 int mr_volume_set_timing(mr_volume* v, int32_t enable);

@@ -12,6 +12,7 @@ LIB_PATH = os.path.join(HERE, "libmrpnn_b200.so")
 MR_OK, MR_ERR_ARG, MR_ERR_CUDA, MR_ERR_TIMEOUT, MR_ERR_LOOP_CAP, MR_ERR_STATE, MR_ERR_NOMEM, MR_ERR_UNSUPPORTED = range(8)
 RT_PT, RT_RPNN, RT_MRPNN = 0, 1, 2
 PREC_FP32, PREC_BF16, PREC_FP8 = 0, 1, 2
+SAMPLER_EXACT, SAMPLER_TEXTURE = 0, 1
 READ_DENSITY, READ_MIP, READ_VARIANCE, READ_TR, READ_HGLUT = range(5)
 WEIGHT_TOTAL = 49673
 
@@ -40,7 +41,7 @@ class RenderParams(C.Structure):
                 ("tr_scale", C.c_float), ("env_color", Float3),
                 ("max_bounces", C.c_int32), ("spp", C.c_int32),
                 ("seed", C.c_uint32), ("sample_offset", C.c_uint32),
-                ("render_type", C.c_int32), ("precision", C.c_int32)]
+                ("render_type", C.c_int32), ("precision", C.c_int32), ("sampler", C.c_int32)]
 
 
 class MRError(RuntimeError):

@@ -54,6 +54,11 @@ struct Volume {
   float lut_g = 0;
   uint32_t lut_seed = 0;
   StageTimer timer;
+  // Texture-unit copies of the tables for MR_SAMPLER_TEXTURE, created on first
+  // use and refreshed when the linear tables change.
+  cudaArray_t mip_arr[9] = {}, tr_arr[8] = {}, lut_arr = nullptr;
+  cudaTextureObject_t mip_tex[9] = {}, tr_tex[8] = {}, lut_tex = 0;
+  bool tex_mips_stale = true, tex_tr_stale = true, tex_lut_stale = true;
   // Per-render scratch owned by the volume (grown on demand).
   void* scratch = nullptr;
   size_t scratch_bytes = 0;
@@ -86,6 +91,8 @@ int ensure_scratch(Volume* v, size_t bytes, cudaStream_t s);
 // Kernels launched from several translation units.
 int launch_update_tr(Volume* v, F3 L, float alpha, cudaStream_t s);
 int launch_update_lut(Volume* v, float g, uint32_t seed, cudaStream_t s);
+int refresh_textures(Volume* v, cudaStream_t s);
+void destroy_textures(Volume* v);
 int sm_count();
 
 }  // namespace mr

@@ -16,6 +16,8 @@ struct Tables {
   const float* __restrict__ mips;
   const float* __restrict__ tr;
   const float* __restrict__ lut;
+  // texture-unit copies (MR_SAMPLER_TEXTURE only)
+  cudaTextureObject_t mip_tex[9], tr_tex[8], lut_tex;
 };
 
 __constant__ unsigned c_mip_off[9] = {0u, 16777216u, 18874368u, 19136512u, 19169280u, 19173376u, 19173888u,
@@ -217,9 +219,10 @@ constexpr unsigned kMipOff[9] = {0u, 16777216u, 18874368u, 19136512u, 19169280u,
                                  19173960u};
 constexpr unsigned kTrOff[8] = {0u, 2097152u, 2359296u, 2392064u, 2396160u, 2396672u, 2396736u, 2396744u};
 
-// Stencil points [I0, I1) at mip level MIP, offset `off`; SPHERE selects the
-// rotated-stencil points (else the points along the light direction).
-template <int MIP, bool SPHERE, int I0, int I1, class Sink>
+// Stencil points [I0, I1) at mip level MIP, offset `off` (sphere points), or
+// the light-direction points with per-point offsets (SPHERE = false). HW
+// samples through the texture units instead of the fp32 software filter.
+template <int MIP, bool SPHERE, bool HW, int I0, int I1, class Sink>
 __device__ __forceinline__ void gather_seg(const Tables& t, const float* __restrict__ stencil, const PixelGather& q,
                                            float off, Sink& sink) {
   constexpr int R = 256 >> MIP;
@@ -228,7 +231,8 @@ __device__ __forceinline__ void gather_seg(const Tables& t, const float* __restr
   const float* mb = t.mips + kMipOff[MIP];
   const float* tb = t.tr + kTrOff[TL];
   const float radius = (float)(1 << MIP) / 256.0f;
-  const float vrow = atanf(0.5f * radius / off) / (3.1415926535f * 60.0f / 180.0f);
+  const float kAng = 3.1415926535f * 60.0f / 180.0f;
+  float vrow = atanf(0.5f * radius / off) / kAng;
 #pragma unroll 2
   for (int i = I0; i < I1; ++i) {
     F3 p;
@@ -240,31 +244,43 @@ __device__ __forceinline__ void gather_seg(const Tables& t, const float* __restr
       c1 = sx * inv;
       c2 = (q.lx * sx + q.ly * sy + q.lz * sz) * inv;
     } else {
+      // light-direction points: offsets (1..8, 9.5.., 26.5.., 60.5..)/256 per
+      // point (core/vector.cu:367-398)
+      const int j = i - I0;
+      off = (MIP == 0 ? (float)(j + 1) : MIP == 1 ? 8.5f + 1.0f + 2.0f * (float)j
+                                       : MIP == 2 ? 26.5f + 4.0f * (float)j : 60.5f + 8.0f * (float)j) / 256.0f;
+      vrow = atanf(0.5f * radius / off) / kAng;
       p = q.pos + q.L * off;
       c1 = q.cXL;
       c2 = q.cLXL;
     }
-    const float xv = __logf(1.0f + q.alpha * tri_border_c<R>(mb, p + 0.5f) / 64.0f);
+    const float dens = HW ? tex3D<float>(t.mip_tex[MIP], p.z + 0.5f, p.y + 0.5f, p.x + 0.5f)
+                          : tri_border_c<R>(mb, p + 0.5f);
+    const float xv = __logf(1.0f + q.alpha * dens / 64.0f);
     float xh;
     if (SPHERE && MIP == 0 && I0 == 0 && i == 0) {
       xh = q.hg0;
     } else {
-      const float h0 = bilinear_clamp(t.lut, kLut, kLut, c1 * 0.5f + 0.5f, vrow);
-      const float h1 = bilinear_clamp(t.lut, kLut, kLut, c2 * 0.5f + 0.5f, vrow);
+      const float u1 = c1 * 0.5f + 0.5f, u2 = c2 * 0.5f + 0.5f;
+      const float h0 = HW ? tex2D<float>(t.lut_tex, u1, vrow) : bilinear_clamp(t.lut, kLut, kLut, u1, vrow);
+      const float h1 = HW ? tex2D<float>(t.lut_tex, u2, vrow) : bilinear_clamp(t.lut, kLut, kLut, u2, vrow);
       xh = __logf(h0 * h1 + 1.0f);
     }
-    float xs;
+    F3 pt = p;
+    float xs = 1.0f;
+    bool fetch = true;
     if (p.x < -0.5f || p.y < -0.5f || p.z < -0.5f || p.x > 0.5f || p.y > 0.5f || p.z > 0.5f) {
-      const float o2 = ray_box_offset(p, q.LX);
-      xs = o2 >= 0 ? tri_clamp_c<RT>(tb, p + q.LX * o2 + 0.5f) : 1.0f;
-    } else {
-      xs = tri_clamp_c<RT>(tb, p + 0.5f);
+      const float o2 = ray_box_offset(p, q.LX);  // ShadowTerm_TRTex (core/renderResources.cu:121-139)
+      fetch = o2 >= 0;
+      pt = p + q.LX * o2;
     }
+    if (fetch)
+      xs = HW ? tex3D<float>(t.tr_tex[TL], pt.z + 0.5f, pt.y + 0.5f, pt.x + 0.5f) : tri_clamp_c<RT>(tb, pt + 0.5f);
     sink(i, xv, xs, xh);
   }
 }
 
-template <class Sink>
+template <bool HW, class Sink>
 __device__ __forceinline__ void gather_fast(const Tables& t, const float* __restrict__ stencil, F3 pos, F3 L,
                                             const Frame& f, float alpha, float g, Sink sink) {
   PixelGather q;
@@ -275,33 +291,18 @@ __device__ __forceinline__ void gather_fast(const Tables& t, const float* __rest
   q.alpha = alpha;
   q.hg0 = __logf(hg_phase(dot(f.X, L), g) + 1.0f);
   const float ms = 0.6f;
-  gather_seg<0, true, 0, 8>(t, stencil, q, 1.0f / 256.0f * lerpf(ms, 1.0f, 1.0f), sink);
-  gather_seg<1, true, 8, 16>(t, stencil, q, 2.5f / 256.0f * lerpf(ms, 1.0f, 0.8f), sink);
-  gather_seg<2, true, 16, 32>(t, stencil, q, 5.5f / 256.0f * lerpf(ms, 1.0f, 0.6f), sink);
-  gather_seg<3, true, 32, 48>(t, stencil, q, 11.5f / 256.0f * lerpf(ms, 1.0f, 0.4f), sink);
-  gather_seg<4, true, 48, 64>(t, stencil, q, 23.5f / 256.0f * lerpf(ms, 1.0f, 0.2f), sink);
-  gather_seg<5, true, 64, 96>(t, stencil, q, 47.5f / 256.0f * ms, sink);
-  gather_seg<6, true, 96, 128>(t, stencil, q, 95.5f / 256.0f * ms, sink);
-  gather_seg<7, true, 128, 160>(t, stencil, q, 191.5f / 256.0f * ms, sink);
-  // light-direction points: offsets vary per point, so one loop per segment
-  // with the offset computed as in the stencil layout
-#pragma unroll 1
-  for (int s = 0; s < 4; ++s) {
-    for (int j = 0; j < 8; ++j) {
-      const int i = 160 + 8 * s + j;
-      const StencilInfo si = stencil_info(i);
-      const F3 p = pos + L * si.offset;
-      const int mip = si.mip;
-      const float xv = __logf(1.0f + alpha * mip_density(t, mip, p) / 64.0f);
-      const float radius = (float)(1 << mip) / 256.0f;
-      const float v = atanf(0.5f * radius / si.offset) / (3.1415926535f * 60.0f / 180.0f);
-      const float h0 = bilinear_clamp(t.lut, kLut, kLut, q.cXL * 0.5f + 0.5f, v);
-      const float h1 = bilinear_clamp(t.lut, kLut, kLut, q.cLXL * 0.5f + 0.5f, v);
-      const float xh = __logf(h0 * h1 + 1.0f);
-      const float xs = shadow_tr(t, p, f.LX, max(mip - 1, 0));
-      sink(i, xv, xs, xh);
-    }
-  }
+  gather_seg<0, true, HW, 0, 8>(t, stencil, q, 1.0f / 256.0f * lerpf(ms, 1.0f, 1.0f), sink);
+  gather_seg<1, true, HW, 8, 16>(t, stencil, q, 2.5f / 256.0f * lerpf(ms, 1.0f, 0.8f), sink);
+  gather_seg<2, true, HW, 16, 32>(t, stencil, q, 5.5f / 256.0f * lerpf(ms, 1.0f, 0.6f), sink);
+  gather_seg<3, true, HW, 32, 48>(t, stencil, q, 11.5f / 256.0f * lerpf(ms, 1.0f, 0.4f), sink);
+  gather_seg<4, true, HW, 48, 64>(t, stencil, q, 23.5f / 256.0f * lerpf(ms, 1.0f, 0.2f), sink);
+  gather_seg<5, true, HW, 64, 96>(t, stencil, q, 47.5f / 256.0f * ms, sink);
+  gather_seg<6, true, HW, 96, 128>(t, stencil, q, 95.5f / 256.0f * ms, sink);
+  gather_seg<7, true, HW, 128, 160>(t, stencil, q, 191.5f / 256.0f * ms, sink);
+  gather_seg<0, false, HW, 160, 168>(t, stencil, q, 1.0f, sink);
+  gather_seg<1, false, HW, 168, 176>(t, stencil, q, 1.0f, sink);
+  gather_seg<2, false, HW, 176, 184>(t, stencil, q, 1.0f, sink);
+  gather_seg<3, false, HW, 184, 192>(t, stencil, q, 1.0f, sink);
 }
 
 // Gather only, for explicit points and frames (test / training entry).
@@ -317,7 +318,7 @@ __global__ void k_gather(Tables t, const float* __restrict__ stencil, const floa
     d[192 + i] = xs;
     d[384 + i] = xh;
   };
-  gather_fast(t, stencil, f3(pos[3 * k], pos[3 * k + 1], pos[3 * k + 2]), L, f, alpha, g, sink);
+  gather_fast<false>(t, stencil, f3(pos[3 * k], pos[3 * k + 1], pos[3 * k + 2]), L, f, alpha, g, sink);
   float* ax = aux + 5 * (size_t)k;
   ax[0] = g;
   ax[1] = acosf(dot(f.X, f.LX));
@@ -327,6 +328,7 @@ __global__ void k_gather(Tables t, const float* __restrict__ stencil, const floa
 // Gather for the compacted records, feature-major: feature i of record k at
 // desc[i*cap + k] (aux likewise), so that a warp's stores and the network's
 // loads of one feature are single coalesced transactions.
+template <bool HW>
 __global__ void __launch_bounds__(128) k_gather_fm(Tables t, const float* __restrict__ stencil, Records rec,
                                                    int cap, F3 L, float alpha, float g, F3 srp,
                                                    float* __restrict__ desc, float* __restrict__ aux) {
@@ -342,7 +344,7 @@ __global__ void __launch_bounds__(128) k_gather_fm(Tables t, const float* __rest
     d[(192 + i) * c] = xs;
     d[(384 + i) * c] = xh;
   };
-  gather_fast(t, stencil, pos, L, f, alpha, g, sink);
+  gather_fast<HW>(t, stencil, pos, L, f, alpha, g, sink);
   aux[k] = g;
   aux[c + k] = acosf(dot(f.X, f.LX));
   aux[2 * c + k] = srp.x;
@@ -417,9 +419,22 @@ int render_neural(Volume* v, const Network* net, const mr_render_params* p, floa
   v->timer.mark(ST_NN_TRACE, s);
   MR_CUDA(cudaGetLastError());
   F3 sr = to_f3(p->scatter_rate) / 1.001f;
+  Tables tabs{v->mips, v->tr, v->lut, {}, {}, 0};
+  const bool hw = p->sampler == MR_SAMPLER_TEXTURE;
+  if (hw) {
+    rc = refresh_textures(v, s);
+    if (rc) return rc;
+    for (int k = 0; k < 9; ++k) tabs.mip_tex[k] = v->mip_tex[k];
+    for (int k = 0; k < 8; ++k) tabs.tr_tex[k] = v->tr_tex[k];
+    tabs.lut_tex = v->lut_tex;
+  }
   v->timer.mark(ST_NN_PREDICT, s);
-  k_gather_fm<<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(Tables{v->mips, v->tr, v->lut}, net->stencil, rec,
-                                                            (int)npx, L, p->alpha, p->g, srp_of(sr), desc, aux);
+  if (hw)
+    k_gather_fm<true><<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(tabs, net->stencil, rec, (int)npx, L, p->alpha,
+                                                                    p->g, srp_of(sr), desc, aux);
+  else
+    k_gather_fm<false><<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(tabs, net->stencil, rec, (int)npx, L, p->alpha,
+                                                                     p->g, srp_of(sr), desc, aux);
   v->timer.mark(ST_NN_PREDICT, s);
   MR_CUDA(cudaGetLastError());
   const long long cap = (long long)npx;
@@ -450,7 +465,7 @@ extern "C" int mr_gather_descriptors(const mr_volume* h, const mr_network* nh, c
   if (!v->mips_valid || !v->tr_valid || !v->lut_valid)
     return set_error(MR_ERR_STATE, "gather needs mr_volume_update, _update_tr and _update_hglut first");
   F3 sr = to_f3(scatter_rate) / 1.001f;
-  k_gather<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(Tables{v->mips, v->tr, v->lut}, nh->n.stencil,
+  k_gather<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(Tables{v->mips, v->tr, v->lut, {}, {}, 0}, nh->n.stencil,
                                                             dev_pos, dev_frame, n, v->tr_light, alpha, g,
                                                             srp_of(sr), dev_desc, dev_aux);
   MR_CUDA(cudaGetLastError());

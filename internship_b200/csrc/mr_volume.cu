@@ -185,6 +185,7 @@ int launch_update_tr(Volume* v, F3 L, float alpha, cudaStream_t s) {
   v->timer.mark(ST_TR, s);
   MR_CUDA(cudaGetLastError());
   v->tr_valid = true;
+  v->tex_tr_stale = true;
   v->tr_light = L;
   v->tr_alpha = alpha;
   return MR_OK;
@@ -196,9 +197,95 @@ int launch_update_lut(Volume* v, float g, uint32_t seed, cudaStream_t s) {
   v->timer.mark(ST_LUT, s);
   MR_CUDA(cudaGetLastError());
   v->lut_valid = true;
+  v->tex_lut_stale = true;
   v->lut_g = g;
   v->lut_seed = seed;
   return MR_OK;
+}
+
+// ---- texture-unit copies (MR_SAMPLER_TEXTURE) --------------------------------------
+// cudaArray extent (width, height, depth) = (z, y, x) of the x-major tables;
+// sampled as tex3D(obj, uv.z, uv.y, uv.x) like the reference's texture refs.
+static int make_tex3(cudaArray_t* arr, cudaTextureObject_t* tex, int r, cudaTextureAddressMode mode) {
+  cudaChannelFormatDesc ch = cudaCreateChannelDesc<float>();
+  MR_CUDA(cudaMalloc3DArray(arr, &ch, make_cudaExtent(r, r, r)));
+  cudaResourceDesc rd = {};
+  rd.resType = cudaResourceTypeArray;
+  rd.res.array.array = *arr;
+  cudaTextureDesc td = {};
+  td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = mode;
+  td.filterMode = cudaFilterModeLinear;
+  td.readMode = cudaReadModeElementType;
+  td.normalizedCoords = 1;
+  MR_CUDA(cudaCreateTextureObject(tex, &rd, &td, nullptr));
+  return MR_OK;
+}
+static int copy_to_array(cudaArray_t arr, const float* src, int r, cudaStream_t s) {
+  cudaMemcpy3DParms cp = {};
+  cp.srcPtr = make_cudaPitchedPtr((void*)src, r * sizeof(float), r, r);
+  cp.dstArray = arr;
+  cp.extent = make_cudaExtent(r, r, r);
+  cp.kind = cudaMemcpyDeviceToDevice;
+  MR_CUDA(cudaMemcpy3DAsync(&cp, s));
+  return MR_OK;
+}
+
+int refresh_textures(Volume* v, cudaStream_t s) {
+  if (!v->lut_arr) {
+    for (int k = 0; k < 9; ++k) {
+      int rc = make_tex3(&v->mip_arr[k], &v->mip_tex[k], 256 >> k, cudaAddressModeBorder);
+      if (rc) return rc;
+    }
+    for (int k = 0; k < 8; ++k) {
+      int rc = make_tex3(&v->tr_arr[k], &v->tr_tex[k], 128 >> k, cudaAddressModeClamp);
+      if (rc) return rc;
+    }
+    cudaChannelFormatDesc ch = cudaCreateChannelDesc<float>();
+    MR_CUDA(cudaMallocArray(&v->lut_arr, &ch, kLut, kLut));
+    cudaResourceDesc rd = {};
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = v->lut_arr;
+    cudaTextureDesc td = {};
+    td.addressMode[0] = td.addressMode[1] = cudaAddressModeClamp;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 1;
+    MR_CUDA(cudaCreateTextureObject(&v->lut_tex, &rd, &td, nullptr));
+    v->tex_mips_stale = v->tex_tr_stale = v->tex_lut_stale = true;
+  }
+  if (v->tex_mips_stale) {
+    for (int k = 0; k < 9; ++k) {
+      int rc = copy_to_array(v->mip_arr[k], v->mips + mip_offset(k), 256 >> k, s);
+      if (rc) return rc;
+    }
+    v->tex_mips_stale = false;
+  }
+  if (v->tex_tr_stale) {
+    for (int k = 0; k < 8; ++k) {
+      int rc = copy_to_array(v->tr_arr[k], v->tr + tr_offset(k), 128 >> k, s);
+      if (rc) return rc;
+    }
+    v->tex_tr_stale = false;
+  }
+  if (v->tex_lut_stale) {
+    MR_CUDA(cudaMemcpy2DToArrayAsync(v->lut_arr, 0, 0, v->lut, kLut * sizeof(float), kLut * sizeof(float), kLut,
+                                     cudaMemcpyDeviceToDevice, s));
+    v->tex_lut_stale = false;
+  }
+  return MR_OK;
+}
+
+void destroy_textures(Volume* v) {
+  for (int k = 0; k < 9; ++k) {
+    if (v->mip_tex[k]) cudaDestroyTextureObject(v->mip_tex[k]);
+    if (v->mip_arr[k]) cudaFreeArray(v->mip_arr[k]);
+  }
+  for (int k = 0; k < 8; ++k) {
+    if (v->tr_tex[k]) cudaDestroyTextureObject(v->tr_tex[k]);
+    if (v->tr_arr[k]) cudaFreeArray(v->tr_arr[k]);
+  }
+  if (v->lut_tex) cudaDestroyTextureObject(v->lut_tex);
+  if (v->lut_arr) cudaFreeArray(v->lut_arr);
 }
 
 int ensure_scratch(Volume* v, size_t bytes, cudaStream_t s) {
@@ -257,6 +344,7 @@ int mr_volume_destroy(mr_volume* h) {
   cudaFree(v->d_max);
   cudaFree(v->d_counters);
   if (v->scratch) cudaFree(v->scratch);
+  destroy_textures(v);
   delete h;
   return MR_OK;
 }
@@ -309,6 +397,7 @@ int mr_volume_update(mr_volume* h, void* stream) {
   MR_CUDA(cudaStreamSynchronize(s));
   v->max_density = md;
   v->mips_valid = true;
+  v->tex_mips_stale = true;
   v->tr_valid = false;
   return MR_OK;
 }

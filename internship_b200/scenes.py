@@ -70,7 +70,8 @@ CAMERA_DIR = np.array([1.0, 0.55, 0.8]) / np.linalg.norm([1.0, 0.55, 0.8])
 
 
 def make_params(width, height, spp=1, rt=_lib.RT_PT, bounces=512, seed=0, alpha=64.0, g=0.857, albedo=0.99,
-                distance=2.5, fov=40.0, sample_offset=0, precision=_lib.PREC_FP32, light_seed=0):
+                distance=2.5, fov=40.0, sample_offset=0, precision=_lib.PREC_FP32, light_seed=0,
+                sampler=_lib.SAMPLER_EXACT):
     ori, up, right = camera_vectors(CAMERA_DIR * distance, fov)
     p = RenderParams()
     p.width, p.height = width, height
@@ -83,7 +84,7 @@ def make_params(width, height, spp=1, rt=_lib.RT_PT, bounces=512, seed=0, alpha=
     p.env_color = f3((0.0, 0.0, 0.0))
     p.max_bounces, p.spp = bounces, spp
     p.seed, p.sample_offset = seed, sample_offset
-    p.render_type, p.precision = rt, precision
+    p.render_type, p.precision, p.sampler = rt, precision, sampler
     return p
 
 

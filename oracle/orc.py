@@ -27,7 +27,7 @@ class RenderParams(C.Structure):
                 ("tr_scale", C.c_float), ("env_color", Float3),
                 ("max_bounces", C.c_int32), ("spp", C.c_int32),
                 ("seed", C.c_uint32), ("sample_offset", C.c_uint32),
-                ("render_type", C.c_int32), ("precision", C.c_int32)]
+                ("render_type", C.c_int32), ("precision", C.c_int32), ("sampler", C.c_int32)]
 
 
 def lib():
