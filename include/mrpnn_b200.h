@@ -179,6 +179,28 @@ int mr_tc_selftest(int32_t n, int32_t k, const uint16_t* host_a, const uint16_t*
  * that timed out): MR_ERR_TIMEOUT if set; `reset` clears it. */
 int mr_network_check(const mr_network* net, int32_t reset);
 
+/* Neural render into a fixed scratch (no reference counterpart): the same
+ * trace / gather / network passes as mr_render with MR_RT_MRPNN, but the
+ * per-pixel records and descriptor columns live in a module-resident device
+ * array of MR_NOALLOC_SCRATCH_MIB MiB instead of the volume's growable
+ * scratch, so the call allocates no device or host memory.
+ *  - width*height must be <= MR_NOALLOC_MAX_PIXELS (else MR_ERR_ARG);
+ *  - sampler must be MR_SAMPLER_EXACT (texture tables are allocated on first
+ *    use), precision FP32 or BF16;
+ *  - the HG table and transmittance pyramid must already be built for p's g,
+ *    seed, light and alpha (mr_volume_update_hglut / _update_tr, or an
+ *    earlier mr_render): MR_ERR_STATE otherwise;
+ *  - the scratch is one per device and process: overlapping calls (several
+ *    streams or threads on one device) race on it and must be serialised by
+ *    the caller;
+ *  - the first call on a device looks the scratch address up (and may load
+ *    the module there), so make it before any stream capture.
+ * Stage timing (mr_volume_set_timing) does not cover this call. */
+#define MR_NOALLOC_MAX_PIXELS 16384
+#define MR_NOALLOC_SCRATCH_MIB 40
+int mr_render_neural_noalloc(mr_volume* v, const mr_network* net, const mr_render_params* p, float* dev_rgb,
+                             void* stream);
+
 /* Wait for `stream` with a watchdog: MR_ERR_TIMEOUT after timeout_ms. */
 int mr_sync(void* stream, int32_t timeout_ms);
 

@@ -25,7 +25,9 @@ EXPORTS = [
     "mr_render_accumulate_f64", "mr_radiance_predict", "mr_gather_descriptors", "mr_sync",
     "mr_volume_counters", "mr_generate_cloud", "mr_cloud_permutation",
     "mr_volume_set_timing", "mr_volume_stage_times", "mr_tc_selftest", "mr_network_check",
+    "mr_render_neural_noalloc",
 ]
+NOALLOC_MAX_PIXELS = 16384
 
 
 class Float3(C.Structure):
@@ -95,6 +97,7 @@ def load():
     L.mr_volume_stage_times.argtypes = [vp, vp, vp, i32]
     L.mr_tc_selftest.argtypes = [i32, i32, vp, vp, vp]
     L.mr_network_check.argtypes = [vp, i32]
+    L.mr_render_neural_noalloc.argtypes = [vp, vp, C.POINTER(RenderParams), vp, vp]
     _lib = L
     return L
 

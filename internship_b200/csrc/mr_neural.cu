@@ -1,11 +1,15 @@
-// Neural render (render type MRPNN), fp32: NNPredict<MRPNN> of
-// core/render.cuh:469-523 split into two stream-ordered kernels.
+// Neural render (render type MRPNN): NNPredict<MRPNN> of
+// core/render.cuh:469-523 split into three stream-ordered kernels.
 //  1. k_nn_trace: per pixel, camera ray + first Woodcock collision
 //     (GetSamplePoint), the two random frames (GetMatrixFromNormal) and the
 //     single-scatter NEE term Tr*HG; active pixels are compacted into a record
 //     list with warp-aggregated atomics, inactive ones get the environment.
-//  2. k_nn_predict_simt: per active record, the 192-point multi-scale
-//     descriptor gather (core/radiancePredict.cu:319-368) and the network body.
+//  2. k_gather_fm: per active record, the 192-point multi-scale descriptor
+//     gather (core/radiancePredict.cu:319-368) into feature-major columns.
+//  3. the network body: k_mlp_simt (fp32, mr_mlp_simt.cu) or k_mlp_tc
+//     (BF16 tcgen05, mr_mlp_tc.cu), which also writes the pixel.
+#include <mutex>
+
 #include "mr_internal.h"
 #include "mr_net_layout.cuh"
 #include "mr_track.cuh"
@@ -364,7 +368,14 @@ extern int check_params(const mr_render_params* p);
 extern CameraModel make_camera(const mr_render_params* p);
 extern PathScene make_path_scene(const mr_render_params* p);
 
-static size_t records_bytes(size_t n) { return n * (sizeof(int) + 16 * sizeof(float)) + 256; }
+constexpr size_t records_bytes(size_t n) { return n * (sizeof(int) + 16 * sizeof(float)) + 256; }
+constexpr size_t records_round(size_t n) { return (records_bytes(n) + 255) / 256 * 256; }
+// Scratch of one neural render of n pixels: records, then 576 feature-major
+// descriptor columns and 5 aux columns.
+constexpr size_t neural_scratch_bytes(size_t n) { return records_round(n) + n * (576 + 5) * sizeof(float) + 256; }
+
+static int neural_passes(Volume* v, const Network* net, const mr_render_params* p, float* dev_rgb, cudaStream_t s,
+                         void* base, bool timed);
 
 static Records carve_records(void* base, size_t n) {
   char* p = (char*)base;
@@ -394,14 +405,24 @@ int render_neural(Volume* v, const Network* net, const mr_render_params* p, floa
     if (rc) return rc;
   }
   size_t npx = (size_t)p->width * p->height;
+  int rc = ensure_scratch(v, neural_scratch_bytes(npx), s);
+  if (rc) return rc;
+  return neural_passes(v, net, p, dev_rgb, s, v->scratch, true);
+}
+
+// Trace, gather and network over scratch at `base` (neural_scratch_bytes of
+// width*height); `timed` = record stage events when the volume's timer is on.
+static int neural_passes(Volume* v, const Network* net, const mr_render_params* p, float* dev_rgb, cudaStream_t s,
+                         void* base, bool timed) {
+  auto mark = [&](int st) { if (timed) v->timer.mark(st, s); };
+  int rc = MR_OK;
+  const F3 L = normalize(to_f3(p->light_dir));
+  const size_t npx = (size_t)p->width * p->height;
   const bool tc = p->precision == MR_PREC_BF16;
   // records, then the feature-major descriptor and aux columns
-  size_t rbytes = (records_bytes(npx) + 255) / 256 * 256;
-  size_t need = rbytes + npx * (576 + 5) * sizeof(float) + 256;
-  int rc = ensure_scratch(v, need, s);
-  if (rc) return rc;
-  Records rec = carve_records(v->scratch, npx);
-  float* desc = (float*)((char*)v->scratch + rbytes);
+  const size_t rbytes = records_round(npx);
+  Records rec = carve_records(base, npx);
+  float* desc = (float*)((char*)base + rbytes);
   float* aux = desc + npx * 576;
   MR_CUDA(cudaMemsetAsync(v->d_counters, 0, kCounters * sizeof(unsigned long long), s));
   MR_CUDA(cudaMemsetAsync(rec.count, 0, sizeof(unsigned), s));
@@ -414,9 +435,9 @@ int render_neural(Volume* v, const Network* net, const mr_render_params* p, floa
   ta.out = dev_rgb;
   ta.rec = rec;
   ta.counters = v->d_counters;
-  v->timer.mark(ST_NN_TRACE, s);
+  mark(ST_NN_TRACE);
   k_nn_trace<<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(ta);
-  v->timer.mark(ST_NN_TRACE, s);
+  mark(ST_NN_TRACE);
   MR_CUDA(cudaGetLastError());
   F3 sr = to_f3(p->scatter_rate) / 1.001f;
   Tables tabs{v->mips, v->tr, v->lut, {}, {}, 0};
@@ -428,24 +449,24 @@ int render_neural(Volume* v, const Network* net, const mr_render_params* p, floa
     for (int k = 0; k < 8; ++k) tabs.tr_tex[k] = v->tr_tex[k];
     tabs.lut_tex = v->lut_tex;
   }
-  v->timer.mark(ST_NN_PREDICT, s);
+  mark(ST_NN_PREDICT);
   if (hw)
     k_gather_fm<true><<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(tabs, net->stencil, rec, (int)npx, L, p->alpha,
                                                                     p->g, srp_of(sr), desc, aux);
   else
     k_gather_fm<false><<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(tabs, net->stencil, rec, (int)npx, L, p->alpha,
                                                                      p->g, srp_of(sr), desc, aux);
-  v->timer.mark(ST_NN_PREDICT, s);
+  mark(ST_NN_PREDICT);
   MR_CUDA(cudaGetLastError());
   const long long cap = (long long)npx;
-  v->timer.mark(ST_NN_MLP, s);
+  mark(ST_NN_MLP);
   if (tc)
     rc = launch_mlp_tc(net, desc, aux, 1, cap, 1, cap, (int)npx, dev_rgb, rec.pix, rec.trph, rec.count,
                        to_f3(p->light_color), to_f3(p->scatter_rate), s);
   else
     rc = launch_mlp_simt(net, desc, aux, 1, cap, 1, cap, (int)npx, rec.count, dev_rgb, rec.pix, rec.trph,
                          to_f3(p->light_color), to_f3(p->scatter_rate), s);
-  v->timer.mark(ST_NN_MLP, s);
+  mark(ST_NN_MLP);
   return rc;
 }
 
@@ -484,4 +505,66 @@ extern "C" int mr_radiance_predict(const mr_network* nh, int32_t precision, cons
   if (precision != MR_PREC_FP32) return set_error(MR_ERR_UNSUPPORTED, "precision %d not built", precision);
   return launch_mlp_simt(&nh->n, dev_desc, dev_aux, 576, 1, 5, 1, n, nullptr, dev_out, nullptr, nullptr, f3(1, 1, 1),
                          f3(1, 1, 1), (cudaStream_t)stream);
+}
+
+// ---- fixed-scratch neural render (mr_render_neural_noalloc) -------------------
+
+namespace mr {
+// Module-resident scratch for mr_render_neural_noalloc: records plus
+// descriptor columns of up to MR_NOALLOC_MAX_PIXELS pixels.
+constexpr size_t kNoallocBytes = (size_t)MR_NOALLOC_SCRATCH_MIB << 20;
+static_assert(neural_scratch_bytes(MR_NOALLOC_MAX_PIXELS) <= kNoallocBytes, "no-alloc scratch too small");
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
+
+constexpr int kNoallocDevices = 64;
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_ptr[kNoallocDevices];
+
+// Address of g_noalloc_scratch on the current device, looked up once per
+// device (cudaGetSymbolAddress also loads the module there on first use).
+static int noalloc_scratch(void** out) {
+  int dev = 0;
+  MR_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoallocDevices) return set_error(MR_ERR_ARG, "device ordinal %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    g_noalloc_ptr[dev] = ptr;
+  }
+  *out = g_noalloc_ptr[dev];
+  return MR_OK;
+}
+}  // namespace mr
+
+extern "C" int mr_render_neural_noalloc(mr_volume* h, const mr_network* nh, const mr_render_params* p,
+                                        float* dev_rgb, void* stream) {
+  clear_error();
+  if (!h || !nh || !p || !dev_rgb) return set_error(MR_ERR_ARG, "mr_render_neural_noalloc: NULL argument");
+  int rc = check_params(p);
+  if (rc) return rc;
+  if (p->render_type != MR_RT_MRPNN)
+    return set_error(MR_ERR_ARG, "mr_render_neural_noalloc renders MR_RT_MRPNN only (got %d)", p->render_type);
+  if (p->precision != MR_PREC_FP32 && p->precision != MR_PREC_BF16)
+    return set_error(MR_ERR_UNSUPPORTED, "precision %d not built", p->precision);
+  if (p->sampler != MR_SAMPLER_EXACT)
+    return set_error(MR_ERR_ARG, "mr_render_neural_noalloc supports MR_SAMPLER_EXACT only "
+                                 "(texture tables are allocated on first use)");
+  const size_t npx = (size_t)p->width * p->height;
+  if (npx > MR_NOALLOC_MAX_PIXELS)
+    return set_error(MR_ERR_ARG, "mr_render_neural_noalloc: %d x %d = %zu pixels exceeds MR_NOALLOC_MAX_PIXELS (%d)",
+                     p->width, p->height, npx, MR_NOALLOC_MAX_PIXELS);
+  Volume* v = &h->v;
+  if (!v->data_set || !v->mips_valid) return set_error(MR_ERR_STATE, "render before mr_volume_set_data / _update");
+  const F3 L = normalize(to_f3(p->light_dir));
+  if (!v->lut_valid || v->lut_g != p->g || v->lut_seed != p->seed)
+    return set_error(MR_ERR_STATE, "HG table not built for g=%g seed=%u: call mr_volume_update_hglut first", p->g,
+                     p->seed);
+  if (!v->tr_valid || L.x != v->tr_light.x || L.y != v->tr_light.y || L.z != v->tr_light.z || p->alpha != v->tr_alpha)
+    return set_error(MR_ERR_STATE, "transmittance pyramid not built for this light/alpha: call mr_volume_update_tr first");
+  void* base = nullptr;
+  rc = noalloc_scratch(&base);
+  if (rc) return rc;
+  return neural_passes(v, &nh->n, p, dev_rgb, (cudaStream_t)stream, base, false);
 }
