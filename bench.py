@@ -146,7 +146,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--frame", default=None,
+                    help="WxH instead of 1920x1080: a smaller case for profiler captures, not a bench line")
     args = ap.parse_args()
+    if args.frame:
+        global WIDTH, HEIGHT
+        WIDTH, HEIGHT = (int(x) for x in args.frame.lower().split("x"))
     args.warmup = max(args.warmup, 3)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

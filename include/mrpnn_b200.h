@@ -197,7 +197,7 @@ int mr_network_check(const mr_network* net, int32_t reset);
  *    the module there), so make it before any stream capture.
  * Stage timing (mr_volume_set_timing) does not cover this call. */
 #define MR_NOALLOC_MAX_PIXELS 16384
-#define MR_NOALLOC_SCRATCH_MIB 40
+#define MR_NOALLOC_SCRATCH_MIB 45
 int mr_render_neural_noalloc(mr_volume* v, const mr_network* net, const mr_render_params* p, float* dev_rgb,
                              void* stream);
 

@@ -69,6 +69,7 @@ struct Network {
   float* stencil = nullptr;  // 160 x 3
   void* packed = nullptr;    // tensor-core operand images (bf16/fp8), see mr_mlp_tc.cu
   size_t packed_bytes = 0;
+  std::vector<float> h_rowwise;  // fp32 per-row weights passed as kernel parameters (mr_mlp_tc.cu)
   float h_stencil[MR_STENCIL_POINTS * 3];
 };
 

@@ -1,8 +1,9 @@
 // FP32 radiance-predictor network, one thread per pixel, activations in
 // registers (core/radiancePredict.cu:370-485 in fp32).
 //
-// Descriptors are read as (row k, feature i) -> desc[k*rs + i*fs]; the render
-// path passes a feature-major buffer (rs = 1, fs = capacity) so that a warp's
+// Descriptors are read in chunks of 4 features: (row k, features 4j..4j+3) is
+// the float4 at desc[k*rs + j*cs]; the render path passes chunk-of-4
+// feature-major columns (rs = 4, cs = 4*capacity) so that a warp's
 // 32 loads of one feature are one coalesced transaction. Every layer up to
 // 32 wide is fully unrolled with compile-time register indices; the three
 // branches of a block are evaluated together (three independent FMA chains),
@@ -20,7 +21,7 @@ struct SimtArgs {
   const float* __restrict__ w;
   const float* __restrict__ desc;
   const float* __restrict__ aux;
-  long long rs, fs;      // desc strides (row, feature)
+  long long rs, cs;      // desc strides (row, 4-feature chunk)
   long long ars, afs;    // aux strides
   int n;
   const unsigned* __restrict__ count;  // device row count (render path) or null
@@ -62,8 +63,11 @@ __device__ __forceinline__ void dense3(const float (&x)[3][32], float (&y)[3][32
 
 struct RowIO {
   const float* __restrict__ d;
-  long long fs;
-  __device__ __forceinline__ float operator()(int i) const { return __ldg(d + i * fs); }
+  long long cs;
+  // features i..i+3, i a multiple of 4
+  __device__ __forceinline__ float4 ld4(int i) const {
+    return __ldg(reinterpret_cast<const float4*>(d + (i >> 2) * cs));
+  }
 };
 
 // SE / SERES block of width S (radiancePredict.cu:240-294). MODE 0: SE +
@@ -78,10 +82,10 @@ __device__ __forceinline__ void simt_block(const RowIO& in, const float* __restr
   for (int b = 0; b < 3; ++b) {
     float s = 0.0f, m = -10000.0f;
 #pragma unroll
-    for (int i = 0; i < S; ++i) {
-      float v = in(b * 192 + from + i);
-      s += v;
-      m = fmaxf(m, v);
+    for (int i = 0; i < S; i += 4) {
+      const float4 q = in.ld4(b * 192 + from + i);
+      s += q.x; s += q.y; s += q.z; s += q.w;
+      m = fmaxf(m, q.x); m = fmaxf(m, q.y); m = fmaxf(m, q.z); m = fmaxf(m, q.w);
     }
     mean[b] = s / (float)S;
     mx[b] = m;
@@ -115,22 +119,31 @@ __device__ __forceinline__ void simt_block(const RowIO& in, const float* __restr
 #pragma unroll
   for (int b = 0; b < 3; ++b)
 #pragma unroll
-    for (int i = 0; i < S; ++i) {
-      float v = in(b * 192 + from + i) * gate[b];
-      x[b][i] = MODE == 0 ? v : v + y[b][i];
+    for (int i = 0; i < S; i += 4) {
+      const float4 q = in.ld4(b * 192 + from + i);
+      const float qv[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        float v = qv[u] * gate[b];
+        x[b][i + u] = MODE == 0 ? v : v + y[b][i + u];
+      }
     }
   float yn[3][32];
   dense3<S>(x, yn, w, wa, wb, wc);
 #pragma unroll
   for (int b = 0; b < 3; ++b)
 #pragma unroll
-    for (int i = 0; i < S; ++i) {
-      float s = in(b * 192 + from + i);
-      if (MODE == 2) {
-        y[b][i] = yn[b][i];
-        y[b][S + i] = s;
-      } else {
-        y[b][i] = yn[b][i] + s;
+    for (int i = 0; i < S; i += 4) {
+      const float4 q = in.ld4(b * 192 + from + i);
+      const float qv[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (MODE == 2) {
+          y[b][i + u] = yn[b][i + u];
+          y[b][S + i + u] = qv[u];
+        } else {
+          y[b][i + u] = yn[b][i + u] + qv[u];
+        }
       }
     }
 }
@@ -260,7 +273,7 @@ __global__ void __launch_bounds__(kSimtThreads) k_mlp_simt(SimtArgs a) {
   const int k = blockIdx.x * kSimtThreads + threadIdx.x;
   if (k >= n) return;
   const float* __restrict__ w = a.w;
-  RowIO in{a.desc + (long long)k * a.rs, a.fs};
+  RowIO in{a.desc + (long long)k * a.rs, a.cs};
   const float* ax = a.aux + (long long)k * a.ars;
   const float g = __ldg(ax), gamma = __ldg(ax + a.afs);
   const float srp[3] = {__ldg(ax + 2 * a.afs), __ldg(ax + 3 * a.afs), __ldg(ax + 4 * a.afs)};
@@ -344,7 +357,7 @@ __global__ void __launch_bounds__(kSimtThreads) k_mlp_simt(SimtArgs a) {
   }
 }
 
-int launch_mlp_simt(const Network* net, const float* desc, const float* aux, long long rs, long long fs,
+int launch_mlp_simt(const Network* net, const float* desc, const float* aux, long long rs, long long cs,
                     long long ars, long long afs, int n, const unsigned* count, float* out, const int* pix,
                     const float* trph, F3 light_color, F3 scatter, cudaStream_t s) {
   SimtArgs a;
@@ -352,7 +365,7 @@ int launch_mlp_simt(const Network* net, const float* desc, const float* aux, lon
   a.desc = desc;
   a.aux = aux;
   a.rs = rs;
-  a.fs = fs;
+  a.cs = cs;
   a.ars = ars;
   a.afs = afs;
   a.n = n;

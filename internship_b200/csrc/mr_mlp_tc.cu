@@ -55,18 +55,54 @@ constexpr int tc_offset(int i) { int o = 0; for (int j = 0; j < i; ++j) o += tc_
 constexpr int kWBytes = tc_offset(kTcLayers);
 static_assert(kWBytes == 100352, "packed weight image size");
 
+// fp32 arrays read by the per-row code (squeeze-excitation, SEFin, LGGS,
+// LX12 and the biases of the MMA layers), compacted into an image that is
+// passed in the kernel's parameter space: uniform constant-bank operands
+// instead of one load instruction per weight and row.
+constexpr bool rowwise_used(int id) {
+  for (int i = 0; i < kTcLayers; ++i)
+    if (kTc[i].b == id) return true;
+  constexpr int ids[] = {MR_W_LSEFin1W, MR_W_LSEFin2W, MR_W_LGGSW, MR_W_LGGSB, MR_W_LX12W, MR_W_LX12B,
+                         MR_W_LSE01W, MR_W_LSE02W, MR_W_LSE11W, MR_W_LSE12W, MR_W_LSE21W, MR_W_LSE22W,
+                         MR_W_LSE31W, MR_W_LSE32W, MR_W_LSE41W, MR_W_LSE42W, MR_W_LSE51W, MR_W_LSE52W,
+                         MR_W_LSE61W, MR_W_LSE62W, MR_W_LSE71W, MR_W_LSE72W, MR_W_LDSE01W, MR_W_LDSE02W,
+                         MR_W_LDSE11W, MR_W_LDSE12W, MR_W_LDSE21W, MR_W_LDSE22W, MR_W_LDSE31W, MR_W_LDSE32W};
+  for (int x : ids)
+    if (x == id) return true;
+  return false;
+}
+struct RowTable { int off[MR_W_COUNT]; int total; };
+constexpr RowTable make_row_table() {
+  RowTable t{};
+  const WeightTable wt = make_weight_table();
+  int o = 0;
+  for (int i = 0; i < MR_W_COUNT; ++i) {
+    t.off[i] = rowwise_used(i) ? o : -1;
+    if (rowwise_used(i)) o += wt.size[i];
+  }
+  t.total = o;
+  return t;
+}
+constexpr int kRowFloats = make_row_table().total;
+template <int ID>
+struct ROff {
+  static constexpr int value = make_row_table().off[ID];
+  static_assert(value >= 0, "weight array not in the row-wise image");
+};
+#define ROFF(name) (::mr::ROff<MR_W_##name>::value)
+
 struct TcTables { int woff[kTcLayers]; int boff[kTcLayers]; };
 constexpr TcTables make_tc_tables() {
   TcTables t{};
-  WeightTable wt = make_weight_table();
-  for (int i = 0; i < kTcLayers; ++i) { t.woff[i] = tc_offset(i); t.boff[i] = wt.off[kTc[i].b]; }
+  const RowTable rt = make_row_table();
+  for (int i = 0; i < kTcLayers; ++i) { t.woff[i] = tc_offset(i); t.boff[i] = rt.off[kTc[i].b]; }
   return t;
 }
 __constant__ TcTables c_tc = make_tc_tables();
 __device__ __forceinline__ int tc_offset_dev(int i) { return c_tc.woff[i]; }
 __device__ __forceinline__ int kTcBias(int i) { return c_tc.boff[i]; }
 
-constexpr int kGroups = 3;
+constexpr int kGroups = 4;
 constexpr int kTrunkBytes = 3 * 128 * 32 * 2;  // 24 KB
 constexpr int kHeadBytes = 128 * 128 * 2;      // 32 KB
 // The trunk tiles and the head tile of a group share one region: every
@@ -208,11 +244,14 @@ __device__ __forceinline__ void issue_layer(uint32_t tmem_d, uint32_t a_addr, ui
 
 __device__ __forceinline__ float sigm(float x) { return 1.0f / (1.0f + expf(-x)); }
 
+// Read of the row-wise weight image (kernel parameter space).
+__device__ __forceinline__ float ldw(const float* p) { return *p; }
+
 struct TcArgs {
   const uint8_t* __restrict__ wpack;  // kWBytes packed bf16 image
-  const float* __restrict__ w;        // fp32 blob (biases, SE and small layers)
-  const float* __restrict__ desc;     // row k feature i at desc[k*rs + i*fs]
-  long long rs, fs, ars, afs;         // descriptor / aux strides
+  const float* __restrict__ w;        // fp32 blob
+  const float* __restrict__ desc;     // row k, chunk j (features 4j..4j+3) at desc[k*rs + j*cs]
+  long long rs, cs, ars, afs;         // descriptor / aux strides
   const float* __restrict__ aux;      // n x 5
   int n;
   float* out;                         // n x 3, or image when pix != null
@@ -220,15 +259,28 @@ struct TcArgs {
   const float* __restrict__ trph;     // compose mode: single-scatter term
   const unsigned* __restrict__ count; // compose mode: number of records (device)
   F3 light_color, scatter;
+  float* spill;                       // 120 x spill_cap ungated head columns (multi-channel tiles)
+  long long spill_cap;
   int* err;                           // set on a wait timeout
+  float rw[kRowFloats];               // row-wise fp32 weights (make_row_table)
 };
 
-// One descriptor row: feature i at p[i*fs] (fs = 1 row-major, fs = capacity
-// feature-major).
+// One descriptor row in chunk-of-4 order: features i..i+3 (i a multiple of
+// 4) are the float4 at p + (i/4)*cs, cs = 4*capacity for the render path's
+// chunked columns and 4 for row-major input. The address is formed inside
+// the asm so that the compiler cannot keep hundreds of row addresses live
+// across the MMA waits.
 struct DIn {
   const float* __restrict__ p;
-  long long fs;
-  __device__ __forceinline__ float operator[](int i) const { return __ldg(p + i * fs); }
+  int cs16;  // chunk stride in bytes
+  __device__ __forceinline__ float4 ld4(int i) const {
+    float4 v;
+    asm volatile(
+        "{\n\t.reg .u64 a;\n\tmad.wide.s32 a, %4, %5, %6;\n\tld.global.nc.v4.f32 {%0,%1,%2,%3}, [a];\n\t}\n"
+        : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+        : "r"(i >> 2), "r"(cs16), "l"(p));
+    return v;
+  }
 };
 
 struct GroupCtx {
@@ -272,130 +324,235 @@ __device__ __forceinline__ void epi_relu(const GroupCtx& c, int col, const float
 #pragma unroll
     for (int i = 0; i < 16; ++i)
       if (16 * h + i < N) {
-        float a = __ldg(bias + 16 * h + i) + v[i];
+        float a = ldw(bias + 16 * h + i) + v[i];
         y[16 * h + i] = a >= 0.0f ? a : 0.0f;
       }
   }
 }
 
-// SE / SERES block of the trunks (radiancePredict.cu:240-294) for branch
-// width S on the descriptor row d, pooling into the SEFin1 accumulators.
-// MODE: 0 = SE, then ADD3; 1 = SERES, then ADD3; 2 = SERES, then REP3.
-template <int S, int MODE>
-__device__ __noinline__ void trunk_block(GroupCtx& c, const DIn& d, const float* __restrict__ w,
-                                            int from, int pid, int sew0, int sew1, int layer0, float g, float gamma,
-                                            float (&y)[3][32], float* fin) {
-  constexpr int KP = S < 16 ? 16 : S;
-  // pooled statistics of the three descriptor segments
+// Split MMA round: issue (after making this group's A rows visible to the
+// tensor core), then wait. Work between the two overlaps the MMA.
+template <typename IssueFn>
+__device__ __forceinline__ void mma_issue(GroupCtx& c, IssueFn issue) {
+  fence_async_smem();
+  tc_fence_before();
+  group_bar(c.g);
+  if (c.t == 0) {
+    tc_fence_after();
+    issue();
+    umma_commit(c.mbar);
+  }
+}
+__device__ __forceinline__ void mma_wait(GroupCtx& c) {
+  if (c.ok && !mbar_wait(c.mbar, c.phase)) c.ok = false;
+  c.phase ^= 1u;
+  tc_fence_after();
+}
+
+// 8 fp32 values to / from this thread's TMEM lane (columns col..col+7).
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const float* v) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};\n" ::"r"(taddr),
+               "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+               "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+               "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7]))
+               : "memory");
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v) {
+  uint32_t r[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+constexpr int kBr = 128 * 32 * 2;  // bytes of one branch tile (K <= 32)
+
+// Pooled statistics of one trunk block's three descriptor segments
+// (radiancePredict.cu:240-294): mean and max, their LSEFin1 contributions
+// (pool[pid+br], pool[36+pid+br]) and the block's squeeze-excitation gates.
+// Depends only on the descriptor, g and gamma, so it runs while the previous
+// layer's MMA is in flight.
+template <int S>
+__device__ __forceinline__ void block_prep(const DIn& d, const float* __restrict__ w, int from, int pid, int sew0,
+                                           int sew1, float g, float gamma, float* fin, float* gate) {
   float mean[3], mx[3];
 #pragma unroll
   for (int br = 0; br < 3; ++br) {
     float s = 0.0f, m = -10000.0f;
 #pragma unroll
-    for (int i = 0; i < S; ++i) {
-      float v = d[br * 192 + from + i];
-      s += v;
-      m = fmaxf(m, v);
+    for (int i = 0; i < S; i += 4) {
+      const float4 q = d.ld4(br * 192 + from + i);
+      s += q.x; s += q.y; s += q.z; s += q.w;
+      m = fmaxf(fmaxf(m, q.x), fmaxf(q.y, fmaxf(q.z, q.w)));
     }
     mean[br] = s / (float)S;
     mx[br] = m;
   }
-  // LSEFin1 (16 x 75) contributions of pool[pid+br] and pool[36+pid+br]
-  const float* f1 = w + WOFF(LSEFin1W);
+  const float* f1 = w + ROFF(LSEFin1W);
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
     float a = fin[j];
 #pragma unroll
     for (int br = 0; br < 3; ++br) {
-      a += mean[br] * __ldg(f1 + j * 75 + pid + br);
-      a += mx[br] * __ldg(f1 + j * 75 + 36 + pid + br);
+      a += mean[br] * ldw(f1 + j * 75 + pid + br);
+      a += mx[br] * ldw(f1 + j * 75 + 36 + pid + br);
     }
     fin[j] = a;
   }
-  // squeeze-excitation gates
-  float tmp[8] = {mean[0], mean[1], mean[2], mx[0], mx[1], mx[2], g, gamma};
+  const float tmp[8] = {mean[0], mean[1], mean[2], mx[0], mx[1], mx[2], g, gamma};
   float h[8];
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     float a = 0.0f;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) a += tmp[j] * __ldg(w + sew0 + j + i * 8);
+    for (int j = 0; j < 8; ++j) a += tmp[j] * ldw(w + sew0 + j + i * 8);
     h[i] = a >= 0.0f ? a : 0.0f;
   }
-  float gate[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
     float a = 0.0f;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) a += h[j] * __ldg(w + sew1 + j + i * 8);
+    for (int j = 0; j < 8; ++j) a += h[j] * ldw(w + sew1 + j + i * 8);
     gate[i] = sigm(a);
   }
-  // layer inputs x = seg * gate (+ previous output)
+}
+
+// A rows of a block that starts a trunk (SE, no residual input): seg * gate.
+template <int S>
+__device__ __forceinline__ void store_first(GroupCtx& c, const DIn& d, int from, const float* gate) {
+  constexpr int KP = S < 16 ? 16 : S;
 #pragma unroll
   for (int br = 0; br < 3; ++br) {
     float x[KP];
 #pragma unroll
-    for (int i = 0; i < KP; ++i) {
-      float v = 0.0f;
+    for (int i = 0; i < KP; i += 4) {
       if (i < S) {
-        v = d[br * 192 + from + i] * gate[br];
-        if (MODE != 0) v = v + y[br][i];
+        const float4 q = d.ld4(br * 192 + from + i);
+        x[i] = q.x * gate[br]; x[i + 1] = q.y * gate[br]; x[i + 2] = q.z * gate[br]; x[i + 3] = q.w * gate[br];
+      } else {
+        x[i] = x[i + 1] = x[i + 2] = x[i + 3] = 0.0f;
       }
-      x[i] = v;
     }
-    store_row<KP>(c.trunk + br * (128 * 32 * 2), c.t, x);
+    store_row<KP>(c.trunk + br * kBr, c.t, x);
   }
-  const uint32_t tb = smem_u32(c.trunk), wb = smem_u32(c.wsm);
-  mma_round(c, [&]() {
-#pragma unroll
-    for (int br = 0; br < 3; ++br)
-      issue_layer<KP, KP>(c.tmem + 32 * br, tb + br * (128 * 32 * 2), wb + tc_offset_dev(layer0 + br));
-  });
-  // epilogue: ReLU(W x + b), then ADD3 / REP3
+}
+
+// Epilogue of trunk block (S, MODE) at descriptor offset `from`:
+// yn = ReLU(acc + b); y = yn + seg (ADD3) or [yn, seg] (REP3, MODE 2).
+// NEXT = 0: writes the next block's A rows seg2 * gate2 + y (SERES input,
+// radiancePredict.cu:259-294); NEXT = 1: writes y (input of L81 / LD41).
+template <int S, int MODE, int NEXT>
+__device__ __forceinline__ void block_epi(GroupCtx& c, const DIn& d, const float* __restrict__ w, int layer0, int from,
+                                          int from2, const float* gate2) {
+  constexpr int W = MODE == 2 ? 2 * S : S;
+  constexpr int KP = W < 16 ? 16 : W;
 #pragma unroll
   for (int br = 0; br < 3; ++br) {
-    float yn[32];
-    epi_relu<S>(c, 32 * br, w + kTcBias(layer0 + br), yn);
+    const float* bias = w + kTcBias(layer0 + br);
+    float y[KP];
 #pragma unroll
-    for (int i = 0; i < S; ++i) {
-      float s = d[br * 192 + from + i];
-      if (MODE == 2) {
-        y[br][i] = yn[i];
-        y[br][S + i] = s;
-      } else {
-        y[br][i] = yn[i] + s;
+    for (int h = 0; h < (S + 15) / 16; ++h) {
+      float v[16];
+      tmem_ld16(c.tmem + c.tlane + 32 * br + 16 * h, v);
+#pragma unroll
+      for (int i = 0; i < 16; ++i)
+        if (16 * h + i < S) {
+          const float a = v[i] + ldw(bias + 16 * h + i);
+          y[16 * h + i] = a >= 0.0f ? a : 0.0f;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < S; i += 4) {
+      const float4 q = d.ld4(br * 192 + from + i);
+      const float sv[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (MODE == 2) y[S + i + u] = sv[u];
+        else y[i + u] = y[i + u] + sv[u];
       }
     }
+#pragma unroll
+    for (int i = W; i < KP; ++i) y[i] = 0.0f;
+    if (NEXT == 0) {
+#pragma unroll
+      for (int i = 0; i < W; i += 4) {
+        const float4 q = d.ld4(br * 192 + from2 + i);
+        y[i] = q.x * gate2[br] + y[i];
+        y[i + 1] = q.y * gate2[br] + y[i + 1];
+        y[i + 2] = q.z * gate2[br] + y[i + 2];
+        y[i + 3] = q.w * gate2[br] + y[i + 3];
+      }
+    }
+    store_row<KP>(c.trunk + br * kBr, c.t, y);
+  }
+}
+
+template <int KP>
+__device__ __forceinline__ void issue_trunk(GroupCtx& c, int layer0) {
+  const uint32_t tb = smem_u32(c.trunk), wb = smem_u32(c.wsm);
+  mma_issue(c, [&]() {
+#pragma unroll
+    for (int br = 0; br < 3; ++br) issue_layer<KP, KP>(c.tmem + 32 * br, tb + br * kBr, wb + tc_offset_dev(layer0 + br));
+  });
+}
+
+// Channel-dependent head gates: LGGS(g, gamma, srp) -> x8 (head columns
+// 120..127) and the six SEFin gates sep (radiancePredict.cu:439-452).
+__device__ __forceinline__ void head_gates(const float* __restrict__ w, const float* fin, float g, float gamma,
+                                           float srp, float* x8, float* sep) {
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    float a = g * ldw(w + ROFF(LGGSW) + 3 * i) + gamma * ldw(w + ROFF(LGGSW) + 3 * i + 1) +
+              srp * ldw(w + ROFF(LGGSW) + 3 * i + 2);
+    a += ldw(w + ROFF(LGGSB) + i);
+    x8[i] = a >= 0.0f ? a : 0.0f;
+  }
+  float sew[16];
+  const float* f1 = w + ROFF(LSEFin1W);
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const float a = fin[j] + g * ldw(f1 + j * 75 + 72) + gamma * ldw(f1 + j * 75 + 73) + srp * ldw(f1 + j * 75 + 74);
+    sew[j] = a >= 0.0f ? a : 0.0f;
+  }
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    float a = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) a += sew[j] * ldw(w + ROFF(LSEFin2W) + j + i * 16);
+    sep[i] = sigm(a);
   }
 }
 
 // Head SC(p) (radiancePredict.cu:439-473) for one albedo channel; the
 // gated 128-wide input is already in c.head (bf16). Returns the output X.
-__device__ __noinline__ float head_chain(GroupCtx& c, const float* __restrict__ w) {
+__device__ __forceinline__ float head_chain(GroupCtx& c, const float* __restrict__ w) {
   const uint32_t hb = smem_u32(c.head), tb = smem_u32(c.trunk), wb = smem_u32(c.wsm);
   float v[32];
   // LC0 128 -> 128, read back and re-stored 32 columns at a time
   mma_round(c, [&]() { issue_layer<128, 128>(c.tmem, hb, wb + tc_offset(TC_LC0)); });
 #pragma unroll 1
   for (int h = 0; h < 4; ++h) {
-    epi_relu<32>(c, 32 * h, w + WOFF(LC0B) + 32 * h, v);
+    epi_relu<32>(c, 32 * h, w + ROFF(LC0B) + 32 * h, v);
     store_cols<128, 32>(c.head, c.t, 32 * h, v);
   }
   // LC1 128 -> 64
   mma_round(c, [&]() { issue_layer<64, 128>(c.tmem, hb, wb + tc_offset(TC_LC1)); });
 #pragma unroll 1
   for (int h = 0; h < 2; ++h) {
-    epi_relu<32>(c, 32 * h, w + WOFF(LC1B) + 32 * h, v);
+    epi_relu<32>(c, 32 * h, w + ROFF(LC1B) + 32 * h, v);
     store_cols<64, 32>(c.trunk, c.t, 32 * h, v);
   }
   // LC2 64 -> 32
   mma_round(c, [&]() { issue_layer<32, 64>(c.tmem, tb, wb + tc_offset(TC_LC2)); });
-  epi_relu<32>(c, 0, w + WOFF(LC2B), v);
+  epi_relu<32>(c, 0, w + ROFF(LC2B), v);
   store_row<32>(c.trunk, c.t, v);
   // LX 32 -> 16
   mma_round(c, [&]() { issue_layer<16, 32>(c.tmem, tb, wb + tc_offset(TC_LX)); });
   float a[16], b[16];
-  epi_relu<16>(c, 0, w + WOFF(LXB), a);
+  epi_relu<16>(c, 0, w + ROFF(LXB), a);
   // six residual pairs (:454-471)
 #pragma unroll 1
   for (int r = 0; r < 6; ++r) {
@@ -412,66 +569,45 @@ __device__ __noinline__ float head_chain(GroupCtx& c, const float* __restrict__ 
   // LX12 16 -> 1, bias after the sum (LinearReLU, :41-56)
   float o = 0.0f;
 #pragma unroll
-  for (int i = 0; i < 16; ++i) o += a[i] * __ldg(w + WOFF(LX12W) + i);
-  o += __ldg(w + WOFF(LX12B));
+  for (int i = 0; i < 16; ++i) o += a[i] * ldw(w + ROFF(LX12W) + i);
+  o += ldw(w + ROFF(LX12B));
   return o >= 0.0f ? o : 0.0f;
 }
 
-// Builds the gated head input for albedo channel value srp into c.head.
-__device__ __noinline__ void head_input(GroupCtx& c, const float* __restrict__ w, const float* comb_raw,
-                                           const float* fin, float g, float gamma, float srp) {
-  // pool[72..74] = g, gamma, srp: LGGS (3 -> 8, bias last) and LSEFin1's last columns
-  float x8[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    float a = g * __ldg(w + WOFF(LGGSW) + 3 * i) + gamma * __ldg(w + WOFF(LGGSW) + 3 * i + 1) +
-              srp * __ldg(w + WOFF(LGGSW) + 3 * i + 2);
-    a += __ldg(w + WOFF(LGGSB) + i);
-    x8[i] = a >= 0.0f ? a : 0.0f;
-  }
+// Head input of a further albedo channel, from the ungated head columns the
+// first pass spilled (feature-major, comb[i] at spill[i*cap + row]).
+__device__ __forceinline__ void head_input_spilled(GroupCtx& c, const float* __restrict__ w, const float* spill,
+                                                long long cap, int row, const float* fin, float g, float gamma,
+                                                float srp) {
+  float x8[8], sep[6];
+  head_gates(w, fin, g, gamma, srp, x8, sep);
   store_cols<128, 8>(c.head, c.t, 120, x8);
-  float sew[16];
-  const float* f1 = w + WOFF(LSEFin1W);
-#pragma unroll
-  for (int j = 0; j < 16; ++j) {
-    float a = fin[j] + g * __ldg(f1 + j * 75 + 72) + gamma * __ldg(f1 + j * 75 + 73) + srp * __ldg(f1 + j * 75 + 74);
-    sew[j] = a >= 0.0f ? a : 0.0f;
-  }
-  float sep[6];
-#pragma unroll
-  for (int i = 0; i < 6; ++i) {
-    float a = 0.0f;
-#pragma unroll
-    for (int j = 0; j < 16; ++j) a += sew[j] * __ldg(w + WOFF(LSEFin2W) + j + i * 16);
-    sep[i] = sigm(a);
-  }
-  // gated comb, 8 columns at a time: segments [0,32) [32,64) [64,96) use
-  // gates 0..2, [96,104) [104,112) [112,120) gates 3..5
 #pragma unroll 1
   for (int g8 = 0; g8 < 15; ++g8) {
     const float s = sep[g8 < 12 ? g8 / 4 : g8 - 9];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) x8[i] = comb_raw[8 * g8 + i] * s;
+    for (int i = 0; i < 8; ++i) x8[i] = spill[(8 * g8 + i) * cap + row] * s;
     store_cols<128, 8>(c.head, c.t, 8 * g8, x8);
   }
 }
 
-// Light-direction trunk block (width 8).
-template <int MODE>
-__device__ __forceinline__ void di_block(GroupCtx& c, const DIn& d, const float* __restrict__ w,
-                                         int blk, float g, float gamma, float (&y)[3][32], float* fin) {
-  const int sew0[4] = {WOFF(LDSE01W), WOFF(LDSE11W), WOFF(LDSE21W), WOFF(LDSE31W)};
-  const int sew1[4] = {WOFF(LDSE02W), WOFF(LDSE12W), WOFF(LDSE22W), WOFF(LDSE32W)};
-  trunk_block<8, MODE>(c, d, w, 160 + 8 * blk, 24 + 3 * blk, sew0[blk], sew1[blk], TC_DI + 3 * blk, g, gamma, y, fin);
+// Group-wide OR of a per-row flag (named barrier g+1 with reduction).
+__device__ __forceinline__ bool group_any(int g, bool x) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.or.pred q, %2, 128, p;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)x), "r"(g + 1)
+      : "memory");
+  return r != 0;
 }
 
-__global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(TcArgs a) {
+__global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(const __grid_constant__ TcArgs a) {
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* wsm = smem;
   uint8_t* gbase = smem + kWBytes;
   uint64_t* mbars = reinterpret_cast<uint64_t*>(smem + kWBytes + kGroups * kGroupBytes);
   uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(mbars + kGroups);
-  volatile unsigned* need_slot = tmem_holder + 1;  // kGroups slots
   const int tid = threadIdx.x, warp = tid >> 5;
   const int g = tid >> 7, t = tid & 127;
   // weights -> shared memory (16-byte vectors)
@@ -500,8 +636,11 @@ __global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(TcArgs a) {
   c.t = t;
   c.wsm = wsm;
   c.ok = true;
-  const float* __restrict__ w = a.w;
+  const float* __restrict__ w = a.rw;
   const int n = a.pix ? (int)min(*a.count, (unsigned)a.n) : a.n;
+  // TMEM columns 96..119 of the group hold the light trunk's LD41 output
+  // while the main trunk (columns 0..95) runs.
+  const uint32_t tcomb = c.tmem + c.tlane + 96;
 
   for (int it = 0;; ++it) {
     // static tile striding over (CTA, group)
@@ -509,85 +648,148 @@ __global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(TcArgs a) {
     if (tile * 128 >= n) break;  // group-uniform exit
     const int row = tile * 128 + t;
     const int kk = row < n ? row : n - 1;
-    const DIn d{a.desc + (long long)kk * a.rs, a.fs};
+    const DIn d{a.desc + (long long)kk * a.rs, (int)(a.cs * 4)};
     const float* ax = a.aux + (long long)kk * a.ars;
     const float gg = __ldg(ax), gamma = __ldg(ax + a.afs);
     float srp[3] = {__ldg(ax + 2 * a.afs), __ldg(ax + 3 * a.afs), __ldg(ax + 4 * a.afs)};
+    // further heads (radiancePredict.cu:478-483), decided for the whole tile
+    const bool need1 = group_any(g, srp[1] != srp[0]);
+    const bool need2 = group_any(g, srp[2] != srp[0] && srp[2] != srp[1]);
     float fin[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) fin[j] = 0.0f;
-    float y[3][32];
-    // comb (the head input before gating) lives in local memory through an
-    // opaque offset; it is written in chunks and read once per head.
-    float comb_store[120];
-    int zero = 0;
-    asm volatile("" : "+r"(zero));
-    float* comb = comb_store + zero;
-    // main trunk (radiancePredict.cu:396-421)
-    trunk_block<8, 0>(c, d, w, 0, 0, WOFF(LSE01W), WOFF(LSE02W), TC_MAIN + 0, gg, gamma, y, fin);
-    trunk_block<8, 2>(c, d, w, 8, 3, WOFF(LSE11W), WOFF(LSE12W), TC_MAIN + 3, gg, gamma, y, fin);
-    trunk_block<16, 1>(c, d, w, 16, 6, WOFF(LSE21W), WOFF(LSE22W), TC_MAIN + 6, gg, gamma, y, fin);
-    trunk_block<16, 1>(c, d, w, 32, 9, WOFF(LSE31W), WOFF(LSE32W), TC_MAIN + 9, gg, gamma, y, fin);
-    trunk_block<16, 2>(c, d, w, 48, 12, WOFF(LSE41W), WOFF(LSE42W), TC_MAIN + 12, gg, gamma, y, fin);
-    trunk_block<32, 1>(c, d, w, 64, 15, WOFF(LSE51W), WOFF(LSE52W), TC_MAIN + 15, gg, gamma, y, fin);
-    trunk_block<32, 1>(c, d, w, 96, 18, WOFF(LSE61W), WOFF(LSE62W), TC_MAIN + 18, gg, gamma, y, fin);
-    trunk_block<32, 1>(c, d, w, 128, 21, WOFF(LSE71W), WOFF(LSE72W), TC_MAIN + 21, gg, gamma, y, fin);
-    {  // L81 per branch -> comb[0..96)
+    float gate[3];
+
+    // light-direction trunk (:424-437): blocks at 160, 168, 176, 184
+    block_prep<8>(d, w, 160, 24, ROFF(LDSE01W), ROFF(LDSE02W), gg, gamma, fin, gate);
+    store_first<8>(c, d, 160, gate);
+    issue_trunk<16>(c, TC_DI + 0);
+    block_prep<8>(d, w, 168, 27, ROFF(LDSE11W), ROFF(LDSE12W), gg, gamma, fin, gate);
+    mma_wait(c);
+    block_epi<8, 0, 0>(c, d, w, TC_DI + 0, 160, 168, gate);
+    issue_trunk<16>(c, TC_DI + 3);
+    block_prep<8>(d, w, 176, 30, ROFF(LDSE21W), ROFF(LDSE22W), gg, gamma, fin, gate);
+    mma_wait(c);
+    block_epi<8, 1, 0>(c, d, w, TC_DI + 3, 168, 176, gate);
+    issue_trunk<16>(c, TC_DI + 6);
+    block_prep<8>(d, w, 184, 33, ROFF(LDSE31W), ROFF(LDSE32W), gg, gamma, fin, gate);
+    mma_wait(c);
+    block_epi<8, 1, 0>(c, d, w, TC_DI + 6, 176, 184, gate);
+    issue_trunk<16>(c, TC_DI + 9);
+    block_prep<8>(d, w, 0, 0, ROFF(LSE01W), ROFF(LSE02W), gg, gamma, fin, gate);  // main block 0
+    mma_wait(c);
+    block_epi<8, 1, 1>(c, d, w, TC_DI + 9, 184, 0, nullptr);
+    issue_trunk<16>(c, TC_LD41);
+    mma_wait(c);
+    // LD41 -> comb[96..120), parked in TMEM
 #pragma unroll
-      for (int br = 0; br < 3; ++br) store_row<32>(c.trunk + br * (128 * 32 * 2), c.t, y[br]);
-      const uint32_t tb = smem_u32(c.trunk), wb = smem_u32(c.wsm);
-      mma_round(c, [&]() {
+    for (int br = 0; br < 3; ++br) {
+      float v[8];
+      tmem_ld8(c.tmem + c.tlane + 32 * br, v);
+      const float* bias = w + kTcBias(TC_LD41 + br);
 #pragma unroll
-        for (int br = 0; br < 3; ++br)
-          issue_layer<32, 32>(c.tmem + 32 * br, tb + br * (128 * 32 * 2), wb + tc_offset(TC_L81) + 2048 * br);
-      });
-#pragma unroll
-      for (int br = 0; br < 3; ++br) epi_relu<32>(c, 32 * br, w + kTcBias(TC_L81 + br), comb + 32 * br);
-    }
-    // light-direction trunk (:424-437)
-    di_block<0>(c, d, w, 0, gg, gamma, y, fin);
-    di_block<1>(c, d, w, 1, gg, gamma, y, fin);
-    di_block<1>(c, d, w, 2, gg, gamma, y, fin);
-    di_block<1>(c, d, w, 3, gg, gamma, y, fin);
-    {  // LD41 per branch -> comb[96..120)
-#pragma unroll
-      for (int br = 0; br < 3; ++br) {
-        float x[16];
-#pragma unroll
-        for (int i = 0; i < 16; ++i) x[i] = i < 8 ? y[br][i] : 0.0f;
-        store_row<16>(c.trunk + br * (128 * 32 * 2), c.t, x);
+      for (int i = 0; i < 8; ++i) {
+        const float x = v[i] + ldw(bias + i);
+        v[i] = x >= 0.0f ? x : 0.0f;
       }
-      const uint32_t tb = smem_u32(c.trunk), wb = smem_u32(c.wsm);
-      mma_round(c, [&]() {
-#pragma unroll
-        for (int br = 0; br < 3; ++br)
-          issue_layer<16, 16>(c.tmem + 32 * br, tb + br * (128 * 32 * 2), wb + tc_offset(TC_LD41) + 512 * br);
-      });
-#pragma unroll
-      for (int br = 0; br < 3; ++br) epi_relu<8>(c, 32 * br, w + kTcBias(TC_LD41 + br), comb + 96 + 8 * br);
+      tmem_st8(tcomb + 8 * br, v);
     }
-    // heads per distinct albedo channel (group-uniform decision)
-    float X[3];
-    head_input(c, w, comb, fin, gg, gamma, srp[0]);
-    X[0] = head_chain(c, w);
+
+    // main trunk (:396-421)
+    store_first<8>(c, d, 0, gate);
+    issue_trunk<16>(c, TC_MAIN + 0);
+    block_prep<8>(d, w, 8, 3, ROFF(LSE11W), ROFF(LSE12W), gg, gamma, fin, gate);
+    mma_wait(c);
+    block_epi<8, 0, 0>(c, d, w, TC_MAIN + 0, 0, 8, gate);
+    issue_trunk<16>(c, TC_MAIN + 3);
+    block_prep<16>(d, w, 16, 6, ROFF(LSE21W), ROFF(LSE22W), gg, gamma, fin, gate);
+    mma_wait(c);
+    block_epi<8, 2, 0>(c, d, w, TC_MAIN + 3, 8, 16, gate);
+    issue_trunk<16>(c, TC_MAIN + 6);
+    block_prep<16>(d, w, 32, 9, ROFF(LSE31W), ROFF(LSE32W), gg, gamma, fin, gate);
+    mma_wait(c);
+    block_epi<16, 1, 0>(c, d, w, TC_MAIN + 6, 16, 32, gate);
+    issue_trunk<16>(c, TC_MAIN + 9);
+    block_prep<16>(d, w, 48, 12, ROFF(LSE41W), ROFF(LSE42W), gg, gamma, fin, gate);
+    mma_wait(c);
+    block_epi<16, 1, 0>(c, d, w, TC_MAIN + 9, 32, 48, gate);
+    issue_trunk<16>(c, TC_MAIN + 12);
+    block_prep<32>(d, w, 64, 15, ROFF(LSE51W), ROFF(LSE52W), gg, gamma, fin, gate);
+    mma_wait(c);
+    block_epi<16, 2, 0>(c, d, w, TC_MAIN + 12, 48, 64, gate);
+    issue_trunk<32>(c, TC_MAIN + 15);
+    block_prep<32>(d, w, 96, 18, ROFF(LSE61W), ROFF(LSE62W), gg, gamma, fin, gate);
+    mma_wait(c);
+    block_epi<32, 1, 0>(c, d, w, TC_MAIN + 15, 64, 96, gate);
+    issue_trunk<32>(c, TC_MAIN + 18);
+    block_prep<32>(d, w, 128, 21, ROFF(LSE71W), ROFF(LSE72W), gg, gamma, fin, gate);
+    mma_wait(c);
+    block_epi<32, 1, 0>(c, d, w, TC_MAIN + 18, 96, 128, gate);
+    issue_trunk<32>(c, TC_MAIN + 21);
+    mma_wait(c);
+    block_epi<32, 1, 1>(c, d, w, TC_MAIN + 21, 128, 0, nullptr);
+    issue_trunk<32>(c, TC_L81);
+    // channel-0 head gates while L81 runs (fin is complete)
+    float x8[8], sep[6];
+    head_gates(w, fin, gg, gamma, srp[0], x8, sep);
+    mma_wait(c);
+    // L81 -> comb[0..96); gated head input for channel 0 (:439-452)
+    const bool spill = (need1 || need2) && a.spill != nullptr;
+    const long long cap = a.spill_cap;
+#pragma unroll
+    for (int br = 0; br < 3; ++br) {
+      const float* bias = w + kTcBias(TC_L81 + br);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        float v[16];
+        tmem_ld16(c.tmem + c.tlane + 32 * br + 16 * h, v);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const float x = v[i] + ldw(bias + 16 * h + i);
+          v[i] = x >= 0.0f ? x : 0.0f;
+        }
+        if (spill && row < n) {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) a.spill[(32 * br + 16 * h + i) * cap + row] = v[i];
+        }
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[i] *= sep[br];
+        store_cols<128, 16>(c.head, c.t, 32 * br + 16 * h, v);
+      }
+    }
+#pragma unroll
+    for (int br = 0; br < 3; ++br) {
+      float v[8];
+      tmem_ld8(tcomb + 8 * br, v);
+      if (spill && row < n) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) a.spill[(96 + 8 * br + i) * cap + row] = v[i];
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) v[i] *= sep[3 + br];
+      store_cols<128, 8>(c.head, c.t, 96 + 8 * br, v);
+    }
+    store_cols<128, 8>(c.head, c.t, 120, x8);
+    // heads: channel 0, then the further distinct channels of the tile
+    float X[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll 1
-    for (int ch = 1; ch < 3; ++ch) {
-      // The head runs for the whole tile if any row's channel differs from
-      // the channels already evaluated (radiancePredict.cu:478-483).
-      const bool same = srp[ch] == srp[0] || (ch == 2 && srp[2] == srp[1]);
-      if (t == 0) need_slot[g] = 0u;
-      group_bar(g);
-      if (!same) need_slot[g] = 1u;
-      group_bar(g);
-      const bool any = need_slot[g] != 0u;
-      group_bar(g);
-      if (any) {
-        head_input(c, w, comb, fin, gg, gamma, srp[ch]);
-        X[ch] = head_chain(c, w);
-      } else {
-        X[ch] = srp[ch] == srp[0] ? X[0] : X[1];
+    for (int ch = 0; ch < 3; ++ch) {
+      if ((ch == 1 && !need1) || (ch == 2 && !need2)) continue;
+      if (ch > 0) {
+        if (a.spill == nullptr) {  // host contract: multi-channel tiles need the spill buffer
+          c.ok = false;
+          break;
+        }
+        head_input_spilled(c, w, a.spill, cap, row < n ? row : 0, fin, gg, gamma, ch == 1 ? srp[1] : srp[2]);
       }
+      const float x = head_chain(c, w);
+      if (ch == 0) X[0] = x;
+      else if (ch == 1) X[1] = x;
+      else X[2] = x;
     }
+    if (srp[1] == srp[0]) X[1] = X[0];
+    if (srp[2] == srp[0]) X[2] = X[0];
+    else if (srp[2] == srp[1]) X[2] = X[1];
     if (row < n) {
       float o[3];
 #pragma unroll
@@ -613,7 +815,6 @@ __global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(TcArgs a) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_holder), "r"(kTmemCols));
   }
 }
-
 // One tile through the same descriptors: D[128 x N] = A[128 x K] * B[N x K]^T.
 template <int N, int K>
 __global__ void __launch_bounds__(128, 1) k_tc_selftest(const uint16_t* __restrict__ A, const uint16_t* __restrict__ B,
@@ -691,6 +892,11 @@ int pack_network(Network* n) {
         std::memcpy(base + canon_off(r, k, kp), &b, 2);
       }
   }
+  // row-wise fp32 image for the kernel parameters
+  const RowTable rt = make_row_table();
+  n->h_rowwise.assign(kRowFloats, 0.0f);
+  for (int id = 0; id < MR_W_COUNT; ++id)
+    if (rt.off[id] >= 0) std::memcpy(&n->h_rowwise[rt.off[id]], w.data() + wt.off[id], wt.size[id] * sizeof(float));
   cudaError_t e = cudaMalloc(&n->packed, kWBytes + 256);
   if (e == cudaSuccess) e = cudaMemcpy(n->packed, img.data(), kWBytes, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset((uint8_t*)n->packed + kWBytes, 0, 256);
@@ -706,10 +912,14 @@ void free_packed(Network* n) {
 }
 
 // Launch the tensor-core network. pix/trph/count != null selects compose
-// mode (out = image). The error word lives after the packed image.
-int launch_mlp_tc(const Network* net, const float* desc, const float* aux, long long rs, long long fs,
+// mode (out = image). `spill` (120 x n floats) is required when rows may have
+// distinct albedo channels; the kernel reports a missing one through the
+// error word. The error word lives after the packed image.
+int launch_mlp_tc(const Network* net, const float* desc, const float* aux, long long rs, long long cs,
                   long long ars, long long afs, int n, float* out, const int* pix, const float* trph,
-                  const unsigned* count, F3 light_color, F3 scatter, cudaStream_t s) {
+                  const unsigned* count, F3 light_color, F3 scatter, float* spill, cudaStream_t s) {
+  if (cs * 4 > 0x7FFFFFFFll || n > (1 << 28))
+    return set_error(MR_ERR_ARG, "tensor-core network: %d rows / chunk stride %lld out of range", n, cs);
   static bool attr = false;
   if (!attr) {
     MR_CUDA(cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
@@ -721,7 +931,7 @@ int launch_mlp_tc(const Network* net, const float* desc, const float* aux, long 
   a.desc = desc;
   a.aux = aux;
   a.rs = rs;
-  a.fs = fs;
+  a.cs = cs;
   a.ars = ars;
   a.afs = afs;
   a.n = n;
@@ -731,6 +941,10 @@ int launch_mlp_tc(const Network* net, const float* desc, const float* aux, long 
   a.count = count;
   a.light_color = light_color;
   a.scatter = scatter;
+  a.spill = spill;
+  a.spill_cap = n;
+  if (net->h_rowwise.size() != (size_t)kRowFloats) return set_error(MR_ERR_STATE, "network not packed");
+  std::memcpy(a.rw, net->h_rowwise.data(), sizeof(a.rw));
   a.err = (int*)((uint8_t*)net->packed + kWBytes);
   int tiles = (n + 127) / 128;
   int grid = std::min(sm_count(), std::max(1, (tiles + kGroups - 1) / kGroups));

@@ -237,8 +237,12 @@ __device__ __forceinline__ void gather_seg(const Tables& t, const float* __restr
   const float radius = (float)(1 << MIP) / 256.0f;
   const float kAng = 3.1415926535f * 60.0f / 180.0f;
   float vrow = atanf(0.5f * radius / off) / kAng;
-#pragma unroll 2
-  for (int i = I0; i < I1; ++i) {
+  static_assert(I0 % 4 == 0 && I1 % 4 == 0, "segments are whole 4-feature chunks");
+#pragma unroll 1
+  for (int i0 = I0; i0 < I1; i0 += 4)
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int i = i0 + u;
     F3 p;
     float c1, c2;
     if (SPHERE) {
@@ -280,7 +284,7 @@ __device__ __forceinline__ void gather_seg(const Tables& t, const float* __restr
     }
     if (fetch)
       xs = HW ? tex3D<float>(t.tr_tex[TL], pt.z + 0.5f, pt.y + 0.5f, pt.x + 0.5f) : tri_clamp_c<RT>(tb, pt + 0.5f);
-    sink(i, xv, xs, xh);
+    sink(i, u, xv, xs, xh);
   }
 }
 
@@ -317,7 +321,7 @@ __global__ void k_gather(Tables t, const float* __restrict__ stencil, const floa
   if (k >= n) return;
   Frame f = load_frame(frame + 12 * (size_t)k);
   float* d = desc + 576 * (size_t)k;
-  auto sink = [&](int i, float xv, float xs, float xh) {
+  auto sink = [&](int i, int, float xv, float xs, float xh) {
     d[i] = xv;
     d[192 + i] = xs;
     d[384 + i] = xh;
@@ -329,9 +333,10 @@ __global__ void k_gather(Tables t, const float* __restrict__ stencil, const floa
   ax[2] = srp.x; ax[3] = srp.y; ax[4] = srp.z;
 }
 
-// Gather for the compacted records, feature-major: feature i of record k at
-// desc[i*cap + k] (aux likewise), so that a warp's stores and the network's
-// loads of one feature are single coalesced transactions.
+// Gather for the compacted records in chunk-of-4 feature-major order:
+// features 4j..4j+3 of record k at desc[(j*cap + k)*4 .. +3] (aux: feature i at
+// aux[i*cap + k]). A warp's 16-byte stores and the network's 16-byte loads of
+// one chunk are contiguous 512-byte transactions.
 template <bool HW>
 __global__ void __launch_bounds__(128) k_gather_fm(Tables t, const float* __restrict__ stencil, Records rec,
                                                    int cap, F3 L, float alpha, float g, F3 srp,
@@ -341,12 +346,20 @@ __global__ void __launch_bounds__(128) k_gather_fm(Tables t, const float* __rest
   if (k >= n) return;
   F3 pos = f3(rec.pos[3 * (size_t)k], rec.pos[3 * (size_t)k + 1], rec.pos[3 * (size_t)k + 2]);
   Frame f = load_frame(rec.frame + 12 * (size_t)k);
-  float* d = desc + k;
+  // chunk-of-4 feature-major: features 4j..4j+3 of record k are the float4
+  // at desc[(j*cap + k)*4]; a warp's store of one chunk is 512 contiguous bytes
+  float4* d = reinterpret_cast<float4*>(desc) + k;
   const size_t c = (size_t)cap;
-  auto sink = [&](int i, float xv, float xs, float xh) {
-    d[i * c] = xv;
-    d[(192 + i) * c] = xs;
-    d[(384 + i) * c] = xh;
+  float4 bv, bs, bh;
+  auto sink = [&](int i, int u, float xv, float xs, float xh) {
+    (&bv.x)[u] = xv;
+    (&bs.x)[u] = xs;
+    (&bh.x)[u] = xh;
+    if (u == 3) {
+      d[(i >> 2) * c] = bv;
+      d[(48 + (i >> 2)) * c] = bs;
+      d[(96 + (i >> 2)) * c] = bh;
+    }
   };
   gather_fast<HW>(t, stencil, pos, L, f, alpha, g, sink);
   aux[k] = g;
@@ -356,10 +369,10 @@ __global__ void __launch_bounds__(128) k_gather_fm(Tables t, const float* __rest
   aux[4 * c + k] = srp.z;
 }
 
-int launch_mlp_tc(const Network* net, const float* desc, const float* aux, long long rs, long long fs,
+int launch_mlp_tc(const Network* net, const float* desc, const float* aux, long long rs, long long cs,
                   long long ars, long long afs, int n, float* out, const int* pix, const float* trph,
-                  const unsigned* count, F3 light_color, F3 scatter, cudaStream_t s);
-int launch_mlp_simt(const Network* net, const float* desc, const float* aux, long long rs, long long fs,
+                  const unsigned* count, F3 light_color, F3 scatter, float* spill, cudaStream_t s);
+int launch_mlp_simt(const Network* net, const float* desc, const float* aux, long long rs, long long cs,
                     long long ars, long long afs, int n, const unsigned* count, float* out, const int* pix,
                     const float* trph, F3 light_color, F3 scatter, cudaStream_t s);
 int mlp_tc_error(const Network* net, bool reset);
@@ -371,8 +384,14 @@ extern PathScene make_path_scene(const mr_render_params* p);
 constexpr size_t records_bytes(size_t n) { return n * (sizeof(int) + 16 * sizeof(float)) + 256; }
 constexpr size_t records_round(size_t n) { return (records_bytes(n) + 255) / 256 * 256; }
 // Scratch of one neural render of n pixels: records, then 576 feature-major
-// descriptor columns and 5 aux columns.
-constexpr size_t neural_scratch_bytes(size_t n) { return records_round(n) + n * (576 + 5) * sizeof(float) + 256; }
+// descriptor columns and 5 aux columns, then (when the albedo channels
+// differ) 120 spill columns of the tensor-core network's head input.
+constexpr size_t neural_scratch_bytes(size_t n, bool spill) {
+  return records_round(n) + n * (576 + 5 + (spill ? 120 : 0)) * sizeof(float) + 256;
+}
+static bool distinct_channels(const mr_render_params* p) {
+  return p->scatter_rate.x != p->scatter_rate.y || p->scatter_rate.x != p->scatter_rate.z;
+}
 
 static int neural_passes(Volume* v, const Network* net, const mr_render_params* p, float* dev_rgb, cudaStream_t s,
                          void* base, bool timed);
@@ -405,7 +424,7 @@ int render_neural(Volume* v, const Network* net, const mr_render_params* p, floa
     if (rc) return rc;
   }
   size_t npx = (size_t)p->width * p->height;
-  int rc = ensure_scratch(v, neural_scratch_bytes(npx), s);
+  int rc = ensure_scratch(v, neural_scratch_bytes(npx, distinct_channels(p)), s);
   if (rc) return rc;
   return neural_passes(v, net, p, dev_rgb, s, v->scratch, true);
 }
@@ -424,6 +443,7 @@ static int neural_passes(Volume* v, const Network* net, const mr_render_params* 
   Records rec = carve_records(base, npx);
   float* desc = (float*)((char*)base + rbytes);
   float* aux = desc + npx * 576;
+  float* spill = distinct_channels(p) ? aux + npx * 5 : nullptr;
   MR_CUDA(cudaMemsetAsync(v->d_counters, 0, kCounters * sizeof(unsigned long long), s));
   MR_CUDA(cudaMemsetAsync(rec.count, 0, sizeof(unsigned), s));
   NNTraceArgs ta;
@@ -461,10 +481,10 @@ static int neural_passes(Volume* v, const Network* net, const mr_render_params* 
   const long long cap = (long long)npx;
   mark(ST_NN_MLP);
   if (tc)
-    rc = launch_mlp_tc(net, desc, aux, 1, cap, 1, cap, (int)npx, dev_rgb, rec.pix, rec.trph, rec.count,
-                       to_f3(p->light_color), to_f3(p->scatter_rate), s);
+    rc = launch_mlp_tc(net, desc, aux, 4, 4 * cap, 1, cap, (int)npx, dev_rgb, rec.pix, rec.trph, rec.count,
+                       to_f3(p->light_color), to_f3(p->scatter_rate), spill, s);
   else
-    rc = launch_mlp_simt(net, desc, aux, 1, cap, 1, cap, (int)npx, rec.count, dev_rgb, rec.pix, rec.trph,
+    rc = launch_mlp_simt(net, desc, aux, 4, 4 * cap, 1, cap, (int)npx, rec.count, dev_rgb, rec.pix, rec.trph,
                          to_f3(p->light_color), to_f3(p->scatter_rate), s);
   mark(ST_NN_MLP);
   return rc;
@@ -499,11 +519,21 @@ extern "C" int mr_radiance_predict(const mr_network* nh, int32_t precision, cons
   if (!nh || !dev_desc || !dev_aux || !dev_out) return set_error(MR_ERR_ARG, "mr_radiance_predict: NULL argument");
   if (n < 0) return set_error(MR_ERR_ARG, "n < 0");
   if (n == 0) return MR_OK;
-  if (precision == MR_PREC_BF16)
-    return launch_mlp_tc(&nh->n, dev_desc, dev_aux, 576, 1, 5, 1, n, dev_out, nullptr, nullptr, nullptr, f3(1, 1, 1),
-                         f3(1, 1, 1), (cudaStream_t)stream);
+  if (reinterpret_cast<uintptr_t>(dev_desc) & 15)
+    return set_error(MR_ERR_ARG, "mr_radiance_predict: dev_desc must be 16-byte aligned");
+  if (precision == MR_PREC_BF16) {
+    // rows may carry distinct albedo channels: spill space for further heads
+    cudaStream_t s = (cudaStream_t)stream;
+    float* spill = nullptr;
+    cudaError_t e = cudaMallocAsync(&spill, (size_t)n * 120 * sizeof(float), s);
+    if (e != cudaSuccess) return set_error(MR_ERR_NOMEM, "spill allocation failed: %s", cudaGetErrorString(e));
+    int rc = launch_mlp_tc(&nh->n, dev_desc, dev_aux, 576, 4, 5, 1, n, dev_out, nullptr, nullptr, nullptr,
+                           f3(1, 1, 1), f3(1, 1, 1), spill, s);
+    MR_CUDA(cudaFreeAsync(spill, s));
+    return rc;
+  }
   if (precision != MR_PREC_FP32) return set_error(MR_ERR_UNSUPPORTED, "precision %d not built", precision);
-  return launch_mlp_simt(&nh->n, dev_desc, dev_aux, 576, 1, 5, 1, n, nullptr, dev_out, nullptr, nullptr, f3(1, 1, 1),
+  return launch_mlp_simt(&nh->n, dev_desc, dev_aux, 576, 4, 5, 1, n, nullptr, dev_out, nullptr, nullptr, f3(1, 1, 1),
                          f3(1, 1, 1), (cudaStream_t)stream);
 }
 
@@ -513,7 +543,7 @@ namespace mr {
 // Module-resident scratch for mr_render_neural_noalloc: records plus
 // descriptor columns of up to MR_NOALLOC_MAX_PIXELS pixels.
 constexpr size_t kNoallocBytes = (size_t)MR_NOALLOC_SCRATCH_MIB << 20;
-static_assert(neural_scratch_bytes(MR_NOALLOC_MAX_PIXELS) <= kNoallocBytes, "no-alloc scratch too small");
+static_assert(neural_scratch_bytes(MR_NOALLOC_MAX_PIXELS, true) <= kNoallocBytes, "no-alloc scratch too small");
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
 
 constexpr int kNoallocDevices = 64;
