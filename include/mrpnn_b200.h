@@ -201,6 +201,45 @@ int mr_network_check(const mr_network* net, int32_t reset);
 int mr_render_neural_noalloc(mr_volume* v, const mr_network* net, const mr_render_params* p, float* dev_rgb,
                              void* stream);
 
+/* ---- training (replaces dataGen.cu and the offline training of NNWeight.cuh) --- */
+
+typedef struct mr_trainer mr_trainer;
+
+/* MeanFreePathSample / GetDesiredCountSample (dataGen.cu:148-216): n_rays rays
+ * from the sphere of radius 0.5 towards the volume, up to four Woodcock
+ * vertices each (extinction scale alpha, HG g), jittered by up to 1/128 and
+ * paired with the primary or current ray direction as the reference does.
+ * Writes up to `cap` points (dev_pos, dev_dir: cap x 3) and their number. */
+int mr_train_points(mr_volume* v, float alpha, float g, uint32_t seed, int32_t n_rays, int32_t cap, float* dev_pos,
+                    float* dev_dir, int32_t* host_count, void* stream);
+/* GetSamples (core/volume.cu:550-626, core/render.cuh:276-315): training
+ * labels, the multiple-scattering radiance at each point along its view
+ * direction for light L (unit intensity), albedo and g, over `spp` paths of at
+ * most max_bounces vertices. Adds the FP64 radiance sums to dev_sum (n
+ * doubles, caller-zeroed); label = sum / spp. */
+int mr_train_labels(mr_volume* v, const float* dev_pos, const float* dev_dir, int32_t n, mr_float3 light_dir,
+                    float alpha, float g, float albedo, int32_t max_bounces, int32_t spp, uint32_t seed,
+                    double* dev_sum, void* stream);
+/* The random view / light frames NNPredict draws (core/render.cuh:355-369) for
+ * n view directions: dev_frame n x 12 (X, Y, Z, LX) for mr_gather_descriptors. */
+int mr_train_frames(const float* dev_dir, int32_t n, mr_float3 light_dir, uint32_t seed, float* dev_frame,
+                    void* stream);
+/* A trainer holds fp32 master weights (blob layout), Adam moments and a
+ * gradient buffer. The loss of a row is (X - log(1 + label / srp.x))^2, X the
+ * head output of the first albedo channel (the network predicts
+ * max(exp(X) - 1, 0) * srp); the step loss is its mean over the n rows.
+ * dev_desc n x 576 and dev_aux n x 5 as mr_gather_descriptors writes them. */
+int mr_trainer_create(const float* host_weights, size_t count, mr_trainer** out);
+int mr_trainer_destroy(mr_trainer* t);
+/* Gradient of the mean loss (MR_WEIGHT_TOTAL floats) without updating. */
+int mr_trainer_gradient(mr_trainer* t, const float* dev_desc, const float* dev_aux, const float* dev_label,
+                        int32_t n, float* host_grad, float* host_loss, void* stream);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8, bias-corrected) at rate lr;
+ * host_loss (optional) receives the batch loss before the update. */
+int mr_trainer_step(mr_trainer* t, const float* dev_desc, const float* dev_aux, const float* dev_label, int32_t n,
+                    float lr, float* host_loss, void* stream);
+int mr_trainer_weights(const mr_trainer* t, float* host_out, size_t count);
+
 /* Wait for `stream` with a watchdog: MR_ERR_TIMEOUT after timeout_ms. */
 int mr_sync(void* stream, int32_t timeout_ms);
 

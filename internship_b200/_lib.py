@@ -25,7 +25,8 @@ EXPORTS = [
     "mr_render_accumulate_f64", "mr_radiance_predict", "mr_gather_descriptors", "mr_sync",
     "mr_volume_counters", "mr_generate_cloud", "mr_cloud_permutation",
     "mr_volume_set_timing", "mr_volume_stage_times", "mr_tc_selftest", "mr_network_check",
-    "mr_render_neural_noalloc",
+    "mr_render_neural_noalloc", "mr_train_points", "mr_train_labels", "mr_train_frames", "mr_trainer_create",
+    "mr_trainer_destroy", "mr_trainer_gradient", "mr_trainer_step", "mr_trainer_weights",
 ]
 NOALLOC_MAX_PIXELS = 16384
 
@@ -98,6 +99,14 @@ def load():
     L.mr_tc_selftest.argtypes = [i32, i32, vp, vp, vp]
     L.mr_network_check.argtypes = [vp, i32]
     L.mr_render_neural_noalloc.argtypes = [vp, vp, C.POINTER(RenderParams), vp, vp]
+    L.mr_train_points.argtypes = [vp, fp, fp, u32, i32, i32, vp, vp, C.POINTER(i32), vp]
+    L.mr_train_labels.argtypes = [vp, vp, vp, i32, Float3, fp, fp, fp, i32, i32, u32, vp, vp]
+    L.mr_train_frames.argtypes = [vp, i32, Float3, u32, vp, vp]
+    L.mr_trainer_create.argtypes = [vp, sz, C.POINTER(vp)]
+    L.mr_trainer_destroy.argtypes = [vp]
+    L.mr_trainer_gradient.argtypes = [vp, vp, vp, vp, i32, vp, C.POINTER(fp), vp]
+    L.mr_trainer_step.argtypes = [vp, vp, vp, vp, i32, fp, C.POINTER(fp), vp]
+    L.mr_trainer_weights.argtypes = [vp, vp, sz]
     _lib = L
     return L
 

@@ -75,6 +75,23 @@ __device__ __forceinline__ float transmittance(const Medium& m, Rng& rng, F3 pos
   return tr;
 }
 
+// GetMatrixFromNormal (core/render.cuh:355-369), rejection capped at 64 tries.
+__device__ __forceinline__ void frame_from(Rng& rng, F3 v1, F3& a, F3& b, F3& c) {
+  v1 = normalize(v1);
+  for (int tries = 0; tries < 64; ++tries) {
+    float ex = rng.next();
+    float ey = rng.next();
+    F3 r = uniform_sphere(ex, ey);
+    if (fabsf(dot(r, v1)) < 0.01f) continue;
+    F3 v2 = normalize(cross(v1, r));
+    a = v1; b = v2; c = cross(v2, v1);
+    return;
+  }
+  F3 r = fabsf(v1.x) < 0.5f ? f3(1, 0, 0) : f3(0, 1, 0);
+  F3 v2 = normalize(cross(v1, r));
+  a = v1; b = v2; c = cross(v2, v1);
+}
+
 struct PathScene {
   F3 L;            // normalized light direction
   F3 light_color;

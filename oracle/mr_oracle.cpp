@@ -872,4 +872,83 @@ void orc_get_samples(const float* density, int res, float max_density, const flo
   }
 }
 
+
+// Training points (dataGen.cu:148-216 MeanFreePathSample on rays of
+// GetDesiredCountSample), in ray order: per ray the stream (seed; r, 0, .,
+// TAG_GEN), four draws for origin and direction, then per Woodcock vertex the
+// free-flight draws and six more (keep, jitter, 3 offsets, view). Returns the
+// number of points (<= cap written).
+int orc_train_points(const float* density, int res, float max_density, float alpha, float g, uint32_t seed,
+                     int n_rays, int cap, float* pos, float* dir) {
+  Vol vol{density, res, max_density, nullptr, nullptr, nullptr};
+  Scene sc{};
+  sc.alpha = alpha; sc.g = g; sc.tr_scale = 1.0f;
+  Tracker tk{vol, sc};
+  int count = 0;
+  for (int r = 0; r < n_rays; ++r) {
+    Rng rng(seed, (uint32_t)r, 0u, TAG_GEN);
+    float e0 = rng.next(), e1 = rng.next(), e2 = rng.next(), e3 = rng.next();
+    V3 ori = uniform_sphere(e0, e1) * 0.5f;
+    V3 d = normalize(uniform_sphere(e2, e3) + normalize(ori * -1.0f));
+    float dis = ray_box_offset(ori, d);
+    if (dis < 0) continue;
+    V3 sp = ori + d * dis, rd = d;
+    for (int i = 0; i < 4; ++i) {
+      float dd = ray_box_distance(sp, rd);
+      V3 np, nd;
+      if (!tk.next_vertex(rng, alpha, g, sp, rd, dd, np, nd)) break;
+      float uk = rng.next(), uj = rng.next(), jx = rng.next(), jy = rng.next(), jz = rng.next(), uv = rng.next();
+      V3 dv = sp - np;
+      if (i == 0 || dot(dv, dv) > 1.0f / 64.0f || uk > 0.9f) {
+        V3 p = np;
+        if (uj > 0.5f) p = p + v3(jx * 2.0f - 1.0f, jy * 2.0f - 1.0f, jz * 2.0f - 1.0f) * (1.0f / 128.0f);
+        V3 v = uv > 0.25f ? d : rd;
+        if (count < cap) {
+          pos[3 * count] = p.x; pos[3 * count + 1] = p.y; pos[3 * count + 2] = p.z;
+          dir[3 * count] = v.x; dir[3 * count + 1] = v.y; dir[3 * count + 2] = v.z;
+        }
+        ++count;
+      }
+      sp = np;
+      rd = nd;
+    }
+  }
+  return count;
+}
+
+// Frames of NNPredict for view directions (stream (seed; k, 1, ., TAG_MISC)).
+void orc_train_frames(const float* dir, int n, const float* light, uint32_t seed, float* frame) {
+  V3 L = normalize(v3(light[0], light[1], light[2]));
+  for (int k = 0; k < n; ++k) {
+    Rng rng(seed, (uint32_t)k, 1u, TAG_MISC);
+    V3 X, Y, Z, LX, ly, lz;
+    frame_from(rng, v3(dir[3 * k], dir[3 * k + 1], dir[3 * k + 2]), X, Y, Z);
+    frame_from(rng, L, LX, ly, lz);
+    float* f = frame + 12 * k;
+    f[0] = X.x; f[1] = X.y; f[2] = X.z; f[3] = Y.x; f[4] = Y.y; f[5] = Y.z;
+    f[6] = Z.x; f[7] = Z.y; f[8] = Z.z; f[9] = LX.x; f[10] = LX.y; f[11] = LX.z;
+  }
+}
+
+// Training loss of the network on n rows: mean of (X - log(1 + label/srp.x))^2,
+// X the head output (before exp) of the first albedo channel.
+double orc_train_loss(const float* weights, const float* desc, const float* aux, const float* label, int n) {
+  Net net(weights);
+  double loss = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : loss)
+  for (int k = 0; k < n; ++k) {
+    NetState s;
+    std::memcpy(s.xv, desc + 576 * k, 192 * sizeof(float));
+    std::memcpy(s.xs, desc + 576 * k + 192, 192 * sizeof(float));
+    std::memcpy(s.xh, desc + 576 * k + 384, 192 * sizeof(float));
+    const float* ax = aux + 5 * k;
+    trunks(s, net, ax[0], ax[1]);
+    float X = head(s, net, ax[2]);
+    float T = std::log1p(std::max(label[k], 0.0f) / ax[2]);
+    double e = (double)X - (double)T;
+    loss += e * e;
+  }
+  return loss / n;
+}
+
 }  // extern "C"

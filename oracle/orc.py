@@ -67,6 +67,12 @@ def lib():
         L.orc_predict.argtypes = [f32p, f32p, f32p, C.c_int, f32p]
         L.orc_get_samples.argtypes = [f32p, C.c_int, C.c_float, f32p, f32p, f32p, f32p, f32p,
                                       f32p, C.c_int, C.c_int, C.c_int, C.c_uint32, f64p, C.c_int]
+        L.orc_train_points.argtypes = [f32p, C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint32, C.c_int,
+                                       C.c_int, f32p, f32p]
+        L.orc_train_points.restype = C.c_int
+        L.orc_train_frames.argtypes = [f32p, C.c_int, f32p, C.c_uint32, f32p]
+        L.orc_train_loss.argtypes = [f32p, f32p, f32p, f32p, C.c_int]
+        L.orc_train_loss.restype = C.c_double
         _lib = L
     return _lib
 
@@ -180,3 +186,25 @@ def cloud(res, seed, octaves=6, base_freq=4.0, lacunarity=2.0, gain=0.5, thresho
     L.orc_cloud(res, permutation(seed).astype(np.int32), octaves, base_freq, lacunarity, gain, threshold, out,
                 nthreads())
     return out
+
+
+def train_points(density, max_density, alpha, g, seed, n_rays, cap):
+    density = _a(density)
+    res = round(density.size ** (1 / 3))
+    pos = np.zeros((cap, 3), np.float32)
+    dirs = np.zeros((cap, 3), np.float32)
+    n = lib().orc_train_points(density.ravel(), res, float(max_density), float(alpha), float(g), int(seed),
+                               int(n_rays), int(cap), pos.ravel(), dirs.ravel())
+    n = min(n, cap)
+    return pos[:n], dirs[:n]
+
+
+def train_frames(dirs, light, seed):
+    dirs = _a(dirs)
+    out = np.zeros((len(dirs), 12), np.float32)
+    lib().orc_train_frames(dirs.ravel(), len(dirs), _a(light), int(seed), out.ravel())
+    return out
+
+
+def train_loss(weights, desc, aux, label):
+    return float(lib().orc_train_loss(_a(weights), _a(desc).ravel(), _a(aux).ravel(), _a(label), len(label)))

@@ -243,3 +243,32 @@ def test_neural_render_matches_reference_statistically():
     tot_se = np.sqrt((ref_var / n_ref + var / K).sum()) / ref_mean.size
     assert abs(mean.mean() - ref_mean.mean()) < 4 * tot_se
     assert ref_mean.mean() > 0
+
+
+def test_oracle_training_points_frames_and_loss():
+    from internship_b200 import scenes
+    from internship_b200.weights import active_random_weights
+    dens = scenes.sphere_density(48)
+    md, _, _ = orc.build_mips(dens)
+    p1, d1 = orc.train_points(dens, md, 16.0, 0.857, 3, 1500, 10000)
+    p2, d2 = orc.train_points(dens, md, 16.0, 0.857, 3, 1500, 10000)
+    assert len(p1) > 100
+    np.testing.assert_array_equal(p1, p2)  # one stream per ray: deterministic
+    assert np.all(np.abs(p1) <= 0.5 + 1.0 / 128 + 1e-6)
+    # samples lie where the medium is: inside the sphere of radius 0.25 (+ jitter)
+    assert np.all(np.linalg.norm(p1, axis=1) < 0.25 + 0.02)
+    fr = orc.train_frames(d1[:50], np.array([0, 0, 1], np.float32), 1)
+    X, Y, Z = fr[:, 0:3], fr[:, 3:6], fr[:, 6:9]
+    np.testing.assert_allclose(X, d1[:50] / np.linalg.norm(d1[:50], axis=1, keepdims=True), atol=1e-6)
+    np.testing.assert_allclose(np.sum(X * Y, 1), 0, atol=1e-5)
+    np.testing.assert_allclose(np.cross(Y, X), Z, atol=1e-5)
+    rng = np.random.default_rng(0)
+    desc = rng.uniform(0, 1, (8, 576)).astype(np.float32)
+    aux = np.tile(np.array([0.85, 1.0, 0.9, 0.9, 0.9], np.float32), (8, 1))
+    w = active_random_weights(1)
+    out = orc.predict(w, desc, aux)
+    X0 = np.log1p(out[:, 0] / 0.9)
+    # loss against the network's own output is ~0; against shifted labels it is the shift squared
+    assert orc.train_loss(w, desc, aux, out[:, 0]) < 1e-9
+    lab = (np.expm1(X0 + 0.5) * 0.9).astype(np.float32)
+    assert orc.train_loss(w, desc, aux, lab) == pytest.approx(0.25, rel=1e-3)
