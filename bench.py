@@ -121,6 +121,107 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+TRAINED = os.path.join(ROOT, "internship_b200", "data", "mrpnn_trained.npy")
+
+
+def matched_rmse(v, p, sp, oracle_spp=16384, small=(480, 270)):
+    """Neural vs delta tracking at matched RMSE against an FP64-accumulated
+    `oracle_spp` delta-tracking image of the same view.
+
+    Errors are measured at `small` resolution (same camera; every pixel of it
+    covers 4 x 4 pixels of the 1080p frame) and converted into 1080p frames/s:
+    delta tracking is unbiased, so its RMSE at s spp is c / sqrt(s) with c
+    fitted over s = 1..64; the matched spp is s* = (c / RMSE_neural)^2 and the
+    delta-tracking frame rate at matched RMSE is 1 / (s* t1), t1 = the measured
+    time of one 1-spp 1080p delta-tracking frame. The neural form uses the
+    network trained by internship_b200.train (BF16 tensor cores, texture
+    sampler, one pass per frame)."""
+    import torch
+    import internship_b200 as mr
+    from internship_b200 import _lib
+    L = _lib.load()
+    if not os.path.exists(TRAINED):
+        return {"unavailable": "no trained weights at internship_b200/data/mrpnn_trained.npy"}
+    w_tr = np.load(TRAINED)
+    net = mr.Network(w_tr, mr.builtin_stencil())
+    W, H = small
+    q = _lib.RenderParams.from_buffer_copy(p)
+    q.width, q.height = W, H
+    npx = W * H * 3
+    # oracle: FP64 sums over oracle_spp samples (seed 1000, independent of the measured images)
+    s64 = torch.zeros(npx, device="cuda", dtype=torch.float64)
+    q.render_type, q.seed, q.spp = _lib.RT_PT, 1000, 256
+    torch.cuda.synchronize()
+    t0 = time.time()
+    for k in range(oracle_spp // 256):
+        q.sample_offset = 256 * k
+        _lib.check(L.mr_render_accumulate_f64(v.handle, C.byref(q), C.c_void_p(s64.data_ptr()), None, sp))
+    torch.cuda.synchronize()
+    t_oracle = time.time() - t0
+    oracle = (s64 / oracle_spp).float()
+    img = torch.empty(npx, device="cuda")
+
+    def rmse(x):
+        return float(torch.sqrt(torch.mean((x - oracle) ** 2)))
+
+    # delta tracking at s spp (seed 2000)
+    q.seed = 2000
+    dt = {}
+    for spp in (1, 4, 16, 64):
+        q.spp, q.sample_offset = spp, 0
+        _lib.check(L.mr_render(v.handle, None, C.byref(q), C.c_void_p(img.data_ptr()), sp))
+        torch.cuda.synchronize()
+        dt[spp] = rmse(img)
+    c = float(np.exp(np.mean([np.log(e * np.sqrt(s)) for s, e in dt.items()])))
+    # neural form, trained weights, one pass per frame; same LUT seed as the bench frames
+    q.render_type, q.spp, q.seed = _lib.RT_MRPNN, 1, p.seed
+    out = {}
+    for name, prec, smp in (("fp32_exact", _lib.PREC_FP32, _lib.SAMPLER_EXACT),
+                            ("bf16_exact", _lib.PREC_BF16, _lib.SAMPLER_EXACT),
+                            ("bf16_texture", _lib.PREC_BF16, _lib.SAMPLER_TEXTURE)):
+        q.precision, q.sampler = prec, smp
+        errs, imgs = [], []
+        for k in range(8):
+            q.sample_offset = 50 + k
+            _lib.check(L.mr_render(v.handle, net.handle, C.byref(q), C.c_void_p(img.data_ptr()), sp))
+            torch.cuda.synchronize()
+            errs.append(rmse(img))
+            imgs.append(img.clone())
+        out[name] = {"rmse_1pass": float(np.mean(errs)), "imgs": imgs}
+    ref32 = torch.stack(out["fp32_exact"]["imgs"])
+    for name in out:
+        x = torch.stack(out[name].pop("imgs"))
+        rel = torch.abs(x - ref32) / (torch.abs(ref32) + 1e-3)
+        out[name]["max_rel_vs_fp32"] = float(rel.max())
+        out[name]["rmse_vs_fp32"] = float(torch.sqrt(torch.mean((x - ref32) ** 2)))
+    # 1-spp delta tracking at 1080p
+    q.width, q.height = p.width, p.height
+    q.render_type, q.spp, q.seed = _lib.RT_PT, 1, 3000
+    full = torch.empty(p.width * p.height * 3, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for k in range(2):
+        q.sample_offset = k
+        _lib.check(L.mr_render(v.handle, None, C.byref(q), C.c_void_p(full.data_ptr()), sp))
+    reps = 5
+    e0.record()
+    for k in range(reps):
+        q.sample_offset = 10 + k
+        _lib.check(L.mr_render(v.handle, None, C.byref(q), C.c_void_p(full.data_ptr()), sp))
+    e1.record()
+    torch.cuda.synchronize()
+    t1 = e0.elapsed_time(e1) / reps / 1000.0
+    net.close()
+    e_nn = out["bf16_texture"]["rmse_1pass"]
+    s_star = (c / e_nn) ** 2
+    return {"oracle": {"spp": oracle_spp, "resolution": "%dx%d" % (W, H), "accumulation": "fp64",
+                       "seconds": t_oracle},
+            "dt_rmse_by_spp": {str(k): e for k, e in dt.items()}, "dt_rmse_coefficient": c,
+            "neural": out, "matched_spp": s_star, "dt_1080p_ms_per_spp": 1000 * t1,
+            "dt_1080p_samples_per_s": p.width * p.height / t1,
+            "dt_fps_at_matched_rmse": 1.0 / (s_star * t1),
+            "weights": "trained by internship_b200.train (config: 32 fBm clouds, 4096-spp FP64 labels)"}
+
+
 def cpu_baseline_sample(v, dens_dev, p, w, st):
     """Bounded sample of the same frame on the oracle (all host cores)."""
     from internship_b200 import _lib
@@ -146,6 +247,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-rmse", action="store_true", help="skip the matched-RMSE comparison")
     ap.add_argument("--frame", default=None,
                     help="WxH instead of 1920x1080: a smaller case for profiler captures, not a bench line")
     args = ap.parse_args()
@@ -315,6 +417,13 @@ def main():
             "active_pixels_per_frame": active,
             "density_fetches_per_frame": fetches,
             "variants": variants}
+    if not args.no_rmse:
+        m = matched_rmse(v, p, sp)
+        if "matched_spp" in m:
+            nn_fps = variants["bf16_texture"]["value"] / world
+            m["neural_fps"] = nn_fps
+            m["neural_over_dt_at_matched_rmse"] = nn_fps / m["dt_fps_at_matched_rmse"]
+        line["matched_rmse"] = m
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(v, dens, p, w, st)
     if rank == 0:

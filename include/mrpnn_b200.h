@@ -201,6 +201,45 @@ int mr_network_check(const mr_network* net, int32_t reset);
 int mr_render_neural_noalloc(mr_volume* v, const mr_network* net, const mr_render_params* p, float* dev_rgb,
                              void* stream);
 
+/* ---- interactive rendering (VolumeRender::Render(float3*, Histogram*, unsigned*, ...),
+ *      core/volume.cu:469-547, with RenderCamera / Denoise / ReprojectionDenoise
+ *      core/volume.cu:57-145,181-295) ------------------------------------------- */
+
+/* Histogram (core/volume.hpp:12-19): 10 bins per channel of x / (1 + x), the
+ * sample count, and running means of l^2 and l, l = sum over channels of
+ * x / (1 + x). In the neural mode the three scalars hold the previous
+ * frame's colour (the reference's reprojection history). */
+typedef struct {
+  float bin[30];
+  float total_samples;
+  float x2;
+  float x;
+} mr_histogram;
+
+/* Per-frame settings of the interactive path. */
+typedef struct {
+  mr_float3 prev_ori, prev_up, prev_right; /* camera of the previous frame (neural reprojection) */
+  int32_t frame_index;  /* randseed / frameNum: 0 restarts the accumulation; also the sample index */
+  int32_t checkerboard; /* SetCheckboard: delta tracking renders half the pixels per frame,
+                           alternating with frame_index parity */
+  int32_t tone;         /* 0 none, 1 gamma 2.2, 2 ACES */
+  int32_t denoise;      /* histogram-weighted 11 x 11 filter (delta tracking) */
+  float exposure;       /* SetExposure */
+} mr_interactive;
+
+/* One interactive frame. PT: one delta-tracking sample per (rendered) pixel
+ * blended into dev_accum (W*H*3 running mean) and the histograms (W*H), then
+ * Denoise into dev_bgra (W*H, 0xAARRGGBB). MRPNN: the neural render of this
+ * frame blended with the previous frame's colour at the reprojected pixel
+ * (dev_hist holds the history), then tone mapped and packed. Buffers are the
+ * caller's device memory; rows are top-first like mr_render. */
+int mr_render_interactive(mr_volume* v, const mr_network* net, const mr_render_params* p, const mr_interactive* it,
+                          float* dev_accum, mr_histogram* dev_hist, uint32_t* dev_bgra, void* stream);
+/* Denoise<denoise> (core/volume.cu:210-264) alone: filter, exposure, tone map
+ * and pack of an accumulated image and its histograms. */
+int mr_denoise(const float* dev_accum, const mr_histogram* dev_hist, uint32_t* dev_bgra, int32_t width,
+               int32_t height, const mr_interactive* it, void* stream);
+
 /* ---- training (replaces dataGen.cu and the offline training of NNWeight.cuh) --- */
 
 typedef struct mr_trainer mr_trainer;

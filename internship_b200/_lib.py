@@ -27,6 +27,7 @@ EXPORTS = [
     "mr_volume_set_timing", "mr_volume_stage_times", "mr_tc_selftest", "mr_network_check",
     "mr_render_neural_noalloc", "mr_train_points", "mr_train_labels", "mr_train_frames", "mr_trainer_create",
     "mr_trainer_destroy", "mr_trainer_gradient", "mr_trainer_step", "mr_trainer_weights",
+    "mr_render_interactive", "mr_denoise",
 ]
 NOALLOC_MAX_PIXELS = 16384
 
@@ -45,6 +46,20 @@ class RenderParams(C.Structure):
                 ("max_bounces", C.c_int32), ("spp", C.c_int32),
                 ("seed", C.c_uint32), ("sample_offset", C.c_uint32),
                 ("render_type", C.c_int32), ("precision", C.c_int32), ("sampler", C.c_int32)]
+
+
+class Histogram(C.Structure):
+    """mr_histogram (the reference's Histogram, core/volume.hpp:14-19)."""
+    _fields_ = [("bin", C.c_float * 30), ("total_samples", C.c_float), ("x2", C.c_float), ("x", C.c_float)]
+
+
+class Interactive(C.Structure):
+    """mr_interactive."""
+    _fields_ = [("prev_ori", Float3), ("prev_up", Float3), ("prev_right", Float3), ("frame_index", C.c_int32),
+                ("checkerboard", C.c_int32), ("tone", C.c_int32), ("denoise", C.c_int32), ("exposure", C.c_float)]
+
+
+TONE_NONE, TONE_GAMMA, TONE_ACES = 0, 1, 2
 
 
 class MRError(RuntimeError):
@@ -107,6 +122,8 @@ def load():
     L.mr_trainer_gradient.argtypes = [vp, vp, vp, vp, i32, vp, C.POINTER(fp), vp]
     L.mr_trainer_step.argtypes = [vp, vp, vp, vp, i32, fp, C.POINTER(fp), vp]
     L.mr_trainer_weights.argtypes = [vp, vp, sz]
+    L.mr_render_interactive.argtypes = [vp, vp, C.POINTER(RenderParams), C.POINTER(Interactive), vp, vp, vp, vp]
+    L.mr_denoise.argtypes = [vp, vp, vp, i32, i32, C.POINTER(Interactive), vp]
     _lib = L
     return L
 

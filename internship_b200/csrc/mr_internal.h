@@ -62,6 +62,9 @@ struct Volume {
   // Per-render scratch owned by the volume (grown on demand).
   void* scratch = nullptr;
   size_t scratch_bytes = 0;
+  // Interactive neural mode: radiance and first-hit distance of the frame.
+  void* inter = nullptr;
+  size_t inter_bytes = 0;
 };
 
 struct Network {

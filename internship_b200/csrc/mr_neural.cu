@@ -61,6 +61,7 @@ struct NNTraceArgs {
   CameraModel cam;
   uint32_t seed, frame_index;
   float* out;
+  float* dist;  // optional first-hit distance per pixel (< 0: escaped), interactive reprojection
   Records rec;
   unsigned long long* counters;
 };
@@ -102,6 +103,7 @@ __global__ void __launch_bounds__(128) k_nn_trace(NNTraceArgs a) {
     F3 ly, lz;
     frame_from(rng, dir, f.X, f.Y, f.Z);
     frame_from(rng, a.sc.L, f.LX, ly, lz);
+    if (a.dist) a.dist[pix] = active ? length(a.cam.ori - pos) : -1.0f;
     if (!active) {
       a.out[3 * (size_t)pix + 0] = fmaxf(a.sc.env.x, 0.0f);
       a.out[3 * (size_t)pix + 1] = fmaxf(a.sc.env.y, 0.0f);
@@ -377,7 +379,7 @@ static bool distinct_channels(const mr_render_params* p) {
 }
 
 static int neural_passes(Volume* v, const Network* net, const mr_render_params* p, float* dev_rgb, cudaStream_t s,
-                         void* base, bool timed);
+                         void* base, bool timed, float* dev_dist = nullptr);
 
 static Records carve_records(void* base, size_t n) {
   char* p = (char*)base;
@@ -390,7 +392,19 @@ static Records carve_records(void* base, size_t n) {
   return r;
 }
 
+static int render_neural_impl(Volume* v, const Network* net, const mr_render_params* p, float* dev_rgb,
+                              float* dev_dist, cudaStream_t s);
 int render_neural(Volume* v, const Network* net, const mr_render_params* p, float* dev_rgb, cudaStream_t s) {
+  return render_neural_impl(v, net, p, dev_rgb, nullptr, s);
+}
+// Same, also writing the first-hit distance of every pixel (interactive mode).
+int render_neural_dist(Volume* v, const Network* net, const mr_render_params* p, float* dev_rgb, float* dev_dist,
+                       cudaStream_t s) {
+  return render_neural_impl(v, net, p, dev_rgb, dev_dist, s);
+}
+
+static int render_neural_impl(Volume* v, const Network* net, const mr_render_params* p, float* dev_rgb,
+                              float* dev_dist, cudaStream_t s) {
   if (!net) return set_error(MR_ERR_ARG, "MRPNN render needs a network (mr_network_create)");
   if (!v->data_set) return set_error(MR_ERR_STATE, "render before mr_volume_set_data");
   if (!v->mips_valid) return set_error(MR_ERR_STATE, "render before mr_volume_update");
@@ -409,13 +423,13 @@ int render_neural(Volume* v, const Network* net, const mr_render_params* p, floa
   size_t npx = (size_t)p->width * p->height;
   int rc = ensure_scratch(v, neural_scratch_bytes(npx, distinct_channels(p)), s);
   if (rc) return rc;
-  return neural_passes(v, net, p, dev_rgb, s, v->scratch, true);
+  return neural_passes(v, net, p, dev_rgb, s, v->scratch, true, dev_dist);
 }
 
 // Trace, gather and network over scratch at `base` (neural_scratch_bytes of
 // width*height); `timed` = record stage events when the volume's timer is on.
 static int neural_passes(Volume* v, const Network* net, const mr_render_params* p, float* dev_rgb, cudaStream_t s,
-                         void* base, bool timed) {
+                         void* base, bool timed, float* dev_dist) {
   auto mark = [&](int st) { if (timed) v->timer.mark(st, s); };
   int rc = MR_OK;
   const F3 L = normalize(to_f3(p->light_dir));
@@ -436,6 +450,7 @@ static int neural_passes(Volume* v, const Network* net, const mr_render_params* 
   ta.seed = p->seed;
   ta.frame_index = p->sample_offset;
   ta.out = dev_rgb;
+  ta.dist = dev_dist;
   ta.rec = rec;
   ta.counters = v->d_counters;
   mark(ST_NN_TRACE);

@@ -344,6 +344,7 @@ int mr_volume_destroy(mr_volume* h) {
   cudaFree(v->d_max);
   cudaFree(v->d_counters);
   if (v->scratch) cudaFree(v->scratch);
+  if (v->inter) cudaFree(v->inter);
   destroy_textures(v);
   delete h;
   return MR_OK;

@@ -951,4 +951,129 @@ double orc_train_loss(const float* weights, const float* desc, const float* aux,
   return loss / n;
 }
 
+
+// ---- interactive path: histograms, Denoise, tone mapping (core/volume.cu:101-124,
+// 181-264; core/render.cuh:640-732) -------------------------------------------------
+static inline float lerp_f(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+
+// One frame's histogram / running-mean update from this frame's radiance
+// (RenderCamera<false>, core/volume.cu:101-124); hist is W*H x 33 floats.
+void orc_histogram_frame(const float* rad, int n, int fnum, float* accum, float* hist) {
+  const float rate = 1.0f / (float)(1 + fnum);
+  for (int p = 0; p < n; ++p) {
+    float* h = hist + 33 * p;
+    if (fnum == 0)
+      for (int i = 0; i < 33; ++i) h[i] = 0.0f;
+    float r[3];
+    for (int c = 0; c < 3; ++c) {
+      const float L = std::max(rad[3 * p + c], 0.0f);
+      accum[3 * p + c] = lerp_f(accum[3 * p + c], L, rate);
+      r[c] = L / (L + 1.0f);
+    }
+    h[30] += 1.0f;
+    for (int c = 0; c < 3; ++c) h[(int)std::floor(std::min(r[c], 0.999f) * 10) + 10 * c] += 1.0f;
+    const float l = r[0] + r[1] + r[2];
+    h[32] = lerp_f(h[32], l, rate);
+    h[31] = lerp_f(h[31], l * l, rate);
+  }
+}
+
+static float hist_compare(const float* x, const float* y) {
+  const float nx = x[30], ny = y[30];
+  const float syx = std::sqrt(ny / nx), sxy = std::sqrt(nx / ny);
+  float p = 0.0f, res = 0.0f;
+  for (int i = 0; i < 30; ++i) {
+    const float hx = x[i], hy = y[i];
+    if (hx != 0.0f || hy != 0.0f) {
+      p += 1.0f;
+      const float t = syx * hx - sxy * hy;
+      res += t * t / (hx + hy);
+    }
+  }
+  return p == 0.0f ? 0.0f : res / p;
+}
+
+static V3 mul3(const float* m, V3 x) {
+  return v3(m[0] * x.x + m[1] * x.y + m[2] * x.z, m[3] * x.x + m[4] * x.y + m[5] * x.z,
+            m[6] * x.x + m[7] * x.y + m[8] * x.z);
+}
+static V3 gamma22_h(V3 c) {
+  return v3(std::pow(std::max(c.x, 0.0f), 1.0f / 2.2f), std::pow(std::max(c.y, 0.0f), 1.0f / 2.2f),
+            std::pow(std::max(c.z, 0.0f), 1.0f / 2.2f));
+}
+static V3 aces_h(V3 c) {
+  static const float srgb_ap0[9] = {0.4397010f, 0.3829780f, 0.1773350f, 0.0897923f, 0.8134230f,
+                                    0.0967616f, 0.0175440f, 0.1115440f, 0.8707040f};
+  static const float ap0_ap1[9] = {1.4514393161f, -0.2365107469f, -0.2149285693f, -0.0765537734f, 1.1762296998f,
+                                   -0.0996759264f, 0.0083161484f, -0.0060324498f, 0.9977163014f};
+  static const float ap1_xyz[9] = {0.6624541811f, 0.1340042065f, 0.1561876870f, 0.2722287168f, 0.6740817658f,
+                                   0.0536895174f, -0.0055746495f, 0.0040607335f, 1.0103391003f};
+  static const float xyz_ap1[9] = {1.6410233797f, -0.3248032942f, -0.2364246952f, -0.6636628587f, 1.6153315917f,
+                                   0.0167563477f, 0.0117218943f, -0.0082844420f, 0.9883948585f};
+  static const float d60_d65[9] = {0.98722400f, -0.00611327f, 0.0159533f, -0.00759836f, 1.00186000f,
+                                   0.0053302f, 0.00307257f, -0.00509595f, 1.0816800f};
+  static const float xyz_709[9] = {3.2409699419f, -1.5373831776f, -0.4986107603f, -0.9692436363f, 1.8759675015f,
+                                   0.0415550574f, 0.0556300797f, -0.2039769589f, 1.0569715142f};
+  const V3 ap1_y = v3(0.272229f, 0.674082f, 0.0536895f);
+  V3 x = mul3(ap0_ap1, mul3(srgb_ap0, c));
+  float y = dot(x, ap1_y);
+  x = v3(y, y, y) * (1.0f - 0.96f) + x * 0.96f;
+  auto ts = [](float t) { return (t * (t * 278.5085f + 10.7772f)) / (t * (t * 293.6045f + 88.7122f) + 80.6889f); };
+  x = v3(ts(x.x), ts(x.y), ts(x.z));
+  V3 XYZ = mul3(ap1_xyz, x);
+  const float div = std::max(XYZ.x + XYZ.y + XYZ.z, 1e-4f);
+  const float cx = XYZ.x / div, cy = XYZ.y / div;
+  const float Y = std::pow(std::min(std::max(XYZ.y, 0.0f), 65504.0f), 0.9811f);
+  const float m = Y / std::max(cy, 1e-4f);
+  x = mul3(xyz_ap1, v3(cx * m, Y, (1.0f - cx - cy) * m));
+  y = dot(x, ap1_y);
+  x = v3(y, y, y) * (1.0f - 0.93f) + x * 0.93f;
+  return gamma22_h(mul3(xyz_709, mul3(d60_d65, mul3(ap1_xyz, x))));
+}
+static uint32_t pack_h(V3 res, float exposure, int tone) {
+  V3 v = res * exposure;
+  if (tone == 1) v = gamma22_h(v);
+  else if (tone == 2) v = aces_h(v);
+  auto q = [](float t) { return (uint32_t)(255.0f * std::min(std::max(t, 0.0f), 1.0f)); };
+  return 0xff000000u | (q(v.x) << 16) | (q(v.y) << 8) | q(v.z);
+}
+
+// Denoise<denoise> + tone map + pack (core/volume.cu:210-264), row-major.
+void orc_denoise(const float* accum, const float* hist, int W, int H, int frame, int flip, int tone, int denoise,
+                 float exposure, uint32_t* out) {
+  auto at = [&](int r, int c) {
+    r = std::min(std::max(r, 0), H - 1);
+    c = std::min(std::max(c, 0), W - 1);
+    return r * W + c;
+  };
+  auto col3 = [&](int q) { return v3(accum[3 * q], accum[3 * q + 1], accum[3 * q + 2]); };
+  for (int r = 0; r < H; ++r)
+    for (int c = 0; c < W; ++c) {
+      const int id = r * W + c;
+      V3 res;
+      if (frame == 0) {
+        if ((((r + flip) % 2) + c) % 2 == 0) res = col3(id);
+        else res = (col3(at(r - 1, c)) + col3(at(r + 1, c)) + col3(at(r, c - 1)) + col3(at(r, c + 1))) / 4.0f;
+      } else {
+        const float* h = hist + 33 * id;
+        const float variance = std::fabs(h[31] - h[32] * h[32]);
+        if (denoise && variance > 0.01f) {
+          res = v3(0, 0, 0);
+          float ws = 0.0f;
+          for (int i = -5; i <= 5; ++i)
+            for (int j = -5; j <= 5; ++j) {
+              const int t = at(r + i, c + j);
+              const float w = std::max(0.0f, 1.0f - 1.2f * hist_compare(h, hist + 33 * t));
+              res = res + col3(t) * w;
+              ws += w;
+            }
+          res = res / ws;
+        } else {
+          res = col3(id);
+        }
+      }
+      out[id] = pack_h(res, exposure, tone);
+    }
+}
+
 }  // extern "C"

@@ -73,6 +73,8 @@ def lib():
         L.orc_train_frames.argtypes = [f32p, C.c_int, f32p, C.c_uint32, f32p]
         L.orc_train_loss.argtypes = [f32p, f32p, f32p, f32p, C.c_int]
         L.orc_train_loss.restype = C.c_double
+        L.orc_histogram_frame.argtypes = [f32p, C.c_int, C.c_int, f32p, f32p]
+        L.orc_denoise.argtypes = [f32p, f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, u32p]
         _lib = L
     return _lib
 
@@ -208,3 +210,15 @@ def train_frames(dirs, light, seed):
 
 def train_loss(weights, desc, aux, label):
     return float(lib().orc_train_loss(_a(weights), _a(desc).ravel(), _a(aux).ravel(), _a(label), len(label)))
+
+
+def histogram_frame(rad, fnum, accum, hist):
+    """In-place per-frame update of accum (n x 3) and hist (n x 33) from rad (n x 3)."""
+    lib().orc_histogram_frame(_a(rad).ravel(), len(accum), int(fnum), accum.ravel(), hist.ravel())
+
+
+def denoise(accum, hist, W, H, frame, flip, tone, denoise, exposure):
+    out = np.zeros(W * H, np.uint32)
+    lib().orc_denoise(_a(accum).ravel(), _a(hist).ravel(), W, H, int(frame), int(flip), int(tone), int(denoise),
+                      float(exposure), out)
+    return out

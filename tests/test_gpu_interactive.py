@@ -1,0 +1,160 @@
+"""Interactive path on the GPU: histogram accumulation, the histogram
+denoiser with tone mapping / packing (against the oracle's restatement of
+Denoise), checkerboard rendering and the neural mode's reprojection."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import orc
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    assert t.cuda.is_available()
+    return t
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def _state(frame, tone=2, denoise=1, checker=0, exposure=1.0, prev=None):
+    from internship_b200 import _lib
+    it = _lib.Interactive()
+    if prev is not None:
+        it.prev_ori, it.prev_up, it.prev_right = prev.ori, prev.up, prev.right
+    it.frame_index, it.tone, it.denoise, it.checkerboard, it.exposure = frame, tone, denoise, checker, exposure
+    return it
+
+
+def _unpack(x):
+    x = np.asarray(x, np.uint32)
+    return np.stack([(x >> 16) & 255, (x >> 8) & 255, x & 255], -1).astype(np.int32)
+
+
+@pytest.mark.parametrize("tone,denoise,frame", [(2, 1, 7), (1, 1, 3), (0, 0, 5), (2, 1, 0), (1, 0, 0)])
+def test_denoise_matches_oracle(torch, tone, denoise, frame):
+    from internship_b200 import _lib
+    W, H = 45, 29  # ragged against the 16 x 16 tiles
+    rng = np.random.default_rng(tone * 10 + frame)
+    acc = np.zeros((W * H, 3), np.float32)
+    hist = np.zeros((W * H, 33), np.float32)
+    # a noisy image with smooth structure: exponential samples around a gradient
+    base = np.linspace(0.05, 2.0, W * H, dtype=np.float32)[:, None]
+    for f in range(max(frame, 1) + 1):
+        orc.histogram_frame((base * rng.exponential(1.0, (W * H, 3))).astype(np.float32), f, acc, hist)
+    ref = orc.denoise(acc, hist, W, H, frame, frame & 1, tone, denoise, 1.3)
+    da, dh = torch.from_numpy(acc).cuda(), torch.from_numpy(hist).cuda()
+    out = torch.empty(W * H, dtype=torch.int32, device="cuda")
+    it = _state(frame, tone, denoise, exposure=1.3)
+    _lib.check(_lib.load().mr_denoise(_ptr(da), _ptr(dh), _ptr(out), W, H, C.byref(it), None))
+    got = out.cpu().numpy().view(np.uint32)
+    assert np.all(got >> 24 == 255)
+    d = np.abs(_unpack(got) - _unpack(ref))
+    # pow / sqrt / division rounding: at most one 8-bit step, rarely
+    assert d.max() <= 1 and (d > 0).mean() < 0.01
+
+
+def _cloud_volume(res=64):
+    import internship_b200 as mr
+    from internship_b200 import scenes
+    dens = scenes.sphere_density(res)
+    v = mr.VolumeRender(res)
+    v.SetDatas(dens)
+    v.Update()
+    return v, dens
+
+
+def test_interactive_pt_accumulates_like_progressive_render(torch):
+    """K frames of the interactive path = the K-sample mean of the same
+    streams (sample index = frame index); every pixel's histogram holds K
+    samples per channel."""
+    from internship_b200 import _lib, scenes
+    v, dens = _cloud_volume()
+    W, H, K = 40, 24, 8
+    p = scenes.make_params(W, H, 1, bounces=64)
+    acc = torch.zeros(W * H * 3, device="cuda")
+    hist = torch.zeros(W * H * 33, device="cuda")
+    out = torch.empty(W * H, dtype=torch.int32, device="cuda")
+    for f in range(K):
+        it = _state(f, tone=2, denoise=1)
+        _lib.check(_lib.load().mr_render_interactive(v.handle, None, C.byref(p), C.byref(it), _ptr(acc), _ptr(hist),
+                                                     _ptr(out), None))
+    torch.cuda.synchronize()
+    a = acc.cpu().numpy()
+    h = hist.cpu().numpy().reshape(-1, 33)
+    assert np.all(h[:, 30] == K)
+    for c in range(3):
+        assert np.all(h[:, 10 * c:10 * c + 10].sum(1) == K)
+    p.spp = K
+    s, _, _ = orc.render_pt(dens, v.max_density, p)
+    ref = (s / K).astype(np.float32)
+    close = np.abs(a - ref) <= 1e-3 * (np.abs(ref) + 1e-3) + 1e-5
+    assert close.mean() > 0.9
+    assert abs(a.mean() - ref.mean()) < 0.01 * ref.mean() + 1e-6
+    v.close()
+
+
+def test_interactive_checkerboard_alternates(torch):
+    from internship_b200 import _lib, scenes
+    v, _ = _cloud_volume()
+    W, H = 33, 20
+    p = scenes.make_params(W, H, 1, bounces=32)
+    acc = torch.zeros(W * H * 3, device="cuda")
+    hist = torch.zeros(W * H * 33, device="cuda")
+    out = torch.empty(W * H, dtype=torch.int32, device="cuda")
+    for f in range(4):
+        it = _state(f, checker=1)
+        _lib.check(_lib.load().mr_render_interactive(v.handle, None, C.byref(p), C.byref(it), _ptr(acc), _ptr(hist),
+                                                     _ptr(out), None))
+    torch.cuda.synchronize()
+    h = hist.cpu().numpy().reshape(H, W, 33)
+    # every pixel is rendered on alternate frames: twice in four frames
+    assert np.all(h[..., 30] == 2)
+    v.close()
+
+
+def test_interactive_neural_reprojection_static_camera(torch):
+    """With an unmoved camera the reprojected pixel is the pixel itself. The
+    blend rate is 1 / (1 + n), capped at 0.2 where the ray hit the medium, and
+    the history starts cleared (ClearHis): frame 0 = 0.2 r0 (hit) or r0
+    (escaped); frame 1 = 0.8 frame0 + 0.2 r1 (hit) or 0.5 frame0 + 0.5 r1."""
+    import internship_b200 as mr
+    from internship_b200 import _lib, scenes
+    from internship_b200.weights import active_random_weights
+    v, _ = _cloud_volume()
+    v.SetWeights(active_random_weights(1), mr.builtin_stencil())
+    W, H = 32, 32
+    p = scenes.make_params(W, H, 1, rt=_lib.RT_MRPNN)
+    acc = torch.zeros(W * H * 3, device="cuda")
+    hist = torch.zeros(W * H * 33, device="cuda")
+    out = torch.empty(W * H, dtype=torch.int32, device="cuda")
+    frames = []
+    for f in range(2):
+        it = _state(f, tone=0, denoise=0, prev=p)
+        _lib.check(_lib.load().mr_render_interactive(v.handle, v.network.handle, C.byref(p), C.byref(it), _ptr(acc),
+                                                     _ptr(hist), _ptr(out), None))
+        torch.cuda.synchronize()
+        frames.append(acc.cpu().numpy().reshape(-1, 3).copy())
+    # this frame's radiance from the plain neural render with the same sample index
+    rad = []
+    for f in range(2):
+        p.sample_offset = f
+        img = np.zeros(W * H * 3, np.float32)
+        _lib.check(_lib.load().mr_render_host(v.handle, v.network.handle, C.byref(p), img.ctypes.data))
+        rad.append(img.reshape(-1, 3))
+    sky = np.all(rad[1] == 0, axis=1) & np.all(rad[0] == 0, axis=1)
+    exp0 = np.where(sky[:, None], rad[0], 0.2 * rad[0])
+    np.testing.assert_allclose(frames[0], exp0, rtol=1e-6, atol=1e-7)
+    exp = np.where(sky[:, None], 0.5 * exp0 + 0.5 * rad[1], 0.8 * exp0 + 0.2 * rad[1])
+    # jitter can move the reprojected point across a pixel edge for a few pixels
+    ok = np.all(np.abs(frames[1] - exp) <= 1e-4 * (np.abs(exp) + 1e-3), axis=1)
+    assert ok.mean() > 0.9
+    # history written back for the next frame
+    h = hist.cpu().numpy().reshape(-1, 33)
+    np.testing.assert_allclose(np.stack([h[:, 30], h[:, 32], h[:, 31]], 1), frames[1], rtol=0, atol=0)
+    v.close()
