@@ -240,6 +240,40 @@ int mr_render_interactive(mr_volume* v, const mr_network* net, const mr_render_p
 int mr_denoise(const float* dev_accum, const mr_histogram* dev_hist, uint32_t* dev_bgra, int32_t width,
                int32_t height, const mr_interactive* it, void* stream);
 
+/* ---- batched neural rendering (no reference counterpart: the reference renders
+ *      one volume and one view per call, core/volume.cu:410-467) ---------------- */
+
+typedef struct mr_batch mr_batch;
+
+/* A batch of (volume, view) jobs rendered together: the jobs' pixels are one
+ * flattened space processed in waves (one batched trace, gather and network
+ * launch per wave over all jobs' records). Every job is MR_RT_MRPNN; all
+ * share one precision and sampler; jobs on one volume must share its light,
+ * alpha, g and seed (each volume holds one set of tables). */
+int mr_batch_create(mr_batch** out);
+int mr_batch_destroy(mr_batch* b);
+/* Adds a job: p as for mr_render; dev_rgb = width*height*3 floats. Its
+ * sample index starts at p->sample_offset and advances by one per frame. */
+int mr_batch_add(mr_batch* b, mr_volume* v, const mr_render_params* p, float* dev_rgb);
+/* Builds the jobs' tables, uploads the job table and allocates the wave
+ * scratch (wave_pixels 0 = min(total, 4 Mi)). Must follow the last add. */
+int mr_batch_prepare(mr_batch* b, const mr_network* net, int64_t wave_pixels, void* stream);
+/* Times full frames over wave sizes 1/2/4 Mi pixels, then the trace and
+ * gather block sizes 64/128/256, keeps the fastest and reports them. The
+ * timed frames advance the jobs' sample indices. */
+int mr_batch_autotune(mr_batch* b, const mr_network* net, int64_t* host_wave, int32_t* host_trace_block,
+                      int32_t* host_gather_block, void* stream);
+/* Renders one frame of every job (stream-ordered launches). */
+int mr_batch_render(mr_batch* b, const mr_network* net, void* stream);
+/* Captures one frame of the batch into a CUDA graph on `stream` (not the
+ * legacy default stream); renders one eager frame first. */
+int mr_batch_capture(mr_batch* b, const mr_network* net, void* stream);
+/* Replays the captured graph: one more frame of every job. */
+int mr_batch_launch(mr_batch* b, void* stream);
+/* Counters of the frames since mr_batch_prepare's last reset: [0] density
+ * fetches, [2] loop-cap hits, [3] active pixels (of the last frame). */
+int mr_batch_counters(const mr_batch* b, uint64_t* host_out4);
+
 /* ---- training (replaces dataGen.cu and the offline training of NNWeight.cuh) --- */
 
 typedef struct mr_trainer mr_trainer;

@@ -27,7 +27,8 @@ EXPORTS = [
     "mr_volume_set_timing", "mr_volume_stage_times", "mr_tc_selftest", "mr_network_check",
     "mr_render_neural_noalloc", "mr_train_points", "mr_train_labels", "mr_train_frames", "mr_trainer_create",
     "mr_trainer_destroy", "mr_trainer_gradient", "mr_trainer_step", "mr_trainer_weights",
-    "mr_render_interactive", "mr_denoise",
+    "mr_render_interactive", "mr_denoise", "mr_batch_create", "mr_batch_destroy", "mr_batch_add", "mr_batch_prepare",
+    "mr_batch_autotune", "mr_batch_render", "mr_batch_capture", "mr_batch_launch", "mr_batch_counters",
 ]
 NOALLOC_MAX_PIXELS = 16384
 
@@ -124,6 +125,15 @@ def load():
     L.mr_trainer_weights.argtypes = [vp, vp, sz]
     L.mr_render_interactive.argtypes = [vp, vp, C.POINTER(RenderParams), C.POINTER(Interactive), vp, vp, vp, vp]
     L.mr_denoise.argtypes = [vp, vp, vp, i32, i32, C.POINTER(Interactive), vp]
+    L.mr_batch_create.argtypes = [C.POINTER(vp)]
+    L.mr_batch_destroy.argtypes = [vp]
+    L.mr_batch_add.argtypes = [vp, vp, C.POINTER(RenderParams), vp]
+    L.mr_batch_prepare.argtypes = [vp, vp, C.c_int64, vp]
+    L.mr_batch_autotune.argtypes = [vp, vp, C.POINTER(C.c_int64), C.POINTER(i32), C.POINTER(i32), vp]
+    L.mr_batch_render.argtypes = [vp, vp, vp]
+    L.mr_batch_capture.argtypes = [vp, vp, vp]
+    L.mr_batch_launch.argtypes = [vp, vp]
+    L.mr_batch_counters.argtypes = [vp, vp]
     _lib = L
     return L
 

@@ -76,6 +76,13 @@ struct Network {
   float h_stencil[MR_STENCIL_POINTS * 3];
 };
 
+// Output of one job of a batched neural render: its image, light colour and
+// per-channel albedo (the network kernels' compose step reads them per row).
+struct BatchOut {
+  float* out;
+  F3 light_color, scatter;
+};
+
 // Error reporting: thread-local message, returns the code.
 int set_error(int code, const char* fmt, ...);
 int cuda_error(cudaError_t e, const char* what);

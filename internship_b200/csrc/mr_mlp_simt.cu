@@ -29,6 +29,8 @@ struct SimtArgs {
   const int* __restrict__ pix;
   const float* __restrict__ trph;
   F3 light_color, scatter;
+  const int* job;        // batched compose: job of each record (null: single image)
+  const BatchOut* bout;  // batched compose: per-job outputs
 };
 
 __device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
@@ -348,9 +350,17 @@ __global__ void __launch_bounds__(kSimtThreads) k_mlp_simt(SimtArgs a) {
   if (a.pix) {
     const int px = a.pix[k];
     const float tr = a.trph[k];
-    a.out[3 * (size_t)px + 0] = fmaxf(((o[0] + tr) * a.light_color.x) * a.scatter.x, 0.0f);
-    a.out[3 * (size_t)px + 1] = fmaxf(((o[1] + tr) * a.light_color.y) * a.scatter.y, 0.0f);
-    a.out[3 * (size_t)px + 2] = fmaxf(((o[2] + tr) * a.light_color.z) * a.scatter.z, 0.0f);
+    F3 lc = a.light_color, sc = a.scatter;
+    float* dst = a.out;
+    if (a.job) {
+      const BatchOut& bo = a.bout[a.job[k]];
+      lc = bo.light_color;
+      sc = bo.scatter;
+      dst = bo.out;
+    }
+    dst[3 * (size_t)px + 0] = fmaxf(((o[0] + tr) * lc.x) * sc.x, 0.0f);
+    dst[3 * (size_t)px + 1] = fmaxf(((o[1] + tr) * lc.y) * sc.y, 0.0f);
+    dst[3 * (size_t)px + 2] = fmaxf(((o[2] + tr) * lc.z) * sc.z, 0.0f);
   } else {
 #pragma unroll
     for (int c = 0; c < 3; ++c) a.out[3 * (size_t)k + c] = o[c];
@@ -359,7 +369,8 @@ __global__ void __launch_bounds__(kSimtThreads) k_mlp_simt(SimtArgs a) {
 
 int launch_mlp_simt(const Network* net, const float* desc, const float* aux, long long rs, long long cs,
                     long long ars, long long afs, int n, const unsigned* count, float* out, const int* pix,
-                    const float* trph, F3 light_color, F3 scatter, cudaStream_t s) {
+                    const float* trph, F3 light_color, F3 scatter, cudaStream_t s, const int* job,
+                    const BatchOut* bout) {
   SimtArgs a;
   a.w = net->w;
   a.desc = desc;
@@ -375,6 +386,8 @@ int launch_mlp_simt(const Network* net, const float* desc, const float* aux, lon
   a.trph = trph;
   a.light_color = light_color;
   a.scatter = scatter;
+  a.job = job;
+  a.bout = bout;
   k_mlp_simt<<<(unsigned)((n + kSimtThreads - 1) / kSimtThreads), kSimtThreads, 0, s>>>(a);
   MR_CUDA(cudaGetLastError());
   return MR_OK;

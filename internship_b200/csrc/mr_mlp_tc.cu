@@ -259,6 +259,8 @@ struct TcArgs {
   const float* __restrict__ trph;     // compose mode: single-scatter term
   const unsigned* __restrict__ count; // compose mode: number of records (device)
   F3 light_color, scatter;
+  const int* __restrict__ job;        // batched compose: job of each record (null: single image)
+  const BatchOut* __restrict__ bout;  // batched compose: per-job outputs
   float* spill;                       // 120 x spill_cap ungated head columns (multi-channel tiles)
   long long spill_cap;
   int* err;                           // set on a wait timeout
@@ -797,10 +799,18 @@ __global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(const __grid_consta
       if (a.pix) {
         const int px = a.pix[row];
         const float tr = a.trph[row];
-        const float lc[3] = {a.light_color.x, a.light_color.y, a.light_color.z};
-        const float sc[3] = {a.scatter.x, a.scatter.y, a.scatter.z};
+        F3 lcv = a.light_color, scv = a.scatter;
+        float* dst = a.out;
+        if (a.job) {
+          const BatchOut& bo = a.bout[a.job[row]];
+          lcv = bo.light_color;
+          scv = bo.scatter;
+          dst = bo.out;
+        }
+        const float lc[3] = {lcv.x, lcv.y, lcv.z};
+        const float sc[3] = {scv.x, scv.y, scv.z};
 #pragma unroll
-        for (int ch = 0; ch < 3; ++ch) a.out[3 * (size_t)px + ch] = fmaxf(((o[ch] + tr) * lc[ch]) * sc[ch], 0.0f);
+        for (int ch = 0; ch < 3; ++ch) dst[3 * (size_t)px + ch] = fmaxf(((o[ch] + tr) * lc[ch]) * sc[ch], 0.0f);
       } else {
 #pragma unroll
         for (int ch = 0; ch < 3; ++ch) a.out[3 * (size_t)row + ch] = o[ch];
@@ -917,7 +927,8 @@ void free_packed(Network* n) {
 // error word. The error word lives after the packed image.
 int launch_mlp_tc(const Network* net, const float* desc, const float* aux, long long rs, long long cs,
                   long long ars, long long afs, int n, float* out, const int* pix, const float* trph,
-                  const unsigned* count, F3 light_color, F3 scatter, float* spill, cudaStream_t s) {
+                  const unsigned* count, F3 light_color, F3 scatter, float* spill, cudaStream_t s,
+                  const int* job, const BatchOut* bout) {
   if (cs * 4 > 0x7FFFFFFFll || n > (1 << 28))
     return set_error(MR_ERR_ARG, "tensor-core network: %d rows / chunk stride %lld out of range", n, cs);
   static bool attr = false;
@@ -943,6 +954,8 @@ int launch_mlp_tc(const Network* net, const float* desc, const float* aux, long 
   a.scatter = scatter;
   a.spill = spill;
   a.spill_cap = n;
+  a.job = job;
+  a.bout = bout;
   if (net->h_rowwise.size() != (size_t)kRowFloats) return set_error(MR_ERR_STATE, "network not packed");
   std::memcpy(a.rw, net->h_rowwise.data(), sizeof(a.rw));
   a.err = (int*)((uint8_t*)net->packed + kWBytes);

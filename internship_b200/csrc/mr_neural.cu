@@ -8,7 +8,9 @@
 //     gather (core/radiancePredict.cu:319-368) into feature-major columns.
 //  3. the network body: k_mlp_simt (fp32, mr_mlp_simt.cu) or k_mlp_tc
 //     (BF16 tcgen05, mr_mlp_tc.cu), which also writes the pixel.
+#include <algorithm>
 #include <mutex>
+#include <vector>
 
 #include "mr_internal.h"
 #include "mr_net_layout.cuh"
@@ -53,6 +55,7 @@ struct Records {
   float* frame;    // 12n: X, Y, Z, LX
   float* trph;     // n
   unsigned* count; // 1
+  int* job;        // n, batched renders only (null otherwise)
 };
 
 struct NNTraceArgs {
@@ -77,55 +80,57 @@ __device__ __forceinline__ unsigned claim_slot(unsigned* counter) {
   return base + __popc(mask & ((1u << lane) - 1u));
 }
 
-__global__ void __launch_bounds__(128) k_nn_trace(NNTraceArgs a) {
-  int pix = blockIdx.x * blockDim.x + threadIdx.x;
-  int npx = a.cam.width * a.cam.height;
-  TrackStats st{0, 0};
-  unsigned act = 0;
-  if (pix < npx) {
-    int row = pix / a.cam.width, col = pix - row * a.cam.width;
-    Rng rng;
-    rng.init(a.seed, (uint32_t)pix, a.frame_index, TAG_NN);
-    float jx = rng.next(), jy = rng.next();
-    F3 dir = camera_dir(a.cam, row, col, jx, jy);
-    // GetSamplePoint (core/render.cuh:174-198)
-    bool active = false;
-    F3 pos = f3(0, 0, 0);
-    float dis = ray_box_offset(a.cam.ori, dir);
-    if (dis >= 0) {
-      F3 sp = a.cam.ori + dir * dis;
-      float maxd = ray_box_distance(sp, dir);
-      F3 p0, p1;
-      active = next_vertex(a.m, rng, a.sc.alpha, 0.0f, sp, dir, maxd, p0, p1, st);
-      if (active) pos = p0;
-    }
-    Frame f;
-    F3 ly, lz;
-    frame_from(rng, dir, f.X, f.Y, f.Z);
-    frame_from(rng, a.sc.L, f.LX, ly, lz);
-    if (a.dist) a.dist[pix] = active ? length(a.cam.ori - pos) : -1.0f;
-    if (!active) {
-      a.out[3 * (size_t)pix + 0] = fmaxf(a.sc.env.x, 0.0f);
-      a.out[3 * (size_t)pix + 1] = fmaxf(a.sc.env.y, 0.0f);
-      a.out[3 * (size_t)pix + 2] = fmaxf(a.sc.env.z, 0.0f);
-    } else {
-      float d2 = ray_box_distance(pos, f.LX);
-      float ph = hg_phase(dot(f.X, f.LX), a.sc.g);
-      float tr = transmittance(a.m, rng, pos, f.LX, d2, a.sc.alpha, st) * ph;
-      unsigned k = claim_slot(a.rec.count);
-      a.rec.pix[k] = pix;
-      a.rec.pos[3 * (size_t)k + 0] = pos.x;
-      a.rec.pos[3 * (size_t)k + 1] = pos.y;
-      a.rec.pos[3 * (size_t)k + 2] = pos.z;
-      float* fr = a.rec.frame + 12 * (size_t)k;
-      fr[0] = f.X.x; fr[1] = f.X.y; fr[2] = f.X.z;
-      fr[3] = f.Y.x; fr[4] = f.Y.y; fr[5] = f.Y.z;
-      fr[6] = f.Z.x; fr[7] = f.Z.y; fr[8] = f.Z.z;
-      fr[9] = f.LX.x; fr[10] = f.LX.y; fr[11] = f.LX.z;
-      a.rec.trph[k] = tr;
-      act = 1;
-    }
+// One pixel of NNPredict's first half: returns 1 when the pixel became an
+// active record (job = its batch job, -1 for a single render).
+__device__ __forceinline__ unsigned trace_pixel(const Medium& m, const PathScene& sc, const CameraModel& cam,
+                                                uint32_t seed, uint32_t frame_index, int pix, float* out,
+                                                float* dist, const Records& rec, int job, TrackStats& st) {
+  int row = pix / cam.width, col = pix - row * cam.width;
+  Rng rng;
+  rng.init(seed, (uint32_t)pix, frame_index, TAG_NN);
+  float jx = rng.next(), jy = rng.next();
+  F3 dir = camera_dir(cam, row, col, jx, jy);
+  // GetSamplePoint (core/render.cuh:174-198)
+  bool active = false;
+  F3 pos = f3(0, 0, 0);
+  float dis = ray_box_offset(cam.ori, dir);
+  if (dis >= 0) {
+    F3 sp = cam.ori + dir * dis;
+    float maxd = ray_box_distance(sp, dir);
+    F3 p0, p1;
+    active = next_vertex(m, rng, sc.alpha, 0.0f, sp, dir, maxd, p0, p1, st);
+    if (active) pos = p0;
   }
+  Frame f;
+  F3 ly, lz;
+  frame_from(rng, dir, f.X, f.Y, f.Z);
+  frame_from(rng, sc.L, f.LX, ly, lz);
+  if (dist) dist[pix] = active ? length(cam.ori - pos) : -1.0f;
+  if (!active) {
+    out[3 * (size_t)pix + 0] = fmaxf(sc.env.x, 0.0f);
+    out[3 * (size_t)pix + 1] = fmaxf(sc.env.y, 0.0f);
+    out[3 * (size_t)pix + 2] = fmaxf(sc.env.z, 0.0f);
+    return 0;
+  }
+  float d2 = ray_box_distance(pos, f.LX);
+  float ph = hg_phase(dot(f.X, f.LX), sc.g);
+  float tr = transmittance(m, rng, pos, f.LX, d2, sc.alpha, st) * ph;
+  unsigned k = claim_slot(rec.count);
+  rec.pix[k] = pix;
+  if (rec.job) rec.job[k] = job;
+  rec.pos[3 * (size_t)k + 0] = pos.x;
+  rec.pos[3 * (size_t)k + 1] = pos.y;
+  rec.pos[3 * (size_t)k + 2] = pos.z;
+  float* fr = rec.frame + 12 * (size_t)k;
+  fr[0] = f.X.x; fr[1] = f.X.y; fr[2] = f.X.z;
+  fr[3] = f.Y.x; fr[4] = f.Y.y; fr[5] = f.Y.z;
+  fr[6] = f.Z.x; fr[7] = f.Z.y; fr[8] = f.Z.z;
+  fr[9] = f.LX.x; fr[10] = f.LX.y; fr[11] = f.LX.z;
+  rec.trph[k] = tr;
+  return 1;
+}
+
+__device__ __forceinline__ void trace_counters(unsigned long long* counters, const TrackStats& st, unsigned act) {
   unsigned fsum = st.fetches, csum = st.caps;
   for (int o = 16; o; o >>= 1) {
     fsum += __shfl_xor_sync(0xffffffffu, fsum, o);
@@ -133,10 +138,19 @@ __global__ void __launch_bounds__(128) k_nn_trace(NNTraceArgs a) {
     act += __shfl_xor_sync(0xffffffffu, act, o);
   }
   if ((threadIdx.x & 31) == 0) {
-    atomicAdd(a.counters + 0, (unsigned long long)fsum);
-    if (csum) atomicAdd(a.counters + 2, (unsigned long long)csum);
-    atomicAdd(a.counters + 3, (unsigned long long)act);
+    atomicAdd(counters + 0, (unsigned long long)fsum);
+    if (csum) atomicAdd(counters + 2, (unsigned long long)csum);
+    atomicAdd(counters + 3, (unsigned long long)act);
   }
+}
+
+__global__ void __launch_bounds__(128) k_nn_trace(NNTraceArgs a) {
+  int pix = blockIdx.x * blockDim.x + threadIdx.x;
+  int npx = a.cam.width * a.cam.height;
+  TrackStats st{0, 0};
+  unsigned act = 0;
+  if (pix < npx) act = trace_pixel(a.m, a.sc, a.cam, a.seed, a.frame_index, pix, a.out, a.dist, a.rec, -1, st);
+  trace_counters(a.counters, st, act);
 }
 
 inline __device__ Frame load_frame(const float* fr) {
@@ -356,10 +370,12 @@ __global__ void __launch_bounds__(128) k_gather_fm(Tables t, const float* __rest
 
 int launch_mlp_tc(const Network* net, const float* desc, const float* aux, long long rs, long long cs,
                   long long ars, long long afs, int n, float* out, const int* pix, const float* trph,
-                  const unsigned* count, F3 light_color, F3 scatter, float* spill, cudaStream_t s);
+                  const unsigned* count, F3 light_color, F3 scatter, float* spill, cudaStream_t s,
+                  const int* job = nullptr, const BatchOut* bout = nullptr);
 int launch_mlp_simt(const Network* net, const float* desc, const float* aux, long long rs, long long cs,
                     long long ars, long long afs, int n, const unsigned* count, float* out, const int* pix,
-                    const float* trph, F3 light_color, F3 scatter, cudaStream_t s);
+                    const float* trph, F3 light_color, F3 scatter, cudaStream_t s, const int* job = nullptr,
+                    const BatchOut* bout = nullptr);
 int mlp_tc_error(const Network* net, bool reset);
 
 extern int check_params(const mr_render_params* p);
@@ -384,6 +400,7 @@ static int neural_passes(Volume* v, const Network* net, const mr_render_params* 
 static Records carve_records(void* base, size_t n) {
   char* p = (char*)base;
   Records r;
+  r.job = nullptr;
   r.count = (unsigned*)p; p += 256;
   r.pix = (int*)p; p += n * sizeof(int);
   r.pos = (float*)p; p += 3 * n * sizeof(float);
@@ -595,4 +612,400 @@ extern "C" int mr_render_neural_noalloc(mr_volume* h, const mr_network* nh, cons
   rc = noalloc_scratch(&base);
   if (rc) return rc;
   return neural_passes(v, &nh->n, p, dev_rgb, (cudaStream_t)stream, base, false);
+}
+
+// ---- batched neural render ------------------------------------------------------------
+// Many (volume, view) jobs rendered together: the jobs' pixels form one
+// flattened space, processed in waves of `wave` pixels; each wave is one
+// batched trace, one batched gather and one network launch over the records
+// of all jobs in it. Every launch of a batch frame can be captured into one
+// CUDA graph; the graph ends with a kernel that advances the jobs' sample
+// indices, so each replay renders the next frame.
+
+namespace mr {
+
+struct BatchJob {
+  Medium m;
+  PathScene sc;
+  CameraModel cam;
+  uint32_t seed, frame;
+  Tables tabs;      // the job's volume tables (and texture objects for the texture sampler)
+  F3 srp;           // (albedo / 1.001)^4
+  long long pix0;   // first pixel of the job in the flattened pixel space
+  int npx;
+};
+
+__global__ void __launch_bounds__(256) k_trace_batch(const BatchJob* __restrict__ jobs, int njobs, long long w0,
+                                                     long long w1, const BatchOut* __restrict__ bout, Records rec,
+                                                     unsigned long long* counters) {
+  const long long p = w0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  TrackStats st{0, 0};
+  unsigned act = 0;
+  if (p < w1) {
+    int lo = 0, hi = njobs - 1;  // last job with pix0 <= p
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (jobs[mid].pix0 <= p) lo = mid;
+      else hi = mid - 1;
+    }
+    const BatchJob& j = jobs[lo];
+    act = trace_pixel(j.m, j.sc, j.cam, j.seed, j.frame, (int)(p - j.pix0), bout[lo].out, nullptr, rec, lo, st);
+  }
+  trace_counters(counters, st, act);
+}
+
+template <bool HW>
+__global__ void __launch_bounds__(256) k_gather_batch(const BatchJob* __restrict__ jobs,
+                                                      const float* __restrict__ stencil, Records rec, int cap,
+                                                      float* __restrict__ desc, float* __restrict__ aux) {
+  const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned n = min(*rec.count, (unsigned)cap);
+  if (k >= n) return;
+  const BatchJob& j = jobs[rec.job[k]];
+  const F3 pos = f3(rec.pos[3 * (size_t)k], rec.pos[3 * (size_t)k + 1], rec.pos[3 * (size_t)k + 2]);
+  const Frame f = load_frame(rec.frame + 12 * (size_t)k);
+  float4* d = reinterpret_cast<float4*>(desc) + k;
+  const size_t c = (size_t)cap;
+  float4 bv, bs, bh;
+  auto sink = [&](int i, int u, float xv, float xs, float xh) {
+    (&bv.x)[u] = xv;
+    (&bs.x)[u] = xs;
+    (&bh.x)[u] = xh;
+    if (u == 3) {
+      d[(i >> 2) * c] = bv;
+      d[(48 + (i >> 2)) * c] = bs;
+      d[(96 + (i >> 2)) * c] = bh;
+    }
+  };
+  gather_fast<HW>(j.tabs, stencil, pos, j.sc.L, f, j.sc.alpha, j.sc.g, sink);
+  aux[k] = j.sc.g;
+  aux[c + k] = acosf(dot(f.X, f.LX));
+  aux[2 * c + k] = j.srp.x;
+  aux[3 * c + k] = j.srp.y;
+  aux[4 * c + k] = j.srp.z;
+}
+
+__global__ void k_batch_advance(BatchJob* jobs, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) jobs[i].frame += 1u;
+}
+
+struct Batch {
+  struct HostJob {
+    Volume* v;
+    mr_render_params p;
+    float* out;
+  };
+  std::vector<HostJob> jobs;
+  BatchJob* d_jobs = nullptr;
+  BatchOut* d_out = nullptr;
+  unsigned long long* counters = nullptr;
+  void* scratch = nullptr;
+  size_t scratch_bytes = 0;
+  long long total = 0, wave = 0;
+  int trace_block = 128, gather_block = 128;
+  int precision = MR_PREC_BF16, sampler = MR_SAMPLER_EXACT;
+  bool spill = false, prepared = false;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+
+  void drop_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+  }
+  void release() {
+    drop_graph();
+    if (d_jobs) cudaFree(d_jobs);
+    if (d_out) cudaFree(d_out);
+    if (counters) cudaFree(counters);
+    if (scratch) cudaFree(scratch);
+    d_jobs = nullptr;
+    d_out = nullptr;
+    counters = nullptr;
+    scratch = nullptr;
+    scratch_bytes = 0;
+    prepared = false;
+  }
+};
+
+static size_t batch_scratch_bytes(long long wave, bool spill) {
+  return neural_scratch_bytes((size_t)wave, spill) + ((size_t)wave * sizeof(int) + 255) / 256 * 256;
+}
+
+// Stream-ordered launches of one batch frame (eager or under capture).
+static int batch_launches(Batch& b, const Network* net, cudaStream_t s) {
+  const size_t cap = (size_t)b.wave;
+  const size_t rbytes = records_round(cap);
+  Records rec = carve_records(b.scratch, cap);
+  float* desc = (float*)((char*)b.scratch + rbytes);
+  float* aux = desc + cap * 576;
+  float* spill = b.spill ? aux + cap * 5 : nullptr;
+  rec.job = (int*)((char*)b.scratch + neural_scratch_bytes(cap, b.spill));
+  const bool tc = b.precision == MR_PREC_BF16;
+  const bool hw = b.sampler == MR_SAMPLER_TEXTURE;
+  const int nj = (int)b.jobs.size();
+  MR_CUDA(cudaMemsetAsync(b.counters, 0, kCounters * sizeof(unsigned long long), s));
+  for (long long w0 = 0; w0 < b.total; w0 += b.wave) {
+    const long long w1 = std::min(b.total, w0 + b.wave);
+    MR_CUDA(cudaMemsetAsync(rec.count, 0, sizeof(unsigned), s));
+    const unsigned tgrid = (unsigned)((w1 - w0 + b.trace_block - 1) / b.trace_block);
+    k_trace_batch<<<tgrid, b.trace_block, 0, s>>>(b.d_jobs, nj, w0, w1, b.d_out, rec, b.counters);
+    MR_CUDA(cudaGetLastError());
+    const unsigned ggrid = (unsigned)((w1 - w0 + b.gather_block - 1) / b.gather_block);
+    if (hw)
+      k_gather_batch<true><<<ggrid, b.gather_block, 0, s>>>(b.d_jobs, net->stencil, rec, (int)cap, desc, aux);
+    else
+      k_gather_batch<false><<<ggrid, b.gather_block, 0, s>>>(b.d_jobs, net->stencil, rec, (int)cap, desc, aux);
+    MR_CUDA(cudaGetLastError());
+    const long long ccap = (long long)cap;
+    int rc;
+    if (tc)
+      rc = launch_mlp_tc(net, desc, aux, 4, 4 * ccap, 1, ccap, (int)cap, nullptr, rec.pix, rec.trph, rec.count,
+                         f3(1, 1, 1), f3(1, 1, 1), spill, s, rec.job, b.d_out);
+    else
+      rc = launch_mlp_simt(net, desc, aux, 4, 4 * ccap, 1, ccap, (int)cap, rec.count, nullptr, rec.pix, rec.trph,
+                           f3(1, 1, 1), f3(1, 1, 1), s, rec.job, b.d_out);
+    if (rc) return rc;
+  }
+  k_batch_advance<<<(nj + 127) / 128, 128, 0, s>>>(b.d_jobs, nj);
+  MR_CUDA(cudaGetLastError());
+  return MR_OK;
+}
+
+static int batch_alloc_scratch(Batch& b, long long wave) {
+  const size_t need = batch_scratch_bytes(wave, b.spill);
+  if (b.scratch_bytes >= need) return MR_OK;
+  if (b.scratch) MR_CUDA(cudaFree(b.scratch));
+  b.scratch = nullptr;
+  b.scratch_bytes = 0;
+  cudaError_t e = cudaMalloc(&b.scratch, need);
+  if (e != cudaSuccess) return set_error(MR_ERR_NOMEM, "batch scratch of %zu bytes: %s", need, cudaGetErrorString(e));
+  b.scratch_bytes = need;
+  return MR_OK;
+}
+
+}  // namespace mr
+
+struct mr_batch { mr::Batch b; };
+
+extern "C" int mr_batch_create(mr_batch** out) {
+  clear_error();
+  if (!out) return set_error(MR_ERR_ARG, "mr_batch_create: NULL argument");
+  *out = new mr_batch();
+  return MR_OK;
+}
+
+extern "C" int mr_batch_destroy(mr_batch* h) {
+  if (!h) return MR_OK;
+  h->b.release();
+  delete h;
+  return MR_OK;
+}
+
+extern "C" int mr_batch_add(mr_batch* h, mr_volume* v, const mr_render_params* p, float* dev_rgb) {
+  clear_error();
+  if (!h || !v || !p || !dev_rgb) return set_error(MR_ERR_ARG, "mr_batch_add: NULL argument");
+  int rc = check_params(p);
+  if (rc) return rc;
+  if (p->render_type != MR_RT_MRPNN) return set_error(MR_ERR_ARG, "batched renders are neural (MR_RT_MRPNN)");
+  if (!v->v.data_set || !v->v.mips_valid) return set_error(MR_ERR_STATE, "volume needs mr_volume_set_data / _update");
+  Batch& b = h->b;
+  if (!b.jobs.empty() && (p->precision != b.jobs[0].p.precision || p->sampler != b.jobs[0].p.sampler))
+    return set_error(MR_ERR_ARG, "all jobs of a batch share one precision and sampler");
+  b.jobs.push_back({&v->v, *p, dev_rgb});
+  b.prepared = false;
+  b.drop_graph();
+  return MR_OK;
+}
+
+extern "C" int mr_batch_prepare(mr_batch* h, const mr_network* nh, int64_t wave_pixels, void* stream) {
+  clear_error();
+  if (!h || !nh) return set_error(MR_ERR_ARG, "mr_batch_prepare: NULL argument");
+  Batch& b = h->b;
+  if (b.jobs.empty()) return set_error(MR_ERR_STATE, "empty batch");
+  if (wave_pixels < 0) return set_error(MR_ERR_ARG, "wave_pixels < 0");
+  cudaStream_t s = (cudaStream_t)stream;
+  b.drop_graph();
+  b.precision = b.jobs[0].p.precision;
+  b.sampler = b.jobs[0].p.sampler;
+  if (b.precision != MR_PREC_FP32 && b.precision != MR_PREC_BF16)
+    return set_error(MR_ERR_UNSUPPORTED, "precision %d not built", b.precision);
+  std::vector<BatchJob> hj(b.jobs.size());
+  std::vector<BatchOut> ho(b.jobs.size());
+  long long off = 0;
+  b.spill = false;
+  for (size_t i = 0; i < b.jobs.size(); ++i) {
+    Batch::HostJob& J = b.jobs[i];
+    Volume* v = J.v;
+    const mr_render_params* p = &J.p;
+    const F3 L = normalize(to_f3(p->light_dir));
+    // a volume's tables serve one (g, seed) and one (light, alpha): the first
+    // job on a volume builds them, later jobs must agree
+    bool first = true;
+    for (size_t k = 0; k < i; ++k) first = first && b.jobs[k].v != v;
+    const bool lut_ok = v->lut_valid && v->lut_g == p->g && v->lut_seed == p->seed;
+    const bool tr_ok = v->tr_valid && L.x == v->tr_light.x && L.y == v->tr_light.y && L.z == v->tr_light.z &&
+                       p->alpha == v->tr_alpha;
+    if (!first && (!lut_ok || !tr_ok))
+      return set_error(MR_ERR_ARG, "job %zu: shares a volume with an earlier job but needs other light/alpha/g "
+                                   "tables; give it its own volume", i);
+    if (!lut_ok) {
+      int rc = launch_update_lut(v, p->g, p->seed, s);
+      if (rc) return rc;
+    }
+    if (!tr_ok) {
+      int rc = launch_update_tr(v, L, p->alpha, s);
+      if (rc) return rc;
+    }
+    if (b.sampler == MR_SAMPLER_TEXTURE) {
+      int rc = refresh_textures(v, s);
+      if (rc) return rc;
+    }
+    BatchJob& j = hj[i];
+    j.m = Medium{v->density, v->res, v->max_density, p->tr_scale};
+    j.sc = make_path_scene(p);
+    j.cam = make_camera(p);
+    j.seed = p->seed;
+    j.frame = p->sample_offset;
+    j.tabs = Tables{v->mips, v->tr, v->lut, {}, {}, 0};
+    for (int k = 0; k < 9; ++k) j.tabs.mip_tex[k] = v->mip_tex[k];
+    for (int k = 0; k < 8; ++k) j.tabs.tr_tex[k] = v->tr_tex[k];
+    j.tabs.lut_tex = v->lut_tex;
+    j.srp = srp_of(to_f3(p->scatter_rate) / 1.001f);
+    j.pix0 = off;
+    j.npx = p->width * p->height;
+    off += j.npx;
+    ho[i] = BatchOut{J.out, to_f3(p->light_color), to_f3(p->scatter_rate)};
+    if (distinct_channels(p)) b.spill = true;
+  }
+  b.total = off;
+  b.wave = wave_pixels > 0 ? std::min<long long>(wave_pixels, b.total) : std::min<long long>(b.total, 4ll << 20);
+  if (b.wave > (1ll << 28)) return set_error(MR_ERR_ARG, "wave of %lld pixels too large", b.wave);
+  if (b.d_jobs) cudaFree(b.d_jobs);
+  if (b.d_out) cudaFree(b.d_out);
+  b.d_jobs = nullptr;
+  b.d_out = nullptr;
+  MR_CUDA(cudaMalloc(&b.d_jobs, hj.size() * sizeof(BatchJob)));
+  MR_CUDA(cudaMalloc(&b.d_out, ho.size() * sizeof(BatchOut)));
+  if (!b.counters) MR_CUDA(cudaMalloc(&b.counters, kCounters * sizeof(unsigned long long)));
+  MR_CUDA(cudaMemcpyAsync(b.d_jobs, hj.data(), hj.size() * sizeof(BatchJob), cudaMemcpyHostToDevice, s));
+  MR_CUDA(cudaMemcpyAsync(b.d_out, ho.data(), ho.size() * sizeof(BatchOut), cudaMemcpyHostToDevice, s));
+  int rc = batch_alloc_scratch(b, b.wave);
+  if (rc) return rc;
+  MR_CUDA(cudaStreamSynchronize(s));
+  b.prepared = true;
+  return MR_OK;
+}
+
+extern "C" int mr_batch_render(mr_batch* h, const mr_network* nh, void* stream) {
+  clear_error();
+  if (!h || !nh) return set_error(MR_ERR_ARG, "mr_batch_render: NULL argument");
+  if (!h->b.prepared) return set_error(MR_ERR_STATE, "mr_batch_prepare first");
+  return batch_launches(h->b, &nh->n, (cudaStream_t)stream);
+}
+
+extern "C" int mr_batch_autotune(mr_batch* h, const mr_network* nh, int64_t* host_wave, int32_t* host_trace_block,
+                                 int32_t* host_gather_block, void* stream) {
+  clear_error();
+  if (!h || !nh) return set_error(MR_ERR_ARG, "mr_batch_autotune: NULL argument");
+  Batch& b = h->b;
+  if (!b.prepared) return set_error(MR_ERR_STATE, "mr_batch_prepare first");
+  cudaStream_t s = (cudaStream_t)stream;
+  b.drop_graph();
+  cudaEvent_t e0, e1;
+  MR_CUDA(cudaEventCreate(&e0));
+  MR_CUDA(cudaEventCreate(&e1));
+  auto timed = [&](float* ms) -> int {
+    MR_CUDA(cudaEventRecord(e0, s));
+    int rc = batch_launches(b, &nh->n, s);
+    if (rc) return rc;
+    MR_CUDA(cudaEventRecord(e1, s));
+    MR_CUDA(cudaEventSynchronize(e1));
+    MR_CUDA(cudaEventElapsedTime(ms, e0, e1));
+    return MR_OK;
+  };
+  int rc = MR_OK;
+  float best = 1e30f, ms = 0;
+  // wave size first (default blocks), then the trace and gather block sizes
+  const long long waves[] = {1ll << 20, 2ll << 20, 4ll << 20};
+  long long best_wave = b.wave;
+  for (long long w : waves) {
+    const long long ww = std::min(w, b.total);
+    if ((rc = batch_alloc_scratch(b, ww))) break;
+    b.wave = ww;
+    if ((rc = timed(&ms)) || (rc = timed(&ms))) break;
+    if (ms < best) { best = ms; best_wave = ww; }
+    if (ww == b.total) break;
+  }
+  b.wave = best_wave;
+  const int blocks[] = {64, 128, 256};
+  for (int pass = 0; pass < 2 && !rc; ++pass) {
+    int* knob = pass == 0 ? &b.trace_block : &b.gather_block;
+    int best_blk = *knob;
+    best = 1e30f;
+    for (int blk : blocks) {
+      *knob = blk;
+      if ((rc = timed(&ms)) || (rc = timed(&ms))) break;
+      if (ms < best) { best = ms; best_blk = blk; }
+    }
+    *knob = best_blk;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  if (host_wave) *host_wave = b.wave;
+  if (host_trace_block) *host_trace_block = b.trace_block;
+  if (host_gather_block) *host_gather_block = b.gather_block;
+  return MR_OK;
+}
+
+extern "C" int mr_batch_capture(mr_batch* h, const mr_network* nh, void* stream) {
+  clear_error();
+  if (!h || !nh) return set_error(MR_ERR_ARG, "mr_batch_capture: NULL argument");
+  Batch& b = h->b;
+  if (!b.prepared) return set_error(MR_ERR_STATE, "mr_batch_prepare first");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (s == nullptr) return set_error(MR_ERR_ARG, "graph capture needs a non-default stream");
+  b.drop_graph();
+  // one eager frame first: loads the modules and sets kernel attributes
+  // outside the capture
+  int rc = batch_launches(b, &nh->n, s);
+  if (rc) return rc;
+  MR_CUDA(cudaStreamSynchronize(s));
+  MR_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  rc = batch_launches(b, &nh->n, s);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(s, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return cuda_error(e, "cudaStreamEndCapture");
+  b.graph = g;
+  e = cudaGraphInstantiate(&b.exec, g, 0);
+  if (e != cudaSuccess) {
+    b.drop_graph();
+    return cuda_error(e, "cudaGraphInstantiate");
+  }
+  return MR_OK;
+}
+
+extern "C" int mr_batch_launch(mr_batch* h, void* stream) {
+  clear_error();
+  if (!h) return set_error(MR_ERR_ARG, "mr_batch_launch: NULL argument");
+  if (!h->b.exec) return set_error(MR_ERR_STATE, "mr_batch_capture first");
+  MR_CUDA(cudaGraphLaunch(h->b.exec, (cudaStream_t)stream));
+  return MR_OK;
+}
+
+extern "C" int mr_batch_counters(const mr_batch* h, uint64_t* host_out4) {
+  clear_error();
+  if (!h || !host_out4) return set_error(MR_ERR_ARG, "mr_batch_counters: NULL argument");
+  if (!h->b.counters) return set_error(MR_ERR_STATE, "mr_batch_prepare first");
+  unsigned long long c[kCounters];
+  MR_CUDA(cudaMemcpy(c, h->b.counters, sizeof(c), cudaMemcpyDeviceToHost));
+  for (int i = 0; i < 4; ++i) host_out4[i] = c[i];
+  return MR_OK;
 }

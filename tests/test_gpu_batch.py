@@ -1,0 +1,145 @@
+"""Batched neural rendering: a batch of (volume, view) jobs must render what
+the single-render path renders for each job, eagerly and through the captured
+CUDA graph, with the autotuner's choices."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    assert t.cuda.is_available()
+    return t
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def _jobs(mr, precision, sampler):
+    from internship_b200 import _lib, scenes
+    from internship_b200.weights import active_random_weights
+    from oracle import cloud_np
+    va = mr.VolumeRender(64)
+    va.SetDatas(scenes.sphere_density(64))
+    va.Update()
+    vb = mr.VolumeRender(48)
+    vb.SetDatas(cloud_np.cloud(48, 3))
+    vb.Update()
+    net = mr.Network(active_random_weights(1), mr.builtin_stencil())
+    pa1 = scenes.make_params(40, 24, 1, rt=_lib.RT_MRPNN, precision=precision, sampler=sampler, alpha=32.0)
+    pa2 = scenes.make_params(33, 50, 1, rt=_lib.RT_MRPNN, precision=precision, sampler=sampler, alpha=32.0,
+                             distance=2.0, fov=50.0, seed=0, sample_offset=5)
+    pb = scenes.make_params(56, 31, 1, rt=_lib.RT_MRPNN, precision=precision, sampler=sampler, alpha=80.0,
+                            light_seed=3, albedo=0.95, sample_offset=2)
+    return [(va, pa1), (va, pa2), (vb, pb)], net
+
+
+def _single(torch, net, jobs, advance):
+    from internship_b200 import _lib
+    out = []
+    for v, p in jobs:
+        q = _lib.RenderParams.from_buffer_copy(p)
+        q.sample_offset = p.sample_offset + advance
+        img = torch.empty(q.width * q.height * 3, device="cuda")
+        _lib.check(_lib.load().mr_render(v.handle, net.handle, C.byref(q), _ptr(img), None))
+        torch.cuda.synchronize()
+        out.append(img.cpu().numpy())
+    return out
+
+
+@pytest.mark.parametrize("precision,sampler", [(1, 0), (0, 0), (1, 1)])
+def test_batch_matches_single_renders(torch, precision, sampler):
+    import internship_b200 as mr
+    from internship_b200 import _lib
+    L = _lib.load()
+    jobs, net = _jobs(mr, precision, sampler)
+    outs = [torch.full((p.width * p.height * 3,), -1.0, device="cuda") for _, p in jobs]
+    b = C.c_void_p()
+    _lib.check(L.mr_batch_create(C.byref(b)))
+    for (v, p), o in zip(jobs, outs):
+        _lib.check(L.mr_batch_add(b, v.handle, C.byref(p), _ptr(o)))
+    # waves of 1000 pixels: every wave mixes jobs, records span wave boundaries
+    _lib.check(L.mr_batch_prepare(b, net.handle, 1000, None))
+    _lib.check(L.mr_batch_render(b, net.handle, None))
+    torch.cuda.synchronize()
+    got = [o.cpu().numpy() for o in outs]
+    ref = _single(torch, net, jobs, 0)
+    for g, r in zip(got, ref):
+        assert (r > 0).mean() > 0.05
+        np.testing.assert_allclose(g, r, rtol=1e-6, atol=1e-7)
+    cnt = (C.c_uint64 * 4)()
+    _lib.check(L.mr_batch_counters(b, cnt))
+    assert cnt[3] == sum(int((r.reshape(-1, 3).max(1) > 0).sum()) for r in ref)
+    L.mr_batch_destroy(b)
+    net.close()
+
+
+def test_batch_graph_replays_advance_frames(torch):
+    import internship_b200 as mr
+    from internship_b200 import _lib
+    L = _lib.load()
+    jobs, net = _jobs(mr, 1, 0)
+    outs = [torch.zeros(p.width * p.height * 3, device="cuda") for _, p in jobs]
+    b = C.c_void_p()
+    _lib.check(L.mr_batch_create(C.byref(b)))
+    for (v, p), o in zip(jobs, outs):
+        _lib.check(L.mr_batch_add(b, v.handle, C.byref(p), _ptr(o)))
+    _lib.check(L.mr_batch_prepare(b, net.handle, 0, None))
+    s = torch.cuda.Stream()
+    sp = C.c_void_p(s.cuda_stream)
+    _lib.check(L.mr_batch_capture(b, net.handle, sp))  # renders frame +0 eagerly
+    _lib.check(L.mr_batch_launch(b, sp))               # frame +1
+    _lib.check(L.mr_batch_launch(b, sp))               # frame +2
+    s.synchronize()
+    got = [o.cpu().numpy() for o in outs]
+    for g, r in zip(got, _single(torch, net, jobs, 2)):
+        np.testing.assert_allclose(g, r, rtol=1e-6, atol=1e-7)
+    # the default stream cannot be captured
+    assert L.mr_batch_capture(b, net.handle, None) == _lib.MR_ERR_ARG
+    L.mr_batch_destroy(b)
+    net.close()
+
+
+def test_batch_autotune_and_errors(torch):
+    import internship_b200 as mr
+    from internship_b200 import _lib, scenes
+    L = _lib.load()
+    jobs, net = _jobs(mr, 1, 0)
+    outs = [torch.zeros(p.width * p.height * 3, device="cuda") for _, p in jobs]
+    b = C.c_void_p()
+    _lib.check(L.mr_batch_create(C.byref(b)))
+    assert L.mr_batch_render(b, net.handle, None) == _lib.MR_ERR_STATE  # not prepared
+    for (v, p), o in zip(jobs, outs):
+        _lib.check(L.mr_batch_add(b, v.handle, C.byref(p), _ptr(o)))
+    # a PT job and a mixed precision are rejected
+    bad = scenes.make_params(8, 8, 1)
+    assert L.mr_batch_add(b, jobs[0][0].handle, C.byref(bad), _ptr(outs[0])) == _lib.MR_ERR_ARG
+    bad = scenes.make_params(8, 8, 1, rt=_lib.RT_MRPNN, precision=_lib.PREC_FP32)
+    assert L.mr_batch_add(b, jobs[0][0].handle, C.byref(bad), _ptr(outs[0])) == _lib.MR_ERR_ARG
+    _lib.check(L.mr_batch_prepare(b, net.handle, 0, None))
+    wave, tb, gb = C.c_int64(), C.c_int32(), C.c_int32()
+    _lib.check(L.mr_batch_autotune(b, net.handle, C.byref(wave), C.byref(tb), C.byref(gb), None))
+    total = sum(p.width * p.height for _, p in jobs)
+    assert 0 < wave.value <= total and tb.value in (64, 128, 256) and gb.value in (64, 128, 256)
+    s = torch.cuda.Stream()
+    _lib.check(L.mr_batch_capture(b, net.handle, C.c_void_p(s.cuda_stream)))
+    _lib.check(L.mr_batch_launch(b, C.c_void_p(s.cuda_stream)))
+    s.synchronize()
+    assert all(float(o.max()) > 0 for o in outs)
+    L.mr_batch_destroy(b)
+    # a second job on a volume whose tables serve another light is rejected
+    b2 = C.c_void_p()
+    _lib.check(L.mr_batch_create(C.byref(b2)))
+    v, p = jobs[0]
+    _lib.check(L.mr_batch_add(b2, v.handle, C.byref(p), _ptr(outs[0])))
+    q = _lib.RenderParams.from_buffer_copy(p)
+    q.alpha = p.alpha * 2
+    _lib.check(L.mr_batch_add(b2, v.handle, C.byref(q), _ptr(outs[1])))
+    assert L.mr_batch_prepare(b2, net.handle, 0, None) == _lib.MR_ERR_ARG
+    L.mr_batch_destroy(b2)
+    net.close()
