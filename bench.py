@@ -222,6 +222,88 @@ def matched_rmse(v, p, sp, oracle_spp=16384, small=(480, 270)):
             "weights": "trained by internship_b200.train (config: 32 fBm clouds, 4096-spp FP64 labels)"}
 
 
+BATCH_SIZES = [(256, 256), (512, 512), (1024, 576), (1280, 720), (1920, 1080)]
+
+
+def batched_serving(replays=10, seed=11):
+    """64 seeded fBm clouds (16 each of 64^3, 128^3, 256^3, 512^3), each seen
+    from 4 random views at sizes drawn from 256x256 .. 1920x1080, BF16
+    tensor-core network with the texture sampler, rendered as one batch per
+    CUDA-graph replay with autotuned wave and block sizes. Reports aggregate
+    pixels/s and the p50 / p99 latency of a batch frame (all 256 views)."""
+    import torch
+    import internship_b200 as mr
+    from internship_b200 import _lib, scenes
+    L = _lib.load()
+    stream = torch.cuda.Stream()  # graph capture needs a stream other than the legacy default
+    sp = C.c_void_p(stream.cuda_stream)
+    torch.cuda.synchronize()
+    rng = np.random.default_rng(seed)
+    w = np.load(TRAINED) if os.path.exists(TRAINED) else mr.xavier_weights(1)
+    net = mr.Network(w, mr.builtin_stencil())
+    vols, outs, frames = [], [], []
+    b = C.c_void_p()
+    _lib.check(L.mr_batch_create(C.byref(b)))
+    t0 = time.time()
+    for c in range(64):
+        res = (64, 128, 256, 512)[c // 16]
+        with torch.cuda.stream(stream):
+            dens = torch.empty(res ** 3, device="cuda")
+        scenes.generate_cloud_device(res, 2000 + c, dens.data_ptr(), sp)
+        v = mr.VolumeRender(res)
+        _lib.check(L.mr_volume_set_data_device(v.handle, C.c_void_p(dens.data_ptr()), dens.numel(), sp))
+        _lib.check(L.mr_volume_update(v.handle, sp))
+        del dens
+        vols.append(v)
+        light = int(rng.integers(1 << 30))
+        for k in range(4):
+            W, H = BATCH_SIZES[int(rng.integers(len(BATCH_SIZES)))]
+            d = rng.normal(size=3)
+            d /= np.linalg.norm(d)
+            p = scenes.make_params(W, H, 1, rt=_lib.RT_MRPNN, precision=_lib.PREC_BF16,
+                                   sampler=_lib.SAMPLER_TEXTURE, light_seed=light)
+            ori, up, right = scenes.camera_vectors(d * 2.5, 40.0)
+            p.ori, p.up, p.right = _lib.f3(ori), _lib.f3(up), _lib.f3(right)
+            with torch.cuda.stream(stream):
+                o = torch.empty(W * H * 3, device="cuda")
+            outs.append(o)
+            frames.append((W, H))
+            _lib.check(L.mr_batch_add(b, v.handle, C.byref(p), C.c_void_p(o.data_ptr())))
+    _lib.check(L.mr_batch_prepare(b, net.handle, 0, sp))
+    t_setup = time.time() - t0
+    wave, tb, gb = C.c_int64(), C.c_int32(), C.c_int32()
+    _lib.check(L.mr_batch_autotune(b, net.handle, C.byref(wave), C.byref(tb), C.byref(gb), sp))
+    _lib.check(L.mr_batch_capture(b, net.handle, sp))
+    for _ in range(2):
+        _lib.check(L.mr_batch_launch(b, sp))
+    torch.cuda.synchronize()
+    lat = []
+    for _ in range(replays):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _lib.check(L.mr_batch_launch(b, sp))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        lat.append(e0.elapsed_time(e1))
+    cnt = (C.c_uint64 * 4)()
+    _lib.check(L.mr_batch_counters(b, cnt))
+    total_px = sum(W * H for W, H in frames)
+    L.mr_batch_destroy(b)
+    for v in vols:
+        v.close()
+    net.close()
+    lat = np.array(lat)
+    return {"workload": "64 fBm clouds (16 x 64^3/128^3/256^3/512^3) x 4 views, sizes 256^2..1920x1080, "
+                        "BF16 network, texture sampler, trained weights",
+            "frames_per_batch": len(frames), "pixels_per_batch": total_px,
+            "pixels_per_s": total_px / (float(np.mean(lat)) / 1000.0),
+            "frames_per_s": len(frames) / (float(np.mean(lat)) / 1000.0),
+            "batch_latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                                 "mean": float(np.mean(lat))},
+            "autotuned": {"wave_pixels": int(wave.value), "trace_block": int(tb.value), "gather_block": int(gb.value)},
+            "replays": replays, "graph": "one CUDA graph per batch frame", "setup_s": t_setup}
+
+
 def cpu_baseline_sample(v, dens_dev, p, w, st):
     """Bounded sample of the same frame on the oracle (all host cores)."""
     from internship_b200 import _lib
@@ -248,6 +330,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-rmse", action="store_true", help="skip the matched-RMSE comparison")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-serving measurement")
     ap.add_argument("--frame", default=None,
                     help="WxH instead of 1920x1080: a smaller case for profiler captures, not a bench line")
     args = ap.parse_args()
@@ -417,6 +500,8 @@ def main():
             "active_pixels_per_frame": active,
             "density_fetches_per_frame": fetches,
             "variants": variants}
+    if not args.no_batch and world == 1:
+        line["batched"] = batched_serving()
     if not args.no_rmse:
         m = matched_rmse(v, p, sp)
         if "matched_spp" in m:

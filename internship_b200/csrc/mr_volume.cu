@@ -173,8 +173,9 @@ __global__ void k_hglut(float g, uint32_t seed, float* __restrict__ lut) {
 
 static int grid_for(size_t n, int block) { return (int)((n + block - 1) / block); }
 
+// L is normalised by the caller and is also the key the callers compare with
+// (normalising it again could change it by an ulp and defeat the cache).
 int launch_update_tr(Volume* v, F3 L, float alpha, cudaStream_t s) {
-  L = normalize(L);
   v->timer.mark(ST_TR, s);
   for (int k = 0; k < 8; ++k) {
     int r = 128 >> k;
