@@ -123,6 +123,15 @@ def run_reference(args, rank):
 
 TRAINED = os.path.join(ROOT, "internship_b200", "data", "mrpnn_trained.npy")
 
+# DRAM bytes (read + write) per unit from one ncu capture of each kernel on the
+# 960x540 case of this frame (profiles/*_neural_960x540.md): per active pixel
+# for the gathers and networks, per density fetch for the trace. A launch's
+# traffic = this figure x the launch's units.
+TRAFFIC_PER_UNIT = {"k_mlp_simt": 4422.9, "k_mlp_tc": 2542.6, "k_gather_fm_exact": 2699.0,
+                    "k_gather_fm_texture": 2447.0, "k_nn_trace": 175.9}
+# fp32 FMA rate of the CUDA cores (148 SMs x 128 lanes x 2 FLOP x 1.965 GHz), nominal
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+
 
 def matched_rmse(v, p, sp, oracle_spp=16384, small=(480, 270)):
     """Neural vs delta tracking at matched RMSE against an FP64-accumulated
@@ -468,7 +477,13 @@ def main():
     for s_ in stages.values():
         s_["frac"] = s_["achieved"] / s_["peak"]
         s_["peak_source"] = src
-        s_["traffic"] = None
+    stages["nn_trace"]["traffic"] = TRAFFIC_PER_UNIT["k_nn_trace"] * fetches
+    stages["nn_gather"]["traffic"] = TRAFFIC_PER_UNIT["k_gather_fm_exact"] * active
+    stages["nn_network"]["traffic"] = TRAFFIC_PER_UNIT["k_mlp_simt"] * active
+    stages["nn_network"]["fp32_fma_peak"] = FP32_PEAK_TFLOPS
+    stages["nn_network"]["frac_of_fp32_fma_peak"] = stages["nn_network"]["achieved"] / FP32_PEAK_TFLOPS
+    for s_ in stages.values():
+        s_["traffic_source"] = "ncu dram__bytes_read+write per unit at 960x540, scaled by this launch's units"
     dom = max(stages, key=lambda k: stages[k]["ms"])
     roofline = dict(stages[dom], stage=dom)
     variants = {}
@@ -483,7 +498,8 @@ def main():
                        "peak": hbm, "unit": "GB/s"},
             "network": {"bound": "tensor",
                         "kernel": "k_mlp_tc (tcgen05 BF16 network)" if tc else "k_mlp_simt (fp32 network, CUDA cores)",
-                        "achieved": tf, "peak": bf16, "unit": "TFLOP/s", "frac": tf / bf16, "peak_source": src},
+                        "achieved": tf, "peak": bf16, "unit": "TFLOP/s", "frac": tf / bf16, "peak_source": src,
+                        "traffic": TRAFFIC_PER_UNIT["k_mlp_tc" if tc else "k_mlp_simt"] * lg["active"]},
         }
     line = {"metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
