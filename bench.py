@@ -187,7 +187,8 @@ def matched_rmse(v, p, sp, oracle_spp=16384, small=(480, 270)):
     out = {}
     for name, prec, smp in (("fp32_exact", _lib.PREC_FP32, _lib.SAMPLER_EXACT),
                             ("bf16_exact", _lib.PREC_BF16, _lib.SAMPLER_EXACT),
-                            ("bf16_texture", _lib.PREC_BF16, _lib.SAMPLER_TEXTURE)):
+                            ("bf16_texture", _lib.PREC_BF16, _lib.SAMPLER_TEXTURE),
+                            ("fp8_exact", _lib.PREC_FP8, _lib.SAMPLER_EXACT)):
         q.precision, q.sampler = prec, smp
         errs, imgs = [], []
         for k in range(8):
@@ -438,7 +439,8 @@ def main():
     # the same frames with texture-unit sampling and with the BF16 tensor-core network
     legs = {"fp32_texture": leg(_lib.PREC_FP32, _lib.SAMPLER_TEXTURE, 1000),
             "bf16_exact": leg(_lib.PREC_BF16, _lib.SAMPLER_EXACT, 2000),
-            "bf16_texture": leg(_lib.PREC_BF16, _lib.SAMPLER_TEXTURE, 3000)}
+            "bf16_texture": leg(_lib.PREC_BF16, _lib.SAMPLER_TEXTURE, 3000),
+            "fp8_texture": leg(_lib.PREC_FP8, _lib.SAMPLER_TEXTURE, 4000)}
     p.precision, p.sampler = _lib.PREC_FP32, _lib.SAMPLER_EXACT
 
     # -- end to end through the public API: render + D2H of the frame to pinned memory
@@ -489,7 +491,7 @@ def main():
     variants = {}
     for name, lg in legs.items():
         g_ms, m_ms = lg["stage"][2], lg["stage"][6]
-        tc = name.startswith("bf16")
+        tc = not name.startswith("fp32")
         tf = FLOP_PER_PIXEL * lg["active"] / (m_ms / 1e3) / 1e12
         variants[name] = {
             "value": world * args.steps / (lg["ms"] / 1000.0), "unit": "frames/s", "ms_per_step": lg["ms"] / args.steps,
@@ -497,7 +499,8 @@ def main():
             "gather": {"bound": "hbm", "achieved": lg["active"] * (384 * 32 + 383 * 16 + 581 * 4) / (g_ms / 1e3) / 1e9,
                        "peak": hbm, "unit": "GB/s"},
             "network": {"bound": "tensor",
-                        "kernel": "k_mlp_tc (tcgen05 BF16 network)" if tc else "k_mlp_simt (fp32 network, CUDA cores)",
+                        "kernel": ("k_mlp_tc (tcgen05 %s network)" % ("E4M3" if name.startswith("fp8") else "BF16"))
+                        if tc else "k_mlp_simt (fp32 network, CUDA cores)",
                         "achieved": tf, "peak": bf16, "unit": "TFLOP/s", "frac": tf / bf16, "peak_source": src,
                         "traffic": TRAFFIC_PER_UNIT["k_mlp_tc" if tc else "k_mlp_simt"] * lg["active"]},
         }

@@ -37,7 +37,11 @@ typedef enum {
  * the reference tree and it is not supported here). */
 typedef enum { MR_RT_PT = 0, MR_RT_RPNN = 1, MR_RT_MRPNN = 2 } mr_render_type;
 
-/* Arithmetic of the radiance-predictor MLP. */
+/* Arithmetic of the radiance-predictor MLP.
+ * FP32: CUDA cores, the reference's arithmetic order.
+ * BF16: tcgen05 tensor cores, BF16 operands, FP32 accumulation.
+ * FP8:  tcgen05 tensor cores, E4M3 operands with a power-of-two scale per
+ *       layer (weights) and per row (activations), FP32 accumulation. */
 typedef enum { MR_PREC_FP32 = 0, MR_PREC_BF16 = 1, MR_PREC_FP8 = 2 } mr_precision;
 
 /* What mr_volume_read copies back. */
@@ -175,6 +179,10 @@ int mr_cloud_permutation(uint32_t seed, int32_t* host_out256);
  * n x k are BF16 bit patterns, row-major; host_d receives 128 x n fp32.
  * Shapes (n, k): (16,16) (32,32) (16,32) (32,64) (64,128) (128,128). */
 int mr_tc_selftest(int32_t n, int32_t k, const uint16_t* host_a, const uint16_t* host_b, float* host_d);
+/* The same tile product with E4M3 operands (kind::f8f6f4, no reference
+ * counterpart): host_a 128 x k and host_b n x k are E4M3 bytes, row-major.
+ * Shapes (n, k): (16,32) (32,32) (64,128) (128,128). */
+int mr_tc_selftest_fp8(int32_t n, int32_t k, const uint8_t* host_a, const uint8_t* host_b, float* host_d);
 /* Error word of the tensor-core network kernel of `net` (an mbarrier wait
  * that timed out): MR_ERR_TIMEOUT if set; `reset` clears it. */
 int mr_network_check(const mr_network* net, int32_t reset);

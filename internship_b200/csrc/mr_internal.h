@@ -73,6 +73,7 @@ struct Network {
   void* packed = nullptr;    // tensor-core operand images (bf16/fp8), see mr_mlp_tc.cu
   size_t packed_bytes = 0;
   std::vector<float> h_rowwise;  // fp32 per-row weights passed as kernel parameters (mr_mlp_tc.cu)
+  std::vector<float> h_winv8;    // inverse per-layer scales of the E4M3 weight image
   float h_stencil[MR_STENCIL_POINTS * 3];
 };
 

@@ -91,15 +91,28 @@ struct ROff {
 };
 #define ROFF(name) (::mr::ROff<MR_W_##name>::value)
 
-struct TcTables { int woff[kTcLayers]; int boff[kTcLayers]; };
+// E4M3 image: rows of K padded to a multiple of 32 one-byte elements (the
+// K of one f8f6f4 MMA), N padded to 16.
+constexpr int kp8(int k) { return k <= 32 ? 32 : (k + 31) / 32 * 32; }
+constexpr int tc_bytes8(int i) { return pad16(kTc[i].n) * kp8(kTc[i].k); }
+constexpr int tc_offset8(int i) { int o = 0; for (int j = 0; j < i; ++j) o += tc_bytes8(j); return o; }
+constexpr int kW8Bytes = tc_offset8(kTcLayers);
+
+struct TcTables { int woff[kTcLayers]; int woff8[kTcLayers]; int boff[kTcLayers]; };
 constexpr TcTables make_tc_tables() {
   TcTables t{};
   const RowTable rt = make_row_table();
-  for (int i = 0; i < kTcLayers; ++i) { t.woff[i] = tc_offset(i); t.boff[i] = rt.off[kTc[i].b]; }
+  for (int i = 0; i < kTcLayers; ++i) {
+    t.woff[i] = tc_offset(i);
+    t.woff8[i] = tc_offset8(i);
+    t.boff[i] = rt.off[kTc[i].b];
+  }
   return t;
 }
 __constant__ TcTables c_tc = make_tc_tables();
 __device__ __forceinline__ int tc_offset_dev(int i) { return c_tc.woff[i]; }
+template <bool F8>
+__device__ __forceinline__ int tc_off(int i) { return F8 ? c_tc.woff8[i] : c_tc.woff[i]; }
 __device__ __forceinline__ int kTcBias(int i) { return c_tc.boff[i]; }
 
 constexpr int kGroups = 4;
@@ -109,7 +122,9 @@ constexpr int kHeadBytes = 128 * 128 * 2;      // 32 KB
 // layer's MMA has completed (mbarrier) before its epilogue overwrites it.
 constexpr int kGroupBytes = kHeadBytes;
 static_assert(kTrunkBytes <= kHeadBytes, "trunk tiles alias the head tile");
-constexpr int kSmemBytes = kWBytes + kGroups * kGroupBytes + 64 * kGroups + 16;
+template <bool F8>
+constexpr int smem_bytes() { return (F8 ? kW8Bytes : kWBytes) + kGroups * kGroupBytes + 64 * kGroups + 16; }
+constexpr int kSmemBytes = smem_bytes<false>();
 constexpr int kTmemCols = 512;  // 128 per group (power of two allocation)
 static_assert(128 * kGroups <= kTmemCols, "tensor memory budget");
 static_assert(kSmemBytes <= 232448, "shared memory budget");
@@ -242,6 +257,97 @@ __device__ __forceinline__ void issue_layer(uint32_t tmem_d, uint32_t a_addr, ui
   }
 }
 
+// ---- E4M3 operands (MR_PREC_FP8) ------------------------------------------------
+// 8-bit K-major tiles keep the byte structure of the BF16 ones: 16-byte
+// core-matrix rows (16 elements), 8-row groups SBO apart, K halves of one MMA
+// (K = 32) 128 bytes apart. Values are stored multiplied by a power-of-two
+// scale chosen per row and operand (max |x| -> at most 448, the largest
+// E4M3 value); the epilogue multiplies the FP32 accumulator by the inverse
+// row scale and the layer's inverse weight scale.
+template <bool F8>
+__host__ __device__ constexpr int qoff(int row, int k, int kp) {
+  return F8 ? ((row >> 3) * (kp >> 4) + (k >> 4)) * 128 + (row & 7) * 16 + (k & 15) : canon_off(row, k, kp);
+}
+template <bool F8>
+__host__ __device__ constexpr int qkp(int k) { return F8 ? kp8(k) : pad16(k); }
+
+// two floats -> E4M3x2 (first value in the low byte), round to nearest, saturating
+__device__ __forceinline__ uint32_t pack_e4m3x2(float lo, float hi) {
+  uint16_t r;
+  asm("{\n\t.reg .b16 t;\n\tcvt.rn.satfinite.e4m3x2.f32 t, %2, %1;\n\tmov.b16 %0, t;\n\t}\n"
+      : "=h"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+// Power-of-two scale mapping max |x| = m to at most 448.
+__device__ __forceinline__ float q_scale(float m) {
+  if (!(m > 0.0f)) return 1.0f;
+  const float e = fminf(fmaxf(floorf(log2f(448.0f / m)), -24.0f), 24.0f);
+  return exp2f(e);
+}
+// N (multiple of 8) values x[0..N) to columns k0.. (multiple of 8) of a row;
+// `s` scales the values of an 8-bit tile.
+template <bool F8, int KP, int N>
+__device__ __forceinline__ void store_q(uint8_t* tile, int row, int k0, const float* x, float s) {
+#pragma unroll
+  for (int kg = 0; kg < N / 8; ++kg) {
+    const float* v = x + 8 * kg;
+    if constexpr (F8) {
+      uint2 q;
+      q.x = pack_e4m3x2(v[0] * s, v[1] * s) | (pack_e4m3x2(v[2] * s, v[3] * s) << 16);
+      q.y = pack_e4m3x2(v[4] * s, v[5] * s) | (pack_e4m3x2(v[6] * s, v[7] * s) << 16);
+      *reinterpret_cast<uint2*>(tile + qoff<true>(row, k0 + 8 * kg, KP)) = q;
+    } else {
+      uint4 q;
+      q.x = pack_bf16(v[0], v[1]);
+      q.y = pack_bf16(v[2], v[3]);
+      q.z = pack_bf16(v[4], v[5]);
+      q.w = pack_bf16(v[6], v[7]);
+      *reinterpret_cast<uint4*>(tile + canon_off(row, k0 + 8 * kg, KP)) = q;
+    }
+  }
+}
+// Whole row of KP values with its own scale; returns the inverse scale (1 for BF16).
+template <bool F8, int KP>
+__device__ __forceinline__ float store_row_q(uint8_t* tile, int row, const float* x) {
+  float s = 1.0f;
+  if constexpr (F8) {
+    float m = 0.0f;
+#pragma unroll
+    for (int i = 0; i < KP; ++i) m = fmaxf(m, fabsf(x[i]));
+    s = q_scale(m);
+  }
+  store_q<F8, KP, KP>(tile, row, 0, x, s);
+  return 1.0f / s;
+}
+
+__device__ __forceinline__ void umma_f8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(acc)
+      : "memory");
+}
+// Instruction descriptor: E4M3 x E4M3 -> FP32, A and B K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_e4m3(int m, int n) {
+  return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+// D[tmem] = A[128 x KP] * W[NP x KP]^T; KP in elements of the operand type.
+template <bool F8, int NP, int KP>
+__device__ __forceinline__ void issue_q(uint32_t tmem_d, uint32_t a_addr, uint32_t w_addr) {
+  if constexpr (F8) {
+    static_assert(KP % 32 == 0, "E4M3 K step is 32");
+    constexpr uint32_t id = idesc_e4m3(128, NP);
+#pragma unroll
+    for (int s = 0; s < KP / 32; ++s) {
+      uint64_t da = sdesc(a_addr + s * 256, 128, (KP / 16) * 128);
+      uint64_t db = sdesc(w_addr + s * 256, 128, (KP / 16) * 128);
+      umma_f8(tmem_d, da, db, id, s > 0 ? 1u : 0u);
+    }
+  } else {
+    issue_layer<NP, KP>(tmem_d, a_addr, w_addr);
+  }
+}
+
 __device__ __forceinline__ float sigm(float x) { return 1.0f / (1.0f + expf(-x)); }
 
 // Read of the row-wise weight image (kernel parameter space).
@@ -264,6 +370,8 @@ struct TcArgs {
   float* spill;                       // 120 x spill_cap ungated head columns (multi-channel tiles)
   long long spill_cap;
   int* err;                           // set on a wait timeout
+  const uint8_t* __restrict__ wpack8; // kW8Bytes packed E4M3 image (MR_PREC_FP8)
+  float winv[kTcLayers];              // inverse per-layer weight scales (1 for BF16)
   float rw[kRowFloats];               // row-wise fp32 weights (make_row_table)
 };
 
@@ -318,7 +426,8 @@ __device__ __forceinline__ void mma_round(GroupCtx& c, IssueFn issue) {
 // Reads back N (<= 32) columns at TMEM column `col`, adds the bias and
 // applies ReLU.
 template <int N>
-__device__ __forceinline__ void epi_relu(const GroupCtx& c, int col, const float* __restrict__ bias, float* y) {
+__device__ __forceinline__ void epi_relu(const GroupCtx& c, int col, const float* __restrict__ bias, float* y,
+                                         float sc = 1.0f) {
   float v[16];
 #pragma unroll
   for (int h = 0; h < (N + 15) / 16; ++h) {
@@ -326,7 +435,7 @@ __device__ __forceinline__ void epi_relu(const GroupCtx& c, int col, const float
 #pragma unroll
     for (int i = 0; i < 16; ++i)
       if (16 * h + i < N) {
-        float a = ldw(bias + 16 * h + i) + v[i];
+        float a = ldw(bias + 16 * h + i) + v[i] * sc;
         y[16 * h + i] = a >= 0.0f ? a : 0.0f;
       }
   }
@@ -423,9 +532,9 @@ __device__ __forceinline__ void block_prep(const DIn& d, const float* __restrict
 }
 
 // A rows of a block that starts a trunk (SE, no residual input): seg * gate.
-template <int S>
-__device__ __forceinline__ void store_first(GroupCtx& c, const DIn& d, int from, const float* gate) {
-  constexpr int KP = S < 16 ? 16 : S;
+template <bool F8, int S>
+__device__ __forceinline__ void store_first(GroupCtx& c, const DIn& d, int from, const float* gate, float* ainv) {
+  constexpr int KP = qkp<F8>(S);
 #pragma unroll
   for (int br = 0; br < 3; ++br) {
     float x[KP];
@@ -438,7 +547,7 @@ __device__ __forceinline__ void store_first(GroupCtx& c, const DIn& d, int from,
         x[i] = x[i + 1] = x[i + 2] = x[i + 3] = 0.0f;
       }
     }
-    store_row<KP>(c.trunk + br * kBr, c.t, x);
+    ainv[br] = store_row_q<F8, KP>(c.trunk + br * kBr, c.t, x);
   }
 }
 
@@ -446,14 +555,15 @@ __device__ __forceinline__ void store_first(GroupCtx& c, const DIn& d, int from,
 // yn = ReLU(acc + b); y = yn + seg (ADD3) or [yn, seg] (REP3, MODE 2).
 // NEXT = 0: writes the next block's A rows seg2 * gate2 + y (SERES input,
 // radiancePredict.cu:259-294); NEXT = 1: writes y (input of L81 / LD41).
-template <int S, int MODE, int NEXT>
+template <bool F8, int S, int MODE, int NEXT>
 __device__ __forceinline__ void block_epi(GroupCtx& c, const DIn& d, const float* __restrict__ w, int layer0, int from,
-                                          int from2, const float* gate2) {
+                                          int from2, const float* gate2, float* ainv, const float* winv) {
   constexpr int W = MODE == 2 ? 2 * S : S;
-  constexpr int KP = W < 16 ? 16 : W;
+  constexpr int KP = qkp<F8>(W);
 #pragma unroll
   for (int br = 0; br < 3; ++br) {
     const float* bias = w + kTcBias(layer0 + br);
+    const float sc = F8 ? ainv[br] * winv[layer0 + br] : 1.0f;
     float y[KP];
 #pragma unroll
     for (int h = 0; h < (S + 15) / 16; ++h) {
@@ -462,7 +572,7 @@ __device__ __forceinline__ void block_epi(GroupCtx& c, const DIn& d, const float
 #pragma unroll
       for (int i = 0; i < 16; ++i)
         if (16 * h + i < S) {
-          const float a = v[i] + ldw(bias + 16 * h + i);
+          const float a = v[i] * sc + ldw(bias + 16 * h + i);
           y[16 * h + i] = a >= 0.0f ? a : 0.0f;
         }
     }
@@ -488,16 +598,18 @@ __device__ __forceinline__ void block_epi(GroupCtx& c, const DIn& d, const float
         y[i + 3] = q.w * gate2[br] + y[i + 3];
       }
     }
-    store_row<KP>(c.trunk + br * kBr, c.t, y);
+    ainv[br] = store_row_q<F8, KP>(c.trunk + br * kBr, c.t, y);
   }
 }
 
-template <int KP>
+// Three branch MMAs of a trunk layer with S outputs and S inputs.
+template <bool F8, int S>
 __device__ __forceinline__ void issue_trunk(GroupCtx& c, int layer0) {
   const uint32_t tb = smem_u32(c.trunk), wb = smem_u32(c.wsm);
   mma_issue(c, [&]() {
 #pragma unroll
-    for (int br = 0; br < 3; ++br) issue_layer<KP, KP>(c.tmem + 32 * br, tb + br * kBr, wb + tc_offset_dev(layer0 + br));
+    for (int br = 0; br < 3; ++br)
+      issue_q<F8, pad16(S), qkp<F8>(S)>(c.tmem + 32 * br, tb + br * kBr, wb + tc_off<F8>(layer0 + br));
   });
 }
 
@@ -529,42 +641,75 @@ __device__ __forceinline__ void head_gates(const float* __restrict__ w, const fl
 }
 
 // Head SC(p) (radiancePredict.cu:439-473) for one albedo channel; the
-// gated 128-wide input is already in c.head (bf16). Returns the output X.
-__device__ __forceinline__ float head_chain(GroupCtx& c, const float* __restrict__ w) {
+// gated 128-wide input is already in c.head (inverse row scale ainv for E4M3).
+// Returns the output X. With E4M3 operands every layer's outputs get a new row
+// scale before they are stored as the next layer's A rows (a first pass over
+// TMEM finds the row maximum where the outputs do not fit in registers).
+template <bool F8>
+__device__ __forceinline__ float head_chain(GroupCtx& c, const float* __restrict__ w, const float* winv, float ainv) {
   const uint32_t hb = smem_u32(c.head), tb = smem_u32(c.trunk), wb = smem_u32(c.wsm);
   float v[32];
   // LC0 128 -> 128, read back and re-stored 32 columns at a time
-  mma_round(c, [&]() { issue_layer<128, 128>(c.tmem, hb, wb + tc_offset(TC_LC0)); });
+  mma_round(c, [&]() { issue_q<F8, 128, 128>(c.tmem, hb, wb + tc_off<F8>(TC_LC0)); });
+  float sc = F8 ? ainv * winv[TC_LC0] : 1.0f, s = 1.0f;
+  if constexpr (F8) {
+    float m = 0.0f;
+#pragma unroll 1
+    for (int h = 0; h < 4; ++h) {
+      epi_relu<32>(c, 32 * h, w + ROFF(LC0B) + 32 * h, v, sc);
+#pragma unroll
+      for (int i = 0; i < 32; ++i) m = fmaxf(m, v[i]);
+    }
+    s = q_scale(m);
+  }
 #pragma unroll 1
   for (int h = 0; h < 4; ++h) {
-    epi_relu<32>(c, 32 * h, w + ROFF(LC0B) + 32 * h, v);
-    store_cols<128, 32>(c.head, c.t, 32 * h, v);
+    epi_relu<32>(c, 32 * h, w + ROFF(LC0B) + 32 * h, v, sc);
+    store_q<F8, 128, 32>(c.head, c.t, 32 * h, v, s);
   }
+  ainv = 1.0f / s;
   // LC1 128 -> 64
-  mma_round(c, [&]() { issue_layer<64, 128>(c.tmem, hb, wb + tc_offset(TC_LC1)); });
+  mma_round(c, [&]() { issue_q<F8, 64, 128>(c.tmem, hb, wb + tc_off<F8>(TC_LC1)); });
+  sc = F8 ? ainv * winv[TC_LC1] : 1.0f;
+  if constexpr (F8) {
+    float m = 0.0f;
+#pragma unroll 1
+    for (int h = 0; h < 2; ++h) {
+      epi_relu<32>(c, 32 * h, w + ROFF(LC1B) + 32 * h, v, sc);
+#pragma unroll
+      for (int i = 0; i < 32; ++i) m = fmaxf(m, v[i]);
+    }
+    s = q_scale(m);
+  }
 #pragma unroll 1
   for (int h = 0; h < 2; ++h) {
-    epi_relu<32>(c, 32 * h, w + ROFF(LC1B) + 32 * h, v);
-    store_cols<64, 32>(c.trunk, c.t, 32 * h, v);
+    epi_relu<32>(c, 32 * h, w + ROFF(LC1B) + 32 * h, v, sc);
+    store_q<F8, 64, 32>(c.trunk, c.t, 32 * h, v, s);
   }
+  ainv = 1.0f / s;
   // LC2 64 -> 32
-  mma_round(c, [&]() { issue_layer<32, 64>(c.tmem, tb, wb + tc_offset(TC_LC2)); });
-  epi_relu<32>(c, 0, w + ROFF(LC2B), v);
-  store_row<32>(c.trunk, c.t, v);
+  mma_round(c, [&]() { issue_q<F8, 32, 64>(c.tmem, tb, wb + tc_off<F8>(TC_LC2)); });
+  epi_relu<32>(c, 0, w + ROFF(LC2B), v, F8 ? ainv * winv[TC_LC2] : 1.0f);
+  ainv = store_row_q<F8, 32>(c.trunk, c.t, v);
   // LX 32 -> 16
-  mma_round(c, [&]() { issue_layer<16, 32>(c.tmem, tb, wb + tc_offset(TC_LX)); });
-  float a[16], b[16];
-  epi_relu<16>(c, 0, w + ROFF(LXB), a);
+  mma_round(c, [&]() { issue_q<F8, 16, 32>(c.tmem, tb, wb + tc_off<F8>(TC_LX)); });
+  float a[16], b[32];
+  epi_relu<16>(c, 0, w + ROFF(LXB), a, F8 ? ainv * winv[TC_LX] : 1.0f);
+  constexpr int K16 = qkp<F8>(16);
+#pragma unroll
+  for (int i = 16; i < 32; ++i) b[i] = 0.0f;
   // six residual pairs (:454-471)
 #pragma unroll 1
   for (int r = 0; r < 6; ++r) {
-    store_row<16>(c.trunk, c.t, a);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) b[i] = a[i];
+    ainv = store_row_q<F8, K16>(c.trunk, c.t, b);
     int l0 = TC_LXR + 2 * r, l1 = l0 + 1;
-    mma_round(c, [&]() { issue_layer<16, 16>(c.tmem, tb, wb + tc_offset_dev(l0)); });
-    epi_relu<16>(c, 0, w + kTcBias(l0), b);
-    store_row<16>(c.trunk, c.t, b);
-    mma_round(c, [&]() { issue_layer<16, 16>(c.tmem, tb, wb + tc_offset_dev(l1)); });
-    epi_relu<16>(c, 0, w + kTcBias(l1), b);
+    mma_round(c, [&]() { issue_q<F8, 16, K16>(c.tmem, tb, wb + tc_off<F8>(l0)); });
+    epi_relu<16>(c, 0, w + kTcBias(l0), b, F8 ? ainv * winv[l0] : 1.0f);
+    ainv = store_row_q<F8, K16>(c.trunk, c.t, b);
+    mma_round(c, [&]() { issue_q<F8, 16, K16>(c.tmem, tb, wb + tc_off<F8>(l1)); });
+    epi_relu<16>(c, 0, w + kTcBias(l1), b, F8 ? ainv * winv[l1] : 1.0f);
 #pragma unroll
     for (int i = 0; i < 16; ++i) a[i] = a[i] + b[i];
   }
@@ -577,20 +722,32 @@ __device__ __forceinline__ float head_chain(GroupCtx& c, const float* __restrict
 }
 
 // Head input of a further albedo channel, from the ungated head columns the
-// first pass spilled (feature-major, comb[i] at spill[i*cap + row]).
-__device__ __forceinline__ void head_input_spilled(GroupCtx& c, const float* __restrict__ w, const float* spill,
-                                                long long cap, int row, const float* fin, float g, float gamma,
-                                                float srp) {
+// first pass spilled (feature-major, comb[i] at spill[i*cap + row]); returns
+// the inverse row scale of the stored row.
+template <bool F8>
+__device__ __forceinline__ float head_input_spilled(GroupCtx& c, const float* __restrict__ w, const float* spill,
+                                                    long long cap, int row, const float* fin, float g, float gamma,
+                                                    float srp) {
   float x8[8], sep[6];
   head_gates(w, fin, g, gamma, srp, x8, sep);
-  store_cols<128, 8>(c.head, c.t, 120, x8);
+  float s = 1.0f;
+  if constexpr (F8) {
+    float m = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) m = fmaxf(m, x8[i]);
+#pragma unroll 1
+    for (int i = 0; i < 120; ++i) m = fmaxf(m, spill[i * cap + row] * sep[i < 96 ? i / 32 : 3 + (i - 96) / 8]);
+    s = q_scale(m);
+  }
+  store_q<F8, 128, 8>(c.head, c.t, 120, x8, s);
 #pragma unroll 1
   for (int g8 = 0; g8 < 15; ++g8) {
-    const float s = sep[g8 < 12 ? g8 / 4 : g8 - 9];
+    const float sg = sep[g8 < 12 ? g8 / 4 : g8 - 9];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) x8[i] = spill[(8 * g8 + i) * cap + row] * s;
-    store_cols<128, 8>(c.head, c.t, 8 * g8, x8);
+    for (int i = 0; i < 8; ++i) x8[i] = spill[(8 * g8 + i) * cap + row] * sg;
+    store_q<F8, 128, 8>(c.head, c.t, 8 * g8, x8, s);
   }
+  return 1.0f / s;
 }
 
 // Group-wide OR of a per-row flag (named barrier g+1 with reduction).
@@ -604,17 +761,19 @@ __device__ __forceinline__ bool group_any(int g, bool x) {
   return r != 0;
 }
 
+template <bool F8>
 __global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(const __grid_constant__ TcArgs a) {
+  constexpr int WB = F8 ? kW8Bytes : kWBytes;
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* wsm = smem;
-  uint8_t* gbase = smem + kWBytes;
-  uint64_t* mbars = reinterpret_cast<uint64_t*>(smem + kWBytes + kGroups * kGroupBytes);
+  uint8_t* gbase = smem + WB;
+  uint64_t* mbars = reinterpret_cast<uint64_t*>(smem + WB + kGroups * kGroupBytes);
   uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(mbars + kGroups);
   const int tid = threadIdx.x, warp = tid >> 5;
   const int g = tid >> 7, t = tid & 127;
   // weights -> shared memory (16-byte vectors)
-  for (int i = tid; i < kWBytes / 16; i += blockDim.x)
-    reinterpret_cast<uint4*>(wsm)[i] = __ldg(reinterpret_cast<const uint4*>(a.wpack) + i);
+  const uint4* wsrc = reinterpret_cast<const uint4*>(F8 ? a.wpack8 : a.wpack);
+  for (int i = tid; i < WB / 16; i += blockDim.x) reinterpret_cast<uint4*>(wsm)[i] = __ldg(wsrc + i);
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_holder)),
                  "r"(kTmemCols));
@@ -660,28 +819,29 @@ __global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(const __grid_consta
     float fin[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) fin[j] = 0.0f;
-    float gate[3];
+    float gate[3], ainv[3];  // ainv: inverse E4M3 row scales of the three branch A rows (1 for BF16)
+    const float* winv = a.winv;
 
     // light-direction trunk (:424-437): blocks at 160, 168, 176, 184
     block_prep<8>(d, w, 160, 24, ROFF(LDSE01W), ROFF(LDSE02W), gg, gamma, fin, gate);
-    store_first<8>(c, d, 160, gate);
-    issue_trunk<16>(c, TC_DI + 0);
+    store_first<F8, 8>(c, d, 160, gate, ainv);
+    issue_trunk<F8, 8>(c, TC_DI + 0);
     block_prep<8>(d, w, 168, 27, ROFF(LDSE11W), ROFF(LDSE12W), gg, gamma, fin, gate);
     mma_wait(c);
-    block_epi<8, 0, 0>(c, d, w, TC_DI + 0, 160, 168, gate);
-    issue_trunk<16>(c, TC_DI + 3);
+    block_epi<F8, 8, 0, 0>(c, d, w, TC_DI + 0, 160, 168, gate, ainv, winv);
+    issue_trunk<F8, 8>(c, TC_DI + 3);
     block_prep<8>(d, w, 176, 30, ROFF(LDSE21W), ROFF(LDSE22W), gg, gamma, fin, gate);
     mma_wait(c);
-    block_epi<8, 1, 0>(c, d, w, TC_DI + 3, 168, 176, gate);
-    issue_trunk<16>(c, TC_DI + 6);
+    block_epi<F8, 8, 1, 0>(c, d, w, TC_DI + 3, 168, 176, gate, ainv, winv);
+    issue_trunk<F8, 8>(c, TC_DI + 6);
     block_prep<8>(d, w, 184, 33, ROFF(LDSE31W), ROFF(LDSE32W), gg, gamma, fin, gate);
     mma_wait(c);
-    block_epi<8, 1, 0>(c, d, w, TC_DI + 6, 176, 184, gate);
-    issue_trunk<16>(c, TC_DI + 9);
+    block_epi<F8, 8, 1, 0>(c, d, w, TC_DI + 6, 176, 184, gate, ainv, winv);
+    issue_trunk<F8, 8>(c, TC_DI + 9);
     block_prep<8>(d, w, 0, 0, ROFF(LSE01W), ROFF(LSE02W), gg, gamma, fin, gate);  // main block 0
     mma_wait(c);
-    block_epi<8, 1, 1>(c, d, w, TC_DI + 9, 184, 0, nullptr);
-    issue_trunk<16>(c, TC_LD41);
+    block_epi<F8, 8, 1, 1>(c, d, w, TC_DI + 9, 184, 0, nullptr, ainv, winv);
+    issue_trunk<F8, 8>(c, TC_LD41);
     mma_wait(c);
     // LD41 -> comb[96..120), parked in TMEM
 #pragma unroll
@@ -689,48 +849,49 @@ __global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(const __grid_consta
       float v[8];
       tmem_ld8(c.tmem + c.tlane + 32 * br, v);
       const float* bias = w + kTcBias(TC_LD41 + br);
+      const float sc = F8 ? ainv[br] * winv[TC_LD41 + br] : 1.0f;
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
-        const float x = v[i] + ldw(bias + i);
+        const float x = v[i] * sc + ldw(bias + i);
         v[i] = x >= 0.0f ? x : 0.0f;
       }
       tmem_st8(tcomb + 8 * br, v);
     }
 
     // main trunk (:396-421)
-    store_first<8>(c, d, 0, gate);
-    issue_trunk<16>(c, TC_MAIN + 0);
+    store_first<F8, 8>(c, d, 0, gate, ainv);
+    issue_trunk<F8, 8>(c, TC_MAIN + 0);
     block_prep<8>(d, w, 8, 3, ROFF(LSE11W), ROFF(LSE12W), gg, gamma, fin, gate);
     mma_wait(c);
-    block_epi<8, 0, 0>(c, d, w, TC_MAIN + 0, 0, 8, gate);
-    issue_trunk<16>(c, TC_MAIN + 3);
+    block_epi<F8, 8, 0, 0>(c, d, w, TC_MAIN + 0, 0, 8, gate, ainv, winv);
+    issue_trunk<F8, 8>(c, TC_MAIN + 3);
     block_prep<16>(d, w, 16, 6, ROFF(LSE21W), ROFF(LSE22W), gg, gamma, fin, gate);
     mma_wait(c);
-    block_epi<8, 2, 0>(c, d, w, TC_MAIN + 3, 8, 16, gate);
-    issue_trunk<16>(c, TC_MAIN + 6);
+    block_epi<F8, 8, 2, 0>(c, d, w, TC_MAIN + 3, 8, 16, gate, ainv, winv);
+    issue_trunk<F8, 16>(c, TC_MAIN + 6);
     block_prep<16>(d, w, 32, 9, ROFF(LSE31W), ROFF(LSE32W), gg, gamma, fin, gate);
     mma_wait(c);
-    block_epi<16, 1, 0>(c, d, w, TC_MAIN + 6, 16, 32, gate);
-    issue_trunk<16>(c, TC_MAIN + 9);
+    block_epi<F8, 16, 1, 0>(c, d, w, TC_MAIN + 6, 16, 32, gate, ainv, winv);
+    issue_trunk<F8, 16>(c, TC_MAIN + 9);
     block_prep<16>(d, w, 48, 12, ROFF(LSE41W), ROFF(LSE42W), gg, gamma, fin, gate);
     mma_wait(c);
-    block_epi<16, 1, 0>(c, d, w, TC_MAIN + 9, 32, 48, gate);
-    issue_trunk<16>(c, TC_MAIN + 12);
+    block_epi<F8, 16, 1, 0>(c, d, w, TC_MAIN + 9, 32, 48, gate, ainv, winv);
+    issue_trunk<F8, 16>(c, TC_MAIN + 12);
     block_prep<32>(d, w, 64, 15, ROFF(LSE51W), ROFF(LSE52W), gg, gamma, fin, gate);
     mma_wait(c);
-    block_epi<16, 2, 0>(c, d, w, TC_MAIN + 12, 48, 64, gate);
-    issue_trunk<32>(c, TC_MAIN + 15);
+    block_epi<F8, 16, 2, 0>(c, d, w, TC_MAIN + 12, 48, 64, gate, ainv, winv);
+    issue_trunk<F8, 32>(c, TC_MAIN + 15);
     block_prep<32>(d, w, 96, 18, ROFF(LSE61W), ROFF(LSE62W), gg, gamma, fin, gate);
     mma_wait(c);
-    block_epi<32, 1, 0>(c, d, w, TC_MAIN + 15, 64, 96, gate);
-    issue_trunk<32>(c, TC_MAIN + 18);
+    block_epi<F8, 32, 1, 0>(c, d, w, TC_MAIN + 15, 64, 96, gate, ainv, winv);
+    issue_trunk<F8, 32>(c, TC_MAIN + 18);
     block_prep<32>(d, w, 128, 21, ROFF(LSE71W), ROFF(LSE72W), gg, gamma, fin, gate);
     mma_wait(c);
-    block_epi<32, 1, 0>(c, d, w, TC_MAIN + 18, 96, 128, gate);
-    issue_trunk<32>(c, TC_MAIN + 21);
+    block_epi<F8, 32, 1, 0>(c, d, w, TC_MAIN + 18, 96, 128, gate, ainv, winv);
+    issue_trunk<F8, 32>(c, TC_MAIN + 21);
     mma_wait(c);
-    block_epi<32, 1, 1>(c, d, w, TC_MAIN + 21, 128, 0, nullptr);
-    issue_trunk<32>(c, TC_L81);
+    block_epi<F8, 32, 1, 1>(c, d, w, TC_MAIN + 21, 128, 0, nullptr, ainv, winv);
+    issue_trunk<F8, 32>(c, TC_L81);
     // channel-0 head gates while L81 runs (fin is complete)
     float x8[8], sep[6];
     head_gates(w, fin, gg, gamma, srp[0], x8, sep);
@@ -738,16 +899,40 @@ __global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(const __grid_consta
     // L81 -> comb[0..96); gated head input for channel 0 (:439-452)
     const bool spill = (need1 || need2) && a.spill != nullptr;
     const long long cap = a.spill_cap;
+    float hs = 1.0f;  // E4M3 scale of the head row
+    if constexpr (F8) {
+      float m = 0.0f;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) m = fmaxf(m, x8[i]);
+#pragma unroll
+      for (int br = 0; br < 3; ++br) {
+        const float* bias = w + kTcBias(TC_L81 + br);
+        const float sc = ainv[br] * winv[TC_L81 + br];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          float v[16];
+          tmem_ld16(c.tmem + c.tlane + 32 * br + 16 * h, v);
+#pragma unroll
+          for (int i = 0; i < 16; ++i) m = fmaxf(m, fmaxf(v[i] * sc + ldw(bias + 16 * h + i), 0.0f) * sep[br]);
+        }
+        float v8[8];
+        tmem_ld8(tcomb + 8 * br, v8);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) m = fmaxf(m, v8[i] * sep[3 + br]);
+      }
+      hs = q_scale(m);
+    }
 #pragma unroll
     for (int br = 0; br < 3; ++br) {
       const float* bias = w + kTcBias(TC_L81 + br);
+      const float sc = F8 ? ainv[br] * winv[TC_L81 + br] : 1.0f;
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         float v[16];
         tmem_ld16(c.tmem + c.tlane + 32 * br + 16 * h, v);
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
-          const float x = v[i] + ldw(bias + 16 * h + i);
+          const float x = v[i] * sc + ldw(bias + 16 * h + i);
           v[i] = x >= 0.0f ? x : 0.0f;
         }
         if (spill && row < n) {
@@ -756,7 +941,7 @@ __global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(const __grid_consta
         }
 #pragma unroll
         for (int i = 0; i < 16; ++i) v[i] *= sep[br];
-        store_cols<128, 16>(c.head, c.t, 32 * br + 16 * h, v);
+        store_q<F8, 128, 16>(c.head, c.t, 32 * br + 16 * h, v, hs);
       }
     }
 #pragma unroll
@@ -769,9 +954,9 @@ __global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(const __grid_consta
       }
 #pragma unroll
       for (int i = 0; i < 8; ++i) v[i] *= sep[3 + br];
-      store_cols<128, 8>(c.head, c.t, 96 + 8 * br, v);
+      store_q<F8, 128, 8>(c.head, c.t, 96 + 8 * br, v, hs);
     }
-    store_cols<128, 8>(c.head, c.t, 120, x8);
+    store_q<F8, 128, 8>(c.head, c.t, 120, x8, hs);
     // heads: channel 0, then the further distinct channels of the tile
     float X[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll 1
@@ -782,9 +967,10 @@ __global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(const __grid_consta
           c.ok = false;
           break;
         }
-        head_input_spilled(c, w, a.spill, cap, row < n ? row : 0, fin, gg, gamma, ch == 1 ? srp[1] : srp[2]);
+        hs = 1.0f / head_input_spilled<F8>(c, w, a.spill, cap, row < n ? row : 0, fin, gg, gamma,
+                                               ch == 1 ? srp[1] : srp[2]);
       }
-      const float x = head_chain(c, w);
+      const float x = head_chain<F8>(c, w, winv, 1.0f / hs);
       if (ch == 0) X[0] = x;
       else if (ch == 1) X[1] = x;
       else X[2] = x;
@@ -876,6 +1062,58 @@ __global__ void __launch_bounds__(128, 1) k_tc_selftest(const uint16_t* __restri
   }
 }
 
+// The same through the E4M3 path: D[128 x N] = A[128 x K] * B[N x K]^T with
+// 8-bit operands (kind::f8f6f4).
+template <int N, int K>
+__global__ void __launch_bounds__(128, 1) k_tc_selftest8(const uint8_t* __restrict__ A, const uint8_t* __restrict__ B,
+                                                         float* __restrict__ D, int* err) {
+  extern __shared__ __align__(1024) uint8_t dsm[];
+  uint8_t* sa = dsm;
+  uint8_t* sb = dsm + 128 * K;
+  uint64_t& mbar = *reinterpret_cast<uint64_t*>(dsm + 128 * K + N * K);
+  uint32_t& holder = *reinterpret_cast<uint32_t*>(dsm + 128 * K + N * K + 8);
+  const int t = threadIdx.x, warp = t >> 5;
+  for (int k = 0; k < K; ++k) {
+    sa[qoff<true>(t, k, K)] = A[t * K + k];
+    if (t < N) sb[qoff<true>(t, k, K)] = B[t * K + k];
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&holder)),
+                 "r"(128));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (t == 0) mbar_init(smem_u32(&mbar), 1);
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = holder;
+  if (t == 0) {
+    issue_q<true, N, K>(tmem, smem_u32(sa), smem_u32(sb));
+    umma_commit(smem_u32(&mbar));
+  }
+  const bool ok = mbar_wait(smem_u32(&mbar), 0);
+  tc_fence_after();
+  if (ok) {
+    float v[16];
+#pragma unroll
+    for (int h = 0; h < N / 16; ++h) {
+      tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + 16 * h, v);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) D[t * N + 16 * h + i] = v[i];
+    }
+  } else if (t == 0) {
+    atomicExch(err, 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128));
+  }
+}
+
 // ---- host ----------------------------------------------------------------------
 static uint16_t to_bf16_bits(float f) {
   uint32_t u;
@@ -885,12 +1123,49 @@ static uint16_t to_bf16_bits(float f) {
   return (uint16_t)(u >> 16);
 }
 
+// OCP FP8 E4M3 encoding of f (1 sign, 4 exponent bits with bias 7, 3 mantissa
+// bits; no infinities; largest finite 448), round to nearest even,
+// saturating. Written from the format definition.
+static uint8_t to_e4m3(float f) {
+  const uint8_t sign = std::signbit(f) ? 0x80 : 0x00;
+  const float a = std::fabs(f);
+  if (std::isnan(f)) return 0x7f;
+  if (a >= 448.0f) return sign | 0x7e;
+  if (a < 0.015625f) {  // below 2^-6: subnormal, units of 2^-9
+    const int q = (int)std::nearbyint(a * 512.0f);  // 0..8; 8 is the smallest normal (exponent field 1)
+    return sign | (uint8_t)q;
+  }
+  int e;
+  std::frexp(a, &e);                                  // a = m 2^e, m in [0.5, 1)
+  const float mant = std::ldexp(a, 1 - e);            // [1, 2)
+  int q = (int)std::nearbyint((mant - 1.0f) * 8.0f);  // 0..8
+  int E = e + 6;                                      // biased exponent of 2^(e-1)
+  if (q == 8) { q = 0; ++E; }
+  if (E > 15 || (E == 15 && q == 7)) return sign | 0x7e;
+  return sign | (uint8_t)((E << 3) | q);
+}
+
 int pack_network(Network* n) {
   std::vector<float> w(MR_WEIGHT_TOTAL);
   if (cudaMemcpy(w.data(), n->w, MR_WEIGHT_TOTAL * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
     return set_error(MR_ERR_CUDA, "pack_network: weight read-back failed");
-  std::vector<uint8_t> img(kWBytes, 0);
+  std::vector<uint8_t> img(kWBytes, 0), img8(kW8Bytes, 0);
   const WeightTable wt = make_weight_table();
+  // E4M3 image: per layer, weights times a power-of-two scale that maps the
+  // largest |w| to at most 448
+  n->h_winv8.assign(kTcLayers, 1.0f);
+  for (int i = 0; i < kTcLayers; ++i) {
+    const TcLayer& L = kTc[i];
+    const float* W = w.data() + wt.off[L.w];
+    float m = 0.0f;
+    for (int j = 0; j < L.n * L.k; ++j) m = std::max(m, std::fabs(W[j]));
+    const float sc = m > 0.0f ? std::ldexp(1.0f, (int)std::floor(std::log2(448.0f / m))) : 1.0f;
+    n->h_winv8[i] = 1.0f / sc;
+    const int kp = kp8(L.k);
+    uint8_t* base = img8.data() + tc_offset8(i);
+    for (int r = 0; r < L.n; ++r)
+      for (int k = 0; k < L.k; ++k) base[qoff<true>(r, k, kp)] = to_e4m3(W[k + r * L.k] * sc);
+  }
   for (int i = 0; i < kTcLayers; ++i) {
     const TcLayer& L = kTc[i];
     const int kp = pad16(L.k);
@@ -907,9 +1182,12 @@ int pack_network(Network* n) {
   n->h_rowwise.assign(kRowFloats, 0.0f);
   for (int id = 0; id < MR_W_COUNT; ++id)
     if (rt.off[id] >= 0) std::memcpy(&n->h_rowwise[rt.off[id]], w.data() + wt.off[id], wt.size[id] * sizeof(float));
-  cudaError_t e = cudaMalloc(&n->packed, kWBytes + 256);
+  // [BF16 image | error word (256 B) | E4M3 image]
+  cudaError_t e = cudaMalloc(&n->packed, kWBytes + 256 + kW8Bytes);
   if (e == cudaSuccess) e = cudaMemcpy(n->packed, img.data(), kWBytes, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset((uint8_t*)n->packed + kWBytes, 0, 256);
+  if (e == cudaSuccess)
+    e = cudaMemcpy((uint8_t*)n->packed + kWBytes + 256, img8.data(), kW8Bytes, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return set_error(MR_ERR_NOMEM, "pack_network: %s", cudaGetErrorString(e));
   n->packed_bytes = kWBytes;
   return MR_OK;
@@ -927,13 +1205,14 @@ void free_packed(Network* n) {
 // error word. The error word lives after the packed image.
 int launch_mlp_tc(const Network* net, const float* desc, const float* aux, long long rs, long long cs,
                   long long ars, long long afs, int n, float* out, const int* pix, const float* trph,
-                  const unsigned* count, F3 light_color, F3 scatter, float* spill, cudaStream_t s,
+                  const unsigned* count, F3 light_color, F3 scatter, float* spill, bool f8, cudaStream_t s,
                   const int* job, const BatchOut* bout) {
   if (cs * 4 > 0x7FFFFFFFll || n > (1 << 28))
     return set_error(MR_ERR_ARG, "tensor-core network: %d rows / chunk stride %lld out of range", n, cs);
   static bool attr = false;
   if (!attr) {
-    MR_CUDA(cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+    MR_CUDA(cudaFuncSetAttribute(k_mlp_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes<false>()));
+    MR_CUDA(cudaFuncSetAttribute(k_mlp_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes<true>()));
     attr = true;
   }
   TcArgs a;
@@ -958,10 +1237,13 @@ int launch_mlp_tc(const Network* net, const float* desc, const float* aux, long 
   a.bout = bout;
   if (net->h_rowwise.size() != (size_t)kRowFloats) return set_error(MR_ERR_STATE, "network not packed");
   std::memcpy(a.rw, net->h_rowwise.data(), sizeof(a.rw));
+  a.wpack8 = (const uint8_t*)net->packed + kWBytes + 256;
+  for (int i = 0; i < kTcLayers; ++i) a.winv[i] = f8 ? net->h_winv8[i] : 1.0f;
   a.err = (int*)((uint8_t*)net->packed + kWBytes);
   int tiles = (n + 127) / 128;
   int grid = std::min(sm_count(), std::max(1, (tiles + kGroups - 1) / kGroups));
-  k_mlp_tc<<<grid, 128 * kGroups, kSmemBytes, s>>>(a);
+  if (f8) k_mlp_tc<true><<<grid, 128 * kGroups, smem_bytes<true>(), s>>>(a);
+  else k_mlp_tc<false><<<grid, 128 * kGroups, smem_bytes<false>(), s>>>(a);
   MR_CUDA(cudaGetLastError());
   return MR_OK;
 }
@@ -1008,6 +1290,44 @@ extern "C" int mr_tc_selftest(int32_t n, int32_t k, const uint16_t* host_a, cons
   int he = 0;
   if (rc == MR_OK) cudaMemcpy(&he, err, 4, cudaMemcpyDeviceToHost);
   if (rc == MR_OK && he) rc = set_error(MR_ERR_TIMEOUT, "tc selftest: mbarrier wait timed out");
+  if (rc == MR_OK) cudaMemcpy(host_d, d, 128 * n * 4, cudaMemcpyDeviceToHost);
+  cudaFree(a);
+  cudaFree(b);
+  cudaFree(d);
+  cudaFree(err);
+  return rc;
+}
+
+extern "C" int mr_tc_selftest_fp8(int32_t n, int32_t k, const uint8_t* host_a, const uint8_t* host_b, float* host_d) {
+  clear_error();
+  if (!host_a || !host_b || !host_d) return set_error(MR_ERR_ARG, "mr_tc_selftest_fp8: NULL argument");
+  uint8_t *a = nullptr, *b = nullptr;
+  float* d = nullptr;
+  int* err = nullptr;
+  MR_CUDA(cudaMalloc(&a, 128 * k));
+  MR_CUDA(cudaMalloc(&b, n * k));
+  MR_CUDA(cudaMalloc(&d, 128 * n * 4));
+  MR_CUDA(cudaMalloc(&err, 4));
+  MR_CUDA(cudaMemset(err, 0, 4));
+  MR_CUDA(cudaMemcpy(a, host_a, 128 * k, cudaMemcpyHostToDevice));
+  MR_CUDA(cudaMemcpy(b, host_b, n * k, cudaMemcpyHostToDevice));
+  int rc = MR_OK;
+  const int sm = 128 * k + n * k + 16;
+#define MR_SELFTEST8(NN, KK)                                                                       \
+  if (n == NN && k == KK) {                                                                        \
+    cudaFuncSetAttribute(k_tc_selftest8<NN, KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); \
+    k_tc_selftest8<NN, KK><<<1, 128, sm>>>(a, b, d, err);                                          \
+  } else
+  MR_SELFTEST8(16, 32) MR_SELFTEST8(32, 32) MR_SELFTEST8(64, 128) MR_SELFTEST8(128, 128)
+  rc = set_error(MR_ERR_ARG, "mr_tc_selftest_fp8: shape %dx%d not built", n, k);
+#undef MR_SELFTEST8
+  if (rc == MR_OK) {
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) rc = cuda_error(e, "tc selftest fp8");
+  }
+  int he = 0;
+  if (rc == MR_OK) cudaMemcpy(&he, err, 4, cudaMemcpyDeviceToHost);
+  if (rc == MR_OK && he) rc = set_error(MR_ERR_TIMEOUT, "tc selftest fp8: mbarrier wait timed out");
   if (rc == MR_OK) cudaMemcpy(host_d, d, 128 * n * 4, cudaMemcpyDeviceToHost);
   cudaFree(a);
   cudaFree(b);

@@ -370,7 +370,7 @@ __global__ void __launch_bounds__(128) k_gather_fm(Tables t, const float* __rest
 
 int launch_mlp_tc(const Network* net, const float* desc, const float* aux, long long rs, long long cs,
                   long long ars, long long afs, int n, float* out, const int* pix, const float* trph,
-                  const unsigned* count, F3 light_color, F3 scatter, float* spill, cudaStream_t s,
+                  const unsigned* count, F3 light_color, F3 scatter, float* spill, bool f8, cudaStream_t s,
                   const int* job = nullptr, const BatchOut* bout = nullptr);
 int launch_mlp_simt(const Network* net, const float* desc, const float* aux, long long rs, long long cs,
                     long long ars, long long afs, int n, const unsigned* count, float* out, const int* pix,
@@ -425,8 +425,8 @@ static int render_neural_impl(Volume* v, const Network* net, const mr_render_par
   if (!net) return set_error(MR_ERR_ARG, "MRPNN render needs a network (mr_network_create)");
   if (!v->data_set) return set_error(MR_ERR_STATE, "render before mr_volume_set_data");
   if (!v->mips_valid) return set_error(MR_ERR_STATE, "render before mr_volume_update");
-  if (p->precision != MR_PREC_FP32 && p->precision != MR_PREC_BF16)
-    return set_error(MR_ERR_UNSUPPORTED, "precision %d not built", p->precision);
+  if (p->precision != MR_PREC_FP32 && p->precision != MR_PREC_BF16 && p->precision != MR_PREC_FP8)
+    return set_error(MR_ERR_ARG, "unknown precision %d", p->precision);
   F3 L = normalize(to_f3(p->light_dir));
   // UpdateHGLut / Update_TR on demand (core/volume.cu:434-437).
   if (!v->lut_valid || v->lut_g != p->g || v->lut_seed != p->seed) {
@@ -451,7 +451,7 @@ static int neural_passes(Volume* v, const Network* net, const mr_render_params* 
   int rc = MR_OK;
   const F3 L = normalize(to_f3(p->light_dir));
   const size_t npx = (size_t)p->width * p->height;
-  const bool tc = p->precision == MR_PREC_BF16;
+  const bool tc = p->precision != MR_PREC_FP32;
   // records, then the feature-major descriptor and aux columns
   const size_t rbytes = records_round(npx);
   Records rec = carve_records(base, npx);
@@ -497,7 +497,7 @@ static int neural_passes(Volume* v, const Network* net, const mr_render_params* 
   mark(ST_NN_MLP);
   if (tc)
     rc = launch_mlp_tc(net, desc, aux, 4, 4 * cap, 1, cap, (int)npx, dev_rgb, rec.pix, rec.trph, rec.count,
-                       to_f3(p->light_color), to_f3(p->scatter_rate), spill, s);
+                       to_f3(p->light_color), to_f3(p->scatter_rate), spill, p->precision == MR_PREC_FP8, s);
   else
     rc = launch_mlp_simt(net, desc, aux, 4, 4 * cap, 1, cap, (int)npx, rec.count, dev_rgb, rec.pix, rec.trph,
                          to_f3(p->light_color), to_f3(p->scatter_rate), s);
@@ -536,18 +536,18 @@ extern "C" int mr_radiance_predict(const mr_network* nh, int32_t precision, cons
   if (n == 0) return MR_OK;
   if (reinterpret_cast<uintptr_t>(dev_desc) & 15)
     return set_error(MR_ERR_ARG, "mr_radiance_predict: dev_desc must be 16-byte aligned");
-  if (precision == MR_PREC_BF16) {
+  if (precision == MR_PREC_BF16 || precision == MR_PREC_FP8) {
     // rows may carry distinct albedo channels: spill space for further heads
     cudaStream_t s = (cudaStream_t)stream;
     float* spill = nullptr;
     cudaError_t e = cudaMallocAsync(&spill, (size_t)n * 120 * sizeof(float), s);
     if (e != cudaSuccess) return set_error(MR_ERR_NOMEM, "spill allocation failed: %s", cudaGetErrorString(e));
     int rc = launch_mlp_tc(&nh->n, dev_desc, dev_aux, 576, 4, 5, 1, n, dev_out, nullptr, nullptr, nullptr,
-                           f3(1, 1, 1), f3(1, 1, 1), spill, s);
+                           f3(1, 1, 1), f3(1, 1, 1), spill, precision == MR_PREC_FP8, s);
     MR_CUDA(cudaFreeAsync(spill, s));
     return rc;
   }
-  if (precision != MR_PREC_FP32) return set_error(MR_ERR_UNSUPPORTED, "precision %d not built", precision);
+  if (precision != MR_PREC_FP32) return set_error(MR_ERR_ARG, "unknown precision %d", precision);
   return launch_mlp_simt(&nh->n, dev_desc, dev_aux, 576, 4, 5, 1, n, nullptr, dev_out, nullptr, nullptr, f3(1, 1, 1),
                          f3(1, 1, 1), (cudaStream_t)stream);
 }
@@ -592,7 +592,8 @@ extern "C" int mr_render_neural_noalloc(mr_volume* h, const mr_network* nh, cons
   if (p->render_type != MR_RT_MRPNN)
     return set_error(MR_ERR_ARG, "mr_render_neural_noalloc renders MR_RT_MRPNN only (got %d)", p->render_type);
   if (p->precision != MR_PREC_FP32 && p->precision != MR_PREC_BF16)
-    return set_error(MR_ERR_UNSUPPORTED, "precision %d not built", p->precision);
+    return set_error(MR_ERR_UNSUPPORTED, "mr_render_neural_noalloc supports MR_PREC_FP32 and MR_PREC_BF16 (got %d)",
+                     p->precision);
   if (p->sampler != MR_SAMPLER_EXACT)
     return set_error(MR_ERR_ARG, "mr_render_neural_noalloc supports MR_SAMPLER_EXACT only "
                                  "(texture tables are allocated on first use)");
@@ -743,7 +744,7 @@ static int batch_launches(Batch& b, const Network* net, cudaStream_t s) {
   float* aux = desc + cap * 576;
   float* spill = b.spill ? aux + cap * 5 : nullptr;
   rec.job = (int*)((char*)b.scratch + neural_scratch_bytes(cap, b.spill));
-  const bool tc = b.precision == MR_PREC_BF16;
+  const bool tc = b.precision != MR_PREC_FP32;
   const bool hw = b.sampler == MR_SAMPLER_TEXTURE;
   const int nj = (int)b.jobs.size();
   MR_CUDA(cudaMemsetAsync(b.counters, 0, kCounters * sizeof(unsigned long long), s));
@@ -763,7 +764,7 @@ static int batch_launches(Batch& b, const Network* net, cudaStream_t s) {
     int rc;
     if (tc)
       rc = launch_mlp_tc(net, desc, aux, 4, 4 * ccap, 1, ccap, (int)cap, nullptr, rec.pix, rec.trph, rec.count,
-                         f3(1, 1, 1), f3(1, 1, 1), spill, s, rec.job, b.d_out);
+                         f3(1, 1, 1), f3(1, 1, 1), spill, b.precision == MR_PREC_FP8, s, rec.job, b.d_out);
     else
       rc = launch_mlp_simt(net, desc, aux, 4, 4 * ccap, 1, ccap, (int)cap, rec.count, nullptr, rec.pix, rec.trph,
                            f3(1, 1, 1), f3(1, 1, 1), s, rec.job, b.d_out);
@@ -830,8 +831,8 @@ extern "C" int mr_batch_prepare(mr_batch* h, const mr_network* nh, int64_t wave_
   b.drop_graph();
   b.precision = b.jobs[0].p.precision;
   b.sampler = b.jobs[0].p.sampler;
-  if (b.precision != MR_PREC_FP32 && b.precision != MR_PREC_BF16)
-    return set_error(MR_ERR_UNSUPPORTED, "precision %d not built", b.precision);
+  if (b.precision != MR_PREC_FP32 && b.precision != MR_PREC_BF16 && b.precision != MR_PREC_FP8)
+    return set_error(MR_ERR_ARG, "unknown precision %d", b.precision);
   std::vector<BatchJob> hj(b.jobs.size());
   std::vector<BatchOut> ho(b.jobs.size());
   long long off = 0;

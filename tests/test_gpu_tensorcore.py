@@ -137,3 +137,64 @@ def test_bf16_neural_render_close_to_fp32():
     assert np.median(rel) < 0.05
     assert ((a == 0) == (b == 0)).all()
     v.close()
+
+
+# ---- E4M3 (MR_PREC_FP8) -------------------------------------------------------------
+
+def _e4m3_encode(x):
+    """OCP E4M3 bytes of x (round to nearest even, saturating at 448)."""
+    x = np.asarray(x, np.float64)
+    out = np.zeros(x.shape, np.uint8)
+    for idx, v in np.ndenumerate(x):
+        s = 0x80 if v < 0 else 0
+        a = min(abs(v), 448.0)
+        if a < 2.0 ** -6:
+            out[idx] = s | int(np.rint(a * 512))
+            continue
+        e = int(np.floor(np.log2(a)))
+        q = int(np.rint((a / 2.0 ** e - 1) * 8))
+        if q == 8:
+            q, e = 0, e + 1
+        out[idx] = s | ((e + 7) << 3) | q
+    return out
+
+
+def _e4m3_value(b):
+    b = np.asarray(b, np.int32)
+    sgn = np.where(b & 0x80, -1.0, 1.0)
+    E, q = (b >> 3) & 15, b & 7
+    return sgn * np.where(E == 0, q * 2.0 ** -9, (1 + q / 8.0) * 2.0 ** (E - 7.0))
+
+
+@pytest.mark.parametrize("n,k", [(16, 32), (32, 32), (64, 128), (128, 128)])
+def test_fp8_tile_product_matches_matmul(n, k):
+    from internship_b200 import _lib
+    rng = np.random.default_rng(n * 7 + k)
+    a = _e4m3_encode(rng.uniform(-8, 8, (128, k)))
+    b = _e4m3_encode(rng.uniform(-2, 2, (n, k)))
+    d = np.zeros((128, n), np.float32)
+    _lib.check(_lib.load().mr_tc_selftest_fp8(n, k, a.ctypes.data, b.ctypes.data, d.ctypes.data))
+    ref = _e4m3_value(a) @ _e4m3_value(b).T  # E4M3 products are exact in FP32
+    np.testing.assert_allclose(d, ref, rtol=1e-5, atol=1e-5 * k)
+
+
+def test_fp8_network_close_to_fp32():
+    """E4M3 operands carry 3 mantissa bits (up to 6 % rounding error per
+    operand): through ~30 dependent layers the per-layer / per-row scaled
+    network stays within a few percent of the fp32 oracle on X (a wrong scale
+    would be off by a power of two)."""
+    import internship_b200 as mr
+    from internship_b200.weights import active_random_weights
+    w = active_random_weights(1)
+    desc, aux = _descriptors(512, 6)
+    ref = orc.predict(w, desc, aux)
+    f8 = _predict(mr, w, desc, aux, 2)
+    bf = _predict(mr, w, desc, aux, 1)
+    d8, db = _compare(f8, ref), _compare(bf, ref)
+    xr = np.log1p(ref / np.float32((0.99 / 1.001) ** 4))
+    rel8 = d8 / np.maximum(xr, 1e-3)
+    print("median |dX| fp8 %.4f bf16 %.4f, median rel fp8 %.4f" % (np.median(d8), np.median(db), np.median(rel8)))
+    assert np.all(np.isfinite(f8)) and (f8 > 0).mean() > 0.5
+    assert np.median(rel8) < 0.08
+    assert np.quantile(rel8, 0.99) < 0.3
+    assert np.median(d8) > np.median(db)  # coarser than BF16, as it must be
