@@ -367,7 +367,7 @@ def main():
 
     torch.cuda.set_device(local)
     import internship_b200 as mr
-    from internship_b200 import _lib, scenes
+    from internship_b200 import _lib, replicas, scenes
     L = _lib.load()
     stream = torch.cuda.current_stream().cuda_stream
     sp = C.c_void_p(stream)
@@ -384,7 +384,7 @@ def main():
     w, st = mr.xavier_weights(1), mr.builtin_stencil()
     v.SetWeights(w, st)
     net = v.network.handle
-    p = scenes.cloud_scene_params(WIDTH, HEIGHT, seed=rank)
+    p = scenes.cloud_scene_params(WIDTH, HEIGHT, seed=replicas.frame_seed(rank))
     out = torch.empty(WIDTH * HEIGHT * 3, device="cuda", dtype=torch.float32)
     flush = torch.empty(256 * 1024 * 1024 // 4, device="cuda", dtype=torch.float32)
 
@@ -422,9 +422,7 @@ def main():
         cnt = (C.c_uint64 * 4)()
         _lib.check(L.mr_volume_counters(v.handle, cnt))
         if dist is not None:
-            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+            ms = replicas.slowest_ms(ms, dist, "cuda")
             dist.barrier()
         per = [st_ms[i] / max(1, st_n[i]) for i in range(8)]
         return {"ms": ms, "stage": per, "launches": int(sum(st_n[i] for i in range(8))),
@@ -435,7 +433,7 @@ def main():
     head = leg(_lib.PREC_FP32, _lib.SAMPLER_EXACT, 0)
     clk = clocks.stop()
     ms, active, fetches = head["ms"], head["active"], head["fetches"]
-    fps = world * args.steps / (ms / 1000.0)
+    fps = replicas.throughput(args.steps, world, ms)
     # the same frames with texture-unit sampling and with the BF16 tensor-core network
     legs = {"fp32_texture": leg(_lib.PREC_FP32, _lib.SAMPLER_TEXTURE, 1000),
             "bf16_exact": leg(_lib.PREC_BF16, _lib.SAMPLER_EXACT, 2000),
@@ -454,11 +452,8 @@ def main():
     e1.record()
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_fps = world * args.steps / (e2e_ms / 1000.0)
+    e2e_ms = replicas.slowest_ms(e2e_ms, dist, "cuda")
+    e2e_fps = replicas.throughput(args.steps, world, e2e_ms)
 
     hbm, bf16, src = peaks()
     trace_ms, gather_ms, mlp_ms32 = head["stage"][1], head["stage"][2], head["stage"][6]
@@ -494,7 +489,8 @@ def main():
         tc = not name.startswith("fp32")
         tf = FLOP_PER_PIXEL * lg["active"] / (m_ms / 1e3) / 1e12
         variants[name] = {
-            "value": world * args.steps / (lg["ms"] / 1000.0), "unit": "frames/s", "ms_per_step": lg["ms"] / args.steps,
+            "value": replicas.throughput(args.steps, world, lg["ms"]), "unit": "frames/s",
+            "ms_per_step": lg["ms"] / args.steps,
             "stages_ms_per_step": {"nn_trace": lg["stage"][1], "nn_gather": g_ms, "nn_network": m_ms},
             "gather": {"bound": "hbm", "achieved": lg["active"] * (384 * 32 + 383 * 16 + 581 * 4) / (g_ms / 1e3) / 1e9,
                        "peak": hbm, "unit": "GB/s"},
