@@ -9,7 +9,9 @@
 // branches of a block are evaluated together (three independent FMA chains),
 // and blocks of equal width share one code instance through a runtime loop
 // over their weight offsets. Weights are read as warp-uniform float4 loads.
-// The 128-wide head vectors live in per-thread shared-memory columns.
+// The head (LC0 128x128, LC1, LC2: 62 % of the multiply-adds) runs in a second
+// kernel as block GEMMs over shared-memory activation tiles, so that no
+// 128-wide vector has to live in a thread's registers.
 #include "mr_internal.h"
 #include "mr_net_layout.cuh"
 
@@ -36,49 +38,66 @@ struct SimtArgs {
 __device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
 __device__ __forceinline__ float relu0(float x) { return x >= 0.0f ? x : 0.0f; }
 
-// y_b = ReLU(B_b + W_b x_b) for three branches b, S x S, bias first then
-// ascending inputs (LinearReLU<S> / LinearReLU_SFL order).
-template <int S>
-__device__ __forceinline__ void dense3(const float (&x)[3][32], float (&y)[3][32], const float* __restrict__ w,
-                                       int w0, int w1, int w2) {
-  const float* W[3] = {w + w0, w + w1, w + w2};
-#pragma unroll
-  for (int i = 0; i < S; ++i) {
-    float acc[3];
-#pragma unroll
-    for (int b = 0; b < 3; ++b) acc[b] = __ldg(W[b] + S * S + i);
-#pragma unroll
-    for (int j = 0; j < S; j += 4) {
-#pragma unroll
-      for (int b = 0; b < 3; ++b) {
-        float4 q = ldg4(W[b] + i * S + j);
-        acc[b] += x[b][j] * q.x;
-        acc[b] += x[b][j + 1] * q.y;
-        acc[b] += x[b][j + 2] * q.z;
-        acc[b] += x[b][j + 3] * q.w;
-      }
-    }
-#pragma unroll
-    for (int b = 0; b < 3; ++b) y[b][i] = relu0(acc[b]);
-  }
-}
-
+// One descriptor row; the address of each chunk is formed inside the asm so
+// that the compiler does not keep a row address per feature live for reuse
+// (each feature is read three times: statistics, block input, residual).
 struct RowIO {
   const float* __restrict__ d;
-  long long cs;
+  int cs16;  // chunk stride in bytes
   // features i..i+3, i a multiple of 4
   __device__ __forceinline__ float4 ld4(int i) const {
-    return __ldg(reinterpret_cast<const float4*>(d + (i >> 2) * cs));
+    float4 v;
+    asm volatile(
+        "{\n\t.reg .u64 a;\n\tmad.wide.s32 a, %4, %5, %6;\n\tld.global.nc.v4.f32 {%0,%1,%2,%3}, [a];\n\t}\n"
+        : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+        : "r"(i >> 2), "r"(cs16), "l"(d));
+    return v;
   }
 };
 
+// yn = ReLU(B + W x) for one branch, S x S (bias stored after W): bias first,
+// then ascending inputs (LinearReLU<S> order), four outputs interleaved.
+template <int S>
+__device__ __forceinline__ void dense1(const float* x, float* yn, const float* __restrict__ W) {
+#pragma unroll
+  for (int i0 = 0; i0 < S; i0 += 4) {
+    float acc[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] = __ldg(W + S * S + i0 + q);
+#pragma unroll
+    for (int j = 0; j < S; j += 4) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const float4 wv = ldg4(W + (i0 + q) * S + j);
+        acc[q] += x[j] * wv.x;
+        acc[q] += x[j + 1] * wv.y;
+        acc[q] += x[j + 2] * wv.z;
+        acc[q] += x[j + 3] * wv.w;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) yn[i0 + q] = relu0(acc[q]);
+  }
+}
+
 // SE / SERES block of width S (radiancePredict.cu:240-294). MODE 0: SE +
-// ADD3, 1: SERES + ADD3, 2: SERES + REP3. Weight offsets are runtime values
-// so that blocks of equal width and mode share this code.
+// ADD3, 1: SERES + ADD3, 2: SERES + REP3. The block's pooled statistics
+// (pool[pid+b], pool[36+pid+b]) go straight into the 16 LSEFin1 sums `fin`;
+// the three branches are evaluated one after another to keep register
+// pressure low. Weight offsets are runtime values so that blocks of equal
+// width and mode share this code.
+// The running trunk state y of a row (3 branches x up to 32 values) in
+// shared memory, one column per thread: conflict-free, and out of the
+// registers, which hold one branch's input and output at a time.
+struct YS {
+  float* p;  // smem base + thread index
+  __device__ __forceinline__ float& at(int b, int i) const { return p[(b * 32 + i) * kSimtThreads]; }
+};
+
 template <int S, int MODE>
 __device__ __forceinline__ void simt_block(const RowIO& in, const float* __restrict__ w, int from, int pid, int sew0,
-                                           int sew1, int wa, int wb, int wc, float g, float gamma,
-                                           float (&y)[3][32], float (&pool)[75]) {
+                                           int sew1, int wa, int wb, int wc, float g, float gamma, const YS& y,
+                                           float (&fin)[16]) {
   float mean[3], mx[3];
 #pragma unroll
   for (int b = 0; b < 3; ++b) {
@@ -92,15 +111,18 @@ __device__ __forceinline__ void simt_block(const RowIO& in, const float* __restr
     mean[b] = s / (float)S;
     mx[b] = m;
   }
-  // pool[pid + b] and pool[36 + pid + b]: written through a small switch-free
-  // store into the register array (pid is one of 12 known values).
+  const float* f1 = w + WOFF(LSEFin1W);
 #pragma unroll
-  for (int q = 0; q < 36; q += 3)
-    if (q == pid) {
+  for (int j = 0; j < 16; ++j) {
+    float acc = fin[j];
 #pragma unroll
-      for (int b = 0; b < 3; ++b) { pool[q + b] = mean[b]; pool[36 + q + b] = mx[b]; }
+    for (int b = 0; b < 3; ++b) {
+      acc += mean[b] * __ldg(f1 + j * 75 + pid + b);
+      acc += mx[b] * __ldg(f1 + j * 75 + 36 + pid + b);
     }
-  float tmp[8] = {mean[0], mean[1], mean[2], mx[0], mx[1], mx[2], g, gamma};
+    fin[j] = acc;
+  }
+  const float tmp[8] = {mean[0], mean[1], mean[2], mx[0], mx[1], mx[2], g, gamma};
   float h[8];
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
@@ -117,23 +139,21 @@ __device__ __forceinline__ void simt_block(const RowIO& in, const float* __restr
     for (int j = 0; j < 8; ++j) a += h[j] * __ldg(w + sew1 + j + i * 8);
     gate[i] = 1.0f / (1.0f + expf(-a));
   }
-  float x[3][32];
+  const int wofs[3] = {wa, wb, wc};
 #pragma unroll
-  for (int b = 0; b < 3; ++b)
+  for (int b = 0; b < 3; ++b) {
+    float x[32], yn[32];
 #pragma unroll
     for (int i = 0; i < S; i += 4) {
       const float4 q = in.ld4(b * 192 + from + i);
       const float qv[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
-        float v = qv[u] * gate[b];
-        x[b][i + u] = MODE == 0 ? v : v + y[b][i + u];
+        const float v = qv[u] * gate[b];
+        x[i + u] = MODE == 0 ? v : v + y.at(b, i + u);
       }
     }
-  float yn[3][32];
-  dense3<S>(x, yn, w, wa, wb, wc);
-#pragma unroll
-  for (int b = 0; b < 3; ++b)
+    dense1<S>(x, yn, w + wofs[b]);
 #pragma unroll
     for (int i = 0; i < S; i += 4) {
       const float4 q = in.ld4(b * 192 + from + i);
@@ -141,42 +161,13 @@ __device__ __forceinline__ void simt_block(const RowIO& in, const float* __restr
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         if (MODE == 2) {
-          y[b][i + u] = yn[b][i + u];
-          y[b][S + i + u] = qv[u];
+          y.at(b, i + u) = yn[i + u];
+          y.at(b, S + i + u) = qv[u];
         } else {
-          y[b][i + u] = yn[b][i + u] + qv[u];
+          y.at(b, i + u) = yn[i + u] + qv[u];
         }
       }
     }
-}
-
-// out[i] = ReLU(B[i] + sum_j in[j] W[i*FROM + j]): the FROM inputs are
-// loaded into registers once (compile-time indices), the TO outputs are
-// produced 8 per loop trip and stored with a runtime index.
-template <int FROM, int TO>
-__device__ __forceinline__ void dense_loc(const float* in, float* out, const float* __restrict__ W,
-                                          const float* __restrict__ B) {
-  float x[FROM];
-#pragma unroll
-  for (int j = 0; j < FROM; ++j) x[j] = in[j];
-#pragma unroll 1
-  for (int i0 = 0; i0 < TO; i0 += 8) {
-    float acc[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) acc[q] = __ldg(B + i0 + q);
-#pragma unroll
-    for (int j = 0; j < FROM; j += 4) {
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        float4 wv = ldg4(W + (i0 + q) * FROM + j);
-        acc[q] += x[j] * wv.x;
-        acc[q] += x[j + 1] * wv.y;
-        acc[q] += x[j + 2] * wv.z;
-        acc[q] += x[j + 3] * wv.w;
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < 8; ++q) out[i0 + q] = relu0(acc[q]);
   }
 }
 
@@ -198,109 +189,42 @@ __device__ __forceinline__ void dense16(const float (&x)[16], float (&y)[16], co
   }
 }
 
-// Head SC(p) for one albedo channel (radiancePredict.cu:439-473) from the raw
-// comb[0..120) and the pooled statistics; returns the pre-exponential X.
-__device__ __noinline__ float simt_head(const float* comb, const float (&pool)[75], float srpc,
-                                        const float* __restrict__ w) {
-  float hA[128], hB[128];
-#pragma unroll
-  for (int i = 0; i < 120; ++i) hA[i] = comb[i];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {  // LGGS 3 -> 8, bias after the sum
-    float acc = pool[72] * __ldg(w + WOFF(LGGSW) + 3 * i) + pool[73] * __ldg(w + WOFF(LGGSW) + 3 * i + 1) +
-                srpc * __ldg(w + WOFF(LGGSW) + 3 * i + 2);
-    acc += __ldg(w + WOFF(LGGSB) + i);
-    hA[120 + i] = relu0(acc);
-  }
-  float sew[16];
-#pragma unroll
-  for (int j = 0; j < 16; ++j) {  // LSEFin1 75 -> 16 (pool[74] = srp)
-    float acc = 0.0f;
-#pragma unroll
-    for (int i = 0; i < 74; ++i) acc += pool[i] * __ldg(w + WOFF(LSEFin1W) + j * 75 + i);
-    acc += srpc * __ldg(w + WOFF(LSEFin1W) + j * 75 + 74);
-    sew[j] = relu0(acc);
-  }
-  float sep[6];
-#pragma unroll
-  for (int i = 0; i < 6; ++i) {  // LSEFin2 16 -> 6
-    float acc = 0.0f;
-#pragma unroll
-    for (int j = 0; j < 16; ++j) acc += sew[j] * __ldg(w + WOFF(LSEFin2W) + j + i * 16);
-    sep[i] = 1.0f / (1.0f + expf(-acc));
-  }
-#pragma unroll
-  for (int i = 0; i < 32; ++i) { hA[i] *= sep[0]; hA[32 + i] *= sep[1]; hA[64 + i] *= sep[2]; }
-#pragma unroll
-  for (int i = 0; i < 8; ++i) { hA[96 + i] *= sep[3]; hA[104 + i] *= sep[4]; hA[112 + i] *= sep[5]; }
-  dense_loc<128, 128>(hA, hB, w + WOFF(LC0W), w + WOFF(LC0B));
-  dense_loc<128, 64>(hB, hA, w + WOFF(LC1W), w + WOFF(LC1B));
-  dense_loc<64, 32>(hA, hB, w + WOFF(LC2W), w + WOFF(LC2B));
-  float x32[32];
-#pragma unroll
-  for (int i = 0; i < 32; ++i) x32[i] = hB[i];
-  float a16[16];
-#pragma unroll
-  for (int i = 0; i < 16; ++i) {  // LX 32 -> 16
-    float acc = __ldg(w + WOFF(LXB) + i);
-#pragma unroll
-    for (int j = 0; j < 32; j += 4) {
-      float4 q = ldg4(w + WOFF(LXW) + i * 32 + j);
-      acc += x32[j] * q.x;
-      acc += x32[j + 1] * q.y;
-      acc += x32[j + 2] * q.z;
-      acc += x32[j + 3] * q.w;
-    }
-    a16[i] = relu0(acc);
-  }
-  const int lx[12] = {WOFF(LX0W), WOFF(LX1W), WOFF(LX2W), WOFF(LX3W), WOFF(LX4W), WOFF(LX5W),
-                      WOFF(LX6W), WOFF(LX7W), WOFF(LX8W), WOFF(LX9W), WOFF(LX10W), WOFF(LX11W)};
-#pragma unroll 1
-  for (int r = 0; r < 6; ++r) {  // residual pairs (:454-471)
-    float b16[16], c16[16];
-    dense16(a16, b16, w + lx[2 * r], w + lx[2 * r] + 256);
-    dense16(b16, c16, w + lx[2 * r + 1], w + lx[2 * r + 1] + 256);
-#pragma unroll
-    for (int i = 0; i < 16; ++i) a16[i] = a16[i] + c16[i];
-  }
-  float o = 0.0f;  // LX12 16 -> 1, bias after the sum
-#pragma unroll
-  for (int i = 0; i < 16; ++i) o += a16[i] * __ldg(w + WOFF(LX12W) + i);
-  o += __ldg(w + WOFF(LX12B));
-  return relu0(o);
-}
+// Trunk outputs per row, handed from the trunk kernel to the head kernel:
+// comb[0..120) (the L81 / LD41 outputs before gating) and fin[0..16) (the
+// LSEFin1 sums over pool[0..74), without the albedo term), 136 values in
+// chunks of 4: chunk c of row k is the float4 at t[k*rs + c*cs].
+struct TrunkOut {
+  float* t;
+  long long rs, cs;
+};
 
-__global__ void __launch_bounds__(kSimtThreads) k_mlp_simt(SimtArgs a) {
+// Trunks of RadiancePredict (radiancePredict.cu:385-437), one thread per row.
+__global__ void __launch_bounds__(kSimtThreads) k_simt_trunk(SimtArgs a, TrunkOut to) {
   const int n = a.count ? (int)min(*a.count, (unsigned)a.n) : a.n;
   const int k = blockIdx.x * kSimtThreads + threadIdx.x;
   if (k >= n) return;
   const float* __restrict__ w = a.w;
-  RowIO in{a.desc + (long long)k * a.rs, a.cs};
+  RowIO in{a.desc + (long long)k * a.rs, (int)(a.cs * 4)};
   const float* ax = a.aux + (long long)k * a.ars;
   const float g = __ldg(ax), gamma = __ldg(ax + a.afs);
-  const float srp[3] = {__ldg(ax + 2 * a.afs), __ldg(ax + 3 * a.afs), __ldg(ax + 4 * a.afs)};
-  float pool[75];
-  float y[3][32];
+  float fin[16];
 #pragma unroll
-  for (int b = 0; b < 3; ++b)
-#pragma unroll
-    for (int i = 0; i < 32; ++i) y[b][i] = 0.0f;
-  pool[72] = g;
-  pool[73] = gamma;
-  pool[74] = 0.0f;
+  for (int j = 0; j < 16; ++j) fin[j] = 0.0f;
+  __shared__ float ysm[96 * kSimtThreads];
+  const YS y{ysm + threadIdx.x};
   // main trunk (radiancePredict.cu:396-421)
-  simt_block<8, 0>(in, w, 0, 0, WOFF(LSE01W), WOFF(LSE02W), WOFF(L01W), WOFF(L_Tr01W), WOFF(L_Hg01W), g, gamma, y, pool);
-  simt_block<8, 2>(in, w, 8, 3, WOFF(LSE11W), WOFF(LSE12W), WOFF(L11W), WOFF(L_Tr11W), WOFF(L_Hg11W), g, gamma, y, pool);
+  simt_block<8, 0>(in, w, 0, 0, WOFF(LSE01W), WOFF(LSE02W), WOFF(L01W), WOFF(L_Tr01W), WOFF(L_Hg01W), g, gamma, y, fin);
+  simt_block<8, 2>(in, w, 8, 3, WOFF(LSE11W), WOFF(LSE12W), WOFF(L11W), WOFF(L_Tr11W), WOFF(L_Hg11W), g, gamma, y, fin);
   {
     const int p16[2][5] = {{WOFF(LSE21W), WOFF(LSE22W), WOFF(L21W), WOFF(L_Tr21W), WOFF(L_Hg21W)},
                            {WOFF(LSE31W), WOFF(LSE32W), WOFF(L31W), WOFF(L_Tr31W), WOFF(L_Hg31W)}};
 #pragma unroll 1
     for (int b = 0; b < 2; ++b)
       simt_block<16, 1>(in, w, 16 + 16 * b, 6 + 3 * b, p16[b][0], p16[b][1], p16[b][2], p16[b][3], p16[b][4], g,
-                        gamma, y, pool);
+                        gamma, y, fin);
   }
   simt_block<16, 2>(in, w, 48, 12, WOFF(LSE41W), WOFF(LSE42W), WOFF(L41W), WOFF(L_Tr41W), WOFF(L_Hg41W), g, gamma, y,
-                    pool);
+                    fin);
   {
     const int p32[3][5] = {{WOFF(LSE51W), WOFF(LSE52W), WOFF(L51W), WOFF(L_Tr51W), WOFF(L_Hg51W)},
                            {WOFF(LSE61W), WOFF(LSE62W), WOFF(L61W), WOFF(L_Tr61W), WOFF(L_Hg61W)},
@@ -308,20 +232,27 @@ __global__ void __launch_bounds__(kSimtThreads) k_mlp_simt(SimtArgs a) {
 #pragma unroll 1
     for (int b = 0; b < 3; ++b)
       simt_block<32, 1>(in, w, 64 + 32 * b, 15 + 3 * b, p32[b][0], p32[b][1], p32[b][2], p32[b][3], p32[b][4], g,
-                        gamma, y, pool);
+                        gamma, y, fin);
   }
-  float comb[120];
-  {  // L81: comb[0..96)
-    float c3[3][32];
-    dense3<32>(y, c3, w, WOFF(L81W), WOFF(L_Tr81W), WOFF(L_Hg81W));
+  float* orow = to.t + (long long)k * to.rs;
+  auto put4 = [&](int c, float x0, float x1, float x2, float x3) {
+    *reinterpret_cast<float4*>(orow + c * to.cs) = make_float4(x0, x1, x2, x3);
+  };
+  {  // L81: comb[0..96), one branch at a time, stored right away
+    const int wl[3] = {WOFF(L81W), WOFF(L_Tr81W), WOFF(L_Hg81W)};
 #pragma unroll
-    for (int b = 0; b < 3; ++b)
+    for (int b = 0; b < 3; ++b) {
+      float xin[32], c[32];
 #pragma unroll
-      for (int i = 0; i < 32; ++i) comb[32 * b + i] = c3[b][i];
+      for (int i = 0; i < 32; ++i) xin[i] = y.at(b, i);
+      dense1<32>(xin, c, w + wl[b]);
+#pragma unroll
+      for (int i = 0; i < 32; i += 4) put4((32 * b + i) / 4, c[i], c[i + 1], c[i + 2], c[i + 3]);
+    }
   }
   // light-direction trunk (:424-437)
   simt_block<8, 0>(in, w, 160, 24, WOFF(LDSE01W), WOFF(LDSE02W), WOFF(LD01W), WOFF(LD_Tr01W), WOFF(LD_Hg01W), g, gamma,
-                   y, pool);
+                   y, fin);
   {
     const int pd[3][5] = {{WOFF(LDSE11W), WOFF(LDSE12W), WOFF(LD11W), WOFF(LD_Tr11W), WOFF(LD_Hg11W)},
                           {WOFF(LDSE21W), WOFF(LDSE22W), WOFF(LD21W), WOFF(LD_Tr21W), WOFF(LD_Hg21W)},
@@ -329,31 +260,229 @@ __global__ void __launch_bounds__(kSimtThreads) k_mlp_simt(SimtArgs a) {
 #pragma unroll 1
     for (int b = 0; b < 3; ++b)
       simt_block<8, 1>(in, w, 168 + 8 * b, 27 + 3 * b, pd[b][0], pd[b][1], pd[b][2], pd[b][3], pd[b][4], g, gamma, y,
-                       pool);
+                       fin);
   }
   {  // LD41: comb[96..120)
-    float c3[3][32];
-    dense3<8>(y, c3, w, WOFF(LD41W), WOFF(LD_Tr41W), WOFF(LD_Hg41W));
+    const int wl[3] = {WOFF(LD41W), WOFF(LD_Tr41W), WOFF(LD_Hg41W)};
 #pragma unroll
-    for (int b = 0; b < 3; ++b)
+    for (int b = 0; b < 3; ++b) {
+      float xin[8], c[8];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) comb[96 + 8 * b + i] = c3[b][i];
+      for (int i = 0; i < 8; ++i) xin[i] = y.at(b, i);
+      dense1<8>(xin, c, w + wl[b]);
+#pragma unroll
+      for (int i = 0; i < 8; i += 4) put4((96 + 8 * b + i) / 4, c[i], c[i + 1], c[i + 2], c[i + 3]);
+    }
   }
-  // heads per distinct albedo channel (:475-483)
-  float X = simt_head(comb, pool, srp[0], w), Y, Z;
-  if (srp[1] == srp[0]) Y = X; else Y = simt_head(comb, pool, srp[1], w);
-  if (srp[2] == srp[0]) Z = X;
-  else if (srp[2] == srp[1]) Z = Y;
-  else Z = simt_head(comb, pool, srp[2], w);
-  float o[3] = {fmaxf(expf(X) - 1.0f, 0.0f) * srp[0], fmaxf(expf(Y) - 1.0f, 0.0f) * srp[1],
-                fmaxf(expf(Z) - 1.0f, 0.0f) * srp[2]};
+  // LSEFin1's g and gamma columns (pool[72], pool[73]); the albedo column is
+  // added per channel by the head
+#pragma unroll
+  for (int j = 0; j < 16; ++j)
+    fin[j] += g * __ldg(w + WOFF(LSEFin1W) + j * 75 + 72) + gamma * __ldg(w + WOFF(LSEFin1W) + j * 75 + 73);
+#pragma unroll
+  for (int j0 = 0; j0 < 16; j0 += 4) put4(30 + j0 / 4, fin[j0], fin[j0 + 1], fin[j0 + 2], fin[j0 + 3]);
+}
+
+// ---- head: block GEMMs over shared-memory activation tiles ---------------------------
+
+constexpr int kHeadRows = 128;  // rows (pixels) per block = threads per block
+constexpr int kHeadSmem = (2 * 128 * kHeadRows + 32 * 128) * (int)sizeof(float);  // X, Y, weight chunk
+
+struct HeadArgs {
+  const float* __restrict__ w;
+  const float* __restrict__ t;  // trunk outputs (TrunkOut layout)
+  long long trs, tcs;
+  const float* __restrict__ aux;
+  long long ars, afs;
+  int n;
+  const unsigned* __restrict__ count;
+  float* out;
+  const int* __restrict__ pix;
+  const float* __restrict__ trph;
+  F3 light_color, scatter;
+  const int* job;
+  const BatchOut* bout;
+};
+
+// Yt[c][r] = ReLU(B[c] + sum_k Xt[k][r] W[c][k]) for the block's 128 rows (Xt
+// and Yt column-major: element (row r, feature k) at [k*128 + r]); W is the
+// N x K row-major fp32 layer. Each thread owns an 8-row x TCOL-column output
+// tile; the sum starts at the bias and runs over k in ascending order, as
+// LinearReLU does. W is staged 32 inputs at a time, transposed, in Wc.
+template <int K, int N>
+__device__ __forceinline__ void block_gemm(const float* __restrict__ Xt, float* __restrict__ Yt,
+                                           float* __restrict__ Wc, const float* __restrict__ W,
+                                           const float* __restrict__ B) {
+  constexpr int TCOL = N >= 64 ? 8 : N / 8;
+  constexpr int PASSES = N >= 64 ? N / 64 : 1;
+  constexpr int PN = N / PASSES;  // columns per pass
+  const int t = threadIdx.x, r0 = (t >> 3) * 8, cl = (t & 7) * TCOL;
+#pragma unroll 1
+  for (int pass = 0; pass < PASSES; ++pass) {
+    const int cb = pass * PN;
+    float acc[8][TCOL];
+#pragma unroll
+    for (int j = 0; j < TCOL; ++j) {
+      const float b = __ldg(B + cb + cl + j);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) acc[i][j] = b;
+    }
+#pragma unroll 1
+    for (int k0 = 0; k0 < K; k0 += 32) {
+      __syncthreads();  // the previous chunk is consumed
+      for (int idx = t; idx < PN * 8; idx += kHeadRows) {
+        const int cc = idx >> 3, q = idx & 7;
+        const float4 v = __ldg(reinterpret_cast<const float4*>(W + (size_t)(cb + cc) * K + k0 + 4 * q));
+        Wc[(4 * q + 0) * PN + cc] = v.x;
+        Wc[(4 * q + 1) * PN + cc] = v.y;
+        Wc[(4 * q + 2) * PN + cc] = v.z;
+        Wc[(4 * q + 3) * PN + cc] = v.w;
+      }
+      __syncthreads();
+#pragma unroll 4
+      for (int kk = 0; kk < 32; ++kk) {
+        const float4 xa = *reinterpret_cast<const float4*>(Xt + (k0 + kk) * kHeadRows + r0);
+        const float4 xb = *reinterpret_cast<const float4*>(Xt + (k0 + kk) * kHeadRows + r0 + 4);
+        const float xv[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
+        float wv[TCOL];
+#pragma unroll
+        for (int j = 0; j < TCOL; j += 4) {
+          const float4 q = *reinterpret_cast<const float4*>(Wc + kk * PN + cl + j);
+          wv[j] = q.x; wv[j + 1] = q.y; wv[j + 2] = q.z; wv[j + 3] = q.w;
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+          for (int j = 0; j < TCOL; ++j) acc[i][j] = fmaf(xv[i], wv[j], acc[i][j]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < TCOL; ++j) {
+      float* dst = Yt + (cb + cl + j) * kHeadRows + r0;
+      *reinterpret_cast<float4*>(dst) = make_float4(relu0(acc[0][j]), relu0(acc[1][j]), relu0(acc[2][j]), relu0(acc[3][j]));
+      *reinterpret_cast<float4*>(dst + 4) =
+          make_float4(relu0(acc[4][j]), relu0(acc[5][j]), relu0(acc[6][j]), relu0(acc[7][j]));
+    }
+  }
+}
+
+// Head SC(p) (radiancePredict.cu:439-473) per distinct albedo channel for a
+// block of 128 rows: the gated 128-wide input is built per row into Xt, LC0 /
+// LC1 / LC2 run as block GEMMs, LX and the residual pairs per row.
+__global__ void __launch_bounds__(kHeadRows) k_simt_head(HeadArgs a) {
+  extern __shared__ __align__(16) float hsm[];
+  float* Xt = hsm;
+  float* Yt = hsm + 128 * kHeadRows;
+  float* Wc = hsm + 2 * 128 * kHeadRows;
+  const int n = a.count ? (int)min(*a.count, (unsigned)a.n) : a.n;
+  const int row0 = blockIdx.x * kHeadRows;
+  if (row0 >= n) return;  // block-uniform
+  const int r = threadIdx.x, row = row0 + r;
+  const bool valid = row < n;
+  const int kr = valid ? row : n - 1;
+  const float* __restrict__ w = a.w;
+  const float* trow = a.t + (long long)kr * a.trs;
+  const float* ax = a.aux + (long long)kr * a.ars;
+  const float g = __ldg(ax), gamma = __ldg(ax + a.afs);
+  const float srp[3] = {__ldg(ax + 2 * a.afs), __ldg(ax + 3 * a.afs), __ldg(ax + 4 * a.afs)};
+  float fin[16];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const float4 q = __ldg(reinterpret_cast<const float4*>(trow + (30 + c) * a.tcs));
+    fin[4 * c] = q.x; fin[4 * c + 1] = q.y; fin[4 * c + 2] = q.z; fin[4 * c + 3] = q.w;
+  }
+  const bool need1 = __syncthreads_or(valid && srp[1] != srp[0]);
+  const bool need2 = __syncthreads_or(valid && srp[2] != srp[0] && srp[2] != srp[1]);
+  float X[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll 1
+  for (int ch = 0; ch < 3; ++ch) {
+    if ((ch == 1 && !need1) || (ch == 2 && !need2)) continue;
+    const float sc = ch == 0 ? srp[0] : ch == 1 ? srp[1] : srp[2];
+    // gates of this channel (LGGS, LSEFin1's albedo column, LSEFin2)
+    float sep[6];
+    {
+      float sew[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) sew[j] = relu0(fin[j] + sc * __ldg(w + WOFF(LSEFin1W) + j * 75 + 74));
+#pragma unroll
+      for (int i = 0; i < 6; ++i) {
+        float acc = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) acc += sew[j] * __ldg(w + WOFF(LSEFin2W) + j + i * 16);
+        sep[i] = 1.0f / (1.0f + expf(-acc));
+      }
+    }
+    // gated head input, column-major in Xt
+#pragma unroll 2
+    for (int c = 0; c < 30; ++c) {
+      const float4 q = __ldg(reinterpret_cast<const float4*>(trow + c * a.tcs));
+      const float s = c < 24 ? sep[c >> 3] : sep[3 + ((c - 24) >> 1)];
+      Xt[(4 * c + 0) * kHeadRows + r] = q.x * s;
+      Xt[(4 * c + 1) * kHeadRows + r] = q.y * s;
+      Xt[(4 * c + 2) * kHeadRows + r] = q.z * s;
+      Xt[(4 * c + 3) * kHeadRows + r] = q.w * s;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {  // LGGS 3 -> 8, bias after the sum
+      float acc = g * __ldg(w + WOFF(LGGSW) + 3 * i) + gamma * __ldg(w + WOFF(LGGSW) + 3 * i + 1) +
+                  sc * __ldg(w + WOFF(LGGSW) + 3 * i + 2);
+      acc += __ldg(w + WOFF(LGGSB) + i);
+      Xt[(120 + i) * kHeadRows + r] = relu0(acc);
+    }
+    block_gemm<128, 128>(Xt, Yt, Wc, w + WOFF(LC0W), w + WOFF(LC0B));
+    block_gemm<128, 64>(Yt, Xt, Wc, w + WOFF(LC1W), w + WOFF(LC1B));
+    block_gemm<64, 32>(Xt, Yt, Wc, w + WOFF(LC2W), w + WOFF(LC2B));
+    __syncthreads();
+    float x32[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) x32[i] = Yt[i * kHeadRows + r];
+    float a16[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {  // LX 32 -> 16
+      float acc = __ldg(w + WOFF(LXB) + i);
+#pragma unroll
+      for (int j = 0; j < 32; j += 4) {
+        float4 q = ldg4(w + WOFF(LXW) + i * 32 + j);
+        acc += x32[j] * q.x;
+        acc += x32[j + 1] * q.y;
+        acc += x32[j + 2] * q.z;
+        acc += x32[j + 3] * q.w;
+      }
+      a16[i] = relu0(acc);
+    }
+    const int lx[12] = {WOFF(LX0W), WOFF(LX1W), WOFF(LX2W), WOFF(LX3W), WOFF(LX4W), WOFF(LX5W),
+                        WOFF(LX6W), WOFF(LX7W), WOFF(LX8W), WOFF(LX9W), WOFF(LX10W), WOFF(LX11W)};
+#pragma unroll 1
+    for (int rr = 0; rr < 6; ++rr) {  // residual pairs (:454-471)
+      float b16[16], c16[16];
+      dense16(a16, b16, w + lx[2 * rr], w + lx[2 * rr] + 256);
+      dense16(b16, c16, w + lx[2 * rr + 1], w + lx[2 * rr + 1] + 256);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) a16[i] = a16[i] + c16[i];
+    }
+    float o = 0.0f;  // LX12 16 -> 1, bias after the sum
+#pragma unroll
+    for (int i = 0; i < 16; ++i) o += a16[i] * __ldg(w + WOFF(LX12W) + i);
+    o += __ldg(w + WOFF(LX12B));
+    const float xo = relu0(o);
+    if (ch == 0) X[0] = xo;
+    else if (ch == 1) X[1] = xo;
+    else X[2] = xo;
+    __syncthreads();  // Xt / Yt are rebuilt by the next channel
+  }
+  if (srp[1] == srp[0]) X[1] = X[0];
+  if (srp[2] == srp[0]) X[2] = X[0];
+  else if (srp[2] == srp[1]) X[2] = X[1];
+  if (!valid) return;
+  float o[3] = {fmaxf(expf(X[0]) - 1.0f, 0.0f) * srp[0], fmaxf(expf(X[1]) - 1.0f, 0.0f) * srp[1],
+                fmaxf(expf(X[2]) - 1.0f, 0.0f) * srp[2]};
   if (a.pix) {
-    const int px = a.pix[k];
-    const float tr = a.trph[k];
+    const int px = a.pix[row];
+    const float tr = a.trph[row];
     F3 lc = a.light_color, sc = a.scatter;
     float* dst = a.out;
     if (a.job) {
-      const BatchOut& bo = a.bout[a.job[k]];
+      const BatchOut& bo = a.bout[a.job[row]];
       lc = bo.light_color;
       sc = bo.scatter;
       dst = bo.out;
@@ -363,14 +492,24 @@ __global__ void __launch_bounds__(kSimtThreads) k_mlp_simt(SimtArgs a) {
     dst[3 * (size_t)px + 2] = fmaxf(((o[2] + tr) * lc.z) * sc.z, 0.0f);
   } else {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) a.out[3 * (size_t)k + c] = o[c];
+    for (int c = 0; c < 3; ++c) a.out[3 * (size_t)row + c] = o[c];
   }
 }
 
+// Trunk kernel then head kernel. `tout` receives the trunk outputs (TrunkOut
+// layout with strides trs / tcs): the render path passes its own descriptor
+// columns, whose first 34 chunks of a row are no longer needed once that row's
+// trunks are done.
 int launch_mlp_simt(const Network* net, const float* desc, const float* aux, long long rs, long long cs,
                     long long ars, long long afs, int n, const unsigned* count, float* out, const int* pix,
                     const float* trph, F3 light_color, F3 scatter, cudaStream_t s, const int* job,
-                    const BatchOut* bout) {
+                    const BatchOut* bout, float* tout, long long trs, long long tcs) {
+  if (!tout) return set_error(MR_ERR_ARG, "fp32 network: no buffer for the trunk outputs");
+  static bool attr = false;
+  if (!attr) {
+    MR_CUDA(cudaFuncSetAttribute(k_simt_head, cudaFuncAttributeMaxDynamicSharedMemorySize, kHeadSmem));
+    attr = true;
+  }
   SimtArgs a;
   a.w = net->w;
   a.desc = desc;
@@ -388,7 +527,26 @@ int launch_mlp_simt(const Network* net, const float* desc, const float* aux, lon
   a.scatter = scatter;
   a.job = job;
   a.bout = bout;
-  k_mlp_simt<<<(unsigned)((n + kSimtThreads - 1) / kSimtThreads), kSimtThreads, 0, s>>>(a);
+  k_simt_trunk<<<(unsigned)((n + kSimtThreads - 1) / kSimtThreads), kSimtThreads, 0, s>>>(a, TrunkOut{tout, trs, tcs});
+  MR_CUDA(cudaGetLastError());
+  HeadArgs h;
+  h.w = net->w;
+  h.t = tout;
+  h.trs = trs;
+  h.tcs = tcs;
+  h.aux = aux;
+  h.ars = ars;
+  h.afs = afs;
+  h.n = n;
+  h.count = count;
+  h.out = out;
+  h.pix = pix;
+  h.trph = trph;
+  h.light_color = light_color;
+  h.scatter = scatter;
+  h.job = job;
+  h.bout = bout;
+  k_simt_head<<<(unsigned)((n + kHeadRows - 1) / kHeadRows), kHeadRows, kHeadSmem, s>>>(h);
   MR_CUDA(cudaGetLastError());
   return MR_OK;
 }

@@ -6,7 +6,7 @@
 //     list with warp-aggregated atomics, inactive ones get the environment.
 //  2. k_gather_fm: per active record, the 192-point multi-scale descriptor
 //     gather (core/radiancePredict.cu:319-368) into feature-major columns.
-//  3. the network body: k_mlp_simt (fp32, mr_mlp_simt.cu) or k_mlp_tc
+//  3. the network body: k_simt_trunk + k_simt_head (fp32, mr_mlp_simt.cu) or k_mlp_tc
 //     (BF16 tcgen05, mr_mlp_tc.cu), which also writes the pixel.
 #include <algorithm>
 #include <mutex>
@@ -374,8 +374,8 @@ int launch_mlp_tc(const Network* net, const float* desc, const float* aux, long 
                   const int* job = nullptr, const BatchOut* bout = nullptr);
 int launch_mlp_simt(const Network* net, const float* desc, const float* aux, long long rs, long long cs,
                     long long ars, long long afs, int n, const unsigned* count, float* out, const int* pix,
-                    const float* trph, F3 light_color, F3 scatter, cudaStream_t s, const int* job = nullptr,
-                    const BatchOut* bout = nullptr);
+                    const float* trph, F3 light_color, F3 scatter, cudaStream_t s, const int* job, const BatchOut* bout,
+                    float* tout, long long trs, long long tcs);
 int mlp_tc_error(const Network* net, bool reset);
 
 extern int check_params(const mr_render_params* p);
@@ -500,7 +500,7 @@ static int neural_passes(Volume* v, const Network* net, const mr_render_params* 
                        to_f3(p->light_color), to_f3(p->scatter_rate), spill, p->precision == MR_PREC_FP8, s);
   else
     rc = launch_mlp_simt(net, desc, aux, 4, 4 * cap, 1, cap, (int)npx, rec.count, dev_rgb, rec.pix, rec.trph,
-                         to_f3(p->light_color), to_f3(p->scatter_rate), s);
+                         to_f3(p->light_color), to_f3(p->scatter_rate), s, nullptr, nullptr, desc, 4, 4 * cap);
   mark(ST_NN_MLP);
   return rc;
 }
@@ -548,8 +548,15 @@ extern "C" int mr_radiance_predict(const mr_network* nh, int32_t precision, cons
     return rc;
   }
   if (precision != MR_PREC_FP32) return set_error(MR_ERR_ARG, "unknown precision %d", precision);
-  return launch_mlp_simt(&nh->n, dev_desc, dev_aux, 576, 4, 5, 1, n, nullptr, dev_out, nullptr, nullptr, f3(1, 1, 1),
-                         f3(1, 1, 1), (cudaStream_t)stream);
+  // the caller's descriptors stay untouched: trunk outputs go to a temporary
+  cudaStream_t s = (cudaStream_t)stream;
+  float* tout = nullptr;
+  cudaError_t e = cudaMallocAsync(&tout, (size_t)n * 136 * sizeof(float), s);
+  if (e != cudaSuccess) return set_error(MR_ERR_NOMEM, "trunk buffer: %s", cudaGetErrorString(e));
+  int rc = launch_mlp_simt(&nh->n, dev_desc, dev_aux, 576, 4, 5, 1, n, nullptr, dev_out, nullptr, nullptr,
+                           f3(1, 1, 1), f3(1, 1, 1), s, nullptr, nullptr, tout, 136, 4);
+  MR_CUDA(cudaFreeAsync(tout, s));
+  return rc;
 }
 
 // ---- fixed-scratch neural render (mr_render_neural_noalloc) -------------------
@@ -767,7 +774,7 @@ static int batch_launches(Batch& b, const Network* net, cudaStream_t s) {
                          f3(1, 1, 1), f3(1, 1, 1), spill, b.precision == MR_PREC_FP8, s, rec.job, b.d_out);
     else
       rc = launch_mlp_simt(net, desc, aux, 4, 4 * ccap, 1, ccap, (int)cap, rec.count, nullptr, rec.pix, rec.trph,
-                           f3(1, 1, 1), f3(1, 1, 1), s, rec.job, b.d_out);
+                           f3(1, 1, 1), f3(1, 1, 1), s, rec.job, b.d_out, desc, 4, 4 * ccap);
     if (rc) return rc;
   }
   k_batch_advance<<<(nj + 127) / 128, 128, 0, s>>>(b.d_jobs, nj);
