@@ -139,9 +139,10 @@ __device__ __forceinline__ void simt_block(const RowIO& in, const float* __restr
     for (int j = 0; j < 8; ++j) a += h[j] * __ldg(w + sew1 + j + i * 8);
     gate[i] = 1.0f / (1.0f + expf(-a));
   }
-  const int wofs[3] = {wa, wb, wc};
-#pragma unroll
+#pragma unroll 1
   for (int b = 0; b < 3; ++b) {
+    const int wo = b == 0 ? wa : b == 1 ? wb : wc;
+    const float gb = b == 0 ? gate[0] : b == 1 ? gate[1] : gate[2];
     float x[32], yn[32];
 #pragma unroll
     for (int i = 0; i < S; i += 4) {
@@ -149,11 +150,11 @@ __device__ __forceinline__ void simt_block(const RowIO& in, const float* __restr
       const float qv[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
-        const float v = qv[u] * gate[b];
+        const float v = qv[u] * gb;
         x[i + u] = MODE == 0 ? v : v + y.at(b, i + u);
       }
     }
-    dense1<S>(x, yn, w + wofs[b]);
+    dense1<S>(x, yn, w + wo);
 #pragma unroll
     for (int i = 0; i < S; i += 4) {
       const float4 q = in.ld4(b * 192 + from + i);
@@ -286,11 +287,12 @@ __global__ void __launch_bounds__(kSimtThreads) k_simt_trunk(SimtArgs a, TrunkOu
 // ---- head: block GEMMs over shared-memory activation tiles ---------------------------
 
 constexpr int kHeadRows = 128;  // rows (pixels) per block = threads per block
-constexpr int kHeadSmem = (2 * 128 * kHeadRows + 32 * 128) * (int)sizeof(float);  // X, Y, weight chunk
+constexpr int kHeadSmem = 2 * 128 * kHeadRows * (int)sizeof(float);  // Xt, Yt
 
 struct HeadArgs {
   const float* __restrict__ w;
-  const float* __restrict__ t;  // trunk outputs (TrunkOut layout)
+  const float* __restrict__ wt;  // LC0 / LC1 / LC2 transposed, [in][out]
+  const float* __restrict__ t;   // trunk outputs (TrunkOut layout)
   long long trs, tcs;
   const float* __restrict__ aux;
   long long ars, afs;
@@ -305,62 +307,51 @@ struct HeadArgs {
 };
 
 // Yt[c][r] = ReLU(B[c] + sum_k Xt[k][r] W[c][k]) for the block's 128 rows (Xt
-// and Yt column-major: element (row r, feature k) at [k*128 + r]); W is the
-// N x K row-major fp32 layer. Each thread owns an 8-row x TCOL-column output
-// tile; the sum starts at the bias and runs over k in ascending order, as
-// LinearReLU does. W is staged 32 inputs at a time, transposed, in Wc.
+// and Yt column-major: element (row r, feature k) at [k*128 + r]); WT is the
+// layer transposed to [K][N]. Thread t owns rows {4g..4g+3, 64+4g..64+4g+3}
+// (g = t % 16) and TCOL consecutive columns (group t / 16); the sum starts at
+// the bias and runs over k in ascending order, as LinearReLU does. The eight
+// threads of a quarter warp read and write 128 contiguous bytes of Xt / Yt,
+// and a warp's weight loads touch two addresses (L1 broadcast).
 template <int K, int N>
 __device__ __forceinline__ void block_gemm(const float* __restrict__ Xt, float* __restrict__ Yt,
-                                           float* __restrict__ Wc, const float* __restrict__ W,
-                                           const float* __restrict__ B) {
+                                           const float* __restrict__ WT, const float* __restrict__ B) {
   constexpr int TCOL = N >= 64 ? 8 : N / 8;
   constexpr int PASSES = N >= 64 ? N / 64 : 1;
   constexpr int PN = N / PASSES;  // columns per pass
-  const int t = threadIdx.x, r0 = (t >> 3) * 8, cl = (t & 7) * TCOL;
+  const int t = threadIdx.x, r0 = 4 * (t & 15), cl = (t >> 4) * TCOL;
+  __syncthreads();  // Xt complete, Yt free
 #pragma unroll 1
   for (int pass = 0; pass < PASSES; ++pass) {
-    const int cb = pass * PN;
+    const int c0 = pass * PN + cl;
     float acc[8][TCOL];
 #pragma unroll
     for (int j = 0; j < TCOL; ++j) {
-      const float b = __ldg(B + cb + cl + j);
+      const float b = __ldg(B + c0 + j);
 #pragma unroll
       for (int i = 0; i < 8; ++i) acc[i][j] = b;
     }
-#pragma unroll 1
-    for (int k0 = 0; k0 < K; k0 += 32) {
-      __syncthreads();  // the previous chunk is consumed
-      for (int idx = t; idx < PN * 8; idx += kHeadRows) {
-        const int cc = idx >> 3, q = idx & 7;
-        const float4 v = __ldg(reinterpret_cast<const float4*>(W + (size_t)(cb + cc) * K + k0 + 4 * q));
-        Wc[(4 * q + 0) * PN + cc] = v.x;
-        Wc[(4 * q + 1) * PN + cc] = v.y;
-        Wc[(4 * q + 2) * PN + cc] = v.z;
-        Wc[(4 * q + 3) * PN + cc] = v.w;
-      }
-      __syncthreads();
 #pragma unroll 4
-      for (int kk = 0; kk < 32; ++kk) {
-        const float4 xa = *reinterpret_cast<const float4*>(Xt + (k0 + kk) * kHeadRows + r0);
-        const float4 xb = *reinterpret_cast<const float4*>(Xt + (k0 + kk) * kHeadRows + r0 + 4);
-        const float xv[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
-        float wv[TCOL];
+    for (int k = 0; k < K; ++k) {
+      const float4 xa = *reinterpret_cast<const float4*>(Xt + k * kHeadRows + r0);
+      const float4 xb = *reinterpret_cast<const float4*>(Xt + k * kHeadRows + 64 + r0);
+      const float xv[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
+      float wv[TCOL];
 #pragma unroll
-        for (int j = 0; j < TCOL; j += 4) {
-          const float4 q = *reinterpret_cast<const float4*>(Wc + kk * PN + cl + j);
-          wv[j] = q.x; wv[j + 1] = q.y; wv[j + 2] = q.z; wv[j + 3] = q.w;
-        }
-#pragma unroll
-        for (int i = 0; i < 8; ++i)
-#pragma unroll
-          for (int j = 0; j < TCOL; ++j) acc[i][j] = fmaf(xv[i], wv[j], acc[i][j]);
+      for (int j = 0; j < TCOL; j += 4) {
+        const float4 q = __ldg(reinterpret_cast<const float4*>(WT + k * N + c0 + j));
+        wv[j] = q.x; wv[j + 1] = q.y; wv[j + 2] = q.z; wv[j + 3] = q.w;
       }
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < TCOL; ++j) acc[i][j] = fmaf(xv[i], wv[j], acc[i][j]);
     }
 #pragma unroll
     for (int j = 0; j < TCOL; ++j) {
-      float* dst = Yt + (cb + cl + j) * kHeadRows + r0;
+      float* dst = Yt + (c0 + j) * kHeadRows + r0;
       *reinterpret_cast<float4*>(dst) = make_float4(relu0(acc[0][j]), relu0(acc[1][j]), relu0(acc[2][j]), relu0(acc[3][j]));
-      *reinterpret_cast<float4*>(dst + 4) =
+      *reinterpret_cast<float4*>(dst + 64) =
           make_float4(relu0(acc[4][j]), relu0(acc[5][j]), relu0(acc[6][j]), relu0(acc[7][j]));
     }
   }
@@ -373,7 +364,6 @@ __global__ void __launch_bounds__(kHeadRows) k_simt_head(HeadArgs a) {
   extern __shared__ __align__(16) float hsm[];
   float* Xt = hsm;
   float* Yt = hsm + 128 * kHeadRows;
-  float* Wc = hsm + 2 * 128 * kHeadRows;
   const int n = a.count ? (int)min(*a.count, (unsigned)a.n) : a.n;
   const int row0 = blockIdx.x * kHeadRows;
   if (row0 >= n) return;  // block-uniform
@@ -429,9 +419,9 @@ __global__ void __launch_bounds__(kHeadRows) k_simt_head(HeadArgs a) {
       acc += __ldg(w + WOFF(LGGSB) + i);
       Xt[(120 + i) * kHeadRows + r] = relu0(acc);
     }
-    block_gemm<128, 128>(Xt, Yt, Wc, w + WOFF(LC0W), w + WOFF(LC0B));
-    block_gemm<128, 64>(Yt, Xt, Wc, w + WOFF(LC1W), w + WOFF(LC1B));
-    block_gemm<64, 32>(Xt, Yt, Wc, w + WOFF(LC2W), w + WOFF(LC2B));
+    block_gemm<128, 128>(Xt, Yt, a.wt, w + WOFF(LC0B));
+    block_gemm<128, 64>(Yt, Xt, a.wt + 128 * 128, w + WOFF(LC1B));
+    block_gemm<64, 32>(Xt, Yt, a.wt + 128 * 128 + 128 * 64, w + WOFF(LC2B));
     __syncthreads();
     float x32[32];
 #pragma unroll
@@ -531,6 +521,7 @@ int launch_mlp_simt(const Network* net, const float* desc, const float* aux, lon
   MR_CUDA(cudaGetLastError());
   HeadArgs h;
   h.w = net->w;
+  h.wt = net->head_t;
   h.t = tout;
   h.trs = trs;
   h.tcs = tcs;
