@@ -286,12 +286,16 @@ __global__ void __launch_bounds__(kSimtThreads) k_simt_trunk(SimtArgs a, TrunkOu
 
 // ---- head: block GEMMs over shared-memory activation tiles ---------------------------
 
-constexpr int kHeadRows = 128;  // rows (pixels) per block = threads per block
-constexpr int kHeadSmem = 2 * 128 * kHeadRows * (int)sizeof(float);  // Xt, Yt
+constexpr int kHeadRows = 128;     // rows (pixels) per block
+constexpr int kHeadThreads = 256;  // two threads per row in the per-row stages
+constexpr int kChunk = 2048;       // floats per weight chunk (8 KB)
+constexpr int kHeadChunks = 13;    // LC0 8, LC1 4, LC2 1 chunks
+constexpr int kStages = 3;         // weight chunks in flight
+constexpr int kHeadSmem = (2 * 128 * kHeadRows + kStages * kChunk) * (int)sizeof(float);  // Xt, Yt, ring
 
 struct HeadArgs {
   const float* __restrict__ w;
-  const float* __restrict__ wt;  // LC0 / LC1 / LC2 transposed, [in][out]
+  const float* __restrict__ wt;  // LC0 / LC1 / LC2 transposed, [in][out], concatenated
   const float* __restrict__ t;   // trunk outputs (TrunkOut layout)
   long long trs, tcs;
   const float* __restrict__ aux;
@@ -306,68 +310,106 @@ struct HeadArgs {
   const BatchOut* bout;
 };
 
+__device__ __forceinline__ void cp_async16(float* dst, const float* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+
+// The head weights (LC0, LC1, LC2 transposed; 13 chunks of 8 KB, repeated
+// per albedo channel) stream through a ring of kStages shared-memory buffers
+// with cp.async: chunk c + kStages - 1 is in flight while chunk c is used.
+struct WStream {
+  const float* __restrict__ src;
+  float* ring;
+  int issued, total;
+  __device__ __forceinline__ void issue() {
+    if (issued < total) {
+      const float* s = src + (issued % kHeadChunks) * kChunk + threadIdx.x * 8;
+      float* d = ring + (issued % kStages) * kChunk + threadIdx.x * 8;
+      cp_async16(d, s);
+      cp_async16(d + 4, s + 4);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    ++issued;
+  }
+  // Buffer of chunk c (chunks are acquired in order by all threads); the
+  // barrier also orders the block's shared-memory writes before it.
+  __device__ __forceinline__ const float* acquire(int c) {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(kStages - 2) : "memory");
+    __syncthreads();
+    issue();
+    return ring + (c % kStages) * kChunk;
+  }
+};
+
 // Yt[c][r] = ReLU(B[c] + sum_k Xt[k][r] W[c][k]) for the block's 128 rows (Xt
-// and Yt column-major: element (row r, feature k) at [k*128 + r]); WT is the
-// layer transposed to [K][N]. Thread t owns rows {4g..4g+3, 64+4g..64+4g+3}
-// (g = t % 16) and TCOL consecutive columns (group t / 16); the sum starts at
-// the bias and runs over k in ascending order, as LinearReLU does. The eight
-// threads of a quarter warp read and write 128 contiguous bytes of Xt / Yt,
-// and a warp's weight loads touch two addresses (L1 broadcast).
+// and Yt column-major: element (row r, feature k) at [k*128 + r]); the weights
+// arrive as chunks of 2048 / N rows of the transposed [K][N] layer. Thread t
+// owns rows {4g..4g+3, 64+4g..64+4g+3} (g = t % 16) and N / 16 consecutive
+// columns (group t / 16); the sum starts at the bias and runs over k in
+// ascending order, as LinearReLU does. The eight threads of a quarter warp
+// read and write 128 contiguous bytes of Xt / Yt, and a warp's weight loads
+// touch two addresses (broadcast).
 template <int K, int N>
 __device__ __forceinline__ void block_gemm(const float* __restrict__ Xt, float* __restrict__ Yt,
-                                           const float* __restrict__ WT, const float* __restrict__ B) {
-  constexpr int TCOL = N >= 64 ? 8 : N / 8;
-  constexpr int PASSES = N >= 64 ? N / 64 : 1;
-  constexpr int PN = N / PASSES;  // columns per pass
-  const int t = threadIdx.x, r0 = 4 * (t & 15), cl = (t >> 4) * TCOL;
-  __syncthreads();  // Xt complete, Yt free
+                                           const float* __restrict__ B, WStream& ws, int& chunk) {
+  constexpr int TCOL = N / 16;
+  constexpr int KC = kChunk / N;
+  const int t = threadIdx.x, r0 = 4 * (t & 15), c0 = (t >> 4) * TCOL;
+  float acc[8][TCOL];
+#pragma unroll
+  for (int j = 0; j < TCOL; ++j) {
+    const float b = __ldg(B + c0 + j);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) acc[i][j] = b;
+  }
 #pragma unroll 1
-  for (int pass = 0; pass < PASSES; ++pass) {
-    const int c0 = pass * PN + cl;
-    float acc[8][TCOL];
-#pragma unroll
-    for (int j = 0; j < TCOL; ++j) {
-      const float b = __ldg(B + c0 + j);
-#pragma unroll
-      for (int i = 0; i < 8; ++i) acc[i][j] = b;
-    }
+  for (int kc = 0; kc < K; kc += KC) {
+    const float* __restrict__ W = ws.acquire(chunk++);
 #pragma unroll 4
-    for (int k = 0; k < K; ++k) {
-      const float4 xa = *reinterpret_cast<const float4*>(Xt + k * kHeadRows + r0);
-      const float4 xb = *reinterpret_cast<const float4*>(Xt + k * kHeadRows + 64 + r0);
+    for (int k = 0; k < KC; ++k) {
+      const float4 xa = *reinterpret_cast<const float4*>(Xt + (kc + k) * kHeadRows + r0);
+      const float4 xb = *reinterpret_cast<const float4*>(Xt + (kc + k) * kHeadRows + 64 + r0);
       const float xv[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
       float wv[TCOL];
+      if constexpr (TCOL >= 4) {
 #pragma unroll
-      for (int j = 0; j < TCOL; j += 4) {
-        const float4 q = __ldg(reinterpret_cast<const float4*>(WT + k * N + c0 + j));
-        wv[j] = q.x; wv[j + 1] = q.y; wv[j + 2] = q.z; wv[j + 3] = q.w;
+        for (int j = 0; j < TCOL; j += 4) {
+          const float4 q = *reinterpret_cast<const float4*>(W + k * N + c0 + j);
+          wv[j] = q.x; wv[j + 1] = q.y; wv[j + 2] = q.z; wv[j + 3] = q.w;
+        }
+      } else {
+        const float2 q = *reinterpret_cast<const float2*>(W + k * N + c0);
+        wv[0] = q.x; wv[1] = q.y;
       }
 #pragma unroll
       for (int i = 0; i < 8; ++i)
 #pragma unroll
         for (int j = 0; j < TCOL; ++j) acc[i][j] = fmaf(xv[i], wv[j], acc[i][j]);
     }
+  }
 #pragma unroll
-    for (int j = 0; j < TCOL; ++j) {
-      float* dst = Yt + (c0 + j) * kHeadRows + r0;
-      *reinterpret_cast<float4*>(dst) = make_float4(relu0(acc[0][j]), relu0(acc[1][j]), relu0(acc[2][j]), relu0(acc[3][j]));
-      *reinterpret_cast<float4*>(dst + 64) =
-          make_float4(relu0(acc[4][j]), relu0(acc[5][j]), relu0(acc[6][j]), relu0(acc[7][j]));
-    }
+  for (int j = 0; j < TCOL; ++j) {
+    float* dst = Yt + (c0 + j) * kHeadRows + r0;
+    *reinterpret_cast<float4*>(dst) = make_float4(relu0(acc[0][j]), relu0(acc[1][j]), relu0(acc[2][j]), relu0(acc[3][j]));
+    *reinterpret_cast<float4*>(dst + 64) =
+        make_float4(relu0(acc[4][j]), relu0(acc[5][j]), relu0(acc[6][j]), relu0(acc[7][j]));
   }
 }
 
 // Head SC(p) (radiancePredict.cu:439-473) per distinct albedo channel for a
-// block of 128 rows: the gated 128-wide input is built per row into Xt, LC0 /
-// LC1 / LC2 run as block GEMMs, LX and the residual pairs per row.
-__global__ void __launch_bounds__(kHeadRows) k_simt_head(HeadArgs a) {
+// block of 128 rows: the gated 128-wide input is built per row into Xt (two
+// threads per row, half the features each), LC0 / LC1 / LC2 run as block
+// GEMMs over all 256 threads, LX and the residual pairs per row on the first
+// 128 threads.
+__global__ void __launch_bounds__(kHeadThreads, 1) k_simt_head(HeadArgs a) {
   extern __shared__ __align__(16) float hsm[];
   float* Xt = hsm;
   float* Yt = hsm + 128 * kHeadRows;
   const int n = a.count ? (int)min(*a.count, (unsigned)a.n) : a.n;
   const int row0 = blockIdx.x * kHeadRows;
   if (row0 >= n) return;  // block-uniform
-  const int r = threadIdx.x, row = row0 + r;
+  const int r = threadIdx.x & (kHeadRows - 1), half = threadIdx.x >> 7, row = row0 + r;
   const bool valid = row < n;
   const int kr = valid ? row : n - 1;
   const float* __restrict__ w = a.w;
@@ -383,6 +425,10 @@ __global__ void __launch_bounds__(kHeadRows) k_simt_head(HeadArgs a) {
   }
   const bool need1 = __syncthreads_or(valid && srp[1] != srp[0]);
   const bool need2 = __syncthreads_or(valid && srp[2] != srp[0] && srp[2] != srp[1]);
+  WStream ws{a.wt, hsm + 2 * 128 * kHeadRows, 0, kHeadChunks * (1 + (int)need1 + (int)need2)};
+#pragma unroll
+  for (int i = 0; i < kStages - 1; ++i) ws.issue();
+  int chunk = 0;
   float X[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll 1
   for (int ch = 0; ch < 3; ++ch) {
@@ -402,9 +448,10 @@ __global__ void __launch_bounds__(kHeadRows) k_simt_head(HeadArgs a) {
         sep[i] = 1.0f / (1.0f + expf(-acc));
       }
     }
-    // gated head input, column-major in Xt
-#pragma unroll 2
-    for (int c = 0; c < 30; ++c) {
+    // gated head input, column-major in Xt: chunks 0..14 by the first thread
+    // of a row, 15..29 and LGGS by the second
+#pragma unroll 3
+    for (int c = 15 * half; c < 15 * half + 15; ++c) {
       const float4 q = __ldg(reinterpret_cast<const float4*>(trow + c * a.tcs));
       const float s = c < 24 ? sep[c >> 3] : sep[3 + ((c - 24) >> 1)];
       Xt[(4 * c + 0) * kHeadRows + r] = q.x * s;
@@ -412,17 +459,20 @@ __global__ void __launch_bounds__(kHeadRows) k_simt_head(HeadArgs a) {
       Xt[(4 * c + 2) * kHeadRows + r] = q.z * s;
       Xt[(4 * c + 3) * kHeadRows + r] = q.w * s;
     }
+    if (half) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {  // LGGS 3 -> 8, bias after the sum
-      float acc = g * __ldg(w + WOFF(LGGSW) + 3 * i) + gamma * __ldg(w + WOFF(LGGSW) + 3 * i + 1) +
-                  sc * __ldg(w + WOFF(LGGSW) + 3 * i + 2);
-      acc += __ldg(w + WOFF(LGGSB) + i);
-      Xt[(120 + i) * kHeadRows + r] = relu0(acc);
+      for (int i = 0; i < 8; ++i) {  // LGGS 3 -> 8, bias after the sum
+        float acc = g * __ldg(w + WOFF(LGGSW) + 3 * i) + gamma * __ldg(w + WOFF(LGGSW) + 3 * i + 1) +
+                    sc * __ldg(w + WOFF(LGGSW) + 3 * i + 2);
+        acc += __ldg(w + WOFF(LGGSB) + i);
+        Xt[(120 + i) * kHeadRows + r] = relu0(acc);
+      }
     }
-    block_gemm<128, 128>(Xt, Yt, a.wt, w + WOFF(LC0B));
-    block_gemm<128, 64>(Yt, Xt, a.wt + 128 * 128, w + WOFF(LC1B));
-    block_gemm<64, 32>(Xt, Yt, a.wt + 128 * 128 + 128 * 64, w + WOFF(LC2B));
+    block_gemm<128, 128>(Xt, Yt, w + WOFF(LC0B), ws, chunk);
+    block_gemm<128, 64>(Yt, Xt, w + WOFF(LC1B), ws, chunk);
+    block_gemm<64, 32>(Xt, Yt, w + WOFF(LC2B), ws, chunk);
     __syncthreads();
+    if (half) continue;  // the per-row tail runs on the first 128 threads
     float x32[32];
 #pragma unroll
     for (int i = 0; i < 32; ++i) x32[i] = Yt[i * kHeadRows + r];
@@ -458,8 +508,10 @@ __global__ void __launch_bounds__(kHeadRows) k_simt_head(HeadArgs a) {
     if (ch == 0) X[0] = xo;
     else if (ch == 1) X[1] = xo;
     else X[2] = xo;
-    __syncthreads();  // Xt / Yt are rebuilt by the next channel
+    // Xt and Yt are next written after the first barrier of the next channel
   }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  if (half) return;
   if (srp[1] == srp[0]) X[1] = X[0];
   if (srp[2] == srp[0]) X[2] = X[0];
   else if (srp[2] == srp[1]) X[2] = X[1];
@@ -537,7 +589,7 @@ int launch_mlp_simt(const Network* net, const float* desc, const float* aux, lon
   h.scatter = scatter;
   h.job = job;
   h.bout = bout;
-  k_simt_head<<<(unsigned)((n + kHeadRows - 1) / kHeadRows), kHeadRows, kHeadSmem, s>>>(h);
+  k_simt_head<<<(unsigned)((n + kHeadRows - 1) / kHeadRows), kHeadThreads, kHeadSmem, s>>>(h);
   MR_CUDA(cudaGetLastError());
   return MR_OK;
 }
