@@ -74,7 +74,7 @@ struct Network {
   size_t packed_bytes = 0;
   std::vector<float> h_rowwise;  // fp32 per-row weights passed as kernel parameters (mr_mlp_tc.cu)
   std::vector<float> h_winv8;    // inverse per-layer scales of the E4M3 weight image
-  float* head_t = nullptr;       // LC0 / LC1 / LC2 transposed to [in][out] for the fp32 head (mr_mlp_simt.cu)
+  float* simt_img = nullptr;     // weight image of the fp32 network kernels (simt_weight_image)
   float h_stencil[MR_STENCIL_POINTS * 3];
 };
 

@@ -1,42 +1,104 @@
-// FP32 radiance-predictor network, one thread per pixel, activations in
-// registers (core/radiancePredict.cu:370-485 in fp32).
+// FP32 radiance-predictor network on the CUDA cores, in two kernels
+// (core/radiancePredict.cu:370-485 in fp32).
 //
 // Descriptors are read in chunks of 4 features: (row k, features 4j..4j+3) is
 // the float4 at desc[k*rs + j*cs]; the render path passes chunk-of-4
-// feature-major columns (rs = 4, cs = 4*capacity) so that a warp's
-// 32 loads of one feature are one coalesced transaction. Every layer up to
-// 32 wide is fully unrolled with compile-time register indices; the three
-// branches of a block are evaluated together (three independent FMA chains),
-// and blocks of equal width share one code instance through a runtime loop
-// over their weight offsets. Weights are read as warp-uniform float4 loads.
-// The head (LC0 128x128, LC1, LC2: 62 % of the multiply-adds) runs in a second
-// kernel as block GEMMs over shared-memory activation tiles, so that no
-// 128-wide vector has to live in a thread's registers.
+// feature-major columns (rs = 4, cs = 4*capacity) so that a warp's 32 loads
+// of one chunk are one coalesced transaction.
+//
+// Both kernels work on tiles of 128 rows whose activations live in shared
+// memory, column-major (feature f of tile row r at [f*128 + r]):
+//  * k_simt_trunk: the two trunks. The squeeze-excitation statistics and
+//    gates, the width-8 blocks and LD41 run per row (one thread per row);
+//    the width-16 and width-32 layers (77 % of the trunk's multiply-adds) run
+//    as register-tiled block GEMMs over the tile, with their weights
+//    pre-transposed and double-buffered in shared memory by cp.async.
+//  * k_simt_head: the head (LC0 128x128, LC1, LC2: 62 % of all multiply-adds)
+//    as block GEMMs, then LX and the residual pairs per row.
+// Every dot product starts at the bias and adds the inputs in ascending
+// order, as LinearReLU does.
+#include <vector>
+
 #include "mr_internal.h"
 #include "mr_net_layout.cuh"
 
 namespace mr {
 
-constexpr int kSimtThreads = 128;
-
-struct SimtArgs {
-  const float* __restrict__ w;
-  const float* __restrict__ desc;
-  const float* __restrict__ aux;
-  long long rs, cs;      // desc strides (row, 4-feature chunk)
-  long long ars, afs;    // aux strides
-  int n;
-  const unsigned* __restrict__ count;  // device row count (render path) or null
-  float* out;                          // n x 3, or image (compose mode)
-  const int* __restrict__ pix;
-  const float* __restrict__ trph;
-  F3 light_color, scatter;
-  const int* job;        // batched compose: job of each record (null: single image)
-  const BatchOut* bout;  // batched compose: per-job outputs
-};
+constexpr int kTile = 128;  // rows per tile
 
 __device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
 __device__ __forceinline__ float relu0(float x) { return x >= 0.0f ? x : 0.0f; }
+
+__device__ __forceinline__ void cp_async16(float* dst, const float* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+
+// ---- weight image of the fp32 kernels -------------------------------------------------
+// [head: LC0 | LC1 | LC2, each transposed to [in][out]]
+// [trunk stages 0..6: blocks 2..7 of the main trunk and L81; per stage the
+//  three branches' [in][out] weights, each followed by its bias]
+constexpr int kHeadImage = 128 * 128 + 128 * 64 + 64 * 32;
+constexpr int kTrunkStages = 7;
+__host__ __device__ constexpr int stage_width(int g) { return g < 3 ? 16 : 32; }
+__host__ __device__ constexpr int stage_floats(int g) { return 3 * (stage_width(g) * stage_width(g) + stage_width(g)); }
+__host__ __device__ constexpr int stage_offset(int g) { return g <= 3 ? 816 * g : 2448 + 3168 * (g - 3); }
+static_assert(stage_offset(1) == stage_floats(0) && stage_offset(4) == stage_offset(3) + stage_floats(3),
+              "stage offsets");
+constexpr int kSimtImage = kHeadImage + stage_offset(kTrunkStages);
+
+void simt_weight_image(const float* w, std::vector<float>& img) {
+  const WeightTable wt = make_weight_table();
+  img.assign(kSimtImage, 0.0f);
+  auto put_t = [&](size_t o, int id, int N, int K) {  // W[N][K] -> [K][N] at o
+    const float* W = w + wt.off[id];
+    for (int k = 0; k < K; ++k)
+      for (int c = 0; c < N; ++c) img[o + (size_t)k * N + c] = W[(size_t)c * K + k];
+  };
+  put_t(0, MR_W_LC0W, 128, 128);
+  put_t(128 * 128, MR_W_LC1W, 64, 128);
+  put_t(128 * 128 + 128 * 64, MR_W_LC2W, 32, 64);
+  const int ids[kTrunkStages][3][2] = {
+      {{MR_W_L21W, MR_W_L21B}, {MR_W_L_Tr21W, MR_W_L_Tr21B}, {MR_W_L_Hg21W, MR_W_L_Hg21B}},
+      {{MR_W_L31W, MR_W_L31B}, {MR_W_L_Tr31W, MR_W_L_Tr31B}, {MR_W_L_Hg31W, MR_W_L_Hg31B}},
+      {{MR_W_L41W, MR_W_L41B}, {MR_W_L_Tr41W, MR_W_L_Tr41B}, {MR_W_L_Hg41W, MR_W_L_Hg41B}},
+      {{MR_W_L51W, MR_W_L51B}, {MR_W_L_Tr51W, MR_W_L_Tr51B}, {MR_W_L_Hg51W, MR_W_L_Hg51B}},
+      {{MR_W_L61W, MR_W_L61B}, {MR_W_L_Tr61W, MR_W_L_Tr61B}, {MR_W_L_Hg61W, MR_W_L_Hg61B}},
+      {{MR_W_L71W, MR_W_L71B}, {MR_W_L_Tr71W, MR_W_L_Tr71B}, {MR_W_L_Hg71W, MR_W_L_Hg71B}},
+      {{MR_W_L81W, MR_W_L81B}, {MR_W_L_Tr81W, MR_W_L_Tr81B}, {MR_W_L_Hg81W, MR_W_L_Hg81B}}};
+  for (int g = 0; g < kTrunkStages; ++g) {
+    const int S = stage_width(g);
+    size_t o = kHeadImage + stage_offset(g);
+    for (int b = 0; b < 3; ++b) {
+      put_t(o, ids[g][b][0], S, S);
+      for (int c = 0; c < S; ++c) img[o + S * S + c] = w[wt.off[ids[g][b][1]] + c];
+      o += S * S + S;
+    }
+  }
+}
+
+// ---- trunk ---------------------------------------------------------------------------
+
+struct TrunkArgs {
+  const float* __restrict__ w;
+  const float* __restrict__ img;  // simt_weight_image
+  const float* __restrict__ desc;
+  const float* __restrict__ aux;
+  long long rs, cs;    // desc strides (row, 4-feature chunk)
+  long long ars, afs;  // aux strides
+  int n;
+  const unsigned* __restrict__ count;  // device row count (render path) or null
+};
+
+// Trunk outputs per row, handed from the trunk kernel to the head kernel:
+// comb[0..120) (the L81 / LD41 outputs before gating) and fin[0..16) (the
+// LSEFin1 sums over pool[0..74), without the albedo term), 136 values in
+// chunks of 4: chunk c of row k is the float4 at t[k*rs + c*cs].
+struct TrunkOut {
+  float* t;
+  long long rs, cs;
+};
 
 // One descriptor row; the address of each chunk is formed inside the asm so
 // that the compiler does not keep a row address per feature live for reuse
@@ -53,6 +115,13 @@ struct RowIO {
         : "r"(i >> 2), "r"(cs16), "l"(d));
     return v;
   }
+};
+
+// The running trunk state y of a row (3 branches x up to 32 values) in the
+// tile, one column per thread: conflict-free.
+struct YS {
+  float* p;  // tile base + row
+  __device__ __forceinline__ float& at(int b, int i) const { return p[(b * 32 + i) * kTile]; }
 };
 
 // yn = ReLU(B + W x) for one branch, S x S (bias stored after W): bias first,
@@ -80,24 +149,13 @@ __device__ __forceinline__ void dense1(const float* x, float* yn, const float* _
   }
 }
 
-// SE / SERES block of width S (radiancePredict.cu:240-294). MODE 0: SE +
-// ADD3, 1: SERES + ADD3, 2: SERES + REP3. The block's pooled statistics
-// (pool[pid+b], pool[36+pid+b]) go straight into the 16 LSEFin1 sums `fin`;
-// the three branches are evaluated one after another to keep register
-// pressure low. Weight offsets are runtime values so that blocks of equal
-// width and mode share this code.
-// The running trunk state y of a row (3 branches x up to 32 values) in
-// shared memory, one column per thread: conflict-free, and out of the
-// registers, which hold one branch's input and output at a time.
-struct YS {
-  float* p;  // smem base + thread index
-  __device__ __forceinline__ float& at(int b, int i) const { return p[(b * 32 + i) * kSimtThreads]; }
-};
-
-template <int S, int MODE>
-__device__ __forceinline__ void simt_block(const RowIO& in, const float* __restrict__ w, int from, int pid, int sew0,
-                                           int sew1, int wa, int wb, int wc, float g, float gamma, const YS& y,
-                                           float (&fin)[16]) {
+// Squeeze-excitation of a block of width S (radiancePredict.cu:240-294):
+// pooled statistics of the block input (mean, max per branch), which also go
+// straight into the 16 LSEFin1 sums `fin` (pool[pid+b], pool[36+pid+b]), and
+// the three branch gates.
+template <int S>
+__device__ __forceinline__ void se_gates(const RowIO& in, const float* __restrict__ w, int from, int pid, int sew0,
+                                         int sew1, float g, float gamma, float (&fin)[16], float (&gate)[3]) {
   float mean[3], mx[3];
 #pragma unroll
   for (int b = 0; b < 3; ++b) {
@@ -131,7 +189,6 @@ __device__ __forceinline__ void simt_block(const RowIO& in, const float* __restr
     for (int j = 0; j < 8; ++j) a += tmp[j] * __ldg(w + sew0 + j + i * 8);
     h[i] = relu0(a);
   }
-  float gate[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
     float a = 0.0f;
@@ -139,13 +196,24 @@ __device__ __forceinline__ void simt_block(const RowIO& in, const float* __restr
     for (int j = 0; j < 8; ++j) a += h[j] * __ldg(w + sew1 + j + i * 8);
     gate[i] = 1.0f / (1.0f + expf(-a));
   }
+}
+
+// Block of width 8, per row. MODE 0: SE + ADD3, 1: SERES + ADD3, 2: SERES +
+// REP3. Weight offsets are runtime values so that blocks of equal mode share
+// this code.
+template <int MODE>
+__device__ __forceinline__ void row_block8(const RowIO& in, const float* __restrict__ w, int from, int pid, int sew0,
+                                           int sew1, int wa, int wb, int wc, float g, float gamma, const YS& y,
+                                           float (&fin)[16]) {
+  float gate[3];
+  se_gates<8>(in, w, from, pid, sew0, sew1, g, gamma, fin, gate);
 #pragma unroll 1
   for (int b = 0; b < 3; ++b) {
     const int wo = b == 0 ? wa : b == 1 ? wb : wc;
     const float gb = b == 0 ? gate[0] : b == 1 ? gate[1] : gate[2];
-    float x[32], yn[32];
+    float x[8], yn[8];
 #pragma unroll
-    for (int i = 0; i < S; i += 4) {
+    for (int i = 0; i < 8; i += 4) {
       const float4 q = in.ld4(b * 192 + from + i);
       const float qv[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
@@ -154,16 +222,16 @@ __device__ __forceinline__ void simt_block(const RowIO& in, const float* __restr
         x[i + u] = MODE == 0 ? v : v + y.at(b, i + u);
       }
     }
-    dense1<S>(x, yn, w + wo);
+    dense1<8>(x, yn, w + wo);
 #pragma unroll
-    for (int i = 0; i < S; i += 4) {
+    for (int i = 0; i < 8; i += 4) {
       const float4 q = in.ld4(b * 192 + from + i);
       const float qv[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         if (MODE == 2) {
           y.at(b, i + u) = yn[i + u];
-          y.at(b, S + i + u) = qv[u];
+          y.at(b, 8 + i + u) = qv[u];
         } else {
           y.at(b, i + u) = yn[i + u] + qv[u];
         }
@@ -172,96 +240,182 @@ __device__ __forceinline__ void simt_block(const RowIO& in, const float* __restr
   }
 }
 
-// 16 -> 16 layer in registers.
-__device__ __forceinline__ void dense16(const float (&x)[16], float (&y)[16], const float* __restrict__ W,
-                                        const float* __restrict__ B) {
+// Per-row half of a width-S SERES block run as a block GEMM: gates, then the
+// layer input x = in * gate + y written over y in the tile.
+template <int S>
+__device__ __forceinline__ void row_gate_input(const RowIO& in, const float* __restrict__ w, int from, int pid,
+                                               int sew0, int sew1, float g, float gamma, const YS& y,
+                                               float (&fin)[16]) {
+  float gate[3];
+  se_gates<S>(in, w, from, pid, sew0, sew1, g, gamma, fin, gate);
 #pragma unroll
-  for (int i = 0; i < 16; ++i) {
-    float acc = __ldg(B + i);
+  for (int b = 0; b < 3; ++b) {
+#pragma unroll 4
+    for (int i = 0; i < S; i += 4) {
+      const float4 q = in.ld4(b * 192 + from + i);
+      const float qv[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
-    for (int j = 0; j < 16; j += 4) {
-      float4 q = ldg4(W + i * 16 + j);
-      acc += x[j] * q.x;
-      acc += x[j + 1] * q.y;
-      acc += x[j + 2] * q.z;
-      acc += x[j + 3] * q.w;
+      for (int u = 0; u < 4; ++u) {
+        const float v = qv[u] * gate[b];
+        y.at(b, i + u) = v + y.at(b, i + u);
+      }
     }
-    y[i] = relu0(acc);
   }
 }
 
-// Trunk outputs per row, handed from the trunk kernel to the head kernel:
-// comb[0..120) (the L81 / LD41 outputs before gating) and fin[0..16) (the
-// LSEFin1 sums over pool[0..74), without the albedo term), 136 values in
-// chunks of 4: chunk c of row k is the float4 at t[k*rs + c*cs].
-struct TrunkOut {
-  float* t;
-  long long rs, cs;
-};
+// Trunk weight stage g into ring buffer g % 2 (one commit group per call,
+// empty past the last stage).
+__device__ __forceinline__ void trunk_stage_issue(const float* __restrict__ img, float* ring, int g) {
+  if (g < kTrunkStages) {
+    const float* src = img + kHeadImage + stage_offset(g);
+    float* dst = ring + (g & 1) * stage_floats(kTrunkStages - 1);
+    const int pieces = stage_floats(g) / 4;
+    for (int i = threadIdx.x; i < pieces; i += kTile) cp_async16(dst + 4 * i, src + 4 * i);
+  }
+  cp_async_commit();
+}
 
-// Trunks of RadiancePredict (radiancePredict.cu:385-437), one thread per row.
-__global__ void __launch_bounds__(kSimtThreads) k_simt_trunk(SimtArgs a, TrunkOut to) {
+// The three branch layers of a trunk stage of width S as block GEMMs over the
+// tile: out_b = ReLU(B_b + W_b x_b), x_b = tile columns [32b, 32b+S). Thread
+// t owns 4 consecutive columns (c0) and S/4 rows in quads: for S = 32 rows
+// 4g..4g+3 and 64+4g..64+4g+3 (g = t % 16, c0 = 4 (t / 16)); for S = 16
+// rows 4g..4g+3 (g = t % 32, c0 = 4 (t / 32)). Epilogue EPI 0: y = out + in
+// (SERES + ADD3); 1: y[0..S) = out, y[S..2S) = in (SERES + REP3); 2: the
+// outputs go to comb (L81).
+template <int S, int EPI>
+__device__ __forceinline__ void trunk_gemm(float* tile, const float* W, const float* __restrict__ desc, long long rs,
+                                           long long cs, int row0, int n, int from, const TrunkOut& to) {
+  constexpr int NQ = S / 16;            // row quads per thread
+  constexpr int G = 32 / NQ;            // row groups
+  constexpr int QS = kTile / NQ;        // distance between a thread's quads
+  const int t = threadIdx.x, r0 = 4 * (t % G), c0 = 4 * (t / G);
+#pragma unroll 1
+  for (int b = 0; b < 3; ++b) {
+    const float* X = tile + b * 32 * kTile;
+    const float* Wb = W + b * (S * S + S);
+    float acc[4 * NQ][4];
+    {
+      const float4 bias = *reinterpret_cast<const float4*>(Wb + S * S + c0);
+#pragma unroll
+      for (int i = 0; i < 4 * NQ; ++i) {
+        acc[i][0] = bias.x; acc[i][1] = bias.y; acc[i][2] = bias.z; acc[i][3] = bias.w;
+      }
+    }
+#pragma unroll 8
+    for (int k = 0; k < S; ++k) {
+      const float4 wv = *reinterpret_cast<const float4*>(Wb + k * S + c0);
+      const float wa[4] = {wv.x, wv.y, wv.z, wv.w};
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        const float4 xv = *reinterpret_cast<const float4*>(X + k * kTile + q * QS + r0);
+        const float xa[4] = {xv.x, xv.y, xv.z, xv.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[4 * q + i][j] = fmaf(xa[i], wa[j], acc[4 * q + i][j]);
+      }
+    }
+    if (EPI != 2) __syncthreads();  // every read of x_b is done before y_b overwrites it
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int rr = q * QS + r0 + i, row = row0 + rr;
+        const int kr = row < n ? row : n - 1;
+        float o[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) o[j] = relu0(acc[4 * q + i][j]);
+        if (EPI == 2) {
+          if (row < n)
+            *reinterpret_cast<float4*>(to.t + (long long)row * to.rs + (8 * b + c0 / 4) * to.cs) =
+                make_float4(o[0], o[1], o[2], o[3]);
+        } else {
+          const float4 inv = ldg4(desc + (long long)kr * rs + ((b * 192 + from + c0) >> 2) * cs);
+          const float iv[4] = {inv.x, inv.y, inv.z, inv.w};
+          float* yc = tile + (b * 32 + c0) * kTile + rr;
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            if (EPI == 0) {
+              yc[j * kTile] = o[j] + iv[j];
+            } else {
+              yc[j * kTile] = o[j];
+              yc[(S + j) * kTile] = iv[j];
+            }
+          }
+        }
+      }
+  }
+}
+
+constexpr int kTrunkSmem = (96 * kTile + 2 * 3 * (32 * 32 + 32)) * (int)sizeof(float);
+
+// Trunks of RadiancePredict (radiancePredict.cu:385-437) for a tile of 128
+// rows, one thread per row in the per-row parts.
+__global__ void __launch_bounds__(kTile, 3) k_simt_trunk(TrunkArgs a, TrunkOut to) {
+  extern __shared__ __align__(16) float tsm[];
+  float* tile = tsm;
+  float* ring = tsm + 96 * kTile;
   const int n = a.count ? (int)min(*a.count, (unsigned)a.n) : a.n;
-  const int k = blockIdx.x * kSimtThreads + threadIdx.x;
-  if (k >= n) return;
+  const int row0 = blockIdx.x * kTile;
+  if (row0 >= n) return;  // block-uniform
+  trunk_stage_issue(a.img, ring, 0);
+  trunk_stage_issue(a.img, ring, 1);
+  const int r = threadIdx.x, row = row0 + r;
+  const int kr = row < n ? row : n - 1;
   const float* __restrict__ w = a.w;
-  RowIO in{a.desc + (long long)k * a.rs, (int)(a.cs * 4)};
-  const float* ax = a.aux + (long long)k * a.ars;
+  RowIO in{a.desc + (long long)kr * a.rs, (int)(a.cs * 4)};
+  const float* ax = a.aux + (long long)kr * a.ars;
   const float g = __ldg(ax), gamma = __ldg(ax + a.afs);
   float fin[16];
 #pragma unroll
   for (int j = 0; j < 16; ++j) fin[j] = 0.0f;
-  __shared__ float ysm[96 * kSimtThreads];
-  const YS y{ysm + threadIdx.x};
-  // main trunk (radiancePredict.cu:396-421)
-  simt_block<8, 0>(in, w, 0, 0, WOFF(LSE01W), WOFF(LSE02W), WOFF(L01W), WOFF(L_Tr01W), WOFF(L_Hg01W), g, gamma, y, fin);
-  simt_block<8, 2>(in, w, 8, 3, WOFF(LSE11W), WOFF(LSE12W), WOFF(L11W), WOFF(L_Tr11W), WOFF(L_Hg11W), g, gamma, y, fin);
-  {
-    const int p16[2][5] = {{WOFF(LSE21W), WOFF(LSE22W), WOFF(L21W), WOFF(L_Tr21W), WOFF(L_Hg21W)},
-                           {WOFF(LSE31W), WOFF(LSE32W), WOFF(L31W), WOFF(L_Tr31W), WOFF(L_Hg31W)}};
+  const YS y{tile + r};
+  // main trunk (radiancePredict.cu:396-421): blocks 0, 1 per row, 2..7 as GEMMs
+  row_block8<0>(in, w, 0, 0, WOFF(LSE01W), WOFF(LSE02W), WOFF(L01W), WOFF(L_Tr01W), WOFF(L_Hg01W), g, gamma, y, fin);
+  row_block8<2>(in, w, 8, 3, WOFF(LSE11W), WOFF(LSE12W), WOFF(L11W), WOFF(L_Tr11W), WOFF(L_Hg11W), g, gamma, y, fin);
+  const int se[6][2] = {{WOFF(LSE21W), WOFF(LSE22W)}, {WOFF(LSE31W), WOFF(LSE32W)}, {WOFF(LSE41W), WOFF(LSE42W)},
+                        {WOFF(LSE51W), WOFF(LSE52W)}, {WOFF(LSE61W), WOFF(LSE62W)}, {WOFF(LSE71W), WOFF(LSE72W)}};
 #pragma unroll 1
-    for (int b = 0; b < 2; ++b)
-      simt_block<16, 1>(in, w, 16 + 16 * b, 6 + 3 * b, p16[b][0], p16[b][1], p16[b][2], p16[b][3], p16[b][4], g,
-                        gamma, y, fin);
+  for (int st = 0; st < 6; ++st) {
+    const int S = stage_width(st), from = st < 3 ? 16 + 16 * st : 64 + 32 * (st - 3), pid = 6 + 3 * st;
+    if (S == 16)
+      row_gate_input<16>(in, w, from, pid, se[st][0], se[st][1], g, gamma, y, fin);
+    else
+      row_gate_input<32>(in, w, from, pid, se[st][0], se[st][1], g, gamma, y, fin);
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    __syncthreads();  // stage st's weights and every row's input are in the tile
+    const float* W = ring + (st & 1) * stage_floats(kTrunkStages - 1);
+    if (st < 2)
+      trunk_gemm<16, 0>(tile, W, a.desc, a.rs, a.cs, row0, n, from, to);
+    else if (st == 2)
+      trunk_gemm<16, 1>(tile, W, a.desc, a.rs, a.cs, row0, n, from, to);
+    else
+      trunk_gemm<32, 0>(tile, W, a.desc, a.rs, a.cs, row0, n, from, to);
+    trunk_stage_issue(a.img, ring, st + 2);  // ring buffer st % 2 is free: every thread passed the GEMM's barriers
+    __syncthreads();                          // y complete for the per-row part
   }
-  simt_block<16, 2>(in, w, 48, 12, WOFF(LSE41W), WOFF(LSE42W), WOFF(L41W), WOFF(L_Tr41W), WOFF(L_Hg41W), g, gamma, y,
-                    fin);
-  {
-    const int p32[3][5] = {{WOFF(LSE51W), WOFF(LSE52W), WOFF(L51W), WOFF(L_Tr51W), WOFF(L_Hg51W)},
-                           {WOFF(LSE61W), WOFF(LSE62W), WOFF(L61W), WOFF(L_Tr61W), WOFF(L_Hg61W)},
-                           {WOFF(LSE71W), WOFF(LSE72W), WOFF(L71W), WOFF(L_Tr71W), WOFF(L_Hg71W)}};
-#pragma unroll 1
-    for (int b = 0; b < 3; ++b)
-      simt_block<32, 1>(in, w, 64 + 32 * b, 15 + 3 * b, p32[b][0], p32[b][1], p32[b][2], p32[b][3], p32[b][4], g,
-                        gamma, y, fin);
-  }
-  float* orow = to.t + (long long)k * to.rs;
+  // L81 -> comb[0..96)
+  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+  __syncthreads();
+  trunk_gemm<32, 2>(tile, ring + (6 & 1) * stage_floats(kTrunkStages - 1), a.desc, a.rs, a.cs, row0, n, 0, to);
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncthreads();  // the tile is free for the light-direction trunk
+  const bool valid = row < n;
+  float* orow = to.t + (long long)row * to.rs;
   auto put4 = [&](int c, float x0, float x1, float x2, float x3) {
-    *reinterpret_cast<float4*>(orow + c * to.cs) = make_float4(x0, x1, x2, x3);
+    if (valid) *reinterpret_cast<float4*>(orow + c * to.cs) = make_float4(x0, x1, x2, x3);
   };
-  {  // L81: comb[0..96), one branch at a time, stored right away
-    const int wl[3] = {WOFF(L81W), WOFF(L_Tr81W), WOFF(L_Hg81W)};
-#pragma unroll
-    for (int b = 0; b < 3; ++b) {
-      float xin[32], c[32];
-#pragma unroll
-      for (int i = 0; i < 32; ++i) xin[i] = y.at(b, i);
-      dense1<32>(xin, c, w + wl[b]);
-#pragma unroll
-      for (int i = 0; i < 32; i += 4) put4((32 * b + i) / 4, c[i], c[i + 1], c[i + 2], c[i + 3]);
-    }
-  }
-  // light-direction trunk (:424-437)
-  simt_block<8, 0>(in, w, 160, 24, WOFF(LDSE01W), WOFF(LDSE02W), WOFF(LD01W), WOFF(LD_Tr01W), WOFF(LD_Hg01W), g, gamma,
-                   y, fin);
+  // light-direction trunk (:424-437), per row
+  row_block8<0>(in, w, 160, 24, WOFF(LDSE01W), WOFF(LDSE02W), WOFF(LD01W), WOFF(LD_Tr01W), WOFF(LD_Hg01W), g, gamma,
+                y, fin);
   {
     const int pd[3][5] = {{WOFF(LDSE11W), WOFF(LDSE12W), WOFF(LD11W), WOFF(LD_Tr11W), WOFF(LD_Hg11W)},
                           {WOFF(LDSE21W), WOFF(LDSE22W), WOFF(LD21W), WOFF(LD_Tr21W), WOFF(LD_Hg21W)},
                           {WOFF(LDSE31W), WOFF(LDSE32W), WOFF(LD31W), WOFF(LD_Tr31W), WOFF(LD_Hg31W)}};
 #pragma unroll 1
     for (int b = 0; b < 3; ++b)
-      simt_block<8, 1>(in, w, 168 + 8 * b, 27 + 3 * b, pd[b][0], pd[b][1], pd[b][2], pd[b][3], pd[b][4], g, gamma, y,
-                       fin);
+      row_block8<1>(in, w, 168 + 8 * b, 27 + 3 * b, pd[b][0], pd[b][1], pd[b][2], pd[b][3], pd[b][4], g, gamma, y,
+                    fin);
   }
   {  // LD41: comb[96..120)
     const int wl[3] = {WOFF(LD41W), WOFF(LD_Tr41W), WOFF(LD_Hg41W)};
@@ -284,9 +438,27 @@ __global__ void __launch_bounds__(kSimtThreads) k_simt_trunk(SimtArgs a, TrunkOu
   for (int j0 = 0; j0 < 16; j0 += 4) put4(30 + j0 / 4, fin[j0], fin[j0 + 1], fin[j0 + 2], fin[j0 + 3]);
 }
 
+// 16 -> 16 layer in registers.
+__device__ __forceinline__ void dense16(const float (&x)[16], float (&y)[16], const float* __restrict__ W,
+                                        const float* __restrict__ B) {
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    float acc = __ldg(B + i);
+#pragma unroll
+    for (int j = 0; j < 16; j += 4) {
+      float4 q = ldg4(W + i * 16 + j);
+      acc += x[j] * q.x;
+      acc += x[j + 1] * q.y;
+      acc += x[j + 2] * q.z;
+      acc += x[j + 3] * q.w;
+    }
+    y[i] = relu0(acc);
+  }
+}
+
 // ---- head: block GEMMs over shared-memory activation tiles ---------------------------
 
-constexpr int kHeadRows = 128;     // rows (pixels) per block
+constexpr int kHeadRows = kTile;   // rows (pixels) per block
 constexpr int kHeadThreads = 256;  // two threads per row in the per-row stages
 constexpr int kChunk = 2048;       // floats per weight chunk (8 KB)
 constexpr int kHeadChunks = 13;    // LC0 8, LC1 4, LC2 1 chunks
@@ -309,11 +481,6 @@ struct HeadArgs {
   const int* job;
   const BatchOut* bout;
 };
-
-__device__ __forceinline__ void cp_async16(float* dst, const float* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
-               : "memory");
-}
 
 // The head weights (LC0, LC1, LC2 transposed; 13 chunks of 8 KB, repeated
 // per albedo channel) stream through a ring of kStages shared-memory buffers
@@ -550,10 +717,12 @@ int launch_mlp_simt(const Network* net, const float* desc, const float* aux, lon
   static bool attr = false;
   if (!attr) {
     MR_CUDA(cudaFuncSetAttribute(k_simt_head, cudaFuncAttributeMaxDynamicSharedMemorySize, kHeadSmem));
+    MR_CUDA(cudaFuncSetAttribute(k_simt_trunk, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrunkSmem));
     attr = true;
   }
-  SimtArgs a;
+  TrunkArgs a;
   a.w = net->w;
+  a.img = net->simt_img;
   a.desc = desc;
   a.aux = aux;
   a.rs = rs;
@@ -562,18 +731,11 @@ int launch_mlp_simt(const Network* net, const float* desc, const float* aux, lon
   a.afs = afs;
   a.n = n;
   a.count = count;
-  a.out = out;
-  a.pix = pix;
-  a.trph = trph;
-  a.light_color = light_color;
-  a.scatter = scatter;
-  a.job = job;
-  a.bout = bout;
-  k_simt_trunk<<<(unsigned)((n + kSimtThreads - 1) / kSimtThreads), kSimtThreads, 0, s>>>(a, TrunkOut{tout, trs, tcs});
+  k_simt_trunk<<<(unsigned)((n + kTile - 1) / kTile), kTile, kTrunkSmem, s>>>(a, TrunkOut{tout, trs, tcs});
   MR_CUDA(cudaGetLastError());
   HeadArgs h;
   h.w = net->w;
-  h.wt = net->head_t;
+  h.wt = net->simt_img;
   h.t = tout;
   h.trs = trs;
   h.tcs = tcs;

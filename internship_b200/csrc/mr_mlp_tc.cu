@@ -1145,6 +1145,8 @@ static uint8_t to_e4m3(float f) {
   return sign | (uint8_t)((E << 3) | q);
 }
 
+void simt_weight_image(const float* w, std::vector<float>& img);  // mr_mlp_simt.cu
+
 int pack_network(Network* n) {
   std::vector<float> w(MR_WEIGHT_TOTAL);
   if (cudaMemcpy(w.data(), n->w, MR_WEIGHT_TOTAL * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
@@ -1182,20 +1184,12 @@ int pack_network(Network* n) {
   n->h_rowwise.assign(kRowFloats, 0.0f);
   for (int id = 0; id < MR_W_COUNT; ++id)
     if (rt.off[id] >= 0) std::memcpy(&n->h_rowwise[rt.off[id]], w.data() + wt.off[id], wt.size[id] * sizeof(float));
-  // LC0 / LC1 / LC2 transposed ([in][out]) for the fp32 head kernel
+  // weight image of the fp32 kernels
   {
-    const int ids[3] = {MR_W_LC0W, MR_W_LC1W, MR_W_LC2W}, nk[3][2] = {{128, 128}, {64, 128}, {32, 64}};
-    std::vector<float> ht(128 * 128 + 128 * 64 + 64 * 32);
-    size_t o = 0;
-    for (int l = 0; l < 3; ++l) {
-      const float* W = w.data() + wt.off[ids[l]];
-      const int N = nk[l][0], K = nk[l][1];
-      for (int k = 0; k < K; ++k)
-        for (int c = 0; c < N; ++c) ht[o + (size_t)k * N + c] = W[(size_t)c * K + k];
-      o += (size_t)N * K;
-    }
-    cudaError_t e = cudaMalloc(&n->head_t, ht.size() * sizeof(float));
-    if (e == cudaSuccess) e = cudaMemcpy(n->head_t, ht.data(), ht.size() * sizeof(float), cudaMemcpyHostToDevice);
+    std::vector<float> si;
+    simt_weight_image(w.data(), si);
+    cudaError_t e = cudaMalloc(&n->simt_img, si.size() * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemcpy(n->simt_img, si.data(), si.size() * sizeof(float), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return set_error(MR_ERR_NOMEM, "pack_network: %s", cudaGetErrorString(e));
   }
   // [BF16 image | error word (256 B) | E4M3 image]
@@ -1210,8 +1204,8 @@ int pack_network(Network* n) {
 }
 
 void free_packed(Network* n) {
-  if (n->head_t) cudaFree(n->head_t);
-  n->head_t = nullptr;
+  if (n->simt_img) cudaFree(n->simt_img);
+  n->simt_img = nullptr;
   if (n->packed) cudaFree(n->packed);
   n->packed = nullptr;
   n->packed_bytes = 0;
