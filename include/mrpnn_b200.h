@@ -183,6 +183,16 @@ int mr_tc_selftest(int32_t n, int32_t k, const uint16_t* host_a, const uint16_t*
  * counterpart): host_a 128 x k and host_b n x k are E4M3 bytes, row-major.
  * Shapes (n, k): (16,32) (32,32) (64,128) (128,128). */
 int mr_tc_selftest_fp8(int32_t n, int32_t k, const uint8_t* host_a, const uint8_t* host_b, float* host_d);
+/* Self-test of the exact sampler's two forms (no reference counterpart): for
+ * n points uv (host_uv, n x 3, texture space) over one
+ * MR_SAMPLER_SELFTEST_RES^3 fp32 table (host_table, index (x*R+y)*R+z),
+ * host_out (n x 6) receives the trilinear border-0 filter from texel loads and
+ * from texture gathers, the trilinear clamp filter from loads and gathers, and
+ * the bilinear clamp filter of the table's first R x R values at (uv.x, uv.y)
+ * from loads and gathers. The two forms agree bit for bit except where a
+ * texel is subnormal (the texture unit reads those as 0). */
+#define MR_SAMPLER_SELFTEST_RES 32
+int mr_sampler_selftest(int32_t n, const float* host_table, const float* host_uv, float* host_out);
 /* Error word of the tensor-core network kernel of `net` (an mbarrier wait
  * that timed out): MR_ERR_TIMEOUT if set; `reset` clears it. */
 int mr_network_check(const mr_network* net, int32_t reset);

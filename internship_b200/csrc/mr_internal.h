@@ -59,6 +59,12 @@ struct Volume {
   cudaArray_t mip_arr[9] = {}, tr_arr[8] = {}, lut_arr = nullptr;
   cudaTextureObject_t mip_tex[9] = {}, tr_tex[8] = {}, lut_tex = 0;
   bool tex_mips_stale = true, tex_tr_stale = true, tex_lut_stale = true;
+  // Layered copies of the same tables (layer = x) read by the exact sampler
+  // through texture gathers, which return a 2 x 2 texel footprint unfiltered;
+  // created on first use, refreshed when the linear tables change.
+  cudaArray_t gth_mip_arr[9] = {}, gth_tr_arr[8] = {}, gth_lut_arr = nullptr;
+  cudaTextureObject_t gth_mip_tex[9] = {}, gth_tr_tex[8] = {}, gth_lut_tex = 0;
+  bool gth_mips_stale = true, gth_tr_stale = true, gth_lut_stale = true;
   // Per-render scratch owned by the volume (grown on demand).
   void* scratch = nullptr;
   size_t scratch_bytes = 0;
@@ -105,6 +111,10 @@ int ensure_scratch(Volume* v, size_t bytes, cudaStream_t s);
 int launch_update_tr(Volume* v, F3 L, float alpha, cudaStream_t s);
 int launch_update_lut(Volume* v, float g, uint32_t seed, cudaStream_t s);
 int refresh_textures(Volume* v, cudaStream_t s);
+int refresh_gather_textures(Volume* v, cudaStream_t s);
+// r^3 x-major fp32 table <-> cudaArray (3-D or layered, extent z, y, x)
+int copy_to_array(cudaArray_t arr, const float* src, int r, cudaStream_t s);
+int make_gather_tex(cudaArray_t* arr, cudaTextureObject_t* tex, int r, cudaTextureAddressMode mode);
 void destroy_textures(Volume* v);
 int sm_count();
 

@@ -317,33 +317,41 @@ __device__ __forceinline__ void trunk_gemm(float* tile, const float* W, const fl
     }
     if (EPI != 2) __syncthreads();  // every read of x_b is done before y_b overwrites it
 #pragma unroll
-    for (int q = 0; q < NQ; ++q)
+    for (int q = 0; q < NQ; ++q) {
+      const int rq = q * QS + r0;  // first of the quad's 4 rows
+      float o[4][4];               // [row][column]
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int rr = q * QS + r0 + i, row = row0 + rr;
-        const int kr = row < n ? row : n - 1;
-        float o[4];
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) o[j] = relu0(acc[4 * q + i][j]);
-        if (EPI == 2) {
-          if (row < n)
-            *reinterpret_cast<float4*>(to.t + (long long)row * to.rs + (8 * b + c0 / 4) * to.cs) =
-                make_float4(o[0], o[1], o[2], o[3]);
-        } else {
-          const float4 inv = ldg4(desc + (long long)kr * rs + ((b * 192 + from + c0) >> 2) * cs);
-          const float iv[4] = {inv.x, inv.y, inv.z, inv.w};
-          float* yc = tile + (b * 32 + c0) * kTile + rr;
+        for (int j = 0; j < 4; ++j) o[i][j] = relu0(acc[4 * q + i][j]);
+      if (EPI == 2) {
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            if (EPI == 0) {
-              yc[j * kTile] = o[j] + iv[j];
-            } else {
-              yc[j * kTile] = o[j];
-              yc[(S + j) * kTile] = iv[j];
-            }
+        for (int i = 0; i < 4; ++i)
+          if (row0 + rq + i < n)
+            *reinterpret_cast<float4*>(to.t + (long long)(row0 + rq + i) * to.rs + (8 * b + c0 / 4) * to.cs) =
+                make_float4(o[i][0], o[i][1], o[i][2], o[i][3]);
+      } else {
+        float iv[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int row = row0 + rq + i, kr = row < n ? row : n - 1;
+          const float4 v = ldg4(desc + (long long)kr * rs + ((b * 192 + from + c0) >> 2) * cs);
+          iv[i][0] = v.x; iv[i][1] = v.y; iv[i][2] = v.z; iv[i][3] = v.w;
+        }
+        // one float4 of 4 rows per column: a quarter warp stores 128 contiguous bytes
+        float* yc = tile + (b * 32 + c0) * kTile + rq;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          if (EPI == 0) {
+            *reinterpret_cast<float4*>(yc + j * kTile) =
+                make_float4(o[0][j] + iv[0][j], o[1][j] + iv[1][j], o[2][j] + iv[2][j], o[3][j] + iv[3][j]);
+          } else {
+            *reinterpret_cast<float4*>(yc + j * kTile) = make_float4(o[0][j], o[1][j], o[2][j], o[3][j]);
+            *reinterpret_cast<float4*>(yc + (S + j) * kTile) = make_float4(iv[0][j], iv[1][j], iv[2][j], iv[3][j]);
           }
         }
       }
+    }
   }
 }
 

@@ -24,7 +24,15 @@ struct Tables {
   const float* __restrict__ lut;
   // texture-unit copies (MR_SAMPLER_TEXTURE only)
   cudaTextureObject_t mip_tex[9], tr_tex[8], lut_tex;
+  // layered copies read by texture gathers (exact sampler, kSampGather)
+  cudaTextureObject_t mip_g[9], tr_g[8], lut_g;
 };
+
+// Sampler forms of the descriptor gather: the fp32 software filter over
+// texel loads, the texture units' linear filter (MR_SAMPLER_TEXTURE), and the
+// fp32 software filter over texture gathers (same values as the loads: the
+// default form of MR_SAMPLER_EXACT).
+enum { kSampLoad = 0, kSampTex = 1, kSampGather = 2 };
 
 __constant__ unsigned c_mip_off[9] = {0u, 16777216u, 18874368u, 19136512u, 19169280u, 19173376u, 19173888u,
                                       19173952u, 19173960u};
@@ -211,6 +219,63 @@ __device__ __forceinline__ float tri_clamp_c(const float* __restrict__ d, F3 uv)
                lerpf(lerpf(c100, c101, wz), lerpf(c110, c111, wz), wy), wx);
 }
 
+// The four texels of the 2 x 2 footprint whose first texel is (i, j) (layer
+// `layer` of a layered texture), unfiltered: with unnormalised coordinates
+// (i + 1, j + 1) the footprint is texels i, i+1 and j, j+1 exactly, and the
+// address mode supplies out-of-range texels. tld4 returns them in the order
+// (i, j+1), (i+1, j+1), (i+1, j), (i, j); the result is reordered to
+// {(i, j), (i+1, j), (i, j+1), (i+1, j+1)}.
+__device__ __forceinline__ float4 gather_a2d(cudaTextureObject_t t, int layer, float fi, float fj) {
+  float a, b, c, d;
+  asm("tld4.r.a2d.v4.f32.f32 {%0, %1, %2, %3}, [%4, {%5, %6, %7, %8}];"
+      : "=f"(a), "=f"(b), "=f"(c), "=f"(d)
+      : "l"(t), "r"(layer), "f"(fi + 1.0f), "f"(fj + 1.0f), "f"(0.0f));
+  return make_float4(d, c, a, b);
+}
+__device__ __forceinline__ float4 gather_2d(cudaTextureObject_t t, float fi, float fj) {
+  float a, b, c, d;
+  asm("tld4.r.2d.v4.f32.f32 {%0, %1, %2, %3}, [%4, {%5, %6}];"
+      : "=f"(a), "=f"(b), "=f"(c), "=f"(d)
+      : "l"(t), "f"(fi + 1.0f), "f"(fj + 1.0f));
+  return make_float4(d, c, a, b);
+}
+
+// tri_border_c / tri_clamp_c / bilinear_clamp over texture gathers: two
+// footprints (layers x and x+1) per trilinear sample, one per bilinear.
+// Same corner values and the same fp32 arithmetic.
+template <int RES>
+__device__ __forceinline__ float tri_border_g(cudaTextureObject_t t, F3 uv) {
+  float px = uv.x * RES - 0.5f, py = uv.y * RES - 0.5f, pz = uv.z * RES - 0.5f;
+  float fx = floorf(px), fy = floorf(py), fz = floorf(pz);
+  int x = (int)fx;
+  float wx = px - fx, wy = py - fy, wz = pz - fz;
+  const float4 z4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const float4 a = (unsigned)x < (unsigned)RES ? gather_a2d(t, x, fz, fy) : z4;
+  const float4 b = (unsigned)(x + 1) < (unsigned)RES ? gather_a2d(t, x + 1, fz, fy) : z4;
+  return lerpf(lerpf(lerpf(a.x, a.y, wz), lerpf(a.z, a.w, wz), wy),
+               lerpf(lerpf(b.x, b.y, wz), lerpf(b.z, b.w, wz), wy), wx);
+}
+template <int RES>
+__device__ __forceinline__ float tri_clamp_g(cudaTextureObject_t t, F3 uv) {
+  float px = uv.x * RES - 0.5f, py = uv.y * RES - 0.5f, pz = uv.z * RES - 0.5f;
+  float fx = floorf(px), fy = floorf(py), fz = floorf(pz);
+  int x = (int)fx;
+  float wx = px - fx, wy = py - fy, wz = pz - fz;
+  const float4 a = gather_a2d(t, min(max(x, 0), RES - 1), fz, fy);
+  const float4 b = gather_a2d(t, min(max(x + 1, 0), RES - 1), fz, fy);
+  return lerpf(lerpf(lerpf(a.x, a.y, wz), lerpf(a.z, a.w, wz), wy),
+               lerpf(lerpf(b.x, b.y, wz), lerpf(b.z, b.w, wz), wy), wx);
+}
+__device__ __forceinline__ float bilinear_clamp_g(cudaTextureObject_t t, int w, int h, float u, float v) {
+  float px = u * w - 0.5f, py = v * h - 0.5f;
+  float fx = floorf(px), fy = floorf(py);
+  float wx = px - fx, wy = py - fy;
+  const float4 c = gather_2d(t, fx, fy);
+  float a = lerpf(c.x, c.y, wx);
+  float b = lerpf(c.z, c.w, wx);
+  return lerpf(a, b, wy);
+}
+
 struct PixelGather {
   F3 pos, L, X, Y, Z, LX;
   float lx, ly, lz;   // LX in the (X, Y, Z) frame
@@ -225,7 +290,7 @@ constexpr unsigned kTrOff[8] = {0u, 2097152u, 2359296u, 2392064u, 2396160u, 2396
 // Stencil points [I0, I1) at mip level MIP, offset `off` (sphere points), or
 // the light-direction points with per-point offsets (SPHERE = false). HW
 // samples through the texture units instead of the fp32 software filter.
-template <int MIP, bool SPHERE, bool HW, int I0, int I1, class Sink>
+template <int MIP, bool SPHERE, int SAMP, int I0, int I1, class Sink>
 __device__ __forceinline__ void gather_seg(const Tables& t, const float* __restrict__ stencil, const PixelGather& q,
                                            float off, Sink& sink) {
   constexpr int R = 256 >> MIP;
@@ -261,16 +326,26 @@ __device__ __forceinline__ void gather_seg(const Tables& t, const float* __restr
       c1 = q.cXL;
       c2 = q.cLXL;
     }
-    const float dens = HW ? tex3D<float>(t.mip_tex[MIP], p.z + 0.5f, p.y + 0.5f, p.x + 0.5f)
-                          : tri_border_c<R>(mb, p + 0.5f);
+    const float dens = SAMP == kSampTex      ? tex3D<float>(t.mip_tex[MIP], p.z + 0.5f, p.y + 0.5f, p.x + 0.5f)
+                       : SAMP == kSampGather ? tri_border_g<R>(t.mip_g[MIP], p + 0.5f)
+                                             : tri_border_c<R>(mb, p + 0.5f);
     const float xv = __logf(1.0f + q.alpha * dens / 64.0f);
     float xh;
     if (SPHERE && MIP == 0 && I0 == 0 && i == 0) {
       xh = q.hg0;
     } else {
       const float u1 = c1 * 0.5f + 0.5f, u2 = c2 * 0.5f + 0.5f;
-      const float h0 = HW ? tex2D<float>(t.lut_tex, u1, vrow) : bilinear_clamp(t.lut, kLut, kLut, u1, vrow);
-      const float h1 = HW ? tex2D<float>(t.lut_tex, u2, vrow) : bilinear_clamp(t.lut, kLut, kLut, u2, vrow);
+      float h0, h1;
+      if (SAMP == kSampTex) {
+        h0 = tex2D<float>(t.lut_tex, u1, vrow);
+        h1 = tex2D<float>(t.lut_tex, u2, vrow);
+      } else if (SAMP == kSampGather) {
+        h0 = bilinear_clamp_g(t.lut_g, kLut, kLut, u1, vrow);
+        h1 = bilinear_clamp_g(t.lut_g, kLut, kLut, u2, vrow);
+      } else {
+        h0 = bilinear_clamp(t.lut, kLut, kLut, u1, vrow);
+        h1 = bilinear_clamp(t.lut, kLut, kLut, u2, vrow);
+      }
       xh = __logf(h0 * h1 + 1.0f);
     }
     F3 pt = p;
@@ -282,12 +357,14 @@ __device__ __forceinline__ void gather_seg(const Tables& t, const float* __restr
       pt = p + q.LX * o2;
     }
     if (fetch)
-      xs = HW ? tex3D<float>(t.tr_tex[TL], pt.z + 0.5f, pt.y + 0.5f, pt.x + 0.5f) : tri_clamp_c<RT>(tb, pt + 0.5f);
+      xs = SAMP == kSampTex      ? tex3D<float>(t.tr_tex[TL], pt.z + 0.5f, pt.y + 0.5f, pt.x + 0.5f)
+           : SAMP == kSampGather ? tri_clamp_g<RT>(t.tr_g[TL], pt + 0.5f)
+                                 : tri_clamp_c<RT>(tb, pt + 0.5f);
     sink(i, u, xv, xs, xh);
   }
 }
 
-template <bool HW, class Sink>
+template <int SAMP, class Sink>
 __device__ __forceinline__ void gather_fast(const Tables& t, const float* __restrict__ stencil, F3 pos, F3 L,
                                             const Frame& f, float alpha, float g, Sink sink) {
   PixelGather q;
@@ -298,18 +375,18 @@ __device__ __forceinline__ void gather_fast(const Tables& t, const float* __rest
   q.alpha = alpha;
   q.hg0 = __logf(hg_phase(dot(f.X, L), g) + 1.0f);
   const float ms = 0.6f;
-  gather_seg<0, true, HW, 0, 8>(t, stencil, q, 1.0f / 256.0f * lerpf(ms, 1.0f, 1.0f), sink);
-  gather_seg<1, true, HW, 8, 16>(t, stencil, q, 2.5f / 256.0f * lerpf(ms, 1.0f, 0.8f), sink);
-  gather_seg<2, true, HW, 16, 32>(t, stencil, q, 5.5f / 256.0f * lerpf(ms, 1.0f, 0.6f), sink);
-  gather_seg<3, true, HW, 32, 48>(t, stencil, q, 11.5f / 256.0f * lerpf(ms, 1.0f, 0.4f), sink);
-  gather_seg<4, true, HW, 48, 64>(t, stencil, q, 23.5f / 256.0f * lerpf(ms, 1.0f, 0.2f), sink);
-  gather_seg<5, true, HW, 64, 96>(t, stencil, q, 47.5f / 256.0f * ms, sink);
-  gather_seg<6, true, HW, 96, 128>(t, stencil, q, 95.5f / 256.0f * ms, sink);
-  gather_seg<7, true, HW, 128, 160>(t, stencil, q, 191.5f / 256.0f * ms, sink);
-  gather_seg<0, false, HW, 160, 168>(t, stencil, q, 1.0f, sink);
-  gather_seg<1, false, HW, 168, 176>(t, stencil, q, 1.0f, sink);
-  gather_seg<2, false, HW, 176, 184>(t, stencil, q, 1.0f, sink);
-  gather_seg<3, false, HW, 184, 192>(t, stencil, q, 1.0f, sink);
+  gather_seg<0, true, SAMP, 0, 8>(t, stencil, q, 1.0f / 256.0f * lerpf(ms, 1.0f, 1.0f), sink);
+  gather_seg<1, true, SAMP, 8, 16>(t, stencil, q, 2.5f / 256.0f * lerpf(ms, 1.0f, 0.8f), sink);
+  gather_seg<2, true, SAMP, 16, 32>(t, stencil, q, 5.5f / 256.0f * lerpf(ms, 1.0f, 0.6f), sink);
+  gather_seg<3, true, SAMP, 32, 48>(t, stencil, q, 11.5f / 256.0f * lerpf(ms, 1.0f, 0.4f), sink);
+  gather_seg<4, true, SAMP, 48, 64>(t, stencil, q, 23.5f / 256.0f * lerpf(ms, 1.0f, 0.2f), sink);
+  gather_seg<5, true, SAMP, 64, 96>(t, stencil, q, 47.5f / 256.0f * ms, sink);
+  gather_seg<6, true, SAMP, 96, 128>(t, stencil, q, 95.5f / 256.0f * ms, sink);
+  gather_seg<7, true, SAMP, 128, 160>(t, stencil, q, 191.5f / 256.0f * ms, sink);
+  gather_seg<0, false, SAMP, 160, 168>(t, stencil, q, 1.0f, sink);
+  gather_seg<1, false, SAMP, 168, 176>(t, stencil, q, 1.0f, sink);
+  gather_seg<2, false, SAMP, 176, 184>(t, stencil, q, 1.0f, sink);
+  gather_seg<3, false, SAMP, 184, 192>(t, stencil, q, 1.0f, sink);
 }
 
 // Gather only, for explicit points and frames (test / training entry).
@@ -325,7 +402,7 @@ __global__ void k_gather(Tables t, const float* __restrict__ stencil, const floa
     d[192 + i] = xs;
     d[384 + i] = xh;
   };
-  gather_fast<false>(t, stencil, f3(pos[3 * k], pos[3 * k + 1], pos[3 * k + 2]), L, f, alpha, g, sink);
+  gather_fast<kSampLoad>(t, stencil, f3(pos[3 * k], pos[3 * k + 1], pos[3 * k + 2]), L, f, alpha, g, sink);
   float* ax = aux + 5 * (size_t)k;
   ax[0] = g;
   ax[1] = acosf(dot(f.X, f.LX));
@@ -336,7 +413,7 @@ __global__ void k_gather(Tables t, const float* __restrict__ stencil, const floa
 // features 4j..4j+3 of record k at desc[(j*cap + k)*4 .. +3] (aux: feature i at
 // aux[i*cap + k]). A warp's 16-byte stores and the network's 16-byte loads of
 // one chunk are contiguous 512-byte transactions.
-template <bool HW>
+template <int SAMP>
 __global__ void __launch_bounds__(128) k_gather_fm(Tables t, const float* __restrict__ stencil, Records rec,
                                                    int cap, F3 L, float alpha, float g, F3 srp,
                                                    float* __restrict__ desc, float* __restrict__ aux) {
@@ -360,7 +437,7 @@ __global__ void __launch_bounds__(128) k_gather_fm(Tables t, const float* __rest
       d[(96 + (i >> 2)) * c] = bh;
     }
   };
-  gather_fast<HW>(t, stencil, pos, L, f, alpha, g, sink);
+  gather_fast<SAMP>(t, stencil, pos, L, f, alpha, g, sink);
   aux[k] = g;
   aux[c + k] = acosf(dot(f.X, f.LX));
   aux[2 * c + k] = srp.x;
@@ -395,7 +472,30 @@ static bool distinct_channels(const mr_render_params* p) {
 }
 
 static int neural_passes(Volume* v, const Network* net, const mr_render_params* p, float* dev_rgb, cudaStream_t s,
-                         void* base, bool timed, float* dev_dist = nullptr);
+                         void* base, bool timed, float* dev_dist = nullptr, bool no_alloc = false);
+
+// Linear tables of a volume plus the texture objects sampler form `samp`
+// reads, whose copies are brought up to date on stream s.
+static int fill_tables(Volume* v, int samp, Tables* t, cudaStream_t s) {
+  *t = Tables{};
+  t->mips = v->mips;
+  t->tr = v->tr;
+  t->lut = v->lut;
+  if (samp == kSampTex) {
+    int rc = refresh_textures(v, s);
+    if (rc) return rc;
+    for (int k = 0; k < 9; ++k) t->mip_tex[k] = v->mip_tex[k];
+    for (int k = 0; k < 8; ++k) t->tr_tex[k] = v->tr_tex[k];
+    t->lut_tex = v->lut_tex;
+  } else if (samp == kSampGather) {
+    int rc = refresh_gather_textures(v, s);
+    if (rc) return rc;
+    for (int k = 0; k < 9; ++k) t->mip_g[k] = v->gth_mip_tex[k];
+    for (int k = 0; k < 8; ++k) t->tr_g[k] = v->gth_tr_tex[k];
+    t->lut_g = v->gth_lut_tex;
+  }
+  return MR_OK;
+}
 
 static Records carve_records(void* base, size_t n) {
   char* p = (char*)base;
@@ -446,7 +546,7 @@ static int render_neural_impl(Volume* v, const Network* net, const mr_render_par
 // Trace, gather and network over scratch at `base` (neural_scratch_bytes of
 // width*height); `timed` = record stage events when the volume's timer is on.
 static int neural_passes(Volume* v, const Network* net, const mr_render_params* p, float* dev_rgb, cudaStream_t s,
-                         void* base, bool timed, float* dev_dist) {
+                         void* base, bool timed, float* dev_dist, bool no_alloc) {
   auto mark = [&](int st) { if (timed) v->timer.mark(st, s); };
   int rc = MR_OK;
   const F3 L = normalize(to_f3(p->light_dir));
@@ -475,22 +575,23 @@ static int neural_passes(Volume* v, const Network* net, const mr_render_params* 
   mark(ST_NN_TRACE);
   MR_CUDA(cudaGetLastError());
   F3 sr = to_f3(p->scatter_rate) / 1.001f;
-  Tables tabs{v->mips, v->tr, v->lut, {}, {}, 0};
-  const bool hw = p->sampler == MR_SAMPLER_TEXTURE;
-  if (hw) {
-    rc = refresh_textures(v, s);
-    if (rc) return rc;
-    for (int k = 0; k < 9; ++k) tabs.mip_tex[k] = v->mip_tex[k];
-    for (int k = 0; k < 8; ++k) tabs.tr_tex[k] = v->tr_tex[k];
-    tabs.lut_tex = v->lut_tex;
-  }
+  // the exact sampler reads texture gathers, or texel loads where nothing
+  // may be allocated (the layered copies are created on first use)
+  const int samp = p->sampler == MR_SAMPLER_TEXTURE ? kSampTex : no_alloc ? kSampLoad : kSampGather;
+  Tables tabs;
+  rc = fill_tables(v, samp, &tabs, s);
+  if (rc) return rc;
   mark(ST_NN_PREDICT);
-  if (hw)
-    k_gather_fm<true><<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(tabs, net->stencil, rec, (int)npx, L, p->alpha,
-                                                                    p->g, srp_of(sr), desc, aux);
+  const unsigned ggrid = (unsigned)((npx + 127) / 128);
+  if (samp == kSampTex)
+    k_gather_fm<kSampTex><<<ggrid, 128, 0, s>>>(tabs, net->stencil, rec, (int)npx, L, p->alpha, p->g, srp_of(sr),
+                                               desc, aux);
+  else if (samp == kSampGather)
+    k_gather_fm<kSampGather><<<ggrid, 128, 0, s>>>(tabs, net->stencil, rec, (int)npx, L, p->alpha, p->g, srp_of(sr),
+                                                  desc, aux);
   else
-    k_gather_fm<false><<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(tabs, net->stencil, rec, (int)npx, L, p->alpha,
-                                                                     p->g, srp_of(sr), desc, aux);
+    k_gather_fm<kSampLoad><<<ggrid, 128, 0, s>>>(tabs, net->stencil, rec, (int)npx, L, p->alpha, p->g, srp_of(sr),
+                                                desc, aux);
   mark(ST_NN_PREDICT);
   MR_CUDA(cudaGetLastError());
   const long long cap = (long long)npx;
@@ -526,6 +627,73 @@ extern "C" int mr_gather_descriptors(const mr_volume* h, const mr_network* nh, c
                                                             srp_of(sr), dev_desc, dev_aux);
   MR_CUDA(cudaGetLastError());
   return MR_OK;
+}
+
+namespace mr {
+// Both exact sampler forms on the same points: texel loads and texture
+// gathers, for the trilinear border / clamp filters and the bilinear clamp.
+__global__ void k_sampler_selftest(cudaTextureObject_t tb, cudaTextureObject_t tc, cudaTextureObject_t t2,
+                                   const float* __restrict__ d, const float* __restrict__ uv, int n, float* out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const F3 p = f3(uv[3 * k], uv[3 * k + 1], uv[3 * k + 2]);
+  float* o = out + 6 * (size_t)k;
+  o[0] = tri_border_c<MR_SAMPLER_SELFTEST_RES>(d, p);
+  o[1] = tri_border_g<MR_SAMPLER_SELFTEST_RES>(tb, p);
+  o[2] = tri_clamp_c<MR_SAMPLER_SELFTEST_RES>(d, p);
+  o[3] = tri_clamp_g<MR_SAMPLER_SELFTEST_RES>(tc, p);
+  o[4] = bilinear_clamp(d, MR_SAMPLER_SELFTEST_RES, MR_SAMPLER_SELFTEST_RES, p.x, p.y);
+  o[5] = bilinear_clamp_g(t2, MR_SAMPLER_SELFTEST_RES, MR_SAMPLER_SELFTEST_RES, p.x, p.y);
+}
+}  // namespace mr
+
+extern "C" int mr_sampler_selftest(int32_t n, const float* host_table, const float* host_uv, float* host_out) {
+  clear_error();
+  if (n <= 0 || !host_table || !host_uv || !host_out) return set_error(MR_ERR_ARG, "mr_sampler_selftest: bad argument");
+  constexpr int R = MR_SAMPLER_SELFTEST_RES;
+  float *d = nullptr, *uv = nullptr, *out = nullptr;
+  cudaArray_t ab = nullptr, ac = nullptr, a2 = nullptr;
+  cudaTextureObject_t tb = 0, tc = 0, t2 = 0;
+  int rc = MR_OK;
+  auto run = [&]() -> int {
+    MR_CUDA(cudaMalloc(&d, (size_t)R * R * R * sizeof(float)));
+    MR_CUDA(cudaMalloc(&uv, 3 * (size_t)n * sizeof(float)));
+    MR_CUDA(cudaMalloc(&out, 6 * (size_t)n * sizeof(float)));
+    MR_CUDA(cudaMemcpy(d, host_table, (size_t)R * R * R * sizeof(float), cudaMemcpyHostToDevice));
+    MR_CUDA(cudaMemcpy(uv, host_uv, 3 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice));
+    int r = make_gather_tex(&ab, &tb, R, cudaAddressModeBorder);
+    if (!r) r = make_gather_tex(&ac, &tc, R, cudaAddressModeClamp);
+    if (!r) r = copy_to_array(ab, d, R, 0);
+    if (!r) r = copy_to_array(ac, d, R, 0);
+    if (r) return r;
+    cudaChannelFormatDesc ch = cudaCreateChannelDesc<float>();
+    MR_CUDA(cudaMallocArray(&a2, &ch, R, R));
+    MR_CUDA(cudaMemcpy2DToArray(a2, 0, 0, d, R * sizeof(float), R * sizeof(float), R, cudaMemcpyDeviceToDevice));
+    cudaResourceDesc rd = {};
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = a2;
+    cudaTextureDesc td = {};
+    td.addressMode[0] = td.addressMode[1] = cudaAddressModeClamp;
+    td.filterMode = cudaFilterModePoint;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    MR_CUDA(cudaCreateTextureObject(&t2, &rd, &td, nullptr));
+    k_sampler_selftest<<<(n + 127) / 128, 128>>>(tb, tc, t2, d, uv, n, out);
+    MR_CUDA(cudaGetLastError());
+    MR_CUDA(cudaMemcpy(host_out, out, 6 * (size_t)n * sizeof(float), cudaMemcpyDeviceToHost));
+    return MR_OK;
+  };
+  rc = run();
+  if (tb) cudaDestroyTextureObject(tb);
+  if (tc) cudaDestroyTextureObject(tc);
+  if (t2) cudaDestroyTextureObject(t2);
+  if (ab) cudaFreeArray(ab);
+  if (ac) cudaFreeArray(ac);
+  if (a2) cudaFreeArray(a2);
+  cudaFree(d);
+  cudaFree(uv);
+  cudaFree(out);
+  return rc;
 }
 
 extern "C" int mr_radiance_predict(const mr_network* nh, int32_t precision, const float* dev_desc,
@@ -619,7 +787,7 @@ extern "C" int mr_render_neural_noalloc(mr_volume* h, const mr_network* nh, cons
   void* base = nullptr;
   rc = noalloc_scratch(&base);
   if (rc) return rc;
-  return neural_passes(v, &nh->n, p, dev_rgb, (cudaStream_t)stream, base, false);
+  return neural_passes(v, &nh->n, p, dev_rgb, (cudaStream_t)stream, base, false, nullptr, true);
 }
 
 // ---- batched neural render ------------------------------------------------------------
@@ -662,7 +830,7 @@ __global__ void __launch_bounds__(256) k_trace_batch(const BatchJob* __restrict_
   trace_counters(counters, st, act);
 }
 
-template <bool HW>
+template <int SAMP>
 __global__ void __launch_bounds__(256) k_gather_batch(const BatchJob* __restrict__ jobs,
                                                       const float* __restrict__ stencil, Records rec, int cap,
                                                       float* __restrict__ desc, float* __restrict__ aux) {
@@ -685,7 +853,7 @@ __global__ void __launch_bounds__(256) k_gather_batch(const BatchJob* __restrict
       d[(96 + (i >> 2)) * c] = bh;
     }
   };
-  gather_fast<HW>(j.tabs, stencil, pos, j.sc.L, f, j.sc.alpha, j.sc.g, sink);
+  gather_fast<SAMP>(j.tabs, stencil, pos, j.sc.L, f, j.sc.alpha, j.sc.g, sink);
   aux[k] = j.sc.g;
   aux[c + k] = acosf(dot(f.X, f.LX));
   aux[2 * c + k] = j.srp.x;
@@ -763,9 +931,9 @@ static int batch_launches(Batch& b, const Network* net, cudaStream_t s) {
     MR_CUDA(cudaGetLastError());
     const unsigned ggrid = (unsigned)((w1 - w0 + b.gather_block - 1) / b.gather_block);
     if (hw)
-      k_gather_batch<true><<<ggrid, b.gather_block, 0, s>>>(b.d_jobs, net->stencil, rec, (int)cap, desc, aux);
+      k_gather_batch<kSampTex><<<ggrid, b.gather_block, 0, s>>>(b.d_jobs, net->stencil, rec, (int)cap, desc, aux);
     else
-      k_gather_batch<false><<<ggrid, b.gather_block, 0, s>>>(b.d_jobs, net->stencil, rec, (int)cap, desc, aux);
+      k_gather_batch<kSampGather><<<ggrid, b.gather_block, 0, s>>>(b.d_jobs, net->stencil, rec, (int)cap, desc, aux);
     MR_CUDA(cudaGetLastError());
     const long long ccap = (long long)cap;
     int rc;
@@ -867,20 +1035,16 @@ extern "C" int mr_batch_prepare(mr_batch* h, const mr_network* nh, int64_t wave_
       int rc = launch_update_tr(v, L, p->alpha, s);
       if (rc) return rc;
     }
-    if (b.sampler == MR_SAMPLER_TEXTURE) {
-      int rc = refresh_textures(v, s);
-      if (rc) return rc;
-    }
     BatchJob& j = hj[i];
     j.m = Medium{v->density, v->res, v->max_density, p->tr_scale};
     j.sc = make_path_scene(p);
     j.cam = make_camera(p);
     j.seed = p->seed;
     j.frame = p->sample_offset;
-    j.tabs = Tables{v->mips, v->tr, v->lut, {}, {}, 0};
-    for (int k = 0; k < 9; ++k) j.tabs.mip_tex[k] = v->mip_tex[k];
-    for (int k = 0; k < 8; ++k) j.tabs.tr_tex[k] = v->tr_tex[k];
-    j.tabs.lut_tex = v->lut_tex;
+    {
+      int rc = fill_tables(v, b.sampler == MR_SAMPLER_TEXTURE ? kSampTex : kSampGather, &j.tabs, s);
+      if (rc) return rc;
+    }
     j.srp = srp_of(to_f3(p->scatter_rate) / 1.001f);
     j.pix0 = off;
     j.npx = p->width * p->height;

@@ -187,6 +187,7 @@ int launch_update_tr(Volume* v, F3 L, float alpha, cudaStream_t s) {
   MR_CUDA(cudaGetLastError());
   v->tr_valid = true;
   v->tex_tr_stale = true;
+  v->gth_tr_stale = true;
   v->tr_light = L;
   v->tr_alpha = alpha;
   return MR_OK;
@@ -199,6 +200,7 @@ int launch_update_lut(Volume* v, float g, uint32_t seed, cudaStream_t s) {
   MR_CUDA(cudaGetLastError());
   v->lut_valid = true;
   v->tex_lut_stale = true;
+  v->gth_lut_stale = true;
   v->lut_g = g;
   v->lut_seed = seed;
   return MR_OK;
@@ -221,7 +223,7 @@ static int make_tex3(cudaArray_t* arr, cudaTextureObject_t* tex, int r, cudaText
   MR_CUDA(cudaCreateTextureObject(tex, &rd, &td, nullptr));
   return MR_OK;
 }
-static int copy_to_array(cudaArray_t arr, const float* src, int r, cudaStream_t s) {
+int copy_to_array(cudaArray_t arr, const float* src, int r, cudaStream_t s) {
   cudaMemcpy3DParms cp = {};
   cp.srcPtr = make_cudaPitchedPtr((void*)src, r * sizeof(float), r, r);
   cp.dstArray = arr;
@@ -276,7 +278,83 @@ int refresh_textures(Volume* v, cudaStream_t s) {
   return MR_OK;
 }
 
+// ---- layered copies for the exact sampler's texture gathers ------------------------
+// Layered cudaArray of r layers (x) of r x r texels (width z, height y), read
+// with unnormalised coordinates and point sampling: tld4 returns the four
+// texels of a 2 x 2 (z, y) footprint unchanged, and the y / z borders come
+// from the address mode (border 0 for the density levels, clamp for the
+// transmittance levels), as in the fp32 software filter.
+int make_gather_tex(cudaArray_t* arr, cudaTextureObject_t* tex, int r, cudaTextureAddressMode mode) {
+  cudaChannelFormatDesc ch = cudaCreateChannelDesc<float>();
+  MR_CUDA(cudaMalloc3DArray(arr, &ch, make_cudaExtent(r, r, r), cudaArrayLayered));
+  cudaResourceDesc rd = {};
+  rd.resType = cudaResourceTypeArray;
+  rd.res.array.array = *arr;
+  cudaTextureDesc td = {};
+  td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = mode;
+  td.filterMode = cudaFilterModePoint;
+  td.readMode = cudaReadModeElementType;
+  td.normalizedCoords = 0;
+  MR_CUDA(cudaCreateTextureObject(tex, &rd, &td, nullptr));
+  return MR_OK;
+}
+
+int refresh_gather_textures(Volume* v, cudaStream_t s) {
+  if (!v->gth_lut_arr) {
+    for (int k = 0; k < 9; ++k) {
+      int rc = make_gather_tex(&v->gth_mip_arr[k], &v->gth_mip_tex[k], 256 >> k, cudaAddressModeBorder);
+      if (rc) return rc;
+    }
+    for (int k = 0; k < 8; ++k) {
+      int rc = make_gather_tex(&v->gth_tr_arr[k], &v->gth_tr_tex[k], 128 >> k, cudaAddressModeClamp);
+      if (rc) return rc;
+    }
+    cudaChannelFormatDesc ch = cudaCreateChannelDesc<float>();
+    MR_CUDA(cudaMallocArray(&v->gth_lut_arr, &ch, kLut, kLut));
+    cudaResourceDesc rd = {};
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = v->gth_lut_arr;
+    cudaTextureDesc td = {};
+    td.addressMode[0] = td.addressMode[1] = cudaAddressModeClamp;
+    td.filterMode = cudaFilterModePoint;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    MR_CUDA(cudaCreateTextureObject(&v->gth_lut_tex, &rd, &td, nullptr));
+    v->gth_mips_stale = v->gth_tr_stale = v->gth_lut_stale = true;
+  }
+  if (v->gth_mips_stale) {
+    for (int k = 0; k < 9; ++k) {
+      int rc = copy_to_array(v->gth_mip_arr[k], v->mips + mip_offset(k), 256 >> k, s);
+      if (rc) return rc;
+    }
+    v->gth_mips_stale = false;
+  }
+  if (v->gth_tr_stale) {
+    for (int k = 0; k < 8; ++k) {
+      int rc = copy_to_array(v->gth_tr_arr[k], v->tr + tr_offset(k), 128 >> k, s);
+      if (rc) return rc;
+    }
+    v->gth_tr_stale = false;
+  }
+  if (v->gth_lut_stale) {
+    MR_CUDA(cudaMemcpy2DToArrayAsync(v->gth_lut_arr, 0, 0, v->lut, kLut * sizeof(float), kLut * sizeof(float), kLut,
+                                     cudaMemcpyDeviceToDevice, s));
+    v->gth_lut_stale = false;
+  }
+  return MR_OK;
+}
+
 void destroy_textures(Volume* v) {
+  for (int k = 0; k < 9; ++k) {
+    if (v->gth_mip_tex[k]) cudaDestroyTextureObject(v->gth_mip_tex[k]);
+    if (v->gth_mip_arr[k]) cudaFreeArray(v->gth_mip_arr[k]);
+  }
+  for (int k = 0; k < 8; ++k) {
+    if (v->gth_tr_tex[k]) cudaDestroyTextureObject(v->gth_tr_tex[k]);
+    if (v->gth_tr_arr[k]) cudaFreeArray(v->gth_tr_arr[k]);
+  }
+  if (v->gth_lut_tex) cudaDestroyTextureObject(v->gth_lut_tex);
+  if (v->gth_lut_arr) cudaFreeArray(v->gth_lut_arr);
   for (int k = 0; k < 9; ++k) {
     if (v->mip_tex[k]) cudaDestroyTextureObject(v->mip_tex[k]);
     if (v->mip_arr[k]) cudaFreeArray(v->mip_arr[k]);
@@ -400,6 +478,7 @@ int mr_volume_update(mr_volume* h, void* stream) {
   v->max_density = md;
   v->mips_valid = true;
   v->tex_mips_stale = true;
+  v->gth_mips_stale = true;
   v->tr_valid = false;
   return MR_OK;
 }
