@@ -46,7 +46,18 @@ __host__ __device__ constexpr int stage_floats(int g) { return 3 * (stage_width(
 __host__ __device__ constexpr int stage_offset(int g) { return g <= 3 ? 816 * g : 2448 + 3168 * (g - 3); }
 static_assert(stage_offset(1) == stage_floats(0) && stage_offset(4) == stage_offset(3) + stage_floats(3),
               "stage offsets");
-constexpr int kSimtImage = kHeadImage + stage_offset(kTrunkStages);
+// [squeeze-excitation blocks 0..11 (main trunk 0..7, light trunk 8..11): per
+//  block kSeFloats = the LSEFin1 weights of its pool entries as [6][16] (mean
+//  b0, max b0, mean b1, max b1, mean b2, max b2; 16 outputs), then SE1 8x8 and
+//  SE2 3x8 row-major]
+// [head per-row weights: LSEFin2 6x16, LSEFin1's albedo column (16), LGGS W
+//  8x3 + B 8, LX12 W 16 + B 1, padded to kHeadRowFloats]
+constexpr int kSeBlocks = 12, kSeFloats = 96 + 64 + 24;
+constexpr int kSeOff = kHeadImage + stage_offset(kTrunkStages);
+constexpr int kHeadRowOff = kSeOff + kSeBlocks * kSeFloats;
+constexpr int kHeadRowFloats = 96 + 16 + 32 + 20;
+constexpr int kSimtImage = kHeadRowOff + kHeadRowFloats;
+static_assert(kSeOff % 4 == 0 && kSeFloats % 4 == 0 && kHeadRowOff % 4 == 0, "float4 alignment");
 
 void simt_weight_image(const float* w, std::vector<float>& img) {
   const WeightTable wt = make_weight_table();
@@ -76,6 +87,30 @@ void simt_weight_image(const float* w, std::vector<float>& img) {
       o += S * S + S;
     }
   }
+  const int se[kSeBlocks][2] = {{MR_W_LSE01W, MR_W_LSE02W}, {MR_W_LSE11W, MR_W_LSE12W}, {MR_W_LSE21W, MR_W_LSE22W},
+                                {MR_W_LSE31W, MR_W_LSE32W}, {MR_W_LSE41W, MR_W_LSE42W}, {MR_W_LSE51W, MR_W_LSE52W},
+                                {MR_W_LSE61W, MR_W_LSE62W}, {MR_W_LSE71W, MR_W_LSE72W}, {MR_W_LDSE01W, MR_W_LDSE02W},
+                                {MR_W_LDSE11W, MR_W_LDSE12W}, {MR_W_LDSE21W, MR_W_LDSE22W},
+                                {MR_W_LDSE31W, MR_W_LDSE32W}};
+  const float* f1 = w + wt.off[MR_W_LSEFin1W];  // 16 x 75
+  for (int blk = 0; blk < kSeBlocks; ++blk) {
+    float* o = img.data() + kSeOff + blk * kSeFloats;
+    const int pid = 3 * blk;
+    for (int b = 0; b < 3; ++b)
+      for (int j = 0; j < 16; ++j) {
+        o[(2 * b) * 16 + j] = f1[j * 75 + pid + b];
+        o[(2 * b + 1) * 16 + j] = f1[j * 75 + 36 + pid + b];
+      }
+    for (int i = 0; i < 64; ++i) o[96 + i] = w[wt.off[se[blk][0]] + i];
+    for (int i = 0; i < 24; ++i) o[160 + i] = w[wt.off[se[blk][1]] + i];
+  }
+  float* hr = img.data() + kHeadRowOff;
+  for (int i = 0; i < 96; ++i) hr[i] = w[wt.off[MR_W_LSEFin2W] + i];
+  for (int j = 0; j < 16; ++j) hr[96 + j] = f1[j * 75 + 74];
+  for (int i = 0; i < 24; ++i) hr[112 + i] = w[wt.off[MR_W_LGGSW] + i];
+  for (int i = 0; i < 8; ++i) hr[136 + i] = w[wt.off[MR_W_LGGSB] + i];
+  for (int i = 0; i < 16; ++i) hr[144 + i] = w[wt.off[MR_W_LX12W] + i];
+  hr[160] = w[wt.off[MR_W_LX12B]];
 }
 
 // ---- trunk ---------------------------------------------------------------------------
@@ -154,9 +189,9 @@ __device__ __forceinline__ void dense1(const float* x, float* yn, const float* _
 // straight into the 16 LSEFin1 sums `fin` (pool[pid+b], pool[36+pid+b]), and
 // the three branch gates.
 template <int S>
-__device__ __forceinline__ void se_gates(const RowIO& in, const float* __restrict__ w, int from, int pid, int sew0,
-                                         int sew1, float g, float gamma, float (&fin)[16], float (&gate)[3]) {
-  float mean[3], mx[3];
+__device__ __forceinline__ void se_gates(const RowIO& in, const float* __restrict__ sw, int from, float g,
+                                         float gamma, float (&fin)[16], float (&gate)[3]) {
+  float st[6];  // mean b0, max b0, mean b1, max b1, mean b2, max b2
 #pragma unroll
   for (int b = 0; b < 3; ++b) {
     float s = 0.0f, m = -10000.0f;
@@ -166,34 +201,46 @@ __device__ __forceinline__ void se_gates(const RowIO& in, const float* __restric
       s += q.x; s += q.y; s += q.z; s += q.w;
       m = fmaxf(m, q.x); m = fmaxf(m, q.y); m = fmaxf(m, q.z); m = fmaxf(m, q.w);
     }
-    mean[b] = s / (float)S;
-    mx[b] = m;
+    st[2 * b] = s / (float)S;
+    st[2 * b + 1] = m;
   }
-  const float* f1 = w + WOFF(LSEFin1W);
+  // LSEFin1 over this block's pool entries, in the order mean b, max b
 #pragma unroll
-  for (int j = 0; j < 16; ++j) {
-    float acc = fin[j];
+  for (int k = 0; k < 6; ++k)
 #pragma unroll
-    for (int b = 0; b < 3; ++b) {
-      acc += mean[b] * __ldg(f1 + j * 75 + pid + b);
-      acc += mx[b] * __ldg(f1 + j * 75 + 36 + pid + b);
+    for (int j = 0; j < 16; j += 4) {
+      const float4 f = ldg4(sw + k * 16 + j);
+      fin[j] += st[k] * f.x;
+      fin[j + 1] += st[k] * f.y;
+      fin[j + 2] += st[k] * f.z;
+      fin[j + 3] += st[k] * f.w;
     }
-    fin[j] = acc;
-  }
-  const float tmp[8] = {mean[0], mean[1], mean[2], mx[0], mx[1], mx[2], g, gamma};
+  const float tmp[8] = {st[0], st[2], st[4], st[1], st[3], st[5], g, gamma};
   float h[8];
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     float a = 0.0f;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) a += tmp[j] * __ldg(w + sew0 + j + i * 8);
+    for (int j = 0; j < 8; j += 4) {
+      const float4 q = ldg4(sw + 96 + i * 8 + j);
+      a += tmp[j] * q.x;
+      a += tmp[j + 1] * q.y;
+      a += tmp[j + 2] * q.z;
+      a += tmp[j + 3] * q.w;
+    }
     h[i] = relu0(a);
   }
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
     float a = 0.0f;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) a += h[j] * __ldg(w + sew1 + j + i * 8);
+    for (int j = 0; j < 8; j += 4) {
+      const float4 q = ldg4(sw + 160 + i * 8 + j);
+      a += h[j] * q.x;
+      a += h[j + 1] * q.y;
+      a += h[j + 2] * q.z;
+      a += h[j + 3] * q.w;
+    }
     gate[i] = 1.0f / (1.0f + expf(-a));
   }
 }
@@ -202,11 +249,11 @@ __device__ __forceinline__ void se_gates(const RowIO& in, const float* __restric
 // REP3. Weight offsets are runtime values so that blocks of equal mode share
 // this code.
 template <int MODE>
-__device__ __forceinline__ void row_block8(const RowIO& in, const float* __restrict__ w, int from, int pid, int sew0,
-                                           int sew1, int wa, int wb, int wc, float g, float gamma, const YS& y,
+__device__ __forceinline__ void row_block8(const RowIO& in, const float* __restrict__ w, const float* __restrict__ sw,
+                                           int from, int wa, int wb, int wc, float g, float gamma, const YS& y,
                                            float (&fin)[16]) {
   float gate[3];
-  se_gates<8>(in, w, from, pid, sew0, sew1, g, gamma, fin, gate);
+  se_gates<8>(in, sw, from, g, gamma, fin, gate);
 #pragma unroll 1
   for (int b = 0; b < 3; ++b) {
     const int wo = b == 0 ? wa : b == 1 ? wb : wc;
@@ -243,11 +290,10 @@ __device__ __forceinline__ void row_block8(const RowIO& in, const float* __restr
 // Per-row half of a width-S SERES block run as a block GEMM: gates, then the
 // layer input x = in * gate + y written over y in the tile.
 template <int S>
-__device__ __forceinline__ void row_gate_input(const RowIO& in, const float* __restrict__ w, int from, int pid,
-                                               int sew0, int sew1, float g, float gamma, const YS& y,
-                                               float (&fin)[16]) {
+__device__ __forceinline__ void row_gate_input(const RowIO& in, const float* __restrict__ sw, int from, float g,
+                                               float gamma, const YS& y, float (&fin)[16]) {
   float gate[3];
-  se_gates<S>(in, w, from, pid, sew0, sew1, g, gamma, fin, gate);
+  se_gates<S>(in, sw, from, g, gamma, fin, gate);
 #pragma unroll
   for (int b = 0; b < 3; ++b) {
 #pragma unroll 4
@@ -379,17 +425,17 @@ __global__ void __launch_bounds__(kTile, 3) k_simt_trunk(TrunkArgs a, TrunkOut t
   for (int j = 0; j < 16; ++j) fin[j] = 0.0f;
   const YS y{tile + r};
   // main trunk (radiancePredict.cu:396-421): blocks 0, 1 per row, 2..7 as GEMMs
-  row_block8<0>(in, w, 0, 0, WOFF(LSE01W), WOFF(LSE02W), WOFF(L01W), WOFF(L_Tr01W), WOFF(L_Hg01W), g, gamma, y, fin);
-  row_block8<2>(in, w, 8, 3, WOFF(LSE11W), WOFF(LSE12W), WOFF(L11W), WOFF(L_Tr11W), WOFF(L_Hg11W), g, gamma, y, fin);
-  const int se[6][2] = {{WOFF(LSE21W), WOFF(LSE22W)}, {WOFF(LSE31W), WOFF(LSE32W)}, {WOFF(LSE41W), WOFF(LSE42W)},
-                        {WOFF(LSE51W), WOFF(LSE52W)}, {WOFF(LSE61W), WOFF(LSE62W)}, {WOFF(LSE71W), WOFF(LSE72W)}};
+  const float* __restrict__ sw = a.img + kSeOff;  // squeeze-excitation block weights
+  row_block8<0>(in, w, sw, 0, WOFF(L01W), WOFF(L_Tr01W), WOFF(L_Hg01W), g, gamma, y, fin);
+  row_block8<2>(in, w, sw + kSeFloats, 8, WOFF(L11W), WOFF(L_Tr11W), WOFF(L_Hg11W), g, gamma, y, fin);
 #pragma unroll 1
   for (int st = 0; st < 6; ++st) {
-    const int S = stage_width(st), from = st < 3 ? 16 + 16 * st : 64 + 32 * (st - 3), pid = 6 + 3 * st;
+    const int S = stage_width(st), from = st < 3 ? 16 + 16 * st : 64 + 32 * (st - 3);
+    const float* sws = sw + (2 + st) * kSeFloats;
     if (S == 16)
-      row_gate_input<16>(in, w, from, pid, se[st][0], se[st][1], g, gamma, y, fin);
+      row_gate_input<16>(in, sws, from, g, gamma, y, fin);
     else
-      row_gate_input<32>(in, w, from, pid, se[st][0], se[st][1], g, gamma, y, fin);
+      row_gate_input<32>(in, sws, from, g, gamma, y, fin);
     asm volatile("cp.async.wait_group 1;\n" ::: "memory");
     __syncthreads();  // stage st's weights and every row's input are in the tile
     const float* W = ring + (st & 1) * stage_floats(kTrunkStages - 1);
@@ -414,16 +460,14 @@ __global__ void __launch_bounds__(kTile, 3) k_simt_trunk(TrunkArgs a, TrunkOut t
     if (valid) *reinterpret_cast<float4*>(orow + c * to.cs) = make_float4(x0, x1, x2, x3);
   };
   // light-direction trunk (:424-437), per row
-  row_block8<0>(in, w, 160, 24, WOFF(LDSE01W), WOFF(LDSE02W), WOFF(LD01W), WOFF(LD_Tr01W), WOFF(LD_Hg01W), g, gamma,
-                y, fin);
+  row_block8<0>(in, w, sw + 8 * kSeFloats, 160, WOFF(LD01W), WOFF(LD_Tr01W), WOFF(LD_Hg01W), g, gamma, y, fin);
   {
-    const int pd[3][5] = {{WOFF(LDSE11W), WOFF(LDSE12W), WOFF(LD11W), WOFF(LD_Tr11W), WOFF(LD_Hg11W)},
-                          {WOFF(LDSE21W), WOFF(LDSE22W), WOFF(LD21W), WOFF(LD_Tr21W), WOFF(LD_Hg21W)},
-                          {WOFF(LDSE31W), WOFF(LDSE32W), WOFF(LD31W), WOFF(LD_Tr31W), WOFF(LD_Hg31W)}};
+    const int pd[3][3] = {{WOFF(LD11W), WOFF(LD_Tr11W), WOFF(LD_Hg11W)},
+                          {WOFF(LD21W), WOFF(LD_Tr21W), WOFF(LD_Hg21W)},
+                          {WOFF(LD31W), WOFF(LD_Tr31W), WOFF(LD_Hg31W)}};
 #pragma unroll 1
     for (int b = 0; b < 3; ++b)
-      row_block8<1>(in, w, 168 + 8 * b, 27 + 3 * b, pd[b][0], pd[b][1], pd[b][2], pd[b][3], pd[b][4], g, gamma, y,
-                    fin);
+      row_block8<1>(in, w, sw + (9 + b) * kSeFloats, 168 + 8 * b, pd[b][0], pd[b][1], pd[b][2], g, gamma, y, fin);
   }
   {  // LD41: comb[96..120)
     const int wl[3] = {WOFF(LD41W), WOFF(LD_Tr41W), WOFF(LD_Hg41W)};
@@ -444,24 +488,6 @@ __global__ void __launch_bounds__(kTile, 3) k_simt_trunk(TrunkArgs a, TrunkOut t
     fin[j] += g * __ldg(w + WOFF(LSEFin1W) + j * 75 + 72) + gamma * __ldg(w + WOFF(LSEFin1W) + j * 75 + 73);
 #pragma unroll
   for (int j0 = 0; j0 < 16; j0 += 4) put4(30 + j0 / 4, fin[j0], fin[j0 + 1], fin[j0 + 2], fin[j0 + 3]);
-}
-
-// 16 -> 16 layer in registers.
-__device__ __forceinline__ void dense16(const float (&x)[16], float (&y)[16], const float* __restrict__ W,
-                                        const float* __restrict__ B) {
-#pragma unroll
-  for (int i = 0; i < 16; ++i) {
-    float acc = __ldg(B + i);
-#pragma unroll
-    for (int j = 0; j < 16; j += 4) {
-      float4 q = ldg4(W + i * 16 + j);
-      acc += x[j] * q.x;
-      acc += x[j + 1] * q.y;
-      acc += x[j + 2] * q.z;
-      acc += x[j + 3] * q.w;
-    }
-    y[i] = relu0(acc);
-  }
 }
 
 // ---- head: block GEMMs over shared-memory activation tiles ---------------------------
@@ -572,11 +598,41 @@ __device__ __forceinline__ void block_gemm(const float* __restrict__ Xt, float* 
   }
 }
 
+// Half of a 16 -> 16 layer: outputs 8h..8h+7 of ReLU(B + W x), bias first,
+// ascending inputs.
+__device__ __forceinline__ void dense16_half(const float (&x)[16], float (&y)[8], const float* __restrict__ W,
+                                             const float* __restrict__ B, int h) {
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    float acc = __ldg(B + 8 * h + q);
+#pragma unroll
+    for (int j = 0; j < 16; j += 4) {
+      const float4 v = ldg4(W + (8 * h + q) * 16 + j);
+      acc += x[j] * v.x;
+      acc += x[j + 1] * v.y;
+      acc += x[j + 2] * v.z;
+      acc += x[j + 3] * v.w;
+    }
+    y[q] = relu0(acc);
+  }
+}
+
+// The full 16-vector from the two halves held by lanes l and l ^ 16.
+__device__ __forceinline__ void join16(const float (&mine)[8], float (&full)[16], int h) {
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const float other = __shfl_xor_sync(0xffffffffu, mine[q], 16);
+    full[q] = h ? other : mine[q];
+    full[8 + q] = h ? mine[q] : other;
+  }
+}
+
 // Head SC(p) (radiancePredict.cu:439-473) per distinct albedo channel for a
-// block of 128 rows: the gated 128-wide input is built per row into Xt (two
-// threads per row, half the features each), LC0 / LC1 / LC2 run as block
-// GEMMs over all 256 threads, LX and the residual pairs per row on the first
-// 128 threads.
+// block of 128 rows. The gated 128-wide input is built per row into Xt (two
+// threads per row, half the features each); LC0 / LC1 / LC2 run as block
+// GEMMs; LX and the residual pairs run per row with the row's two threads in
+// one warp (lanes l and l ^ 16), each computing half the outputs of every
+// layer and exchanging them by shuffle.
 __global__ void __launch_bounds__(kHeadThreads, 1) k_simt_head(HeadArgs a) {
   extern __shared__ __align__(16) float hsm[];
   float* Xt = hsm;
@@ -584,10 +640,14 @@ __global__ void __launch_bounds__(kHeadThreads, 1) k_simt_head(HeadArgs a) {
   const int n = a.count ? (int)min(*a.count, (unsigned)a.n) : a.n;
   const int row0 = blockIdx.x * kHeadRows;
   if (row0 >= n) return;  // block-uniform
+  // input mapping: row r, feature half `half`
   const int r = threadIdx.x & (kHeadRows - 1), half = threadIdx.x >> 7, row = row0 + r;
   const bool valid = row < n;
   const int kr = valid ? row : n - 1;
+  // tail mapping: row rt, output half ht
+  const int lane = threadIdx.x & 31, rt = (threadIdx.x >> 5) * 16 + (lane & 15), ht = lane >> 4;
   const float* __restrict__ w = a.w;
+  const float* __restrict__ hr = a.wt + kHeadRowOff;
   const float* trow = a.t + (long long)kr * a.trs;
   const float* ax = a.aux + (long long)kr * a.ars;
   const float g = __ldg(ax), gamma = __ldg(ax + a.afs);
@@ -604,7 +664,7 @@ __global__ void __launch_bounds__(kHeadThreads, 1) k_simt_head(HeadArgs a) {
 #pragma unroll
   for (int i = 0; i < kStages - 1; ++i) ws.issue();
   int chunk = 0;
-  float X[3] = {0.0f, 0.0f, 0.0f};
+  float X[3] = {0.0f, 0.0f, 0.0f};  // of row rt
 #pragma unroll 1
   for (int ch = 0; ch < 3; ++ch) {
     if ((ch == 1 && !need1) || (ch == 2 && !need2)) continue;
@@ -614,12 +674,24 @@ __global__ void __launch_bounds__(kHeadThreads, 1) k_simt_head(HeadArgs a) {
     {
       float sew[16];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) sew[j] = relu0(fin[j] + sc * __ldg(w + WOFF(LSEFin1W) + j * 75 + 74));
+      for (int j = 0; j < 16; j += 4) {
+        const float4 f = ldg4(hr + 96 + j);
+        sew[j] = relu0(fin[j] + sc * f.x);
+        sew[j + 1] = relu0(fin[j + 1] + sc * f.y);
+        sew[j + 2] = relu0(fin[j + 2] + sc * f.z);
+        sew[j + 3] = relu0(fin[j + 3] + sc * f.w);
+      }
 #pragma unroll
       for (int i = 0; i < 6; ++i) {
         float acc = 0.0f;
 #pragma unroll
-        for (int j = 0; j < 16; ++j) acc += sew[j] * __ldg(w + WOFF(LSEFin2W) + j + i * 16);
+        for (int j = 0; j < 16; j += 4) {
+          const float4 f = ldg4(hr + i * 16 + j);
+          acc += sew[j] * f.x;
+          acc += sew[j + 1] * f.y;
+          acc += sew[j + 2] * f.z;
+          acc += sew[j + 3] * f.w;
+        }
         sep[i] = 1.0f / (1.0f + expf(-acc));
       }
     }
@@ -637,9 +709,8 @@ __global__ void __launch_bounds__(kHeadThreads, 1) k_simt_head(HeadArgs a) {
     if (half) {
 #pragma unroll
       for (int i = 0; i < 8; ++i) {  // LGGS 3 -> 8, bias after the sum
-        float acc = g * __ldg(w + WOFF(LGGSW) + 3 * i) + gamma * __ldg(w + WOFF(LGGSW) + 3 * i + 1) +
-                    sc * __ldg(w + WOFF(LGGSW) + 3 * i + 2);
-        acc += __ldg(w + WOFF(LGGSB) + i);
+        float acc = g * __ldg(hr + 112 + 3 * i) + gamma * __ldg(hr + 112 + 3 * i + 1) + sc * __ldg(hr + 112 + 3 * i + 2);
+        acc += __ldg(hr + 136 + i);
         Xt[(120 + i) * kHeadRows + r] = relu0(acc);
       }
     }
@@ -647,38 +718,50 @@ __global__ void __launch_bounds__(kHeadThreads, 1) k_simt_head(HeadArgs a) {
     block_gemm<128, 64>(Yt, Xt, w + WOFF(LC1B), ws, chunk);
     block_gemm<64, 32>(Xt, Yt, w + WOFF(LC2B), ws, chunk);
     __syncthreads();
-    if (half) continue;  // the per-row tail runs on the first 128 threads
-    float x32[32];
-#pragma unroll
-    for (int i = 0; i < 32; ++i) x32[i] = Yt[i * kHeadRows + r];
+    // LX 32 -> 16 and the residual pairs (:454-471), tail mapping
     float a16[16];
+    {
+      float x32[32];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {  // LX 32 -> 16
-      float acc = __ldg(w + WOFF(LXB) + i);
+      for (int i = 0; i < 32; ++i) x32[i] = Yt[i * kHeadRows + rt];
+      float a8[8];
 #pragma unroll
-      for (int j = 0; j < 32; j += 4) {
-        float4 q = ldg4(w + WOFF(LXW) + i * 32 + j);
-        acc += x32[j] * q.x;
-        acc += x32[j + 1] * q.y;
-        acc += x32[j + 2] * q.z;
-        acc += x32[j + 3] * q.w;
+      for (int q = 0; q < 8; ++q) {
+        float acc = __ldg(w + WOFF(LXB) + 8 * ht + q);
+#pragma unroll
+        for (int j = 0; j < 32; j += 4) {
+          const float4 v = ldg4(w + WOFF(LXW) + (8 * ht + q) * 32 + j);
+          acc += x32[j] * v.x;
+          acc += x32[j + 1] * v.y;
+          acc += x32[j + 2] * v.z;
+          acc += x32[j + 3] * v.w;
+        }
+        a8[q] = relu0(acc);
       }
-      a16[i] = relu0(acc);
+      join16(a8, a16, ht);
     }
     const int lx[12] = {WOFF(LX0W), WOFF(LX1W), WOFF(LX2W), WOFF(LX3W), WOFF(LX4W), WOFF(LX5W),
                         WOFF(LX6W), WOFF(LX7W), WOFF(LX8W), WOFF(LX9W), WOFF(LX10W), WOFF(LX11W)};
 #pragma unroll 1
-    for (int rr = 0; rr < 6; ++rr) {  // residual pairs (:454-471)
-      float b16[16], c16[16];
-      dense16(a16, b16, w + lx[2 * rr], w + lx[2 * rr] + 256);
-      dense16(b16, c16, w + lx[2 * rr + 1], w + lx[2 * rr + 1] + 256);
+    for (int rr = 0; rr < 6; ++rr) {
+      float h8[8], b16[16], c16[16];
+      dense16_half(a16, h8, w + lx[2 * rr], w + lx[2 * rr] + 256, ht);
+      join16(h8, b16, ht);
+      dense16_half(b16, h8, w + lx[2 * rr + 1], w + lx[2 * rr + 1] + 256, ht);
+      join16(h8, c16, ht);
 #pragma unroll
       for (int i = 0; i < 16; ++i) a16[i] = a16[i] + c16[i];
     }
     float o = 0.0f;  // LX12 16 -> 1, bias after the sum
 #pragma unroll
-    for (int i = 0; i < 16; ++i) o += a16[i] * __ldg(w + WOFF(LX12W) + i);
-    o += __ldg(w + WOFF(LX12B));
+    for (int i = 0; i < 16; i += 4) {
+      const float4 v = ldg4(hr + 144 + i);
+      o += a16[i] * v.x;
+      o += a16[i + 1] * v.y;
+      o += a16[i + 2] * v.z;
+      o += a16[i + 3] * v.w;
+    }
+    o += __ldg(hr + 160);
     const float xo = relu0(o);
     if (ch == 0) X[0] = xo;
     else if (ch == 1) X[1] = xo;
@@ -686,20 +769,23 @@ __global__ void __launch_bounds__(kHeadThreads, 1) k_simt_head(HeadArgs a) {
     // Xt and Yt are next written after the first barrier of the next channel
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");
-  if (half) return;
-  if (srp[1] == srp[0]) X[1] = X[0];
-  if (srp[2] == srp[0]) X[2] = X[0];
-  else if (srp[2] == srp[1]) X[2] = X[1];
-  if (!valid) return;
-  float o[3] = {fmaxf(expf(X[0]) - 1.0f, 0.0f) * srp[0], fmaxf(expf(X[1]) - 1.0f, 0.0f) * srp[1],
-                fmaxf(expf(X[2]) - 1.0f, 0.0f) * srp[2]};
+  // output of row rt by its first thread
+  const int rowt = row0 + rt;
+  if (ht || rowt >= n) return;
+  const float* axt = a.aux + (long long)rowt * a.ars;
+  const float st[3] = {__ldg(axt + 2 * a.afs), __ldg(axt + 3 * a.afs), __ldg(axt + 4 * a.afs)};
+  if (st[1] == st[0]) X[1] = X[0];
+  if (st[2] == st[0]) X[2] = X[0];
+  else if (st[2] == st[1]) X[2] = X[1];
+  float o[3] = {fmaxf(expf(X[0]) - 1.0f, 0.0f) * st[0], fmaxf(expf(X[1]) - 1.0f, 0.0f) * st[1],
+                fmaxf(expf(X[2]) - 1.0f, 0.0f) * st[2]};
   if (a.pix) {
-    const int px = a.pix[row];
-    const float tr = a.trph[row];
+    const int px = a.pix[rowt];
+    const float tr = a.trph[rowt];
     F3 lc = a.light_color, sc = a.scatter;
     float* dst = a.out;
     if (a.job) {
-      const BatchOut& bo = a.bout[a.job[row]];
+      const BatchOut& bo = a.bout[a.job[rowt]];
       lc = bo.light_color;
       sc = bo.scatter;
       dst = bo.out;
@@ -709,7 +795,7 @@ __global__ void __launch_bounds__(kHeadThreads, 1) k_simt_head(HeadArgs a) {
     dst[3 * (size_t)px + 2] = fmaxf(((o[2] + tr) * lc.z) * sc.z, 0.0f);
   } else {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) a.out[3 * (size_t)row + c] = o[c];
+    for (int c = 0; c < 3; ++c) a.out[3 * (size_t)rowt + c] = o[c];
   }
 }
 
