@@ -168,6 +168,41 @@ __device__ __forceinline__ float tri_border(const float* __restrict__ d, int res
   return lerpf(lerpf(lerpf(c000, c001, wz), lerpf(c010, c011, wz), wy),
                lerpf(lerpf(c100, c101, wz), lerpf(c110, c111, wz), wy), wx);
 }
+// The four texels of the 2 x 2 footprint whose first texel is (i, j) (layer
+// `layer` of a layered texture), unfiltered: with unnormalised coordinates
+// (i + 1, j + 1) the footprint is texels i, i+1 and j, j+1 exactly, and the
+// address mode supplies out-of-range texels. tld4 returns them in the order
+// (i, j+1), (i+1, j+1), (i+1, j), (i, j); the result is reordered to
+// {(i, j), (i+1, j), (i, j+1), (i+1, j+1)}.
+__device__ __forceinline__ float4 gather_a2d(cudaTextureObject_t t, int layer, float fi, float fj) {
+  float a, b, c, d;
+  asm("tld4.r.a2d.v4.f32.f32 {%0, %1, %2, %3}, [%4, {%5, %6, %7, %8}];"
+      : "=f"(a), "=f"(b), "=f"(c), "=f"(d)
+      : "l"(t), "r"(layer), "f"(fi + 1.0f), "f"(fj + 1.0f), "f"(0.0f));
+  return make_float4(d, c, a, b);
+}
+__device__ __forceinline__ float4 gather_2d(cudaTextureObject_t t, float fi, float fj) {
+  float a, b, c, d;
+  asm("tld4.r.2d.v4.f32.f32 {%0, %1, %2, %3}, [%4, {%5, %6}];"
+      : "=f"(a), "=f"(b), "=f"(c), "=f"(d)
+      : "l"(t), "f"(fi + 1.0f), "f"(fj + 1.0f));
+  return make_float4(d, c, a, b);
+}
+
+// tri_border over a layered copy of the grid (layer x, texel (z, y), border
+// address mode), through two texture gathers: the same corner values (except
+// subnormal ones, which the texture unit reads as 0) and the same arithmetic.
+__device__ __forceinline__ float tri_border_tex(cudaTextureObject_t t, int res, F3 uv) {
+  float px = uv.x * res - 0.5f, py = uv.y * res - 0.5f, pz = uv.z * res - 0.5f;
+  float fx = floorf(px), fy = floorf(py), fz = floorf(pz);
+  int x = (int)fx;
+  float wx = px - fx, wy = py - fy, wz = pz - fz;
+  const float4 z4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const float4 a = (unsigned)x < (unsigned)res ? gather_a2d(t, x, fz, fy) : z4;
+  const float4 b = (unsigned)(x + 1) < (unsigned)res ? gather_a2d(t, x + 1, fz, fy) : z4;
+  return lerpf(lerpf(lerpf(a.x, a.y, wz), lerpf(a.z, a.w, wz), wy),
+               lerpf(lerpf(b.x, b.y, wz), lerpf(b.z, b.w, wz), wy), wx);
+}
 // Trilinear, clamp to edge (the TR tables, core/volume.cu:1412-1417).
 __device__ __forceinline__ float tri_clamp(const float* __restrict__ d, int res, F3 uv) {
   float px = uv.x * res - 0.5f, py = uv.y * res - 0.5f, pz = uv.z * res - 0.5f;

@@ -345,7 +345,9 @@ extern "C" int mr_render_interactive(mr_volume* h, const mr_network* net, const 
   const int fnum = it->checkerboard ? it->frame_index / 2 : it->frame_index;
   if (p->render_type == MR_RT_PT) {
     InterArgs a;
-    a.m = Medium{v->density, v->res, v->max_density, p->tr_scale};
+    a.m = Medium{v->density, v->res, v->max_density, p->tr_scale, 0};
+    rc = density_gather_texture(v, s, &a.m.tex);
+    if (rc) return rc;
     a.sc = make_path_scene(p);
     a.cam = make_camera(p);
     a.seed = p->seed;

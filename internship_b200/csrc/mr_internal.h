@@ -65,6 +65,10 @@ struct Volume {
   cudaArray_t gth_mip_arr[9] = {}, gth_tr_arr[8] = {}, gth_lut_arr = nullptr;
   cudaTextureObject_t gth_mip_tex[9] = {}, gth_tr_tex[8] = {}, gth_lut_tex = 0;
   bool gth_mips_stale = true, gth_tr_stale = true, gth_lut_stale = true;
+  // layered copy of the density grid for the trackers' texture gathers
+  cudaArray_t gth_den_arr = nullptr;
+  cudaTextureObject_t gth_den_tex = 0;
+  bool gth_den_stale = true;
   // Per-render scratch owned by the volume (grown on demand).
   void* scratch = nullptr;
   size_t scratch_bytes = 0;
@@ -112,6 +116,9 @@ int launch_update_tr(Volume* v, F3 L, float alpha, cudaStream_t s);
 int launch_update_lut(Volume* v, float g, uint32_t seed, cudaStream_t s);
 int refresh_textures(Volume* v, cudaStream_t s);
 int refresh_gather_textures(Volume* v, cudaStream_t s);
+// Texture object of the density grid's layered copy (created on first use,
+// refreshed after mr_volume_set_data*).
+int density_gather_texture(Volume* v, cudaStream_t s, cudaTextureObject_t* out);
 // r^3 x-major fp32 table <-> cudaArray (3-D or layered, extent z, y, x)
 int copy_to_array(cudaArray_t arr, const float* src, int r, cudaStream_t s);
 int make_gather_tex(cudaArray_t* arr, cudaTextureObject_t* tex, int r, cudaTextureAddressMode mode);

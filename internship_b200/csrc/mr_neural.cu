@@ -219,27 +219,6 @@ __device__ __forceinline__ float tri_clamp_c(const float* __restrict__ d, F3 uv)
                lerpf(lerpf(c100, c101, wz), lerpf(c110, c111, wz), wy), wx);
 }
 
-// The four texels of the 2 x 2 footprint whose first texel is (i, j) (layer
-// `layer` of a layered texture), unfiltered: with unnormalised coordinates
-// (i + 1, j + 1) the footprint is texels i, i+1 and j, j+1 exactly, and the
-// address mode supplies out-of-range texels. tld4 returns them in the order
-// (i, j+1), (i+1, j+1), (i+1, j), (i, j); the result is reordered to
-// {(i, j), (i+1, j), (i, j+1), (i+1, j+1)}.
-__device__ __forceinline__ float4 gather_a2d(cudaTextureObject_t t, int layer, float fi, float fj) {
-  float a, b, c, d;
-  asm("tld4.r.a2d.v4.f32.f32 {%0, %1, %2, %3}, [%4, {%5, %6, %7, %8}];"
-      : "=f"(a), "=f"(b), "=f"(c), "=f"(d)
-      : "l"(t), "r"(layer), "f"(fi + 1.0f), "f"(fj + 1.0f), "f"(0.0f));
-  return make_float4(d, c, a, b);
-}
-__device__ __forceinline__ float4 gather_2d(cudaTextureObject_t t, float fi, float fj) {
-  float a, b, c, d;
-  asm("tld4.r.2d.v4.f32.f32 {%0, %1, %2, %3}, [%4, {%5, %6}];"
-      : "=f"(a), "=f"(b), "=f"(c), "=f"(d)
-      : "l"(t), "f"(fi + 1.0f), "f"(fj + 1.0f));
-  return make_float4(d, c, a, b);
-}
-
 // tri_border_c / tri_clamp_c / bilinear_clamp over texture gathers: two
 // footprints (layers x and x+1) per trilinear sample, one per bilinear.
 // Same corner values and the same fp32 arithmetic.
@@ -413,8 +392,10 @@ __global__ void k_gather(Tables t, const float* __restrict__ stencil, const floa
 // features 4j..4j+3 of record k at desc[(j*cap + k)*4 .. +3] (aux: feature i at
 // aux[i*cap + k]). A warp's 16-byte stores and the network's 16-byte loads of
 // one chunk are contiguous 512-byte transactions.
+// The texture forms are bound by fetch latency: registers capped for six
+// 128-thread blocks per SM.
 template <int SAMP>
-__global__ void __launch_bounds__(128) k_gather_fm(Tables t, const float* __restrict__ stencil, Records rec,
+__global__ void __launch_bounds__(128, SAMP == kSampLoad ? 1 : 6) k_gather_fm(Tables t, const float* __restrict__ stencil, Records rec,
                                                    int cap, F3 L, float alpha, float g, F3 srp,
                                                    float* __restrict__ desc, float* __restrict__ aux) {
   unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -561,7 +542,11 @@ static int neural_passes(Volume* v, const Network* net, const mr_render_params* 
   MR_CUDA(cudaMemsetAsync(v->d_counters, 0, kCounters * sizeof(unsigned long long), s));
   MR_CUDA(cudaMemsetAsync(rec.count, 0, sizeof(unsigned), s));
   NNTraceArgs ta;
-  ta.m = Medium{v->density, v->res, v->max_density, p->tr_scale};
+  ta.m = Medium{v->density, v->res, v->max_density, p->tr_scale, 0};
+  if (!no_alloc) {
+    rc = density_gather_texture(v, s, &ta.m.tex);
+    if (rc) return rc;
+  }
   ta.sc = make_path_scene(p);
   ta.cam = make_camera(p);
   ta.seed = p->seed;
@@ -831,7 +816,7 @@ __global__ void __launch_bounds__(256) k_trace_batch(const BatchJob* __restrict_
 }
 
 template <int SAMP>
-__global__ void __launch_bounds__(256) k_gather_batch(const BatchJob* __restrict__ jobs,
+__global__ void __launch_bounds__(256, 3) k_gather_batch(const BatchJob* __restrict__ jobs,
                                                       const float* __restrict__ stencil, Records rec, int cap,
                                                       float* __restrict__ desc, float* __restrict__ aux) {
   const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1036,7 +1021,11 @@ extern "C" int mr_batch_prepare(mr_batch* h, const mr_network* nh, int64_t wave_
       if (rc) return rc;
     }
     BatchJob& j = hj[i];
-    j.m = Medium{v->density, v->res, v->max_density, p->tr_scale};
+    j.m = Medium{v->density, v->res, v->max_density, p->tr_scale, 0};
+    {
+      int rc = density_gather_texture(v, s, &j.m.tex);
+      if (rc) return rc;
+    }
     j.sc = make_path_scene(p);
     j.cam = make_camera(p);
     j.seed = p->seed;

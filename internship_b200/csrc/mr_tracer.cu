@@ -143,7 +143,11 @@ int launch_delta_track(Volume* v, const mr_render_params* p, float* sum32, doubl
   if (!v->data_set) return set_error(MR_ERR_STATE, "render before mr_volume_set_data");
   if (!v->mips_valid) return set_error(MR_ERR_STATE, "render before mr_volume_update");
   DTArgs a;
-  a.m = Medium{v->density, v->res, v->max_density, p->tr_scale};
+  a.m = Medium{v->density, v->res, v->max_density, p->tr_scale, 0};
+  {
+    int rc = density_gather_texture(v, s, &a.m.tex);
+    if (rc) return rc;
+  }
   a.sc = make_path_scene(p);
   a.cam = make_camera(p);
   a.seed = p->seed;

@@ -10,6 +10,7 @@ struct Medium {
   int res;
   float max_density;  // global majorant (before alpha)
   float tr_scale;
+  cudaTextureObject_t tex;  // layered copy of density read by texture gathers, or 0: texel loads
 };
 
 struct TrackStats {
@@ -19,7 +20,7 @@ struct TrackStats {
 
 __device__ __forceinline__ float fetch_density(const Medium& m, F3 pos, TrackStats& st) {
   ++st.fetches;
-  return tri_border(m.density, m.res, pos + 0.5f);
+  return m.tex ? tri_border_tex(m.tex, m.res, pos + 0.5f) : tri_border(m.density, m.res, pos + 0.5f);
 }
 
 // DeterminateNextVertex (core/render.cuh:138-172).

@@ -344,7 +344,24 @@ int refresh_gather_textures(Volume* v, cudaStream_t s) {
   return MR_OK;
 }
 
+int density_gather_texture(Volume* v, cudaStream_t s, cudaTextureObject_t* out) {
+  if (!v->gth_den_arr) {
+    int rc = make_gather_tex(&v->gth_den_arr, &v->gth_den_tex, v->res, cudaAddressModeBorder);
+    if (rc) return rc;
+    v->gth_den_stale = true;
+  }
+  if (v->gth_den_stale) {
+    int rc = copy_to_array(v->gth_den_arr, v->density, v->res, s);
+    if (rc) return rc;
+    v->gth_den_stale = false;
+  }
+  *out = v->gth_den_tex;
+  return MR_OK;
+}
+
 void destroy_textures(Volume* v) {
+  if (v->gth_den_tex) cudaDestroyTextureObject(v->gth_den_tex);
+  if (v->gth_den_arr) cudaFreeArray(v->gth_den_arr);
   for (int k = 0; k < 9; ++k) {
     if (v->gth_mip_tex[k]) cudaDestroyTextureObject(v->gth_mip_tex[k]);
     if (v->gth_mip_arr[k]) cudaFreeArray(v->gth_mip_arr[k]);
@@ -437,6 +454,7 @@ int mr_volume_set_data(mr_volume* h, const float* host_data, size_t count) {
   if (count != n) return set_error(MR_ERR_ARG, "mr_volume_set_data: count %zu != res^3 = %zu", count, n);
   MR_CUDA(cudaMemcpy(v->density, host_data, n * sizeof(float), cudaMemcpyHostToDevice));
   v->data_set = true;
+  v->gth_den_stale = true;
   v->mips_valid = v->tr_valid = false;
   return MR_OK;
 }
@@ -449,6 +467,7 @@ int mr_volume_set_data_device(mr_volume* h, const float* dev_data, size_t count,
   if (count != n) return set_error(MR_ERR_ARG, "mr_volume_set_data_device: count %zu != res^3 = %zu", count, n);
   MR_CUDA(cudaMemcpyAsync(v->density, dev_data, n * sizeof(float), cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
   v->data_set = true;
+  v->gth_den_stale = true;
   v->mips_valid = v->tr_valid = false;
   return MR_OK;
 }
