@@ -125,10 +125,12 @@ TRAINED = os.path.join(ROOT, "internship_b200", "data", "mrpnn_trained.npy")
 
 # DRAM bytes (read + write) per unit from one ncu capture of each kernel on the
 # 960x540 case of this frame (profiles/*_neural_960x540.md): per active pixel
-# for the gathers and networks, per density fetch for the trace. A launch's
-# traffic = this figure x the launch's units.
-TRAFFIC_PER_UNIT = {"k_mlp_simt": 4422.9, "k_mlp_tc": 2542.6, "k_gather_fm_exact": 2699.0,
-                    "k_gather_fm_texture": 2447.0, "k_nn_trace": 175.9}
+# for the gathers and networks (the fp32 network: k_simt_trunk + k_simt_head),
+# per density fetch for the trace. A launch's traffic = this figure x the
+# launch's units.
+TRAFFIC_PER_UNIT = {"k_simt": 3146.6, "k_mlp_tc": 2542.6, "k_gather_fm_exact": 2489.0,
+                    "k_gather_fm_texture": 2447.0, "k_nn_trace": 137.2}
+SIMT_KERNELS = "k_simt_trunk + k_simt_head (fp32 network, CUDA cores)"
 # fp32 FMA rate of the CUDA cores (148 SMs x 128 lanes x 2 FLOP x 1.965 GHz), nominal
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
@@ -465,9 +467,9 @@ def main():
     stages = {
         "nn_trace": {"bound": "hbm", "kernel": "k_nn_trace", "ms": trace_ms,
                      "achieved": trace_bytes / (trace_ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s"},
-        "nn_gather": {"bound": "hbm", "kernel": "k_gather_fm<false> (exact sampler)", "ms": gather_ms,
+        "nn_gather": {"bound": "hbm", "kernel": "k_gather_fm<kSampGather> (exact sampler, texture gathers)", "ms": gather_ms,
                       "achieved": gather_bytes / (gather_ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s"},
-        "nn_network": {"bound": "tensor", "kernel": "k_mlp_simt (fp32 network, CUDA cores)", "ms": mlp_ms32,
+        "nn_network": {"bound": "tensor", "kernel": SIMT_KERNELS, "ms": mlp_ms32,
                        "achieved": FLOP_PER_PIXEL * active / (mlp_ms32 / 1e3) / 1e12, "peak": bf16,
                        "unit": "TFLOP/s"},
     }
@@ -476,7 +478,7 @@ def main():
         s_["peak_source"] = src
     stages["nn_trace"]["traffic"] = TRAFFIC_PER_UNIT["k_nn_trace"] * fetches
     stages["nn_gather"]["traffic"] = TRAFFIC_PER_UNIT["k_gather_fm_exact"] * active
-    stages["nn_network"]["traffic"] = TRAFFIC_PER_UNIT["k_mlp_simt"] * active
+    stages["nn_network"]["traffic"] = TRAFFIC_PER_UNIT["k_simt"] * active
     stages["nn_network"]["fp32_fma_peak"] = FP32_PEAK_TFLOPS
     stages["nn_network"]["frac_of_fp32_fma_peak"] = stages["nn_network"]["achieved"] / FP32_PEAK_TFLOPS
     for s_ in stages.values():
@@ -496,9 +498,9 @@ def main():
                        "peak": hbm, "unit": "GB/s"},
             "network": {"bound": "tensor",
                         "kernel": ("k_mlp_tc (tcgen05 %s network)" % ("E4M3" if name.startswith("fp8") else "BF16"))
-                        if tc else "k_mlp_simt (fp32 network, CUDA cores)",
+                        if tc else SIMT_KERNELS,
                         "achieved": tf, "peak": bf16, "unit": "TFLOP/s", "frac": tf / bf16, "peak_source": src,
-                        "traffic": TRAFFIC_PER_UNIT["k_mlp_tc" if tc else "k_mlp_simt"] * lg["active"]},
+                        "traffic": TRAFFIC_PER_UNIT["k_mlp_tc" if tc else "k_simt"] * lg["active"]},
         }
     line = {"metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
