@@ -152,7 +152,9 @@ __device__ __forceinline__ void trace_counters(unsigned long long* counters, con
   }
 }
 
-__global__ void __launch_bounds__(128) k_nn_trace(NNTraceArgs a) {
+// Bound by the latency of dependent density fetches: registers capped for
+// twelve 128-thread blocks per SM.
+__global__ void __launch_bounds__(128, 12) k_nn_trace(NNTraceArgs a) {
   int pix = blockIdx.x * blockDim.x + threadIdx.x;
   int npx = a.cam.width * a.cam.height;
   TrackStats st{0, 0};
