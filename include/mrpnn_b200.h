@@ -183,6 +183,14 @@ int mr_tc_selftest(int32_t n, int32_t k, const uint16_t* host_a, const uint16_t*
  * counterpart): host_a 128 x k and host_b n x k are E4M3 bytes, row-major.
  * Shapes (n, k): (16,32) (32,32) (64,128) (128,128). */
 int mr_tc_selftest_fp8(int32_t n, int32_t k, const uint8_t* host_a, const uint8_t* host_b, float* host_d);
+/* The same tile product with fp32 operands on the TF32 path (kind::tf32, no
+ * reference counterpart): host_a 128 x k and host_b n x k fp32, row-major.
+ * split != 0: each operand is split into a TF32 part and an fp32 remainder
+ * and D sums three TF32 products (A_hi B_hi + A_hi B_lo + A_lo B_hi), which
+ * carries about 22 bits of the product; split == 0: one TF32 product.
+ * Shapes (n, k): (16,16) (32,32) (32,64) (64,128). */
+int mr_tc_selftest_tf32(int32_t n, int32_t k, const float* host_a, const float* host_b, float* host_d,
+                        int32_t split);
 /* Self-test of the exact sampler's two forms (no reference counterpart): for
  * n points uv (host_uv, n x 3, texture space) over one
  * MR_SAMPLER_SELFTEST_RES^3 fp32 table (host_table, index (x*R+y)*R+z),

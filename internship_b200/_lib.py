@@ -29,7 +29,7 @@ EXPORTS = [
     "mr_trainer_destroy", "mr_trainer_gradient", "mr_trainer_step", "mr_trainer_weights",
     "mr_render_interactive", "mr_denoise", "mr_batch_create", "mr_batch_destroy", "mr_batch_add", "mr_batch_prepare",
     "mr_batch_autotune", "mr_batch_render", "mr_batch_capture", "mr_batch_launch", "mr_batch_counters",
-    "mr_tc_selftest_fp8", "mr_sampler_selftest",
+    "mr_tc_selftest_fp8", "mr_sampler_selftest", "mr_tc_selftest_tf32",
 ]
 NOALLOC_MAX_PIXELS = 16384
 
@@ -116,6 +116,7 @@ def load():
     L.mr_tc_selftest.argtypes = [i32, i32, vp, vp, vp]
     L.mr_tc_selftest_fp8.argtypes = [i32, i32, vp, vp, vp]
     L.mr_sampler_selftest.argtypes = [i32, vp, vp, vp]
+    L.mr_tc_selftest_tf32.argtypes = [i32, i32, vp, vp, vp, i32]
     L.mr_network_check.argtypes = [vp, i32]
     L.mr_render_neural_noalloc.argtypes = [vp, vp, C.POINTER(RenderParams), vp, vp]
     L.mr_train_points.argtypes = [vp, fp, fp, u32, i32, i32, vp, vp, C.POINTER(i32), vp]

@@ -1062,6 +1062,119 @@ __global__ void __launch_bounds__(128, 1) k_tc_selftest(const uint16_t* __restri
   }
 }
 
+// ---- fp32-accurate products from TF32 operands --------------------------------
+// Canonical K-major no-swizzle offset of element (row, k) of a 4-byte-element
+// tile with KP columns: core matrices of 8 rows x 16 B (4 elements), adjacent
+// along K (LBO 128 B), 8-row groups (KP/4)*128 B apart (SBO). One kind::tf32
+// MMA consumes 8 columns = 32 B, the same byte step as the BF16 layout.
+__host__ __device__ constexpr int canon32(int row, int k, int kp) {
+  return ((row >> 3) * (kp >> 2) + (k >> 2)) * 128 + (row & 7) * 16 + (k & 3) * 4;
+}
+// TF32 x TF32 -> FP32, A and B K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_tf32(int m, int n) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(acc)
+      : "memory");
+}
+// x = hi + lo with hi = x rounded to TF32 (low 13 bits zero) and lo = x - hi
+// exactly; the MMA reads lo to TF32 precision, so hi*b + lo*b carries about
+// 22 bits of x.
+__device__ __forceinline__ void split_tf32(float x, float& hi, float& lo) {
+  uint32_t h;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
+  hi = __uint_as_float(h);
+  lo = x - hi;
+}
+// D[tmem] (+)= A_hi W_hi^T + A_hi W_lo^T + A_lo W_hi^T over KP columns: the
+// small terms first, then the large one.
+template <int NP, int KP>
+__device__ __forceinline__ void issue_tf32x3(uint32_t tmem_d, uint32_t a_hi, uint32_t a_lo, uint32_t w_hi,
+                                             uint32_t w_lo, bool accumulate) {
+  constexpr uint32_t id = idesc_tf32(128, NP);
+  constexpr uint32_t sbo = (KP / 4) * 128;
+#pragma unroll
+  for (int term = 0; term < 3; ++term) {
+    const uint32_t a = term == 1 ? a_lo : a_hi, w = term == 0 ? w_lo : w_hi;
+#pragma unroll
+    for (int s = 0; s < KP / 8; ++s)
+      umma_tf32(tmem_d, sdesc(a + s * 256, 128, sbo), sdesc(w + s * 256, 128, sbo), id,
+                (accumulate || term > 0 || s > 0) ? 1u : 0u);
+  }
+}
+
+// Self-test of the fp32-accurate TF32 path: D[128 x N] = A[128 x K] * B[N x K]^T
+// as three TF32 products per element (split 1) or one (split 0).
+template <int N, int K>
+__global__ void __launch_bounds__(128, 1) k_tc_selftest32(const float* __restrict__ A, const float* __restrict__ B,
+                                                          float* __restrict__ D, int* err, int split) {
+  extern __shared__ __align__(1024) uint8_t dsm[];
+  uint8_t* ah = dsm;
+  uint8_t* al = ah + 128 * K * 4;
+  uint8_t* bh = al + 128 * K * 4;
+  uint8_t* bl = bh + N * K * 4;
+  uint64_t& mbar = *reinterpret_cast<uint64_t*>(bl + N * K * 4);
+  uint32_t& holder = *reinterpret_cast<uint32_t*>(bl + N * K * 4 + 8);
+  const int t = threadIdx.x, warp = t >> 5;
+  for (int k = 0; k < K; ++k) {
+    float h, l;
+    split_tf32(A[t * K + k], h, l);
+    *reinterpret_cast<float*>(ah + canon32(t, k, K)) = split ? h : A[t * K + k];
+    *reinterpret_cast<float*>(al + canon32(t, k, K)) = l;
+    if (t < N) {
+      split_tf32(B[t * K + k], h, l);
+      *reinterpret_cast<float*>(bh + canon32(t, k, K)) = split ? h : B[t * K + k];
+      *reinterpret_cast<float*>(bl + canon32(t, k, K)) = l;
+    }
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&holder)),
+                 "r"(128));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (t == 0) mbar_init(smem_u32(&mbar), 1);
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = holder;
+  if (t == 0) {
+    if (split) {
+      issue_tf32x3<N, K>(tmem, smem_u32(ah), smem_u32(al), smem_u32(bh), smem_u32(bl), false);
+    } else {
+#pragma unroll
+      for (int s = 0; s < K / 8; ++s)
+        umma_tf32(tmem, sdesc(smem_u32(ah) + s * 256, 128, (K / 4) * 128),
+                  sdesc(smem_u32(bh) + s * 256, 128, (K / 4) * 128), idesc_tf32(128, N), s > 0 ? 1u : 0u);
+    }
+    umma_commit(smem_u32(&mbar));
+  }
+  const bool ok = mbar_wait(smem_u32(&mbar), 0);
+  tc_fence_after();
+  if (ok) {
+    float v[16];
+#pragma unroll
+    for (int h = 0; h < N / 16; ++h) {
+      tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + 16 * h, v);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) D[t * N + 16 * h + i] = v[i];
+    }
+  } else if (t == 0) {
+    atomicExch(err, 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128));
+  }
+}
+
 // The same through the E4M3 path: D[128 x N] = A[128 x K] * B[N x K]^T with
 // 8-bit operands (kind::f8f6f4).
 template <int N, int K>
@@ -1302,6 +1415,44 @@ extern "C" int mr_tc_selftest(int32_t n, int32_t k, const uint16_t* host_a, cons
   int he = 0;
   if (rc == MR_OK) cudaMemcpy(&he, err, 4, cudaMemcpyDeviceToHost);
   if (rc == MR_OK && he) rc = set_error(MR_ERR_TIMEOUT, "tc selftest: mbarrier wait timed out");
+  if (rc == MR_OK) cudaMemcpy(host_d, d, 128 * n * 4, cudaMemcpyDeviceToHost);
+  cudaFree(a);
+  cudaFree(b);
+  cudaFree(d);
+  cudaFree(err);
+  return rc;
+}
+
+extern "C" int mr_tc_selftest_tf32(int32_t n, int32_t k, const float* host_a, const float* host_b, float* host_d,
+                                   int32_t split) {
+  clear_error();
+  if (!host_a || !host_b || !host_d) return set_error(MR_ERR_ARG, "mr_tc_selftest_tf32: NULL argument");
+  float *a = nullptr, *b = nullptr, *d = nullptr;
+  int* err = nullptr;
+  MR_CUDA(cudaMalloc(&a, 128 * k * 4));
+  MR_CUDA(cudaMalloc(&b, n * k * 4));
+  MR_CUDA(cudaMalloc(&d, 128 * n * 4));
+  MR_CUDA(cudaMalloc(&err, 4));
+  MR_CUDA(cudaMemset(err, 0, 4));
+  MR_CUDA(cudaMemcpy(a, host_a, 128 * k * 4, cudaMemcpyHostToDevice));
+  MR_CUDA(cudaMemcpy(b, host_b, n * k * 4, cudaMemcpyHostToDevice));
+  int rc = MR_OK;
+  const int sm = 2 * (128 * k + n * k) * 4 + 16;
+#define MR_SELFTEST32(NN, KK)                                                                       \
+  if (n == NN && k == KK) {                                                                         \
+    cudaFuncSetAttribute(k_tc_selftest32<NN, KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm); \
+    k_tc_selftest32<NN, KK><<<1, 128, sm>>>(a, b, d, err, split ? 1 : 0);                           \
+  } else
+  MR_SELFTEST32(16, 16) MR_SELFTEST32(32, 32) MR_SELFTEST32(32, 64) MR_SELFTEST32(64, 128)
+  rc = set_error(MR_ERR_ARG, "mr_tc_selftest_tf32: shape %dx%d not built", n, k);
+#undef MR_SELFTEST32
+  if (rc == MR_OK) {
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) rc = cuda_error(e, "tc selftest tf32");
+  }
+  int he = 0;
+  if (rc == MR_OK) cudaMemcpy(&he, err, 4, cudaMemcpyDeviceToHost);
+  if (rc == MR_OK && he) rc = set_error(MR_ERR_TIMEOUT, "tc selftest tf32: mbarrier wait timed out");
   if (rc == MR_OK) cudaMemcpy(host_d, d, 128 * n * 4, cudaMemcpyDeviceToHost);
   cudaFree(a);
   cudaFree(b);

@@ -198,3 +198,28 @@ def test_fp8_network_close_to_fp32():
     assert np.median(rel8) < 0.08
     assert np.quantile(rel8, 0.99) < 0.3
     assert np.median(d8) > np.median(db)  # coarser than BF16, as it must be
+
+
+@pytest.mark.parametrize("n,k", [(16, 16), (32, 32), (32, 64), (64, 128)])
+def test_tf32_split_tile_product_is_fp32_accurate(n, k):
+    """kind::tf32 tile product through the K-major 4-byte operand layout:
+    one TF32 product carries ~11 bits per operand; the three-term split
+    (A_hi B_hi + A_hi B_lo + A_lo B_hi) carries ~22, i.e. the error of an
+    fp32 dot product."""
+    from internship_b200 import _lib
+    rng = np.random.default_rng(n * 13 + k)
+    a = rng.standard_normal((128, k)).astype(np.float32)
+    b = rng.standard_normal((n, k)).astype(np.float32)
+    ref = a.astype(np.float64) @ b.astype(np.float64).T
+    scale = np.abs(a).astype(np.float64) @ np.abs(b).astype(np.float64).T  # sum of |terms|
+    L = _lib.load()
+    d1 = np.zeros((128, n), np.float32)
+    _lib.check(L.mr_tc_selftest_tf32(n, k, a.ctypes.data, b.ctypes.data, d1.ctypes.data, 0))
+    d3 = np.zeros((128, n), np.float32)
+    _lib.check(L.mr_tc_selftest_tf32(n, k, a.ctypes.data, b.ctypes.data, d3.ctypes.data, 1))
+    e1 = np.abs(d1 - ref) / scale
+    e3 = np.abs(d3 - ref) / scale
+    print("max error / sum|terms|: tf32 %.3g, split %.3g" % (e1.max(), e3.max()))
+    assert e1.max() < 2e-3  # one TF32 product per element
+    assert e3.max() < 1e-6  # fp32-level
+    assert e3.max() < e1.max() / 100
