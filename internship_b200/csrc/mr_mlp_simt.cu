@@ -19,8 +19,12 @@
 // order, as LinearReLU does.
 #include <vector>
 
+#include <algorithm>
+#include <cstring>
+
 #include "mr_internal.h"
 #include "mr_net_layout.cuh"
+#include "mr_tcgen05.cuh"
 
 namespace mr {
 
@@ -56,7 +60,31 @@ constexpr int kSeBlocks = 12, kSeFloats = 96 + 64 + 24;
 constexpr int kSeOff = kHeadImage + stage_offset(kTrunkStages);
 constexpr int kHeadRowOff = kSeOff + kSeBlocks * kSeFloats;
 constexpr int kHeadRowFloats = 96 + 16 + 32 + 20;
-constexpr int kSimtImage = kHeadRowOff + kHeadRowFloats;
+// [tensor-core head: LC0 / LC1 / LC2 as chunks of 32 input columns, each
+//  chunk the TF32 part then the fp32 remainder of its N x 32 weights in the
+//  canonical K-major layout (canon32); then the biases LC0B, LC1B, LC2B]
+constexpr int kTcKC = 32;     // input columns per weight chunk
+constexpr int kTcChunks = 10;  // per albedo channel: LC0 4, LC1 4, LC2 2
+__host__ __device__ constexpr int tc_chunk_n(int c) { return c < 4 ? 128 : c < 8 ? 64 : 32; }
+__host__ __device__ constexpr int tc_chunk_floats(int c) { return 2 * kTcKC * tc_chunk_n(c); }
+__host__ __device__ constexpr int tc_chunk_off(int c) {
+  return c < 4 ? 8192 * c : c < 8 ? 32768 + 4096 * (c - 4) : 49152 + 2048 * (c - 8);
+}
+constexpr int kTcHeadOff = (kHeadRowOff + kHeadRowFloats + 63) / 64 * 64;  // 256-byte aligned
+constexpr int kTcBiasOff = kTcHeadOff + tc_chunk_off(kTcChunks);  // LC0B 128, LC1B 64, LC2B 32
+constexpr int kSimtImage = kTcBiasOff + 224;
+static_assert(kTcHeadOff % 64 == 0 && kTcBiasOff % 4 == 0, "image alignment");
+
+// fp32 -> TF32 rounded to nearest, ties away from zero (cvt.rna.tf32.f32 on
+// the device), for finite x.
+static float tf32_rna(float x) {
+  uint32_t u;
+  std::memcpy(&u, &x, 4);
+  u = (u + 0x1000u) & 0xFFFFE000u;
+  float r;
+  std::memcpy(&r, &u, 4);
+  return r;
+}
 static_assert(kSeOff % 4 == 0 && kSeFloats % 4 == 0 && kHeadRowOff % 4 == 0, "float4 alignment");
 
 void simt_weight_image(const float* w, std::vector<float>& img) {
@@ -111,6 +139,27 @@ void simt_weight_image(const float* w, std::vector<float>& img) {
   for (int i = 0; i < 8; ++i) hr[136 + i] = w[wt.off[MR_W_LGGSB] + i];
   for (int i = 0; i < 16; ++i) hr[144 + i] = w[wt.off[MR_W_LX12W] + i];
   hr[160] = w[wt.off[MR_W_LX12B]];
+  // tensor-core head
+  const int lw[3] = {MR_W_LC0W, MR_W_LC1W, MR_W_LC2W}, lb[3] = {MR_W_LC0B, MR_W_LC1B, MR_W_LC2B};
+  const int lk[3] = {128, 128, 64};
+  int c = 0;
+  for (int l = 0; l < 3; ++l) {
+    const int N = tc_chunk_n(c), K = lk[l];
+    const float* W = w + wt.off[lw[l]];  // W[N][K]
+    for (int j = 0; j < K / kTcKC; ++j, ++c) {
+      float* hi = img.data() + kTcHeadOff + tc_chunk_off(c);
+      float* lo = hi + N * kTcKC;
+      for (int nn = 0; nn < N; ++nn)
+        for (int kl = 0; kl < kTcKC; ++kl) {
+          const float x = W[(size_t)nn * K + kTcKC * j + kl], h = tf32_rna(x);
+          hi[canon32(nn, kl, kTcKC) / 4] = h;
+          lo[canon32(nn, kl, kTcKC) / 4] = x - h;
+        }
+    }
+  }
+  for (int i = 0; i < 128; ++i) img[kTcBiasOff + i] = w[wt.off[lb[0]] + i];
+  for (int i = 0; i < 64; ++i) img[kTcBiasOff + 128 + i] = w[wt.off[lb[1]] + i];
+  for (int i = 0; i < 32; ++i) img[kTcBiasOff + 192 + i] = w[wt.off[lb[2]] + i];
 }
 
 // ---- trunk ---------------------------------------------------------------------------
@@ -514,6 +563,7 @@ struct HeadArgs {
   F3 light_color, scatter;
   const int* job;
   const BatchOut* bout;
+  int* err;  // tensor-core head: set when a bounded wait gave up
 };
 
 // The head weights (LC0, LC1, LC2 transposed; 13 chunks of 8 KB, repeated
@@ -799,6 +849,346 @@ __global__ void __launch_bounds__(kHeadThreads, 1) k_simt_head(HeadArgs a) {
   }
 }
 
+// ---- head on the tensor cores (fp32-accurate) ---------------------------------------
+// LC0 / LC1 / LC2 as M = 128 tcgen05 MMAs of kind::tf32 with FP32 accumulators
+// in TMEM: every product is the sum of three TF32 products (A_hi W_hi + A_hi
+// W_lo + A_lo W_hi, split_tf32), which carries about 22 bits of each operand,
+// the accuracy of an fp32 dot product. Activations live in two canonical
+// K-major tiles (TF32 part and fp32 remainder, 128 rows x K <= 128).
+// Persistent blocks (one per SM) walk the row tiles. Thread 0 streams the
+// split weight chunks (32 input columns each, the same 10-chunk sequence for
+// every albedo channel) into a 3-slot shared-memory ring with bulk copies two
+// chunks ahead of the MMAs that consume them (per-slot full / empty
+// mbarriers), and issues the MMAs; the other threads only wait for a layer's
+// MMAs before its epilogue, which runs per row on the TMEM lanes (bias, ReLU,
+// split into the next layer's tiles). Gates, LX and the residual pairs stay
+// per row on the CUDA cores.
+constexpr int kTcSlots = 3;
+constexpr int kTcStage = 2 * kTcKC * 128;  // floats per ring slot (largest chunk: 32 KB)
+constexpr int kTcATile = 128 * 128;        // floats per A tile
+constexpr int kTcHeadSmem = (2 * kTcATile + kTcSlots * kTcStage) * (int)sizeof(float) + 64;
+
+struct TcFeed {  // thread 0's view of the weight ring
+  const float* __restrict__ src;  // chunk images
+  uint32_t ring, full, empty;     // shared addresses: slot 0, full[0], empty[0] (slots 8 B apart)
+  int x;                          // next chunk to consume (running over channels and tiles)
+  bool ok;
+  __device__ __forceinline__ void load(int z) {  // chunk z into slot z % 3
+    const int c = z % kTcChunks, s = z % kTcSlots;
+    const uint32_t bytes = (uint32_t)tc_chunk_floats(c) * 4u;
+    mbar_expect_tx(full + 8 * s, bytes);
+    bulk_g2s(ring + (uint32_t)(s * kTcStage * 4), src + tc_chunk_off(c), bytes, full + 8 * s);
+  }
+};
+
+// Thread 0: the MMAs of one head layer D[tmem] = A (128 x K) W^T (K -> N),
+// K / 32 chunks of three TF32 products (4 MMAs of K = 8 each), refilling
+// each consumed slot with the chunk three places later; then a commit on
+// `done` that completes when every MMA of the layer has.
+template <int N, int K>
+__device__ __forceinline__ void tc_issue_layer(TcFeed& f, uint32_t tmem, uint32_t ahi, uint32_t alo, uint32_t done) {
+  constexpr uint32_t id = idesc_tf32(128, N), sbo_a = (K / 4) * 128, sbo_b = (kTcKC / 4) * 128;
+#pragma unroll 1
+  for (int j = 0; j < K / kTcKC; ++j) {
+    const int x = f.x, s = x % kTcSlots;
+    if (f.ok && !mbar_wait(f.full + 8 * s, (uint32_t)(x / kTcSlots) & 1u)) f.ok = false;
+    tc_fence_after();
+    if (f.ok) {
+      const uint32_t bh = f.ring + (uint32_t)(s * kTcStage * 4), bl = bh + N * kTcKC * 4;
+#pragma unroll
+      for (int term = 0; term < 3; ++term) {  // remainder terms first, then TF32 x TF32
+        const uint32_t a = (term == 1 ? alo : ahi) + j * (kTcKC / 4) * 128, b = term == 0 ? bl : bh;
+#pragma unroll
+        for (int k8 = 0; k8 < kTcKC / 8; ++k8)
+          umma_tf32(tmem, sdesc(a + k8 * 256, 128, sbo_a), sdesc(b + k8 * 256, 128, sbo_b), id,
+                    (j | term | k8) ? 1u : 0u);
+      }
+    }
+    umma_commit(f.empty + 8 * s);
+    if (x >= 1) {  // chunk x - 1's MMAs are done with their slot: chunk x + 2 goes there
+      const int y = x - 1, ys = y % kTcSlots;
+      if (f.ok && !mbar_wait(f.empty + 8 * ys, (uint32_t)(y / kTcSlots) & 1u)) f.ok = false;
+      if (f.ok) f.load(x + 2);
+    }
+    ++f.x;
+  }
+  umma_commit(done);
+}
+
+// All threads: the layer's MMAs are complete (bounded wait).
+__device__ __forceinline__ void tc_layer_wait(uint32_t done, uint32_t& parity, bool& ok) {
+  if (ok && !mbar_wait(done, parity)) ok = false;
+  parity ^= 1u;
+  tc_fence_after();
+}
+
+// 4 activations of row r at columns k..k+3 into the K-major split tiles.
+__device__ __forceinline__ void put_split4(float* ahi, float* alo, int r, int k, int kp, float x0, float x1, float x2,
+                                           float x3) {
+  float4 h, l;
+  split_tf32(x0, h.x, l.x);
+  split_tf32(x1, h.y, l.y);
+  split_tf32(x2, h.z, l.z);
+  split_tf32(x3, h.w, l.w);
+  const int o = canon32(r, k, kp) / 4;
+  *reinterpret_cast<float4*>(ahi + o) = h;
+  *reinterpret_cast<float4*>(alo + o) = l;
+}
+
+// Epilogue of a layer with N outputs: this thread's N/2 columns (half `h`) of
+// its TMEM lane, ReLU(acc + bias), into the next layer's tiles (K = N).
+template <int N>
+__device__ __forceinline__ void tc_epi_split(uint32_t tl, const float* __restrict__ bias, float* ahi, float* alo, int r,
+                                             int h) {
+#pragma unroll
+  for (int q = 0; q < N / 32; ++q) {
+    const int c0 = h * (N / 2) + 16 * q;
+    float v[16];
+    tmem_ld16(tl + c0, v);
+#pragma unroll
+    for (int i = 0; i < 16; i += 4) {
+      const float4 b = ldg4(bias + c0 + i);
+      put_split4(ahi, alo, r, c0 + i, N, relu0(v[i] + b.x), relu0(v[i + 1] + b.y), relu0(v[i + 2] + b.z),
+                 relu0(v[i + 3] + b.w));
+    }
+  }
+}
+
+// Head SC(p) (radiancePredict.cu:439-473) per distinct albedo channel for
+// tiles of 128 rows, LC0 / LC1 / LC2 on the tensor cores. Thread t serves
+// row r = 32 (warp % 4) + lane (its TMEM lane) and column half warp / 4.
+__global__ void __launch_bounds__(kHeadThreads, 1) k_tc32_head(HeadArgs a) {
+  extern __shared__ __align__(1024) float tcsm[];
+  float* Ahi = tcsm;
+  float* Alo = tcsm + kTcATile;
+  float* ring = tcsm + 2 * kTcATile;
+  uint64_t* mb = reinterpret_cast<uint64_t*>(ring + kTcSlots * kTcStage);  // full[3], empty[3], done
+  uint32_t* holder = reinterpret_cast<uint32_t*>(mb + 2 * kTcSlots + 1);
+  const int n = a.count ? (int)min(*a.count, (unsigned)a.n) : a.n;
+  const int ntiles = (n + kHeadRows - 1) / kHeadRows;
+  if ((int)blockIdx.x >= ntiles) return;  // block-uniform
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r = 32 * (warp & 3) + lane, half = warp >> 2;
+  const float* __restrict__ w = a.w;
+  const float* __restrict__ hr = a.wt + kHeadRowOff;
+  const float* __restrict__ bias = a.wt + kTcBiasOff;
+  const uint32_t done = smem_u32(mb + 2 * kTcSlots);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(holder)),
+                 "r"(128));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 2 * kTcSlots + 1; ++i) mbar_init(smem_u32(mb + i), 1);
+  }
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *holder;
+  const uint32_t tl = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
+  const uint32_t ahi = smem_u32(Ahi), alo = smem_u32(Alo);
+  TcFeed feed{a.wt + kTcHeadOff, smem_u32(ring), smem_u32(mb), smem_u32(mb + kTcSlots), 0, true};
+  if (threadIdx.x == 0)
+    for (int z = 0; z < kTcSlots; ++z) feed.load(z);
+  uint32_t dpar = 0;
+  bool ok = true;
+#pragma unroll 1
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int row = tile * kHeadRows + r;
+    const bool valid = row < n;
+    const int kr = valid ? row : n - 1;
+    const float* trow = a.t + (long long)kr * a.trs;
+    const float* ax = a.aux + (long long)kr * a.ars;
+    const float g = __ldg(ax), gamma = __ldg(ax + a.afs);
+    const float srp[3] = {__ldg(ax + 2 * a.afs), __ldg(ax + 3 * a.afs), __ldg(ax + 4 * a.afs)};
+    float fin[16];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const float4 q = __ldg(reinterpret_cast<const float4*>(trow + (30 + c) * a.tcs));
+      fin[4 * c] = q.x; fin[4 * c + 1] = q.y; fin[4 * c + 2] = q.z; fin[4 * c + 3] = q.w;
+    }
+    tc_fence_before();  // the previous tile's TMEM reads
+    const bool need1 = __syncthreads_or(valid && srp[1] != srp[0]);
+    const bool need2 = __syncthreads_or(valid && srp[2] != srp[0] && srp[2] != srp[1]);
+    float X[3] = {0.0f, 0.0f, 0.0f};  // of row r
+#pragma unroll 1
+    for (int ch = 0; ch < 3; ++ch) {
+      if ((ch == 1 && !need1) || (ch == 2 && !need2)) continue;
+      const float sc = ch == 0 ? srp[0] : ch == 1 ? srp[1] : srp[2];
+      // gates of this channel (LGGS, LSEFin1's albedo column, LSEFin2)
+      float sep[6];
+      {
+        float sew[16];
+#pragma unroll
+        for (int j = 0; j < 16; j += 4) {
+          const float4 f = ldg4(hr + 96 + j);
+          sew[j] = relu0(fin[j] + sc * f.x);
+          sew[j + 1] = relu0(fin[j + 1] + sc * f.y);
+          sew[j + 2] = relu0(fin[j + 2] + sc * f.z);
+          sew[j + 3] = relu0(fin[j + 3] + sc * f.w);
+        }
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+          float acc = 0.0f;
+#pragma unroll
+          for (int j = 0; j < 16; j += 4) {
+            const float4 f = ldg4(hr + i * 16 + j);
+            acc += sew[j] * f.x;
+            acc += sew[j + 1] * f.y;
+            acc += sew[j + 2] * f.z;
+            acc += sew[j + 3] * f.w;
+          }
+          sep[i] = 1.0f / (1.0f + expf(-acc));
+        }
+      }
+      // gated head input into the LC0 tiles: columns 64 half .. 64 half + 63
+#pragma unroll 4
+      for (int c = 16 * half; c < 16 * half + 16; ++c) {
+        if (c < 30) {
+          const float4 q = __ldg(reinterpret_cast<const float4*>(trow + c * a.tcs));
+          const float s = c < 24 ? sep[c >> 3] : sep[3 + ((c - 24) >> 1)];
+          put_split4(Ahi, Alo, r, 4 * c, 128, q.x * s, q.y * s, q.z * s, q.w * s);
+        } else {
+          float x[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {  // LGGS 3 -> 8, bias after the sum
+            const int i = 4 * (c - 30) + u;
+            float acc =
+                g * __ldg(hr + 112 + 3 * i) + gamma * __ldg(hr + 112 + 3 * i + 1) + sc * __ldg(hr + 112 + 3 * i + 2);
+            acc += __ldg(hr + 136 + i);
+            x[u] = relu0(acc);
+          }
+          put_split4(Ahi, Alo, r, 4 * c, 128, x[0], x[1], x[2], x[3]);
+        }
+      }
+      // LC0
+      fence_async_smem();
+      tc_fence_before();
+      __syncthreads();
+      if (threadIdx.x == 0) tc_issue_layer<128, 128>(feed, tmem, ahi, alo, done);
+      tc_layer_wait(done, dpar, ok);
+      tc_epi_split<128>(tl, bias, Ahi, Alo, r, half);
+      // LC1
+      fence_async_smem();
+      tc_fence_before();
+      __syncthreads();
+      if (threadIdx.x == 0) tc_issue_layer<64, 128>(feed, tmem, ahi, alo, done);
+      tc_layer_wait(done, dpar, ok);
+      tc_epi_split<64>(tl, bias + 128, Ahi, Alo, r, half);
+      // LC2
+      fence_async_smem();
+      tc_fence_before();
+      __syncthreads();
+      if (threadIdx.x == 0) tc_issue_layer<32, 64>(feed, tmem, ahi, alo, done);
+      tc_layer_wait(done, dpar, ok);
+      // LX 32 -> 16, the residual pairs (:454-471) and LX12, per row on the
+      // first four warps
+      if (half == 0) {
+        float x32[32];
+        tmem_ld16(tl, x32);
+        tmem_ld16(tl + 16, x32 + 16);
+#pragma unroll
+        for (int i = 0; i < 32; i += 4) {
+          const float4 b = ldg4(bias + 192 + i);
+          x32[i] = relu0(x32[i] + b.x);
+          x32[i + 1] = relu0(x32[i + 1] + b.y);
+          x32[i + 2] = relu0(x32[i + 2] + b.z);
+          x32[i + 3] = relu0(x32[i + 3] + b.w);
+        }
+        float a16[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          float acc = __ldg(w + WOFF(LXB) + q);
+#pragma unroll
+          for (int j = 0; j < 32; j += 4) {
+            const float4 v = ldg4(w + WOFF(LXW) + q * 32 + j);
+            acc += x32[j] * v.x;
+            acc += x32[j + 1] * v.y;
+            acc += x32[j + 2] * v.z;
+            acc += x32[j + 3] * v.w;
+          }
+          a16[q] = relu0(acc);
+        }
+        const int lx[12] = {WOFF(LX0W), WOFF(LX1W), WOFF(LX2W), WOFF(LX3W), WOFF(LX4W), WOFF(LX5W),
+                            WOFF(LX6W), WOFF(LX7W), WOFF(LX8W), WOFF(LX9W), WOFF(LX10W), WOFF(LX11W)};
+#pragma unroll 1
+        for (int rr = 0; rr < 6; ++rr) {
+          float b16[16], c16[16], h8[8];
+          dense16_half(a16, h8, w + lx[2 * rr], w + lx[2 * rr] + 256, 0);
+#pragma unroll
+          for (int i = 0; i < 8; ++i) b16[i] = h8[i];
+          dense16_half(a16, h8, w + lx[2 * rr], w + lx[2 * rr] + 256, 1);
+#pragma unroll
+          for (int i = 0; i < 8; ++i) b16[8 + i] = h8[i];
+          dense16_half(b16, h8, w + lx[2 * rr + 1], w + lx[2 * rr + 1] + 256, 0);
+#pragma unroll
+          for (int i = 0; i < 8; ++i) c16[i] = h8[i];
+          dense16_half(b16, h8, w + lx[2 * rr + 1], w + lx[2 * rr + 1] + 256, 1);
+#pragma unroll
+          for (int i = 0; i < 8; ++i) c16[8 + i] = h8[i];
+#pragma unroll
+          for (int i = 0; i < 16; ++i) a16[i] = a16[i] + c16[i];
+        }
+        float o = 0.0f;  // LX12 16 -> 1, bias after the sum
+#pragma unroll
+        for (int i = 0; i < 16; i += 4) {
+          const float4 v = ldg4(hr + 144 + i);
+          o += a16[i] * v.x;
+          o += a16[i + 1] * v.y;
+          o += a16[i + 2] * v.z;
+          o += a16[i + 3] * v.w;
+        }
+        o += __ldg(hr + 160);
+        const float xo = relu0(o);
+        if (ch == 0) X[0] = xo;
+        else if (ch == 1) X[1] = xo;
+        else X[2] = xo;
+      }
+    }
+    if (half == 0 && valid) {
+      if (srp[1] == srp[0]) X[1] = X[0];
+      if (srp[2] == srp[0]) X[2] = X[0];
+      else if (srp[2] == srp[1]) X[2] = X[1];
+      float o[3] = {fmaxf(expf(X[0]) - 1.0f, 0.0f) * srp[0], fmaxf(expf(X[1]) - 1.0f, 0.0f) * srp[1],
+                    fmaxf(expf(X[2]) - 1.0f, 0.0f) * srp[2]};
+      if (a.pix) {
+        const int px = a.pix[row];
+        const float tr = a.trph[row];
+        F3 lc = a.light_color, scv = a.scatter;
+        float* dst = a.out;
+        if (a.job) {
+          const BatchOut& bo = a.bout[a.job[row]];
+          lc = bo.light_color;
+          scv = bo.scatter;
+          dst = bo.out;
+        }
+        dst[3 * (size_t)px + 0] = fmaxf(((o[0] + tr) * lc.x) * scv.x, 0.0f);
+        dst[3 * (size_t)px + 1] = fmaxf(((o[1] + tr) * lc.y) * scv.y, 0.0f);
+        dst[3 * (size_t)px + 2] = fmaxf(((o[2] + tr) * lc.z) * scv.z, 0.0f);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) a.out[3 * (size_t)row + c] = o[c];
+      }
+    }
+  }
+  // the two chunks loaded ahead of the last consumed one land before exit
+  if (threadIdx.x == 0) {
+    for (int z = feed.x; z < feed.x + 2; ++z)
+      if (feed.ok && !mbar_wait(feed.full + 8 * (z % kTcSlots), (uint32_t)(z / kTcSlots) & 1u)) feed.ok = false;
+    if (!feed.ok) ok = false;
+  }
+  if (!ok && a.err) atomicExch(a.err, 1);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128));
+  }
+}
+
+int* mlp_error_word(const Network* net);  // mr_mlp_tc.cu
+
 // Trunk kernel then head kernel. `tout` receives the trunk outputs (TrunkOut
 // layout with strides trs / tcs): the render path passes its own descriptor
 // columns, whose first 34 chunks of a row are no longer needed once that row's
@@ -811,6 +1201,7 @@ int launch_mlp_simt(const Network* net, const float* desc, const float* aux, lon
   static bool attr = false;
   if (!attr) {
     MR_CUDA(cudaFuncSetAttribute(k_simt_head, cudaFuncAttributeMaxDynamicSharedMemorySize, kHeadSmem));
+    MR_CUDA(cudaFuncSetAttribute(k_tc32_head, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcHeadSmem));
     MR_CUDA(cudaFuncSetAttribute(k_simt_trunk, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrunkSmem));
     attr = true;
   }
@@ -845,7 +1236,9 @@ int launch_mlp_simt(const Network* net, const float* desc, const float* aux, lon
   h.scatter = scatter;
   h.job = job;
   h.bout = bout;
-  k_simt_head<<<(unsigned)((n + kHeadRows - 1) / kHeadRows), kHeadThreads, kHeadSmem, s>>>(h);
+  h.err = mlp_error_word(net);
+  const int tiles = (n + kHeadRows - 1) / kHeadRows;
+  k_tc32_head<<<(unsigned)std::min(tiles, sm_count()), kHeadThreads, kTcHeadSmem, s>>>(h);
   MR_CUDA(cudaGetLastError());
   return MR_OK;
 }
