@@ -954,6 +954,24 @@ __device__ __forceinline__ void tc_epi_split(uint32_t tl, const float* __restric
   }
 }
 
+// L2 prefetch of tile `tile`'s trunk outputs (rows below n): one range per
+// 4-float chunk when rows are 16 bytes apart (render path), else one range of
+// whole rows when the chunks of a row are contiguous.
+__device__ __forceinline__ void prefetch_tile(const HeadArgs& a, int tile, int n) {
+  const long long r0 = (long long)tile * kHeadRows;
+  if (r0 >= n) return;
+  const int rows = (int)min((long long)kHeadRows, n - r0);
+  if (a.trs == 4) {
+    for (int c = 0; c < 34; ++c)
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a.t + r0 * 4 + c * a.tcs), "r"(rows * 16)
+                   : "memory");
+  } else if (a.tcs == 4 && a.trs % 4 == 0) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a.t + r0 * a.trs),
+                 "r"((unsigned)(rows * a.trs * 4))
+                 : "memory");
+  }
+}
+
 // Head SC(p) (radiancePredict.cu:439-473) per distinct albedo channel for
 // tiles of 128 rows, LC0 / LC1 / LC2 on the tensor cores. Thread t serves
 // row r = 32 (warp % 4) + lane (its TMEM lane) and column half warp / 4.
@@ -968,7 +986,8 @@ __global__ void __launch_bounds__(kHeadThreads, 1) k_tc32_head(HeadArgs a) {
   const int ntiles = (n + kHeadRows - 1) / kHeadRows;
   if ((int)blockIdx.x >= ntiles) return;  // block-uniform
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int r = 32 * (warp & 3) + lane, half = warp >> 2;
+  const int r = 32 * (warp & 3) + lane, half = warp >> 2;  // TMEM lane mapping
+  const int rt = 16 * warp + (lane & 15), ht = lane >> 4;      // tail mapping (lane pairs)
   const float* __restrict__ w = a.w;
   const float* __restrict__ hr = a.wt + kHeadRowOff;
   const float* __restrict__ bias = a.wt + kTcBiasOff;
@@ -1003,15 +1022,20 @@ __global__ void __launch_bounds__(kHeadThreads, 1) k_tc32_head(HeadArgs a) {
     const float g = __ldg(ax), gamma = __ldg(ax + a.afs);
     const float srp[3] = {__ldg(ax + 2 * a.afs), __ldg(ax + 3 * a.afs), __ldg(ax + 4 * a.afs)};
     float fin[16];
+    float4 tin[16];  // this thread's trunk-output chunks 16 half .. 16 half + 15 (those below 30)
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+      if (16 * half + i < 30) tin[i] = __ldg(reinterpret_cast<const float4*>(trow + (16 * half + i) * a.tcs));
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       const float4 q = __ldg(reinterpret_cast<const float4*>(trow + (30 + c) * a.tcs));
       fin[4 * c] = q.x; fin[4 * c + 1] = q.y; fin[4 * c + 2] = q.z; fin[4 * c + 3] = q.w;
     }
+    if (threadIdx.x == 0) prefetch_tile(a, tile + gridDim.x, n);  // the next tile's trunk outputs -> L2
     tc_fence_before();  // the previous tile's TMEM reads
     const bool need1 = __syncthreads_or(valid && srp[1] != srp[0]);
     const bool need2 = __syncthreads_or(valid && srp[2] != srp[0] && srp[2] != srp[1]);
-    float X[3] = {0.0f, 0.0f, 0.0f};  // of row r
+    float X[3] = {0.0f, 0.0f, 0.0f};  // of row rt
 #pragma unroll 1
     for (int ch = 0; ch < 3; ++ch) {
       if ((ch == 1 && !need1) || (ch == 2 && !need2)) continue;
@@ -1043,10 +1067,11 @@ __global__ void __launch_bounds__(kHeadThreads, 1) k_tc32_head(HeadArgs a) {
         }
       }
       // gated head input into the LC0 tiles: columns 64 half .. 64 half + 63
-#pragma unroll 4
-      for (int c = 16 * half; c < 16 * half + 16; ++c) {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int c = 16 * half + i;
         if (c < 30) {
-          const float4 q = __ldg(reinterpret_cast<const float4*>(trow + c * a.tcs));
+          const float4 q = tin[i];
           const float s = c < 24 ? sep[c >> 3] : sep[3 + ((c - 24) >> 1)];
           put_split4(Ahi, Alo, r, 4 * c, 128, q.x * s, q.y * s, q.z * s, q.w * s);
         } else {
@@ -1082,51 +1107,55 @@ __global__ void __launch_bounds__(kHeadThreads, 1) k_tc32_head(HeadArgs a) {
       __syncthreads();
       if (threadIdx.x == 0) tc_issue_layer<32, 64>(feed, tmem, ahi, alo, done);
       tc_layer_wait(done, dpar, ok);
-      // LX 32 -> 16, the residual pairs (:454-471) and LX12, per row on the
-      // first four warps
-      if (half == 0) {
-        float x32[32];
-        tmem_ld16(tl, x32);
-        tmem_ld16(tl + 16, x32 + 16);
+      // LC2 outputs (bias, ReLU) to shared memory, [column][row] over the A
+      // tile, free now
+      {
+        float v[16];
+        tmem_ld16(tl + 16 * half, v);
 #pragma unroll
-        for (int i = 0; i < 32; i += 4) {
-          const float4 b = ldg4(bias + 192 + i);
-          x32[i] = relu0(x32[i] + b.x);
-          x32[i + 1] = relu0(x32[i + 1] + b.y);
-          x32[i + 2] = relu0(x32[i + 2] + b.z);
-          x32[i + 3] = relu0(x32[i + 3] + b.w);
+        for (int i = 0; i < 16; i += 4) {
+          const float4 b = ldg4(bias + 192 + 16 * half + i);
+          Ahi[(16 * half + i) * kHeadRows + r] = relu0(v[i] + b.x);
+          Ahi[(16 * half + i + 1) * kHeadRows + r] = relu0(v[i + 1] + b.y);
+          Ahi[(16 * half + i + 2) * kHeadRows + r] = relu0(v[i + 2] + b.z);
+          Ahi[(16 * half + i + 3) * kHeadRows + r] = relu0(v[i + 3] + b.w);
         }
+      }
+      tc_fence_before();
+      __syncthreads();
+      // LX 32 -> 16, the residual pairs (:454-471) and LX12 for row rt, split
+      // over lanes l and l ^ 16 (half ht of every 16-wide layer each)
+      {
+        float x32[32];
+#pragma unroll
+        for (int i = 0; i < 32; ++i) x32[i] = Ahi[i * kHeadRows + rt];
         float a16[16];
+        {
+          float a8[8];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          float acc = __ldg(w + WOFF(LXB) + q);
+          for (int q = 0; q < 8; ++q) {
+            float acc = __ldg(w + WOFF(LXB) + 8 * ht + q);
 #pragma unroll
-          for (int j = 0; j < 32; j += 4) {
-            const float4 v = ldg4(w + WOFF(LXW) + q * 32 + j);
-            acc += x32[j] * v.x;
-            acc += x32[j + 1] * v.y;
-            acc += x32[j + 2] * v.z;
-            acc += x32[j + 3] * v.w;
+            for (int j = 0; j < 32; j += 4) {
+              const float4 v = ldg4(w + WOFF(LXW) + (8 * ht + q) * 32 + j);
+              acc += x32[j] * v.x;
+              acc += x32[j + 1] * v.y;
+              acc += x32[j + 2] * v.z;
+              acc += x32[j + 3] * v.w;
+            }
+            a8[q] = relu0(acc);
           }
-          a16[q] = relu0(acc);
+          join16(a8, a16, ht);
         }
         const int lx[12] = {WOFF(LX0W), WOFF(LX1W), WOFF(LX2W), WOFF(LX3W), WOFF(LX4W), WOFF(LX5W),
                             WOFF(LX6W), WOFF(LX7W), WOFF(LX8W), WOFF(LX9W), WOFF(LX10W), WOFF(LX11W)};
 #pragma unroll 1
         for (int rr = 0; rr < 6; ++rr) {
-          float b16[16], c16[16], h8[8];
-          dense16_half(a16, h8, w + lx[2 * rr], w + lx[2 * rr] + 256, 0);
-#pragma unroll
-          for (int i = 0; i < 8; ++i) b16[i] = h8[i];
-          dense16_half(a16, h8, w + lx[2 * rr], w + lx[2 * rr] + 256, 1);
-#pragma unroll
-          for (int i = 0; i < 8; ++i) b16[8 + i] = h8[i];
-          dense16_half(b16, h8, w + lx[2 * rr + 1], w + lx[2 * rr + 1] + 256, 0);
-#pragma unroll
-          for (int i = 0; i < 8; ++i) c16[i] = h8[i];
-          dense16_half(b16, h8, w + lx[2 * rr + 1], w + lx[2 * rr + 1] + 256, 1);
-#pragma unroll
-          for (int i = 0; i < 8; ++i) c16[8 + i] = h8[i];
+          float h8[8], b16[16], c16[16];
+          dense16_half(a16, h8, w + lx[2 * rr], w + lx[2 * rr] + 256, ht);
+          join16(h8, b16, ht);
+          dense16_half(b16, h8, w + lx[2 * rr + 1], w + lx[2 * rr + 1] + 256, ht);
+          join16(h8, c16, ht);
 #pragma unroll
           for (int i = 0; i < 16; ++i) a16[i] = a16[i] + c16[i];
         }
@@ -1145,20 +1174,25 @@ __global__ void __launch_bounds__(kHeadThreads, 1) k_tc32_head(HeadArgs a) {
         else if (ch == 1) X[1] = xo;
         else X[2] = xo;
       }
+      __syncthreads();  // the next channel's input overwrites the tile
     }
-    if (half == 0 && valid) {
-      if (srp[1] == srp[0]) X[1] = X[0];
-      if (srp[2] == srp[0]) X[2] = X[0];
-      else if (srp[2] == srp[1]) X[2] = X[1];
-      float o[3] = {fmaxf(expf(X[0]) - 1.0f, 0.0f) * srp[0], fmaxf(expf(X[1]) - 1.0f, 0.0f) * srp[1],
-                    fmaxf(expf(X[2]) - 1.0f, 0.0f) * srp[2]};
+    // output of row rt by its first thread
+    const int rowt = tile * kHeadRows + rt;
+    if (ht == 0 && rowt < n) {
+      const float* axt = a.aux + (long long)rowt * a.ars;
+      const float srt[3] = {__ldg(axt + 2 * a.afs), __ldg(axt + 3 * a.afs), __ldg(axt + 4 * a.afs)};
+      if (srt[1] == srt[0]) X[1] = X[0];
+      if (srt[2] == srt[0]) X[2] = X[0];
+      else if (srt[2] == srt[1]) X[2] = X[1];
+      float o[3] = {fmaxf(expf(X[0]) - 1.0f, 0.0f) * srt[0], fmaxf(expf(X[1]) - 1.0f, 0.0f) * srt[1],
+                    fmaxf(expf(X[2]) - 1.0f, 0.0f) * srt[2]};
       if (a.pix) {
-        const int px = a.pix[row];
-        const float tr = a.trph[row];
+        const int px = a.pix[rowt];
+        const float tr = a.trph[rowt];
         F3 lc = a.light_color, scv = a.scatter;
         float* dst = a.out;
         if (a.job) {
-          const BatchOut& bo = a.bout[a.job[row]];
+          const BatchOut& bo = a.bout[a.job[rowt]];
           lc = bo.light_color;
           scv = bo.scatter;
           dst = bo.out;
@@ -1168,7 +1202,7 @@ __global__ void __launch_bounds__(kHeadThreads, 1) k_tc32_head(HeadArgs a) {
         dst[3 * (size_t)px + 2] = fmaxf(((o[2] + tr) * lc.z) * scv.z, 0.0f);
       } else {
 #pragma unroll
-        for (int c = 0; c < 3; ++c) a.out[3 * (size_t)row + c] = o[c];
+        for (int c = 0; c < 3; ++c) a.out[3 * (size_t)rowt + c] = o[c];
       }
     }
   }
