@@ -271,9 +271,49 @@ constexpr unsigned kTrOff[8] = {0u, 2097152u, 2359296u, 2392064u, 2396160u, 2396
 // Stencil points [I0, I1) at mip level MIP, offset `off` (sphere points), or
 // the light-direction points with per-point offsets (SPHERE = false). HW
 // samples through the texture units instead of the fp32 software filter.
+// Bilinear HG-table sample in sampler form SAMP.
+template <int SAMP>
+__device__ __forceinline__ float lut_sample(const Tables& t, float u, float v) {
+  if (SAMP == kSampTex) return tex2D<float>(t.lut_tex, u, v);
+  if (SAMP == kSampGather) return bilinear_clamp_g(t.lut_g, kLut, kLut, u, v);
+  return bilinear_clamp(t.lut, kLut, kLut, u, v);
+}
+
+// Per-point constants of the gather, the same for every pixel (kPtTable
+// floats): [0, 192) the first HG-table factor of each sphere point (it
+// depends only on the stencil point - the cone cosine dot(X, md) = s.x / |s|
+// in an orthonormal frame - and the segment's table row), [192, 384) the
+// table row v of every point (atan(radius / 2 off) / 60 degrees). Segment
+// [I0, I1) by the block's threads; SPHERE = false: light-direction points
+// with per-point offsets (1..8, 9.5.., 26.5.., 60.5..)/256
+// (core/vector.cu:367-398).
+constexpr int kPtTable = 384;
+template <int MIP, bool SPHERE, int SAMP, int I0, int I1>
+__device__ __forceinline__ void point_table_seg(const Tables& t, const float* __restrict__ stencil, float off,
+                                                float* tab) {
+  const float radius = (float)(1 << MIP) / 256.0f;
+  const float kAng = 3.1415926535f * 60.0f / 180.0f;
+  for (int i = I0 + (int)threadIdx.x; i < I1; i += (int)blockDim.x) {
+    if (SPHERE) {
+      const float vrow = atanf(0.5f * radius / off) / kAng;
+      const float sx = __ldg(stencil + 3 * i), sy = __ldg(stencil + 3 * i + 1), sz = __ldg(stencil + 3 * i + 2);
+      const float inv = rsqrtf(sx * sx + sy * sy + sz * sz);
+      const float c1 = sx * inv;
+      tab[i] = lut_sample<SAMP>(t, c1 * 0.5f + 0.5f, vrow);
+      tab[192 + i] = vrow;
+    } else {
+      const int j = i - I0;
+      const float o = (MIP == 0 ? (float)(j + 1) : MIP == 1 ? 8.5f + 1.0f + 2.0f * (float)j
+                                 : MIP == 2 ? 26.5f + 4.0f * (float)j : 60.5f + 8.0f * (float)j) / 256.0f;
+      tab[i] = 0.0f;
+      tab[192 + i] = atanf(0.5f * radius / o) / kAng;
+    }
+  }
+}
+
 template <int MIP, bool SPHERE, int SAMP, int I0, int I1, class Sink>
 __device__ __forceinline__ void gather_seg(const Tables& t, const float* __restrict__ stencil, const PixelGather& q,
-                                           float off, Sink& sink) {
+                                           float off, const float* h0s, Sink& sink) {
   constexpr int R = 256 >> MIP;
   constexpr int TL = MIP > 0 ? MIP - 1 : 0;
   constexpr int RT = 128 >> TL;
@@ -281,7 +321,7 @@ __device__ __forceinline__ void gather_seg(const Tables& t, const float* __restr
   const float* tb = t.tr + kTrOff[TL];
   const float radius = (float)(1 << MIP) / 256.0f;
   const float kAng = 3.1415926535f * 60.0f / 180.0f;
-  float vrow = atanf(0.5f * radius / off) / kAng;
+  float vrow = h0s ? h0s[192 + I0] : atanf(0.5f * radius / off) / kAng;
   static_assert(I0 % 4 == 0 && I1 % 4 == 0, "segments are whole 4-feature chunks");
 #pragma unroll 1
   for (int i0 = I0; i0 < I1; i0 += 4)
@@ -302,7 +342,7 @@ __device__ __forceinline__ void gather_seg(const Tables& t, const float* __restr
       const int j = i - I0;
       off = (MIP == 0 ? (float)(j + 1) : MIP == 1 ? 8.5f + 1.0f + 2.0f * (float)j
                                        : MIP == 2 ? 26.5f + 4.0f * (float)j : 60.5f + 8.0f * (float)j) / 256.0f;
-      vrow = atanf(0.5f * radius / off) / kAng;
+      vrow = h0s ? h0s[192 + i] : atanf(0.5f * radius / off) / kAng;
       p = q.pos + q.L * off;
       c1 = q.cXL;
       c2 = q.cLXL;
@@ -316,17 +356,8 @@ __device__ __forceinline__ void gather_seg(const Tables& t, const float* __restr
       xh = q.hg0;
     } else {
       const float u1 = c1 * 0.5f + 0.5f, u2 = c2 * 0.5f + 0.5f;
-      float h0, h1;
-      if (SAMP == kSampTex) {
-        h0 = tex2D<float>(t.lut_tex, u1, vrow);
-        h1 = tex2D<float>(t.lut_tex, u2, vrow);
-      } else if (SAMP == kSampGather) {
-        h0 = bilinear_clamp_g(t.lut_g, kLut, kLut, u1, vrow);
-        h1 = bilinear_clamp_g(t.lut_g, kLut, kLut, u2, vrow);
-      } else {
-        h0 = bilinear_clamp(t.lut, kLut, kLut, u1, vrow);
-        h1 = bilinear_clamp(t.lut, kLut, kLut, u2, vrow);
-      }
+      const float h0 = SPHERE && h0s ? h0s[i] : lut_sample<SAMP>(t, u1, vrow);
+      const float h1 = lut_sample<SAMP>(t, u2, vrow);
       xh = __logf(h0 * h1 + 1.0f);
     }
     F3 pt = p;
@@ -345,9 +376,36 @@ __device__ __forceinline__ void gather_seg(const Tables& t, const float* __restr
   }
 }
 
+// The per-point table (see point_table_seg), with the segment offsets of
+// gather_fast.
+template <int SAMP>
+__device__ __forceinline__ void point_table(const Tables& t, const float* __restrict__ stencil, float* tab) {
+  const float ms = 0.6f;
+  point_table_seg<0, true, SAMP, 0, 8>(t, stencil, 1.0f / 256.0f * lerpf(ms, 1.0f, 1.0f), tab);
+  point_table_seg<1, true, SAMP, 8, 16>(t, stencil, 2.5f / 256.0f * lerpf(ms, 1.0f, 0.8f), tab);
+  point_table_seg<2, true, SAMP, 16, 32>(t, stencil, 5.5f / 256.0f * lerpf(ms, 1.0f, 0.6f), tab);
+  point_table_seg<3, true, SAMP, 32, 48>(t, stencil, 11.5f / 256.0f * lerpf(ms, 1.0f, 0.4f), tab);
+  point_table_seg<4, true, SAMP, 48, 64>(t, stencil, 23.5f / 256.0f * lerpf(ms, 1.0f, 0.2f), tab);
+  point_table_seg<5, true, SAMP, 64, 96>(t, stencil, 47.5f / 256.0f * ms, tab);
+  point_table_seg<6, true, SAMP, 96, 128>(t, stencil, 95.5f / 256.0f * ms, tab);
+  point_table_seg<7, true, SAMP, 128, 160>(t, stencil, 191.5f / 256.0f * ms, tab);
+  point_table_seg<0, false, SAMP, 160, 168>(t, stencil, 1.0f, tab);
+  point_table_seg<1, false, SAMP, 168, 176>(t, stencil, 1.0f, tab);
+  point_table_seg<2, false, SAMP, 176, 184>(t, stencil, 1.0f, tab);
+  point_table_seg<3, false, SAMP, 184, 192>(t, stencil, 1.0f, tab);
+}
+
+// The table, once per render (one block), into h0s[kPtTable].
+template <int SAMP>
+__global__ void k_sphere_h0(Tables t, const float* __restrict__ stencil, float* __restrict__ h0s) {
+  point_table<SAMP>(t, stencil, h0s);
+}
+
+// h0s: the per-point table (k_sphere_h0), or null to compute its entries per
+// point.
 template <int SAMP, class Sink>
 __device__ __forceinline__ void gather_fast(const Tables& t, const float* __restrict__ stencil, F3 pos, F3 L,
-                                            const Frame& f, float alpha, float g, Sink sink) {
+                                            const Frame& f, float alpha, float g, const float* h0s, Sink sink) {
   PixelGather q;
   q.pos = pos; q.L = L; q.X = f.X; q.Y = f.Y; q.Z = f.Z; q.LX = f.LX;
   q.lx = dot(f.LX, f.X); q.ly = dot(f.LX, f.Y); q.lz = dot(f.LX, f.Z);
@@ -356,18 +414,18 @@ __device__ __forceinline__ void gather_fast(const Tables& t, const float* __rest
   q.alpha = alpha;
   q.hg0 = __logf(hg_phase(dot(f.X, L), g) + 1.0f);
   const float ms = 0.6f;
-  gather_seg<0, true, SAMP, 0, 8>(t, stencil, q, 1.0f / 256.0f * lerpf(ms, 1.0f, 1.0f), sink);
-  gather_seg<1, true, SAMP, 8, 16>(t, stencil, q, 2.5f / 256.0f * lerpf(ms, 1.0f, 0.8f), sink);
-  gather_seg<2, true, SAMP, 16, 32>(t, stencil, q, 5.5f / 256.0f * lerpf(ms, 1.0f, 0.6f), sink);
-  gather_seg<3, true, SAMP, 32, 48>(t, stencil, q, 11.5f / 256.0f * lerpf(ms, 1.0f, 0.4f), sink);
-  gather_seg<4, true, SAMP, 48, 64>(t, stencil, q, 23.5f / 256.0f * lerpf(ms, 1.0f, 0.2f), sink);
-  gather_seg<5, true, SAMP, 64, 96>(t, stencil, q, 47.5f / 256.0f * ms, sink);
-  gather_seg<6, true, SAMP, 96, 128>(t, stencil, q, 95.5f / 256.0f * ms, sink);
-  gather_seg<7, true, SAMP, 128, 160>(t, stencil, q, 191.5f / 256.0f * ms, sink);
-  gather_seg<0, false, SAMP, 160, 168>(t, stencil, q, 1.0f, sink);
-  gather_seg<1, false, SAMP, 168, 176>(t, stencil, q, 1.0f, sink);
-  gather_seg<2, false, SAMP, 176, 184>(t, stencil, q, 1.0f, sink);
-  gather_seg<3, false, SAMP, 184, 192>(t, stencil, q, 1.0f, sink);
+  gather_seg<0, true, SAMP, 0, 8>(t, stencil, q, 1.0f / 256.0f * lerpf(ms, 1.0f, 1.0f), h0s, sink);
+  gather_seg<1, true, SAMP, 8, 16>(t, stencil, q, 2.5f / 256.0f * lerpf(ms, 1.0f, 0.8f), h0s, sink);
+  gather_seg<2, true, SAMP, 16, 32>(t, stencil, q, 5.5f / 256.0f * lerpf(ms, 1.0f, 0.6f), h0s, sink);
+  gather_seg<3, true, SAMP, 32, 48>(t, stencil, q, 11.5f / 256.0f * lerpf(ms, 1.0f, 0.4f), h0s, sink);
+  gather_seg<4, true, SAMP, 48, 64>(t, stencil, q, 23.5f / 256.0f * lerpf(ms, 1.0f, 0.2f), h0s, sink);
+  gather_seg<5, true, SAMP, 64, 96>(t, stencil, q, 47.5f / 256.0f * ms, h0s, sink);
+  gather_seg<6, true, SAMP, 96, 128>(t, stencil, q, 95.5f / 256.0f * ms, h0s, sink);
+  gather_seg<7, true, SAMP, 128, 160>(t, stencil, q, 191.5f / 256.0f * ms, h0s, sink);
+  gather_seg<0, false, SAMP, 160, 168>(t, stencil, q, 1.0f, h0s, sink);
+  gather_seg<1, false, SAMP, 168, 176>(t, stencil, q, 1.0f, h0s, sink);
+  gather_seg<2, false, SAMP, 176, 184>(t, stencil, q, 1.0f, h0s, sink);
+  gather_seg<3, false, SAMP, 184, 192>(t, stencil, q, 1.0f, h0s, sink);
 }
 
 // Gather only, for explicit points and frames (test / training entry).
@@ -383,7 +441,7 @@ __global__ void k_gather(Tables t, const float* __restrict__ stencil, const floa
     d[192 + i] = xs;
     d[384 + i] = xh;
   };
-  gather_fast<kSampLoad>(t, stencil, f3(pos[3 * k], pos[3 * k + 1], pos[3 * k + 2]), L, f, alpha, g, sink);
+  gather_fast<kSampLoad>(t, stencil, f3(pos[3 * k], pos[3 * k + 1], pos[3 * k + 2]), L, f, alpha, g, nullptr, sink);
   float* ax = aux + 5 * (size_t)k;
   ax[0] = g;
   ax[1] = acosf(dot(f.X, f.LX));
@@ -397,9 +455,9 @@ __global__ void k_gather(Tables t, const float* __restrict__ stencil, const floa
 // The texture forms are bound by fetch latency: registers capped for six
 // 128-thread blocks per SM.
 template <int SAMP>
-__global__ void __launch_bounds__(128, SAMP == kSampLoad ? 1 : 6) k_gather_fm(Tables t, const float* __restrict__ stencil, Records rec,
-                                                   int cap, F3 L, float alpha, float g, F3 srp,
-                                                   float* __restrict__ desc, float* __restrict__ aux) {
+__global__ void __launch_bounds__(128, SAMP == kSampLoad ? 1 : 6)
+    k_gather_fm(Tables t, const float* __restrict__ stencil, const float* __restrict__ h0s, Records rec, int cap, F3 L,
+                float alpha, float g, F3 srp, float* __restrict__ desc, float* __restrict__ aux) {
   unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned n = min(*rec.count, (unsigned)cap);
   if (k >= n) return;
@@ -420,7 +478,7 @@ __global__ void __launch_bounds__(128, SAMP == kSampLoad ? 1 : 6) k_gather_fm(Ta
       d[(96 + (i >> 2)) * c] = bh;
     }
   };
-  gather_fast<SAMP>(t, stencil, pos, L, f, alpha, g, sink);
+  gather_fast<SAMP>(t, stencil, pos, L, f, alpha, g, h0s, sink);
   aux[k] = g;
   aux[c + k] = acosf(dot(f.X, f.LX));
   aux[2 * c + k] = srp.x;
@@ -446,10 +504,12 @@ constexpr size_t records_bytes(size_t n) { return n * (sizeof(int) + 16 * sizeof
 constexpr size_t records_round(size_t n) { return (records_bytes(n) + 255) / 256 * 256; }
 // Scratch of one neural render of n pixels: records, then 576 feature-major
 // descriptor columns and 5 aux columns, then (when the albedo channels
-// differ) 120 spill columns of the tensor-core network's head input.
-constexpr size_t neural_scratch_bytes(size_t n, bool spill) {
-  return records_round(n) + n * (576 + 5 + (spill ? 120 : 0)) * sizeof(float) + 256;
+// differ) 120 spill columns of the tensor-core network's head input, then the
+// per-point table (k_sphere_h0, kPtTable floats).
+constexpr size_t h0_offset(size_t n, bool spill) {
+  return (records_round(n) + n * (576 + 5 + (spill ? 120 : 0)) * sizeof(float) + 255) / 256 * 256;
 }
+constexpr size_t neural_scratch_bytes(size_t n, bool spill) { return h0_offset(n, spill) + 2048; }
 static bool distinct_channels(const mr_render_params* p) {
   return p->scatter_rate.x != p->scatter_rate.y || p->scatter_rate.x != p->scatter_rate.z;
 }
@@ -569,16 +629,21 @@ static int neural_passes(Volume* v, const Network* net, const mr_render_params* 
   rc = fill_tables(v, samp, &tabs, s);
   if (rc) return rc;
   mark(ST_NN_PREDICT);
+  float* h0s = (float*)((char*)base + h0_offset(npx, distinct_channels(p)));
   const unsigned ggrid = (unsigned)((npx + 127) / 128);
-  if (samp == kSampTex)
-    k_gather_fm<kSampTex><<<ggrid, 128, 0, s>>>(tabs, net->stencil, rec, (int)npx, L, p->alpha, p->g, srp_of(sr),
-                                               desc, aux);
-  else if (samp == kSampGather)
-    k_gather_fm<kSampGather><<<ggrid, 128, 0, s>>>(tabs, net->stencil, rec, (int)npx, L, p->alpha, p->g, srp_of(sr),
-                                                  desc, aux);
-  else
-    k_gather_fm<kSampLoad><<<ggrid, 128, 0, s>>>(tabs, net->stencil, rec, (int)npx, L, p->alpha, p->g, srp_of(sr),
-                                                desc, aux);
+  if (samp == kSampTex) {
+    k_sphere_h0<kSampTex><<<1, 192, 0, s>>>(tabs, net->stencil, h0s);
+    k_gather_fm<kSampTex><<<ggrid, 128, 0, s>>>(tabs, net->stencil, h0s, rec, (int)npx, L, p->alpha, p->g,
+                                               srp_of(sr), desc, aux);
+  } else if (samp == kSampGather) {
+    k_sphere_h0<kSampGather><<<1, 192, 0, s>>>(tabs, net->stencil, h0s);
+    k_gather_fm<kSampGather><<<ggrid, 128, 0, s>>>(tabs, net->stencil, h0s, rec, (int)npx, L, p->alpha, p->g,
+                                                  srp_of(sr), desc, aux);
+  } else {
+    k_sphere_h0<kSampLoad><<<1, 192, 0, s>>>(tabs, net->stencil, h0s);
+    k_gather_fm<kSampLoad><<<ggrid, 128, 0, s>>>(tabs, net->stencil, h0s, rec, (int)npx, L, p->alpha, p->g,
+                                                srp_of(sr), desc, aux);
+  }
   mark(ST_NN_PREDICT);
   MR_CUDA(cudaGetLastError());
   const long long cap = (long long)npx;
@@ -840,7 +905,7 @@ __global__ void __launch_bounds__(256, 3) k_gather_batch(const BatchJob* __restr
       d[(96 + (i >> 2)) * c] = bh;
     }
   };
-  gather_fast<SAMP>(j.tabs, stencil, pos, j.sc.L, f, j.sc.alpha, j.sc.g, sink);
+  gather_fast<SAMP>(j.tabs, stencil, pos, j.sc.L, f, j.sc.alpha, j.sc.g, nullptr, sink);
   aux[k] = j.sc.g;
   aux[c + k] = acosf(dot(f.X, f.LX));
   aux[2 * c + k] = j.srp.x;
