@@ -1,26 +1,25 @@
-// FP32 radiance-predictor network on the CUDA cores, in two kernels
-// (core/radiancePredict.cu:370-485 in fp32).
+// FP32 radiance-predictor network (core/radiancePredict.cu:370-485 in fp32),
+// in two kernels over tiles of 128 rows.
 //
 // Descriptors are read in chunks of 4 features: (row k, features 4j..4j+3) is
 // the float4 at desc[k*rs + j*cs]; the render path passes chunk-of-4
 // feature-major columns (rs = 4, cs = 4*capacity) so that a warp's 32 loads
 // of one chunk are one coalesced transaction.
 //
-// Both kernels work on tiles of 128 rows whose activations live in shared
-// memory, column-major (feature f of tile row r at [f*128 + r]):
-//  * k_simt_trunk: the two trunks. The squeeze-excitation statistics and
-//    gates, the width-8 blocks and LD41 run per row (one thread per row);
-//    the width-16 and width-32 layers (77 % of the trunk's multiply-adds) run
-//    as register-tiled block GEMMs over the tile, with their weights
-//    pre-transposed and double-buffered in shared memory by cp.async.
-//  * k_simt_head: the head (LC0 128x128, LC1, LC2: 62 % of all multiply-adds)
-//    as block GEMMs, then LX and the residual pairs per row.
-// Every dot product starts at the bias and adds the inputs in ascending
-// order, as LinearReLU does.
-#include <vector>
-
+//  * k_simt_trunk (CUDA cores): the two trunks over a shared-memory tile,
+//    column-major (feature f of tile row r at [f*128 + r]). The
+//    squeeze-excitation statistics and gates, the width-8 blocks and LD41 run
+//    per row (one thread per row); the width-16 and width-32 layers (77 % of
+//    the trunk's multiply-adds) run as register-tiled block GEMMs over the
+//    tile, starting at the bias and adding the inputs in ascending order as
+//    LinearReLU does, with their weights pre-transposed and double-buffered
+//    in shared memory by cp.async.
+//  * k_tc32_head (tensor cores): the head. LC0 / LC1 / LC2 (62 % of all
+//    multiply-adds) as tcgen05 MMAs whose every product is the sum of three
+//    TF32 products (fp32-accurate); gates, LX and the residual pairs per row.
 #include <algorithm>
 #include <cstring>
+#include <vector>
 
 #include "mr_internal.h"
 #include "mr_net_layout.cuh"
@@ -40,10 +39,8 @@ __device__ __forceinline__ void cp_async16(float* dst, const float* src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 
 // ---- weight image of the fp32 kernels -------------------------------------------------
-// [head: LC0 | LC1 | LC2, each transposed to [in][out]]
 // [trunk stages 0..6: blocks 2..7 of the main trunk and L81; per stage the
 //  three branches' [in][out] weights, each followed by its bias]
-constexpr int kHeadImage = 128 * 128 + 128 * 64 + 64 * 32;
 constexpr int kTrunkStages = 7;
 __host__ __device__ constexpr int stage_width(int g) { return g < 3 ? 16 : 32; }
 __host__ __device__ constexpr int stage_floats(int g) { return 3 * (stage_width(g) * stage_width(g) + stage_width(g)); }
@@ -57,7 +54,7 @@ static_assert(stage_offset(1) == stage_floats(0) && stage_offset(4) == stage_off
 // [head per-row weights: LSEFin2 6x16, LSEFin1's albedo column (16), LGGS W
 //  8x3 + B 8, LX12 W 16 + B 1, padded to kHeadRowFloats]
 constexpr int kSeBlocks = 12, kSeFloats = 96 + 64 + 24;
-constexpr int kSeOff = kHeadImage + stage_offset(kTrunkStages);
+constexpr int kSeOff = stage_offset(kTrunkStages);
 constexpr int kHeadRowOff = kSeOff + kSeBlocks * kSeFloats;
 constexpr int kHeadRowFloats = 96 + 16 + 32 + 20;
 // [tensor-core head: LC0 / LC1 / LC2 as chunks of 32 input columns, each
@@ -95,9 +92,6 @@ void simt_weight_image(const float* w, std::vector<float>& img) {
     for (int k = 0; k < K; ++k)
       for (int c = 0; c < N; ++c) img[o + (size_t)k * N + c] = W[(size_t)c * K + k];
   };
-  put_t(0, MR_W_LC0W, 128, 128);
-  put_t(128 * 128, MR_W_LC1W, 64, 128);
-  put_t(128 * 128 + 128 * 64, MR_W_LC2W, 32, 64);
   const int ids[kTrunkStages][3][2] = {
       {{MR_W_L21W, MR_W_L21B}, {MR_W_L_Tr21W, MR_W_L_Tr21B}, {MR_W_L_Hg21W, MR_W_L_Hg21B}},
       {{MR_W_L31W, MR_W_L31B}, {MR_W_L_Tr31W, MR_W_L_Tr31B}, {MR_W_L_Hg31W, MR_W_L_Hg31B}},
@@ -108,7 +102,7 @@ void simt_weight_image(const float* w, std::vector<float>& img) {
       {{MR_W_L81W, MR_W_L81B}, {MR_W_L_Tr81W, MR_W_L_Tr81B}, {MR_W_L_Hg81W, MR_W_L_Hg81B}}};
   for (int g = 0; g < kTrunkStages; ++g) {
     const int S = stage_width(g);
-    size_t o = kHeadImage + stage_offset(g);
+    size_t o = stage_offset(g);
     for (int b = 0; b < 3; ++b) {
       put_t(o, ids[g][b][0], S, S);
       for (int c = 0; c < S; ++c) img[o + S * S + c] = w[wt.off[ids[g][b][1]] + c];
@@ -362,7 +356,7 @@ __device__ __forceinline__ void row_gate_input(const RowIO& in, const float* __r
 // empty past the last stage).
 __device__ __forceinline__ void trunk_stage_issue(const float* __restrict__ img, float* ring, int g) {
   if (g < kTrunkStages) {
-    const float* src = img + kHeadImage + stage_offset(g);
+    const float* src = img + stage_offset(g);
     float* dst = ring + (g & 1) * stage_floats(kTrunkStages - 1);
     const int pieces = stage_floats(g) / 4;
     for (int i = threadIdx.x; i < pieces; i += kTile) cp_async16(dst + 4 * i, src + 4 * i);
@@ -539,18 +533,13 @@ __global__ void __launch_bounds__(kTile, 3) k_simt_trunk(TrunkArgs a, TrunkOut t
   for (int j0 = 0; j0 < 16; j0 += 4) put4(30 + j0 / 4, fin[j0], fin[j0 + 1], fin[j0 + 2], fin[j0 + 3]);
 }
 
-// ---- head: block GEMMs over shared-memory activation tiles ---------------------------
+// ---- head --------------------------------------------------------------------------
 
-constexpr int kHeadRows = kTile;   // rows (pixels) per block
-constexpr int kHeadThreads = 256;  // two threads per row in the per-row stages
-constexpr int kChunk = 2048;       // floats per weight chunk (8 KB)
-constexpr int kHeadChunks = 13;    // LC0 8, LC1 4, LC2 1 chunks
-constexpr int kStages = 3;         // weight chunks in flight
-constexpr int kHeadSmem = (2 * 128 * kHeadRows + kStages * kChunk) * (int)sizeof(float);  // Xt, Yt, ring
-
+constexpr int kHeadRows = kTile;   // rows (pixels) per tile
+constexpr int kHeadThreads = 256;  // two threads per row
 struct HeadArgs {
   const float* __restrict__ w;
-  const float* __restrict__ wt;  // LC0 / LC1 / LC2 transposed, [in][out], concatenated
+  const float* __restrict__ wt;  // simt_weight_image
   const float* __restrict__ t;   // trunk outputs (TrunkOut layout)
   long long trs, tcs;
   const float* __restrict__ aux;
@@ -565,88 +554,6 @@ struct HeadArgs {
   const BatchOut* bout;
   int* err;  // tensor-core head: set when a bounded wait gave up
 };
-
-// The head weights (LC0, LC1, LC2 transposed; 13 chunks of 8 KB, repeated
-// per albedo channel) stream through a ring of kStages shared-memory buffers
-// with cp.async: chunk c + kStages - 1 is in flight while chunk c is used.
-struct WStream {
-  const float* __restrict__ src;
-  float* ring;
-  int issued, total;
-  __device__ __forceinline__ void issue() {
-    if (issued < total) {
-      const float* s = src + (issued % kHeadChunks) * kChunk + threadIdx.x * 8;
-      float* d = ring + (issued % kStages) * kChunk + threadIdx.x * 8;
-      cp_async16(d, s);
-      cp_async16(d + 4, s + 4);
-    }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-    ++issued;
-  }
-  // Buffer of chunk c (chunks are acquired in order by all threads); the
-  // barrier also orders the block's shared-memory writes before it.
-  __device__ __forceinline__ const float* acquire(int c) {
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(kStages - 2) : "memory");
-    __syncthreads();
-    issue();
-    return ring + (c % kStages) * kChunk;
-  }
-};
-
-// Yt[c][r] = ReLU(B[c] + sum_k Xt[k][r] W[c][k]) for the block's 128 rows (Xt
-// and Yt column-major: element (row r, feature k) at [k*128 + r]); the weights
-// arrive as chunks of 2048 / N rows of the transposed [K][N] layer. Thread t
-// owns rows {4g..4g+3, 64+4g..64+4g+3} (g = t % 16) and N / 16 consecutive
-// columns (group t / 16); the sum starts at the bias and runs over k in
-// ascending order, as LinearReLU does. The eight threads of a quarter warp
-// read and write 128 contiguous bytes of Xt / Yt, and a warp's weight loads
-// touch two addresses (broadcast).
-template <int K, int N>
-__device__ __forceinline__ void block_gemm(const float* __restrict__ Xt, float* __restrict__ Yt,
-                                           const float* __restrict__ B, WStream& ws, int& chunk) {
-  constexpr int TCOL = N / 16;
-  constexpr int KC = kChunk / N;
-  const int t = threadIdx.x, r0 = 4 * (t & 15), c0 = (t >> 4) * TCOL;
-  float acc[8][TCOL];
-#pragma unroll
-  for (int j = 0; j < TCOL; ++j) {
-    const float b = __ldg(B + c0 + j);
-#pragma unroll
-    for (int i = 0; i < 8; ++i) acc[i][j] = b;
-  }
-#pragma unroll 1
-  for (int kc = 0; kc < K; kc += KC) {
-    const float* __restrict__ W = ws.acquire(chunk++);
-#pragma unroll 4
-    for (int k = 0; k < KC; ++k) {
-      const float4 xa = *reinterpret_cast<const float4*>(Xt + (kc + k) * kHeadRows + r0);
-      const float4 xb = *reinterpret_cast<const float4*>(Xt + (kc + k) * kHeadRows + 64 + r0);
-      const float xv[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
-      float wv[TCOL];
-      if constexpr (TCOL >= 4) {
-#pragma unroll
-        for (int j = 0; j < TCOL; j += 4) {
-          const float4 q = *reinterpret_cast<const float4*>(W + k * N + c0 + j);
-          wv[j] = q.x; wv[j + 1] = q.y; wv[j + 2] = q.z; wv[j + 3] = q.w;
-        }
-      } else {
-        const float2 q = *reinterpret_cast<const float2*>(W + k * N + c0);
-        wv[0] = q.x; wv[1] = q.y;
-      }
-#pragma unroll
-      for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < TCOL; ++j) acc[i][j] = fmaf(xv[i], wv[j], acc[i][j]);
-    }
-  }
-#pragma unroll
-  for (int j = 0; j < TCOL; ++j) {
-    float* dst = Yt + (c0 + j) * kHeadRows + r0;
-    *reinterpret_cast<float4*>(dst) = make_float4(relu0(acc[0][j]), relu0(acc[1][j]), relu0(acc[2][j]), relu0(acc[3][j]));
-    *reinterpret_cast<float4*>(dst + 64) =
-        make_float4(relu0(acc[4][j]), relu0(acc[5][j]), relu0(acc[6][j]), relu0(acc[7][j]));
-  }
-}
 
 // Half of a 16 -> 16 layer: outputs 8h..8h+7 of ReLU(B + W x), bias first,
 // ascending inputs.
@@ -674,178 +581,6 @@ __device__ __forceinline__ void join16(const float (&mine)[8], float (&full)[16]
     const float other = __shfl_xor_sync(0xffffffffu, mine[q], 16);
     full[q] = h ? other : mine[q];
     full[8 + q] = h ? mine[q] : other;
-  }
-}
-
-// Head SC(p) (radiancePredict.cu:439-473) per distinct albedo channel for a
-// block of 128 rows. The gated 128-wide input is built per row into Xt (two
-// threads per row, half the features each); LC0 / LC1 / LC2 run as block
-// GEMMs; LX and the residual pairs run per row with the row's two threads in
-// one warp (lanes l and l ^ 16), each computing half the outputs of every
-// layer and exchanging them by shuffle.
-__global__ void __launch_bounds__(kHeadThreads, 1) k_simt_head(HeadArgs a) {
-  extern __shared__ __align__(16) float hsm[];
-  float* Xt = hsm;
-  float* Yt = hsm + 128 * kHeadRows;
-  const int n = a.count ? (int)min(*a.count, (unsigned)a.n) : a.n;
-  const int row0 = blockIdx.x * kHeadRows;
-  if (row0 >= n) return;  // block-uniform
-  // input mapping: row r, feature half `half`
-  const int r = threadIdx.x & (kHeadRows - 1), half = threadIdx.x >> 7, row = row0 + r;
-  const bool valid = row < n;
-  const int kr = valid ? row : n - 1;
-  // tail mapping: row rt, output half ht
-  const int lane = threadIdx.x & 31, rt = (threadIdx.x >> 5) * 16 + (lane & 15), ht = lane >> 4;
-  const float* __restrict__ w = a.w;
-  const float* __restrict__ hr = a.wt + kHeadRowOff;
-  const float* trow = a.t + (long long)kr * a.trs;
-  const float* ax = a.aux + (long long)kr * a.ars;
-  const float g = __ldg(ax), gamma = __ldg(ax + a.afs);
-  const float srp[3] = {__ldg(ax + 2 * a.afs), __ldg(ax + 3 * a.afs), __ldg(ax + 4 * a.afs)};
-  float fin[16];
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    const float4 q = __ldg(reinterpret_cast<const float4*>(trow + (30 + c) * a.tcs));
-    fin[4 * c] = q.x; fin[4 * c + 1] = q.y; fin[4 * c + 2] = q.z; fin[4 * c + 3] = q.w;
-  }
-  const bool need1 = __syncthreads_or(valid && srp[1] != srp[0]);
-  const bool need2 = __syncthreads_or(valid && srp[2] != srp[0] && srp[2] != srp[1]);
-  WStream ws{a.wt, hsm + 2 * 128 * kHeadRows, 0, kHeadChunks * (1 + (int)need1 + (int)need2)};
-#pragma unroll
-  for (int i = 0; i < kStages - 1; ++i) ws.issue();
-  int chunk = 0;
-  float X[3] = {0.0f, 0.0f, 0.0f};  // of row rt
-#pragma unroll 1
-  for (int ch = 0; ch < 3; ++ch) {
-    if ((ch == 1 && !need1) || (ch == 2 && !need2)) continue;
-    const float sc = ch == 0 ? srp[0] : ch == 1 ? srp[1] : srp[2];
-    // gates of this channel (LGGS, LSEFin1's albedo column, LSEFin2)
-    float sep[6];
-    {
-      float sew[16];
-#pragma unroll
-      for (int j = 0; j < 16; j += 4) {
-        const float4 f = ldg4(hr + 96 + j);
-        sew[j] = relu0(fin[j] + sc * f.x);
-        sew[j + 1] = relu0(fin[j + 1] + sc * f.y);
-        sew[j + 2] = relu0(fin[j + 2] + sc * f.z);
-        sew[j + 3] = relu0(fin[j + 3] + sc * f.w);
-      }
-#pragma unroll
-      for (int i = 0; i < 6; ++i) {
-        float acc = 0.0f;
-#pragma unroll
-        for (int j = 0; j < 16; j += 4) {
-          const float4 f = ldg4(hr + i * 16 + j);
-          acc += sew[j] * f.x;
-          acc += sew[j + 1] * f.y;
-          acc += sew[j + 2] * f.z;
-          acc += sew[j + 3] * f.w;
-        }
-        sep[i] = 1.0f / (1.0f + expf(-acc));
-      }
-    }
-    // gated head input, column-major in Xt: chunks 0..14 by the first thread
-    // of a row, 15..29 and LGGS by the second
-#pragma unroll 3
-    for (int c = 15 * half; c < 15 * half + 15; ++c) {
-      const float4 q = __ldg(reinterpret_cast<const float4*>(trow + c * a.tcs));
-      const float s = c < 24 ? sep[c >> 3] : sep[3 + ((c - 24) >> 1)];
-      Xt[(4 * c + 0) * kHeadRows + r] = q.x * s;
-      Xt[(4 * c + 1) * kHeadRows + r] = q.y * s;
-      Xt[(4 * c + 2) * kHeadRows + r] = q.z * s;
-      Xt[(4 * c + 3) * kHeadRows + r] = q.w * s;
-    }
-    if (half) {
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {  // LGGS 3 -> 8, bias after the sum
-        float acc = g * __ldg(hr + 112 + 3 * i) + gamma * __ldg(hr + 112 + 3 * i + 1) + sc * __ldg(hr + 112 + 3 * i + 2);
-        acc += __ldg(hr + 136 + i);
-        Xt[(120 + i) * kHeadRows + r] = relu0(acc);
-      }
-    }
-    block_gemm<128, 128>(Xt, Yt, w + WOFF(LC0B), ws, chunk);
-    block_gemm<128, 64>(Yt, Xt, w + WOFF(LC1B), ws, chunk);
-    block_gemm<64, 32>(Xt, Yt, w + WOFF(LC2B), ws, chunk);
-    __syncthreads();
-    // LX 32 -> 16 and the residual pairs (:454-471), tail mapping
-    float a16[16];
-    {
-      float x32[32];
-#pragma unroll
-      for (int i = 0; i < 32; ++i) x32[i] = Yt[i * kHeadRows + rt];
-      float a8[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        float acc = __ldg(w + WOFF(LXB) + 8 * ht + q);
-#pragma unroll
-        for (int j = 0; j < 32; j += 4) {
-          const float4 v = ldg4(w + WOFF(LXW) + (8 * ht + q) * 32 + j);
-          acc += x32[j] * v.x;
-          acc += x32[j + 1] * v.y;
-          acc += x32[j + 2] * v.z;
-          acc += x32[j + 3] * v.w;
-        }
-        a8[q] = relu0(acc);
-      }
-      join16(a8, a16, ht);
-    }
-    const int lx[12] = {WOFF(LX0W), WOFF(LX1W), WOFF(LX2W), WOFF(LX3W), WOFF(LX4W), WOFF(LX5W),
-                        WOFF(LX6W), WOFF(LX7W), WOFF(LX8W), WOFF(LX9W), WOFF(LX10W), WOFF(LX11W)};
-#pragma unroll 1
-    for (int rr = 0; rr < 6; ++rr) {
-      float h8[8], b16[16], c16[16];
-      dense16_half(a16, h8, w + lx[2 * rr], w + lx[2 * rr] + 256, ht);
-      join16(h8, b16, ht);
-      dense16_half(b16, h8, w + lx[2 * rr + 1], w + lx[2 * rr + 1] + 256, ht);
-      join16(h8, c16, ht);
-#pragma unroll
-      for (int i = 0; i < 16; ++i) a16[i] = a16[i] + c16[i];
-    }
-    float o = 0.0f;  // LX12 16 -> 1, bias after the sum
-#pragma unroll
-    for (int i = 0; i < 16; i += 4) {
-      const float4 v = ldg4(hr + 144 + i);
-      o += a16[i] * v.x;
-      o += a16[i + 1] * v.y;
-      o += a16[i + 2] * v.z;
-      o += a16[i + 3] * v.w;
-    }
-    o += __ldg(hr + 160);
-    const float xo = relu0(o);
-    if (ch == 0) X[0] = xo;
-    else if (ch == 1) X[1] = xo;
-    else X[2] = xo;
-    // Xt and Yt are next written after the first barrier of the next channel
-  }
-  asm volatile("cp.async.wait_all;\n" ::: "memory");
-  // output of row rt by its first thread
-  const int rowt = row0 + rt;
-  if (ht || rowt >= n) return;
-  const float* axt = a.aux + (long long)rowt * a.ars;
-  const float st[3] = {__ldg(axt + 2 * a.afs), __ldg(axt + 3 * a.afs), __ldg(axt + 4 * a.afs)};
-  if (st[1] == st[0]) X[1] = X[0];
-  if (st[2] == st[0]) X[2] = X[0];
-  else if (st[2] == st[1]) X[2] = X[1];
-  float o[3] = {fmaxf(expf(X[0]) - 1.0f, 0.0f) * st[0], fmaxf(expf(X[1]) - 1.0f, 0.0f) * st[1],
-                fmaxf(expf(X[2]) - 1.0f, 0.0f) * st[2]};
-  if (a.pix) {
-    const int px = a.pix[rowt];
-    const float tr = a.trph[rowt];
-    F3 lc = a.light_color, sc = a.scatter;
-    float* dst = a.out;
-    if (a.job) {
-      const BatchOut& bo = a.bout[a.job[rowt]];
-      lc = bo.light_color;
-      sc = bo.scatter;
-      dst = bo.out;
-    }
-    dst[3 * (size_t)px + 0] = fmaxf(((o[0] + tr) * lc.x) * sc.x, 0.0f);
-    dst[3 * (size_t)px + 1] = fmaxf(((o[1] + tr) * lc.y) * sc.y, 0.0f);
-    dst[3 * (size_t)px + 2] = fmaxf(((o[2] + tr) * lc.z) * sc.z, 0.0f);
-  } else {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) a.out[3 * (size_t)rowt + c] = o[c];
   }
 }
 
@@ -1234,7 +969,6 @@ int launch_mlp_simt(const Network* net, const float* desc, const float* aux, lon
   if (!tout) return set_error(MR_ERR_ARG, "fp32 network: no buffer for the trunk outputs");
   static bool attr = false;
   if (!attr) {
-    MR_CUDA(cudaFuncSetAttribute(k_simt_head, cudaFuncAttributeMaxDynamicSharedMemorySize, kHeadSmem));
     MR_CUDA(cudaFuncSetAttribute(k_tc32_head, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcHeadSmem));
     MR_CUDA(cudaFuncSetAttribute(k_simt_trunk, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrunkSmem));
     attr = true;
