@@ -26,7 +26,7 @@ typedef enum {
   MR_OK = 0,
   MR_ERR_ARG = 1,         /* invalid argument (size, pointer, range) */
   MR_ERR_CUDA = 2,        /* a CUDA runtime call failed */
-  MR_ERR_TIMEOUT = 3,     /* mr_sync watchdog expired */
+  MR_ERR_TIMEOUT = 3,     /* mr_sync / mr_render_host_wait watchdog expired */
   MR_ERR_LOOP_CAP = 4,    /* a device loop hit its iteration cap and reported it */
   MR_ERR_STATE = 5,       /* call made in the wrong state (e.g. render before update) */
   MR_ERR_NOMEM = 6,       /* device allocation failed */
@@ -143,6 +143,19 @@ int mr_render(mr_volume* v, const mr_network* net, const mr_render_params* p, fl
               void* stream);
 /* Same, synchronous, into host memory (the reference returns vector<float3>). */
 int mr_render_host(mr_volume* v, const mr_network* net, const mr_render_params* p, float* host_rgb);
+/* Pipelined form of mr_render_host for a stream of frames (VolumeRender::Render,
+ * core/volume.cu:410-467, called once per frame): renders on `stream` into one
+ * of two device frames owned by the volume, used in turn, and copies the frame
+ * to host_rgb on a copy stream owned by the volume, so that the copy of one
+ * frame overlaps the render of the next. Returns once both are queued;
+ * *ticket (may be NULL) numbers the frame for mr_render_host_wait. host_rgb
+ * must stay valid until that wait; page-locked memory lets the copy overlap. */
+int mr_render_host_async(mr_volume* v, const mr_network* net, const mr_render_params* p, float* host_rgb,
+                         void* stream, int64_t* ticket);
+/* Blocks until frame `ticket` (and every frame issued before it) is in host
+ * memory; ticket < 0 waits for all frames. timeout_ms < 0 waits without limit;
+ * MR_ERR_TIMEOUT when the copy is still running after timeout_ms. */
+int mr_render_host_wait(mr_volume* v, int64_t ticket, int32_t timeout_ms);
 /* Delta tracking with FP64 accumulation: adds this call's per-pixel radiance
  * sums and sums of squares (width*height*3 doubles each, caller-zeroed) so
  * that many calls build a high-spp reference image. */

@@ -29,7 +29,8 @@ EXPORTS = [
     "mr_trainer_destroy", "mr_trainer_gradient", "mr_trainer_step", "mr_trainer_weights",
     "mr_render_interactive", "mr_denoise", "mr_batch_create", "mr_batch_destroy", "mr_batch_add", "mr_batch_prepare",
     "mr_batch_autotune", "mr_batch_render", "mr_batch_capture", "mr_batch_launch", "mr_batch_counters",
-    "mr_tc_selftest_fp8", "mr_sampler_selftest", "mr_tc_selftest_tf32",
+    "mr_tc_selftest_fp8", "mr_sampler_selftest", "mr_tc_selftest_tf32", "mr_render_host_async",
+    "mr_render_host_wait",
 ]
 NOALLOC_MAX_PIXELS = 16384
 
@@ -104,6 +105,8 @@ def load():
     L.mr_weights_xavier.argtypes = [u32, vp, sz]
     L.mr_render.argtypes = [vp, vp, C.POINTER(RenderParams), vp, vp]
     L.mr_render_host.argtypes = [vp, vp, C.POINTER(RenderParams), vp]
+    L.mr_render_host_async.argtypes = [vp, vp, C.POINTER(RenderParams), vp, vp, C.POINTER(C.c_int64)]
+    L.mr_render_host_wait.argtypes = [vp, C.c_int64, i32]
     L.mr_render_accumulate_f64.argtypes = [vp, C.POINTER(RenderParams), vp, vp, vp]
     L.mr_radiance_predict.argtypes = [vp, i32, vp, vp, i32, vp, vp]
     L.mr_gather_descriptors.argtypes = [vp, vp, vp, vp, i32, fp, fp, Float3, vp, vp, vp]

@@ -193,6 +193,70 @@ int mr_render_host(mr_volume* h, const mr_network* net, const mr_render_params* 
   return rc;
 }
 
+int mr_render_host_async(mr_volume* h, const mr_network* net, const mr_render_params* p, float* host_rgb,
+                         void* stream, int64_t* ticket) {
+  clear_error();
+  if (!h || !host_rgb) return set_error(MR_ERR_ARG, "mr_render_host_async: NULL argument");
+  int rc = check_params(p);
+  if (rc) return rc;
+  Volume* v = &h->v;
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t bytes = (size_t)p->width * p->height * 3 * sizeof(float);
+  if (!v->copy_stream) {
+    MR_CUDA(cudaStreamCreateWithFlags(&v->copy_stream, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; ++i) {
+      MR_CUDA(cudaEventCreateWithFlags(&v->rendered[i], cudaEventDisableTiming));
+      MR_CUDA(cudaEventCreateWithFlags(&v->copied[i], cudaEventDisableTiming));
+    }
+  }
+  if (v->frame_bytes < bytes) {
+    MR_CUDA(cudaStreamSynchronize(v->copy_stream));  // earlier copies still read the old frames
+    for (int i = 0; i < 2; ++i) {
+      if (v->frame[i]) MR_CUDA(cudaFree(v->frame[i]));
+      v->frame[i] = nullptr;
+    }
+    v->frame_bytes = 0;
+    for (int i = 0; i < 2; ++i) {
+      cudaError_t e = cudaMalloc(&v->frame[i], bytes);
+      if (e != cudaSuccess) return set_error(MR_ERR_NOMEM, "frame buffer of %zu bytes: %s", bytes, cudaGetErrorString(e));
+    }
+    v->frame_bytes = bytes;
+  }
+  const int slot = (int)(v->frame_seq & 1);
+  // the frame two calls back must be on the host before this render overwrites it
+  MR_CUDA(cudaStreamWaitEvent(s, v->copied[slot], 0));
+  rc = mr_render(h, net, p, v->frame[slot], stream);
+  if (rc) return rc;
+  MR_CUDA(cudaEventRecord(v->rendered[slot], s));
+  MR_CUDA(cudaStreamWaitEvent(v->copy_stream, v->rendered[slot], 0));
+  MR_CUDA(cudaMemcpyAsync(host_rgb, v->frame[slot], bytes, cudaMemcpyDeviceToHost, v->copy_stream));
+  MR_CUDA(cudaEventRecord(v->copied[slot], v->copy_stream));
+  if (ticket) *ticket = v->frame_seq;
+  ++v->frame_seq;
+  return MR_OK;
+}
+
+int mr_render_host_wait(mr_volume* h, int64_t ticket, int32_t timeout_ms) {
+  clear_error();
+  if (!h) return set_error(MR_ERR_ARG, "mr_render_host_wait: NULL argument");
+  Volume* v = &h->v;
+  if (ticket >= v->frame_seq) return set_error(MR_ERR_ARG, "frame %lld has not been issued", (long long)ticket);
+  if (!v->copy_stream || v->frame_seq == 0) return MR_OK;
+  // copies run in issue order on the copy stream: the last copy recorded for
+  // the ticket's frame buffer is that frame's or a later one
+  cudaEvent_t e = ticket < 0 ? v->copied[(v->frame_seq - 1) & 1] : v->copied[ticket & 1];
+  auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    cudaError_t q = cudaEventQuery(e);
+    if (q == cudaSuccess) return MR_OK;
+    if (q != cudaErrorNotReady) return cuda_error(q, "cudaEventQuery(frame copy)");
+    auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0).count();
+    if (timeout_ms >= 0 && ms > timeout_ms)
+      return set_error(MR_ERR_TIMEOUT, "frame copy still running after %d ms", timeout_ms);
+    std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+}
+
 int mr_sync(void* stream, int32_t timeout_ms) {
   clear_error();
   auto t0 = std::chrono::steady_clock::now();

@@ -75,6 +75,14 @@ struct Volume {
   // Interactive neural mode: radiance and first-hit distance of the frame.
   void* inter = nullptr;
   size_t inter_bytes = 0;
+  // Pipelined host delivery (mr_render_host_async): two device frames used in
+  // turn, a copy stream, and per frame the events "rendered" (on the caller's
+  // stream) and "copied" (on the copy stream).
+  float* frame[2] = {};
+  size_t frame_bytes = 0;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t rendered[2] = {}, copied[2] = {};
+  long long frame_seq = 0;  // frames issued so far; frame t uses frame[t % 2]
 };
 
 struct Network {

@@ -444,6 +444,20 @@ __device__ __forceinline__ void trunk_gemm(float* tile, const float* W, const fl
   }
 }
 
+// L2 prefetch of descriptor features [f0, f1) of the three branches for the
+// tile's rows, one bulk prefetch per 4-feature chunk (thread i issues chunk
+// i), when each chunk's rows are contiguous (chunk-of-4 feature-major
+// columns, rows 16 bytes apart).
+__device__ __forceinline__ void desc_prefetch(const TrunkArgs& a, int row0, int n, int f0, int f1) {
+  if (a.rs != 4) return;
+  const int per = (f1 - f0) / 4, i = threadIdx.x;
+  if (i >= 3 * per) return;
+  const int chunk = (i / per) * 48 + f0 / 4 + i % per;
+  const unsigned bytes = (unsigned)min(kTile, n - row0) * 16u;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a.desc + chunk * a.cs + row0 * 4), "r"(bytes)
+               : "memory");
+}
+
 constexpr int kTrunkSmem = (96 * kTile + 2 * 3 * (32 * 32 + 32)) * (int)sizeof(float);
 
 // Trunks of RadiancePredict (radiancePredict.cu:385-437) for a tile of 128
@@ -457,6 +471,7 @@ __global__ void __launch_bounds__(kTile, 3) k_simt_trunk(TrunkArgs a, TrunkOut t
   if (row0 >= n) return;  // block-uniform
   trunk_stage_issue(a.img, ring, 0);
   trunk_stage_issue(a.img, ring, 1);
+  desc_prefetch(a, row0, n, 0, 48);  // blocks 0..3; each stage prefetches the block two stages ahead
   const int r = threadIdx.x, row = row0 + r;
   const int kr = row < n ? row : n - 1;
   const float* __restrict__ w = a.w;
@@ -475,6 +490,10 @@ __global__ void __launch_bounds__(kTile, 3) k_simt_trunk(TrunkArgs a, TrunkOut t
   for (int st = 0; st < 6; ++st) {
     const int S = stage_width(st), from = st < 3 ? 16 + 16 * st : 64 + 32 * (st - 3);
     const float* sws = sw + (2 + st) * kSeFloats;
+    if (st < 4)
+      desc_prefetch(a, row0, n, st == 0 ? 48 : 32 * st + 32, st == 0 ? 64 : 32 * st + 64);
+    else if (st == 4)
+      desc_prefetch(a, row0, n, 160, 192);
     if (S == 16)
       row_gate_input<16>(in, sws, from, g, gamma, y, fin);
     else

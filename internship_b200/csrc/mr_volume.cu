@@ -441,6 +441,16 @@ int mr_volume_destroy(mr_volume* h) {
   cudaFree(v->d_counters);
   if (v->scratch) cudaFree(v->scratch);
   if (v->inter) cudaFree(v->inter);
+  if (v->copy_stream) {
+    cudaStreamSynchronize(v->copy_stream);  // host copies still reading the frames
+    for (int i = 0; i < 2; ++i) {
+      cudaEventDestroy(v->rendered[i]);
+      cudaEventDestroy(v->copied[i]);
+    }
+    cudaStreamDestroy(v->copy_stream);
+  }
+  for (int i = 0; i < 2; ++i)
+    if (v->frame[i]) cudaFree(v->frame[i]);
   destroy_textures(v);
   delete h;
   return MR_OK;

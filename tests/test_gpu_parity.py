@@ -226,6 +226,38 @@ def test_render_errors(mr):
     assert L.mr_volume_destroy(h) == 0
 
 
+def test_render_host_async_matches_sync(mr):
+    """mr_render_host_async delivers the same frames as mr_render_host, in
+    order, across a frame-size change and for both render types."""
+    from internship_b200 import _lib, scenes
+    L = _lib.load()
+    v = _volume(mr, scenes.sphere_density(128))
+    v.SetWeights(_test_weights(mr), mr.builtin_stencil())
+    net = v.network.handle
+    jobs = []
+    for k in range(5):
+        w, h = (40, 24) if k < 3 else (56, 40)  # grows the volume's frames at k = 3
+        p = scenes.make_params(w, h, 1 if k % 2 == 0 else 4, rt=_lib.RT_MRPNN if k % 2 == 0 else _lib.RT_PT)
+        p.sample_offset = 7 * k
+        jobs.append(p)
+    outs, tickets = [], []
+    for p in jobs:
+        out = np.full(p.width * p.height * 3, np.nan, np.float32)
+        t = C.c_int64(-5)
+        _lib.check(L.mr_render_host_async(v.handle, net, C.byref(p), out.ctypes.data, None, C.byref(t)))
+        outs.append(out)
+        tickets.append(t.value)
+    assert tickets == list(range(len(jobs)))
+    _lib.check(L.mr_render_host_wait(v.handle, 1, 10000))
+    _lib.check(L.mr_render_host_wait(v.handle, -1, 10000))
+    for p, out in zip(jobs, outs):
+        np.testing.assert_array_equal(out, _render(mr, v, p, net))
+    assert L.mr_render_host_wait(v.handle, len(jobs), 0) == _lib.MR_ERR_ARG
+    p = jobs[0]
+    assert L.mr_render_host_async(v.handle, net, C.byref(p), None, None, None) == _lib.MR_ERR_ARG
+    v.close()
+
+
 def test_sync_watchdog(mr):
     from internship_b200 import _lib
     assert _lib.load().mr_sync(None, 1000) == _lib.MR_OK
