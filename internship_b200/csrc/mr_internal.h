@@ -83,6 +83,10 @@ struct Volume {
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t rendered[2] = {}, copied[2] = {};
   long long frame_seq = 0;  // frames issued so far; frame t uses frame[t % 2]
+  // Side stream of a neural render (the per-point table beside the trace),
+  // forked from and joined back to the caller's stream by events.
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t side_fork = nullptr, side_join = nullptr;
 };
 
 struct Network {
@@ -93,6 +97,7 @@ struct Network {
   std::vector<float> h_rowwise;  // fp32 per-row weights passed as kernel parameters (mr_mlp_tc.cu)
   std::vector<float> h_winv8;    // inverse per-layer scales of the E4M3 weight image
   float* simt_img = nullptr;     // weight image of the fp32 network kernels (simt_weight_image)
+  std::vector<float> h_tail;     // LXW .. LX12B, kernel parameters of the fp32 head's tail (mr_mlp_simt.cu)
   float h_stencil[MR_STENCIL_POINTS * 3];
 };
 

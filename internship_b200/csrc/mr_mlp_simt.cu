@@ -572,6 +572,8 @@ struct HeadArgs {
   const int* job;
   const BatchOut* bout;
   int* err;  // tensor-core head: set when a bounded wait gave up
+  float* stg;  // LC2 outputs per albedo channel: chunk 8 ch + c of row k at stg[k*srs + c*scs]
+  long long srs, scs;
 };
 
 // Half of a 16 -> 16 layer: outputs 8h..8h+7 of ReLU(B + W x), bias first,
@@ -741,7 +743,6 @@ __global__ void __launch_bounds__(kHeadThreads, 1) k_tc32_head(HeadArgs a) {
   if ((int)blockIdx.x >= ntiles) return;  // block-uniform
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int r = 32 * (warp & 3) + lane, half = warp >> 2;  // TMEM lane mapping
-  const int rt = 16 * warp + (lane & 15), ht = lane >> 4;      // tail mapping (lane pairs)
   const float* __restrict__ w = a.w;
   const float* __restrict__ hr = a.wt + kHeadRowOff;
   const float* __restrict__ bias = a.wt + kTcBiasOff;
@@ -789,7 +790,6 @@ __global__ void __launch_bounds__(kHeadThreads, 1) k_tc32_head(HeadArgs a) {
     tc_fence_before();  // the previous tile's TMEM reads
     const bool need1 = __syncthreads_or(valid && srp[1] != srp[0]);
     const bool need2 = __syncthreads_or(valid && srp[2] != srp[0] && srp[2] != srp[1]);
-    float X[3] = {0.0f, 0.0f, 0.0f};  // of row rt
 #pragma unroll 1
     for (int ch = 0; ch < 3; ++ch) {
       if ((ch == 1 && !need1) || (ch == 2 && !need2)) continue;
@@ -861,102 +861,20 @@ __global__ void __launch_bounds__(kHeadThreads, 1) k_tc32_head(HeadArgs a) {
       __syncthreads();
       if (threadIdx.x == 0) tc_issue_layer<32, 64>(feed, tmem, ahi, alo, done);
       tc_layer_wait(done, dpar, ok);
-      // LC2 outputs (bias, ReLU) to shared memory, [column][row] over the A
-      // tile, free now
+      // LC2 outputs (bias, ReLU) of this channel to the staging columns; the
+      // tail runs in k_tc32_tail
       {
         float v[16];
         tmem_ld16(tl + 16 * half, v);
+        if (valid) {
+          float* srow = a.stg + (long long)row * a.srs;
 #pragma unroll
-        for (int i = 0; i < 16; i += 4) {
-          const float4 b = ldg4(bias + 192 + 16 * half + i);
-          Ahi[(16 * half + i) * kHeadRows + r] = relu0(v[i] + b.x);
-          Ahi[(16 * half + i + 1) * kHeadRows + r] = relu0(v[i + 1] + b.y);
-          Ahi[(16 * half + i + 2) * kHeadRows + r] = relu0(v[i + 2] + b.z);
-          Ahi[(16 * half + i + 3) * kHeadRows + r] = relu0(v[i + 3] + b.w);
-        }
-      }
-      tc_fence_before();
-      __syncthreads();
-      // LX 32 -> 16, the residual pairs (:454-471) and LX12 for row rt, split
-      // over lanes l and l ^ 16 (half ht of every 16-wide layer each)
-      {
-        float x32[32];
-#pragma unroll
-        for (int i = 0; i < 32; ++i) x32[i] = Ahi[i * kHeadRows + rt];
-        float a16[16];
-        {
-          float a8[8];
-#pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            float acc = __ldg(w + WOFF(LXB) + 8 * ht + q);
-#pragma unroll
-            for (int j = 0; j < 32; j += 4) {
-              const float4 v = ldg4(w + WOFF(LXW) + (8 * ht + q) * 32 + j);
-              acc += x32[j] * v.x;
-              acc += x32[j + 1] * v.y;
-              acc += x32[j + 2] * v.z;
-              acc += x32[j + 3] * v.w;
-            }
-            a8[q] = relu0(acc);
+          for (int i = 0; i < 16; i += 4) {
+            const float4 b = ldg4(bias + 192 + 16 * half + i);
+            *reinterpret_cast<float4*>(srow + (8 * ch + (16 * half + i) / 4) * a.scs) =
+                make_float4(relu0(v[i] + b.x), relu0(v[i + 1] + b.y), relu0(v[i + 2] + b.z), relu0(v[i + 3] + b.w));
           }
-          join16(a8, a16, ht);
         }
-        const int lx[12] = {WOFF(LX0W), WOFF(LX1W), WOFF(LX2W), WOFF(LX3W), WOFF(LX4W), WOFF(LX5W),
-                            WOFF(LX6W), WOFF(LX7W), WOFF(LX8W), WOFF(LX9W), WOFF(LX10W), WOFF(LX11W)};
-#pragma unroll 1
-        for (int rr = 0; rr < 6; ++rr) {
-          float h8[8], b16[16], c16[16];
-          dense16_half(a16, h8, w + lx[2 * rr], w + lx[2 * rr] + 256, ht);
-          join16(h8, b16, ht);
-          dense16_half(b16, h8, w + lx[2 * rr + 1], w + lx[2 * rr + 1] + 256, ht);
-          join16(h8, c16, ht);
-#pragma unroll
-          for (int i = 0; i < 16; ++i) a16[i] = a16[i] + c16[i];
-        }
-        float o = 0.0f;  // LX12 16 -> 1, bias after the sum
-#pragma unroll
-        for (int i = 0; i < 16; i += 4) {
-          const float4 v = ldg4(hr + 144 + i);
-          o += a16[i] * v.x;
-          o += a16[i + 1] * v.y;
-          o += a16[i + 2] * v.z;
-          o += a16[i + 3] * v.w;
-        }
-        o += __ldg(hr + 160);
-        const float xo = relu0(o);
-        if (ch == 0) X[0] = xo;
-        else if (ch == 1) X[1] = xo;
-        else X[2] = xo;
-      }
-      __syncthreads();  // the next channel's input overwrites the tile
-    }
-    // output of row rt by its first thread
-    const int rowt = tile * kHeadRows + rt;
-    if (ht == 0 && rowt < n) {
-      const float* axt = a.aux + (long long)rowt * a.ars;
-      const float srt[3] = {__ldg(axt + 2 * a.afs), __ldg(axt + 3 * a.afs), __ldg(axt + 4 * a.afs)};
-      if (srt[1] == srt[0]) X[1] = X[0];
-      if (srt[2] == srt[0]) X[2] = X[0];
-      else if (srt[2] == srt[1]) X[2] = X[1];
-      float o[3] = {fmaxf(expf(X[0]) - 1.0f, 0.0f) * srt[0], fmaxf(expf(X[1]) - 1.0f, 0.0f) * srt[1],
-                    fmaxf(expf(X[2]) - 1.0f, 0.0f) * srt[2]};
-      if (a.pix) {
-        const int px = a.pix[rowt];
-        const float tr = a.trph[rowt];
-        F3 lc = a.light_color, scv = a.scatter;
-        float* dst = a.out;
-        if (a.job) {
-          const BatchOut& bo = a.bout[a.job[rowt]];
-          lc = bo.light_color;
-          scv = bo.scatter;
-          dst = bo.out;
-        }
-        dst[3 * (size_t)px + 0] = fmaxf(((o[0] + tr) * lc.x) * scv.x, 0.0f);
-        dst[3 * (size_t)px + 1] = fmaxf(((o[1] + tr) * lc.y) * scv.y, 0.0f);
-        dst[3 * (size_t)px + 2] = fmaxf(((o[2] + tr) * lc.z) * scv.z, 0.0f);
-      } else {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) a.out[3 * (size_t)rowt + c] = o[c];
       }
     }
   }
@@ -975,6 +893,116 @@ __global__ void __launch_bounds__(kHeadThreads, 1) k_tc32_head(HeadArgs a) {
   }
 }
 
+// ---- tail of the head ----------------------------------------------------------------
+// LX 32 -> 16, the six residual pairs of 16 -> 16 layers and LX12 16 -> 1
+// (radiancePredict.cu:454-471) for each row and albedo channel, then the
+// output (:472-483). One thread per row; the 3809 weights (LXW .. LX12B, in
+// blob order) are kernel parameters, so each is a uniform constant-bank
+// operand of its multiply-add and the layers issue no loads.
+constexpr int kTailFloats = 512 + 16 + 12 * 272 + 16 + 1;
+struct TailParams {
+  float w[kTailFloats];
+};
+struct TailArgs {
+  const float* __restrict__ stg;  // LC2 outputs (HeadArgs::stg layout)
+  long long srs, scs;
+  const float* __restrict__ aux;
+  long long ars, afs;
+  int n;
+  const unsigned* __restrict__ count;
+  float* out;
+  const int* __restrict__ pix;
+  const float* __restrict__ trph;
+  F3 light_color, scatter;
+  const int* job;
+  const BatchOut* bout;
+};
+
+// Host image of TailParams: the blob's LXW .. LX12B, which are contiguous.
+void tail_param_image(const float* w, std::vector<float>& out) {
+  const WeightTable wt = make_weight_table();
+  out.assign(w + wt.off[MR_W_LXW], w + wt.off[MR_W_LXW] + kTailFloats);
+}
+static_assert(sizeof(TailParams) + sizeof(TailArgs) <= 32000, "kernel parameter space");
+
+// One row and channel: x = the channel's 32 LC2 outputs (chunks 8 ch .. 8 ch + 7).
+__device__ __forceinline__ float tail_row(const float* srow, long long scs, int ch, const TailParams& P) {
+  float x[32];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const float4 q = __ldg(reinterpret_cast<const float4*>(srow + (8 * ch + c) * scs));
+    x[4 * c] = q.x; x[4 * c + 1] = q.y; x[4 * c + 2] = q.z; x[4 * c + 3] = q.w;
+  }
+  float a16[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {  // LX, bias first, ascending inputs
+    float acc = P.w[512 + q];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) acc += x[j] * P.w[q * 32 + j];
+    a16[q] = relu0(acc);
+  }
+#pragma unroll
+  for (int rr = 0; rr < 6; ++rr) {
+    const float* W1 = P.w + 528 + 272 * (2 * rr);
+    const float* W2 = W1 + 272;
+    float h16[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      float acc = W1[256 + q];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) acc += a16[j] * W1[q * 16 + j];
+      h16[q] = relu0(acc);
+    }
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {  // a16 is dead once h16 exists: the residual sum goes in place
+      float acc = W2[256 + q];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) acc += h16[j] * W2[q * 16 + j];
+      a16[q] = a16[q] + relu0(acc);
+    }
+  }
+  float o = 0.0f;  // LX12 16 -> 1, bias after the sum
+#pragma unroll
+  for (int i = 0; i < 16; ++i) o += a16[i] * P.w[3792 + i];
+  o += P.w[3808];
+  return relu0(o);
+}
+
+// Straight-line code per channel (a loop over the channels would let the
+// compiler hoist the constant operands out of it into registers).
+__global__ void __launch_bounds__(128, 6) k_tc32_tail(TailArgs a, const TailParams P) {
+  const int n = a.count ? (int)min(*a.count, (unsigned)a.n) : a.n;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const float* ax = a.aux + (long long)k * a.ars;
+  const float srp[3] = {__ldg(ax + 2 * a.afs), __ldg(ax + 3 * a.afs), __ldg(ax + 4 * a.afs)};
+  const float* srow = a.stg + (long long)k * a.srs;
+  float X[3];
+  X[0] = tail_row(srow, a.scs, 0, P);
+  X[1] = srp[1] != srp[0] ? tail_row(srow, a.scs, 1, P) : X[0];
+  X[2] = srp[2] == srp[0] ? X[0] : srp[2] == srp[1] ? X[1] : tail_row(srow, a.scs, 2, P);
+  const float o[3] = {fmaxf(expf(X[0]) - 1.0f, 0.0f) * srp[0], fmaxf(expf(X[1]) - 1.0f, 0.0f) * srp[1],
+                      fmaxf(expf(X[2]) - 1.0f, 0.0f) * srp[2]};
+  if (a.pix) {
+    const int px = a.pix[k];
+    const float tr = a.trph[k];
+    F3 lc = a.light_color, scv = a.scatter;
+    float* dst = a.out;
+    if (a.job) {
+      const BatchOut& bo = a.bout[a.job[k]];
+      lc = bo.light_color;
+      scv = bo.scatter;
+      dst = bo.out;
+    }
+    dst[3 * (size_t)px + 0] = fmaxf(((o[0] + tr) * lc.x) * scv.x, 0.0f);
+    dst[3 * (size_t)px + 1] = fmaxf(((o[1] + tr) * lc.y) * scv.y, 0.0f);
+    dst[3 * (size_t)px + 2] = fmaxf(((o[2] + tr) * lc.z) * scv.z, 0.0f);
+  } else {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) a.out[3 * (size_t)k + c] = o[c];
+  }
+}
+
 int* mlp_error_word(const Network* net);  // mr_mlp_tc.cu
 
 // Trunk kernel then head kernel. `tout` receives the trunk outputs (TrunkOut
@@ -984,8 +1012,10 @@ int* mlp_error_word(const Network* net);  // mr_mlp_tc.cu
 int launch_mlp_simt(const Network* net, const float* desc, const float* aux, long long rs, long long cs,
                     long long ars, long long afs, int n, const unsigned* count, float* out, const int* pix,
                     const float* trph, F3 light_color, F3 scatter, cudaStream_t s, const int* job,
-                    const BatchOut* bout, float* tout, long long trs, long long tcs) {
-  if (!tout) return set_error(MR_ERR_ARG, "fp32 network: no buffer for the trunk outputs");
+                    const BatchOut* bout, float* tout, long long trs, long long tcs, float* stg, long long srs,
+                    long long scs) {
+  if (!tout || !stg) return set_error(MR_ERR_ARG, "fp32 network: no buffer for the trunk or LC2 outputs");
+  if (net->h_tail.size() != (size_t)kTailFloats) return set_error(MR_ERR_STATE, "network not packed");
   static bool attr = false;
   if (!attr) {
     MR_CUDA(cudaFuncSetAttribute(k_tc32_head, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcHeadSmem));
@@ -1024,8 +1054,31 @@ int launch_mlp_simt(const Network* net, const float* desc, const float* aux, lon
   h.job = job;
   h.bout = bout;
   h.err = mlp_error_word(net);
+  h.stg = stg;
+  h.srs = srs;
+  h.scs = scs;
   const int tiles = (n + kHeadRows - 1) / kHeadRows;
   k_tc32_head<<<(unsigned)std::min(tiles, sm_count()), kHeadThreads, kTcHeadSmem, s>>>(h);
+  MR_CUDA(cudaGetLastError());
+  TailArgs t;
+  t.stg = stg;
+  t.srs = srs;
+  t.scs = scs;
+  t.aux = aux;
+  t.ars = ars;
+  t.afs = afs;
+  t.n = n;
+  t.count = count;
+  t.out = out;
+  t.pix = pix;
+  t.trph = trph;
+  t.light_color = light_color;
+  t.scatter = scatter;
+  t.job = job;
+  t.bout = bout;
+  TailParams P;
+  std::memcpy(P.w, net->h_tail.data(), sizeof(P.w));
+  k_tc32_tail<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(t, P);
   MR_CUDA(cudaGetLastError());
   return MR_OK;
 }

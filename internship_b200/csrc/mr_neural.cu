@@ -493,7 +493,7 @@ int launch_mlp_tc(const Network* net, const float* desc, const float* aux, long 
 int launch_mlp_simt(const Network* net, const float* desc, const float* aux, long long rs, long long cs,
                     long long ars, long long afs, int n, const unsigned* count, float* out, const int* pix,
                     const float* trph, F3 light_color, F3 scatter, cudaStream_t s, const int* job, const BatchOut* bout,
-                    float* tout, long long trs, long long tcs);
+                    float* tout, long long trs, long long tcs, float* stg, long long srs, long long scs);
 int mlp_tc_error(const Network* net, bool reset);
 
 extern int check_params(const mr_render_params* p);
@@ -617,33 +617,52 @@ static int neural_passes(Volume* v, const Network* net, const mr_render_params* 
   ta.dist = dev_dist;
   ta.rec = rec;
   ta.counters = v->d_counters;
-  mark(ST_NN_TRACE);
-  k_nn_trace<<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(ta);
-  mark(ST_NN_TRACE);
-  MR_CUDA(cudaGetLastError());
-  F3 sr = to_f3(p->scatter_rate) / 1.001f;
   // the exact sampler reads texture gathers, or texel loads where nothing
   // may be allocated (the layered copies are created on first use)
   const int samp = p->sampler == MR_SAMPLER_TEXTURE ? kSampTex : no_alloc ? kSampLoad : kSampGather;
   Tables tabs;
   rc = fill_tables(v, samp, &tabs, s);
   if (rc) return rc;
-  mark(ST_NN_PREDICT);
+  // The per-point table (one block) runs on the volume's side stream beside
+  // the trace, which does not read it; the gather waits for it. Where nothing
+  // may be created it runs in line.
   float* h0s = (float*)((char*)base + h0_offset(npx, distinct_channels(p)));
+  cudaStream_t hs = s;
+  if (!no_alloc) {
+    if (!v->side_stream) {
+      MR_CUDA(cudaStreamCreateWithFlags(&v->side_stream, cudaStreamNonBlocking));
+      MR_CUDA(cudaEventCreateWithFlags(&v->side_fork, cudaEventDisableTiming));
+      MR_CUDA(cudaEventCreateWithFlags(&v->side_join, cudaEventDisableTiming));
+    }
+    hs = v->side_stream;
+    MR_CUDA(cudaEventRecord(v->side_fork, s));
+    MR_CUDA(cudaStreamWaitEvent(hs, v->side_fork, 0));
+  }
+  if (samp == kSampTex)
+    k_sphere_h0<kSampTex><<<1, 192, 0, hs>>>(tabs, net->stencil, h0s);
+  else if (samp == kSampGather)
+    k_sphere_h0<kSampGather><<<1, 192, 0, hs>>>(tabs, net->stencil, h0s);
+  else
+    k_sphere_h0<kSampLoad><<<1, 192, 0, hs>>>(tabs, net->stencil, h0s);
+  MR_CUDA(cudaGetLastError());
+  if (hs != s) MR_CUDA(cudaEventRecord(v->side_join, hs));
+  mark(ST_NN_TRACE);
+  k_nn_trace<<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(ta);
+  mark(ST_NN_TRACE);
+  MR_CUDA(cudaGetLastError());
+  if (hs != s) MR_CUDA(cudaStreamWaitEvent(s, v->side_join, 0));
+  F3 sr = to_f3(p->scatter_rate) / 1.001f;
+  mark(ST_NN_PREDICT);
   const unsigned ggrid = (unsigned)((npx + 127) / 128);
-  if (samp == kSampTex) {
-    k_sphere_h0<kSampTex><<<1, 192, 0, s>>>(tabs, net->stencil, h0s);
+  if (samp == kSampTex)
     k_gather_fm<kSampTex><<<ggrid, 128, 0, s>>>(tabs, net->stencil, h0s, rec, (int)npx, L, p->alpha, p->g,
                                                srp_of(sr), desc, aux);
-  } else if (samp == kSampGather) {
-    k_sphere_h0<kSampGather><<<1, 192, 0, s>>>(tabs, net->stencil, h0s);
+  else if (samp == kSampGather)
     k_gather_fm<kSampGather><<<ggrid, 128, 0, s>>>(tabs, net->stencil, h0s, rec, (int)npx, L, p->alpha, p->g,
                                                   srp_of(sr), desc, aux);
-  } else {
-    k_sphere_h0<kSampLoad><<<1, 192, 0, s>>>(tabs, net->stencil, h0s);
+  else
     k_gather_fm<kSampLoad><<<ggrid, 128, 0, s>>>(tabs, net->stencil, h0s, rec, (int)npx, L, p->alpha, p->g,
                                                 srp_of(sr), desc, aux);
-  }
   mark(ST_NN_PREDICT);
   MR_CUDA(cudaGetLastError());
   const long long cap = (long long)npx;
@@ -652,8 +671,11 @@ static int neural_passes(Volume* v, const Network* net, const mr_render_params* 
     rc = launch_mlp_tc(net, desc, aux, 4, 4 * cap, 1, cap, (int)npx, dev_rgb, rec.pix, rec.trph, rec.count,
                        to_f3(p->light_color), to_f3(p->scatter_rate), spill, p->precision == MR_PREC_FP8, s);
   else
+    // trunk outputs over the row's first 34 descriptor chunks, the head's LC2
+    // outputs over chunks 48..71 (all consumed by the trunk)
     rc = launch_mlp_simt(net, desc, aux, 4, 4 * cap, 1, cap, (int)npx, rec.count, dev_rgb, rec.pix, rec.trph,
-                         to_f3(p->light_color), to_f3(p->scatter_rate), s, nullptr, nullptr, desc, 4, 4 * cap);
+                         to_f3(p->light_color), to_f3(p->scatter_rate), s, nullptr, nullptr, desc, 4, 4 * cap,
+                         desc + 48 * 4 * cap, 4, 4 * cap);
   mark(ST_NN_MLP);
   return rc;
 }
@@ -768,13 +790,14 @@ extern "C" int mr_radiance_predict(const mr_network* nh, int32_t precision, cons
     return rc;
   }
   if (precision != MR_PREC_FP32) return set_error(MR_ERR_ARG, "unknown precision %d", precision);
-  // the caller's descriptors stay untouched: trunk outputs go to a temporary
+  // the caller's descriptors stay untouched: trunk outputs (136) and the
+  // head's LC2 outputs (96) of a row go to a temporary
   cudaStream_t s = (cudaStream_t)stream;
   float* tout = nullptr;
-  cudaError_t e = cudaMallocAsync(&tout, (size_t)n * 136 * sizeof(float), s);
+  cudaError_t e = cudaMallocAsync(&tout, (size_t)n * 232 * sizeof(float), s);
   if (e != cudaSuccess) return set_error(MR_ERR_NOMEM, "trunk buffer: %s", cudaGetErrorString(e));
   int rc = launch_mlp_simt(&nh->n, dev_desc, dev_aux, 576, 4, 5, 1, n, nullptr, dev_out, nullptr, nullptr,
-                           f3(1, 1, 1), f3(1, 1, 1), s, nullptr, nullptr, tout, 136, 4);
+                           f3(1, 1, 1), f3(1, 1, 1), s, nullptr, nullptr, tout, 232, 4, tout + 136, 232, 4);
   MR_CUDA(cudaFreeAsync(tout, s));
   return rc;
 }
@@ -994,7 +1017,8 @@ static int batch_launches(Batch& b, const Network* net, cudaStream_t s) {
                          f3(1, 1, 1), f3(1, 1, 1), spill, b.precision == MR_PREC_FP8, s, rec.job, b.d_out);
     else
       rc = launch_mlp_simt(net, desc, aux, 4, 4 * ccap, 1, ccap, (int)cap, rec.count, nullptr, rec.pix, rec.trph,
-                           f3(1, 1, 1), f3(1, 1, 1), s, rec.job, b.d_out, desc, 4, 4 * ccap);
+                           f3(1, 1, 1), f3(1, 1, 1), s, rec.job, b.d_out, desc, 4, 4 * ccap, desc + 48 * 4 * ccap, 4,
+                           4 * ccap);
     if (rc) return rc;
   }
   k_batch_advance<<<(nj + 127) / 128, 128, 0, s>>>(b.d_jobs, nj);

@@ -451,6 +451,12 @@ int mr_volume_destroy(mr_volume* h) {
   }
   for (int i = 0; i < 2; ++i)
     if (v->frame[i]) cudaFree(v->frame[i]);
+  if (v->side_stream) {
+    cudaStreamSynchronize(v->side_stream);
+    cudaEventDestroy(v->side_fork);
+    cudaEventDestroy(v->side_join);
+    cudaStreamDestroy(v->side_stream);
+  }
   destroy_textures(v);
   delete h;
   return MR_OK;

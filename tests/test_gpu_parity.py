@@ -251,7 +251,12 @@ def test_render_host_async_matches_sync(mr):
     _lib.check(L.mr_render_host_wait(v.handle, 1, 10000))
     _lib.check(L.mr_render_host_wait(v.handle, -1, 10000))
     for p, out in zip(jobs, outs):
-        np.testing.assert_array_equal(out, _render(mr, v, p, net))
+        if p.render_type == _lib.RT_MRPNN:
+            np.testing.assert_array_equal(out, _render(mr, v, p, net))
+        else:
+            # delta tracking sums its samples with fp32 atomics: the order of
+            # the 4 adds per pixel varies from run to run
+            np.testing.assert_allclose(out, _render(mr, v, p, net), rtol=1e-6, atol=1e-7)
     assert L.mr_render_host_wait(v.handle, len(jobs), 0) == _lib.MR_ERR_ARG
     p = jobs[0]
     assert L.mr_render_host_async(v.handle, net, C.byref(p), None, None, None) == _lib.MR_ERR_ARG
