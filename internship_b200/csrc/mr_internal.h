@@ -98,6 +98,7 @@ struct Network {
   std::vector<float> h_winv8;    // inverse per-layer scales of the E4M3 weight image
   float* simt_img = nullptr;     // weight image of the fp32 network kernels (simt_weight_image)
   std::vector<float> h_tail;     // LXW .. LX12B, kernel parameters of the fp32 head's tail (mr_mlp_simt.cu)
+  std::vector<float> h_light;    // kernel parameters of the fp32 light-direction trunk (mr_mlp_simt.cu)
   float h_stencil[MR_STENCIL_POINTS * 3];
 };
 

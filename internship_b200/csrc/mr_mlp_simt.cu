@@ -515,34 +515,12 @@ __global__ void __launch_bounds__(kTile, 3) k_simt_trunk(TrunkArgs a, TrunkOut t
   __syncthreads();
   trunk_gemm<32, 2>(tile, ring + (6 & 1) * stage_floats(kTrunkStages - 1), a.desc, a.rs, a.cs, row0, n, 0, to);
   asm volatile("cp.async.wait_all;\n" ::: "memory");
-  __syncthreads();  // the tile is free for the light-direction trunk
   const bool valid = row < n;
   float* orow = to.t + (long long)row * to.rs;
   auto put4 = [&](int c, float x0, float x1, float x2, float x3) {
     if (valid) *reinterpret_cast<float4*>(orow + c * to.cs) = make_float4(x0, x1, x2, x3);
   };
-  // light-direction trunk (:424-437), per row
-  row_block8<0>(in, w, sw + 8 * kSeFloats, 160, WOFF(LD01W), WOFF(LD_Tr01W), WOFF(LD_Hg01W), g, gamma, y, fin);
-  {
-    const int pd[3][3] = {{WOFF(LD11W), WOFF(LD_Tr11W), WOFF(LD_Hg11W)},
-                          {WOFF(LD21W), WOFF(LD_Tr21W), WOFF(LD_Hg21W)},
-                          {WOFF(LD31W), WOFF(LD_Tr31W), WOFF(LD_Hg31W)}};
-#pragma unroll 1
-    for (int b = 0; b < 3; ++b)
-      row_block8<1>(in, w, sw + (9 + b) * kSeFloats, 168 + 8 * b, pd[b][0], pd[b][1], pd[b][2], g, gamma, y, fin);
-  }
-  {  // LD41: comb[96..120)
-    const int wl[3] = {WOFF(LD41W), WOFF(LD_Tr41W), WOFF(LD_Hg41W)};
-#pragma unroll
-    for (int b = 0; b < 3; ++b) {
-      float xin[8], c[8];
-#pragma unroll
-      for (int i = 0; i < 8; ++i) xin[i] = y.at(b, i);
-      dense1<8>(xin, c, w + wl[b]);
-#pragma unroll
-      for (int i = 0; i < 8; i += 4) put4((96 + 8 * b + i) / 4, c[i], c[i + 1], c[i + 2], c[i + 3]);
-    }
-  }
+  // the light-direction trunk (blocks 8..11, LD41) runs in k_light_trunk
   // LSEFin1's g and gamma columns (pool[72], pool[73]); the albedo column is
   // added per channel by the head
 #pragma unroll
@@ -550,6 +528,126 @@ __global__ void __launch_bounds__(kTile, 3) k_simt_trunk(TrunkArgs a, TrunkOut t
     fin[j] += g * __ldg(w + WOFF(LSEFin1W) + j * 75 + 72) + gamma * __ldg(w + WOFF(LSEFin1W) + j * 75 + 73);
 #pragma unroll
   for (int j0 = 0; j0 < 16; j0 += 4) put4(30 + j0 / 4, fin[j0], fin[j0 + 1], fin[j0 + 2], fin[j0 + 3]);
+}
+
+// ---- light-direction trunk --------------------------------------------------------------
+// Blocks 8..11 (SE + ADD3, then SERES + ADD3, width 8) and LD41
+// (radiancePredict.cu:424-437) per row, after k_simt_trunk: comb[96..120)
+// into trunk-output chunks 24..29 and the blocks' LSEFin1 terms added to the
+// sums in chunks 30..33. One thread per row; the weights (squeeze-excitation
+// of the four blocks, then the fifteen 8 -> 8 layers with their biases) are
+// kernel parameters, uniform constant-bank operands.
+struct LightParams {
+  float se[4][kSeFloats];
+  float dense[15][72];  // LD01, LD11, LD21, LD31, LD41; per block branches density, transmittance, phase
+};
+
+void light_param_image(const float* w, const std::vector<float>& img, std::vector<float>& out) {
+  out.assign(sizeof(LightParams) / sizeof(float), 0.0f);
+  std::copy(img.begin() + kSeOff + 8 * kSeFloats, img.begin() + kSeOff + 12 * kSeFloats, out.begin());
+  const WeightTable wt = make_weight_table();
+  const int ids[15] = {MR_W_LD01W, MR_W_LD_Tr01W, MR_W_LD_Hg01W, MR_W_LD11W, MR_W_LD_Tr11W, MR_W_LD_Hg11W,
+                       MR_W_LD21W, MR_W_LD_Tr21W, MR_W_LD_Hg21W, MR_W_LD31W, MR_W_LD_Tr31W, MR_W_LD_Hg31W,
+                       MR_W_LD41W, MR_W_LD_Tr41W, MR_W_LD_Hg41W};
+  for (int d = 0; d < 15; ++d)
+    std::copy(w + wt.off[ids[d]], w + wt.off[ids[d]] + 72, out.begin() + 4 * kSeFloats + 72 * d);
+}
+
+// 8 -> 8 layer, bias first then ascending inputs (dense1's order), weights
+// from the parameter space.
+__device__ __forceinline__ void dense8p(const float (&x)[8], float (&y)[8], const float* W) {
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    float acc = W[64 + q];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc += x[j] * W[q * 8 + j];
+    y[q] = relu0(acc);
+  }
+}
+
+template <int B>
+__device__ __forceinline__ void light_block(const RowIO& in, const LightParams& P, float g, float gamma,
+                                            float (&y)[3][8], float (&fin)[16]) {
+  constexpr int from = 160 + 8 * B;
+  const float* sw = P.se[B];
+  float st[6];
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+    float s = 0.0f, m = -10000.0f;
+#pragma unroll
+    for (int i = 0; i < 8; i += 4) {
+      const float4 q = in.ld4(b * 192 + from + i);
+      s += q.x; s += q.y; s += q.z; s += q.w;
+      m = fmaxf(m, q.x); m = fmaxf(m, q.y); m = fmaxf(m, q.z); m = fmaxf(m, q.w);
+    }
+    st[2 * b] = s / 8.0f;
+    st[2 * b + 1] = m;
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k)
+#pragma unroll
+    for (int j = 0; j < 16; ++j) fin[j] += st[k] * sw[k * 16 + j];
+  const float tmp[8] = {st[0], st[2], st[4], st[1], st[3], st[5], g, gamma};
+  float h[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    float a = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a += tmp[j] * sw[96 + i * 8 + j];
+    h[i] = relu0(a);
+  }
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+    float a = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a += h[j] * sw[160 + b * 8 + j];
+    const float gate = 1.0f / (1.0f + expf(-a));
+    float v[8], x[8], yn[8];  // the branch's block input (a second read, from L1)
+#pragma unroll
+    for (int i = 0; i < 8; i += 4) {
+      const float4 q = in.ld4(b * 192 + from + i);
+      v[i] = q.x; v[i + 1] = q.y; v[i + 2] = q.z; v[i + 3] = q.w;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const float xv = v[i] * gate;
+      x[i] = B == 0 ? xv : xv + y[b][i];
+    }
+    dense8p(x, yn, P.dense[3 * B + b]);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) y[b][i] = yn[i] + v[i];
+  }
+}
+
+__global__ void __launch_bounds__(128, 6) k_light_trunk(TrunkArgs a, TrunkOut to, const LightParams P) {
+  const int n = a.count ? (int)min(*a.count, (unsigned)a.n) : a.n;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const RowIO in{a.desc + (long long)k * a.rs, (int)(a.cs * 4)};
+  const float* ax = a.aux + (long long)k * a.ars;
+  const float g = __ldg(ax), gamma = __ldg(ax + a.afs);
+  float y[3][8], fin[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) fin[j] = 0.0f;
+  light_block<0>(in, P, g, gamma, y, fin);
+  light_block<1>(in, P, g, gamma, y, fin);
+  light_block<2>(in, P, g, gamma, y, fin);
+  light_block<3>(in, P, g, gamma, y, fin);
+  float* orow = to.t + (long long)k * to.rs;
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {  // LD41: comb[96..120)
+    float c[8];
+    dense8p(y[b], c, P.dense[12 + b]);
+#pragma unroll
+    for (int i = 0; i < 8; i += 4)
+      *reinterpret_cast<float4*>(orow + ((96 + 8 * b + i) / 4) * to.cs) = make_float4(c[i], c[i + 1], c[i + 2], c[i + 3]);
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {  // LSEFin1 sums: the main trunk's (with the g, gamma columns) plus these blocks'
+    float4* f = reinterpret_cast<float4*>(orow + (30 + c) * to.cs);
+    const float4 q = *f;
+    *f = make_float4(q.x + fin[4 * c], q.y + fin[4 * c + 1], q.z + fin[4 * c + 2], q.w + fin[4 * c + 3]);
+  }
 }
 
 // ---- head --------------------------------------------------------------------------
@@ -1015,7 +1113,8 @@ int launch_mlp_simt(const Network* net, const float* desc, const float* aux, lon
                     const BatchOut* bout, float* tout, long long trs, long long tcs, float* stg, long long srs,
                     long long scs) {
   if (!tout || !stg) return set_error(MR_ERR_ARG, "fp32 network: no buffer for the trunk or LC2 outputs");
-  if (net->h_tail.size() != (size_t)kTailFloats) return set_error(MR_ERR_STATE, "network not packed");
+  if (net->h_tail.size() != (size_t)kTailFloats || net->h_light.size() * sizeof(float) != sizeof(LightParams))
+    return set_error(MR_ERR_STATE, "network not packed");
   static bool attr = false;
   if (!attr) {
     MR_CUDA(cudaFuncSetAttribute(k_tc32_head, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcHeadSmem));
@@ -1035,6 +1134,12 @@ int launch_mlp_simt(const Network* net, const float* desc, const float* aux, lon
   a.count = count;
   k_simt_trunk<<<(unsigned)((n + kTile - 1) / kTile), kTile, kTrunkSmem, s>>>(a, TrunkOut{tout, trs, tcs});
   MR_CUDA(cudaGetLastError());
+  {
+    LightParams LP;
+    std::memcpy(&LP, net->h_light.data(), sizeof(LP));
+    k_light_trunk<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(a, TrunkOut{tout, trs, tcs}, LP);
+    MR_CUDA(cudaGetLastError());
+  }
   HeadArgs h;
   h.w = net->w;
   h.wt = net->simt_img;

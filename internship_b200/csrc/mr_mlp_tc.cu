@@ -1168,6 +1168,7 @@ static uint8_t to_e4m3(float f) {
 
 void simt_weight_image(const float* w, std::vector<float>& img);  // mr_mlp_simt.cu
 void tail_param_image(const float* w, std::vector<float>& out);   // mr_mlp_simt.cu
+void light_param_image(const float* w, const std::vector<float>& img, std::vector<float>& out);
 
 int pack_network(Network* n) {
   std::vector<float> w(MR_WEIGHT_TOTAL);
@@ -1211,6 +1212,7 @@ int pack_network(Network* n) {
     std::vector<float> si;
     simt_weight_image(w.data(), si);
     tail_param_image(w.data(), n->h_tail);
+    light_param_image(w.data(), si, n->h_light);
     cudaError_t e = cudaMalloc(&n->simt_img, si.size() * sizeof(float));
     if (e == cudaSuccess) e = cudaMemcpy(n->simt_img, si.data(), si.size() * sizeof(float), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return set_error(MR_ERR_NOMEM, "pack_network: %s", cudaGetErrorString(e));
