@@ -458,32 +458,34 @@ template <int SAMP>
 __global__ void __launch_bounds__(128, SAMP == kSampLoad ? 1 : 6)
     k_gather_fm(Tables t, const float* __restrict__ stencil, const float* __restrict__ h0s, Records rec, int cap, F3 L,
                 float alpha, float g, F3 srp, float* __restrict__ desc, float* __restrict__ aux) {
-  unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned n = min(*rec.count, (unsigned)cap);
-  if (k >= n) return;
-  F3 pos = f3(rec.pos[3 * (size_t)k], rec.pos[3 * (size_t)k + 1], rec.pos[3 * (size_t)k + 2]);
-  Frame f = load_frame(rec.frame + 12 * (size_t)k);
-  // chunk-of-4 feature-major: features 4j..4j+3 of record k are the float4
-  // at desc[(j*cap + k)*4]; a warp's store of one chunk is 512 contiguous bytes
-  float4* d = reinterpret_cast<float4*>(desc) + k;
-  const size_t c = (size_t)cap;
-  float4 bv, bs, bh;
-  auto sink = [&](int i, int u, float xv, float xs, float xh) {
-    (&bv.x)[u] = xv;
-    (&bs.x)[u] = xs;
-    (&bh.x)[u] = xh;
-    if (u == 3) {
-      d[(i >> 2) * c] = bv;
-      d[(48 + (i >> 2)) * c] = bs;
-      d[(96 + (i >> 2)) * c] = bh;
-    }
-  };
-  gather_fast<SAMP>(t, stencil, pos, L, f, alpha, g, h0s, sink);
-  aux[k] = g;
-  aux[c + k] = acosf(dot(f.X, f.LX));
-  aux[2 * c + k] = srp.x;
-  aux[3 * c + k] = srp.y;
-  aux[4 * c + k] = srp.z;
+  const unsigned n = min(*rec.count, (unsigned)cap);
+  // a resident grid strides over the records (the record count is known on
+  // the device only)
+  for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    F3 pos = f3(rec.pos[3 * (size_t)k], rec.pos[3 * (size_t)k + 1], rec.pos[3 * (size_t)k + 2]);
+    Frame f = load_frame(rec.frame + 12 * (size_t)k);
+    // chunk-of-4 feature-major: features 4j..4j+3 of record k are the float4
+    // at desc[(j*cap + k)*4]; a warp's store of one chunk is 512 contiguous bytes
+    float4* d = reinterpret_cast<float4*>(desc) + k;
+    const size_t c = (size_t)cap;
+    float4 bv, bs, bh;
+    auto sink = [&](int i, int u, float xv, float xs, float xh) {
+      (&bv.x)[u] = xv;
+      (&bs.x)[u] = xs;
+      (&bh.x)[u] = xh;
+      if (u == 3) {
+        d[(i >> 2) * c] = bv;
+        d[(48 + (i >> 2)) * c] = bs;
+        d[(96 + (i >> 2)) * c] = bh;
+      }
+    };
+    gather_fast<SAMP>(t, stencil, pos, L, f, alpha, g, h0s, sink);
+    aux[k] = g;
+    aux[c + k] = acosf(dot(f.X, f.LX));
+    aux[2 * c + k] = srp.x;
+    aux[3 * c + k] = srp.y;
+    aux[4 * c + k] = srp.z;
+  }
 }
 
 int launch_mlp_tc(const Network* net, const float* desc, const float* aux, long long rs, long long cs,
@@ -653,7 +655,17 @@ static int neural_passes(Volume* v, const Network* net, const mr_render_params* 
   if (hs != s) MR_CUDA(cudaStreamWaitEvent(s, v->side_join, 0));
   F3 sr = to_f3(p->scatter_rate) / 1.001f;
   mark(ST_NN_PREDICT);
-  const unsigned ggrid = (unsigned)((npx + 127) / 128);
+  // resident grids: as many 128-thread blocks as fit on the GPU at once
+  static int per_sm[3] = {0, 0, 0};
+  if (!per_sm[samp]) {
+    MR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm[samp],
+        samp == kSampTex ? (const void*)k_gather_fm<kSampTex>
+                         : samp == kSampGather ? (const void*)k_gather_fm<kSampGather> : (const void*)k_gather_fm<kSampLoad>,
+        128, 0));
+    per_sm[samp] = std::max(1, per_sm[samp]);
+  }
+  const unsigned ggrid = (unsigned)std::min<size_t>((npx + 127) / 128, (size_t)per_sm[samp] * sm_count());
   if (samp == kSampTex)
     k_gather_fm<kSampTex><<<ggrid, 128, 0, s>>>(tabs, net->stencil, h0s, rec, (int)npx, L, p->alpha, p->g,
                                                srp_of(sr), desc, aux);
