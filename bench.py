@@ -125,13 +125,14 @@ TRAINED = os.path.join(ROOT, "internship_b200", "data", "mrpnn_trained.npy")
 
 # DRAM bytes (read + write) per unit from one ncu capture of each kernel on the
 # 960x540 case of this frame (profiles/*_neural_960x540.md): per active pixel
-# for the gathers and networks (the fp32 network: k_simt_trunk + k_tc32_head),
+# for the gathers and networks (the fp32 network: k_simt_trunk + k_light_trunk +
+# k_tc32_head + k_tc32_tail),
 # per density fetch for the trace. A launch's traffic = this figure x the
 # launch's units.
-TRAFFIC_PER_UNIT = {"k_simt": 3152.8, "k_mlp_tc": 2542.6, "k_gather_fm_exact": 2469.8,
+TRAFFIC_PER_UNIT = {"k_simt": 3309.6, "k_mlp_tc": 2542.6, "k_gather_fm_exact": 2469.8,
                     "k_gather_fm_texture": 2447.0, "k_nn_trace": 137.2}
-SIMT_KERNELS = ("k_simt_trunk + k_tc32_head (fp32 network: CUDA-core trunk, tcgen05 head with fp32-accurate "
-                "three-term TF32 products)")
+SIMT_KERNELS = ("k_simt_trunk + k_light_trunk + k_tc32_head + k_tc32_tail (fp32 network: CUDA-core trunks, "
+                "tcgen05 head with fp32-accurate three-term TF32 products, CUDA-core tail)")
 # fp32 FMA rate of the CUDA cores (148 SMs x 128 lanes x 2 FLOP x 1.965 GHz), nominal
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 

@@ -485,10 +485,7 @@ __device__ __forceinline__ void trunk_tile(const TrunkArgs& a, const TrunkOut& t
   for (int st = 0; st < 6; ++st) {
     const int S = stage_width(st), from = st < 3 ? 16 + 16 * st : 64 + 32 * (st - 3);
     const float* sws = sw + (2 + st) * kSeFloats;
-    if (st < 4)
-      desc_prefetch(a, row0, n, st == 0 ? 48 : 32 * st + 32, st == 0 ? 64 : 32 * st + 64);
-    else if (st == 4)
-      desc_prefetch(a, row0, n, 160, 192);
+    if (st < 4) desc_prefetch(a, row0, n, st == 0 ? 48 : 32 * st + 32, st == 0 ? 64 : 32 * st + 64);
     if (S == 16)
       row_gate_input<16>(in, sws, from, g, gamma, y, fin);
     else
