@@ -124,7 +124,7 @@ def run_reference(args, rank):
 TRAINED = os.path.join(ROOT, "internship_b200", "data", "mrpnn_trained.npy")
 
 # DRAM bytes (read + write) per unit from one ncu capture of each kernel on the
-# 960x540 case of this frame (profiles/*_neural_960x540.md): per active pixel
+# 960x540 case of this frame (ncu --set full, one launch each): per active pixel
 # for the gathers and networks (the fp32 network: k_simt_trunk + k_light_trunk +
 # k_tc32_head + k_tc32_tail),
 # per density fetch for the trace. A launch's traffic = this figure x the
@@ -133,6 +133,10 @@ TRAFFIC_PER_UNIT = {"k_simt": 3309.6, "k_mlp_tc": 2542.6, "k_gather_fm_exact": 2
                     "k_gather_fm_texture": 2447.0, "k_nn_trace": 137.2}
 SIMT_KERNELS = ("k_simt_trunk + k_light_trunk + k_tc32_head + k_tc32_tail (fp32 network: CUDA-core trunks, "
                 "tcgen05 head with fp32-accurate three-term TF32 products, CUDA-core tail)")
+# The library's kernels of one fp32 / exact-sampler frame, in launch order
+# (as an ncu launch list of this command shows them).
+FP32_FRAME_KERNELS = ("k_sphere_h0", "k_nn_trace", "k_gather_fm", "k_simt_trunk", "k_light_trunk", "k_tc32_head",
+                      "k_tc32_tail")
 # fp32 FMA rate of the CUDA cores (148 SMs x 128 lanes x 2 FLOP x 1.965 GHz), nominal
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
@@ -535,7 +539,8 @@ def main():
                     "api": "mr_render_host_async (copy of frame k overlaps the render of frame k+1)",
                     "clock": "host wall clock to the last frame in pinned host memory",
                     "serial_value": serial_fps},
-            "gpu_launches": head["launches"],
+            "gpu_launches": args.steps * len(FP32_FRAME_KERNELS),
+            "gpu_kernels_per_step": list(FP32_FRAME_KERNELS),
             "roofline": roofline, "clocks": clk,
             "stage_rooflines": stages,
             "active_pixels_per_frame": active,
