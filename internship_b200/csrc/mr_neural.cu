@@ -904,48 +904,83 @@ __global__ void __launch_bounds__(256) k_trace_batch(const BatchJob* __restrict_
   const long long p = w0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
   TrackStats st{0, 0};
   unsigned act = 0;
+  int lo = -1;
   if (p < w1) {
-    int lo = 0, hi = njobs - 1;  // last job with pix0 <= p
+    int hi = njobs - 1;  // last job with pix0 <= p
+    lo = 0;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
       if (jobs[mid].pix0 <= p) lo = mid;
       else hi = mid - 1;
     }
-    const BatchJob& j = jobs[lo];
-    act = trace_pixel(j.m, j.sc, j.cam, j.seed, j.frame, (int)(p - j.pix0), bout[lo].out, nullptr, rec, lo, st);
+  }
+  // one job at a time per warp: the density texture handle must be uniform
+  // across the lanes of a texture fetch (see k_gather_batch)
+  unsigned todo = __ballot_sync(0xffffffffu, p < w1);
+  while (todo) {
+    const int jj = __shfl_sync(0xffffffffu, lo, __ffs(todo) - 1);
+    const bool mine = p < w1 && lo == jj;
+    if (mine) {
+      const BatchJob& j = jobs[jj];
+      act = trace_pixel(j.m, j.sc, j.cam, j.seed, j.frame, (int)(p - j.pix0), bout[jj].out, nullptr, rec, jj, st);
+    }
+    todo &= ~__ballot_sync(0xffffffffu, mine);
   }
   trace_counters(counters, st, act);
 }
 
+// The per-point table of every job (point_table over the job's tables), one
+// block per job, into h0[job * kPtTable].
+template <int SAMP>
+__global__ void k_sphere_h0_batch(const BatchJob* __restrict__ jobs, const float* __restrict__ stencil,
+                                  float* __restrict__ h0) {
+  point_table<SAMP>(jobs[blockIdx.x].tabs, stencil, h0 + (size_t)blockIdx.x * kPtTable);
+}
+
 template <int SAMP>
 __global__ void __launch_bounds__(256, 3) k_gather_batch(const BatchJob* __restrict__ jobs,
-                                                      const float* __restrict__ stencil, Records rec, int cap,
+                                                      const float* __restrict__ stencil,
+                                                      const float* __restrict__ h0, Records rec, int cap,
                                                       float* __restrict__ desc, float* __restrict__ aux) {
   const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned n = min(*rec.count, (unsigned)cap);
-  if (k >= n) return;
-  const BatchJob& j = jobs[rec.job[k]];
-  const F3 pos = f3(rec.pos[3 * (size_t)k], rec.pos[3 * (size_t)k + 1], rec.pos[3 * (size_t)k + 2]);
-  const Frame f = load_frame(rec.frame + 12 * (size_t)k);
-  float4* d = reinterpret_cast<float4*>(desc) + k;
-  const size_t c = (size_t)cap;
-  float4 bv, bs, bh;
-  auto sink = [&](int i, int u, float xv, float xs, float xh) {
-    (&bv.x)[u] = xv;
-    (&bs.x)[u] = xs;
-    (&bh.x)[u] = xh;
-    if (u == 3) {
-      d[(i >> 2) * c] = bv;
-      d[(48 + (i >> 2)) * c] = bs;
-      d[(96 + (i >> 2)) * c] = bh;
+  const bool valid = k < n;
+  const int job = valid ? rec.job[k] : -1;
+  // One job at a time per warp. The texture handles of a fetch must be the
+  // same in all its lanes: with records of two volumes in one warp, fetches
+  // returned wrong texels (measured: batches mixing two volumes in one wave
+  // differed from single renders by up to 48 % in 4 % of the values; with
+  // warp-uniform jobs they agree to 3e-6).
+  unsigned todo = __ballot_sync(0xffffffffu, valid);
+  while (todo) {
+    const int jj = __shfl_sync(0xffffffffu, job, __ffs(todo) - 1);
+    const bool mine = valid && job == jj;
+    if (mine) {
+      const BatchJob& j = jobs[jj];
+      const F3 pos = f3(rec.pos[3 * (size_t)k], rec.pos[3 * (size_t)k + 1], rec.pos[3 * (size_t)k + 2]);
+      const Frame f = load_frame(rec.frame + 12 * (size_t)k);
+      float4* d = reinterpret_cast<float4*>(desc) + k;
+      const size_t c = (size_t)cap;
+      float4 bv, bs, bh;
+      auto sink = [&](int i, int u, float xv, float xs, float xh) {
+        (&bv.x)[u] = xv;
+        (&bs.x)[u] = xs;
+        (&bh.x)[u] = xh;
+        if (u == 3) {
+          d[(i >> 2) * c] = bv;
+          d[(48 + (i >> 2)) * c] = bs;
+          d[(96 + (i >> 2)) * c] = bh;
+        }
+      };
+      gather_fast<SAMP>(j.tabs, stencil, pos, j.sc.L, f, j.sc.alpha, j.sc.g, h0 + (size_t)jj * kPtTable, sink);
+      aux[k] = j.sc.g;
+      aux[c + k] = acosf(dot(f.X, f.LX));
+      aux[2 * c + k] = j.srp.x;
+      aux[3 * c + k] = j.srp.y;
+      aux[4 * c + k] = j.srp.z;
     }
-  };
-  gather_fast<SAMP>(j.tabs, stencil, pos, j.sc.L, f, j.sc.alpha, j.sc.g, nullptr, sink);
-  aux[k] = j.sc.g;
-  aux[c + k] = acosf(dot(f.X, f.LX));
-  aux[2 * c + k] = j.srp.x;
-  aux[3 * c + k] = j.srp.y;
-  aux[4 * c + k] = j.srp.z;
+    todo &= ~__ballot_sync(0xffffffffu, mine);
+  }
 }
 
 __global__ void k_batch_advance(BatchJob* jobs, int n) {
@@ -961,6 +996,7 @@ struct Batch {
   };
   std::vector<HostJob> jobs;
   BatchJob* d_jobs = nullptr;
+  float* d_h0 = nullptr;  // per-job point tables (k_sphere_h0_batch), kPtTable floats each
   BatchOut* d_out = nullptr;
   unsigned long long* counters = nullptr;
   void* scratch = nullptr;
@@ -981,10 +1017,12 @@ struct Batch {
   void release() {
     drop_graph();
     if (d_jobs) cudaFree(d_jobs);
+    if (d_h0) cudaFree(d_h0);
     if (d_out) cudaFree(d_out);
     if (counters) cudaFree(counters);
     if (scratch) cudaFree(scratch);
     d_jobs = nullptr;
+    d_h0 = nullptr;
     d_out = nullptr;
     counters = nullptr;
     scratch = nullptr;
@@ -1010,6 +1048,12 @@ static int batch_launches(Batch& b, const Network* net, cudaStream_t s) {
   const bool hw = b.sampler == MR_SAMPLER_TEXTURE;
   const int nj = (int)b.jobs.size();
   MR_CUDA(cudaMemsetAsync(b.counters, 0, kCounters * sizeof(unsigned long long), s));
+  // the jobs' per-point tables, for the network given to this call
+  if (hw)
+    k_sphere_h0_batch<kSampTex><<<nj, 192, 0, s>>>(b.d_jobs, net->stencil, b.d_h0);
+  else
+    k_sphere_h0_batch<kSampGather><<<nj, 192, 0, s>>>(b.d_jobs, net->stencil, b.d_h0);
+  MR_CUDA(cudaGetLastError());
   for (long long w0 = 0; w0 < b.total; w0 += b.wave) {
     const long long w1 = std::min(b.total, w0 + b.wave);
     MR_CUDA(cudaMemsetAsync(rec.count, 0, sizeof(unsigned), s));
@@ -1018,9 +1062,11 @@ static int batch_launches(Batch& b, const Network* net, cudaStream_t s) {
     MR_CUDA(cudaGetLastError());
     const unsigned ggrid = (unsigned)((w1 - w0 + b.gather_block - 1) / b.gather_block);
     if (hw)
-      k_gather_batch<kSampTex><<<ggrid, b.gather_block, 0, s>>>(b.d_jobs, net->stencil, rec, (int)cap, desc, aux);
+      k_gather_batch<kSampTex><<<ggrid, b.gather_block, 0, s>>>(b.d_jobs, net->stencil, b.d_h0, rec, (int)cap, desc,
+                                                                aux);
     else
-      k_gather_batch<kSampGather><<<ggrid, b.gather_block, 0, s>>>(b.d_jobs, net->stencil, rec, (int)cap, desc, aux);
+      k_gather_batch<kSampGather><<<ggrid, b.gather_block, 0, s>>>(b.d_jobs, net->stencil, b.d_h0, rec, (int)cap,
+                                                                   desc, aux);
     MR_CUDA(cudaGetLastError());
     const long long ccap = (long long)cap;
     int rc;
@@ -1148,10 +1194,13 @@ extern "C" int mr_batch_prepare(mr_batch* h, const mr_network* nh, int64_t wave_
   b.wave = wave_pixels > 0 ? std::min<long long>(wave_pixels, b.total) : std::min<long long>(b.total, 4ll << 20);
   if (b.wave > (1ll << 28)) return set_error(MR_ERR_ARG, "wave of %lld pixels too large", b.wave);
   if (b.d_jobs) cudaFree(b.d_jobs);
+  if (b.d_h0) cudaFree(b.d_h0);
   if (b.d_out) cudaFree(b.d_out);
   b.d_jobs = nullptr;
+  b.d_h0 = nullptr;
   b.d_out = nullptr;
   MR_CUDA(cudaMalloc(&b.d_jobs, hj.size() * sizeof(BatchJob)));
+  MR_CUDA(cudaMalloc(&b.d_h0, hj.size() * kPtTable * sizeof(float)));
   MR_CUDA(cudaMalloc(&b.d_out, ho.size() * sizeof(BatchOut)));
   if (!b.counters) MR_CUDA(cudaMalloc(&b.counters, kCounters * sizeof(unsigned long long)));
   MR_CUDA(cudaMemcpyAsync(b.d_jobs, hj.data(), hj.size() * sizeof(BatchJob), cudaMemcpyHostToDevice, s));

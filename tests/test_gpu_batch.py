@@ -52,8 +52,9 @@ def _single(torch, net, jobs, advance):
     return out
 
 
-@pytest.mark.parametrize("precision,sampler", [(1, 0), (0, 0), (1, 1)])
-def test_batch_matches_single_renders(torch, precision, sampler):
+@pytest.mark.parametrize("precision,sampler,wave",
+                         [(1, 0, 1000), (0, 0, 1000), (1, 1, 1000), (0, 0, 0), (0, 1, 0), (1, 1, 0), (1, 0, 0)])
+def test_batch_matches_single_renders(torch, precision, sampler, wave):
     import internship_b200 as mr
     from internship_b200 import _lib
     L = _lib.load()
@@ -63,8 +64,10 @@ def test_batch_matches_single_renders(torch, precision, sampler):
     _lib.check(L.mr_batch_create(C.byref(b)))
     for (v, p), o in zip(jobs, outs):
         _lib.check(L.mr_batch_add(b, v.handle, C.byref(p), _ptr(o)))
-    # waves of 1000 pixels: every wave mixes jobs, records span wave boundaries
-    _lib.check(L.mr_batch_prepare(b, net.handle, 1000, None))
+    # waves of 1000 pixels: every wave mixes jobs, records span wave
+    # boundaries; wave 0: the whole batch in one wave, where the records of
+    # both volumes share warps
+    _lib.check(L.mr_batch_prepare(b, net.handle, wave, None))
     _lib.check(L.mr_batch_render(b, net.handle, None))
     torch.cuda.synchronize()
     got = [o.cpu().numpy() for o in outs]
@@ -73,7 +76,7 @@ def test_batch_matches_single_renders(torch, precision, sampler):
         assert (r > 0).mean() > 0.05
         # the batched and the single-render gathers are separately compiled
         # kernels of the same source; the compiler may contract a few fp32
-        # expressions differently (measured: <= 2e-6 relative in <= 0.3 % of
+        # expressions differently (measured: <= 3e-6 relative in <= 0.5 % of
         # the values, fp32 exact)
         np.testing.assert_allclose(g, r, rtol=5e-6, atol=1e-7)
     cnt = (C.c_uint64 * 4)()
@@ -150,9 +153,8 @@ def test_batch_autotune_and_errors(torch):
 
 
 def test_large_single_render_matches_waved_batch(torch):
-    """A 512 x 512 single render (its gather reads the per-render table of
-    per-point constants) against the same view through the batched path in
-    waves of 64 Ki pixels (whose gather computes those constants per point)."""
+    """A 512 x 512 single render against the same view through the batched
+    path in waves of 64 Ki pixels (both gathers read a per-point table)."""
     import internship_b200 as mr
     from internship_b200 import _lib, scenes
     from internship_b200.weights import active_random_weights
