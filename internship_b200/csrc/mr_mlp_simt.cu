@@ -1,22 +1,26 @@
 // FP32 radiance-predictor network (core/radiancePredict.cu:370-485 in fp32),
-// in two kernels over tiles of 128 rows.
+// in four kernels over rows (tiles of 128 rows where shared state is tiled).
 //
 // Descriptors are read in chunks of 4 features: (row k, features 4j..4j+3) is
 // the float4 at desc[k*rs + j*cs]; the render path passes chunk-of-4
 // feature-major columns (rs = 4, cs = 4*capacity) so that a warp's 32 loads
 // of one chunk are one coalesced transaction.
 //
-//  * k_simt_trunk (CUDA cores): the two trunks over a shared-memory tile,
+//  * k_simt_trunk (CUDA cores): the main trunk over a shared-memory tile,
 //    column-major (feature f of tile row r at [f*128 + r]). The
-//    squeeze-excitation statistics and gates, the width-8 blocks and LD41 run
-//    per row (one thread per row); the width-16 and width-32 layers (77 % of
-//    the trunk's multiply-adds) run as register-tiled block GEMMs over the
+//    squeeze-excitation statistics and gates and blocks 0 and 1 run per row
+//    (one thread per row); the width-16 and width-32 layers and L81 (89 % of
+//    the kernel's multiply-adds) run as register-tiled block GEMMs over the
 //    tile, starting at the bias and adding the inputs in ascending order as
 //    LinearReLU does, with their weights pre-transposed and double-buffered
 //    in shared memory by cp.async.
-//  * k_tc32_head (tensor cores): the head. LC0 / LC1 / LC2 (62 % of all
+//  * k_light_trunk (CUDA cores): the light-direction trunk and LD41, one
+//    thread per row, weights as kernel parameters.
+//  * k_tc32_head (tensor cores): the head. LC0 / LC1 / LC2 (53 % of all
 //    multiply-adds) as tcgen05 MMAs whose every product is the sum of three
-//    TF32 products (fp32-accurate); gates, LX and the residual pairs per row.
+//    TF32 products (fp32-accurate); gates per row; LC2 outputs to staging.
+//  * k_tc32_tail (CUDA cores): LX, the residual pairs, LX12 and the output,
+//    one thread per row, weights as kernel parameters.
 #include <algorithm>
 #include <cstring>
 #include <vector>

@@ -6,8 +6,11 @@
 //     list with warp-aggregated atomics, inactive ones get the environment.
 //  2. k_gather_fm: per active record, the 192-point multi-scale descriptor
 //     gather (core/radiancePredict.cu:319-368) into feature-major columns.
-//  3. the network body: k_simt_trunk + k_simt_head (fp32, mr_mlp_simt.cu) or k_mlp_tc
-//     (BF16 tcgen05, mr_mlp_tc.cu), which also writes the pixel.
+//  3. the network body: k_simt_trunk, k_light_trunk, k_tc32_head and
+//     k_tc32_tail (fp32, mr_mlp_simt.cu) or k_mlp_tc (BF16 / E4M3 tcgen05,
+//     mr_mlp_tc.cu); the last kernel also writes the pixel.
+// The gather's per-point table (k_sphere_h0) runs on a side stream beside
+// the trace.
 #include <algorithm>
 #include <mutex>
 #include <vector>
