@@ -86,6 +86,36 @@ def test_batch_matches_single_renders(torch, precision, sampler, wave):
     net.close()
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batch_with_distinct_albedo_channels(torch, precision):
+    """A job whose three albedo channels differ (one head per channel; the
+    tensor-core network spills its head input for the further channels) in
+    one wave with a gray job on another volume."""
+    import internship_b200 as mr
+    from internship_b200 import _lib
+    L = _lib.load()
+    jobs, net = _jobs(mr, precision, 0)
+    jobs[2][1].scatter_rate = _lib.f3((0.9, 0.95, 0.99))
+    jobs = [jobs[0], jobs[2]]
+    outs = [torch.full((p.width * p.height * 3,), -1.0, device="cuda") for _, p in jobs]
+    b = C.c_void_p()
+    _lib.check(L.mr_batch_create(C.byref(b)))
+    for (v, p), o in zip(jobs, outs):
+        _lib.check(L.mr_batch_add(b, v.handle, C.byref(p), _ptr(o)))
+    _lib.check(L.mr_batch_prepare(b, net.handle, 0, None))
+    _lib.check(L.mr_batch_render(b, net.handle, None))
+    torch.cuda.synchronize()
+    got = [o.cpu().numpy() for o in outs]
+    ref = _single(torch, net, jobs, 0)
+    for g, r in zip(got, ref):
+        np.testing.assert_allclose(g, r, rtol=5e-6, atol=1e-7)  # as in test_batch_matches_single_renders
+    rgb = ref[1].reshape(-1, 3)
+    lit = rgb.max(1) > 0
+    assert not np.allclose(rgb[lit, 0], rgb[lit, 2])  # the channels differ
+    L.mr_batch_destroy(b)
+    net.close()
+
+
 def test_batch_graph_replays_advance_frames(torch):
     import internship_b200 as mr
     from internship_b200 import _lib

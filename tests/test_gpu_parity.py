@@ -187,7 +187,8 @@ def test_gather_and_predict_match_oracle(mr, torch):
     v.close()
 
 
-def test_neural_render_matches_oracle(mr):
+@pytest.mark.parametrize("albedo", [(0.99, 0.99, 0.99), (0.9, 0.95, 0.99)])
+def test_neural_render_matches_oracle(mr, albedo):
     from internship_b200 import _lib, scenes
     dens = scenes.sphere_density(128)
     v = _volume(mr, dens)
@@ -195,6 +196,7 @@ def test_neural_render_matches_oracle(mr):
     st = mr.builtin_stencil()
     v.SetWeights(w, st)
     p = scenes.make_params(24, 24, 1, rt=_lib.RT_MRPNN)
+    p.scatter_rate = _lib.f3(albedo)  # distinct channels: one head per channel
     gpu = _render(mr, v, p, v.network.handle)
     gm, _ = _mips_from(v)
     tr = np.concatenate([v.read(_lib.READ_TR, k) for k in range(8)])

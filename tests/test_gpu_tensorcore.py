@@ -102,6 +102,36 @@ def test_bf16_network_three_albedo_channels():
     assert not np.allclose(ref[:, 0], ref[:, 2])
 
 
+def test_fp32_network_albedo_channel_patterns():
+    """fp32 network rows whose three albedo channels are equal, pairwise
+    equal in each position, or all distinct, mixed within 128-row tiles: the
+    head computes a further channel for a tile when one of its rows needs it,
+    and the tail evaluates per row only the channels that row needs."""
+    import internship_b200 as mr
+    from internship_b200 import _lib
+    from internship_b200.weights import active_random_weights
+    w = active_random_weights(1)
+    n = 700
+    desc, aux = _descriptors(n, 8)
+    a, b, c = 0.9, 0.95, 0.99
+    patterns = np.array([[c, c, c], [a, b, c], [a, a, c], [a, c, c], [c, a, c], [b, b, b]], np.float32)
+    rng = np.random.default_rng(9)
+    pick = rng.integers(0, len(patterns), n)
+    pick[:128] = 0  # one tile with a single channel only
+    sr = patterns[pick] / np.float32(1.001)
+    aux[:, 2:5] = (sr * sr) * (sr * sr)
+    ref = orc.predict(w, desc, aux)
+    got = _predict(mr, w, desc, aux, _lib.PREC_FP32)
+    assert (ref > 0).mean() > 0.9
+    np.testing.assert_allclose(got, ref, rtol=1e-4, atol=1e-6)
+    for k in range(len(patterns)):  # rows with equal channels give equal outputs
+        rows = pick == k
+        sp = aux[rows, 2:5]
+        for i, j in ((0, 1), (1, 2), (0, 2)):
+            same = sp[:, i] == sp[:, j]
+            assert np.array_equal(got[rows][same, i] / sp[same, i], got[rows][same, j] / sp[same, j])
+
+
 @pytest.mark.skipif(not ref_py.available(), reason="oracle/_ref not built")
 def test_bf16_network_with_reference_weights():
     import internship_b200 as mr
