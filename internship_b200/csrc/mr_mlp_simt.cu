@@ -173,10 +173,11 @@ struct TrunkArgs {
   const unsigned* __restrict__ count;  // device row count (render path) or null
 };
 
-// Trunk outputs per row, handed from the trunk kernel to the head kernel:
-// comb[0..120) (the L81 / LD41 outputs before gating) and fin[0..16) (the
-// LSEFin1 sums over pool[0..74), without the albedo term), 136 values in
-// chunks of 4: chunk c of row k is the float4 at t[k*rs + c*cs].
+// Trunk outputs per row, handed from the trunk kernels to the head kernel:
+// comb[0..120) (the L81 / LD41 outputs before gating), fin[0..16) (the
+// LSEFin1 sums over pool[0..74), without the albedo term) and the head's
+// gates of albedo channel 0 (6 + 2 unused, then the 8 LGGS outputs), 152
+// values in chunks of 4: chunk c of row k is the float4 at t[k*rs + c*cs].
 struct TrunkOut {
   float* t;
   long long rs, cs;
@@ -545,7 +546,9 @@ __global__ void __launch_bounds__(kTile, 3) k_simt_trunk(TrunkArgs a, TrunkOut t
 struct LightParams {
   float se[4][kSeFloats];
   float dense[15][72];  // LD01, LD11, LD21, LD31, LD41; per block branches density, transmittance, phase
+  float head[144];      // the head-row image's first 144 floats: LSEFin2, LSEFin1's albedo column, LGGS W, B
 };
+static_assert(sizeof(LightParams) + sizeof(TrunkArgs) + sizeof(TrunkOut) <= 32000, "kernel parameter space");
 
 void light_param_image(const float* w, const std::vector<float>& img, std::vector<float>& out) {
   out.assign(sizeof(LightParams) / sizeof(float), 0.0f);
@@ -556,6 +559,7 @@ void light_param_image(const float* w, const std::vector<float>& img, std::vecto
                        MR_W_LD41W, MR_W_LD_Tr41W, MR_W_LD_Hg41W};
   for (int d = 0; d < 15; ++d)
     std::copy(w + wt.off[ids[d]], w + wt.off[ids[d]] + 72, out.begin() + 4 * kSeFloats + 72 * d);
+  std::copy(img.begin() + kHeadRowOff, img.begin() + kHeadRowOff + 144, out.begin() + 4 * kSeFloats + 15 * 72);
 }
 
 // 8 -> 8 layer, bias first then ascending inputs (dense1's order), weights
@@ -648,8 +652,36 @@ __device__ __forceinline__ void light_row(const TrunkArgs& a, const TrunkOut& to
   for (int c = 0; c < 4; ++c) {  // LSEFin1 sums: the main trunk's (with the g, gamma columns) plus these blocks'
     float4* f = reinterpret_cast<float4*>(orow + (30 + c) * to.cs);
     const float4 q = *f;
-    *f = make_float4(q.x + fin[4 * c], q.y + fin[4 * c + 1], q.z + fin[4 * c + 2], q.w + fin[4 * c + 3]);
+    fin[4 * c] = q.x + fin[4 * c];
+    fin[4 * c + 1] = q.y + fin[4 * c + 1];
+    fin[4 * c + 2] = q.z + fin[4 * c + 2];
+    fin[4 * c + 3] = q.w + fin[4 * c + 3];
+    *f = make_float4(fin[4 * c], fin[4 * c + 1], fin[4 * c + 2], fin[4 * c + 3]);
   }
+  // the head's gates of albedo channel 0 (radiancePredict.cu:439-452), in
+  // k_tc32_head's arithmetic: sep[0..6) in chunks 34..35, LGGS x8 in 36..37
+  const float* H = P.head;
+  const float sc = __ldg(ax + 2 * a.afs);
+  float sew[16], sep[6], x8[8];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) sew[j] = relu0(fin[j] + sc * H[96 + j]);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    float acc = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) acc += sew[j] * H[i * 16 + j];
+    sep[i] = 1.0f / (1.0f + expf(-acc));
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {  // LGGS 3 -> 8, bias after the sum
+    float acc = g * H[112 + 3 * i] + gamma * H[112 + 3 * i + 1] + sc * H[112 + 3 * i + 2];
+    acc += H[136 + i];
+    x8[i] = relu0(acc);
+  }
+  *reinterpret_cast<float4*>(orow + 34 * to.cs) = make_float4(sep[0], sep[1], sep[2], sep[3]);
+  *reinterpret_cast<float4*>(orow + 35 * to.cs) = make_float4(sep[4], sep[5], 0.0f, 0.0f);
+  *reinterpret_cast<float4*>(orow + 36 * to.cs) = make_float4(x8[0], x8[1], x8[2], x8[3]);
+  *reinterpret_cast<float4*>(orow + 37 * to.cs) = make_float4(x8[4], x8[5], x8[6], x8[7]);
 }
 
 // One row per thread, no loop (see k_tc32_tail).
@@ -825,7 +857,7 @@ __device__ __forceinline__ void prefetch_tile(const HeadArgs& a, int tile, int n
   if (r0 >= n) return;
   const int rows = (int)min((long long)kHeadRows, n - r0);
   if (a.trs == 4) {
-    for (int c = 0; c < 34; ++c)
+    for (int c = 0; c < 38; ++c)
       asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a.t + r0 * 4 + c * a.tcs), "r"(rows * 16)
                    : "memory");
   } else if (a.tcs == 4 && a.trs % 4 == 0) {
@@ -893,6 +925,14 @@ __global__ void __launch_bounds__(kHeadThreads, 1) k_tc32_head(HeadArgs a) {
       const float4 q = __ldg(reinterpret_cast<const float4*>(trow + (30 + c) * a.tcs));
       fin[4 * c] = q.x; fin[4 * c + 1] = q.y; fin[4 * c + 2] = q.z; fin[4 * c + 3] = q.w;
     }
+    // channel 0's gates, computed by k_light_trunk: sep in chunks 34..35, LGGS in 36..37
+    const float4 gs0 = __ldg(reinterpret_cast<const float4*>(trow + 34 * a.tcs));
+    const float4 gs1 = __ldg(reinterpret_cast<const float4*>(trow + 35 * a.tcs));
+    float4 gx[2] = {make_float4(0.0f, 0.0f, 0.0f, 0.0f), make_float4(0.0f, 0.0f, 0.0f, 0.0f)};
+    if (half) {  // LC0 input columns 120..127 belong to half 1
+      gx[0] = __ldg(reinterpret_cast<const float4*>(trow + 36 * a.tcs));
+      gx[1] = __ldg(reinterpret_cast<const float4*>(trow + 37 * a.tcs));
+    }
     if (threadIdx.x == 0) prefetch_tile(a, tile + gridDim.x, n);  // the next tile's trunk outputs -> L2
     tc_fence_before();  // the previous tile's TMEM reads
     const bool need1 = __syncthreads_or(valid && srp[1] != srp[0]);
@@ -902,8 +942,8 @@ __global__ void __launch_bounds__(kHeadThreads, 1) k_tc32_head(HeadArgs a) {
       if ((ch == 1 && !need1) || (ch == 2 && !need2)) continue;
       const float sc = ch == 0 ? srp[0] : ch == 1 ? srp[1] : srp[2];
       // gates of this channel (LGGS, LSEFin1's albedo column, LSEFin2)
-      float sep[6];
-      {
+      float sep[6] = {gs0.x, gs0.y, gs0.z, gs0.w, gs1.x, gs1.y};
+      if (ch > 0) {
         float sew[16];
 #pragma unroll
         for (int j = 0; j < 16; j += 4) {
@@ -935,6 +975,9 @@ __global__ void __launch_bounds__(kHeadThreads, 1) k_tc32_head(HeadArgs a) {
           const float4 q = tin[i];
           const float s = c < 24 ? sep[c >> 3] : sep[3 + ((c - 24) >> 1)];
           put_split4(Ahi, Alo, r, 4 * c, 128, q.x * s, q.y * s, q.z * s, q.w * s);
+        } else if (ch == 0) {
+          const float4 q = gx[c - 30];
+          put_split4(Ahi, Alo, r, 4 * c, 128, q.x, q.y, q.z, q.w);
         } else {
           float x[4];
 #pragma unroll
@@ -1119,7 +1162,7 @@ int* mlp_error_word(const Network* net);  // mr_mlp_tc.cu
 
 // Trunk kernel then head kernel. `tout` receives the trunk outputs (TrunkOut
 // layout with strides trs / tcs): the render path passes its own descriptor
-// columns, whose first 34 chunks of a row are no longer needed once that row's
+// columns, whose first 38 chunks of a row are no longer needed once that row's
 // trunks are done.
 int launch_mlp_simt(const Network* net, const float* desc, const float* aux, long long rs, long long cs,
                     long long ars, long long afs, int n, const unsigned* count, float* out, const int* pix,

@@ -686,7 +686,7 @@ static int neural_passes(Volume* v, const Network* net, const mr_render_params* 
     rc = launch_mlp_tc(net, desc, aux, 4, 4 * cap, 1, cap, (int)npx, dev_rgb, rec.pix, rec.trph, rec.count,
                        to_f3(p->light_color), to_f3(p->scatter_rate), spill, p->precision == MR_PREC_FP8, s);
   else
-    // trunk outputs over the row's first 34 descriptor chunks, the head's LC2
+    // trunk outputs over the row's first 38 descriptor chunks, the head's LC2
     // outputs over chunks 48..71 (all consumed by the trunk)
     rc = launch_mlp_simt(net, desc, aux, 4, 4 * cap, 1, cap, (int)npx, rec.count, dev_rgb, rec.pix, rec.trph,
                          to_f3(p->light_color), to_f3(p->scatter_rate), s, nullptr, nullptr, desc, 4, 4 * cap,
@@ -805,14 +805,14 @@ extern "C" int mr_radiance_predict(const mr_network* nh, int32_t precision, cons
     return rc;
   }
   if (precision != MR_PREC_FP32) return set_error(MR_ERR_ARG, "unknown precision %d", precision);
-  // the caller's descriptors stay untouched: trunk outputs (136) and the
+  // the caller's descriptors stay untouched: trunk outputs (152) and the
   // head's LC2 outputs (96) of a row go to a temporary
   cudaStream_t s = (cudaStream_t)stream;
   float* tout = nullptr;
-  cudaError_t e = cudaMallocAsync(&tout, (size_t)n * 232 * sizeof(float), s);
+  cudaError_t e = cudaMallocAsync(&tout, (size_t)n * 248 * sizeof(float), s);
   if (e != cudaSuccess) return set_error(MR_ERR_NOMEM, "trunk buffer: %s", cudaGetErrorString(e));
   int rc = launch_mlp_simt(&nh->n, dev_desc, dev_aux, 576, 4, 5, 1, n, nullptr, dev_out, nullptr, nullptr,
-                           f3(1, 1, 1), f3(1, 1, 1), s, nullptr, nullptr, tout, 232, 4, tout + 136, 232, 4);
+                           f3(1, 1, 1), f3(1, 1, 1), s, nullptr, nullptr, tout, 248, 4, tout + 152, 248, 4);
   MR_CUDA(cudaFreeAsync(tout, s));
   return rc;
 }
