@@ -715,35 +715,6 @@ struct HeadArgs {
   long long srs, scs;
 };
 
-// Half of a 16 -> 16 layer: outputs 8h..8h+7 of ReLU(B + W x), bias first,
-// ascending inputs.
-__device__ __forceinline__ void dense16_half(const float (&x)[16], float (&y)[8], const float* __restrict__ W,
-                                             const float* __restrict__ B, int h) {
-#pragma unroll
-  for (int q = 0; q < 8; ++q) {
-    float acc = __ldg(B + 8 * h + q);
-#pragma unroll
-    for (int j = 0; j < 16; j += 4) {
-      const float4 v = ldg4(W + (8 * h + q) * 16 + j);
-      acc += x[j] * v.x;
-      acc += x[j + 1] * v.y;
-      acc += x[j + 2] * v.z;
-      acc += x[j + 3] * v.w;
-    }
-    y[q] = relu0(acc);
-  }
-}
-
-// The full 16-vector from the two halves held by lanes l and l ^ 16.
-__device__ __forceinline__ void join16(const float (&mine)[8], float (&full)[16], int h) {
-#pragma unroll
-  for (int q = 0; q < 8; ++q) {
-    const float other = __shfl_xor_sync(0xffffffffu, mine[q], 16);
-    full[q] = h ? other : mine[q];
-    full[8 + q] = h ? mine[q] : other;
-  }
-}
-
 // ---- head on the tensor cores (fp32-accurate) ---------------------------------------
 // LC0 / LC1 / LC2 as M = 128 tcgen05 MMAs of kind::tf32 with FP32 accumulators
 // in TMEM: every product is the sum of three TF32 products (A_hi W_hi + A_hi
@@ -882,7 +853,6 @@ __global__ void __launch_bounds__(kHeadThreads, 1) k_tc32_head(HeadArgs a) {
   if ((int)blockIdx.x >= ntiles) return;  // block-uniform
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int r = 32 * (warp & 3) + lane, half = warp >> 2;  // TMEM lane mapping
-  const float* __restrict__ w = a.w;
   const float* __restrict__ hr = a.wt + kHeadRowOff;
   const float* __restrict__ bias = a.wt + kTcBiasOff;
   const uint32_t done = smem_u32(mb + 2 * kTcSlots);
