@@ -183,7 +183,7 @@ def test_batch_autotune_and_errors(torch):
 
 
 def test_large_single_render_matches_waved_batch(torch):
-    """A 512 x 512 single render against the same view through the batched
+    """A 1280 x 1280 single render against the same view through the batched
     path in waves of 64 Ki pixels (both gathers read a per-point table)."""
     import internship_b200 as mr
     from internship_b200 import _lib, scenes
@@ -194,8 +194,8 @@ def test_large_single_render_matches_waved_batch(torch):
     v.SetDatas(cloud_np.cloud(128, 5))
     v.Update()
     net = mr.Network(active_random_weights(1), mr.builtin_stencil())
-    p = scenes.make_params(512, 512, 1, rt=_lib.RT_MRPNN, precision=0, sampler=0, alpha=48.0)
-    out = torch.full((512 * 512 * 3,), -1.0, device="cuda")
+    p = scenes.make_params(1280, 1280, 1, rt=_lib.RT_MRPNN, precision=0, sampler=0, alpha=48.0)
+    out = torch.full((1280 * 1280 * 3,), -1.0, device="cuda")
     b = C.c_void_p()
     _lib.check(L.mr_batch_create(C.byref(b)))
     _lib.check(L.mr_batch_add(b, v.handle, C.byref(p), _ptr(out)))
@@ -204,6 +204,11 @@ def test_large_single_render_matches_waved_batch(torch):
     torch.cuda.synchronize()
     got = out.cpu().numpy()
     ref = _single(torch, net, [(v, p)], 0)[0]
+    cnt = (C.c_uint64 * 4)()
+    _lib.check(L.mr_volume_counters(v.handle, cnt))
+    # more active records than the single render's resident gather grid has
+    # threads (148 SMs x 6 blocks x 128): its threads stride over records
+    assert cnt[3] > 148 * 6 * 128, cnt[3]
     assert (ref > 0).mean() > 0.05
     np.testing.assert_allclose(got, ref, rtol=5e-6, atol=1e-7)
     L.mr_batch_destroy(b)
