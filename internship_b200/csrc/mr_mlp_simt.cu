@@ -806,16 +806,20 @@ __device__ __forceinline__ void put_split4(float* ahi, float* alo, int r, int k,
 template <int N>
 __device__ __forceinline__ void tc_epi_split(uint32_t tl, const float* __restrict__ bias, float* ahi, float* alo, int r,
                                              int h) {
+  static_assert(N % 64 == 0, "pairs of 16-column loads per thread");
 #pragma unroll
-  for (int q = 0; q < N / 32; ++q) {
-    const int c0 = h * (N / 2) + 16 * q;
-    float v[16];
-    tmem_ld16(tl + c0, v);
+  for (int q = 0; q < N / 32; q += 2) {  // two TMEM loads under one wait
+    float v[2][16];
+    tmem_ld16x2(tl + h * (N / 2) + 16 * q, tl + h * (N / 2) + 16 * (q + 1), v[0], v[1]);
 #pragma unroll
-    for (int i = 0; i < 16; i += 4) {
-      const float4 b = ldg4(bias + c0 + i);
-      put_split4(ahi, alo, r, c0 + i, N, relu0(v[i] + b.x), relu0(v[i + 1] + b.y), relu0(v[i + 2] + b.z),
-                 relu0(v[i + 3] + b.w));
+    for (int p = 0; p < 2; ++p) {
+      const int c0 = h * (N / 2) + 16 * (q + p);
+#pragma unroll
+      for (int i = 0; i < 16; i += 4) {
+        const float4 b = ldg4(bias + c0 + i);
+        put_split4(ahi, alo, r, c0 + i, N, relu0(v[p][i] + b.x), relu0(v[p][i + 1] + b.y), relu0(v[p][i + 2] + b.z),
+                   relu0(v[p][i + 3] + b.w));
+      }
     }
   }
 }
