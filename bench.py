@@ -129,7 +129,7 @@ TRAINED = os.path.join(ROOT, "internship_b200", "data", "mrpnn_trained.npy")
 # k_tc32_head + k_tc32_tail),
 # per density fetch for the trace. A launch's traffic = this figure x the
 # launch's units.
-TRAFFIC_PER_UNIT = {"k_simt": 3356.7, "k_mlp_tc": 2542.6, "k_gather_fm_exact": 2469.8,
+TRAFFIC_PER_UNIT = {"k_simt": 3356.7, "k_mlp_tc": 2542.6, "k_gather_fm_exact": 2490.3,
                     "k_gather_fm_texture": 2447.0, "k_nn_trace": 137.2}
 SIMT_KERNELS = ("k_simt_trunk + k_light_trunk + k_tc32_head + k_tc32_tail (fp32 network: CUDA-core trunks, "
                 "tcgen05 head with fp32-accurate three-term TF32 products, CUDA-core tail)")
