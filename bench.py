@@ -13,7 +13,18 @@ Multi-GPU runs are independent replicas (each rank renders its own frames;
 no collective on the data path); `value` is the frames of all ranks divided by
 the slowest rank's device time. `--impl reference` times the CPU
 restatement of the reference path (the oracle, OpenMP on all host cores) on
-a bounded sample of rows of the same frame.
+a bounded sample of rows of the same frame, with the same weights, stencil
+and tables; it loads no part of the library (the weights and the stencil come
+from the oracle, the render request from internship_b200/scenes.py loaded as
+a plain file). Both arms also report the delta-tracking baseline of the
+sphere scene (128^3, 256 x 256, 64 spp) on the host cores.
+
+Extra legs of the default run: the same frame with the texture sampler and
+with the BF16 / FP8 tensor-core networks; the sphere scene's delta tracking on
+the GPU (samples/s, density fetches/s, against the measured L2 read
+bandwidth); an L2 / HBM read-bandwidth probe; batched serving; neural vs delta
+tracking at matched RMSE against a 16384-spp FP64 image at 1920 x 1080; a
+reduced training run (labels, training throughput, held-out error).
 """
 import argparse
 import ctypes as C
@@ -33,7 +44,44 @@ METRIC = "frames/s at 1080p, neural vs delta-tracking at matched RMSE vs 16k-spp
 WIDTH, HEIGHT, RES = 1920, 1080, 512
 FLOP_PER_PIXEL = 97072  # 48,536 MAC of the network per active pixel and albedo channel
 WORKLOAD = ("neural (MRPNN) render 1920x1080, 1 spp, 512^3 Perlin-fBm cloud (6 oct, f0 4, lac 2, gain 0.5, "
-            "thr 0.45, radial falloff), fp32 network, Xavier(seed 1) weights, alpha 64, albedo 0.99, g 0.857")
+            "thr 0.45, radial falloff), fp32 network, Xavier(seed 1) weights, reference stencil, alpha 64, "
+            "albedo 0.99, g 0.857")
+
+
+def config_dict():
+    """The `config` of both arms' lines (identical by construction)."""
+    return {"workload": WORKLOAD, "frame": "%dx%d" % (WIDTH, HEIGHT), "volume": "%d^3" % RES,
+            "sampler": "exact fp32 trilinear", "network": "fp32",
+            "l2": "flushed between steps (256 MiB write outside the timed events)"}
+
+
+def load_scenes():
+    """internship_b200/scenes.py as a plain module (no package import, so no
+    library is loaded)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("mr_scenes_plain", os.path.join(ROOT, "internship_b200", "scenes.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+# the delta-tracking baseline scene: 128^3 sphere, 256 x 256, 64 spp
+DT_W, DT_H, DT_SPP = 256, 256, 64
+
+
+def cpu_delta_tracking():
+    """The oracle's delta tracker (CalculateRadiance restated) on the sphere
+    scene, OpenMP over rows on all host cores: the whole 256 x 256 x 64 image."""
+    from oracle import orc
+    sc = load_scenes()
+    dens, p = sc.sphere_density(128), sc.make_params(DT_W, DT_H, DT_SPP, params_cls=orc.RenderParams)
+    t0 = time.perf_counter()
+    _, _, cnt = orc.render_pt(dens, float(dens.max()), p)
+    dt = time.perf_counter() - t0
+    n = DT_W * DT_H * DT_SPP
+    return {"value": n / dt, "unit": "samples/s", "cores": orc.nthreads(), "kind": "port",
+            "seconds": dt, "density_fetches_per_s": float(cnt[0]) / dt,
+            "sample": "the whole sphere scene: 128^3, 256x256, 64 spp, 512 bounces (oracle, OpenMP)"}
 
 
 def peaks():
@@ -84,19 +132,22 @@ class ClockSampler:
 
 
 def run_reference(args, rank):
-    """CPU restatement (oracle) of the reference path on the host cores."""
+    """CPU restatement (oracle) of the reference path on the host cores: the
+    neural render of the benchmark frame, a bounded sample of rows per step,
+    with the benchmark's weights, stencil and tables. Loads no part of the
+    library."""
     if rank != 0:
         return
-    from internship_b200 import scenes, xavier_weights, builtin_stencil
     from oracle import orc
+    sc = load_scenes()
     threads = orc.nthreads()
     dens = orc.cloud(RES, 7)
     md, mips, _ = orc.build_mips(dens)
-    p = scenes.cloud_scene_params(WIDTH, HEIGHT)
+    p = sc.cloud_scene_params(WIDTH, HEIGHT, params_cls=orc.RenderParams)
     L = np.array([p.light_dir.x, p.light_dir.y, p.light_dir.z], np.float32)
     tr = orc.build_tr(mips, p.alpha, L)
     lut = orc.build_hglut(p.g, p.seed)
-    w, st = xavier_weights(1), builtin_stencil()
+    w, st = orc.xavier_weights(1), orc.reference_stencil()
     rows_per_step = 16
     rows = np.linspace(0, HEIGHT - 1, rows_per_step * (args.steps + args.warmup)).astype(int)
     times = []
@@ -114,9 +165,11 @@ def run_reference(args, rank):
     line = {"metric": METRIC, "value": fps, "unit": "frames/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "parallelism": "host cores (OpenMP)"},
+            "data": "synthetic", "config": config_dict(),
             "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": threads, "kind": "port",
-                             "sample": "%d of %d rows per step, rows spread over the frame" % (rows_per_step, HEIGHT)},
+                             "sample": "%d of %d rows per step, rows spread over the frame (host cores, OpenMP)"
+                                       % (rows_per_step, HEIGHT)},
+            "delta_tracking": cpu_delta_tracking(),
             "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -141,13 +194,12 @@ FP32_FRAME_KERNELS = ("k_sphere_h0", "k_nn_trace", "k_gather_fm", "k_simt_trunk"
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
 
-def matched_rmse(v, p, sp, oracle_spp=16384, small=(480, 270)):
+def matched_rmse(v, p, sp, oracle_spp=16384, small=None):
     """Neural vs delta tracking at matched RMSE against an FP64-accumulated
     `oracle_spp` delta-tracking image of the same view.
 
-    Errors are measured at `small` resolution (same camera; every pixel of it
-    covers 4 x 4 pixels of the 1080p frame) and converted into 1080p frames/s:
-    delta tracking is unbiased, so its RMSE at s spp is c / sqrt(s) with c
+    Errors are measured at the frame's own resolution (or at `small`, same
+    camera) and converted into frames/s: delta tracking is unbiased, so its RMSE at s spp is c / sqrt(s) with c
     fitted over s = 1..64; the matched spp is s* = (c / RMSE_neural)^2 and the
     delta-tracking frame rate at matched RMSE is 1 / (s* t1), t1 = the measured
     time of one 1-spp 1080p delta-tracking frame. The neural form uses the
@@ -160,8 +212,8 @@ def matched_rmse(v, p, sp, oracle_spp=16384, small=(480, 270)):
     if not os.path.exists(TRAINED):
         return {"unavailable": "no trained weights at internship_b200/data/mrpnn_trained.npy"}
     w_tr = np.load(TRAINED)
-    net = mr.Network(w_tr, mr.builtin_stencil())
-    W, H = small
+    net = mr.Network(w_tr, mr.spiral_stencil())  # the shipped weights were trained on the spiral stencil
+    W, H = small if small else (p.width, p.height)
     q = _lib.RenderParams.from_buffer_copy(p)
     q.width, q.height = W, H
     npx = W * H * 3
@@ -257,8 +309,9 @@ def batched_serving(replays=10, seed=11):
     sp = C.c_void_p(stream.cuda_stream)
     torch.cuda.synchronize()
     rng = np.random.default_rng(seed)
-    w = np.load(TRAINED) if os.path.exists(TRAINED) else mr.xavier_weights(1)
-    net = mr.Network(w, mr.builtin_stencil())
+    trained = os.path.exists(TRAINED)
+    w = np.load(TRAINED) if trained else mr.xavier_weights(1)
+    net = mr.Network(w, mr.spiral_stencil() if trained else mr.builtin_stencil())
     vols, outs, frames = [], [], []
     b = C.c_void_p()
     _lib.check(L.mr_batch_create(C.byref(b)))
@@ -322,6 +375,95 @@ def batched_serving(replays=10, seed=11):
             "replays": replays, "graph": "one CUDA graph per batch frame", "setup_s": t_setup}
 
 
+def memory_probe():
+    """Read bandwidth of L2 (a 24 MiB buffer, resident after the first pass)
+    and of HBM (a 4 GiB buffer) through mr_stream_read_probe: 16-byte loads
+    that bypass L1, timed with events on the launching stream."""
+    import torch
+    from internship_b200 import _lib
+    L = _lib.load()
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    sink = torch.zeros(1, dtype=torch.int32, device="cuda")
+    out = {}
+    for name, mib, passes in (("l2", 24, 400), ("hbm", 4096, 3)):
+        buf = torch.ones(mib * 1024 * 1024 // 4, device="cuda")
+        nbytes = buf.numel() * 4
+        for _ in range(2):
+            _lib.check(L.mr_stream_read_probe(C.c_void_p(buf.data_ptr()), nbytes, passes, C.c_void_p(sink.data_ptr()),
+                                              sp))
+        best = 0.0
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            _lib.check(L.mr_stream_read_probe(C.c_void_p(buf.data_ptr()), nbytes, passes,
+                                              C.c_void_p(sink.data_ptr()), sp))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            best = max(best, nbytes * passes / (e0.elapsed_time(e1) / 1e3) / 1e9)
+        out[name + "_read_gbs"] = best
+        del buf
+    out["method"] = "mr_stream_read_probe: ld.global.cg 16-byte loads, 24 MiB x 400 passes (L2), 4 GiB x 3 (HBM); best of 5"
+    return out
+
+
+def gpu_delta_tracking(l2_gbs, steps=10):
+    """Delta tracking of the sphere scene on the GPU (128^3, 256 x 256, 64 spp,
+    512 bounces, unit light): samples/s and density fetches/s, the fetch
+    stream's algorithmic bytes (32 B per trilinear fetch) against the
+    measured L2 read bandwidth (the 8 MiB grid stays in L2)."""
+    import torch
+    import internship_b200 as mr
+    from internship_b200 import _lib, scenes
+    L = _lib.load()
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    dens, p = scenes.sphere_scene(DT_W, DT_H, DT_SPP)
+    v = mr.VolumeRender(128)
+    v.SetDatas(dens)
+    v.Update()
+    out = torch.empty(DT_W * DT_H * 3, device="cuda")
+    for k in range(3):
+        p.sample_offset = 1000 * k
+        _lib.check(L.mr_render(v.handle, None, C.byref(p), C.c_void_p(out.data_ptr()), sp))
+    torch.cuda.synchronize()
+    ms, fetches = 0.0, 0
+    cnt = (C.c_uint64 * 4)()
+    for k in range(steps):
+        p.sample_offset = 10000 + DT_SPP * k
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _lib.check(L.mr_render(v.handle, None, C.byref(p), C.c_void_p(out.data_ptr()), sp))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+        _lib.check(L.mr_volume_counters(v.handle, cnt))
+        fetches += int(cnt[0])
+    v.close()
+    sec = ms / 1e3
+    n = steps * DT_W * DT_H * DT_SPP
+    ach = fetches * 32.0 / sec / 1e9
+    return {"workload": "delta tracking, 128^3 sphere (alpha 64, albedo 0.99, g 0.857), 256x256, 64 spp, "
+                        "512 bounces", "kernel": "k_delta_track",
+            "samples_per_s": n / sec, "density_fetches_per_s": fetches / sec, "ms_per_frame": ms / steps,
+            "frames": steps,
+            "roofline": {"bound": "l2", "achieved": ach, "peak": l2_gbs, "unit": "GB/s", "frac": ach / l2_gbs,
+                         "peak_source": "measured in this run (mr_stream_read_probe, 24 MiB)",
+                         "algorithmic_bytes": "32 B per trilinear density fetch"}}
+
+
+def training_leg(configs=8, samples=400_000, spp=1024, epochs=20):
+    """Reduced configuration-4 run of the learned part: labels from the
+    project's delta tracker on seeded fBm clouds (FP64 sums), training with
+    the hand-written kernels, held-out error with and without the network."""
+    from internship_b200 import train
+    _, rep = train.run(configs=configs, samples=samples, spp=spp, bounces=512, epochs=epochs, batch=65536, lr=1e-3)
+    rep["workload"] = ("%d seeded fBm clouds (128^3 / 256^3 / 512^3), alpha 16-256, albedo 0.9-1.0, g 0.7-0.9, "
+                       "%d rows, %d spp per label, %d epochs (configuration 4 reduced: 32 clouds, 5 M rows, "
+                       "4096 spp)" % (configs, samples, spp, epochs))
+    return rep
+
+
 def cpu_baseline_sample(v, dens_dev, p, w, st):
     """Bounded sample of the same frame on the oracle (all host cores)."""
     from internship_b200 import _lib
@@ -349,6 +491,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-rmse", action="store_true", help="skip the matched-RMSE comparison")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-serving measurement")
+    ap.add_argument("--no-train", action="store_true", help="skip the reduced training run")
     ap.add_argument("--frame", default=None,
                     help="WxH instead of 1920x1080: a smaller case for profiler captures, not a bench line")
     args = ap.parse_args()
@@ -483,6 +626,8 @@ def main():
     serial_fps = replicas.throughput(args.steps, world, serial_ms)
 
     hbm, bf16, src = peaks()
+    probe = memory_probe()
+    l2 = probe["l2_read_gbs"]
     trace_ms, gather_ms, mlp_ms32 = head["stage"][1], head["stage"][2], head["stage"][6]
     # algorithmic bytes: trace = density fetches x 32 B (8 fp32 texels);
     # gather = 192 + 192 trilinear fetches x 32 B + 383 bilinear x 16 B + the
@@ -492,8 +637,8 @@ def main():
     stages = {
         "nn_trace": {"bound": "hbm", "kernel": "k_nn_trace", "ms": trace_ms,
                      "achieved": trace_bytes / (trace_ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s"},
-        "nn_gather": {"bound": "hbm", "kernel": "k_gather_fm<kSampGather> (exact sampler, texture gathers)", "ms": gather_ms,
-                      "achieved": gather_bytes / (gather_ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s"},
+        "nn_gather": {"bound": "l2", "kernel": "k_gather_fm<kSampGather> (exact sampler, texture gathers)",
+                      "ms": gather_ms, "achieved": gather_bytes / (gather_ms / 1e3) / 1e9, "peak": l2, "unit": "GB/s"},
         "nn_network": {"bound": "tensor", "kernel": SIMT_KERNELS, "ms": mlp_ms32,
                        "achieved": FLOP_PER_PIXEL * active / (mlp_ms32 / 1e3) / 1e12, "peak": bf16,
                        "unit": "TFLOP/s"},
@@ -501,6 +646,7 @@ def main():
     for s_ in stages.values():
         s_["frac"] = s_["achieved"] / s_["peak"]
         s_["peak_source"] = src
+    stages["nn_gather"]["peak_source"] = "measured in this run (L2 read probe, 24 MiB)"
     stages["nn_trace"]["traffic"] = TRAFFIC_PER_UNIT["k_nn_trace"] * fetches
     stages["nn_gather"]["traffic"] = TRAFFIC_PER_UNIT["k_gather_fm_exact"] * active
     stages["nn_network"]["traffic"] = TRAFFIC_PER_UNIT["k_simt"] * active
@@ -519,8 +665,8 @@ def main():
             "value": replicas.throughput(args.steps, world, lg["ms"]), "unit": "frames/s",
             "ms_per_step": lg["ms"] / args.steps,
             "stages_ms_per_step": {"nn_trace": lg["stage"][1], "nn_gather": g_ms, "nn_network": m_ms},
-            "gather": {"bound": "hbm", "achieved": lg["active"] * (384 * 32 + 383 * 16 + 581 * 4) / (g_ms / 1e3) / 1e9,
-                       "peak": hbm, "unit": "GB/s"},
+            "gather": {"bound": "l2", "achieved": lg["active"] * (384 * 32 + 383 * 16 + 581 * 4) / (g_ms / 1e3) / 1e9,
+                       "peak": l2, "unit": "GB/s"},
             "network": {"bound": "tensor",
                         "kernel": ("k_mlp_tc (tcgen05 %s network)" % ("E4M3" if name.startswith("fp8") else "BF16"))
                         if tc else SIMT_KERNELS,
@@ -530,10 +676,8 @@ def main():
     line = {"metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "frame": "%dx%d" % (WIDTH, HEIGHT), "volume": "%d^3" % RES,
-                       "sampler": "exact fp32 trilinear",
-                       "l2": "flushed between steps (256 MiB write outside the timed events)",
-                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "config": config_dict(),
+            "parallelism": "replicas" if world > 1 else "single GPU",
             "e2e": {"value": e2e_fps, "unit": "frames/s", "h2d_bytes_per_step": C.sizeof(_lib.RenderParams),
                     "d2h_bytes_per_step": WIDTH * HEIGHT * 3 * 4,
                     "api": "mr_render_host_async (copy of frame k overlaps the render of frame k+1)",
@@ -545,7 +689,10 @@ def main():
             "stage_rooflines": stages,
             "active_pixels_per_frame": active,
             "density_fetches_per_frame": fetches,
-            "variants": variants}
+            "variants": variants,
+            "memory_probe": probe}
+    if world == 1:
+        line["delta_tracking"] = gpu_delta_tracking(l2)
     if not args.no_batch and world == 1:
         line["batched"] = batched_serving()
     if not args.no_rmse:
@@ -555,8 +702,11 @@ def main():
             m["neural_fps"] = nn_fps
             m["neural_over_dt_at_matched_rmse"] = nn_fps / m["dt_fps_at_matched_rmse"]
         line["matched_rmse"] = m
+    if not args.no_train and world == 1:
+        line["training"] = training_leg()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(v, dens, p, w, st)
+        line["cpu_baseline"]["delta_tracking"] = cpu_delta_tracking()
     if rank == 0:
         print(json.dumps(line), flush=True)
     v.close()

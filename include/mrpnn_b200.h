@@ -96,6 +96,19 @@ const char* mr_last_error(void);
 
 /* VolumeRender(int resolution) + MallocMemory (core/volume.cu:748-773,831-833). */
 int mr_volume_create(int32_t resolution, mr_volume** out);
+/* VolumeRender(string path) (core/volume.cu:835-911): reads <path>.bin if it
+ * exists (int32 resolution r, then r^3 fp32, index (x*r+y)*r+z), else a .txt
+ * file (r, then r^3 whitespace-separated values) or a .vox file (256^3;
+ * header lines start with 'w', 'h' or 'd'; data lines hold 64 integers, each
+ * value * 64 / 255), then creates the volume and runs mr_volume_update. After
+ * reading a .txt or .vox file it writes <path>.bin as the reference does,
+ * unless write_cache is 0. A missing or malformed file is MR_ERR_ARG (the
+ * reference printed "File not found!" and returned). */
+int mr_volume_load(const char* path, int32_t write_cache, mr_volume** out, void* stream);
+/* The parsing step of mr_volume_load alone (host only, no device use):
+ * *resolution receives r; host_out (may be NULL to query r) receives r^3
+ * floats if capacity allows. */
+int mr_volume_file_read(const char* path, float* host_out, size_t capacity, int32_t* resolution);
 /* ~VolumeRender (core/volume.cu:913-936). */
 int mr_volume_destroy(mr_volume* v);
 /* SetDatas / SetData (core/volume.cu:938-944): host array, index (x*res+y)*res+z. */
@@ -120,15 +133,20 @@ int mr_volume_read(const mr_volume* v, int32_t what, int32_t level, float* host_
 /* ---- network (replaces the NNWeight.cuh constants: core/NNWeight.cuh) ------ */
 
 /* Upload MR_WEIGHT_TOTAL fp32 weights in the blob layout of mrpnn_weights.h.
- * `stencil_xyz` is 160 x 3 floats of stencil directions (the tables of
- * core/vector.cu:77-172); NULL selects the library's built-in stencil. */
+ * `stencil_xyz` is 160 x 3 floats of stencil directions; NULL selects the
+ * reference's own directions (core/vector.cu:77-172), the ones the weights
+ * of core/NNWeight.cuh were trained on. */
 int mr_network_create(const float* host_weights, size_t count, const float* stencil_xyz,
                       mr_network** out);
 int mr_network_destroy(mr_network* net);
 
-/* The library's built-in 160-point stencil (used when mr_network_create gets
- * NULL): 480 floats. */
+/* The default 160-point stencil (used when mr_network_create gets NULL): the
+ * reference's directions, core/vector.cu:77-172 (Spn0..Spn4, SpVn5..SpVn7),
+ * as SphereRandom3 reads them with the identity frame: 480 floats. */
 int mr_builtin_stencil(float* host_out, size_t count);
+/* An alternative stencil in the same shell layout (no reference
+ * counterpart): golden-angle spirals, for networks trained on it. 480 floats. */
+int mr_spiral_stencil(float* host_out, size_t count);
 /* Xavier-uniform initial weights for the blob layout (zero biases), from
  * Philox with the given seed: MR_WEIGHT_TOTAL floats. */
 int mr_weights_xavier(uint32_t seed, float* host_out, size_t count);
@@ -214,6 +232,12 @@ int mr_tc_selftest_tf32(int32_t n, int32_t k, const float* host_a, const float* 
  * texel is subnormal (the texture unit reads those as 0). */
 #define MR_SAMPLER_SELFTEST_RES 32
 int mr_sampler_selftest(int32_t n, const float* host_table, const float* host_uv, float* host_out);
+/* Memory-path probe (no reference counterpart): reads dev_buf (`bytes`, a
+ * multiple of 16, 16-byte aligned) `passes` times with 16-byte loads that
+ * bypass L1, from a resident grid; dev_sink is one device word. Time it with
+ * events on `stream`: a buffer that fits in L2 gives the L2 read bandwidth, a
+ * buffer far larger than L2 the HBM read bandwidth. */
+int mr_stream_read_probe(const void* dev_buf, size_t bytes, int32_t passes, uint32_t* dev_sink, void* stream);
 /* Error word of the tensor-core network kernel of `net` (an mbarrier wait
  * that timed out): MR_ERR_TIMEOUT if set; `reset` clears it. */
 int mr_network_check(const mr_network* net, int32_t reset);

@@ -7,10 +7,10 @@ loads the library and fails loudly when it has not been built.
 """
 from . import _lib
 from ._lib import MRError, RenderParams, load, check
-from .volume import (MRPNN, PT, RPNN, Camera, Network, VolumeRender, builtin_stencil, save_bmp, tone_aces,
+from .volume import (MRPNN, PT, RPNN, Camera, Network, VolumeRender, builtin_stencil, spiral_stencil, save_bmp, tone_aces,
                      tone_gamma, tone_none, xavier_weights)
 
-__all__ = ["VolumeRender", "Camera", "Network", "builtin_stencil", "xavier_weights", "tone_aces", "tone_gamma",
+__all__ = ["VolumeRender", "Camera", "Network", "builtin_stencil", "spiral_stencil", "xavier_weights", "tone_aces", "tone_gamma",
            "tone_none", "save_bmp", "PT", "RPNN", "MRPNN", "MRError", "RenderParams", "load", "check"]
 
 load()

@@ -30,7 +30,7 @@ EXPORTS = [
     "mr_render_interactive", "mr_denoise", "mr_batch_create", "mr_batch_destroy", "mr_batch_add", "mr_batch_prepare",
     "mr_batch_autotune", "mr_batch_render", "mr_batch_capture", "mr_batch_launch", "mr_batch_counters",
     "mr_tc_selftest_fp8", "mr_sampler_selftest", "mr_tc_selftest_tf32", "mr_render_host_async",
-    "mr_render_host_wait",
+    "mr_render_host_wait", "mr_spiral_stencil", "mr_stream_read_probe", "mr_volume_load", "mr_volume_file_read",
 ]
 NOALLOC_MAX_PIXELS = 16384
 
@@ -102,6 +102,10 @@ def load():
     L.mr_network_create.argtypes = [vp, sz, vp, C.POINTER(vp)]
     L.mr_network_destroy.argtypes = [vp]
     L.mr_builtin_stencil.argtypes = [vp, sz]
+    L.mr_spiral_stencil.argtypes = [vp, sz]
+    L.mr_stream_read_probe.argtypes = [vp, sz, i32, vp, vp]
+    L.mr_volume_load.argtypes = [C.c_char_p, i32, C.POINTER(vp), vp]
+    L.mr_volume_file_read.argtypes = [C.c_char_p, vp, sz, C.POINTER(i32)]
     L.mr_weights_xavier.argtypes = [u32, vp, sz]
     L.mr_render.argtypes = [vp, vp, C.POINTER(RenderParams), vp, vp]
     L.mr_render_host.argtypes = [vp, vp, C.POINTER(RenderParams), vp]

@@ -32,12 +32,17 @@ int check_params(const mr_render_params* p);
 int pack_network(Network* n);
 void free_packed(Network* n);
 
-// Built-in stencil: 160 directions in the reference's shell layout
-// (core/vector.cu:77-172: shells of 8, 8, 16, 16, 16 unit points, the first
-// point of shell 0 at the centre, then three shells of 32 points inside the
-// unit ball). Shells 0-4 are golden-angle spirals about rotated axes,
+// Default stencil: the reference's 160 directions (core/vector.cu:77-172),
+// the points the reference network's weights were trained on.
+#include "mr_ref_stencil.inc"
+static void builtin_stencil(float* out) { std::memcpy(out, kRefStencil, sizeof(kRefStencil)); }
+
+// Spiral stencil (opt-in, mr_spiral_stencil): 160 directions in the
+// reference's shell layout (shells of 8, 8, 16, 16, 16 unit points, the
+// first point of shell 0 at the centre, then three shells of 32 points inside
+// the unit ball). Shells 0-4 are golden-angle spirals about rotated axes,
 // shells 5-7 spirals with radii cbrt of a stratified sequence.
-static void builtin_stencil(float* out) {
+static void spiral_stencil(float* out) {
   const double ga = 2.39996322972865332;  // golden angle
   int k = 0;
   auto put = [&](double x, double y, double z) { out[3 * k] = (float)x; out[3 * k + 1] = (float)y; out[3 * k + 2] = (float)z; ++k; };
@@ -82,6 +87,13 @@ int mr_builtin_stencil(float* host_out, size_t count) {
   clear_error();
   if (!host_out || count != MR_STENCIL_POINTS * 3) return set_error(MR_ERR_ARG, "stencil needs 480 floats");
   builtin_stencil(host_out);
+  return MR_OK;
+}
+
+int mr_spiral_stencil(float* host_out, size_t count) {
+  clear_error();
+  if (!host_out || count != MR_STENCIL_POINTS * 3) return set_error(MR_ERR_ARG, "stencil needs 480 floats");
+  spiral_stencil(host_out);
   return MR_OK;
 }
 

@@ -4,7 +4,11 @@
 //  * k_interactive_pt: one delta-tracking sample per pixel and frame (half the
 //    pixels with the checkerboard option), running mean of the radiance and the
 //    per-pixel histogram of x / (1 + x) (10 bins per channel) with running
-//    means of the luminance l = sum(x / (1 + x)) and of l^2.
+//    means of the luminance l = sum(x / (1 + x)) and of l^2. The means are
+//    kept as FP64 sums (the volume's moment buffer) and written to the fp32
+//    accumulation and Histogram fields as sum / n, so that no rounding builds
+//    up over the frames; the denoiser's variance E[l^2] - E[l]^2 is taken
+//    from the same FP64 sums.
 //  * k_denoise: the histogram-weighted 11 x 11 filter of Denoise<true>
 //    (weights max(0, 1 - 1.2 Compare(h_center, h_neighbour)) where the
 //    luminance variance exceeds 0.01), the frame-0 checkerboard fill, exposure,
@@ -90,9 +94,22 @@ struct InterArgs {
   int frame, fnum, checker, flip;
   float* accum;
   mr_histogram* hist;
+  double* mom;  // 5 x npx FP64 sums: r, g, b, l, l^2
+  size_t npx;
 };
 
-__device__ __forceinline__ float lerp1(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+// Rebuilds the FP64 sums from the fp32 state (accum and the Histogram's count
+// and means) when the moment buffer is new for this histogram buffer while an
+// accumulation is under way (frame_index > 0).
+__global__ void k_seed_moments(const float* __restrict__ accum, const mr_histogram* __restrict__ hist,
+                               double* __restrict__ mom, size_t npx) {
+  const size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (p >= npx) return;
+  const double n = (double)hist[p].total_samples;
+  for (int c = 0; c < 3; ++c) mom[c * npx + p] = (double)accum[3 * p + c] * n;
+  mom[3 * npx + p] = (double)hist[p].x * n;
+  mom[4 * npx + p] = (double)hist[p].x2 * n;
+}
 
 __global__ void __launch_bounds__(128) k_interactive_pt(InterArgs a) {
   const int W = a.cam.width, H = a.cam.height;
@@ -110,17 +127,15 @@ __global__ void __launch_bounds__(128) k_interactive_pt(InterArgs a) {
   float tt;
   F3 L = path_radiance(a.m, a.sc, rng, a.cam.ori, camera_dir(a.cam, row, col, jx, jy), &tt, st);
   L = vmax(L, f3(0, 0, 0));
-  const float rate = 1.0f / (float)(1 + a.fnum);
-  float* acc = a.accum + 3 * (size_t)pix;
-  acc[0] = lerp1(acc[0], L.x, rate);
-  acc[1] = lerp1(acc[1], L.y, rate);
-  acc[2] = lerp1(acc[2], L.z, rate);
   mr_histogram& h = a.hist[pix];
+  double* m = a.mom + pix;
+  const size_t N = a.npx;
   if (a.fnum == 0) {
     for (int i = 0; i < 3 * kBins; ++i) h.bin[i] = 0.0f;
     h.total_samples = 0.0f;
     h.x2 = 0.0f;
     h.x = 0.0f;
+    for (int k = 0; k < 5; ++k) m[k * N] = 0.0;
   }
   const F3 r = f3(L.x / (L.x + 1.0f), L.y / (L.y + 1.0f), L.z / (L.z + 1.0f));
   h.total_samples += 1.0f;
@@ -128,8 +143,22 @@ __global__ void __launch_bounds__(128) k_interactive_pt(InterArgs a) {
   h.bin[(int)floorf(fminf(r.y, 0.999f) * kBins) + kBins] += 1.0f;
   h.bin[(int)floorf(fminf(r.z, 0.999f) * kBins) + 2 * kBins] += 1.0f;
   const float l = r.x + r.y + r.z;
-  h.x = lerp1(h.x, l, rate);
-  h.x2 = lerp1(h.x2, l * l, rate);
+  // FP64 sums; the fp32 fields hold sum / n, n = fnum + 1 (the reference's
+  // running means with rate 1 / (1 + fnum))
+  const double s0 = m[0] + (double)L.x, s1 = m[N] + (double)L.y, s2 = m[2 * N] + (double)L.z;
+  const double s3 = m[3 * N] + (double)l, s4 = m[4 * N] + (double)l * (double)l;
+  m[0] = s0;
+  m[N] = s1;
+  m[2 * N] = s2;
+  m[3 * N] = s3;
+  m[4 * N] = s4;
+  const double inv = 1.0 / (double)(1 + a.fnum);
+  float* acc = a.accum + 3 * (size_t)pix;
+  acc[0] = (float)(s0 * inv);
+  acc[1] = (float)(s1 * inv);
+  acc[2] = (float)(s2 * inv);
+  h.x = (float)(s3 * inv);
+  h.x2 = (float)(s4 * inv);
 }
 
 // ---- denoise + tone map + pack ----------------------------------------------------
@@ -161,6 +190,8 @@ struct DenoiseArgs {
   uint32_t* out;
   int W, H, frame, flip, tone, denoise;
   float exposure;
+  const double* mom;  // FP64 sums of l and l^2 (interactive path), or null: the Histogram's fp32 means
+  size_t npx;
 };
 
 __global__ void __launch_bounds__(256) k_denoise(DenoiseArgs a) {
@@ -202,7 +233,16 @@ __global__ void __launch_bounds__(256) k_denoise(DenoiseArgs a) {
     }
   } else {
     const float* ch = sh + li * kHistFloats;
-    const float variance = fabsf(ch[3 * kBins + 1] - ch[3 * kBins + 2] * ch[3 * kBins + 2]);
+    float variance;
+    if (a.mom) {
+      // |E[l^2] - E[l]^2| from the FP64 sums over the pixel's samples
+      const size_t p = (size_t)row * a.W + col;
+      const double n = (double)ch[3 * kBins];
+      const double el = a.mom[3 * a.npx + p] / n, el2 = a.mom[4 * a.npx + p] / n;
+      variance = (float)fabs(el2 - el * el);
+    } else {
+      variance = fabsf(ch[3 * kBins + 1] - ch[3 * kBins + 2] * ch[3 * kBins + 2]);
+    }
     if (filter && variance > 0.01f) {
       float cb[3 * kBins];
 #pragma unroll
@@ -294,13 +334,15 @@ int render_neural_dist(Volume* v, const Network* net, const mr_render_params* p,
                        cudaStream_t s);
 
 static int launch_denoise(const float* accum, const mr_histogram* hist, uint32_t* bgra, int W, int H,
-                          const mr_interactive* it, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
+                          const mr_interactive* it, cudaStream_t s, const double* mom = nullptr) {
+  static DeviceCache attr;  // the attribute belongs to each device's context
+  int rc = attr.once([] {
     MR_CUDA(cudaFuncSetAttribute(k_denoise, cudaFuncAttributeMaxDynamicSharedMemorySize, kDenoiseSmem));
-    attr = true;
-  }
-  DenoiseArgs a{accum, hist, bgra, W, H, it->frame_index, it->frame_index & 1, it->tone, it->denoise, it->exposure};
+    return (int)MR_OK;
+  });
+  if (rc) return rc;
+  DenoiseArgs a{accum, hist, bgra, W, H, it->frame_index, it->frame_index & 1, it->tone, it->denoise, it->exposure,
+                mom, (size_t)W * H};
   dim3 grid((W + kTile - 1) / kTile, (H + kTile - 1) / kTile);
   k_denoise<<<grid, 256, kDenoiseSmem, s>>>(a);
   MR_CUDA(cudaGetLastError());
@@ -357,11 +399,33 @@ extern "C" int mr_render_interactive(mr_volume* h, const mr_network* net, const 
     a.flip = it->frame_index & 1;
     a.accum = dev_accum;
     a.hist = dev_hist;
+    // FP64 moment buffer of this histogram buffer (grown on demand; rebuilt
+    // from the fp32 state when it is new mid-accumulation)
+    const size_t npx = (size_t)W * H;
+    const size_t need = 5 * npx * sizeof(double);
+    bool fresh = v->mom_hist != (const void*)dev_hist || v->mom_npx != npx;
+    if (v->mom_bytes < need) {
+      if (v->mom) MR_CUDA(cudaFreeAsync(v->mom, s));
+      v->mom = nullptr;
+      v->mom_bytes = 0;
+      cudaError_t e = cudaMallocAsync(&v->mom, need, s);
+      if (e != cudaSuccess) return set_error(MR_ERR_NOMEM, "interactive moment buffer: %s", cudaGetErrorString(e));
+      v->mom_bytes = need;
+      fresh = true;
+    }
+    v->mom_hist = dev_hist;
+    v->mom_npx = npx;
+    if (fresh && it->frame_index > 0) {
+      k_seed_moments<<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(dev_accum, dev_hist, v->mom, npx);
+      MR_CUDA(cudaGetLastError());
+    }
+    a.mom = v->mom;
+    a.npx = npx;
     const int per_row = a.checker ? (W + 1) / 2 : W;
     const long long n = (long long)per_row * H;
     k_interactive_pt<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(a);
     MR_CUDA(cudaGetLastError());
-    return launch_denoise(dev_accum, dev_hist, dev_bgra, W, H, it, s);
+    return launch_denoise(dev_accum, dev_hist, dev_bgra, W, H, it, s, v->mom);
   }
   if (p->render_type != MR_RT_MRPNN) return set_error(MR_ERR_UNSUPPORTED, "render type %d", p->render_type);
   if (!net) return set_error(MR_ERR_ARG, "neural interactive render needs a network");

@@ -5,6 +5,7 @@
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -75,6 +76,12 @@ struct Volume {
   // Interactive neural mode: radiance and first-hit distance of the frame.
   void* inter = nullptr;
   size_t inter_bytes = 0;
+  // Interactive delta tracking: FP64 per-pixel sums of the radiance (3), of
+  // the histogram luminance l and of l^2, SoA (sum k of pixel p at
+  // mom[k * mom_npx + p]), for the histogram buffer mom_hist they belong to.
+  double* mom = nullptr;
+  size_t mom_bytes = 0, mom_npx = 0;
+  const void* mom_hist = nullptr;
   // Pipelined host delivery (mr_render_host_async): two device frames used in
   // turn, a copy stream, and per frame the events "rendered" (on the caller's
   // stream) and "copied" (on the copy stream).
@@ -107,6 +114,42 @@ struct Network {
 struct BatchOut {
   float* out;
   F3 light_color, scatter;
+};
+
+// A value that belongs to one device (an SM count, an occupancy, whether a
+// kernel attribute was set there), computed the first time a thread asks for
+// it with that device current and kept for the process. Safe to use from
+// several threads and devices at once.
+constexpr int kMaxDevices = 64;
+struct DeviceCache {
+  std::mutex mu;
+  int value[kMaxDevices] = {};
+  bool ready[kMaxDevices] = {};
+  // f() -> int, evaluated under the lock on the first call per device.
+  template <class F>
+  int get(F&& f) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return f();
+    std::lock_guard<std::mutex> lock(mu);
+    if (!ready[dev]) {
+      value[dev] = f();
+      ready[dev] = true;
+    }
+    return value[dev];
+  }
+  // f() -> mr_status, run once per device; only a success is kept, so a
+  // failed first attempt is retried by the next call.
+  template <class F>
+  int once(F&& f) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) return f();
+    std::lock_guard<std::mutex> lock(mu);
+    if (ready[dev]) return 0;
+    int rc = f();
+    if (rc == 0) ready[dev] = true;
+    return rc;
+  }
 };
 
 // Error reporting: thread-local message, returns the code.

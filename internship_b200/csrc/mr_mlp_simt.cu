@@ -1146,12 +1146,13 @@ int launch_mlp_simt(const Network* net, const float* desc, const float* aux, lon
   if (!tout || !stg) return set_error(MR_ERR_ARG, "fp32 network: no buffer for the trunk or LC2 outputs");
   if (net->h_tail.size() != (size_t)kTailFloats || net->h_light.size() * sizeof(float) != sizeof(LightParams))
     return set_error(MR_ERR_STATE, "network not packed");
-  static bool attr = false;
-  if (!attr) {
+  static DeviceCache attr;  // the attributes belong to each device's context
+  int rc = attr.once([] {
     MR_CUDA(cudaFuncSetAttribute(k_tc32_head, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcHeadSmem));
     MR_CUDA(cudaFuncSetAttribute(k_simt_trunk, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrunkSmem));
-    attr = true;
-  }
+    return (int)MR_OK;
+  });
+  if (rc) return rc;
   TrunkArgs a;
   a.w = net->w;
   a.img = net->simt_img;

@@ -405,12 +405,15 @@ __device__ __forceinline__ void tmem_st8(uint32_t taddr, const float* v) {
                : "memory");
   asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
+// 8 columns; load and wait in one asm statement, so that no use of the
+// loaded registers is scheduled before the wait.
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v) {
   uint32_t r[8];
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n\t"
+               "tcgen05.wait::ld.sync.aligned;\n"
                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-               : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+               : "r"(taddr)
+               : "memory");
 #pragma unroll
   for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
@@ -1246,12 +1249,13 @@ int launch_mlp_tc(const Network* net, const float* desc, const float* aux, long 
                   const int* job, const BatchOut* bout) {
   if (cs * 4 > 0x7FFFFFFFll || n > (1 << 28))
     return set_error(MR_ERR_ARG, "tensor-core network: %d rows / chunk stride %lld out of range", n, cs);
-  static bool attr = false;
-  if (!attr) {
+  static DeviceCache attr;  // the attributes belong to each device's context
+  int rc = attr.once([] {
     MR_CUDA(cudaFuncSetAttribute(k_mlp_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes<false>()));
     MR_CUDA(cudaFuncSetAttribute(k_mlp_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes<true>()));
-    attr = true;
-  }
+    return (int)MR_OK;
+  });
+  if (rc) return rc;
   TcArgs a;
   a.wpack = (const uint8_t*)net->packed;
   a.w = net->w;

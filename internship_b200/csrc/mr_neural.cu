@@ -659,16 +659,17 @@ static int neural_passes(Volume* v, const Network* net, const mr_render_params* 
   F3 sr = to_f3(p->scatter_rate) / 1.001f;
   mark(ST_NN_PREDICT);
   // resident grids: as many 128-thread blocks as fit on the GPU at once
-  static int per_sm[3] = {0, 0, 0};
-  if (!per_sm[samp]) {
-    MR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm[samp],
+  static DeviceCache gather_occ[3];  // per sampler, per device
+  const int per_sm = gather_occ[samp].get([samp] {
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &n,
         samp == kSampTex ? (const void*)k_gather_fm<kSampTex>
                          : samp == kSampGather ? (const void*)k_gather_fm<kSampGather> : (const void*)k_gather_fm<kSampLoad>,
-        128, 0));
-    per_sm[samp] = std::max(1, per_sm[samp]);
-  }
-  const unsigned ggrid = (unsigned)std::min<size_t>((npx + 127) / 128, (size_t)per_sm[samp] * sm_count());
+        128, 0);
+    return std::max(1, n);
+  });
+  const unsigned ggrid = (unsigned)std::min<size_t>((npx + 127) / 128, (size_t)per_sm * sm_count());
   if (samp == kSampTex)
     k_gather_fm<kSampTex><<<ggrid, 128, 0, s>>>(tabs, net->stencil, h0s, rec, (int)npx, L, p->alpha, p->g,
                                                srp_of(sr), desc, aux);

@@ -77,26 +77,26 @@ __global__ void k_scale(float* x, size_t n, float s) {
   if (i < n) x[i] *= s;
 }
 
+// SM count of the current device.
 int sm_count() {
-  static int cached = 0;
-  if (!cached) {
-    int dev = 0;
+  static DeviceCache cache;
+  return cache.get([] {
+    int dev = 0, n = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&cached, cudaDevAttrMultiProcessorCount, dev);
-    if (cached <= 0) cached = 1;
-  }
-  return cached;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 1;
+  });
 }
 
+// Resident grid of the delta tracker on the current device.
 static int dt_grid() {
-  static int blocks = 0;
-  if (!blocks) {
+  static DeviceCache cache;
+  return cache.get([] {
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_delta_track, 128, 0);
     if (per_sm <= 0) per_sm = 1;
-    blocks = per_sm * sm_count();
-  }
-  return blocks;
+    return per_sm * sm_count();
+  });
 }
 
 CameraModel make_camera(const mr_render_params* p) {

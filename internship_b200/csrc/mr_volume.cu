@@ -93,25 +93,38 @@ __global__ void k_tr_level(const float* __restrict__ src, int r, float a, F3 L, 
   dst[i] = expf(-sum * a * step);
 }
 
-__device__ __forceinline__ float radical_inverse(uint32_t base, uint32_t a) {
-  const float inv_base = 1.0f / (float)base;
+// Scrambled radical inverse of a in base B: digit d of a becomes digit
+// perm(d), perm packed four bits per digit in P (digit d at bits 4d..4d+3),
+// and the infinite tail of perm(0) digits is added in closed form,
+// perm(0) / (B - 1) times the last digit weight; clamped below 1
+// (ScrambledRadicalInverse, core/volume.cu:1060-1076).
+template <uint32_t B, uint64_t P>
+__device__ __forceinline__ float scrambled_radical_inverse(uint32_t a) {
+  const float inv_base = 1.0f / (float)B;
   uint32_t rev = 0;
   float inv_bn = 1.0f;
   while (a) {
-    uint32_t next = a / base;
-    uint32_t digit = a - next * base;
-    rev = rev * base + digit;
+    uint32_t next = a / B;
+    uint32_t digit = a - next * B;
+    rev = rev * B + (uint32_t)((P >> (4u * digit)) & 15u);
     inv_bn *= inv_base;
     a = next;
   }
-  return fminf((float)rev * inv_bn, 0.99999994f);
+  return fminf(inv_bn * ((float)rev + inv_base * (float)(P & 15u) / (1.0f - inv_base)), 0.99999994f);
 }
+// Digit permutations of the four Halton dimensions the HG table draws
+// (dimensions 0, 1, 2 and 4: bases 2, 3, 5 and 11). They are the entries of
+// the reference's permutation table for those bases (core/volume.cu:956-958:
+// {0,1}, {2,1,0}, {4,1,2,3,0}, {8,3,5,4,7,2,6,9,1,10,0}); the table's sample
+// points, and so its values, depend on them.
+constexpr uint64_t kPermB2 = 0x10ull, kPermB3 = 0x12ull, kPermB5 = 0x3214ull, kPermB11 = 0xa196274538ull;
 __device__ __forceinline__ float fracf_(float f) { return f - (float)(long long)f; }
 
 // Fill_Hg (core/volume.cu:1082-1160): lut[i + j*512] = mean of HG over a ball
 // of radius tan(angle_j) centred at unit distance along cos_i, estimated with
-// 1024 Halton points (bases 2,3,5,11) mixing HG-sampled chords and uniform
-// ball points. Per-texel Cranley-Patterson offset from Philox (TAG_LUT).
+// 1024 scrambled Halton points (bases 2,3,5,11) mixing HG-sampled chords and
+// uniform ball points. Per-texel Cranley-Patterson offset from Philox
+// (TAG_LUT) where the reference draws it from curand.
 __global__ void k_hglut(float g, uint32_t seed, float* __restrict__ lut) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -143,8 +156,9 @@ __global__ void k_hglut(float g, uint32_t seed, float* __restrict__ lut) {
     mis = 1.0f - 1.0f / (1.0f + a * mis / (1.0f - a));
   }
   for (int k = 0; k < 1024; ++k) {
-    float r0 = fracf_(radical_inverse(2, k) + bn), r1 = fracf_(radical_inverse(3, k) + bn);
-    if (fracf_(radical_inverse(11, k) + bn) < mis) {
+    float r0 = fracf_(scrambled_radical_inverse<2, kPermB2>(k) + bn);
+    float r1 = fracf_(scrambled_radical_inverse<3, kPermB3>(k) + bn);
+    if (fracf_(scrambled_radical_inverse<11, kPermB11>(k) + bn) < mis) {
       F3 l = hg_sample_dir(r0, r1, view, g);
       float sdotl = dot(D, l);
       float p = R * R - 1 + sdotl * sdotl;
@@ -156,7 +170,7 @@ __global__ void k_hglut(float g, uint32_t seed, float* __restrict__ lut) {
       float d = d1 * d1 * d1 - d0 * d0 * d0;
       hg += fmaxf(0.0f, d / 4);
     } else {
-      float r2 = fracf_(radical_inverse(5, k) + bn);
+      float r2 = fracf_(scrambled_radical_inverse<5, kPermB5>(k) + bn);
       float theta = r0 * 2.0f * 3.1415926535f;
       float phi = acosf(2.0f * r1 - 1.0f);
       float rr = cbrtf(r2);
@@ -441,6 +455,7 @@ int mr_volume_destroy(mr_volume* h) {
   cudaFree(v->d_counters);
   if (v->scratch) cudaFree(v->scratch);
   if (v->inter) cudaFree(v->inter);
+  if (v->mom) cudaFree(v->mom);
   if (v->copy_stream) {
     cudaStreamSynchronize(v->copy_stream);  // host copies still reading the frames
     for (int i = 0; i < 2; ++i) {

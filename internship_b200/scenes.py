@@ -8,14 +8,17 @@ sphere_scene  : 128^3 solid sphere (centre 0.5, radius 0.25, density 1),
 cloud_scene   : 512^3 seeded Perlin-fBm cloud (6 octaves, base frequency 4,
                 lacunarity 2, gain 0.5, threshold 0.45, radial falloff) with
                 the sphere scene's light, medium and camera at 1920 x 1080.
+
+The module is plain Python and loads no library at import (the device
+helpers import the package's loader when called), so a CPU-only process can
+load it by path to build the same render requests.
 """
 import ctypes as C
 import math
 
 import numpy as np
 
-from . import _lib
-from ._lib import RenderParams, check, f3
+RT_PT, RT_MRPNN = 0, 2  # mr_render_type
 
 M0, M1, W0, W1 = 0xD2511F53, 0xCD9E8D57, 0x9E3779B9, 0xBB67AE85
 
@@ -69,19 +72,28 @@ def sphere_density(res=128):
 CAMERA_DIR = np.array([1.0, 0.55, 0.8]) / np.linalg.norm([1.0, 0.55, 0.8])
 
 
-def make_params(width, height, spp=1, rt=_lib.RT_PT, bounces=512, seed=0, alpha=64.0, g=0.857, albedo=0.99,
-                distance=2.5, fov=40.0, sample_offset=0, precision=_lib.PREC_FP32, light_seed=0,
-                sampler=_lib.SAMPLER_EXACT):
+def _set3(field, v):
+    field.x, field.y, field.z = (float(c) for c in v)
+
+
+def make_params(width, height, spp=1, rt=RT_PT, bounces=512, seed=0, alpha=64.0, g=0.857, albedo=0.99,
+                distance=2.5, fov=40.0, sample_offset=0, precision=0, light_seed=0, sampler=0, params_cls=None):
+    """An mr_render_params request (params_cls: the ctypes mirror to fill,
+    default the package's RenderParams)."""
+    if params_cls is None:
+        from ._lib import RenderParams as params_cls
     ori, up, right = camera_vectors(CAMERA_DIR * distance, fov)
-    p = RenderParams()
+    p = params_cls()
     p.width, p.height = width, height
-    p.ori, p.up, p.right = f3(ori), f3(up), f3(right)
-    p.light_dir = f3(seeded_light(light_seed))
-    p.light_color = f3((1.0, 1.0, 1.0))
+    _set3(p.ori, ori)
+    _set3(p.up, up)
+    _set3(p.right, right)
+    _set3(p.light_dir, seeded_light(light_seed))
+    _set3(p.light_color, (1.0, 1.0, 1.0))
     p.alpha, p.g = alpha, g
-    p.scatter_rate = f3((albedo, albedo, albedo))
+    _set3(p.scatter_rate, (albedo, albedo, albedo))
     p.tr_scale = 1.0
-    p.env_color = f3((0.0, 0.0, 0.0))
+    _set3(p.env_color, (0.0, 0.0, 0.0))
     p.max_bounces, p.spp = bounces, spp
     p.seed, p.sample_offset = seed, sample_offset
     p.render_type, p.precision, p.sampler = rt, precision, sampler
@@ -96,17 +108,19 @@ CLOUD_ARGS = dict(octaves=6, base_freq=4.0, lacunarity=2.0, gain=0.5, threshold=
 
 
 def generate_cloud_device(res, seed, dev_ptr, stream=None, **over):
+    from . import _lib
     a = dict(CLOUD_ARGS, **over)
-    check(_lib.load().mr_generate_cloud(res, seed, a["octaves"], a["base_freq"], a["lacunarity"], a["gain"],
+    _lib.check(_lib.load().mr_generate_cloud(res, seed, a["octaves"], a["base_freq"], a["lacunarity"], a["gain"],
                                         a["threshold"], C.c_void_p(dev_ptr), stream))
 
 
 def cloud_permutation(seed):
+    from . import _lib
     out = np.zeros(256, np.int32)
-    check(_lib.load().mr_cloud_permutation(seed, out.ctypes.data))
+    _lib.check(_lib.load().mr_cloud_permutation(seed, out.ctypes.data))
     return out
 
 
 def cloud_scene_params(width=1920, height=1080, **kw):
-    kw.setdefault("rt", _lib.RT_MRPNN)
+    kw.setdefault("rt", RT_MRPNN)
     return make_params(width, height, 1, **kw)

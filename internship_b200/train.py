@@ -198,6 +198,42 @@ def targets(aux, label):
     return torch.log1p(torch.clamp(label, min=0) / aux[:, 2])
 
 
+def run(configs=32, samples=5_000_000, spp=4096, bounces=512, epochs=20, batch=65536, lr=1e-3, holdout=0.05,
+        seed=0, log=None):
+    """The whole learned part: generate the rows, train from initial_weights(1)
+    and evaluate on a held-out share. Returns (weights, report); the report
+    holds the row count, the held-out RMSE of X = log(1 + L / srp) with the
+    trained network and with no network (X = 0: single scattering only), and
+    the label / training throughput."""
+    import torch
+    t0 = time.time()
+    cfgs = scene_configs(configs, seed)
+    desc, aux, label = generate(cfgs, math.ceil(samples / configs), spp, bounces, seed)
+    torch.cuda.synchronize()
+    t1 = time.time()
+    n = len(label)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    perm = torch.randperm(n, device="cuda", generator=gen)
+    nh = max(1, int(n * holdout))
+    hold, trn = perm[:nh], perm[nh:]
+    w0 = initial_weights(1)
+    w, hist = fit(desc[trn], aux[trn], label[trn], w0, epochs, batch, lr, seed, log=log)
+    torch.cuda.synchronize()
+    t2 = time.time()
+    T = targets(aux[hold], label[hold])
+    dh, ah = desc[hold].contiguous(), aux[hold].contiguous()
+    rmse = float(torch.sqrt(torch.mean((predict_x(w, dh, ah) - T) ** 2)))
+    rmse_init = float(torch.sqrt(torch.mean((predict_x(w0, dh, ah) - T) ** 2)))
+    rmse0 = float(torch.sqrt(torch.mean(T ** 2)))
+    rows_trained = (n - nh) * epochs
+    return w, {"rows": n, "configs": configs, "spp": spp, "bounces": bounces, "epochs": epochs, "batch": batch,
+               "lr": lr, "holdout_rmse_log": rmse, "untrained_rmse_log": rmse_init, "no_network_rmse_log": rmse0,
+               "generate_s": t1 - t0, "train_s": t2 - t1, "labels_per_s": n / (t1 - t0),
+               "label_paths_per_s": n * spp / (t1 - t0), "train_rows_per_s": rows_trained / (t2 - t1),
+               "loss_history": hist}
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--configs", type=int, default=32)
@@ -211,26 +247,10 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default="mrpnn_trained.npy")
     args = ap.parse_args()
-    import torch
-    t0 = time.time()
-    cfgs = scene_configs(args.configs, args.seed)
-    desc, aux, label = generate(cfgs, math.ceil(args.samples / args.configs), args.spp, args.bounces, args.seed)
-    t1 = time.time()
-    n = len(label)
-    gen = torch.Generator(device="cuda")
-    gen.manual_seed(args.seed)
-    perm = torch.randperm(n, device="cuda", generator=gen)
-    nh = max(1, int(n * args.holdout))
-    hold, trn = perm[:nh], perm[nh:]
-    w0 = initial_weights(1)
-    w, hist = fit(desc[trn], aux[trn], label[trn], w0, args.epochs, args.batch, args.lr, args.seed, log=print)
-    t2 = time.time()
-    T = targets(aux[hold], label[hold])
-    rmse = float(torch.sqrt(torch.mean((predict_x(w, desc[hold].contiguous(), aux[hold].contiguous()) - T) ** 2)))
-    rmse0 = float(torch.sqrt(torch.mean(T ** 2)))
+    w, rep = run(args.configs, args.samples, args.spp, args.bounces, args.epochs, args.batch, args.lr, args.holdout,
+                 args.seed, log=print)
     np.save(args.out, w)
-    print(json.dumps({"rows": n, "holdout_rmse_log": rmse, "no_network_rmse_log": rmse0, "epochs": args.epochs,
-                      "generate_s": t1 - t0, "train_s": t2 - t1, "loss_history": hist}))
+    print(json.dumps(rep))
 
 
 if __name__ == "__main__":

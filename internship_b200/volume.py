@@ -6,6 +6,7 @@ C ABI of libmrpnn_b200.so. Images are numpy arrays (H, W, 3) float32,
 row-major, top row first.
 """
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -15,9 +16,29 @@ from ._lib import MRError, RenderParams, check, f3
 PT, RPNN, MRPNN = _lib.RT_PT, _lib.RT_RPNN, _lib.RT_MRPNN
 
 
+def read_volume_file(path):
+    """The density grid of a volume file (.bin / .txt / .vox, resolved as
+    VolumeRender(string) resolves it), parsed on the host: (r, r, r) float32."""
+    L = _lib.load()
+    r = C.c_int32()
+    p = os.fsencode(path)
+    check(L.mr_volume_file_read(p, None, 0, C.byref(r)))
+    out = np.zeros(r.value ** 3, np.float32)
+    check(L.mr_volume_file_read(p, out.ctypes.data, out.size, C.byref(r)))
+    return out.reshape((r.value,) * 3)
+
+
 def builtin_stencil():
+    """The default stencil: the reference's 160 directions (core/vector.cu:77-172)."""
     out = np.zeros(480, np.float32)
     check(_lib.load().mr_builtin_stencil(out.ctypes.data, out.size))
+    return out
+
+
+def spiral_stencil():
+    """The library's golden-angle stencil in the same shell layout (opt-in)."""
+    out = np.zeros(480, np.float32)
+    check(_lib.load().mr_spiral_stencil(out.ctypes.data, out.size))
     return out
 
 
@@ -70,13 +91,29 @@ class VolumeRender:
 
     PT, RPNN, MRPNN = PT, RPNN, MRPNN
 
-    def __init__(self, resolution):
-        self.resolution = int(resolution)
+    def __init__(self, resolution, write_cache=True):
+        """VolumeRender(int resolution), or VolumeRender(string path)
+        (core/volume.cu:835-911): a path loads <path>.bin, a .txt or a .vox
+        file through mr_volume_load, which also runs Update()."""
+        L = _lib.load()
         h = C.c_void_p()
-        check(_lib.load().mr_volume_create(self.resolution, C.byref(h)))
-        self.handle = h
-        self.datas = np.zeros((self.resolution,) * 3, np.float32)
         self.max_density = 0.00001
+        if isinstance(resolution, (str, bytes, os.PathLike)):
+            path = os.fsencode(resolution)
+            check(L.mr_volume_load(path, 1 if write_cache else 0, C.byref(h), None))
+            r = C.c_int32()
+            check(L.mr_volume_resolution(h, C.byref(r)))
+            self.resolution = r.value
+            self.handle = h
+            self.datas = self.read(_lib.READ_DENSITY).reshape((self.resolution,) * 3)
+            md = C.c_float()
+            check(L.mr_volume_max_density(h, C.byref(md)))
+            self.max_density = md.value
+        else:
+            self.resolution = int(resolution)
+            check(L.mr_volume_create(self.resolution, C.byref(h)))
+            self.handle = h
+            self.datas = np.zeros((self.resolution,) * 3, np.float32)
         self.scatter_rate = (1.001, 1.001, 1.001)  # core/render.cuh:16 default
         self.tr_scale = 1.0
         self.exposure = 1.0

@@ -42,6 +42,7 @@ def build_reference(force=False):
     core = os.path.join(REF_SRC, "core")
     if not os.path.isdir(core):
         return None
+    build_reference_volume(force)
     os.makedirs(REF_DIR, exist_ok=True)
     out = os.path.join(REF_DIR, "libref_mrpnn.so")
     ref_dir = os.path.join(HERE, "ref")
@@ -78,6 +79,41 @@ def build_reference(force=False):
     subprocess.check_call(["nvcc", "-shared", "-gencode", "arch=compute_100a,code=sm_100a",
                            "-Xcompiler", "-fPIC", "-o", os.path.join(REF_DIR, "libref_net_inj.so")]
                           + iobjs)
+    return out
+
+
+def build_reference_volume(force=False):
+    """Compile the reference's VolumeRender (core/volume.cu with camera.cu,
+    omp.cpp, vector.cu, renderResources.cu and radiancePredict.cu) with the
+    harness oracle/ref/ref_volume.cu into oracle/_ref/libref_volume.so."""
+    core = os.path.join(REF_SRC, "core")
+    if not os.path.isdir(core):
+        return None
+    os.makedirs(REF_DIR, exist_ok=True)
+    out = os.path.join(REF_DIR, "libref_volume.so")
+    ref_dir = os.path.join(HERE, "ref")
+    shim = os.path.join(ref_dir, "cuda12_texref_shim.cuh")
+    harness = os.path.join(ref_dir, "ref_volume.cu")
+    net_tu = os.path.join(ref_dir, "ref_net_tu.cu")
+    srcs = [os.path.join(core, f) for f in ("vector.cu", "renderResources.cu", "volume.cu", "camera.cu")]
+    deps = [shim, harness, net_tu] + srcs + [os.path.join(core, f) for f in
+                                             ("omp.cpp", "render.cuh", "volume.hpp", "camera.hpp", "NNWeight.cuh")]
+    if not force and _newer(out, deps):
+        return out
+    flags = ["-std=c++17", "-rdc=true", "-gencode", "arch=compute_100a,code=sm_100a",
+             "-use_fast_math", "-maxrregcount=168", "-DLINUX", "-Xcompiler", "-fPIC",
+             "-w", "-include", shim, "-I", core]
+    objs = []
+    for src in srcs + [net_tu, harness]:
+        o = os.path.join(REF_DIR, "vol_" + os.path.basename(src).replace(".cu", ".o"))
+        subprocess.check_call(["nvcc"] + flags + ["-c", src, "-o", o])
+        objs.append(o)
+    o = os.path.join(REF_DIR, "vol_omp.o")
+    subprocess.check_call(["nvcc", "-std=c++17", "-w", "-Xcompiler", "-fPIC", "-I", core, "-x", "cu", "-c",
+                           os.path.join(core, "omp.cpp"), "-o", o])
+    objs.append(o)
+    subprocess.check_call(["nvcc", "-shared", "-gencode", "arch=compute_100a,code=sm_100a",
+                           "-Xcompiler", "-fPIC", "-o", out] + objs)
     return out
 
 

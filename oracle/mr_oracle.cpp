@@ -10,6 +10,7 @@
 #include <omp.h>
 
 #include <atomic>
+#include <cstring>
 #include <vector>
 
 #include "../include/mrpnn_b200.h"
@@ -511,6 +512,47 @@ extern "C" {
 void orc_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
   philox4x32_10(ctr, key[0], key[1], out);
 }
+
+// Xavier-uniform weights of the benchmark network (the workload definition
+// the library's mr_weights_xavier draws): array a of the blob (declaration
+// order of core/NNWeight.cuh), element e uses word e % 4 of
+// Philox(seed, 0; a, e / 4, 0, TAG_MISC); weights uniform in
+// +-sqrt(6 / (fan_in + fan_out)), biases 0. Fan-in / fan-out from the
+// layer shapes of core/radiancePredict.cu:370-485.
+void orc_weights_xavier(uint32_t seed, float* out) {
+  struct Shape { int in, out; };
+  auto shape = [](const char* name, int n) -> Shape {
+    const size_t len = std::strlen(name);
+    if (!std::strcmp(name, "LSEFin1W")) return {75, 16};
+    if (!std::strcmp(name, "LSEFin2W")) return {16, 6};
+    if (!std::strcmp(name, "LGGSW")) return {3, 8};
+    if (!std::strcmp(name, "LC1W")) return {128, 64};
+    if (!std::strcmp(name, "LC2W")) return {64, 32};
+    if (!std::strcmp(name, "LXW")) return {32, 16};
+    if (!std::strcmp(name, "LX12W")) return {16, 1};
+    if (len > 4 && name[len - 2] == '2' && name[len - 1] == 'W' && n == 24) return {8, 3};
+    const int k = (int)std::lround(std::sqrt((double)n));
+    return {k, k};
+  };
+  int a = 0;
+  size_t off = 0;
+#define ORC_XAV(name, n)                                                            \
+  {                                                                                 \
+    const char* nm = #name;                                                         \
+    const bool bias = nm[std::strlen(nm) - 1] == 'B';                               \
+    const Shape sh = shape(nm, (n));                                                \
+    const float lim = bias ? 0.0f : (float)std::sqrt(6.0 / (double)(sh.in + sh.out)); \
+    for (int e = 0; e < (n); ++e) {                                                 \
+      uint32_t ctr[4] = {(uint32_t)a, (uint32_t)(e >> 2), 0u, (uint32_t)TAG_MISC}, o[4]; \
+      philox4x32_10(ctr, seed, 0u, o);                                              \
+      out[off + e] = bias ? 0.0f : (2.0f * u01(o[e & 3]) - 1.0f) * lim;             \
+    }                                                                               \
+    off += (n);                                                                     \
+    ++a;                                                                            \
+  }
+  MR_WEIGHT_LIST(ORC_XAV)
+#undef ORC_XAV
+}
 void orc_uniforms(uint32_t seed, uint32_t a, uint32_t b, uint32_t tag, int n, float* out) {
   Rng r(seed, a, b, tag);
   for (int i = 0; i < n; ++i) out[i] = r.next();
@@ -605,82 +647,98 @@ void orc_build_tr(const float* mips, float alpha, const float* light, float* tr,
   }
 }
 
-// Radical inverse in base b (unscrambled), clamped below 1.
-static float radical_inverse(uint32_t base, uint32_t a) {
+// Scrambled radical inverse (ScrambledRadicalInverse, core/volume.cu:1060-1076):
+// digit d of a in base b is replaced by perm[d]; the tail of perm[0] digits
+// adds perm[0] / (b - 1) of the last digit weight; clamped below 1.
+static float scrambled_radical_inverse(uint32_t base, const uint8_t* perm, uint32_t a) {
   const float inv_base = 1.0f / (float)base;
   uint32_t rev = 0;
   float inv_bn = 1.0f;
   while (a) {
     uint32_t next = a / base;
     uint32_t digit = a - next * base;
-    rev = rev * base + digit;
+    rev = rev * base + perm[digit];
     inv_bn *= inv_base;
     a = next;
   }
-  return std::min((float)rev * inv_bn, 0.99999994f);
+  return std::min(inv_bn * ((float)rev + inv_base * (float)perm[0] / (1.0f - inv_base)), 0.99999994f);
 }
+// The permutation-table entries of the Halton dimensions Fill_Hg draws
+// (dims 0, 1, 2, 4 = bases 2, 3, 5, 11; core/volume.cu:956-958).
+static const uint8_t kPerm2[2] = {0, 1}, kPerm3[3] = {2, 1, 0}, kPerm5[5] = {4, 1, 2, 3, 0},
+                     kPerm11[11] = {8, 3, 5, 4, 7, 2, 6, 9, 1, 10, 0};
 static inline float fracf(float f) { return f - (float)(long)f; }
 
-// Fill_Hg (core/volume.cu:1082-1160): lut[i + j*512] = average of HG over a
+// One texel of Fill_Hg (core/volume.cu:1082-1160): the average of HG over a
 // ball of radius tan(angle_j) centred on direction cos_i at unit distance,
-// 1024 Halton samples (dims 2,3,5 and 11) mixing HG-sampled chords and
-// uniform ball points; per-texel Cranley-Patterson offset from Philox.
+// 1024 scrambled Halton samples (dims 0,1,2 and 4) mixing HG-sampled chords
+// and uniform ball points, shifted by the texel's offset bn.
+static float hglut_texel(int i, int j, float g, float bn) {
+  float costheta = (((float)i + 0.5f) / 512.0f) * 2.0f - 1.0f;
+  float aa = ((float)j + 0.5f) / 512.0f;
+  float angle = aa * 3.1415926535f * 60.0f / 180.0f;
+  float hg = 0.0f;
+  float R = std::tan(angle);
+  V3 view = v3(1, 0, 0);
+  V3 D = v3(costheta, std::sqrt(1.0f - costheta * costheta), 0.0f);
+  float mis = 0.0f;
+  {
+    float p = R * R - 1 + D.x * D.x;
+    if (p > 0) {
+      float sdotl = g > 0 ? D.x : -D.x;
+      float w = std::sqrt(p);
+      float d0 = std::max(0.0f, sdotl - w) / R;
+      float d1 = (sdotl + w) / R;
+      float d = d1 * d1 * d1 - d0 * d0 * d0;
+      mis = (d1 > d0) ? d : 0.0f;
+    }
+    mis = std::min(std::max(mis, 1e-8f), 1.0f);
+    float a = std::fabs(g);
+    a = a < 0.6f ? 0.0f : (a < 0.7f ? (a - 0.6f) * 9.0f : (std::pow((a - 0.7f) / 0.3f, 0.05f) * 0.1f + 0.9f));
+    mis = 1.0f - 1.0f / (1.0f + a * mis / (1.0f - a));
+  }
+  for (int k = 0; k < 1024; ++k) {
+    float r0 = fracf(scrambled_radical_inverse(2, kPerm2, k) + bn);
+    float r1 = fracf(scrambled_radical_inverse(3, kPerm3, k) + bn);
+    if (fracf(scrambled_radical_inverse(11, kPerm11, k) + bn) < mis) {
+      V3 l = hg_sample_dir(r0, r1, view, g);
+      float sdotl = dot(D, l);
+      float p = R * R - 1 + sdotl * sdotl;
+      if (p <= 0) continue;
+      float w = std::sqrt(p);
+      float d0 = sdotl - w;
+      float d1 = (sdotl + w) / R;
+      d0 = std::max(0.0f, d0) / R;
+      float d = d1 * d1 * d1 - d0 * d0 * d0;
+      hg += std::max(0.0f, d / 4);
+    } else {
+      float r2 = fracf(scrambled_radical_inverse(5, kPerm5, k) + bn);
+      float theta = r0 * 2.0f * 3.1415926535f;
+      float phi = std::acos(2.0f * r1 - 1.0f);
+      float rr = std::cbrt(r2);
+      float x = R * rr * std::sin(phi) * std::cos(theta);
+      float y = R * rr * std::sin(phi) * std::sin(theta);
+      float z = R * rr * std::cos(phi);
+      V3 rp = v3(x, y, z) + D;
+      hg += hg_phase(dot(normalize(rp), view), g);
+    }
+  }
+  return hg / 1024.0f;
+}
+
+// The 512 x 512 table, lut[i + j*512], with the per-texel offset drawn from
+// Philox (seed; i + 512 j, 0, TAG_LUT) where the reference draws it from curand.
 void orc_build_hglut(float g, uint32_t seed, float* lut, int nthreads) {
 #pragma omp parallel for num_threads(nthreads) schedule(static)
   for (int j = 0; j < 512; ++j)
-    for (int i = 0; i < 512; ++i) {
-      float costheta = (((float)i + 0.5f) / 512.0f) * 2.0f - 1.0f;
-      float aa = ((float)j + 0.5f) / 512.0f;
-      float angle = aa * 3.1415926535f * 60.0f / 180.0f;
-      float bn = u01_tag(seed, (uint32_t)(i + j * 512), 0, TAG_LUT);
-      float hg = 0.0f;
-      float R = std::tan(angle);
-      V3 view = v3(1, 0, 0);
-      V3 D = v3(costheta, std::sqrt(1.0f - costheta * costheta), 0.0f);
-      float mis = 0.0f;
-      {
-        float p = R * R - 1 + D.x * D.x;
-        if (p > 0) {
-          float sdotl = g > 0 ? D.x : -D.x;
-          float w = std::sqrt(p);
-          float d0 = std::max(0.0f, sdotl - w) / R;
-          float d1 = (sdotl + w) / R;
-          float d = d1 * d1 * d1 - d0 * d0 * d0;
-          mis = (d1 > d0) ? d : 0.0f;
-        }
-        mis = std::min(std::max(mis, 1e-8f), 1.0f);
-        float a = std::fabs(g);
-        a = a < 0.6f ? 0.0f : (a < 0.7f ? (a - 0.6f) * 9.0f : (std::pow((a - 0.7f) / 0.3f, 0.05f) * 0.1f + 0.9f));
-        mis = 1.0f - 1.0f / (1.0f + a * mis / (1.0f - a));
-      }
-      for (int k = 0; k < 1024; ++k) {
-        if (fracf(radical_inverse(11, k) + bn) < mis) {
-          float r0 = fracf(radical_inverse(2, k) + bn), r1 = fracf(radical_inverse(3, k) + bn);
-          V3 l = hg_sample_dir(r0, r1, view, g);
-          float sdotl = dot(D, l);
-          float p = R * R - 1 + sdotl * sdotl;
-          if (p <= 0) continue;
-          float w = std::sqrt(p);
-          float d0 = sdotl - w;
-          float d1 = (sdotl + w) / R;
-          d0 = std::max(0.0f, d0) / R;
-          float d = d1 * d1 * d1 - d0 * d0 * d0;
-          hg += std::max(0.0f, d / 4);
-        } else {
-          float r0 = fracf(radical_inverse(2, k) + bn), r1 = fracf(radical_inverse(3, k) + bn);
-          float r2 = fracf(radical_inverse(5, k) + bn);
-          float theta = r0 * 2.0f * 3.1415926535f;
-          float phi = std::acos(2.0f * r1 - 1.0f);
-          float rr = std::cbrt(r2);
-          float x = R * rr * std::sin(phi) * std::cos(theta);
-          float y = R * rr * std::sin(phi) * std::sin(theta);
-          float z = R * rr * std::cos(phi);
-          V3 rp = v3(x, y, z) + D;
-          hg += hg_phase(dot(normalize(rp), view), g);
-        }
-      }
-      lut[i + j * 512] = hg / 1024.0f;
-    }
+    for (int i = 0; i < 512; ++i) lut[i + j * 512] = hglut_texel(i, j, g, u01_tag(seed, (uint32_t)(i + j * 512), 0, TAG_LUT));
+}
+
+// n texels (i = texel[k] % 512, j = texel[k] / 512) with given offsets bn[k]:
+// evaluates the table's estimator with the offsets another generator drew.
+void orc_hglut_texels(float g, const int32_t* texel, const float* bn, int n, float* out, int nthreads) {
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+  for (int k = 0; k < n; ++k) out[k] = hglut_texel(texel[k] % 512, texel[k] / 512, g, bn[k]);
 }
 
 // Delta-tracking render (VolumeRender::Render, rt = PT). Pixel (row, col),

@@ -10,6 +10,7 @@ _lib = None
 
 f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
 u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
 
@@ -36,6 +37,7 @@ def lib():
         path = build_oracle()
         L = C.CDLL(path)
         L.orc_philox.argtypes = [u32p, u32p, u32p]
+        L.orc_weights_xavier.argtypes = [C.c_uint32, f32p]
         L.orc_uniforms.argtypes = [C.c_uint32] * 4 + [C.c_int, f32p]
         L.orc_hg.argtypes = [C.c_float, C.c_float]
         L.orc_hg.restype = C.c_float
@@ -58,6 +60,7 @@ def lib():
         L.orc_build_mips.restype = C.c_float
         L.orc_build_tr.argtypes = [f32p, C.c_float, f32p, f32p, C.c_int]
         L.orc_build_hglut.argtypes = [C.c_float, C.c_uint32, f32p, C.c_int]
+        L.orc_hglut_texels.argtypes = [C.c_float, i32p, f32p, C.c_int, f32p, C.c_int]
         L.orc_render_pt.argtypes = [f32p, C.c_int, C.c_float, C.c_void_p, C.c_int,
                                     C.c_int, f64p, f64p, u64p, C.c_int]
         L.orc_render_neural.argtypes = [f32p, C.c_int, C.c_float, f32p, f32p, f32p, f32p, f32p,
@@ -109,6 +112,25 @@ def uniforms(seed, a, b, tag, n):
     return out
 
 
+def xavier_weights(seed):
+    """The benchmark network's Xavier(seed) weights in the blob layout."""
+    out = np.zeros(49673, np.float32)
+    lib().orc_weights_xavier(int(seed), out)
+    return out
+
+
+def reference_stencil():
+    """The reference's 160 stencil directions (core/vector.cu:77-172), read
+    from the table the library is compiled with."""
+    import re
+    txt = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "internship_b200", "csrc",
+                            "mr_ref_stencil.inc")).read()
+    body = txt[txt.index("{") + 1:txt.index("}")]
+    vals = np.array([float(t.rstrip("f")) for t in re.findall(r"-?[0-9.]+(?:e[-+]?[0-9]+)?f", body)], np.float32)
+    assert vals.size == 480
+    return vals
+
+
 def build_mips(density):
     density = _a(density)
     res = round(density.size ** (1 / 3))
@@ -128,6 +150,15 @@ def build_hglut(g, seed):
     lut = np.zeros(512 * 512, np.float32)
     lib().orc_build_hglut(float(g), int(seed), lut, nthreads())
     return lut
+
+
+def hglut_texels(g, texel, bn):
+    """Fill_Hg's estimator at texels `texel` (i + 512 j) with offsets `bn`."""
+    texel = np.ascontiguousarray(texel, np.int32)
+    bn = np.ascontiguousarray(bn, np.float32)
+    out = np.zeros(texel.size, np.float32)
+    lib().orc_hglut_texels(float(g), texel, bn, texel.size, out, nthreads())
+    return out
 
 
 def render_pt(density, max_density, params, row0=0, row1=None):

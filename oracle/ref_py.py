@@ -9,9 +9,12 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_SO = os.path.join(HERE, "_ref", "libref_mrpnn.so")
 INJ_SO = os.path.join(HERE, "_ref", "libref_net_inj.so")
+VOL_SO = os.path.join(HERE, "_ref", "libref_volume.so")
 
 f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
 
 
 def available():
@@ -117,3 +120,91 @@ def raw_to_desc(raw, frame, light, g):
     hg = ((np.float32(1) - g2) / (d * np.sqrt(d))) * np.float32(0.25)
     desc[:, 384] = np.log(hg + np.float32(1))
     return desc
+
+
+def _f(v):
+    return np.ascontiguousarray(v, np.float32).ravel()
+
+
+class RefVolume:
+    """The reference's VolumeRender and its table kernels (ref_volume.cu):
+    Update, Fill_TR, Fill_Hg, Denoise, GetSamples, the interactive Render and
+    SaveBMP, all the reference's own code."""
+
+    def __init__(self, res=None):
+        L = C.CDLL(VOL_SO)
+        L.refv_create.argtypes = [C.c_int]
+        L.refv_create.restype = C.c_void_p
+        L.refv_destroy.argtypes = [C.c_void_p]
+        L.refv_set_density_update.argtypes = [C.c_void_p, f32p, C.POINTER(C.c_float)]
+        L.refv_set_scalars.argtypes = [C.c_void_p, C.c_float, f32p, C.c_float, f32p]
+        L.refv_fill_tr.argtypes = [f32p, C.c_float, f32p, f32p]
+        L.refv_fill_hg.argtypes = [C.c_float, C.c_int, f32p, f32p]
+        L.refv_denoise.argtypes = [f32p, f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, u32p]
+        L.refv_get_samples.argtypes = [C.c_void_p, C.c_int, f32p, f32p, f32p, C.c_float, C.c_float, C.c_float,
+                                       C.c_int, C.c_int, C.c_int, f32p]
+        L.refv_interactive.argtypes = [C.c_void_p, C.c_int, C.c_int, f32p, f32p, f32p, f32p, f32p, C.c_float, C.c_int,
+                                       C.c_float, C.c_int, C.c_int, C.c_int, f32p, f32p, u32p]
+        L.refv_save_bmp.argtypes = [u8p, C.c_int, C.c_int, C.c_char_p]
+        L.refv_tone_host.argtypes = [C.c_int, f32p, C.c_int, f32p]
+        self.L = L
+        self.h = None
+        self.res = res
+        if res is not None:
+            self.h = L.refv_create(int(res))
+
+    def close(self):
+        if self.h:
+            self.L.refv_destroy(self.h)
+            self.h = None
+
+    def set_density(self, density):
+        md = C.c_float()
+        assert self.L.refv_set_density_update(self.h, _f(density), C.byref(md)) == 0
+        return md.value
+
+    def set_scalars(self, tr_scale=1.0, scatter=(0.99,) * 3, env_exp=1.0, env=(0, 0, 0)):
+        assert self.L.refv_set_scalars(self.h, float(tr_scale), _f(scatter), float(env_exp), _f(env)) == 0
+
+    def fill_tr(self, mips, alpha, light):
+        out = np.zeros(sum((128 >> k) ** 3 for k in range(8)), np.float32)
+        assert self.L.refv_fill_tr(_f(mips), float(alpha), _f(light), out) == 0
+        return out
+
+    def fill_hg(self, g, randnum=0):
+        lut = np.zeros(512 * 512, np.float32)
+        bn = np.zeros(512 * 512, np.float32)
+        assert self.L.refv_fill_hg(float(g), int(randnum), lut, bn) == 0
+        return lut, bn
+
+    def denoise(self, accum, hist, w, h, frame, flip, tone, denoise, exposure=1.0):
+        out = np.zeros(w * h, np.uint32)
+        assert self.L.refv_denoise(_f(accum), _f(hist), w, h, int(frame), int(flip), int(tone), int(denoise),
+                                   float(exposure), out) == 0
+        return out
+
+    def get_samples(self, pos, dirs, light, alpha, g, scatter, bounces, spp, randnum=0):
+        n = len(pos)
+        out = np.zeros(3 * n, np.float32)
+        assert self.L.refv_get_samples(self.h, n, _f(pos), _f(dirs), _f(light), float(alpha), float(g), float(scatter),
+                                       int(bounces), int(spp), int(randnum), out) == 0
+        return out.reshape(n, 3)
+
+    def interactive(self, w, h, ori, up, right, light, light_color, alpha, bounces, g, frames, tone=2, denoise=1):
+        acc = np.zeros(w * h * 3, np.float32)
+        hist = np.zeros(w * h * 33, np.float32)
+        bgra = np.zeros(w * h, np.uint32)
+        assert self.L.refv_interactive(self.h, w, h, _f(ori), _f(up), _f(right), _f(light), _f(light_color),
+                                       float(alpha), int(bounces), float(g), int(frames), int(tone), int(denoise),
+                                       acc, hist, bgra) == 0
+        return acc, hist, bgra
+
+    def save_bmp(self, rgba, w, h, path):
+        assert self.L.refv_save_bmp(np.ascontiguousarray(rgba, np.uint8).ravel(), w, h, path.encode()) == 0
+        return path + ".bmp"
+
+    def tone_host(self, rgb, tone):
+        rgb = _f(rgb)
+        out = np.zeros_like(rgb)
+        assert self.L.refv_tone_host(rgb.size // 3, rgb, int(tone), out) == 0
+        return out.reshape(-1, 3)

@@ -62,12 +62,21 @@ def test_xavier_weights_deterministic_and_scaled():
     assert off == _lib.WEIGHT_TOTAL
 
 
-def test_builtin_stencil_shape():
-    s = mr.builtin_stencil().reshape(160, 3)
+@pytest.mark.parametrize("which", ["builtin", "spiral"])
+def test_stencil_shape(which):
+    s = (mr.builtin_stencil() if which == "builtin" else mr.spiral_stencil()).reshape(160, 3)
     r = np.linalg.norm(s, axis=1)
     assert r[0] == 0
     np.testing.assert_allclose(r[1:64], 1.0, atol=1e-6)
     assert (r[64:] <= 1.0 + 1e-6).all() and (r[64:] > 0.3).all()
+
+
+def test_default_stencil_is_the_reference_table():
+    """mr_network_create(stencil=NULL) gathers at the reference's own 160
+    directions (core/vector.cu:77-172), bit for bit as the compiler reads them."""
+    st = W.load_stencil_source(reference_file("core/vector.cu"))
+    assert np.array_equal(mr.builtin_stencil(), st)
+    assert not np.array_equal(mr.spiral_stencil(), st)
 
 
 def test_layout_matches_header_total():
