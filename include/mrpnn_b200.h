@@ -70,7 +70,8 @@ typedef struct {
   float g;                /* Henyey-Greenstein asymmetry */
   mr_float3 scatter_rate; /* per-channel albedo (SetScatterRate) */
   float tr_scale;         /* NEE step scale (SetTrScale), normally 1 */
-  mr_float3 env_color;    /* radiance of escaped rays (constant environment), 0 = black */
+  mr_float3 env_color;    /* radiance of escaped rays (constant environment), 0 = black; with an
+                             environment map (mr_volume_set_hdri) the map's scale (SetEnvExp) */
   int32_t max_bounces;    /* multiScatter */
   int32_t spp;            /* samples per pixel (PT); neural renders 1 primary sample per pass */
   uint32_t seed;          /* Philox key */
@@ -124,6 +125,24 @@ int mr_volume_update_tr(mr_volume* v, mr_float3 light_dir, float alpha, void* st
 /* UpdateHGLut(g) (core/volume.cu:1161-1183): 512x512 cone-averaged HG table.
  * Skipped when g and seed are unchanged. */
 int mr_volume_update_hglut(mr_volume* v, float g, uint32_t seed, void* stream);
+/* SetHDRI (core/volume.cu:1426-1458) from pixels: host_rgba is w x h RGBA
+ * fp32, row 0 looking straight up; direction d maps to column
+ * u = atan2(-d.z, d.x) / 2pi + 1/2 and row v = acos(d.y) / pi, sampled
+ * bilinearly with wrap (SkyBox, core/render.cuh:57-61). Escaped rays of every
+ * render of this volume then see map(d) * env_color (env_color plays the part
+ * of SetEnvExp); neural renders also draw each pass's light from the map or
+ * from the directional light as the reference's Render does
+ * (core/volume.cu:417-432; see mr_render). Waits for the device when it
+ * replaces a map. */
+int mr_volume_set_hdri(mr_volume* v, const float* host_rgba, int32_t w, int32_t h);
+/* SetHDRI(path): a Radiance RGBE (.hdr) file (core/hdr_loader.h:249). */
+int mr_volume_load_hdri(mr_volume* v, const char* path);
+/* Removes the map: escaped rays see the constant env_color again. */
+int mr_volume_clear_hdri(mr_volume* v);
+/* load_hdr_float4 (core/hdr_loader.h:249) alone, host only: *width, *height
+ * receive the size; host_rgba (may be NULL to query the size) receives
+ * width*height RGBA floats (alpha 0) if capacity allows. */
+int mr_hdr_read(const char* path, float* host_rgba, size_t capacity, int32_t* width, int32_t* height);
 /* VolumeRender::max_density after mr_volume_update. */
 int mr_volume_max_density(const mr_volume* v, float* out);
 int mr_volume_resolution(const mr_volume* v, int32_t* out);
@@ -156,7 +175,13 @@ int mr_weights_xavier(uint32_t seed, float* host_out, size_t count);
 /* VolumeRender::Render(int2 size, ...) (core/volume.cu:410-467) into caller
  * device memory: dev_rgb = width*height*3 fp32, row-major, mean radiance over
  * the samples. PT = delta tracking; MRPNN = neural form (network required;
- * call mr_volume_update_tr / _hglut first or let the call do it). */
+ * call mr_volume_update_tr / _hglut first or let the call do it). With an
+ * environment map on the volume, each MRPNN pass (sample_offset) takes its
+ * light from the map with probability 4e / (4e + max(light_color)),
+ * e = max(env_color): direction = the R2 point sample_offset on the sphere,
+ * colour = map * env_color * 4 / that probability, else the directional
+ * light with colour / (1 - probability); the transmittance pyramid is rebuilt
+ * for the chosen light. The coin is Philox(seed; sample_offset, 0, 0, 7). */
 int mr_render(mr_volume* v, const mr_network* net, const mr_render_params* p, float* dev_rgb,
               void* stream);
 /* Same, synchronous, into host memory (the reference returns vector<float3>). */
@@ -232,6 +257,12 @@ int mr_tc_selftest_tf32(int32_t n, int32_t k, const float* host_a, const float* 
  * texel is subnormal (the texture unit reads those as 0). */
 #define MR_SAMPLER_SELFTEST_RES 32
 int mr_sampler_selftest(int32_t n, const float* host_table, const float* host_uv, float* host_out);
+/* Failure path of the kernels' bounded waits (no reference counterpart): one
+ * CTA allocates tensor memory, waits with a limit of limit_us (1 .. 10^6) on an
+ * mbarrier that nothing arrives on, records the timeout and frees the tensor
+ * memory. Returns MR_ERR_TIMEOUT (the expected outcome) with the time the wait
+ * took in *host_waited_ns (may be NULL); the device stays usable. */
+int mr_tc_wait_selftest(int32_t limit_us, int64_t* host_waited_ns);
 /* Memory-path probe (no reference counterpart): reads dev_buf (`bytes`, a
  * multiple of 16, 16-byte aligned) `passes` times with 16-byte loads that
  * bypass L1, from a resident grid; dev_sink is one device word. Time it with

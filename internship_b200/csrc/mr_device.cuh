@@ -117,7 +117,7 @@ __host__ __device__ __forceinline__ float u01(uint32_t x) {
   return ((float)(x >> 9) + 0.5f) * 1.1920928955078125e-7f;
 }
 
-enum StreamTag : uint32_t { TAG_PT = 1, TAG_NN = 2, TAG_LUT = 3, TAG_GEN = 4, TAG_LABEL = 5, TAG_MISC = 6 };
+enum StreamTag : uint32_t { TAG_PT = 1, TAG_NN = 2, TAG_LUT = 3, TAG_GEN = 4, TAG_LABEL = 5, TAG_MISC = 6, TAG_ENV = 7 };
 
 // A path's random stream: key (seed, 0), counter (a, b, block, tag); draw k is
 // word k%4 of block k/4. Four draws per Philox call, kept in registers.

@@ -391,6 +391,7 @@ extern "C" int mr_render_interactive(mr_volume* h, const mr_network* net, const 
     rc = density_gather_texture(v, s, &a.m.tex);
     if (rc) return rc;
     a.sc = make_path_scene(p);
+    attach_env(a.sc, v);
     a.cam = make_camera(p);
     a.seed = p->seed;
     a.frame = it->frame_index;

@@ -76,6 +76,12 @@ struct Volume {
   // Interactive neural mode: radiance and first-hit distance of the frame.
   void* inter = nullptr;
   size_t inter_bytes = 0;
+  // Environment map (SetHDRI): w x h RGBA fp32, row 0 = straight up, on the
+  // device for the trackers' escaped rays and on the host for the neural
+  // render's light selection.
+  float4* env_dev = nullptr;
+  std::vector<float> env_host;
+  int env_w = 0, env_h = 0;
   // Interactive delta tracking: FP64 per-pixel sums of the radiance (3), of
   // the histogram luminance l and of l^2, SoA (sum k of pixel p at
   // mom[k * mom_npx + p]), for the histogram buffer mom_hist they belong to.
@@ -181,6 +187,13 @@ int copy_to_array(cudaArray_t arr, const float* src, int r, cudaStream_t s);
 int make_gather_tex(cudaArray_t* arr, cudaTextureObject_t* tex, int r, cudaTextureAddressMode mode);
 void destroy_textures(Volume* v);
 int sm_count();
+// Points a scene's escaped-ray lookup at the volume's environment map (if any).
+struct PathScene;
+void attach_env(PathScene& sc, const Volume* v);
+// The neural render's light for this pass when the volume has an environment
+// map (the env / light choice of core/volume.cu:417-432): q's light_dir and
+// light_color are replaced in place.
+void select_env_light(const Volume* v, mr_render_params* q);
 
 }  // namespace mr
 

@@ -11,6 +11,7 @@
 //    value * 64 / 255, consecutive in index order.
 // Parsing is host code over the whole file in memory (no iostreams).
 #include <cerrno>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -124,9 +125,124 @@ static int parse_volume(const std::string& path, int* res, std::vector<float>* d
   return set_error(MR_ERR_ARG, "%s: no %s.bin and not a .txt or .vox file", path.c_str(), path.c_str());
 }
 
+// ---- Radiance RGBE (.hdr) images ----------------------------------------------------
+// Header lines up to the resolution line "-Y <h> +X <w>" (the reference's
+// loader, core/hdr_loader.h:43-104, reads the same two numbers and ignores
+// flips); then h scanlines of w pixels, each either flat (4 bytes per pixel)
+// or, for 8 <= w <= 32767, in the new run-length form: the bytes 2, 2,
+// w >> 8, w & 255, then each of the four components of the scanline as runs
+// (count > 128: repeat the next byte count - 128 times) and literal spans
+// (count <= 128: that many bytes). A pixel (r, g, b, e) is the colour
+// (c + 0.5) * 2^(e - 136) per channel, 0 when e = 0 (the Radiance format).
+static int parse_hdr(const std::string& path, int* w_out, int* h_out, std::vector<float>* rgba) {
+  std::vector<char> buf;
+  if (!read_file(path, &buf)) return set_error(MR_ERR_ARG, "%s: cannot read", path.c_str());
+  const size_t size = buf.size() - 1;
+  const unsigned char* b = (const unsigned char*)buf.data();
+  if (size < 2 || b[0] != '#' || b[1] != '?') return set_error(MR_ERR_ARG, "%s: not a Radiance file", path.c_str());
+  size_t pos = 0;
+  int w = 0, h = 0;
+  bool have_res = false;
+  while (pos < size && !have_res) {
+    size_t e = pos;
+    while (e < size && b[e] != '\n') ++e;
+    std::string line((const char*)b + pos, e - pos);
+    pos = e + 1;
+    if (line.compare(0, 7, "FORMAT=") == 0 && line.find("32-bit_rle_rgbe") == std::string::npos &&
+        line.find("32-bit_rle_xyze") == std::string::npos)
+      return set_error(MR_ERR_ARG, "%s: unsupported %s", path.c_str(), line.c_str());
+    if (!line.empty() && (line[0] == '-' || line[0] == '+')) {
+      size_t x = line.find('X'), y = line.find('Y');
+      if (x == std::string::npos || y == std::string::npos)
+        return set_error(MR_ERR_ARG, "%s: bad resolution line", path.c_str());
+      w = std::atoi(line.c_str() + x + 1);
+      h = std::atoi(line.c_str() + y + 1);
+      have_res = true;
+    }
+  }
+  if (!have_res || w <= 0 || h <= 0 || (long long)w * h > (1ll << 28))
+    return set_error(MR_ERR_ARG, "%s: bad or missing resolution", path.c_str());
+  rgba->assign((size_t)w * h * 4, 0.0f);
+  std::vector<unsigned char> line((size_t)w * 4);
+  auto take = [&](size_t n) -> const unsigned char* {
+    if (pos + n > size) return nullptr;
+    const unsigned char* p = b + pos;
+    pos += n;
+    return p;
+  };
+  const bool can_rle = w >= 8 && w <= 0x7fff;
+  for (int j = 0; j < h; ++j) {
+    const unsigned char* hd = (pos + 4 <= size) ? b + pos : nullptr;
+    if (can_rle && hd && hd[0] == 2 && hd[1] == 2 && !(hd[2] & 128)) {
+      pos += 4;
+      if (((hd[2] << 8) | hd[3]) != w) return set_error(MR_ERR_ARG, "%s: scanline %d length mismatch", path.c_str(), j);
+      for (int c = 0; c < 4; ++c) {
+        for (int x = 0; x < w;) {
+          const unsigned char* n = take(1);
+          if (!n) return set_error(MR_ERR_ARG, "%s: truncated scanline %d", path.c_str(), j);
+          int cnt = *n;
+          if (cnt > 128) {
+            cnt &= 127;
+            const unsigned char* v = take(1);
+            if (!v || cnt == 0 || x + cnt > w) return set_error(MR_ERR_ARG, "%s: bad run in scanline %d", path.c_str(), j);
+            for (int k = 0; k < cnt; ++k) line[(size_t)(x++) * 4 + c] = *v;
+          } else {
+            const unsigned char* v = take((size_t)cnt);
+            if (!v || cnt == 0 || x + cnt > w) return set_error(MR_ERR_ARG, "%s: bad span in scanline %d", path.c_str(), j);
+            for (int k = 0; k < cnt; ++k) line[(size_t)(x++) * 4 + c] = v[k];
+          }
+        }
+      }
+    } else {
+      const unsigned char* v = take((size_t)w * 4);
+      if (!v) return set_error(MR_ERR_ARG, "%s: truncated scanline %d", path.c_str(), j);
+      std::memcpy(line.data(), v, (size_t)w * 4);
+    }
+    for (int x = 0; x < w; ++x) {
+      const unsigned char* q = &line[(size_t)x * 4];
+      float* o = &(*rgba)[((size_t)j * w + x) * 4];
+      if (q[3]) {
+        const float sc = std::ldexp(1.0f, (int)q[3] - 136);
+        o[0] = ((float)q[0] + 0.5f) * sc;
+        o[1] = ((float)q[1] + 0.5f) * sc;
+        o[2] = ((float)q[2] + 0.5f) * sc;
+      }
+    }
+  }
+  *w_out = w;
+  *h_out = h;
+  return MR_OK;
+}
+
 }  // namespace mr
 
 using namespace mr;
+
+extern "C" int mr_hdr_read(const char* path, float* host_rgba, size_t capacity, int32_t* width, int32_t* height) {
+  clear_error();
+  if (!path || !width || !height) return set_error(MR_ERR_ARG, "mr_hdr_read: NULL argument");
+  int w = 0, h = 0;
+  std::vector<float> px;
+  int rc = parse_hdr(path, &w, &h, &px);
+  if (rc) return rc;
+  *width = w;
+  *height = h;
+  if (host_rgba) {
+    if (capacity < px.size()) return set_error(MR_ERR_ARG, "mr_hdr_read: %zu floats needed", px.size());
+    std::memcpy(host_rgba, px.data(), px.size() * sizeof(float));
+  }
+  return MR_OK;
+}
+
+extern "C" int mr_volume_load_hdri(mr_volume* v, const char* path) {
+  clear_error();
+  if (!v || !path) return set_error(MR_ERR_ARG, "mr_volume_load_hdri: NULL argument");
+  int w = 0, h = 0;
+  std::vector<float> px;
+  int rc = parse_hdr(path, &w, &h, &px);
+  if (rc) return rc;
+  return mr_volume_set_hdri(v, px.data(), w, h);
+}
 
 extern "C" int mr_volume_file_read(const char* path, float* host_out, size_t capacity, int32_t* resolution) {
   clear_error();

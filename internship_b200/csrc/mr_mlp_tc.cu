@@ -950,6 +950,42 @@ __global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(const __grid_consta
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_holder), "r"(kTmemCols));
   }
 }
+// Failure path of the bounded waits: allocates tensor memory, initialises an
+// mbarrier that nothing will ever arrive on, waits for it with a limit of
+// limit_ns, records the timeout in *err with the time waited, and frees the
+// tensor memory on the way out, as every kernel of this file does when a wait
+// gives up.
+__global__ void __launch_bounds__(128, 1) k_tc_wait_selftest(uint64_t limit_ns, int* err,
+                                                             unsigned long long* waited_ns) {
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t holder;
+  const int t = threadIdx.x, warp = t >> 5;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&holder)),
+                 "r"(128));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (t == 0) mbar_init(smem_u32(&mbar), 1);
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = holder;
+  const uint64_t t0 = globaltimer();
+  const bool ok = mbar_wait(smem_u32(&mbar), 0, limit_ns);  // no arrival: runs out
+  const uint64_t t1 = globaltimer();
+  if (!ok && t == 0) {
+    atomicExch(err, 1);
+    *waited_ns = t1 - t0;
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128));
+  }
+}
+
 // One tile through the same descriptors: D[128 x N] = A[128 x K] * B[N x K]^T.
 template <int N, int K>
 __global__ void __launch_bounds__(128, 1) k_tc_selftest(const uint16_t* __restrict__ A, const uint16_t* __restrict__ B,
@@ -1339,6 +1375,34 @@ extern "C" int mr_tc_selftest(int32_t n, int32_t k, const uint16_t* host_a, cons
   cudaFree(b);
   cudaFree(d);
   cudaFree(err);
+  return rc;
+}
+
+extern "C" int mr_tc_wait_selftest(int32_t limit_us, int64_t* host_waited_ns) {
+  clear_error();
+  if (limit_us <= 0 || limit_us > 1000000) return set_error(MR_ERR_ARG, "mr_tc_wait_selftest: limit %d us", limit_us);
+  int* err = nullptr;
+  unsigned long long* waited = nullptr;
+  MR_CUDA(cudaMalloc(&err, 4));
+  MR_CUDA(cudaMalloc(&waited, 8));
+  MR_CUDA(cudaMemset(err, 0, 4));
+  MR_CUDA(cudaMemset(waited, 0, 8));
+  k_tc_wait_selftest<<<1, 128>>>((uint64_t)limit_us * 1000ull, err, waited);
+  int rc = MR_OK;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) rc = cuda_error(e, "wait selftest");
+  int he = 0;
+  unsigned long long w = 0;
+  if (rc == MR_OK) {
+    cudaMemcpy(&he, err, 4, cudaMemcpyDeviceToHost);
+    cudaMemcpy(&w, waited, 8, cudaMemcpyDeviceToHost);
+    if (host_waited_ns) *host_waited_ns = (int64_t)w;
+    rc = he ? set_error(MR_ERR_TIMEOUT, "wait selftest: the mbarrier wait gave up after %llu ns", w)
+            : set_error(MR_ERR_STATE, "wait selftest: the wait completed although nothing arrived");
+  }
+  cudaFree(err);
+  cudaFree(waited);
   return rc;
 }
 

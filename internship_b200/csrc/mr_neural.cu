@@ -118,9 +118,10 @@ __device__ __forceinline__ unsigned trace_pixel(const Medium& m, const PathScene
   frame_from(rng, sc.L, f.LX, ly, lz);
   if (dist) dist[pix] = active ? length(cam.ori - pos) : -1.0f;
   if (!active) {
-    out[3 * (size_t)pix + 0] = fmaxf(sc.env.x, 0.0f);
-    out[3 * (size_t)pix + 1] = fmaxf(sc.env.y, 0.0f);
-    out[3 * (size_t)pix + 2] = fmaxf(sc.env.z, 0.0f);
+    const F3 e = sky(sc, dir);  // SkyBox(dir) for pixels that see no medium
+    out[3 * (size_t)pix + 0] = fmaxf(e.x, 0.0f);
+    out[3 * (size_t)pix + 1] = fmaxf(e.y, 0.0f);
+    out[3 * (size_t)pix + 2] = fmaxf(e.z, 0.0f);
     return 0;
   }
   float d2 = ray_box_distance(pos, f.LX);
@@ -575,6 +576,11 @@ static int render_neural_impl(Volume* v, const Network* net, const mr_render_par
   if (!v->mips_valid) return set_error(MR_ERR_STATE, "render before mr_volume_update");
   if (p->precision != MR_PREC_FP32 && p->precision != MR_PREC_BF16 && p->precision != MR_PREC_FP8)
     return set_error(MR_ERR_ARG, "unknown precision %d", p->precision);
+  // with an environment map, this pass's light is drawn from it or from the
+  // directional light (the transmittance pyramid follows the chosen light)
+  mr_render_params q = *p;
+  select_env_light(v, &q);
+  p = &q;
   F3 L = normalize(to_f3(p->light_dir));
   // UpdateHGLut / Update_TR on demand (core/volume.cu:434-437).
   if (!v->lut_valid || v->lut_g != p->g || v->lut_seed != p->seed) {
@@ -615,6 +621,7 @@ static int neural_passes(Volume* v, const Network* net, const mr_render_params* 
     if (rc) return rc;
   }
   ta.sc = make_path_scene(p);
+  attach_env(ta.sc, v);
   ta.cam = make_camera(p);
   ta.seed = p->seed;
   ta.frame_index = p->sample_offset;
@@ -1180,6 +1187,7 @@ extern "C" int mr_batch_prepare(mr_batch* h, const mr_network* nh, int64_t wave_
       if (rc) return rc;
     }
     j.sc = make_path_scene(p);
+    attach_env(j.sc, v);  // escaped rays see the map; the light stays the job's directional light
     j.cam = make_camera(p);
     j.seed = p->seed;
     j.frame = p->sample_offset;

@@ -40,8 +40,12 @@ __device__ __forceinline__ uint64_t globaltimer() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// Bounded wait for the mbarrier phase with the given parity (2 s limit).
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+// Bounded wait for the mbarrier phase with the given parity: false once
+// limit_ns (default 2 s of %globaltimer) has passed without the phase
+// completing. Callers then record the failure in an error word, leave the
+// pipeline uniformly and free their tensor memory.
+constexpr uint64_t kWaitLimitNs = 2000000000ull;
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, uint64_t limit_ns = kWaitLimitNs) {
   uint64_t t0 = 0;
   for (uint32_t it = 0;; ++it) {
     uint32_t done;
@@ -53,7 +57,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
         : "memory");
     if (done) return true;
     if (it == 0) t0 = globaltimer();
-    else if ((it & 63) == 0 && globaltimer() - t0 > 2000000000ull) return false;
+    else if ((it & 63) == 0 && globaltimer() - t0 > limit_ns) return false;
   }
 }
 // One arrival on mbar that also expects `bytes` of asynchronous copies.

@@ -3,6 +3,9 @@
 // warp-aggregated atomics and start a new path as soon as theirs ends, so that
 // lanes stay busy however long individual paths run. Replaces the
 // one-launch-per-spp RenderCamera<false> loop of core/volume.cu:147-179,415-459.
+#include <algorithm>
+#include <cmath>
+
 #include "mr_internal.h"
 #include "mr_track.cuh"
 
@@ -119,7 +122,68 @@ PathScene make_path_scene(const mr_render_params* p) {
   sc.alpha = p->alpha;
   sc.g = p->g;
   sc.max_bounces = p->max_bounces;
+  sc.env_map = nullptr;
+  sc.env_w = sc.env_h = 0;
   return sc;
+}
+
+void attach_env(PathScene& sc, const Volume* v) {
+  sc.env_map = v->env_dev;
+  sc.env_w = v->env_w;
+  sc.env_h = v->env_h;
+}
+
+// Image_host::Sample (core/volume.hpp:22-42): bilinear with clamped texel
+// indices at pos = uv * size - 1/2.
+static F3 env_sample_host(const Volume* v, float u, float vv) {
+  const int w = v->env_w, h = v->env_h;
+  auto at = [&](int x, int y) {
+    x = std::min(std::max(x, 0), w - 1);
+    y = std::min(std::max(y, 0), h - 1);
+    const float* q = &v->env_host[((size_t)y * w + x) * 4];
+    return f3(q[0], q[1], q[2]);
+  };
+  const float px = u * (float)w - 0.5f, py = vv * (float)h - 0.5f;
+  const int x = (int)std::floor(px), y = (int)std::floor(py);
+  const float wx = px - (float)x, wy = py - (float)y;
+  auto lerp3 = [](F3 a, F3 b, float t) { return a * (1.0f - t) + b * t; };
+  return lerp3(lerp3(at(x, y), at(x + 1, y), wx), lerp3(at(x, y + 1), at(x + 1, y + 1), wx), wy);
+}
+
+// One light per neural pass (core/volume.cu:417-432): with probability
+// rate = 4e / (4e + max(light colour)), e the environment scale, the light
+// comes from the map: direction = the uniform sphere point of the R2
+// sequence (Roberts2, core/vector.cu:174-178) at the pass index, colour =
+// map(direction) * env * 4 / rate; otherwise the directional light with
+// colour / (1 - rate). The coin is Philox (seed; pass, 0, 0, TAG_ENV) where
+// the reference calls rand().
+void select_env_light(const Volume* v, mr_render_params* q) {
+  if (!v->env_dev || v->env_host.empty()) return;
+  const F3 env = to_f3(q->env_color), lc = to_f3(q->light_color);
+  const float e = std::max(env.x, std::max(env.y, env.z));
+  const float m = std::max(lc.x, std::max(lc.y, lc.z));
+  if (!(e > 0.0f)) return;
+  const float rate = e * 4.0f / (e * 4.0f + m);
+  uint32_t o[4];
+  philox4x32_10(q->sample_offset, 0u, 0u, TAG_ENV, q->seed, 0u, o);
+  if (u01(o[0]) < rate) {
+    const float g = 1.32471795724474602596f;
+    const float ax = 1.0f / g, ay = 1.0f / (g * g);
+    const float n = (float)q->sample_offset;
+    float rx = ax * n + 0.5f, ry = ay * n + 0.5f;
+    rx -= std::floor(rx);
+    ry -= std::floor(ry);
+    const F3 d = uniform_sphere(rx, ry);
+    const float u = std::atan2(-d.z, d.x) * (float)(0.5 / 3.1415926) + 0.5f;
+    const float vv = std::acos(std::max(std::min(d.y, 1.0f), -1.0f)) * (float)(1.0 / 3.1415926);
+    const F3 c = env_sample_host(v, u, vv);
+    const float k = 4.0f / rate;
+    q->light_dir = mr_float3{d.x, d.y, d.z};
+    q->light_color = mr_float3{c.x * env.x * k, c.y * env.y * k, c.z * env.z * k};
+  } else {
+    const float k = 1.0f / (1.0f - rate);
+    q->light_color = mr_float3{lc.x * k, lc.y * k, lc.z * k};
+  }
 }
 
 int check_params(const mr_render_params* p) {
@@ -149,6 +213,7 @@ int launch_delta_track(Volume* v, const mr_render_params* p, float* sum32, doubl
     if (rc) return rc;
   }
   a.sc = make_path_scene(p);
+  attach_env(a.sc, v);
   a.cam = make_camera(p);
   a.seed = p->seed;
   a.sample_offset = p->sample_offset;

@@ -97,10 +97,38 @@ struct PathScene {
   F3 L;            // normalized light direction
   F3 light_color;
   F3 scatter;      // albedo per channel
-  F3 env;          // radiance of escaped rays
+  F3 env;          // radiance of escaped rays, or the scale of the environment map
   float alpha, g;
   int max_bounces;
+  const float4* env_map;  // SetHDRI image (w x h, row 0 = straight up), or null
+  int env_w, env_h;
 };
+
+// Environment radiance seen along dir: SkyBox (core/render.cuh:57-61), the
+// environment map at u = atan2(-d.z, d.x) / 2 pi + 1/2, v = acos(d.y) / pi,
+// bilinear with wrap addressing as the reference's texture filter reads it
+// (here in fp32), times the env scale (SetEnvExp); without a map, the
+// constant env colour.
+__device__ __forceinline__ F3 env_lookup(const float4* __restrict__ map, int w, int h, F3 scale, F3 d) {
+  const float u = atan2f(-d.z, d.x) * (float)(0.5 / 3.1415926) + 0.5f;
+  const float v = acosf(fmaxf(fminf(d.y, 1.0f), -1.0f)) * (float)(1.0 / 3.1415926);
+  const float x = u * (float)w - 0.5f, y = v * (float)h - 0.5f;
+  const float x0 = floorf(x), y0 = floorf(y);
+  const float fx = x - x0, fy = y - y0;
+  int i0 = (int)x0 % w, j0 = (int)y0 % h;
+  if (i0 < 0) i0 += w;
+  if (j0 < 0) j0 += h;
+  const int i1 = i0 + 1 == w ? 0 : i0 + 1, j1 = j0 + 1 == h ? 0 : j0 + 1;
+  const float4 a = __ldg(map + (size_t)j0 * w + i0), b = __ldg(map + (size_t)j0 * w + i1);
+  const float4 c = __ldg(map + (size_t)j1 * w + i0), e = __ldg(map + (size_t)j1 * w + i1);
+  const float r = lerpf(lerpf(a.x, b.x, fx), lerpf(c.x, e.x, fx), fy);
+  const float g = lerpf(lerpf(a.y, b.y, fx), lerpf(c.y, e.y, fx), fy);
+  const float bl = lerpf(lerpf(a.z, b.z, fx), lerpf(c.z, e.z, fx), fy);
+  return f3(r * scale.x, g * scale.y, bl * scale.z);
+}
+__device__ __forceinline__ F3 sky(const PathScene& sc, F3 d) {
+  return sc.env_map ? env_lookup(sc.env_map, sc.env_w, sc.env_h, sc.env, d) : sc.env;
+}
 
 // CalculateRadiance (core/render.cuh:200-258), one sample.
 __device__ __forceinline__ F3 path_radiance(const Medium& m, const PathScene& sc, Rng& rng, F3 ori, F3 dir,
@@ -108,7 +136,7 @@ __device__ __forceinline__ F3 path_radiance(const Medium& m, const PathScene& sc
   dir = normalize(dir);
   float t = -1;
   float dis = ray_box_offset(ori, dir);
-  if (dis < 0) { *first_t = t; return sc.env; }
+  if (dis < 0) { *first_t = t; return sky(sc, dir); }
   F3 res = f3(0, 0, 0);
   F3 pos = ori + dir * dis;
   F3 rd = dir;
@@ -117,7 +145,7 @@ __device__ __forceinline__ F3 path_radiance(const Medium& m, const PathScene& sc
     F3 np, nd;
     float maxd = ray_box_distance(pos, rd);
     bool hit = next_vertex(m, rng, sc.alpha, sc.g, pos, rd, maxd, np, nd, st);
-    if (!hit) { res = res + sc.env * rate; break; }
+    if (!hit) { res = res + sky(sc, rd) * rate; break; }
     if (s == 0) t = length(ori - np);
     pos = np;
     rate = rate * sc.scatter;

@@ -4,8 +4,9 @@
 //
 //  * k_train_points: MeanFreePathSample + GetDesiredCountSample
 //    (dataGen.cu:148-216) on the GPU: rays from a sphere of radius 0.5 towards
-//    the volume, up to four Woodcock vertices each, with the reference's
-//    jitter / view-direction rules; compacted with a global counter.
+//    the volume, up to four Woodcock vertices each over the 256^3 mip level 0
+//    (the density dataGen's host code samples), with the reference's jitter /
+//    view-direction rules; compacted with a global counter.
 //  * k_train_labels: GetSample / GetSamples (core/render.cuh:276-315,
 //    core/volume.cu:550-626): multiple-scattering radiance at a point along
 //    its view direction, FP64 accumulation over the samples of a label.
@@ -29,8 +30,36 @@ namespace mr {
 
 // ---- training points --------------------------------------------------------------
 
-// Six draws per vertex (keep, jitter, 3 x offset, view), always taken so that a
-// ray's stream does not depend on which branches ran.
+// dataGen's host DeterminateNextVertex (dataGen.cu:148-172): Woodcock free
+// flight in which one draw rk per tentative collision sets both the step
+// (t -= log(1 - rk) / S_max) and the acceptance test (S / S_max > rk), unlike
+// the renderer's DeterminateNextVertex (core/render.cuh:138-172), which draws
+// a second number for the test; the correlation shapes where the training
+// points fall, so it is kept.
+__device__ __forceinline__ bool next_vertex_datagen(const Medium& m, Rng& rng, float alpha, float g, F3 pos, F3 dir,
+                                                    float dis, F3& npos, F3& ndir, TrackStats& st) {
+  const float smax = m.max_density * alpha;
+  float t = 0;
+  int loop = 0;
+  bool capped = true;
+  while (loop++ < 10000) {
+    const float rk = rng.next();
+    t -= logf(1 - rk) / smax;
+    if (t > dis) { npos = f3(0, 0, 0); ndir = f3(0, 0, 0); return false; }
+    const float d = fetch_density(m, pos + (dir * t), st);
+    if (d * alpha / smax > rk) { capped = false; break; }
+    if (d < 0) t -= d;
+  }
+  if (capped) ++st.caps;
+  const float e0 = rng.next(), e1 = rng.next();
+  ndir = hg_sample_dir(e0, e1, dir, g);
+  npos = (dir * t) + pos;
+  return true;
+}
+
+// Six draws per vertex (keep, jitter, 3 x jitter point, view), always taken so
+// that a ray's stream does not depend on which branches ran. The jitter is a
+// uniform point of the ball of radius 1/128 (hash3box, dataGen.cu:115-118).
 __global__ void k_train_points(Medium m, float alpha, float g, uint32_t seed, int n_rays, int cap, float* pos,
                                float* dir, unsigned* count, unsigned* caps) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -47,13 +76,13 @@ __global__ void k_train_points(Medium m, float alpha, float g, uint32_t seed, in
     for (int i = 0; i < 4; ++i) {
       const float dd = ray_box_distance(sp, rd);
       F3 np, nd;
-      if (!next_vertex(m, rng, alpha, g, sp, rd, dd, np, nd, st)) break;
-      const float uk = rng.next(), uj = rng.next(), jx = rng.next(), jy = rng.next(), jz = rng.next(),
+      if (!next_vertex_datagen(m, rng, alpha, g, sp, rd, dd, np, nd, st)) break;
+      const float uk = rng.next(), uj = rng.next(), j0 = rng.next(), j1 = rng.next(), j2 = rng.next(),
                   uv = rng.next();
       const F3 dv = sp - np;
       if (i == 0 || dot(dv, dv) > 1.0f / 64.0f || uk > 0.9f) {
         F3 p = np;
-        if (uj > 0.5f) p = p + f3(jx * 2.0f - 1.0f, jy * 2.0f - 1.0f, jz * 2.0f - 1.0f) * (1.0f / 128.0f);
+        if (uj > 0.5f) p = p + uniform_sphere(j0, j1) * (cbrtf(j2) * (1.0f / 128.0f));
         const F3 v = uv > 0.25f ? d : rd;
         const unsigned k = atomicAdd(count, 1u);
         if (k < (unsigned)cap) {
@@ -81,6 +110,7 @@ struct LabelArgs {
   double* sum;
   unsigned long long* queue;  // work counter
   unsigned* caps;
+  PathScene env;  // only the environment fields: map, size and scale (black without a map)
 };
 
 // Work item = (label k, chunk of `chunk` samples), claimed from a global queue
@@ -109,7 +139,11 @@ __global__ void __launch_bounds__(128) k_train_labels(LabelArgs a) {
       for (int b = 0; b < a.max_bounces; ++b) {
         F3 np, nd;
         float dis = ray_box_distance(sp, rd);
-        if (!next_vertex(a.m, rng, a.alpha, a.g, sp, rd, dis, np, nd, st)) break;
+        if (!next_vertex(a.m, rng, a.alpha, a.g, sp, rd, dis, np, nd, st)) {
+          // escaped: SkyBox(dir) * rate (core/render.cuh:294-296), channel 0
+          if (a.env.env_map) res = res + rate * sky(a.env, rd).x;
+          break;
+        }
         sp = np;
         rate = rate * 1.001f * a.albedo;
         dis = ray_box_distance(sp, a.L);
@@ -504,8 +538,11 @@ extern "C" int mr_train_points(mr_volume* h, float alpha, float g, uint32_t seed
   MR_CUDA(cudaMemsetAsync(v->d_counters, 0, kCounters * sizeof(unsigned long long), s));
   unsigned* cnt = reinterpret_cast<unsigned*>(v->d_counters + 4);
   unsigned* caps = reinterpret_cast<unsigned*>(v->d_counters + 5);
+  // dataGen's Woodcock steps read VolumeRender::DensityAtPosition(0, p): the
+  // 256^3 level 0 of the mip pyramid, trilinear with a zero border
+  // (core/volume.cu:1495-1497, 675-703), under the density grid's majorant.
   if (n_rays > 0)
-    k_train_points<<<(n_rays + 127) / 128, 128, 0, s>>>(Medium{v->density, v->res, v->max_density, 1.0f}, alpha, g,
+    k_train_points<<<(n_rays + 127) / 128, 128, 0, s>>>(Medium{v->mips, 256, v->max_density, 1.0f, 0}, alpha, g,
                                                         seed, n_rays, cap, dev_pos, dev_dir, cnt, caps);
   MR_CUDA(cudaGetLastError());
   unsigned c = 0;
@@ -544,6 +581,9 @@ extern "C" int mr_train_labels(mr_volume* h, const float* dev_pos, const float* 
   a.sum = dev_sum;
   a.queue = v->d_counters + 4;
   a.caps = reinterpret_cast<unsigned*>(v->d_counters + 2);
+  a.env = PathScene{};
+  a.env.env = f3(1.0f, 1.0f, 1.0f);  // the map at unit scale; black without one
+  attach_env(a.env, v);
   k_train_labels<<<sm_count() * 16, 128, 0, s>>>(a);
   MR_CUDA(cudaGetLastError());
   return MR_OK;

@@ -3,6 +3,8 @@
 // cone-averaged Henyey-Greenstein table. Replaces VolumeRender::Update /
 // Update_TR / UpdateHGLut (core/volume.cu:1161-1424) and the host OpenMP loops
 // they ran; all tables live as raw fp32 arrays in HBM (index (x*r+y)*r+z).
+#include <cmath>
+
 #include "mr_internal.h"
 
 namespace mr {
@@ -456,6 +458,7 @@ int mr_volume_destroy(mr_volume* h) {
   if (v->scratch) cudaFree(v->scratch);
   if (v->inter) cudaFree(v->inter);
   if (v->mom) cudaFree(v->mom);
+  if (v->env_dev) cudaFree(v->env_dev);
   if (v->copy_stream) {
     cudaStreamSynchronize(v->copy_stream);  // host copies still reading the frames
     for (int i = 0; i < 2; ++i) {
@@ -552,6 +555,50 @@ int mr_volume_update_hglut(mr_volume* h, float g, uint32_t seed, void* stream) {
   Volume* v = &h->v;
   if (v->lut_valid && v->lut_g == g && v->lut_seed == seed) return MR_OK;
   return launch_update_lut(v, g, seed, (cudaStream_t)stream);
+}
+
+// SetHDRI (core/volume.cu:1426-1458) from pixels: w x h RGBA fp32, row 0 =
+// straight up (v = acos(d.y) / pi), column u = atan2(-d.z, d.x) / 2 pi + 1/2.
+int mr_volume_set_hdri(mr_volume* h, const float* host_rgba, int32_t w, int32_t hh) {
+  clear_error();
+  if (!h || !host_rgba) return set_error(MR_ERR_ARG, "mr_volume_set_hdri: NULL argument");
+  if (w <= 0 || hh <= 0 || (long long)w * hh > (1ll << 26)) return set_error(MR_ERR_ARG, "bad HDRI size %d x %d", w, hh);
+  Volume* v = &h->v;
+  const size_t n = (size_t)w * hh * 4;
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(host_rgba[i])) return set_error(MR_ERR_ARG, "HDRI value %zu is not finite", i);
+  float4* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, n * sizeof(float));
+  if (e != cudaSuccess) return set_error(MR_ERR_NOMEM, "HDRI: %s", cudaGetErrorString(e));
+  e = cudaMemcpy(d, host_rgba, n * sizeof(float), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(d);
+    return cuda_error(e, "cudaMemcpy(HDRI)");
+  }
+  // renders still queued may read the old map: wait for the device first
+  if (v->env_dev) {
+    cudaDeviceSynchronize();
+    cudaFree(v->env_dev);
+  }
+  v->env_dev = d;
+  v->env_host.assign(host_rgba, host_rgba + n);
+  v->env_w = w;
+  v->env_h = hh;
+  return MR_OK;
+}
+
+int mr_volume_clear_hdri(mr_volume* h) {
+  clear_error();
+  if (!h) return set_error(MR_ERR_ARG, "mr_volume_clear_hdri: NULL argument");
+  Volume* v = &h->v;
+  if (v->env_dev) {
+    cudaDeviceSynchronize();
+    cudaFree(v->env_dev);
+  }
+  v->env_dev = nullptr;
+  v->env_host.clear();
+  v->env_w = v->env_h = 0;
+  return MR_OK;
 }
 
 int mr_volume_max_density(const mr_volume* h, float* out) {

@@ -28,6 +28,17 @@ def read_volume_file(path):
     return out.reshape((r.value,) * 3)
 
 
+def read_hdr(path):
+    """load_hdr_float4 (core/hdr_loader.h:249): (h, w, 4) float32, alpha 0."""
+    L = _lib.load()
+    w, h = C.c_int32(), C.c_int32()
+    p = os.fsencode(path)
+    check(L.mr_hdr_read(p, None, 0, C.byref(w), C.byref(h)))
+    out = np.zeros(w.value * h.value * 4, np.float32)
+    check(L.mr_hdr_read(p, out.ctypes.data, out.size, C.byref(w), C.byref(h)))
+    return out.reshape(h.value, w.value, 4)
+
+
 def builtin_stencil():
     """The default stencil: the reference's 160 directions (core/vector.cu:77-172)."""
     out = np.zeros(480, np.float32)
@@ -167,6 +178,27 @@ class VolumeRender:
 
     def SetEnvColor(self, color):
         self.env_color = tuple(float(c) for c in color)
+
+    def SetHDRI(self, path_or_rgba):
+        """SetHDRI (core/volume.cu:1426-1458): a Radiance .hdr path or an
+        (h, w, 3|4) float array, row 0 straight up. The environment scale
+        (SetEnvExp) becomes 1 unless one was set."""
+        L = _lib.load()
+        if isinstance(path_or_rgba, (str, bytes, os.PathLike)):
+            check(L.mr_volume_load_hdri(self.handle, os.fsencode(path_or_rgba)))
+        else:
+            a = np.asarray(path_or_rgba, np.float32)
+            if a.ndim != 3 or a.shape[2] not in (3, 4):
+                raise ValueError("HDRI must be (h, w, 3) or (h, w, 4)")
+            rgba = np.zeros(a.shape[:2] + (4,), np.float32)
+            rgba[..., :a.shape[2]] = a
+            check(L.mr_volume_set_hdri(self.handle, rgba.ctypes.data, rgba.shape[1], rgba.shape[0]))
+        if not any(self.env_color):
+            self.env_color = (1.0, 1.0, 1.0)
+
+    def SetEnvExp(self, exp):
+        """SetEnvExp: the scale of the environment map."""
+        self.env_color = (float(exp),) * 3
 
     def SetWeights(self, weights, stencil=None):
         if self.network is not None:

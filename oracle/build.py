@@ -2,7 +2,8 @@
 
 `build_oracle()` compiles the C++ restatement into oracle/liborc.so.
 `build_reference()` compiles the reference's own device sources, in place,
-into oracle/_ref/ (see oracle/ref/README). Both run with g++/nvcc only.
+into oracle/_ref/ with the shim and harnesses of oracle/ref/. Both run with
+g++/nvcc only.
 """
 import os
 import subprocess
@@ -94,10 +95,11 @@ def build_reference_volume(force=False):
     ref_dir = os.path.join(HERE, "ref")
     shim = os.path.join(ref_dir, "cuda12_texref_shim.cuh")
     harness = os.path.join(ref_dir, "ref_volume.cu")
+    datagen = os.path.join(ref_dir, "ref_datagen.cu")
     net_tu = os.path.join(ref_dir, "ref_net_tu.cu")
     srcs = [os.path.join(core, f) for f in ("vector.cu", "renderResources.cu", "volume.cu", "camera.cu")]
-    deps = [shim, harness, net_tu] + srcs + [os.path.join(core, f) for f in
-                                             ("omp.cpp", "render.cuh", "volume.hpp", "camera.hpp", "NNWeight.cuh")]
+    deps = [shim, harness, datagen, net_tu, os.path.join(REF_SRC, "dataGen.cu")] + srcs + [
+        os.path.join(core, f) for f in ("omp.cpp", "render.cuh", "volume.hpp", "camera.hpp", "NNWeight.cuh")]
     if not force and _newer(out, deps):
         return out
     flags = ["-std=c++17", "-rdc=true", "-gencode", "arch=compute_100a,code=sm_100a",
@@ -108,8 +110,15 @@ def build_reference_volume(force=False):
         o = os.path.join(REF_DIR, "vol_" + os.path.basename(src).replace(".cu", ".o"))
         subprocess.check_call(["nvcc"] + flags + ["-c", src, "-o", o])
         objs.append(o)
+    # dataGen.cu (its sampling functions): the GUI header it includes is
+    # replaced by a stub, its main renamed inside ref_datagen.cu
+    o = os.path.join(REF_DIR, "vol_ref_datagen.o")
+    subprocess.check_call(["nvcc"] + flags[:-2] + ["-I", os.path.join(ref_dir, "stub"), "-I", core, "-I", REF_SRC,
+                                                   "-c", datagen, "-o", o])
+    objs.append(o)
     o = os.path.join(REF_DIR, "vol_omp.o")
-    subprocess.check_call(["nvcc", "-std=c++17", "-w", "-Xcompiler", "-fPIC", "-I", core, "-x", "cu", "-c",
+    subprocess.check_call(["nvcc", "-std=c++17", "-w", "-Xcompiler", "-fPIC", "-gencode",
+                           "arch=compute_100a,code=sm_100a", "-I", core, "-x", "cu", "-c",
                            os.path.join(core, "omp.cpp"), "-o", o])
     objs.append(o)
     subprocess.check_call(["nvcc", "-shared", "-gencode", "arch=compute_100a,code=sm_100a",

@@ -88,6 +88,32 @@ struct Scene {
   int max_bounces;
 };
 
+// Environment map set by orc_set_env (w x h RGBA, row 0 straight up); empty
+// = the constant env colour.
+static std::vector<float> g_env;
+static int g_env_w = 0, g_env_h = 0;
+
+// SkyBox (core/render.cuh:57-61): the map at u = atan2(-d.z, d.x) / 2pi + 1/2,
+// v = acos(d.y) / pi, bilinear with wrap, times the env scale.
+static V3 sky(const Scene& sc, V3 d) {
+  if (g_env.empty()) return sc.env;
+  const int w = g_env_w, h = g_env_h;
+  const float u = std::atan2(-d.z, d.x) * (float)(0.5 / 3.1415926) + 0.5f;
+  const float v = std::acos(std::max(std::min(d.y, 1.0f), -1.0f)) * (float)(1.0 / 3.1415926);
+  const float x = u * (float)w - 0.5f, y = v * (float)h - 0.5f;
+  const float x0 = std::floor(x), y0 = std::floor(y);
+  const float fx = x - x0, fy = y - y0;
+  int i0 = (int)x0 % w, j0 = (int)y0 % h;
+  if (i0 < 0) i0 += w;
+  if (j0 < 0) j0 += h;
+  const int i1 = i0 + 1 == w ? 0 : i0 + 1, j1 = j0 + 1 == h ? 0 : j0 + 1;
+  auto px = [&](int i, int j, int c) { return g_env[((size_t)j * w + i) * 4 + c]; };
+  auto lf = [](float a, float b, float t) { return a * (1.0f - t) + b * t; };
+  float r[3];
+  for (int c = 0; c < 3; ++c) r[c] = lf(lf(px(i0, j0, c), px(i1, j0, c), fx), lf(px(i0, j1, c), px(i1, j1, c), fx), fy);
+  return v3(r[0] * sc.env.x, r[1] * sc.env.y, r[2] * sc.env.z);
+}
+
 inline V3 f3(const mr_float3& a) { return v3(a.x, a.y, a.z); }
 
 // ---- delta tracking ---------------------------------------------------------
@@ -156,7 +182,7 @@ struct Tracker {
     V3 L = normalize(sc.light_dir);
     float t = -1;
     float dis = ray_box_offset(ori, dir);
-    if (dis < 0) { *first_t = t; return sc.env; }
+    if (dis < 0) { *first_t = t; return sky(sc, dir); }
     V3 res = v3(0, 0, 0);
     V3 pos = ori + dir * dis;
     V3 rd = dir;
@@ -165,7 +191,7 @@ struct Tracker {
       V3 np, nd;
       float maxd = ray_box_distance(pos, rd);
       bool hit = next_vertex(rng, sc.alpha, sc.g, pos, rd, maxd, np, nd);
-      if (!hit) { res = res + sc.env * rate; break; }
+      if (!hit) { res = res + sky(sc, rd) * rate; break; }
       if (s == 0) t = length(ori - np);
       pos = np;
       rate = rate * sc.scatter;
@@ -483,7 +509,7 @@ V3 neural_pixel(Tracker& tk, const Net& net, const float* stencil, Rng& rng, V3 
   V3 ly, lz;
   frame_from(rng, dir, f.X, f.Y, f.Z);
   frame_from(rng, L, f.LX, ly, lz);
-  if (!active) { *hit_t = -1; return sc.env; }
+  if (!active) { *hit_t = -1; return sky(sc, dir); }
   NetState s;
   gather(s, tk.vol, stencil, pos, L, f, sc.alpha, sc.g);
   V3 scatterrate = sc.scatter / 1.001f;
@@ -508,6 +534,70 @@ inline float u01_tag(uint32_t seed, uint32_t a, uint32_t b, uint32_t tag) {
 // C ABI (ctypes)
 // =============================================================================
 extern "C" {
+
+// Environment map for the trackers (n = 0 clears it).
+void orc_set_env(const float* rgba, int w, int h) {
+  if (!rgba || w <= 0 || h <= 0) {
+    g_env.clear();
+    g_env_w = g_env_h = 0;
+    return;
+  }
+  g_env.assign(rgba, rgba + (size_t)w * h * 4);
+  g_env_w = w;
+  g_env_h = h;
+}
+
+// The light of neural pass p->sample_offset with the environment map set
+// (core/volume.cu:417-432): rate = 4e / (4e + max(light colour)), e =
+// max(env colour); with probability rate (Philox(seed; pass, 0, 0, TAG_ENV)
+// word 0) the direction is the R2 point (core/vector.cu:174-178) of the pass
+// on the uniform sphere and the colour the map there (Image_host::Sample:
+// bilinear, clamped, core/volume.hpp:22-42) * env * 4 / rate; otherwise the
+// colour / (1 - rate). Writes light_dir[3], light_color[3].
+void orc_select_env_light(const mr_render_params* p, float* light_dir, float* light_color) {
+  V3 env = f3(p->env_color), lc = f3(p->light_color), L = f3(p->light_dir);
+  V3 outL = L, outC = lc;
+  const float e = std::max(env.x, std::max(env.y, env.z));
+  const float m = std::max(lc.x, std::max(lc.y, lc.z));
+  if (!g_env.empty() && e > 0.0f) {
+    const float rate = e * 4.0f / (e * 4.0f + m);
+    uint32_t ctr[4] = {p->sample_offset, 0u, 0u, (uint32_t)TAG_ENV}, o[4];
+    philox4x32_10(ctr, p->seed, 0u, o);
+    if (u01(o[0]) < rate) {
+      const float g = 1.32471795724474602596f;
+      const float ax = 1.0f / g, ay = 1.0f / (g * g);
+      const float n = (float)p->sample_offset;
+      float rx = ax * n + 0.5f, ry = ay * n + 0.5f;
+      rx -= std::floor(rx);
+      ry -= std::floor(ry);
+      V3 d = uniform_sphere(rx, ry);
+      const float u = std::atan2(-d.z, d.x) * (float)(0.5 / 3.1415926) + 0.5f;
+      const float vv = std::acos(std::max(std::min(d.y, 1.0f), -1.0f)) * (float)(1.0 / 3.1415926);
+      const int w = g_env_w, h = g_env_h;
+      auto at = [&](int x, int y, int c) {
+        x = std::min(std::max(x, 0), w - 1);
+        y = std::min(std::max(y, 0), h - 1);
+        return g_env[((size_t)y * w + x) * 4 + c];
+      };
+      const float pxf = u * (float)w - 0.5f, pyf = vv * (float)h - 0.5f;
+      const int x = (int)std::floor(pxf), y = (int)std::floor(pyf);
+      const float wx = pxf - (float)x, wy = pyf - (float)y;
+      float c3[3];
+      for (int c = 0; c < 3; ++c) {
+        const float a0 = at(x, y, c) * (1.0f - wx) + at(x + 1, y, c) * wx;
+        const float a1 = at(x, y + 1, c) * (1.0f - wx) + at(x + 1, y + 1, c) * wx;
+        c3[c] = a0 * (1.0f - wy) + a1 * wy;
+      }
+      const float k = 4.0f / rate;
+      outL = d;
+      outC = v3(c3[0] * env.x * k, c3[1] * env.y * k, c3[2] * env.z * k);
+    } else {
+      outC = lc * (1.0f / (1.0f - rate));
+    }
+  }
+  light_dir[0] = outL.x; light_dir[1] = outL.y; light_dir[2] = outL.z;
+  light_color[0] = outC.x; light_color[1] = outC.y; light_color[2] = outC.z;
+}
 
 void orc_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
   philox4x32_10(ctr, key[0], key[1], out);
@@ -901,7 +991,7 @@ void orc_get_samples(const float* density, int res, float max_density, const flo
     sc.alpha = alpha[k]; sc.g = g[k]; sc.tr_scale = 1.0f;
     sc.scatter = v3(scatter[k], scatter[k], scatter[k]);
     sc.light_dir = v3(light[3 * k], light[3 * k + 1], light[3 * k + 2]);
-    sc.light_color = v3(1, 1, 1); sc.env = v3(0, 0, 0); sc.max_bounces = max_bounces;
+    sc.light_color = v3(1, 1, 1); sc.env = g_env.empty() ? v3(0, 0, 0) : v3(1, 1, 1); sc.max_bounces = max_bounces;
     Tracker tk{vol, sc};
     V3 L = normalize(sc.light_dir);
     V3 d0 = v3(dir[3 * k], dir[3 * k + 1], dir[3 * k + 2]);
@@ -916,7 +1006,10 @@ void orc_get_samples(const float* density, int res, float max_density, const flo
       for (int b = 0; b < max_bounces; ++b) {
         V3 np, nd;
         float dis = ray_box_distance(sp, rd);
-        if (!tk.next_vertex(rng, sc.alpha, sc.g, sp, rd, dis, np, nd)) break;
+        if (!tk.next_vertex(rng, sc.alpha, sc.g, sp, rd, dis, np, nd)) {
+          res_acc = res_acc + rate * sky(sc, rd).x;  // SkyBox on escape (black without a map)
+          break;
+        }
         sp = np;
         rate = rate * 1.001f * scatter[k];
         dis = ray_box_distance(sp, L);
@@ -936,6 +1029,9 @@ void orc_get_samples(const float* density, int res, float max_density, const flo
 // TAG_GEN), four draws for origin and direction, then per Woodcock vertex the
 // free-flight draws and six more (keep, jitter, 3 offsets, view). Returns the
 // number of points (<= cap written).
+// `density` is the grid the Woodcock steps read: dataGen's host code samples
+// VolumeRender::DensityAtPosition(0, p), the 256^3 mip level 0
+// (core/volume.cu:1495-1497), with the density grid's max_density as majorant.
 int orc_train_points(const float* density, int res, float max_density, float alpha, float g, uint32_t seed,
                      int n_rays, int cap, float* pos, float* dir) {
   Vol vol{density, res, max_density, nullptr, nullptr, nullptr};
@@ -954,12 +1050,35 @@ int orc_train_points(const float* density, int res, float max_density, float alp
     for (int i = 0; i < 4; ++i) {
       float dd = ray_box_distance(sp, rd);
       V3 np, nd;
-      if (!tk.next_vertex(rng, alpha, g, sp, rd, dd, np, nd)) break;
-      float uk = rng.next(), uj = rng.next(), jx = rng.next(), jy = rng.next(), jz = rng.next(), uv = rng.next();
+      // dataGen.cu:148-172: one draw per tentative collision for both the
+      // step and the acceptance test
+      bool hit = false;
+      {
+        const float smax = max_density * alpha;
+        float t = 0;
+        int loop = 0;
+        while (loop++ < 10000) {
+          const float rk = rng.next();
+          t -= std::log(1 - rk) / smax;
+          if (t > dd) break;
+          const float dv = tk.density(sp + rd * t);
+          if (dv * alpha / smax > rk) { hit = true; break; }
+          if (dv < 0) t -= dv;
+        }
+        if (!hit && loop > 10000) hit = true;  // the step cap accepts, as the reference's loop exit does
+        if (hit) {
+          const float e0 = rng.next(), e1 = rng.next();
+          nd = hg_sample_dir(e0, e1, rd, g);
+          np = rd * t + sp;
+        }
+      }
+      if (!hit) break;
+      float uk = rng.next(), uj = rng.next(), j0 = rng.next(), j1 = rng.next(), j2 = rng.next(), uv = rng.next();
       V3 dv = sp - np;
       if (i == 0 || dot(dv, dv) > 1.0f / 64.0f || uk > 0.9f) {
         V3 p = np;
-        if (uj > 0.5f) p = p + v3(jx * 2.0f - 1.0f, jy * 2.0f - 1.0f, jz * 2.0f - 1.0f) * (1.0f / 128.0f);
+        // hash3box (dataGen.cu:115-118): uniform in the ball of radius 1/128
+        if (uj > 0.5f) p = p + uniform_sphere(j0, j1) * (std::cbrt(j2) * (1.0f / 128.0f));
         V3 v = uv > 0.25f ? d : rd;
         if (count < cap) {
           pos[3 * count] = p.x; pos[3 * count + 1] = p.y; pos[3 * count + 2] = p.z;

@@ -108,7 +108,7 @@ static inline void philox4x32_10(const uint32_t ctr_in[4], uint32_t k0, uint32_t
 static inline float u01(uint32_t x) { return ((float)(x >> 9) + 0.5f) * 1.1920928955078125e-7f; }
 
 // Stream tags (word 3 of the counter).
-enum { TAG_PT = 1, TAG_NN = 2, TAG_LUT = 3, TAG_GEN = 4, TAG_LABEL = 5, TAG_MISC = 6 };
+enum { TAG_PT = 1, TAG_NN = 2, TAG_LUT = 3, TAG_GEN = 4, TAG_LABEL = 5, TAG_MISC = 6, TAG_ENV = 7 };
 
 // One path's random stream: key (seed, 0), counter (a, b, block, tag);
 // draw k is word k%4 of block k/4.

@@ -38,6 +38,8 @@ def lib():
         L = C.CDLL(path)
         L.orc_philox.argtypes = [u32p, u32p, u32p]
         L.orc_weights_xavier.argtypes = [C.c_uint32, f32p]
+        L.orc_set_env.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        L.orc_select_env_light.argtypes = [C.c_void_p, f32p, f32p]
         L.orc_uniforms.argtypes = [C.c_uint32] * 4 + [C.c_int, f32p]
         L.orc_hg.argtypes = [C.c_float, C.c_float]
         L.orc_hg.restype = C.c_float
@@ -110,6 +112,30 @@ def uniforms(seed, a, b, tag, n):
     out = np.zeros(n, np.float32)
     lib().orc_uniforms(seed, a, b, tag, n, out)
     return out
+
+
+def set_env(rgba=None):
+    """Environment map (h, w, 4) for the trackers; None clears it."""
+    global _env_keep
+    if rgba is None:
+        lib().orc_set_env(None, 0, 0)
+        _env_keep = None
+        return
+    a = np.ascontiguousarray(rgba, np.float32)
+    _env_keep = a
+    lib().orc_set_env(a.ctypes.data, a.shape[1], a.shape[0])
+
+
+_env_keep = None
+
+
+def select_env_light(params):
+    """(light_dir, light_color) of neural pass params.sample_offset with the
+    environment map set."""
+    ld = np.zeros(3, np.float32)
+    lc = np.zeros(3, np.float32)
+    lib().orc_select_env_light(C.addressof(params), ld, lc)
+    return ld, lc
 
 
 def xavier_weights(seed):
@@ -222,11 +248,13 @@ def cloud(res, seed, octaves=6, base_freq=4.0, lacunarity=2.0, gain=0.5, thresho
 
 
 def train_points(density, max_density, alpha, g, seed, n_rays, cap):
-    density = _a(density)
-    res = round(density.size ** (1 / 3))
+    """MeanFreePathSample over the 256^3 mip level 0 of `density` (what
+    DensityAtPosition(0, p) samples), under the density's majorant."""
+    _, mips, _ = build_mips(density)
+    mip0 = np.ascontiguousarray(mips[:256 ** 3])
     pos = np.zeros((cap, 3), np.float32)
     dirs = np.zeros((cap, 3), np.float32)
-    n = lib().orc_train_points(density.ravel(), res, float(max_density), float(alpha), float(g), int(seed),
+    n = lib().orc_train_points(mip0, 256, float(max_density), float(alpha), float(g), int(seed),
                                int(n_rays), int(cap), pos.ravel(), dirs.ravel())
     n = min(n, cap)
     return pos[:n], dirs[:n]

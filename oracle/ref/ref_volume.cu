@@ -13,7 +13,9 @@
 //    core/render.cuh:82-91, in the same thread layout);
 //  - Denoise<bool> (core/volume.cu:210-264) on caller-given buffers;
 //  - VolumeRender::Update, GetSamples and the interactive Render overload;
-//  - SaveBMP (core/camera.cu:10-61).
+//  - SaveBMP (core/camera.cu:10-61);
+//  - load_hdr_float4 (core/hdr_loader.h:249), SetHDRI / SetEnvExp and the
+//    offline Render (core/volume.cu:410-467) with the environment map.
 // This TU includes only the reference's headers; the device globals and
 // kernels of core/volume.cu and core/render.cuh are declared extern here.
 #include <algorithm>
@@ -24,6 +26,7 @@
 #include "volume.hpp"
 #include "camera.hpp"
 #include "renderResources.cuh"
+#include "hdr_loader.h"
 
 extern texture<float, cudaTextureType3D, cudaReadModeElementType> texRef;
 extern surface<void, cudaSurfaceType3D> surfRef;
@@ -262,6 +265,45 @@ int refv_save_bmp(const uint8_t* rgba, int w, int h, const char* path) {
   std::vector<unsigned char> img(m * m * 4, 0);
   std::copy(rgba, rgba + (size_t)w * h * 4, img.begin());
   return SaveBMP(img.data(), w, h, path);
+}
+
+// load_hdr_float4 (core/hdr_loader.h:249): *w, *h and, if out is not null
+// and cap allows, w*h*4 floats.
+int refv_load_hdr(const char* path, float* out, size_t cap, int* w, int* h) {
+  float* px = nullptr;
+  unsigned int rx = 0, ry = 0;
+  if (!load_hdr_float4(&px, &rx, &ry, path)) return 1;
+  *w = (int)rx;
+  *h = (int)ry;
+  if (out && cap >= (size_t)rx * ry * 4) std::copy(px, px + (size_t)rx * ry * 4, out);
+  free(px);
+  return 0;
+}
+
+// VolumeRender::SetHDRI(path) and SetEnvExp(exp).
+int refv_set_hdri(void* h, const char* path, float env_exp) {
+  VolumeRender* v = (VolumeRender*)h;
+  v->SetHDRI(path);
+  v->SetEnvExp(env_exp);
+  CK(cudaDeviceSynchronize());
+  return 0;
+}
+
+// The offline VolumeRender::Render (core/volume.cu:410-467), delta tracking:
+// the mean of spp passes, w x hh x 3 (square frames: its indexing assumes
+// w = hh).
+int refv_render_pt(void* h, int w, int hh, const float* ori, const float* up, const float* right, const float* light,
+                   const float* lc, float alpha, int bounces, float g, int spp, float* out) {
+  VolumeRender* v = (VolumeRender*)h;
+  std::vector<float3> r = v->Render(int2{w, hh}, F3(ori), F3(up), F3(right), F3(light), VolumeRender::RenderType::PT,
+                                    g, alpha, F3(lc), bounces, spp);
+  CK(cudaDeviceSynchronize());
+  for (size_t k = 0; k < r.size(); ++k) {
+    out[3 * k] = r[k].x;
+    out[3 * k + 1] = r[k].y;
+    out[3 * k + 2] = r[k].z;
+  }
+  return 0;
 }
 
 // Camera::ACES and Camera::Gamma (core/camera.cu:66-160), the host tone maps

@@ -147,6 +147,11 @@ class RefVolume:
                                        C.c_float, C.c_int, C.c_int, C.c_int, f32p, f32p, u32p]
         L.refv_save_bmp.argtypes = [u8p, C.c_int, C.c_int, C.c_char_p]
         L.refv_tone_host.argtypes = [C.c_int, f32p, C.c_int, f32p]
+        L.refv_load_hdr.argtypes = [C.c_char_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.refv_set_hdri.argtypes = [C.c_void_p, C.c_char_p, C.c_float]
+        L.refv_render_pt.argtypes = [C.c_void_p, C.c_int, C.c_int, f32p, f32p, f32p, f32p, f32p, C.c_float, C.c_int,
+                                     C.c_float, C.c_int, f32p]
+        L.refv_datagen_samples.argtypes = [C.c_void_p, f32p, C.c_float, C.c_float, C.c_int, f32p, f32p]
         self.L = L
         self.h = None
         self.res = res
@@ -208,3 +213,27 @@ class RefVolume:
         out = np.zeros_like(rgb)
         assert self.L.refv_tone_host(rgb.size // 3, rgb, int(tone), out) == 0
         return out.reshape(-1, 3)
+
+    def datagen_samples(self, mip0, max_density, alpha, n):
+        """dataGen's GetDesiredCountSample(v, S, n, alpha, alpha) over the
+        given 256^3 mip level 0: (pos n x 3, view n x 3)."""
+        pos = np.zeros(3 * n, np.float32)
+        view = np.zeros(3 * n, np.float32)
+        m = self.L.refv_datagen_samples(self.h, _f(mip0), float(max_density), float(alpha), int(n), pos, view)
+        return pos.reshape(n, 3)[:m], view.reshape(n, 3)[:m]
+
+    def load_hdr(self, path):
+        w, h = C.c_int(), C.c_int()
+        assert self.L.refv_load_hdr(path.encode(), None, 0, C.byref(w), C.byref(h)) == 0, "load_hdr_float4 failed"
+        out = np.zeros(w.value * h.value * 4, np.float32)
+        assert self.L.refv_load_hdr(path.encode(), out.ctypes.data, out.size, C.byref(w), C.byref(h)) == 0
+        return out.reshape(h.value, w.value, 4)
+
+    def set_hdri(self, path, env_exp=1.0):
+        assert self.L.refv_set_hdri(self.h, path.encode(), float(env_exp)) == 0
+
+    def render_pt(self, w, h, ori, up, right, light, light_color, alpha, bounces, g, spp):
+        out = np.zeros(w * h * 3, np.float32)
+        assert self.L.refv_render_pt(self.h, w, h, _f(ori), _f(up), _f(right), _f(light), _f(light_color),
+                                     float(alpha), int(bounces), float(g), int(spp), out) == 0
+        return out

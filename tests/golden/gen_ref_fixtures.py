@@ -36,6 +36,15 @@ ref_labels.npz   -- GetSamples (training labels) for 48 points of the sphere
                     and 48 of a 64^3 cloud, 8 replicates of 1024 paths.
 ref_bmp.npz      -- SaveBMP bytes of a 6x6 image and the host tone maps
                     Camera::ACES / Camera::Gamma of 256 colours.
+ref_datagen.npz  -- dataGen's GetDesiredCountSample (MeanFreePathSample over
+                    the 256^3 mip level 0, host code, mt19937 draws) on the
+                    64^3 sphere (alpha 16) and the 64^3 cloud (alpha 24):
+                    20000 training points each (position, view direction;
+                    float16). Runs without a GPU.
+ref_hdri.npz     -- the offline VolumeRender::Render (delta tracking) of the
+                    sphere scene (alpha 16) under an environment map loaded
+                    with SetHDRI from a generated .hdr file (its RGBE pixels
+                    are stored), SetEnvExp 1.5, 32x32, 1024 spp: mean image.
 """
 import os
 import sys
@@ -49,7 +58,7 @@ sys.path.insert(0, ROOT)
 from internship_b200 import scenes  # noqa: E402
 from oracle import cloud_np, orc, ref_py  # noqa: E402
 
-SECTIONS = ("network", "pt", "gather", "nn", "tables", "denoise", "labels", "bmp")
+SECTIONS = ("network", "pt", "gather", "nn", "tables", "denoise", "labels", "bmp", "hdri", "datagen")
 
 
 def rand_frames(rng, n, light):
@@ -266,6 +275,44 @@ def gen_bmp(out, rng):
     rgb = np.concatenate([rng.uniform(0, 1, (128, 3)), rng.uniform(0, 20, (128, 3))]).astype(np.float32)
     np.savez_compressed(os.path.join(out, "ref_bmp.npz"), image=img, bmp=data, rgb=rgb, aces=rv.tone_host(rgb, 2),
                         gamma=rv.tone_host(rgb, 1))
+
+
+def gen_datagen(out, rng):
+    res = {}
+    for name, dens, alpha in (("sphere", scenes.sphere_density(64), 16.0),
+                              ("cloud", cloud_np.cloud(CLOUD_RES, CLOUD_SEED), 24.0)):
+        md, mips, _ = orc.build_mips(dens)
+        rv = ref_py.RefVolume(round(dens.size ** (1 / 3)))
+        pos, view = rv.datagen_samples(mips[:256 ** 3], md, alpha, 20000)
+        rv.close()
+        res.update({name + "_pos": pos.astype(np.float16), name + "_view": view.astype(np.float16),
+                    name + "_alpha": np.float32(alpha)})
+    np.savez_compressed(os.path.join(out, "ref_datagen.npz"), **res)
+
+
+def gen_hdri(out, rng):
+    from oracle import hdr_np
+    W = H = 32
+    spp, alpha, env_exp = 1024, 16.0, 1.5
+    v_ = (np.arange(24) + 0.5) / 24
+    u_ = (np.arange(48) + 0.5) / 48
+    U, Vv = np.meshgrid(u_, v_)
+    img = np.stack([0.3 + 0.5 * (1 - Vv), 0.4 + 0.4 * (1 - Vv), 0.8 + 0.2 * np.cos(2 * np.pi * U)], -1)
+    img = img + (40.0 * np.exp(-(((U - 0.3) / 0.05) ** 2 + ((Vv - 0.3) / 0.08) ** 2)))[..., None] * [1.0, 0.9, 0.7]
+    p = scenes.make_params(W, H, 1, alpha=alpha)
+    L = np.array([p.light_dir.x, p.light_dir.y, p.light_dir.z], np.float32)
+    ori, up, right = camera(p)
+    rv = ref_py.RefVolume(128)
+    rv.set_density(scenes.sphere_density(128))
+    rv.set_scalars(1.0, (0.99, 0.99, 0.99), 1.0, (0, 0, 0))
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "sky.hdr")
+        rgbe = hdr_np.write(path, img.astype(np.float32))
+        rv.set_hdri(path, env_exp)
+        image = rv.render_pt(W, H, ori, up, right, L, (1, 1, 1), alpha, 512, p.g, spp)
+    rv.close()
+    np.savez_compressed(os.path.join(out, "ref_hdri.npz"), rgbe=rgbe, image=image, width=W, height=H, spp=spp,
+                        alpha=np.float32(alpha), env_exp=np.float32(env_exp))
 
 
 def main(out, sections):

@@ -32,6 +32,28 @@ def test_tile_product_matches_matmul(n, k):
     np.testing.assert_allclose(d, ref, rtol=1e-5, atol=1e-5 * k)
 
 
+def test_bounded_wait_times_out_and_frees_tensor_memory():
+    """The failure path of the kernels' bounded mbarrier waits: a wait on an
+    mbarrier that nothing arrives on gives up after its limit (5 ms here),
+    the call reports MR_ERR_TIMEOUT, and the tensor memory it held is free
+    again: a tile product right after it allocates and computes normally."""
+    from internship_b200 import _lib
+    L = _lib.load()
+    waited = C.c_int64()
+    rc = L.mr_tc_wait_selftest(5000, C.byref(waited))
+    assert rc == _lib.MR_ERR_TIMEOUT, rc
+    assert b"gave up" in L.mr_last_error()
+    assert 5_000_000 <= waited.value < 500_000_000, waited.value
+    for _ in range(2):
+        rng = np.random.default_rng(7)
+        a = _bf16_bits(rng.uniform(-1, 1, (128, 16)))
+        b = _bf16_bits(rng.uniform(-1, 1, (16, 16)))
+        d = np.zeros((128, 16), np.float32)
+        _lib.check(L.mr_tc_selftest(16, 16, a.ctypes.data, b.ctypes.data, d.ctypes.data))
+        ref = _bf16_value(a).astype(np.float64) @ _bf16_value(b).astype(np.float64).T
+        np.testing.assert_allclose(d, ref, rtol=1e-5, atol=1e-4)
+
+
 def _predict(mr, w, desc, aux, precision):
     import torch
     from internship_b200 import _lib

@@ -181,3 +181,37 @@ def test_oracle_xavier_and_stencil_match_the_library():
     import internship_b200 as mr
     assert np.array_equal(orc.xavier_weights(1), mr.xavier_weights(1))
     assert np.array_equal(orc.reference_stencil(), mr.builtin_stencil())
+
+
+def _two_sample_chi2(a, b, bins):
+    """Two-sample chi-square statistic of histograms a, b (same bins) and its
+    degrees of freedom."""
+    ha, _ = np.histogram(a, bins)
+    hb, _ = np.histogram(b, bins)
+    na, nb = ha.sum(), hb.sum()
+    k1, k2 = np.sqrt(nb / na), np.sqrt(na / nb)
+    m = (ha + hb) > 0
+    stat = float((((k1 * ha - k2 * hb) ** 2)[m] / (ha + hb)[m]).sum())
+    return stat, int(m.sum()) - 1
+
+
+@pytest.mark.parametrize("name", ["sphere", "cloud"])
+def test_training_points_match_reference_datagen(name):
+    """MeanFreePathSample / GetDesiredCountSample (dataGen.cu:148-216) run by
+    the reference (mt19937 draws) against the oracle's restatement (Philox):
+    the distributions of the training points' radius, of each coordinate and
+    of the view directions agree (two-sample chi-square, p > 1e-4)."""
+    from scipy.stats import chi2
+    d = golden("ref_datagen.npz")
+    dens = scenes.sphere_density(64) if name == "sphere" else cloud_np.cloud(CLOUD_RES, CLOUD_SEED)
+    md, _, _ = orc.build_mips(dens)
+    rp, rv = d[name + "_pos"].astype(np.float32), d[name + "_view"].astype(np.float32)
+    op, ov = orc.train_points(dens, md, float(d[name + "_alpha"]), 0.857, 3, 60000, 40000)
+    assert len(op) > 10000
+    checks = [(np.linalg.norm(rp, axis=1), np.linalg.norm(op, axis=1), np.linspace(0, 0.5 * np.sqrt(3), 41))]
+    for c in range(3):
+        checks.append((rp[:, c], op[:, c], np.linspace(-0.51, 0.51, 41)))
+        checks.append((rv[:, c], ov[:, c], np.linspace(-1.0, 1.0, 21)))
+    for a, b, bins in checks:
+        stat, dof = _two_sample_chi2(a, b, bins)
+        assert chi2.sf(stat, dof) > 1e-4, (stat, dof)
