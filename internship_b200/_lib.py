@@ -32,6 +32,7 @@ EXPORTS = [
     "mr_tc_selftest_fp8", "mr_sampler_selftest", "mr_tc_selftest_tf32", "mr_render_host_async",
     "mr_render_host_wait", "mr_spiral_stencil", "mr_stream_read_probe", "mr_volume_load", "mr_volume_file_read",
     "mr_tc_wait_selftest", "mr_volume_set_hdri", "mr_volume_load_hdri", "mr_volume_clear_hdri", "mr_hdr_read",
+    "mr_batch_set_timing", "mr_batch_frame_times",
 ]
 NOALLOC_MAX_PIXELS = 16384
 
@@ -108,6 +109,8 @@ def load():
     L.mr_volume_load.argtypes = [C.c_char_p, i32, C.POINTER(vp), vp]
     L.mr_tc_wait_selftest.argtypes = [i32, C.POINTER(C.c_int64)]
     L.mr_volume_set_hdri.argtypes = [vp, vp, i32, i32]
+    L.mr_batch_set_timing.argtypes = [vp, i32]
+    L.mr_batch_frame_times.argtypes = [vp, vp, i32]
     L.mr_volume_load_hdri.argtypes = [vp, C.c_char_p]
     L.mr_volume_clear_hdri.argtypes = [vp]
     L.mr_hdr_read.argtypes = [C.c_char_p, vp, sz, C.POINTER(i32), C.POINTER(i32)]

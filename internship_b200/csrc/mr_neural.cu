@@ -1018,7 +1018,18 @@ struct Batch {
   bool spill = false, prepared = false;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // Per-frame completion times (mr_batch_set_timing): an event before the
+  // first launch and one after each wave's network.
+  bool timing = false;
+  cudaEvent_t t_start = nullptr;
+  std::vector<cudaEvent_t> t_wave;
 
+  void drop_events() {
+    if (t_start) cudaEventDestroy(t_start);
+    for (cudaEvent_t e : t_wave) cudaEventDestroy(e);
+    t_start = nullptr;
+    t_wave.clear();
+  }
   void drop_graph() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
@@ -1027,6 +1038,7 @@ struct Batch {
   }
   void release() {
     drop_graph();
+    drop_events();
     if (d_jobs) cudaFree(d_jobs);
     if (d_h0) cudaFree(d_h0);
     if (d_out) cudaFree(d_out);
@@ -1058,6 +1070,8 @@ static int batch_launches(Batch& b, const Network* net, cudaStream_t s) {
   const bool tc = b.precision != MR_PREC_FP32;
   const bool hw = b.sampler == MR_SAMPLER_TEXTURE;
   const int nj = (int)b.jobs.size();
+  const bool timed = b.timing && b.t_start && (long long)b.t_wave.size() * b.wave >= b.total;
+  if (timed) MR_CUDA(cudaEventRecord(b.t_start, s));
   MR_CUDA(cudaMemsetAsync(b.counters, 0, kCounters * sizeof(unsigned long long), s));
   // the jobs' per-point tables, for the network given to this call
   if (hw)
@@ -1089,6 +1103,7 @@ static int batch_launches(Batch& b, const Network* net, cudaStream_t s) {
                            f3(1, 1, 1), f3(1, 1, 1), s, rec.job, b.d_out, desc, 4, 4 * ccap, desc + 48 * 4 * ccap, 4,
                            4 * ccap);
     if (rc) return rc;
+    if (timed) MR_CUDA(cudaEventRecord(b.t_wave[(size_t)(w0 / b.wave)], s));
   }
   k_batch_advance<<<(nj + 127) / 128, 128, 0, s>>>(b.d_jobs, nj);
   MR_CUDA(cudaGetLastError());
@@ -1322,6 +1337,38 @@ extern "C" int mr_batch_launch(mr_batch* h, void* stream) {
   if (!h) return set_error(MR_ERR_ARG, "mr_batch_launch: NULL argument");
   if (!h->b.exec) return set_error(MR_ERR_STATE, "mr_batch_capture first");
   MR_CUDA(cudaGraphLaunch(h->b.exec, (cudaStream_t)stream));
+  return MR_OK;
+}
+
+extern "C" int mr_batch_set_timing(mr_batch* h, int32_t enable) {
+  clear_error();
+  if (!h) return set_error(MR_ERR_ARG, "mr_batch_set_timing: NULL argument");
+  Batch& b = h->b;
+  if (!b.prepared) return set_error(MR_ERR_STATE, "mr_batch_prepare first");
+  b.drop_graph();  // a captured graph holds the old event set
+  b.drop_events();
+  b.timing = enable != 0;
+  if (!b.timing) return MR_OK;
+  const size_t waves = (size_t)((b.total + b.wave - 1) / b.wave);
+  MR_CUDA(cudaEventCreate(&b.t_start));
+  b.t_wave.assign(waves, nullptr);
+  for (size_t k = 0; k < waves; ++k) MR_CUDA(cudaEventCreate(&b.t_wave[k]));
+  return MR_OK;
+}
+
+extern "C" int mr_batch_frame_times(mr_batch* h, float* host_ms, int32_t n) {
+  clear_error();
+  if (!h || !host_ms) return set_error(MR_ERR_ARG, "mr_batch_frame_times: NULL argument");
+  Batch& b = h->b;
+  if (!b.timing || !b.t_start || b.t_wave.empty()) return set_error(MR_ERR_STATE, "mr_batch_set_timing(1) first");
+  if (n != (int32_t)b.jobs.size()) return set_error(MR_ERR_ARG, "%d jobs, %d slots", (int)b.jobs.size(), n);
+  MR_CUDA(cudaEventSynchronize(b.t_wave.back()));
+  long long pix = 0;
+  for (int j = 0; j < n; ++j) {
+    pix += (long long)b.jobs[j].p.width * b.jobs[j].p.height;
+    const size_t w = (size_t)((pix - 1) / b.wave);  // the wave holding the job's last pixel
+    MR_CUDA(cudaEventElapsedTime(&host_ms[j], b.t_start, b.t_wave[w]));
+  }
   return MR_OK;
 }
 

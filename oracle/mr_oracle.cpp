@@ -870,9 +870,21 @@ void orc_render_pt(const float* density, int res, float max_density, const mr_re
 // Neural render (rt = MRPNN), one primary sample per pixel with stream
 // (seed; pixel, sample_offset, ., TAG_NN): draws 0,1 jitter, then
 // GetSamplePoint, two frames, and the single-scatter Tr.
+void orc_render_neural_dist(const float* density, int res, float max_density, const float* mips, const float* tr,
+                            const float* lut, const float* weights, const float* stencil, const mr_render_params* p,
+                            int row0, int row1, float* out_rgb, float* out_dist, int nthreads);
 void orc_render_neural(const float* density, int res, float max_density, const float* mips,
                        const float* tr, const float* lut, const float* weights, const float* stencil,
                        const mr_render_params* p, int row0, int row1, float* out_rgb, int nthreads) {
+  orc_render_neural_dist(density, res, max_density, mips, tr, lut, weights, stencil, p, row0, row1, out_rgb, nullptr,
+                         nthreads);
+}
+
+// Same, also writing each pixel's first-hit distance (< 0: no medium), the
+// input of the interactive mode's reprojection.
+void orc_render_neural_dist(const float* density, int res, float max_density, const float* mips, const float* tr,
+                            const float* lut, const float* weights, const float* stencil, const mr_render_params* p,
+                            int row0, int row1, float* out_rgb, float* out_dist, int nthreads) {
   Vol vol{density, res, max_density, mips, tr, lut};
   Scene sc = make_scene(*p);
   Net net(weights);
@@ -888,6 +900,7 @@ void orc_render_neural(const float* density, int res, float max_density, const f
       V3 L = neural_pixel(tk, net, stencil, rng, f3(p->ori), dir, &t);
       L = vmax(L, v3(0, 0, 0));
       out_rgb[pix * 3 + 0] = L.x; out_rgb[pix * 3 + 1] = L.y; out_rgb[pix * 3 + 2] = L.z;
+      if (out_dist) out_dist[pix] = t;
     }
   }
 }
@@ -1152,6 +1165,55 @@ void orc_histogram_frame(const float* rad, int n, int fnum, float* accum, float*
     const float l = r[0] + r[1] + r[2];
     h[32] = lerp_f(h[32], l, rate);
     h[31] = lerp_f(h[31], l * l, rate);
+  }
+}
+
+// The interactive neural mode's temporal reuse (RenderCamera<true>,
+// core/volume.cu:126-143, with this project's camera inversion): the pixel's
+// first-hit point (distance 10 for sky pixels, at least 0.001) is projected
+// into the previous camera (prev_ori, prev_up, prev_right; forward =
+// normalize(-prev_ori)); the history colour stored there (hist scalars
+// total, x, x2) is blended with this frame's radiance at rate 1 / (1 + fnum),
+// capped at 0.2 where the ray hit the medium and the checkerboard is off.
+// Then ReprojectionDenoise (:266-287) keeps the result as the next history.
+// p: this frame's camera and jitter stream (sample_offset = frame index).
+void orc_reproject(const mr_render_params* p, const float* prev_ori, const float* prev_up, const float* prev_right,
+                   int fnum, int checker, const float* rad, const float* dist, float* hist, float* accum) {
+  const int W = p->width, H = p->height;
+  const V3 lori = v3(prev_ori[0], prev_ori[1], prev_ori[2]);
+  const V3 lup = v3(prev_up[0], prev_up[1], prev_up[2]);
+  const V3 lright = v3(prev_right[0], prev_right[1], prev_right[2]);
+  const V3 lf = normalize(lori * -1.0f);
+  std::vector<float> his((size_t)W * H * 3);
+  for (int pix = 0; pix < W * H; ++pix) {
+    his[3 * pix] = hist[33 * pix + 30];
+    his[3 * pix + 1] = hist[33 * pix + 32];
+    his[3 * pix + 2] = hist[33 * pix + 31];
+  }
+  for (int pix = 0; pix < W * H; ++pix) {
+    const int row = pix / W, col = pix - row * W;
+    Rng rng(p->seed, (uint32_t)pix, p->sample_offset, TAG_NN);
+    const float jx = rng.next(), jy = rng.next();
+    const V3 dir = camera_dir(*p, row, col, jx, jy);
+    const float d = dist[pix];
+    const bool skyp = d < 0.0f;
+    const float dis = std::max(0.001f, skyp ? 10.0f : d);
+    const V3 mp = f3(p->ori) + dir * dis;
+    V3 ld = mp - lori;
+    ld = ld / dot(ld, lf);
+    ld = ld - lf;
+    const float lu = 0.5f - dot(ld, lright) / (2.0f * dot(lright, lright));
+    const float lv = 0.5f - dot(ld, lup) / (2.0f * dot(lup, lup));
+    const int lx = std::min(W - 1, std::max(0, (int)(lu * W))), ly = std::min(H - 1, std::max(0, (int)(lv * H)));
+    const size_t q = (size_t)ly * W + lx;
+    float rate = 1.0f / (float)(1 + fnum);
+    if (!skyp && !checker) rate = std::min(0.2f, rate);
+    for (int c = 0; c < 3; ++c) accum[3 * pix + c] = his[3 * q + c] * (1.0f - rate) + rad[3 * pix + c] * rate;
+  }
+  for (int pix = 0; pix < W * H; ++pix) {
+    hist[33 * pix + 30] = accum[3 * pix];
+    hist[33 * pix + 32] = accum[3 * pix + 1];
+    hist[33 * pix + 31] = accum[3 * pix + 2];
   }
 }
 

@@ -38,6 +38,9 @@ def lib():
         L = C.CDLL(path)
         L.orc_philox.argtypes = [u32p, u32p, u32p]
         L.orc_weights_xavier.argtypes = [C.c_uint32, f32p]
+        L.orc_render_neural_dist.argtypes = [f32p, C.c_int, C.c_float, f32p, f32p, f32p, f32p, f32p,
+                                             C.c_void_p, C.c_int, C.c_int, f32p, f32p, C.c_int]
+        L.orc_reproject.argtypes = [C.c_void_p, f32p, f32p, f32p, C.c_int, C.c_int, f32p, f32p, f32p, f32p]
         L.orc_set_env.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.orc_select_env_light.argtypes = [C.c_void_p, f32p, f32p]
         L.orc_uniforms.argtypes = [C.c_uint32] * 4 + [C.c_int, f32p]
@@ -207,6 +210,28 @@ def render_neural(density, max_density, mips, tr, lut, weights, stencil, params,
                             _a(weights), _a(stencil), C.addressof(params), row0,
                             params.height if row1 is None else row1, out, nthreads())
     return out
+
+
+def render_neural_dist(density, max_density, mips, tr, lut, weights, stencil, params):
+    """Neural render plus each pixel's first-hit distance (< 0: no medium)."""
+    density = _a(density)
+    res = round(density.size ** (1 / 3))
+    n = params.width * params.height
+    out = np.zeros(n * 3, np.float32)
+    dist = np.zeros(n, np.float32)
+    lib().orc_render_neural_dist(density.ravel(), res, float(max_density), _a(mips), _a(tr), _a(lut), _a(weights),
+                                 _a(stencil), C.addressof(params), 0, params.height, out, dist, nthreads())
+    return out, dist
+
+
+def reproject(params, prev_ori, prev_up, prev_right, fnum, checker, rad, dist, hist):
+    """One interactive neural frame's reprojection + ReprojectionDenoise:
+    returns the blended colour (n x 3); `hist` (n x 33 float32, contiguous) is
+    updated in place."""
+    accum = np.zeros(params.width * params.height * 3, np.float32)
+    lib().orc_reproject(C.addressof(params), _a(prev_ori), _a(prev_up), _a(prev_right), int(fnum), int(checker),
+                        _a(rad).ravel(), _a(dist).ravel(), hist.ravel(), accum)
+    return accum
 
 
 def gather(mips, tr, lut, stencil, pos, frame, alpha, g, scatter, light):

@@ -214,3 +214,41 @@ def test_large_single_render_matches_waved_batch(torch):
     L.mr_batch_destroy(b)
     net.close()
     v.close()
+
+
+def test_batch_frame_times_follow_the_waves(torch):
+    """mr_batch_set_timing: completion times per frame from events inside the
+    captured graph; frames complete in add order (waves run in order) and
+    the last one with the batch."""
+    import internship_b200 as mr
+    from internship_b200 import _lib
+    L = _lib.load()
+    jobs, net = _jobs(mr, 1, 0)
+    b = C.c_void_p()
+    _lib.check(L.mr_batch_create(C.byref(b)))
+    outs = []
+    for v, p in jobs:
+        o = torch.empty(p.width * p.height * 3, device="cuda")
+        outs.append(o)
+        _lib.check(L.mr_batch_add(b, v.handle, C.byref(p), _ptr(o)))
+    stream = torch.cuda.Stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    _lib.check(L.mr_batch_prepare(b, net.handle, 1000, sp))  # several waves
+    ft = np.zeros(len(jobs), np.float32)
+    assert L.mr_batch_frame_times(b, ft.ctypes.data, len(jobs)) == _lib.MR_ERR_STATE
+    _lib.check(L.mr_batch_set_timing(b, 1))
+    _lib.check(L.mr_batch_capture(b, net.handle, sp))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    _lib.check(L.mr_batch_launch(b, sp))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    _lib.check(L.mr_batch_frame_times(b, ft.ctypes.data, len(jobs)))
+    total = e0.elapsed_time(e1)
+    assert np.all(ft > 0) and np.all(np.diff(ft) >= 0), ft
+    assert ft[-1] <= total * 1.05 + 0.05
+    assert ft[0] < ft[-1]  # the first job's frame finished in an earlier wave
+    _lib.check(L.mr_batch_destroy(b))
+    for v, _ in jobs[::2]:
+        v.close()
+    net.close()
