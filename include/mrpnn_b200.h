@@ -34,8 +34,14 @@ typedef enum {
 } mr_status;
 
 /* core/volume.hpp:88-90 VolumeRender::RenderType (RPNN's weights are not in
- * the reference tree and it is not supported here). */
-typedef enum { MR_RT_PT = 0, MR_RT_RPNN = 1, MR_RT_MRPNN = 2 } mr_render_type;
+ * the reference tree and it is not supported here), plus the marching form of
+ * the neural render, NNPredict<Type::marching_MRPNN> (core/render.cuh:524-633):
+ * the camera ray is marched in 1/1023 steps of its box length (negative
+ * densities skip that distance), the network's point is drawn among the
+ * marched samples in proportion to their absorbed share, and with a surface
+ * IOR (mr_volume_set_surface_ior) the first medium sample is a dielectric
+ * surface that reflects or refracts the ray. */
+typedef enum { MR_RT_PT = 0, MR_RT_RPNN = 1, MR_RT_MRPNN = 2, MR_RT_MARCHING_MRPNN = 3 } mr_render_type;
 
 /* Arithmetic of the radiance-predictor MLP.
  * FP32: CUDA cores, the reference's arithmetic order.
@@ -143,6 +149,9 @@ int mr_volume_clear_hdri(mr_volume* v);
  * receive the size; host_rgba (may be NULL to query the size) receives
  * width*height RGBA floats (alpha 0) if capacity allows. */
 int mr_hdr_read(const char* path, float* host_rgba, size_t capacity, int32_t* width, int32_t* height);
+/* SetSurfaceIOR (core/volume.cu:1490-1493): index of refraction of the
+ * surface of MR_RT_MARCHING_MRPNN renders; <= 0 (the default -1) = no surface. */
+int mr_volume_set_surface_ior(mr_volume* v, float ior);
 /* VolumeRender::max_density after mr_volume_update. */
 int mr_volume_max_density(const mr_volume* v, float* out);
 int mr_volume_resolution(const mr_volume* v, int32_t* out);

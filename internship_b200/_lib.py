@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmrpnn_b200.so")
 
 MR_OK, MR_ERR_ARG, MR_ERR_CUDA, MR_ERR_TIMEOUT, MR_ERR_LOOP_CAP, MR_ERR_STATE, MR_ERR_NOMEM, MR_ERR_UNSUPPORTED = range(8)
-RT_PT, RT_RPNN, RT_MRPNN = 0, 1, 2
+RT_PT, RT_RPNN, RT_MRPNN, RT_MARCHING_MRPNN = 0, 1, 2, 3
 PREC_FP32, PREC_BF16, PREC_FP8 = 0, 1, 2
 SAMPLER_EXACT, SAMPLER_TEXTURE = 0, 1
 READ_DENSITY, READ_MIP, READ_VARIANCE, READ_TR, READ_HGLUT = range(5)
@@ -32,7 +32,7 @@ EXPORTS = [
     "mr_tc_selftest_fp8", "mr_sampler_selftest", "mr_tc_selftest_tf32", "mr_render_host_async",
     "mr_render_host_wait", "mr_spiral_stencil", "mr_stream_read_probe", "mr_volume_load", "mr_volume_file_read",
     "mr_tc_wait_selftest", "mr_volume_set_hdri", "mr_volume_load_hdri", "mr_volume_clear_hdri", "mr_hdr_read",
-    "mr_batch_set_timing", "mr_batch_frame_times",
+    "mr_batch_set_timing", "mr_batch_frame_times", "mr_volume_set_surface_ior",
 ]
 NOALLOC_MAX_PIXELS = 16384
 
@@ -110,6 +110,7 @@ def load():
     L.mr_tc_wait_selftest.argtypes = [i32, C.POINTER(C.c_int64)]
     L.mr_volume_set_hdri.argtypes = [vp, vp, i32, i32]
     L.mr_batch_set_timing.argtypes = [vp, i32]
+    L.mr_volume_set_surface_ior.argtypes = [vp, fp]
     L.mr_batch_frame_times.argtypes = [vp, vp, i32]
     L.mr_volume_load_hdri.argtypes = [vp, C.c_char_p]
     L.mr_volume_clear_hdri.argtypes = [vp]

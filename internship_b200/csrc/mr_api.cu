@@ -28,6 +28,7 @@ void clear_error() { t_error.clear(); }
 
 int render_pt(Volume* v, const mr_render_params* p, float* dev_rgb, cudaStream_t s);
 int render_neural(Volume* v, const Network* net, const mr_render_params* p, float* dev_rgb, cudaStream_t s);
+int render_marching(Volume* v, const Network* net, const mr_render_params* p, float* dev_rgb, cudaStream_t s);
 int check_params(const mr_render_params* p);
 int pack_network(Network* n);
 void free_packed(Network* n);
@@ -79,6 +80,14 @@ static void spiral_stencil(float* out) {
 using namespace mr;
 
 extern "C" {
+
+int mr_volume_set_surface_ior(mr_volume* h, float ior) {
+  clear_error();
+  if (!h) return set_error(MR_ERR_ARG, "mr_volume_set_surface_ior: NULL argument");
+  if (!std::isfinite(ior)) return set_error(MR_ERR_ARG, "IOR is not finite");
+  h->v.surface_ior = ior;
+  return MR_OK;
+}
 
 const char* mr_version(void) { return "mrpnn-b200 0.1.0 (sm_100a)"; }
 const char* mr_last_error(void) { return t_error.c_str(); }
@@ -183,6 +192,7 @@ int mr_render(mr_volume* h, const mr_network* net, const mr_render_params* p, fl
   switch (p->render_type) {
     case MR_RT_PT: return render_pt(&h->v, p, dev_rgb, s);
     case MR_RT_MRPNN: return render_neural(&h->v, net ? &net->n : nullptr, p, dev_rgb, s);
+    case MR_RT_MARCHING_MRPNN: return render_marching(&h->v, net ? &net->n : nullptr, p, dev_rgb, s);
     case MR_RT_RPNN: return set_error(MR_ERR_UNSUPPORTED, "RPNN is not supported (its weights are not published)");
     default: return set_error(MR_ERR_ARG, "unknown render type %d", p->render_type);
   }

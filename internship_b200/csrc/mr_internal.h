@@ -82,6 +82,9 @@ struct Volume {
   float4* env_dev = nullptr;
   std::vector<float> env_host;
   int env_w = 0, env_h = 0;
+  // SetSurfaceIOR: index of refraction of the marching form's surface
+  // (negative: no surface, the reference's default -1).
+  float surface_ior = -1.0f;
   // Interactive delta tracking: FP64 per-pixel sums of the radiance (3), of
   // the histogram luminance l and of l^2, SoA (sum k of pixel p at
   // mom[k * mom_npx + p]), for the histogram buffer mom_hist they belong to.

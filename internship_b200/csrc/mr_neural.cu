@@ -167,6 +167,184 @@ __global__ void __launch_bounds__(128, 12) k_nn_trace(NNTraceArgs a) {
   trace_counters(a.counters, st, act);
 }
 
+// ---- marching variant (NNPredict<Type::marching_MRPNN>, core/render.cuh:524-633) ----
+// The camera ray is marched in fixed steps (1/1023 of the ray's box length,
+// longer where a negative density gives a distance to skip); the network's
+// point is drawn among the marched samples with weight T (1 - exp(-sigma dt))
+// by reservoir sampling. With a surface IOR > 0 the first positive sample is
+// a dielectric surface (normal from the negative-density field): its GGX
+// specular term lit through Tr is kept, and the ray continues reflected or
+// refracted with the Fresnel probability. The pixel is
+// ref + lerp((network + Tr * phase) * light, sky(dir), T_end).
+
+// Normal (core/render.cuh:371-387): central differences of max(0, -density),
+// the step widened by 0.01 (up to 10 times) while the gradient is zero.
+__device__ __forceinline__ F3 surface_normal(const Medium& m, F3 p, TrackStats& st) {
+  float dl = 0.02f;
+  F3 n;
+  int left = 10;
+  do {
+    auto neg = [&](F3 q) { return fmaxf(0.0f, -fetch_density(m, q, st)); };
+    n = f3(neg(p + f3(dl, 0, 0)) - neg(p - f3(dl, 0, 0)), neg(p + f3(0, dl, 0)) - neg(p - f3(0, dl, 0)),
+           neg(p + f3(0, 0, dl)) - neg(p - f3(0, 0, dl)));
+    dl += 0.01f;
+  } while (n.x == 0.0f && n.y == 0.0f && n.z == 0.0f && left-- > 0);
+  return normalize(n);
+}
+__device__ __forceinline__ float sat(float x) { return fminf(fmaxf(x, 0.0f), 1.0f); }
+// GGX distribution (GGXTerm, :389-395).
+__device__ __forceinline__ float ggx_d(float nh, float rough) {
+  const float a2 = rough * rough;
+  const float d = (nh * a2 - nh) * nh + 1.0f;
+  return 0.318309886183790671538f * a2 / (d * d + 1e-7f);
+}
+// Smith joint visibility (SmithJointGGXVisibilityTerm, :400-404).
+__device__ __forceinline__ float smith_v(float nl, float nv, float rough) {
+  const float k = (rough + 0.01f) * (rough + 0.01f) / 1.01f / 1.01f / 2.0f;
+  return (1e-5f + nl * nv) / (1e-5f + lerpf(nl, 1.0f, k) * lerpf(nv, 1.0f, k));
+}
+// Unpolarised dielectric Fresnel reflectance (PhysicsFresnel, :410-419).
+__device__ __forceinline__ float fresnel_dielectric(float ior, F3 i, F3 n) {
+  const float ci = fabsf(dot(i, n));
+  const float si = sqrtf(fmaxf(0.0f, 1.0f - ci * ci));
+  const float st = si / ior;
+  const float ct = sqrtf(fmaxf(0.0f, 1.0f - st * st));
+  const float r1 = (ior * ci - ct) / (ior * ci + ct);
+  const float r2 = (ci - ior * ct) / (ci + ior * ct);
+  return (r1 * r1 + r2 * r2) / 2.0f;
+}
+// Specular BRDF * n.l (Schlick Fresnel from F0 = 0.04, GGX, Smith; roughness
+// 0.008) and, in .w, the dielectric reflectance (BRDF, :428-461).
+__device__ __forceinline__ float4 surface_brdf(F3 n, F3 v, F3 l, float ior) {
+  const F3 h = normalize(l + v);
+  const float shift = dot(n, v);
+  if (shift < 0.0f) n = n + v * (-shift + 1e-5f);
+  const float nv = sat(dot(n, v)), nl = sat(dot(n, l)), nh = sat(dot(n, h)), lh = sat(dot(l, h));
+  const float rough = 0.008f;
+  const float D = ggx_d(nh, rough);
+  const float G = smith_v(nl, nv, rough) * 3.1415926f;
+  const float t = 1.0f - lh;
+  const float F = 0.04f + (1.0f - 0.04f) * (t * t * t * t * t);
+  const float dfg = F * G * D * nl;
+  return make_float4(dfg, dfg, dfg, fresnel_dielectric(ior, v, n));
+}
+__device__ __forceinline__ F3 refract_dir(F3 i, F3 n, float eta) {
+  const float ci = dot(i * -1.0f, n);
+  const float c2 = 1.0f - eta * eta * (1.0f - ci * ci);
+  const F3 t = i * eta + n * (eta * ci - sqrtf(fabsf(c2)));
+  return t * (c2 > 0.0f ? 1.0f : 0.0f);
+}
+__device__ __forceinline__ F3 reflect_dir(F3 i, F3 n) { return i - n * (dot(i, n) * 2.0f); }
+
+struct MarchArgs {
+  Medium m;
+  PathScene sc;
+  CameraModel cam;
+  uint32_t seed, frame_index;
+  float ior;
+  float* out;
+  Records rec;
+  float4* madd;  // per record: xyz = ref + sky * T_end, w = 1 - T_end
+  unsigned long long* counters;
+};
+
+constexpr int kMarchSteps = 1024;
+
+__global__ void __launch_bounds__(128) k_march_trace(MarchArgs a) {
+  const int pix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int npx = a.cam.width * a.cam.height;
+  TrackStats st{0, 0};
+  unsigned act = 0;
+  if (pix < npx) {
+    const PathScene& sc = a.sc;
+    const int row = pix / a.cam.width, col = pix - row * a.cam.width;
+    Rng rng;
+    rng.init(a.seed, (uint32_t)pix, a.frame_index, TAG_NN);
+    const float jx = rng.next(), jy = rng.next();
+    F3 dir = camera_dir(a.cam, row, col, jx, jy);
+    Frame f;
+    F3 ly, lz;
+    frame_from(rng, dir, f.X, f.Y, f.Z);
+    frame_from(rng, sc.L, f.LX, ly, lz);
+    const float offset = ray_box_offset(a.cam.ori, dir);
+    bool go = offset >= 0.0f;
+    F3 ori = a.cam.ori + dir * offset;
+    float dis = ray_box_distance(ori, dir);
+    float inv = dis / (float)(kMarchSteps - 1);
+    float trans = 1.0f, t = 0.0f, hit_dis = -1.0f, total_w = 0.0f;
+    bool surfaced = !(a.ior > 0.0f);
+    F3 ref = f3(0, 0, 0), pos = f3(0, 0, 0);
+    for (int step = 0; go; ++step) {
+      if (trans < 0.005f || t >= dis || step > kMarchSteps * 2) break;
+      const F3 sp = ori + dir * t;
+      const float vd = fetch_density(a.m, sp, st);
+      if (vd > 0.0f && hit_dis == -1.0f) hit_dis = offset + t;
+      t += fmaxf(inv, -vd);
+      if (vd <= 0.0f) continue;
+      if (!surfaced) {
+        F3 n = surface_normal(a.m, sp, st);
+        n = n - dir * fmaxf(0.0f, dot(n, dir) + 0.01f);
+        const float4 b = surface_brdf(n, dir * -1.0f, sc.L, a.ior);
+        const float ldis = ray_box_distance(sp, sc.L);
+        const float tr = transmittance(a.m, rng, sp, sc.L, ldis, sc.alpha, st);
+        ref = f3(b.x, b.y, b.z) * tr * sc.light_color;
+        dir = rng.next() < b.w ? reflect_dir(dir, n) : refract_dir(dir, n, 1.0f / a.ior);
+        ori = sp;
+        t = 0.0f;
+        dis = ray_box_distance(ori, dir);
+        inv = dis / (float)(kMarchSteps - 1);
+        frame_from(rng, dir, f.X, f.Y, f.Z);
+        frame_from(rng, sc.L, f.LX, ly, lz);
+        surfaced = true;
+      }
+      const float tr_step = expf(-vd * sc.alpha * inv);
+      const float w = trans * (1.0f - tr_step);
+      total_w += w;
+      if (rng.next() < w / total_w) pos = sp;
+      trans *= tr_step;
+    }
+    const F3 skyc = sky(sc, dir);
+    if (hit_dis < 0.0f) {
+      const F3 o = ref + skyc;
+      a.out[3 * (size_t)pix] = fmaxf(o.x, 0.0f);
+      a.out[3 * (size_t)pix + 1] = fmaxf(o.y, 0.0f);
+      a.out[3 * (size_t)pix + 2] = fmaxf(o.z, 0.0f);
+    } else {
+      const float d2 = ray_box_distance(pos, f.LX);
+      const float ph = hg_phase(dot(f.X, f.LX), sc.g);
+      const float tr = transmittance(a.m, rng, pos, f.LX, d2, sc.alpha, st) * ph;
+      const unsigned k = claim_slot(a.rec.count);
+      a.rec.pix[k] = pix;
+      a.rec.pos[3 * (size_t)k + 0] = pos.x;
+      a.rec.pos[3 * (size_t)k + 1] = pos.y;
+      a.rec.pos[3 * (size_t)k + 2] = pos.z;
+      float* fr = a.rec.frame + 12 * (size_t)k;
+      fr[0] = f.X.x; fr[1] = f.X.y; fr[2] = f.X.z;
+      fr[3] = f.Y.x; fr[4] = f.Y.y; fr[5] = f.Y.z;
+      fr[6] = f.Z.x; fr[7] = f.Z.y; fr[8] = f.Z.z;
+      fr[9] = f.LX.x; fr[10] = f.LX.y; fr[11] = f.LX.z;
+      a.rec.trph[k] = tr;
+      const F3 add = ref + skyc * trans;
+      a.madd[k] = make_float4(add.x, add.y, add.z, 1.0f - trans);
+      act = 1;
+    }
+  }
+  trace_counters(a.counters, st, act);
+}
+
+// out = ref + sky * T + (network + Tr * phase) * light * (1 - T) for the
+// marching records (the network wrote (network + Tr * phase) * light).
+__global__ void k_march_compose(const unsigned* __restrict__ count, const int* __restrict__ pix,
+                                const float4* __restrict__ madd, float* __restrict__ out) {
+  const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= *count) return;
+  const float4 m = madd[k];
+  float* o = out + 3 * (size_t)pix[k];
+  o[0] = fmaxf(m.x + o[0] * m.w, 0.0f);
+  o[1] = fmaxf(m.y + o[1] * m.w, 0.0f);
+  o[2] = fmaxf(m.z + o[2] * m.w, 0.0f);
+}
+
 inline __device__ Frame load_frame(const float* fr) {
   Frame f;
   f.X = f3(fr[0], fr[1], fr[2]);
@@ -521,7 +699,8 @@ static bool distinct_channels(const mr_render_params* p) {
 }
 
 static int neural_passes(Volume* v, const Network* net, const mr_render_params* p, float* dev_rgb, cudaStream_t s,
-                         void* base, bool timed, float* dev_dist = nullptr, bool no_alloc = false);
+                         void* base, bool timed, float* dev_dist = nullptr, bool no_alloc = false,
+                         bool marching = false);
 
 // Linear tables of a volume plus the texture objects sampler form `samp`
 // reads, whose copies are brought up to date on stream s.
@@ -559,10 +738,15 @@ static Records carve_records(void* base, size_t n) {
 }
 
 static int render_neural_impl(Volume* v, const Network* net, const mr_render_params* p, float* dev_rgb,
-                              float* dev_dist, cudaStream_t s);
+                              float* dev_dist, cudaStream_t s, bool marching = false);
 int render_neural(Volume* v, const Network* net, const mr_render_params* p, float* dev_rgb, cudaStream_t s) {
   return render_neural_impl(v, net, p, dev_rgb, nullptr, s);
 }
+// NNPredict<Type::marching_MRPNN> (ray marching, optional dielectric surface).
+int render_marching(Volume* v, const Network* net, const mr_render_params* p, float* dev_rgb, cudaStream_t s) {
+  return render_neural_impl(v, net, p, dev_rgb, nullptr, s, true);
+}
+static size_t march_extra_bytes(size_t n) { return (n * sizeof(float4) + 255) / 256 * 256; }
 // Same, also writing the first-hit distance of every pixel (interactive mode).
 int render_neural_dist(Volume* v, const Network* net, const mr_render_params* p, float* dev_rgb, float* dev_dist,
                        cudaStream_t s) {
@@ -570,7 +754,7 @@ int render_neural_dist(Volume* v, const Network* net, const mr_render_params* p,
 }
 
 static int render_neural_impl(Volume* v, const Network* net, const mr_render_params* p, float* dev_rgb,
-                              float* dev_dist, cudaStream_t s) {
+                              float* dev_dist, cudaStream_t s, bool marching) {
   if (!net) return set_error(MR_ERR_ARG, "MRPNN render needs a network (mr_network_create)");
   if (!v->data_set) return set_error(MR_ERR_STATE, "render before mr_volume_set_data");
   if (!v->mips_valid) return set_error(MR_ERR_STATE, "render before mr_volume_update");
@@ -592,15 +776,16 @@ static int render_neural_impl(Volume* v, const Network* net, const mr_render_par
     if (rc) return rc;
   }
   size_t npx = (size_t)p->width * p->height;
-  int rc = ensure_scratch(v, neural_scratch_bytes(npx, distinct_channels(p)), s);
+  int rc = ensure_scratch(v, neural_scratch_bytes(npx, distinct_channels(p)) + (marching ? march_extra_bytes(npx) : 0),
+                          s);
   if (rc) return rc;
-  return neural_passes(v, net, p, dev_rgb, s, v->scratch, true, dev_dist);
+  return neural_passes(v, net, p, dev_rgb, s, v->scratch, true, dev_dist, false, marching);
 }
 
 // Trace, gather and network over scratch at `base` (neural_scratch_bytes of
 // width*height); `timed` = record stage events when the volume's timer is on.
 static int neural_passes(Volume* v, const Network* net, const mr_render_params* p, float* dev_rgb, cudaStream_t s,
-                         void* base, bool timed, float* dev_dist, bool no_alloc) {
+                         void* base, bool timed, float* dev_dist, bool no_alloc, bool marching) {
   auto mark = [&](int st) { if (timed) v->timer.mark(st, s); };
   int rc = MR_OK;
   const F3 L = normalize(to_f3(p->light_dir));
@@ -658,8 +843,24 @@ static int neural_passes(Volume* v, const Network* net, const mr_render_params* 
     k_sphere_h0<kSampLoad><<<1, 192, 0, hs>>>(tabs, net->stencil, h0s);
   MR_CUDA(cudaGetLastError());
   if (hs != s) MR_CUDA(cudaEventRecord(v->side_join, hs));
+  float4* madd = marching ? (float4*)((char*)base + neural_scratch_bytes(npx, distinct_channels(p))) : nullptr;
   mark(ST_NN_TRACE);
-  k_nn_trace<<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(ta);
+  if (marching) {
+    MarchArgs ma;
+    ma.m = ta.m;
+    ma.sc = ta.sc;
+    ma.cam = ta.cam;
+    ma.seed = ta.seed;
+    ma.frame_index = ta.frame_index;
+    ma.ior = v->surface_ior;
+    ma.out = dev_rgb;
+    ma.rec = rec;
+    ma.madd = madd;
+    ma.counters = v->d_counters;
+    k_march_trace<<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(ma);
+  } else {
+    k_nn_trace<<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(ta);
+  }
   mark(ST_NN_TRACE);
   MR_CUDA(cudaGetLastError());
   if (hs != s) MR_CUDA(cudaStreamWaitEvent(s, v->side_join, 0));
@@ -689,17 +890,24 @@ static int neural_passes(Volume* v, const Network* net, const mr_render_params* 
   mark(ST_NN_PREDICT);
   MR_CUDA(cudaGetLastError());
   const long long cap = (long long)npx;
+  // the marching form weights the network's light by 1 - T afterwards and
+  // does not multiply it by the albedo (core/render.cuh:631)
+  const F3 out_scale = marching ? f3(1, 1, 1) : to_f3(p->scatter_rate);
   mark(ST_NN_MLP);
   if (tc)
     rc = launch_mlp_tc(net, desc, aux, 4, 4 * cap, 1, cap, (int)npx, dev_rgb, rec.pix, rec.trph, rec.count,
-                       to_f3(p->light_color), to_f3(p->scatter_rate), spill, p->precision == MR_PREC_FP8, s);
+                       to_f3(p->light_color), out_scale, spill, p->precision == MR_PREC_FP8, s);
   else
     // trunk outputs over the row's first 38 descriptor chunks, the head's LC2
     // outputs over chunks 48..71 (all consumed by the trunk)
     rc = launch_mlp_simt(net, desc, aux, 4, 4 * cap, 1, cap, (int)npx, rec.count, dev_rgb, rec.pix, rec.trph,
-                         to_f3(p->light_color), to_f3(p->scatter_rate), s, nullptr, nullptr, desc, 4, 4 * cap,
+                         to_f3(p->light_color), out_scale, s, nullptr, nullptr, desc, 4, 4 * cap,
                          desc + 48 * 4 * cap, 4, 4 * cap);
   mark(ST_NN_MLP);
+  if (rc == MR_OK && marching) {
+    k_march_compose<<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(rec.count, rec.pix, madd, dev_rgb);
+    MR_CUDA(cudaGetLastError());
+  }
   return rc;
 }
 

@@ -69,6 +69,16 @@ def sphere_density(res=128):
     return (d < 0.25).astype(np.float32)
 
 
+def sdf_sphere_density(res=128, radius=0.2):
+    """A medium sphere (density 1) inside a signed-distance field: outside the
+    sphere the density is minus the distance to its surface, the encoding the
+    marching form reads as empty space to skip and as the side of a surface."""
+    i = (np.arange(res) + 0.5) / res
+    x, y, z = np.meshgrid(i, i, i, indexing="ij")
+    d = np.sqrt((x - 0.5) ** 2 + (y - 0.5) ** 2 + (z - 0.5) ** 2)
+    return np.where(d < radius, 1.0, radius - d).astype(np.float32)
+
+
 CAMERA_DIR = np.array([1.0, 0.55, 0.8]) / np.linalg.norm([1.0, 0.55, 0.8])
 
 

@@ -523,6 +523,114 @@ V3 neural_pixel(Tracker& tk, const Net& net, const float* stencil, Rng& rng, V3 
   return (pred * sc.light_color) * sc.scatter;
 }
 
+// ---- NNPredict<Type::marching_MRPNN> (core/render.cuh:371-461, 524-633) ----
+static V3 m_normal(Tracker& tk, V3 p) {  // Normal, :371-387
+  float dl = 0.02f;
+  V3 n;
+  int left = 10;
+  do {
+    auto neg = [&](V3 q) { return std::max(0.0f, -tk.density(q)); };
+    n = v3(neg(p + v3(dl, 0, 0)) - neg(p - v3(dl, 0, 0)), neg(p + v3(0, dl, 0)) - neg(p - v3(0, dl, 0)),
+           neg(p + v3(0, 0, dl)) - neg(p - v3(0, 0, dl)));
+    dl += 0.01f;
+  } while (n.x == 0.0f && n.y == 0.0f && n.z == 0.0f && left-- > 0);
+  return normalize(n);
+}
+static float m_sat(float x) { return std::min(std::max(x, 0.0f), 1.0f); }
+static float m_lerp(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+// BRDF (:428-461): GGX specular (F0 0.04, roughness 0.008) and the dielectric
+// Fresnel reflectance (PhysicsFresnel, :410-419) in w.
+static void m_brdf(V3 n, V3 v, V3 l, float ior, float* spec, float* fres) {
+  const V3 h = normalize(l + v);
+  const float shift = dot(n, v);
+  if (shift < 0.0f) n = n + v * (-shift + 1e-5f);
+  const float nv = m_sat(dot(n, v)), nl = m_sat(dot(n, l)), nh = m_sat(dot(n, h)), lh = m_sat(dot(l, h));
+  const float r = 0.008f, a2 = r * r;
+  const float dd = (nh * a2 - nh) * nh + 1.0f;
+  const float D = 0.318309886183790671538f * a2 / (dd * dd + 1e-7f);
+  const float k = (r + 0.01f) * (r + 0.01f) / 1.01f / 1.01f / 2.0f;
+  const float G = (1e-5f + nl * nv) / (1e-5f + m_lerp(nl, 1.0f, k) * m_lerp(nv, 1.0f, k)) * 3.1415926f;
+  const float t = 1.0f - lh;
+  const float F = 0.04f + (1.0f - 0.04f) * (t * t * t * t * t);
+  *spec = F * G * D * nl;
+  const float ci = std::fabs(dot(v, n));
+  const float si = std::sqrt(std::max(0.0f, 1.0f - ci * ci));
+  const float st = si / ior;
+  const float ct = std::sqrt(std::max(0.0f, 1.0f - st * st));
+  const float r1 = (ior * ci - ct) / (ior * ci + ct);
+  const float r2 = (ci - ior * ct) / (ci + ior * ct);
+  *fres = (r1 * r1 + r2 * r2) / 2.0f;
+}
+static V3 m_refract(V3 i, V3 n, float eta) {
+  const float ci = dot(i * -1.0f, n);
+  const float c2 = 1.0f - eta * eta * (1.0f - ci * ci);
+  const V3 t = i * eta + n * (eta * ci - std::sqrt(std::fabs(c2)));
+  return t * (c2 > 0.0f ? 1.0f : 0.0f);
+}
+static V3 m_reflect(V3 i, V3 n) { return i - n * (dot(i, n) * 2.0f); }
+
+V3 marching_pixel(Tracker& tk, const Net& net, const float* stencil, Rng& rng, V3 ori0, V3 dir, float ior,
+                  float* hit_t) {
+  const Scene& sc = tk.sc;
+  dir = normalize(dir);
+  const V3 L = normalize(sc.light_dir);
+  Frame f;
+  V3 ly, lz;
+  frame_from(rng, dir, f.X, f.Y, f.Z);
+  frame_from(rng, L, f.LX, ly, lz);
+  const float offset = ray_box_offset(ori0, dir);
+  bool go = offset >= 0.0f;
+  V3 ori = ori0 + dir * offset;
+  float dis = ray_box_distance(ori, dir);
+  const int steps = 1024;
+  float inv = dis / (float)(steps - 1);
+  float trans = 1.0f, t = 0.0f, hit_dis = -1.0f, total_w = 0.0f;
+  bool surfaced = !(ior > 0.0f);
+  V3 ref = v3(0, 0, 0), pos = v3(0, 0, 0);
+  for (int step = 0; go; ++step) {
+    if (trans < 0.005f || t >= dis || step > steps * 2) break;
+    const V3 sp = ori + dir * t;
+    const float vd = tk.density(sp);
+    if (vd > 0.0f && hit_dis == -1.0f) hit_dis = offset + t;
+    t += std::max(inv, -vd);
+    if (vd <= 0.0f) continue;
+    if (!surfaced) {
+      V3 n = m_normal(tk, sp);
+      n = n - dir * std::max(0.0f, dot(n, dir) + 0.01f);
+      float spec, fres;
+      m_brdf(n, dir * -1.0f, L, ior, &spec, &fres);
+      const float tr = tk.transmittance(rng, sp, L, ray_box_distance(sp, L), sc.alpha);
+      ref = sc.light_color * (spec * tr);
+      dir = rng.next() < fres ? m_reflect(dir, n) : m_refract(dir, n, 1.0f / ior);
+      ori = sp;
+      t = 0.0f;
+      dis = ray_box_distance(ori, dir);
+      inv = dis / (float)(steps - 1);
+      frame_from(rng, dir, f.X, f.Y, f.Z);
+      frame_from(rng, L, f.LX, ly, lz);
+      surfaced = true;
+    }
+    const float tr_step = std::exp(-vd * sc.alpha * inv);
+    const float w = trans * (1.0f - tr_step);
+    total_w += w;
+    if (rng.next() < w / total_w) pos = sp;
+    trans *= tr_step;
+  }
+  const V3 skyc = sky(sc, dir);
+  *hit_t = hit_dis;
+  if (hit_dis < 0.0f) return ref + skyc;
+  NetState s;
+  gather(s, tk.vol, stencil, pos, L, f, sc.alpha, sc.g);
+  const V3 scatterrate = sc.scatter / 1.001f;
+  const float gamma = std::acos(dot(f.X, f.LX));
+  V3 pred = network(s, net, sc.g, gamma, scatterrate);
+  const float ph = hg_phase(dot(f.X, f.LX), sc.g);
+  const float tr = tk.transmittance(rng, pos, f.LX, ray_box_distance(pos, f.LX), sc.alpha) * ph;
+  pred = pred + tr;
+  const V3 lit = pred * sc.light_color;
+  return ref + lit * (1.0f - trans) + skyc * trans;
+}
+
 inline float u01_tag(uint32_t seed, uint32_t a, uint32_t b, uint32_t tag) {
   Rng r(seed, a, b, tag);
   return r.next();
@@ -878,6 +986,31 @@ void orc_render_neural(const float* density, int res, float max_density, const f
                        const mr_render_params* p, int row0, int row1, float* out_rgb, int nthreads) {
   orc_render_neural_dist(density, res, max_density, mips, tr, lut, weights, stencil, p, row0, row1, out_rgb, nullptr,
                          nthreads);
+}
+
+// NNPredict<Type::marching_MRPNN> render, rows [row0, row1): the marching
+// form with surface index of refraction `ior` (<= 0: no surface); the same
+// per-pixel Philox stream as the neural render.
+void orc_render_marching(const float* density, int res, float max_density, const float* mips, const float* tr,
+                         const float* lut, const float* weights, const float* stencil, const mr_render_params* p,
+                         float ior, int row0, int row1, float* out_rgb, int nthreads) {
+  Vol vol{density, res, max_density, mips, tr, lut};
+  Scene sc = make_scene(*p);
+  Net net(weights);
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+  for (int row = row0; row < row1; ++row) {
+    Tracker tk{vol, sc};
+    for (int col = 0; col < p->width; ++col) {
+      size_t pix = (size_t)row * p->width + col;
+      Rng rng(p->seed, (uint32_t)pix, p->sample_offset, TAG_NN);
+      float jx = rng.next(), jy = rng.next();
+      V3 dir = camera_dir(*p, row, col, jx, jy);
+      float t;
+      V3 L = marching_pixel(tk, net, stencil, rng, f3(p->ori), dir, ior, &t);
+      L = vmax(L, v3(0, 0, 0));
+      out_rgb[pix * 3 + 0] = L.x; out_rgb[pix * 3 + 1] = L.y; out_rgb[pix * 3 + 2] = L.z;
+    }
+  }
 }
 
 // Same, also writing each pixel's first-hit distance (< 0: no medium), the

@@ -40,6 +40,8 @@ def lib():
         L.orc_weights_xavier.argtypes = [C.c_uint32, f32p]
         L.orc_render_neural_dist.argtypes = [f32p, C.c_int, C.c_float, f32p, f32p, f32p, f32p, f32p,
                                              C.c_void_p, C.c_int, C.c_int, f32p, f32p, C.c_int]
+        L.orc_render_marching.argtypes = [f32p, C.c_int, C.c_float, f32p, f32p, f32p, f32p, f32p,
+                                          C.c_void_p, C.c_float, C.c_int, C.c_int, f32p, C.c_int]
         L.orc_reproject.argtypes = [C.c_void_p, f32p, f32p, f32p, C.c_int, C.c_int, f32p, f32p, f32p, f32p]
         L.orc_set_env.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.orc_select_env_light.argtypes = [C.c_void_p, f32p, f32p]
@@ -222,6 +224,16 @@ def render_neural_dist(density, max_density, mips, tr, lut, weights, stencil, pa
     lib().orc_render_neural_dist(density.ravel(), res, float(max_density), _a(mips), _a(tr), _a(lut), _a(weights),
                                  _a(stencil), C.addressof(params), 0, params.height, out, dist, nthreads())
     return out, dist
+
+
+def render_marching(density, max_density, mips, tr, lut, weights, stencil, params, ior=-1.0):
+    """NNPredict<Type::marching_MRPNN> render (surface index of refraction ior)."""
+    density = _a(density)
+    res = round(density.size ** (1 / 3))
+    out = np.zeros(params.width * params.height * 3, np.float32)
+    lib().orc_render_marching(density.ravel(), res, float(max_density), _a(mips), _a(tr), _a(lut), _a(weights),
+                              _a(stencil), C.addressof(params), float(ior), 0, params.height, out, nthreads())
+    return out
 
 
 def reproject(params, prev_ori, prev_up, prev_right, fnum, checker, rad, dist, hist):

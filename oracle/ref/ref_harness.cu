@@ -114,6 +114,25 @@ __global__ void k_pass_nn(float3* out, int2 size, float3 ori, float3 up, float3 
   out[idx] = res;
 }
 
+// NNPredict<Type::marching_MRPNN> (core/render.cuh:524-633), which the
+// reference's own host code never instantiates: one pass, same camera model.
+__global__ void k_pass_march(float3* out, int2 size, float3 ori, float3 up, float3 right, float3 lightDir,
+                             float3 lightColor, float alpha, float g) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  int idx = i * size.x + j;
+  curandState seed;
+  InitRand(&seed);
+  float u = 1 - (j + Rand(&seed)) / size.x;
+  float v = 1 - (i + Rand(&seed)) / size.y;
+  float3 forward = normalize(-ori);
+  float3 dir = normalize(forward + (right * (u * 2 - 1)) + (up * (v * 2 - 1)));
+  float4 r = NNPredict<Type::marching_MRPNN>(ori, dir, lightDir, lightColor, alpha, g);
+  float3 res = max(float3{0, 0, 0}, make_float3(r));
+  if (i >= size.x || j >= size.y) return;
+  out[idx] = res;
+}
+
 __global__ void k_accum(const float3* in, int n, double* sum, double* sumsq) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
@@ -205,7 +224,14 @@ int ref_setup(const float* density, int res, float max_density, const float* mip
   return 0;
 }
 
-// Offline PT render (VolumeRender::Render with rt = PT): spp passes, per-pixel
+// SetSurfaceIOR (the marching form's surface; <= 0: none).
+int ref_set_ior(float ior) {
+  CK(cudaMemcpyToSymbol(IOR, &ior, sizeof(float)));
+  return 0;
+}
+
+// mode 0: offline PT render (VolumeRender::Render with rt = PT); 1: NNPredict<MRPNN>;
+// 2: NNPredict<marching_MRPNN>. spp passes, per-pixel
 // fp64 sums and sums of squares of the per-pass radiance (host buffers).
 int ref_render(int mode, int w, int h, const float* ori, const float* up, const float* right, const float* light,
                const float* light_color, float alpha, int multi_scatter, float g, int spp, double* sum,
@@ -225,8 +251,11 @@ int ref_render(int mode, int w, int h, const float* ori, const float* up, const 
     if (mode == 0)
       k_pass_pt<<<grid, block>>>(d_out, int2{w, h}, F3(ori), F3(up), F3(right), F3(light), F3(light_color), alpha,
                                  multi_scatter, g);
-    else
+    else if (mode == 1)
       k_pass_nn<<<grid, block>>>(d_out, int2{w, h}, F3(ori), F3(up), F3(right), F3(light), F3(light_color), alpha, g);
+    else
+      k_pass_march<<<grid, block>>>(d_out, int2{w, h}, F3(ori), F3(up), F3(right), F3(light), F3(light_color), alpha,
+                                    g);
     k_accum<<<(n + 127) / 128, 128>>>(d_out, n, d_sum, d_sq);
     CK(cudaGetLastError());
   }

@@ -33,6 +33,7 @@ class Ref:
         L.ref_load_weights.argtypes = [f32p, C.c_long]
         L.ref_read_weights.argtypes = [f32p, C.c_long]
         L.ref_read_stencil.argtypes = [f32p]
+        L.ref_set_ior.argtypes = [C.c_float]
         self.L = L
 
     def setup(self, density, max_density, mips, tr, lut, env=(0, 0, 0), scatter=(0.99,) * 3, tr_scale=1.0):
@@ -51,6 +52,9 @@ class Ref:
                                int(bounces), float(g), int(spp), s, s2)
         assert rc == 0, "ref_render failed"
         return s, s2
+
+    def set_ior(self, ior):
+        assert self.L.ref_set_ior(float(ior)) == 0
 
     def predict_frames(self, pos, frame, light, alpha, g, scatterrate):
         n = len(pos)

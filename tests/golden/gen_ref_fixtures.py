@@ -41,6 +41,13 @@ ref_datagen.npz  -- dataGen's GetDesiredCountSample (MeanFreePathSample over
                     64^3 sphere (alpha 16) and the 64^3 cloud (alpha 24):
                     20000 training points each (position, view direction;
                     float16). Runs without a GPU.
+ref_march.npz    -- NNPredict<Type::marching_MRPNN> (instantiated by the
+                    harness; the reference's host code never does) on a
+                    medium sphere inside a signed-distance field
+                    (scenes.sdf_sphere_density(128)), 32x32, 512 passes,
+                    the reference's weights and its own Fill_TR / Fill_Hg
+                    tables, without a surface (IOR -1) and with IOR 1.33:
+                    per-pixel sums / squares.
 ref_hdri.npz     -- the offline VolumeRender::Render (delta tracking) of the
                     sphere scene (alpha 16) under an environment map loaded
                     with SetHDRI from a generated .hdr file (its RGBE pixels
@@ -58,7 +65,7 @@ sys.path.insert(0, ROOT)
 from internship_b200 import scenes  # noqa: E402
 from oracle import cloud_np, orc, ref_py  # noqa: E402
 
-SECTIONS = ("network", "pt", "gather", "nn", "tables", "denoise", "labels", "bmp", "hdri", "datagen")
+SECTIONS = ("network", "pt", "gather", "nn", "tables", "denoise", "labels", "bmp", "hdri", "datagen", "march")
 
 
 def rand_frames(rng, n, light):
@@ -275,6 +282,26 @@ def gen_bmp(out, rng):
     rgb = np.concatenate([rng.uniform(0, 1, (128, 3)), rng.uniform(0, 20, (128, 3))]).astype(np.float32)
     np.savez_compressed(os.path.join(out, "ref_bmp.npz"), image=img, bmp=data, rgb=rgb, aces=rv.tone_host(rgb, 2),
                         gamma=rv.tone_host(rgb, 1))
+
+
+def gen_march(out, rng):
+    dens = scenes.sdf_sphere_density(128)
+    md, mips, _ = orc.build_mips(dens)
+    p = scenes.make_params(32, 32, 1, alpha=32.0)
+    L = np.array([p.light_dir.x, p.light_dir.y, p.light_dir.z], np.float32)
+    rv = ref_py.RefVolume()
+    tr = rv.fill_tr(mips, p.alpha, L)
+    lut, _ = rv.fill_hg(p.g, 0)
+    ref = ref_py.Ref()
+    ref.setup(dens, md, mips, tr, lut, scatter=(0.99, 0.99, 0.99))
+    ori, up, right = camera(p)
+    res = dict(spp=512, width=32, height=32, alpha=np.float32(p.alpha))
+    for name, ior in (("plain", -1.0), ("ior", 1.33)):
+        ref.set_ior(ior)
+        s, s2 = ref.render(2, 32, 32, ori, up, right, L, (1, 1, 1), p.alpha, 512, p.g, 512)
+        res[name + "_sum"], res[name + "_sumsq"] = s, s2
+    ref.set_ior(-1.0)
+    np.savez_compressed(os.path.join(out, "ref_march.npz"), **res)
 
 
 def gen_datagen(out, rng):
