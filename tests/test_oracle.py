@@ -211,9 +211,12 @@ def test_gather_network_matches_reference():
     assert (ref > 0).mean() > 0.5
     # The reference reads through hardware texture filtering (8-bit
     # interpolation weights); the oracle interpolates in fp32.
-    err = np.abs(out - ref) / (np.abs(ref) + 1e-3)
+    diff = np.abs(out - ref)
+    err = diff / (np.abs(ref) + 1e-3)
     assert np.median(err) < 2e-3
-    assert err.max() < 5e-2
+    # every output within 5 % of the reference's, or 1e-4 absolute where the
+    # radiance itself is a few 1e-4 and the 8-bit weights dominate
+    assert np.all((diff < 5e-2 * np.abs(ref)) | (diff < 1e-4)), err.max()
 
 
 def test_neural_render_matches_reference_statistically():

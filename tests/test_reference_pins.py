@@ -136,9 +136,11 @@ def test_labels_match_reference_get_samples(name):
     pos, dirs = d[name + "_pos"], d[name + "_dir"]
     alpha, g, sc, b = float(d[name + "_alpha"]), float(d["g"]), float(d["scatter"]), int(d["bounces"])
     K = 4
-    ests = np.stack([orc.get_samples(dens, md, pos, dirs, d[name + "_light"], np.full(len(pos), alpha, np.float32),
-                                     np.full(len(pos), g, np.float32), np.full(len(pos), sc, np.float32), b, spp,
-                                     seed=11 + k) / spp for k in range(K)])
+    light = np.tile(d[name + "_light"].reshape(1, 3), (len(pos), 1))  # one light for every point
+    n = len(pos)
+    ests = np.stack([orc.get_samples(dens, md, pos, dirs, light, np.full(n, alpha, np.float32),
+                                     np.full(n, g, np.float32), np.full(n, sc, np.float32), b, spp,
+                                     seed=11 + k) for k in range(K)])
     ours = ests.mean(0)
     our_se = ests.std(0, ddof=1) / np.sqrt(K)
     z = (ours - ref_mean) / np.sqrt(ref_se ** 2 + our_se ** 2 + 1e-12)
