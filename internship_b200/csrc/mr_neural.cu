@@ -1279,7 +1279,9 @@ static int batch_launches(Batch& b, const Network* net, cudaStream_t s) {
   const bool hw = b.sampler == MR_SAMPLER_TEXTURE;
   const int nj = (int)b.jobs.size();
   const bool timed = b.timing && b.t_start && (long long)b.t_wave.size() * b.wave >= b.total;
-  if (timed) MR_CUDA(cudaEventRecord(b.t_start, s));
+  // external records: under stream capture they become event-record nodes of
+  // the graph, so the events are recorded on every launch of it
+  if (timed) MR_CUDA(cudaEventRecordWithFlags(b.t_start, s, cudaEventRecordExternal));
   MR_CUDA(cudaMemsetAsync(b.counters, 0, kCounters * sizeof(unsigned long long), s));
   // the jobs' per-point tables, for the network given to this call
   if (hw)
@@ -1311,7 +1313,7 @@ static int batch_launches(Batch& b, const Network* net, cudaStream_t s) {
                            f3(1, 1, 1), f3(1, 1, 1), s, rec.job, b.d_out, desc, 4, 4 * ccap, desc + 48 * 4 * ccap, 4,
                            4 * ccap);
     if (rc) return rc;
-    if (timed) MR_CUDA(cudaEventRecord(b.t_wave[(size_t)(w0 / b.wave)], s));
+    if (timed) MR_CUDA(cudaEventRecordWithFlags(b.t_wave[(size_t)(w0 / b.wave)], s, cudaEventRecordExternal));
   }
   k_batch_advance<<<(nj + 127) / 128, 128, 0, s>>>(b.d_jobs, nj);
   MR_CUDA(cudaGetLastError());

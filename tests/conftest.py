@@ -8,7 +8,7 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-REFERENCE = os.environ.get("MRPNN_REFERENCE", "/root/reference")
+from oracle.build import REF_SRC as REFERENCE  # the reference checkout, located by the build recipe
 
 
 def pytest_configure(config):

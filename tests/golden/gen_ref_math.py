@@ -3,8 +3,8 @@
 Compiles the reference's core/vector.cu (its __host__ __device__ functions)
 together with a small host driver written here, runs it on a fixed grid of
 inputs and stores the outputs. Needs nvcc and the reference checkout
-(MRPNN_REFERENCE, default /root/reference); the committed .npz is what the
-tests read.
+(located by oracle/build.py, MRPNN_REFERENCE overrides it); the committed .npz
+is what the tests read.
 
 Functions pinned: HenyeyGreenstein, SampleHeneyGreenstein,
 SampleHenyeyGreenstein, UniformSampleSphere, RayBoxOffset, RayBoxDistance,
@@ -17,7 +17,8 @@ import tempfile
 
 import numpy as np
 
-REF = os.environ.get("MRPNN_REFERENCE", "/root/reference")
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
+from oracle.build import REF_SRC as REF  # noqa: E402
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_math.npz")
 
 DRIVER = r'''
