@@ -374,14 +374,15 @@ int mr_batch_capture(mr_batch* b, const mr_network* net, void* stream);
 /* Replays the captured graph: one more frame of every job. */
 int mr_batch_launch(mr_batch* b, void* stream);
 /* Per-frame completion times (no reference counterpart). With timing on,
- * every batch frame (eager or a replay captured after this call) records an
- * event before its first launch and one after each wave; the jobs' pixels are
+ * every batch frame (eager or a replay captured after this call) records the
+ * device timer before its first launch and after each wave; the jobs' pixels are
  * laid out in the order they were added, so a job's frame is complete when
  * the wave holding its last pixel is. Call after mr_batch_prepare / _autotune
  * and before mr_batch_capture (it drops a captured graph). */
 int mr_batch_set_timing(mr_batch* b, int32_t enable);
 /* Milliseconds from the start of the last batch frame to the completion of
- * each job's frame (n = number of jobs, in add order); waits for that frame. */
+ * each job's frame (n = number of jobs, in add order), from the device's
+ * global timer (about 1 us resolution); waits for the device. */
 int mr_batch_frame_times(mr_batch* b, float* host_ms, int32_t n);
 /* Counters of the frames since mr_batch_prepare's last reset: [0] density
  * fetches, [2] loop-cap hits, [3] active pixels (of the last frame). */

@@ -1207,6 +1207,14 @@ __global__ void k_batch_advance(BatchJob* jobs, int n) {
   if (i < n) jobs[i].frame += 1u;
 }
 
+// The device's global nanosecond timer, by one thread, when the stream
+// reaches this launch.
+__global__ void k_stamp(unsigned long long* out) {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  *out = t;
+}
+
 struct Batch {
   struct HostJob {
     Volume* v;
@@ -1226,17 +1234,18 @@ struct Batch {
   bool spill = false, prepared = false;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
-  // Per-frame completion times (mr_batch_set_timing): an event before the
-  // first launch and one after each wave's network.
+  // Per-frame completion times (mr_batch_set_timing): one-thread kernels
+  // write the device's global nanosecond timer before the first launch
+  // (slot 0) and after each wave's network (slot 1 + wave). Kernel nodes
+  // behave the same in a captured graph as on a stream.
   bool timing = false;
-  cudaEvent_t t_start = nullptr;
-  std::vector<cudaEvent_t> t_wave;
+  unsigned long long* d_stamps = nullptr;
+  size_t n_stamps = 0;
 
   void drop_events() {
-    if (t_start) cudaEventDestroy(t_start);
-    for (cudaEvent_t e : t_wave) cudaEventDestroy(e);
-    t_start = nullptr;
-    t_wave.clear();
+    if (d_stamps) cudaFree(d_stamps);
+    d_stamps = nullptr;
+    n_stamps = 0;
   }
   void drop_graph() {
     if (exec) cudaGraphExecDestroy(exec);
@@ -1278,10 +1287,11 @@ static int batch_launches(Batch& b, const Network* net, cudaStream_t s) {
   const bool tc = b.precision != MR_PREC_FP32;
   const bool hw = b.sampler == MR_SAMPLER_TEXTURE;
   const int nj = (int)b.jobs.size();
-  const bool timed = b.timing && b.t_start && (long long)b.t_wave.size() * b.wave >= b.total;
-  // external records: under stream capture they become event-record nodes of
-  // the graph, so the events are recorded on every launch of it
-  if (timed) MR_CUDA(cudaEventRecordWithFlags(b.t_start, s, cudaEventRecordExternal));
+  const bool timed = b.timing && b.d_stamps && (long long)(b.n_stamps - 1) * b.wave >= b.total;
+  if (timed) {
+    k_stamp<<<1, 1, 0, s>>>(b.d_stamps);
+    MR_CUDA(cudaGetLastError());
+  }
   MR_CUDA(cudaMemsetAsync(b.counters, 0, kCounters * sizeof(unsigned long long), s));
   // the jobs' per-point tables, for the network given to this call
   if (hw)
@@ -1313,7 +1323,10 @@ static int batch_launches(Batch& b, const Network* net, cudaStream_t s) {
                            f3(1, 1, 1), f3(1, 1, 1), s, rec.job, b.d_out, desc, 4, 4 * ccap, desc + 48 * 4 * ccap, 4,
                            4 * ccap);
     if (rc) return rc;
-    if (timed) MR_CUDA(cudaEventRecordWithFlags(b.t_wave[(size_t)(w0 / b.wave)], s, cudaEventRecordExternal));
+    if (timed) {
+      k_stamp<<<1, 1, 0, s>>>(b.d_stamps + 1 + w0 / b.wave);
+      MR_CUDA(cudaGetLastError());
+    }
   }
   k_batch_advance<<<(nj + 127) / 128, 128, 0, s>>>(b.d_jobs, nj);
   MR_CUDA(cudaGetLastError());
@@ -1560,9 +1573,9 @@ extern "C" int mr_batch_set_timing(mr_batch* h, int32_t enable) {
   b.timing = enable != 0;
   if (!b.timing) return MR_OK;
   const size_t waves = (size_t)((b.total + b.wave - 1) / b.wave);
-  MR_CUDA(cudaEventCreate(&b.t_start));
-  b.t_wave.assign(waves, nullptr);
-  for (size_t k = 0; k < waves; ++k) MR_CUDA(cudaEventCreate(&b.t_wave[k]));
+  MR_CUDA(cudaMalloc(&b.d_stamps, (waves + 1) * sizeof(unsigned long long)));
+  MR_CUDA(cudaMemset(b.d_stamps, 0, (waves + 1) * sizeof(unsigned long long)));
+  b.n_stamps = waves + 1;
   return MR_OK;
 }
 
@@ -1570,14 +1583,17 @@ extern "C" int mr_batch_frame_times(mr_batch* h, float* host_ms, int32_t n) {
   clear_error();
   if (!h || !host_ms) return set_error(MR_ERR_ARG, "mr_batch_frame_times: NULL argument");
   Batch& b = h->b;
-  if (!b.timing || !b.t_start || b.t_wave.empty()) return set_error(MR_ERR_STATE, "mr_batch_set_timing(1) first");
+  if (!b.timing || !b.d_stamps) return set_error(MR_ERR_STATE, "mr_batch_set_timing(1) first");
   if (n != (int32_t)b.jobs.size()) return set_error(MR_ERR_ARG, "%d jobs, %d slots", (int)b.jobs.size(), n);
-  MR_CUDA(cudaEventSynchronize(b.t_wave.back()));
+  MR_CUDA(cudaDeviceSynchronize());
+  std::vector<unsigned long long> st(b.n_stamps);
+  MR_CUDA(cudaMemcpy(st.data(), b.d_stamps, st.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  if (st[0] == 0) return set_error(MR_ERR_STATE, "no batch frame has run since mr_batch_set_timing");
   long long pix = 0;
   for (int j = 0; j < n; ++j) {
     pix += (long long)b.jobs[j].p.width * b.jobs[j].p.height;
     const size_t w = (size_t)((pix - 1) / b.wave);  // the wave holding the job's last pixel
-    MR_CUDA(cudaEventElapsedTime(&host_ms[j], b.t_start, b.t_wave[w]));
+    host_ms[j] = (float)((double)(long long)(st[1 + w] - st[0]) * 1e-6);
   }
   return MR_OK;
 }

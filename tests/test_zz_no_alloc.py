@@ -25,13 +25,17 @@ def _setup():
     return torch, v
 
 
-@pytest.mark.parametrize("width,height", [(128, 128), (100, 37)])
+@pytest.mark.parametrize("width,height,albedo", [(128, 128, None), (100, 37, None), (96, 64, (0.9, 0.95, 0.99))])
 @pytest.mark.parametrize("precision", [0, 1])  # MR_PREC_FP32, MR_PREC_BF16
-def test_noalloc_matches_render_twice(width, height, precision):
+def test_noalloc_matches_render_twice(width, height, albedo, precision):
+    """albedo: three distinct channels, one network head each; the tensor-core
+    network then spills the head inputs into the scratch's spill columns."""
     from internship_b200 import _lib, scenes
     torch, v = _setup()
     L = _lib.load()
     p = scenes.make_params(width, height, 1, rt=_lib.RT_MRPNN, precision=precision)
+    if albedo is not None:
+        p.scatter_rate.x, p.scatter_rate.y, p.scatter_rate.z = albedo
     n = width * height * 3
     ref = torch.empty(n, device="cuda")
     out = torch.full((n,), -1.0, device="cuda")
