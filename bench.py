@@ -505,6 +505,8 @@ def main():
     ap.add_argument("--no-rmse", action="store_true", help="skip the matched-RMSE comparison")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-serving measurement")
     ap.add_argument("--no-train", action="store_true", help="skip the reduced training run")
+    ap.add_argument("--no-probe", action="store_true",
+                    help="skip the L2 / HBM read probe (its 4 GiB buffer) and the delta-tracking leg: profiler runs")
     ap.add_argument("--frame", default=None,
                     help="WxH instead of 1920x1080: a smaller case for profiler captures, not a bench line")
     args = ap.parse_args()
@@ -639,7 +641,7 @@ def main():
     serial_fps = replicas.throughput(args.steps, world, serial_ms)
 
     hbm, bf16, src = peaks()
-    probe = memory_probe()
+    probe = memory_probe() if not args.no_probe else {"l2_read_gbs": float("nan"), "skipped": True}
     l2 = probe["l2_read_gbs"]
     trace_ms, gather_ms, mlp_ms32 = head["stage"][1], head["stage"][2], head["stage"][6]
     # algorithmic bytes: trace = density fetches x 32 B (8 fp32 texels);
@@ -704,7 +706,7 @@ def main():
             "density_fetches_per_frame": fetches,
             "variants": variants,
             "memory_probe": probe}
-    if world == 1:
+    if world == 1 and not args.no_probe:
         line["delta_tracking"] = gpu_delta_tracking(l2)
     if not args.no_batch and world == 1:
         line["batched"] = batched_serving()

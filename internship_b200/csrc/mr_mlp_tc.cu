@@ -689,6 +689,21 @@ __device__ __forceinline__ float head_input_spilled(GroupCtx& c, const float* __
   return 1.0f / s;
 }
 
+// L2 prefetch of descriptor features [f0, f1) of the three branches for the
+// rows of tile `tile`, when a chunk's rows are contiguous (chunk-of-4
+// feature-major columns: row stride 4 floats): one bulk prefetch of up to
+// 2 KB per chunk, thread t of the group issuing chunk t. The trunk's per-row
+// code reads each block's features a few MMA rounds later.
+__device__ __forceinline__ void tile_prefetch(const TcArgs& a, int tile, int n, int t, int f0, int f1) {
+  const int row0 = tile * 128, per = (f1 - f0) / 4;
+  if (a.rs != 4 || row0 >= n || t >= 3 * per) return;
+  const int chunk = (t / per) * 48 + f0 / 4 + t % per;
+  const unsigned bytes = (unsigned)min(128, n - row0) * 16u;
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a.desc + (long long)chunk * a.cs + row0 * 4ll),
+               "r"(bytes)
+               : "memory");
+}
+
 // Group-wide OR of a per-row flag (named barrier g+1 with reduction).
 __device__ __forceinline__ bool group_any(int g, bool x) {
   uint32_t r;
@@ -762,6 +777,8 @@ __global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(const __grid_consta
     const float* winv = a.winv;
 
     // light-direction trunk (:424-437): blocks at 160, 168, 176, 184
+    if (it == 0) tile_prefetch(a, tile, n, t, 160, 192);  // later tiles: prefetched during the previous head
+    tile_prefetch(a, tile, n, t, 0, 16);
     block_prep<8>(d, w, 160, 24, ROFF(LDSE01W), ROFF(LDSE02W), gg, gamma, fin, gate);
     store_first<F8, 8>(c, d, 160, gate, ainv);
     issue_trunk<F8, 8>(c, TC_DI + 0);
@@ -800,6 +817,7 @@ __global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(const __grid_consta
     // main trunk (:396-421)
     store_first<F8, 8>(c, d, 0, gate, ainv);
     issue_trunk<F8, 8>(c, TC_MAIN + 0);
+    tile_prefetch(a, tile, n, t, 16, 64);
     block_prep<8>(d, w, 8, 3, ROFF(LSE11W), ROFF(LSE12W), gg, gamma, fin, gate);
     mma_wait(c);
     block_epi<F8, 8, 0, 0>(c, d, w, TC_MAIN + 0, 0, 8, gate, ainv, winv);
@@ -808,6 +826,7 @@ __global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(const __grid_consta
     mma_wait(c);
     block_epi<F8, 8, 2, 0>(c, d, w, TC_MAIN + 3, 8, 16, gate, ainv, winv);
     issue_trunk<F8, 16>(c, TC_MAIN + 6);
+    tile_prefetch(a, tile, n, t, 64, 128);
     block_prep<16>(d, w, 32, 9, ROFF(LSE31W), ROFF(LSE32W), gg, gamma, fin, gate);
     mma_wait(c);
     block_epi<F8, 16, 1, 0>(c, d, w, TC_MAIN + 6, 16, 32, gate, ainv, winv);
@@ -820,6 +839,7 @@ __global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(const __grid_consta
     mma_wait(c);
     block_epi<F8, 16, 2, 0>(c, d, w, TC_MAIN + 12, 48, 64, gate, ainv, winv);
     issue_trunk<F8, 32>(c, TC_MAIN + 15);
+    tile_prefetch(a, tile, n, t, 128, 160);
     block_prep<32>(d, w, 96, 18, ROFF(LSE61W), ROFF(LSE62W), gg, gamma, fin, gate);
     mma_wait(c);
     block_epi<F8, 32, 1, 0>(c, d, w, TC_MAIN + 15, 64, 96, gate, ainv, winv);
@@ -831,6 +851,7 @@ __global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(const __grid_consta
     mma_wait(c);
     block_epi<F8, 32, 1, 1>(c, d, w, TC_MAIN + 21, 128, 0, nullptr, ainv, winv);
     issue_trunk<F8, 32>(c, TC_L81);
+    tile_prefetch(a, tile + (int)gridDim.x * kGroups, n, t, 160, 192);  // the group's next tile
     // channel-0 head gates while L81 runs (fin is complete)
     float x8[8], sep[6];
     head_gates(w, fin, gg, gamma, srp[0], x8, sep);

@@ -25,70 +25,41 @@ struct DTArgs {
   double* sumsq64;                  // W*H*3 (nullable)
 };
 
-// Per-pixel sums of one finished path's radiance (clamped at 0).
-__device__ __forceinline__ void add_path(const DTArgs& a, unsigned pix, F3 L) {
-  L = vmax(L, f3(0, 0, 0));
-  size_t o = (size_t)pix * 3;
-  if (a.sum32) {
-    atomicAdd(a.sum32 + o, L.x);
-    atomicAdd(a.sum32 + o + 1, L.y);
-    atomicAdd(a.sum32 + o + 2, L.z);
-  }
-  if (a.sum64) {
-    atomicAdd(a.sum64 + o, (double)L.x);
-    atomicAdd(a.sum64 + o + 1, (double)L.y);
-    atomicAdd(a.sum64 + o + 2, (double)L.z);
-  }
-  if (a.sumsq64) {
-    atomicAdd(a.sumsq64 + o, (double)L.x * L.x);
-    atomicAdd(a.sumsq64 + o + 1, (double)L.y * L.y);
-    atomicAdd(a.sumsq64 + o + 2, (double)L.z * L.z);
-  }
-}
-
-// Each iteration of the outer loop is one density fetch per lane with a live
-// path: lanes whose path ended (or never entered the volume) first claim and
-// start new work items, then every lane with a path advances it to its next
-// fetch position, whichever phase of the estimator it is in (PathWalk).
 __global__ void __launch_bounds__(128) k_delta_track(DTArgs a) {
   TrackStats st{0, 0};
   unsigned paths = 0;
   const unsigned long long P = (unsigned long long)a.cam.width * a.cam.height;
-  const float smax = a.m.max_density * a.sc.alpha;
-  PathWalk pw;
-  pw.phase = PW_DONE;
-  unsigned pix = 0;
-  bool live = false;
   for (;;) {
-    bool fetch = false;
-    for (;;) {
-      if (!live) {
-        unsigned long long w = claim_work(a.queue);
-        if (w >= a.total) break;
-        // sample-major order: concurrently traced paths are neighbouring pixels.
-        unsigned s = (unsigned)(w / P);
-        pix = (unsigned)(w - (unsigned long long)s * P);
-        int row = pix / a.cam.width, col = pix - row * a.cam.width;
-        pw.rng.init(a.seed, pix, a.sample_offset + s, TAG_PT);
-        float jx = pw.rng.next(), jy = pw.rng.next();
-        F3 dir = normalize(camera_dir(a.cam, row, col, jx, jy));
-        float dis = ray_box_offset(a.cam.ori, dir);
-        ++paths;
-        if (dis < 0) {
-          add_path(a, pix, sky(a.sc, dir));
-          continue;
-        }
-        pw.pos = a.cam.ori + dir * dis;
-        pw.rd = dir;
-        pw.begin(a.sc);
-        live = true;
-      }
-      if (pw.advance(a.sc, smax, a.m.tr_scale, st)) { fetch = true; break; }
-      add_path(a, pix, pw.res);
-      live = false;
+    unsigned long long w = claim_work(a.queue);
+    if (w >= a.total) break;
+    // sample-major order: concurrently traced paths are neighbouring pixels.
+    unsigned s = (unsigned)(w / P);
+    unsigned pix = (unsigned)(w - (unsigned long long)s * P);
+    int row = pix / a.cam.width, col = pix - row * a.cam.width;
+    Rng rng;
+    rng.init(a.seed, pix, a.sample_offset + s, TAG_PT);
+    float jx = rng.next(), jy = rng.next();
+    F3 dir = camera_dir(a.cam, row, col, jx, jy);
+    float t;
+    F3 L = path_radiance(a.m, a.sc, rng, a.cam.ori, dir, &t, st);
+    L = vmax(L, f3(0, 0, 0));
+    ++paths;
+    size_t o = (size_t)pix * 3;
+    if (a.sum32) {
+      atomicAdd(a.sum32 + o, L.x);
+      atomicAdd(a.sum32 + o + 1, L.y);
+      atomicAdd(a.sum32 + o + 2, L.z);
     }
-    if (!fetch) break;
-    pw.consume(a.sc, fetch_density(a.m, pw.q, st), smax, st);
+    if (a.sum64) {
+      atomicAdd(a.sum64 + o, (double)L.x);
+      atomicAdd(a.sum64 + o + 1, (double)L.y);
+      atomicAdd(a.sum64 + o + 2, (double)L.z);
+    }
+    if (a.sumsq64) {
+      atomicAdd(a.sumsq64 + o, (double)L.x * L.x);
+      atomicAdd(a.sumsq64 + o + 1, (double)L.y * L.y);
+      atomicAdd(a.sumsq64 + o + 2, (double)L.z * L.z);
+    }
   }
   // one atomic per warp for the statistics
   unsigned f = st.fetches, c = st.caps, p = paths;

@@ -158,99 +158,6 @@ __device__ __forceinline__ F3 path_radiance(const Medium& m, const PathScene& sc
   return res;
 }
 
-// path_radiance split at its density fetches. A lane's path is a state
-// machine (free flight, ratio tracking, delta tracking, done) that advance()
-// runs up to its next fetch position; the caller fetches and consume() applies
-// the fetched density. A loop of "advance, fetch, consume" therefore issues one
-// fetch per lane per iteration, whichever phase each lane is in, where the
-// nested loops of path_radiance serialise a warp's lanes phase by phase.
-// Each path draws the same random numbers in the same order as
-// path_radiance (the acceptance draw of a delta-tracking step in Tr comes
-// before its fetch here, after it there; the fetch draws nothing), so its
-// radiance is the same bit for bit.
-enum { PW_FLIGHT = 0, PW_RATIO = 1, PW_DELTA = 2, PW_DONE = 3 };
-struct PathWalk {
-  Rng rng;
-  F3 pos, rd, nd, rate, res, q;
-  float t, dis, tr, ph, rk;
-  int loop, bounce, phase;
-
-  // first vertex search of a bounce (the start of DeterminateNextVertex)
-  __device__ __forceinline__ void begin_flight() {
-    dis = ray_box_distance(pos, rd);
-    t = 0;
-    loop = 0;
-    phase = PW_FLIGHT;
-  }
-  // path start at the volume entry pos, direction rd
-  __device__ __forceinline__ void begin(const PathScene& sc) {
-    rate = f3(1, 1, 1);
-    res = f3(0, 0, 0);
-    bounce = 0;
-    if (sc.max_bounces > 0) begin_flight();
-    else phase = PW_DONE;
-  }
-  // a collision (or the step cap): new direction, NEE set-up (Tr from the
-  // vertex towards the light)
-  __device__ __forceinline__ void vertex(const PathScene& sc) {
-    float e0 = rng.next();
-    float e1 = rng.next();
-    nd = hg_sample_dir(e0, e1, rd, sc.g);
-    pos = (rd * t) + pos;
-    rate = rate * sc.scatter;
-    dis = ray_box_distance(pos, sc.L);
-    ph = hg_phase(dot(rd, sc.L), sc.g);
-    tr = 1;
-    t = 0;
-    loop = 0;
-    phase = PW_RATIO;
-  }
-  __device__ __forceinline__ void end_tr(const PathScene& sc, TrackStats& st) {
-    if (loop > 10000) ++st.caps;
-    res = res + (sc.light_color * rate) * (tr * ph);
-    rd = nd;
-    if (++bounce < sc.max_bounces) begin_flight();
-    else phase = PW_DONE;
-  }
-  // Runs the path to its next fetch (true, position q) or to its end (false).
-  __device__ __forceinline__ bool advance(const PathScene& sc, float smax, float trs, TrackStats& st) {
-    for (;;) {
-      if (phase == PW_DONE) return false;
-      const bool flight = phase == PW_FLIGHT;
-      if (!(loop++ < 10000 && (flight || tr > (phase == PW_RATIO ? 0.5f : 0.001f)))) {
-        if (flight) { ++st.caps; vertex(sc); }
-        else if (phase == PW_RATIO) phase = PW_DELTA;
-        else end_tr(sc, st);
-        continue;
-      }
-      float u = rng.next();
-      t -= logf(1 - u) / smax * (flight ? 1.0f : trs);
-      if (t > dis) {
-        if (flight) { res = res + sky(sc, rd) * rate; phase = PW_DONE; return false; }
-        if (phase == PW_RATIO) phase = PW_DELTA;
-        else end_tr(sc, st);
-        continue;
-      }
-      if (phase != PW_RATIO) rk = rng.next();
-      q = (flight ? rd : sc.L) * t + pos;
-      return true;
-    }
-  }
-  __device__ __forceinline__ void consume(const PathScene& sc, float d, float smax, TrackStats& st) {
-    float s = d * sc.alpha;
-    if (phase == PW_FLIGHT) {
-      if (s / smax > rk) { vertex(sc); return; }
-    } else if (phase == PW_RATIO) {
-      tr *= 1 - fmaxf(0.0f, s / smax);
-    } else if (rk < fmaxf(0.0f, s / smax)) {
-      tr = 0;
-      end_tr(sc, st);
-      return;
-    }
-    if (d < 0) t -= d;
-  }
-};
-
 struct CameraModel {
   F3 ori, fwd, up, right;
   int width, height;
