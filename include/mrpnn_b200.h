@@ -297,7 +297,11 @@ int mr_network_check(const mr_network* net, int32_t reset);
  *    streams or threads on one device) race on it and must be serialised by
  *    the caller;
  *  - the first call on a device looks the scratch address up (and may load
- *    the module there), so make it before any stream capture.
+ *    the module there), so make it before any stream capture;
+ *  - the array belongs to the module of every neural-render kernel: loading
+ *    that module on a device (any neural render there) holds its
+ *    MR_NOALLOC_SCRATCH_MIB MiB of device memory for the life of the process,
+ *    whether or not this entry point is ever called.
  * Stage timing (mr_volume_set_timing) does not cover this call. */
 #define MR_NOALLOC_MAX_PIXELS 16384
 #define MR_NOALLOC_SCRATCH_MIB 45

@@ -178,7 +178,7 @@ __device__ __forceinline__ float compare(const float* cb, float cn, const float*
     if (hx != 0.0f || hy != 0.0f) {
       p += 1.0f;
       const float t = syx * hx - sxy * hy;
-      res += t * t / (hx + hy);
+      res += __fdividef(t * t, hx + hy);  // hx + hy > 0 here; 2-ulp division (121 x 30 per pixel)
     }
   }
   return p == 0.0f ? 0.0f : res / p;
@@ -251,6 +251,7 @@ __global__ void __launch_bounds__(256) k_denoise(DenoiseArgs a) {
       res = f3(0, 0, 0);
       float ws = 0.0f;
       for (int dr = -kHalo; dr <= kHalo; ++dr)
+#pragma unroll
         for (int dc = -kHalo; dc <= kHalo; ++dc) {
           // the staged halo is already clamped, as UnRoll clamps
           const float* nh = sh + (li + dr * kSpan + dc) * kHistFloats;

@@ -112,6 +112,7 @@ struct Network {
   size_t packed_bytes = 0;
   std::vector<float> h_rowwise;  // fp32 per-row weights passed as kernel parameters (mr_mlp_tc.cu)
   std::vector<float> h_winv8;    // inverse per-layer scales of the E4M3 weight image
+  std::vector<float> h_se;       // per-block squeeze-excitation records of the tensor-core trunk (mr_mlp_tc.cu)
   float* simt_img = nullptr;     // weight image of the fp32 network kernels (simt_weight_image)
   std::vector<float> h_tail;     // LXW .. LX12B, kernel parameters of the fp32 head's tail (mr_mlp_simt.cu)
   std::vector<float> h_light;    // kernel parameters of the fp32 light-direction trunk (mr_mlp_simt.cu)

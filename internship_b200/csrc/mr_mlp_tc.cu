@@ -56,18 +56,14 @@ constexpr int tc_offset(int i) { int o = 0; for (int j = 0; j < i; ++j) o += tc_
 constexpr int kWBytes = tc_offset(kTcLayers);
 static_assert(kWBytes == 100352, "packed weight image size");
 
-// fp32 arrays read by the per-row code (squeeze-excitation, SEFin, LGGS,
-// LX12 and the biases of the MMA layers), compacted into an image that is
+// fp32 arrays read by the per-row code of the head (SEFin, LGGS, LX12) and
+// the biases of the MMA layers, compacted into an image that is
 // passed in the kernel's parameter space: uniform constant-bank operands
 // instead of one load instruction per weight and row.
 constexpr bool rowwise_used(int id) {
   for (int i = 0; i < kTcLayers; ++i)
     if (kTc[i].b == id) return true;
-  constexpr int ids[] = {MR_W_LSEFin1W, MR_W_LSEFin2W, MR_W_LGGSW, MR_W_LGGSB, MR_W_LX12W, MR_W_LX12B,
-                         MR_W_LSE01W, MR_W_LSE02W, MR_W_LSE11W, MR_W_LSE12W, MR_W_LSE21W, MR_W_LSE22W,
-                         MR_W_LSE31W, MR_W_LSE32W, MR_W_LSE41W, MR_W_LSE42W, MR_W_LSE51W, MR_W_LSE52W,
-                         MR_W_LSE61W, MR_W_LSE62W, MR_W_LSE71W, MR_W_LSE72W, MR_W_LDSE01W, MR_W_LDSE02W,
-                         MR_W_LDSE11W, MR_W_LDSE12W, MR_W_LDSE21W, MR_W_LDSE22W, MR_W_LDSE31W, MR_W_LDSE32W};
+  constexpr int ids[] = {MR_W_LSEFin1W, MR_W_LSEFin2W, MR_W_LGGSW, MR_W_LGGSB, MR_W_LX12W, MR_W_LX12B};
   for (int x : ids)
     if (x == id) return true;
   return false;
@@ -79,7 +75,7 @@ constexpr RowTable make_row_table() {
   int o = 0;
   for (int i = 0; i < MR_W_COUNT; ++i) {
     t.off[i] = rowwise_used(i) ? o : -1;
-    if (rowwise_used(i)) o += wt.size[i];
+    if (rowwise_used(i)) o += (wt.size[i] + 3) / 4 * 4;  // every array 16-byte aligned: float4 reads
   }
   t.total = o;
   return t;
@@ -91,6 +87,20 @@ struct ROff {
   static_assert(value >= 0, "weight array not in the row-wise image");
 };
 #define ROFF(name) (::mr::ROff<MR_W_##name>::value)
+
+// Squeeze-excitation record of each trunk block (its gates and LSEFin1 terms,
+// radiancePredict.cu:240-294), 192 floats read as float4 kernel parameters:
+// [16 x (LSEFin1 weights of the block's 3 means, then its 3 maxima)],
+// [SE1 8 x 8], [SE2 3 x 8], zero padding. Order of the records: the light
+// trunk's blocks 0..3, then the main trunk's blocks 0..7.
+constexpr int kSeRecFloats = 192, kSeRecs = 12;
+struct SeRecSrc { int pid, se1, se2; };
+constexpr SeRecSrc kSeRecSrc[kSeRecs] = {
+    {24, MR_W_LDSE01W, MR_W_LDSE02W}, {27, MR_W_LDSE11W, MR_W_LDSE12W}, {30, MR_W_LDSE21W, MR_W_LDSE22W},
+    {33, MR_W_LDSE31W, MR_W_LDSE32W}, {0, MR_W_LSE01W, MR_W_LSE02W},    {3, MR_W_LSE11W, MR_W_LSE12W},
+    {6, MR_W_LSE21W, MR_W_LSE22W},    {9, MR_W_LSE31W, MR_W_LSE32W},    {12, MR_W_LSE41W, MR_W_LSE42W},
+    {15, MR_W_LSE51W, MR_W_LSE52W},   {18, MR_W_LSE61W, MR_W_LSE62W},   {21, MR_W_LSE71W, MR_W_LSE72W},
+};
 
 // E4M3 image: rows of K padded to a multiple of 32 one-byte elements (the
 // K of one f8f6f4 MMA), N padded to 16.
@@ -308,8 +318,11 @@ struct TcArgs {
   int* err;                           // set on a wait timeout
   const uint8_t* __restrict__ wpack8; // kW8Bytes packed E4M3 image (MR_PREC_FP8)
   float winv[kTcLayers];              // inverse per-layer weight scales (1 for BF16)
-  float rw[kRowFloats];               // row-wise fp32 weights (make_row_table)
+  float4 se[kSeRecs * kSeRecFloats / 4];  // squeeze-excitation records (kSeRecSrc)
+  alignas(16) float rw[kRowFloats];   // row-wise fp32 weights (make_row_table)
 };
+
+static_assert(sizeof(TcArgs) <= 32764, "kernel parameter space");
 
 // One descriptor row in chunk-of-4 order: features i..i+3 (i a multiple of
 // 4) are the float4 at p + (i/4)*cs, cs = 4*capacity for the render path's
@@ -426,8 +439,8 @@ constexpr int kBr = 128 * 32 * 2;  // bytes of one branch tile (K <= 32)
 // Depends only on the descriptor, g and gamma, so it runs while the previous
 // layer's MMA is in flight.
 template <int S>
-__device__ __forceinline__ void block_prep(const DIn& d, const float* __restrict__ w, int from, int pid, int sew0,
-                                           int sew1, float g, float gamma, float* fin, float* gate) {
+__device__ __forceinline__ void block_prep(const DIn& d, const float4* __restrict__ rec, int from, float g, float gamma,
+                                           float* fin, float* gate) {
   float mean[3], mx[3];
 #pragma unroll
   for (int br = 0; br < 3; ++br) {
@@ -441,31 +454,40 @@ __device__ __forceinline__ void block_prep(const DIn& d, const float* __restrict
     mean[br] = s / (float)S;
     mx[br] = m;
   }
-  const float* f1 = w + ROFF(LSEFin1W);
+  // LSEFin1 terms: per output j the weights of (mean b0..b2, max b0..b2)
 #pragma unroll
-  for (int j = 0; j < 16; ++j) {
-    float a = fin[j];
+  for (int j = 0; j < 16; j += 2) {
+    const float4 q0 = rec[3 * (j / 2)], q1 = rec[3 * (j / 2) + 1], q2 = rec[3 * (j / 2) + 2];
+    const float wa[12] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w};
 #pragma unroll
-    for (int br = 0; br < 3; ++br) {
-      a += mean[br] * ldw(f1 + j * 75 + pid + br);
-      a += mx[br] * ldw(f1 + j * 75 + 36 + pid + br);
+    for (int u = 0; u < 2; ++u) {
+      float a = fin[j + u];
+#pragma unroll
+      for (int br = 0; br < 3; ++br) {
+        a += mean[br] * wa[6 * u + br];
+        a += mx[br] * wa[6 * u + 3 + br];
+      }
+      fin[j + u] = a;
     }
-    fin[j] = a;
   }
   const float tmp[8] = {mean[0], mean[1], mean[2], mx[0], mx[1], mx[2], g, gamma};
   float h[8];
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
+    const float4 q0 = rec[24 + 2 * i], q1 = rec[25 + 2 * i];
+    const float wr[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
     float a = 0.0f;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) a += tmp[j] * ldw(w + sew0 + j + i * 8);
+    for (int j = 0; j < 8; ++j) a += tmp[j] * wr[j];
     h[i] = a >= 0.0f ? a : 0.0f;
   }
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
+    const float4 q0 = rec[40 + 2 * i], q1 = rec[41 + 2 * i];
+    const float wr[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
     float a = 0.0f;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) a += h[j] * ldw(w + sew1 + j + i * 8);
+    for (int j = 0; j < 8; ++j) a += h[j] * wr[j];
     gate[i] = sigm(a);
   }
 }
@@ -492,16 +514,16 @@ __device__ __forceinline__ void store_first(GroupCtx& c, const DIn& d, int from,
 
 // Epilogue of trunk block (S, MODE) at descriptor offset `from`:
 // yn = ReLU(acc + b); y = yn + seg (ADD3) or [yn, seg] (REP3, MODE 2).
-// NEXT = 0: writes the next block's A rows seg2 * gate2 + y (SERES input,
-// radiancePredict.cu:259-294); NEXT = 1: writes y (input of L81 / LD41).
-template <bool F8, int S, int MODE, int NEXT>
+// next_y false: writes the next block's A rows seg2 * gate2 + y (SERES input,
+// radiancePredict.cu:259-294); true: writes y (input of L81 / LD41).
+template <bool F8, int S, int MODE>
 __device__ __forceinline__ void block_epi(GroupCtx& c, const DIn& d, const float* __restrict__ w, int layer0, int from,
-                                          int from2, const float* gate2, float* ainv, const float* winv) {
+                                          int from2, bool next_y, const float* gate2, float* ainv, const float* winv) {
   constexpr int W = MODE == 2 ? 2 * S : S;
   constexpr int KP = qkp<F8>(W);
 #pragma unroll
   for (int br = 0; br < 3; ++br) {
-    const float* bias = w + kTcBias(layer0 + br);
+    const float4* bias = reinterpret_cast<const float4*>(w + kTcBias(layer0 + br));  // 16-byte aligned
     const float sc = F8 ? ainv[br] * winv[layer0 + br] : 1.0f;
     float y[KP];
 #pragma unroll
@@ -509,10 +531,15 @@ __device__ __forceinline__ void block_epi(GroupCtx& c, const DIn& d, const float
       float v[16];
       tmem_ld16(c.tmem + c.tlane + 32 * br + 16 * h, v);
 #pragma unroll
-      for (int i = 0; i < 16; ++i)
+      for (int i = 0; i < 16; i += 4)
         if (16 * h + i < S) {
-          const float a = v[i] * sc + ldw(bias + 16 * h + i);
-          y[16 * h + i] = a >= 0.0f ? a : 0.0f;
+          const float4 bq = bias[(16 * h + i) / 4];
+          const float bb[4] = {bq.x, bq.y, bq.z, bq.w};
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const float a = v[i + u] * sc + bb[u];
+            y[16 * h + i + u] = a >= 0.0f ? a : 0.0f;
+          }
         }
     }
 #pragma unroll
@@ -527,7 +554,7 @@ __device__ __forceinline__ void block_epi(GroupCtx& c, const DIn& d, const float
     }
 #pragma unroll
     for (int i = W; i < KP; ++i) y[i] = 0.0f;
-    if (NEXT == 0) {
+    if (!next_y) {
 #pragma unroll
       for (int i = 0; i < W; i += 4) {
         const float4 q = d.ld4(br * 192 + from2 + i);
@@ -550,6 +577,71 @@ __device__ __forceinline__ void issue_trunk(GroupCtx& c, int layer0) {
     for (int br = 0; br < 3; ++br)
       issue_q<F8, pad16(S), qkp<F8>(S)>(c.tmem + 32 * br, tb + br * kBr, wb + tc_off<F8>(layer0 + br));
   });
+}
+
+// The trunks as a sequence of MMA rounds (radiancePredict.cu:396-437): round
+// r computes the squeeze-excitation gates of the block it issues (prep),
+// waits for the previous round's MMAs, writes their epilogue as this block's
+// A rows (or, for a trunk's first block, the gated descriptor segment), and
+// issues the block's three branch MMAs. The rounds run from this table in
+// one rolled loop, so that every round executes the same few instantiations
+// (three widths) instead of a straight-line copy per block: the four tile
+// groups of a CTA, each at its own round, then share a small instruction
+// working set.
+enum { TS_FIRST = 0, TS_EPI = 1, TS_LD41 = 2 };
+struct TrunkStep {
+  short prep_from, rec, prep_s;              // prep_s 0: no gates to compute; rec: kSeRecSrc index
+  short kind, epi_layer, epi_s, cat, next_y, from, from2;
+  short layer, s;                            // the block issued
+};
+#define TS_PREP(f, rec, S) f, rec, S
+#define TS_NOPREP 0, 0, 0
+__constant__ TrunkStep c_trunk[14] = {
+    // light-direction trunk: blocks at 160, 168, 176, 184, then LD41
+    {TS_PREP(160, 0, 8), TS_FIRST, 0, 0, 0, 0, 160, 0, TC_DI + 0, 8},
+    {TS_PREP(168, 1, 8), TS_EPI, TC_DI + 0, 8, 0, 0, 160, 168, TC_DI + 3, 8},
+    {TS_PREP(176, 2, 8), TS_EPI, TC_DI + 3, 8, 0, 0, 168, 176, TC_DI + 6, 8},
+    {TS_PREP(184, 3, 8), TS_EPI, TC_DI + 6, 8, 0, 0, 176, 184, TC_DI + 9, 8},
+    {TS_PREP(0, 4, 8), TS_EPI, TC_DI + 9, 8, 0, 1, 184, 0, TC_LD41, 8},
+    // main trunk: LD41 parked in TMEM, then blocks 0..7 and L81
+    {TS_NOPREP, TS_LD41, 0, 0, 0, 0, 0, 0, TC_MAIN + 0, 8},
+    {TS_PREP(8, 5, 8), TS_EPI, TC_MAIN + 0, 8, 0, 0, 0, 8, TC_MAIN + 3, 8},
+    {TS_PREP(16, 6, 16), TS_EPI, TC_MAIN + 3, 8, 1, 0, 8, 16, TC_MAIN + 6, 16},
+    {TS_PREP(32, 7, 16), TS_EPI, TC_MAIN + 6, 16, 0, 0, 16, 32, TC_MAIN + 9, 16},
+    {TS_PREP(48, 8, 16), TS_EPI, TC_MAIN + 9, 16, 0, 0, 32, 48, TC_MAIN + 12, 16},
+    {TS_PREP(64, 9, 32), TS_EPI, TC_MAIN + 12, 16, 1, 0, 48, 64, TC_MAIN + 15, 32},
+    {TS_PREP(96, 10, 32), TS_EPI, TC_MAIN + 15, 32, 0, 0, 64, 96, TC_MAIN + 18, 32},
+    {TS_PREP(128, 11, 32), TS_EPI, TC_MAIN + 18, 32, 0, 0, 96, 128, TC_MAIN + 21, 32},
+    {TS_NOPREP, TS_EPI, TC_MAIN + 21, 32, 0, 1, 128, 0, TC_L81, 32},
+};
+#undef TS_PREP
+#undef TS_NOPREP
+
+__device__ __forceinline__ void prep_any(int S, const DIn& d, const float4* __restrict__ rec, int from, float g,
+                                         float gamma, float* fin, float* gate) {
+  if (S == 8) block_prep<8>(d, rec, from, g, gamma, fin, gate);
+  else if (S == 16) block_prep<16>(d, rec, from, g, gamma, fin, gate);
+  else block_prep<32>(d, rec, from, g, gamma, fin, gate);
+}
+template <bool F8>
+__device__ __forceinline__ void epi_any(int S, bool cat, GroupCtx& c, const DIn& d, const float* __restrict__ w,
+                                        int layer0, int from, int from2, bool next_y, const float* gate2, float* ainv,
+                                        const float* winv) {
+  if (S == 8) {
+    if (cat) block_epi<F8, 8, 2>(c, d, w, layer0, from, from2, next_y, gate2, ainv, winv);
+    else block_epi<F8, 8, 1>(c, d, w, layer0, from, from2, next_y, gate2, ainv, winv);
+  } else if (S == 16) {
+    if (cat) block_epi<F8, 16, 2>(c, d, w, layer0, from, from2, next_y, gate2, ainv, winv);
+    else block_epi<F8, 16, 1>(c, d, w, layer0, from, from2, next_y, gate2, ainv, winv);
+  } else {
+    block_epi<F8, 32, 1>(c, d, w, layer0, from, from2, next_y, gate2, ainv, winv);
+  }
+}
+template <bool F8>
+__device__ __forceinline__ void issue_any(int S, GroupCtx& c, int layer0) {
+  if (S == 8) issue_trunk<F8, 8>(c, layer0);
+  else if (S == 16) issue_trunk<F8, 16>(c, layer0);
+  else issue_trunk<F8, 32>(c, layer0);
 }
 
 // Channel-dependent head gates: LGGS(g, gamma, srp) -> x8 (head columns
@@ -689,21 +781,6 @@ __device__ __forceinline__ float head_input_spilled(GroupCtx& c, const float* __
   return 1.0f / s;
 }
 
-// L2 prefetch of descriptor features [f0, f1) of the three branches for the
-// rows of tile `tile`, when a chunk's rows are contiguous (chunk-of-4
-// feature-major columns: row stride 4 floats): one bulk prefetch of up to
-// 2 KB per chunk, thread t of the group issuing chunk t. The trunk's per-row
-// code reads each block's features a few MMA rounds later.
-__device__ __forceinline__ void tile_prefetch(const TcArgs& a, int tile, int n, int t, int f0, int f1) {
-  const int row0 = tile * 128, per = (f1 - f0) / 4;
-  if (a.rs != 4 || row0 >= n || t >= 3 * per) return;
-  const int chunk = (t / per) * 48 + f0 / 4 + t % per;
-  const unsigned bytes = (unsigned)min(128, n - row0) * 16u;
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a.desc + (long long)chunk * a.cs + row0 * 4ll),
-               "r"(bytes)
-               : "memory");
-}
-
 // Group-wide OR of a per-row flag (named barrier g+1 with reduction).
 __device__ __forceinline__ bool group_any(int g, bool x) {
   uint32_t r;
@@ -776,82 +853,35 @@ __global__ void __launch_bounds__(128 * kGroups, 1) k_mlp_tc(const __grid_consta
     float gate[3], ainv[3];  // ainv: inverse E4M3 row scales of the three branch A rows (1 for BF16)
     const float* winv = a.winv;
 
-    // light-direction trunk (:424-437): blocks at 160, 168, 176, 184
-    if (it == 0) tile_prefetch(a, tile, n, t, 160, 192);  // later tiles: prefetched during the previous head
-    tile_prefetch(a, tile, n, t, 0, 16);
-    block_prep<8>(d, w, 160, 24, ROFF(LDSE01W), ROFF(LDSE02W), gg, gamma, fin, gate);
-    store_first<F8, 8>(c, d, 160, gate, ainv);
-    issue_trunk<F8, 8>(c, TC_DI + 0);
-    block_prep<8>(d, w, 168, 27, ROFF(LDSE11W), ROFF(LDSE12W), gg, gamma, fin, gate);
-    mma_wait(c);
-    block_epi<F8, 8, 0, 0>(c, d, w, TC_DI + 0, 160, 168, gate, ainv, winv);
-    issue_trunk<F8, 8>(c, TC_DI + 3);
-    block_prep<8>(d, w, 176, 30, ROFF(LDSE21W), ROFF(LDSE22W), gg, gamma, fin, gate);
-    mma_wait(c);
-    block_epi<F8, 8, 1, 0>(c, d, w, TC_DI + 3, 168, 176, gate, ainv, winv);
-    issue_trunk<F8, 8>(c, TC_DI + 6);
-    block_prep<8>(d, w, 184, 33, ROFF(LDSE31W), ROFF(LDSE32W), gg, gamma, fin, gate);
-    mma_wait(c);
-    block_epi<F8, 8, 1, 0>(c, d, w, TC_DI + 6, 176, 184, gate, ainv, winv);
-    issue_trunk<F8, 8>(c, TC_DI + 9);
-    block_prep<8>(d, w, 0, 0, ROFF(LSE01W), ROFF(LSE02W), gg, gamma, fin, gate);  // main block 0
-    mma_wait(c);
-    block_epi<F8, 8, 1, 1>(c, d, w, TC_DI + 9, 184, 0, nullptr, ainv, winv);
-    issue_trunk<F8, 8>(c, TC_LD41);
-    mma_wait(c);
-    // LD41 -> comb[96..120), parked in TMEM
+#pragma unroll 1
+    for (int r = 0; r < 14; ++r) {
+      const TrunkStep& st = c_trunk[r];
+      if (st.prep_s) prep_any(st.prep_s, d, a.se + st.rec * (kSeRecFloats / 4), st.prep_from, gg, gamma, fin, gate);
+      if (st.kind != TS_FIRST) mma_wait(c);
+      if (st.kind == TS_EPI) {
+        epi_any<F8>(st.epi_s, st.cat != 0, c, d, w, st.epi_layer, st.from, st.from2, st.next_y != 0, gate, ainv,
+                    winv);
+      } else {
+        if (st.kind == TS_LD41) {
+          // LD41 -> comb[96..120), parked in TMEM
 #pragma unroll
-    for (int br = 0; br < 3; ++br) {
-      float v[8];
-      tmem_ld8(c.tmem + c.tlane + 32 * br, v);
-      const float* bias = w + kTcBias(TC_LD41 + br);
-      const float sc = F8 ? ainv[br] * winv[TC_LD41 + br] : 1.0f;
+          for (int br = 0; br < 3; ++br) {
+            float v[8];
+            tmem_ld8(c.tmem + c.tlane + 32 * br, v);
+            const float* bias = w + kTcBias(TC_LD41 + br);
+            const float sc = F8 ? ainv[br] * winv[TC_LD41 + br] : 1.0f;
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const float x = v[i] * sc + ldw(bias + i);
-        v[i] = x >= 0.0f ? x : 0.0f;
+            for (int i = 0; i < 8; ++i) {
+              const float x = v[i] * sc + ldw(bias + i);
+              v[i] = x >= 0.0f ? x : 0.0f;
+            }
+            tmem_st8(tcomb + 8 * br, v);
+          }
+        }
+        store_first<F8, 8>(c, d, st.from, gate, ainv);  // a trunk's first block: seg * gate
       }
-      tmem_st8(tcomb + 8 * br, v);
+      issue_any<F8>(st.s, c, st.layer);
     }
-
-    // main trunk (:396-421)
-    store_first<F8, 8>(c, d, 0, gate, ainv);
-    issue_trunk<F8, 8>(c, TC_MAIN + 0);
-    tile_prefetch(a, tile, n, t, 16, 64);
-    block_prep<8>(d, w, 8, 3, ROFF(LSE11W), ROFF(LSE12W), gg, gamma, fin, gate);
-    mma_wait(c);
-    block_epi<F8, 8, 0, 0>(c, d, w, TC_MAIN + 0, 0, 8, gate, ainv, winv);
-    issue_trunk<F8, 8>(c, TC_MAIN + 3);
-    block_prep<16>(d, w, 16, 6, ROFF(LSE21W), ROFF(LSE22W), gg, gamma, fin, gate);
-    mma_wait(c);
-    block_epi<F8, 8, 2, 0>(c, d, w, TC_MAIN + 3, 8, 16, gate, ainv, winv);
-    issue_trunk<F8, 16>(c, TC_MAIN + 6);
-    tile_prefetch(a, tile, n, t, 64, 128);
-    block_prep<16>(d, w, 32, 9, ROFF(LSE31W), ROFF(LSE32W), gg, gamma, fin, gate);
-    mma_wait(c);
-    block_epi<F8, 16, 1, 0>(c, d, w, TC_MAIN + 6, 16, 32, gate, ainv, winv);
-    issue_trunk<F8, 16>(c, TC_MAIN + 9);
-    block_prep<16>(d, w, 48, 12, ROFF(LSE41W), ROFF(LSE42W), gg, gamma, fin, gate);
-    mma_wait(c);
-    block_epi<F8, 16, 1, 0>(c, d, w, TC_MAIN + 9, 32, 48, gate, ainv, winv);
-    issue_trunk<F8, 16>(c, TC_MAIN + 12);
-    block_prep<32>(d, w, 64, 15, ROFF(LSE51W), ROFF(LSE52W), gg, gamma, fin, gate);
-    mma_wait(c);
-    block_epi<F8, 16, 2, 0>(c, d, w, TC_MAIN + 12, 48, 64, gate, ainv, winv);
-    issue_trunk<F8, 32>(c, TC_MAIN + 15);
-    tile_prefetch(a, tile, n, t, 128, 160);
-    block_prep<32>(d, w, 96, 18, ROFF(LSE61W), ROFF(LSE62W), gg, gamma, fin, gate);
-    mma_wait(c);
-    block_epi<F8, 32, 1, 0>(c, d, w, TC_MAIN + 15, 64, 96, gate, ainv, winv);
-    issue_trunk<F8, 32>(c, TC_MAIN + 18);
-    block_prep<32>(d, w, 128, 21, ROFF(LSE71W), ROFF(LSE72W), gg, gamma, fin, gate);
-    mma_wait(c);
-    block_epi<F8, 32, 1, 0>(c, d, w, TC_MAIN + 18, 96, 128, gate, ainv, winv);
-    issue_trunk<F8, 32>(c, TC_MAIN + 21);
-    mma_wait(c);
-    block_epi<F8, 32, 1, 1>(c, d, w, TC_MAIN + 21, 128, 0, nullptr, ainv, winv);
-    issue_trunk<F8, 32>(c, TC_L81);
-    tile_prefetch(a, tile + (int)gridDim.x * kGroups, n, t, 160, 192);  // the group's next tile
     // channel-0 head gates while L81 runs (fin is complete)
     float x8[8], sep[6];
     head_gates(w, fin, gg, gamma, srp[0], x8, sep);
@@ -1267,6 +1297,19 @@ int pack_network(Network* n) {
   n->h_rowwise.assign(kRowFloats, 0.0f);
   for (int id = 0; id < MR_W_COUNT; ++id)
     if (rt.off[id] >= 0) std::memcpy(&n->h_rowwise[rt.off[id]], w.data() + wt.off[id], wt.size[id] * sizeof(float));
+  // squeeze-excitation records of the tensor-core trunk
+  n->h_se.assign(kSeRecs * kSeRecFloats, 0.0f);
+  for (int r = 0; r < kSeRecs; ++r) {
+    float* o = &n->h_se[r * kSeRecFloats];
+    const float* f1 = w.data() + wt.off[MR_W_LSEFin1W];
+    for (int j = 0; j < 16; ++j)
+      for (int b = 0; b < 3; ++b) {
+        o[6 * j + b] = f1[j * 75 + kSeRecSrc[r].pid + b];
+        o[6 * j + 3 + b] = f1[j * 75 + 36 + kSeRecSrc[r].pid + b];
+      }
+    std::memcpy(o + 96, w.data() + wt.off[kSeRecSrc[r].se1], 64 * sizeof(float));
+    std::memcpy(o + 160, w.data() + wt.off[kSeRecSrc[r].se2], 24 * sizeof(float));
+  }
   // weight image of the fp32 kernels
   {
     std::vector<float> si;
@@ -1335,6 +1378,8 @@ int launch_mlp_tc(const Network* net, const float* desc, const float* aux, long 
   a.bout = bout;
   if (net->h_rowwise.size() != (size_t)kRowFloats) return set_error(MR_ERR_STATE, "network not packed");
   std::memcpy(a.rw, net->h_rowwise.data(), sizeof(a.rw));
+  if (net->h_se.size() * sizeof(float) != sizeof(a.se)) return set_error(MR_ERR_STATE, "network not packed");
+  std::memcpy(a.se, net->h_se.data(), sizeof(a.se));
   a.wpack8 = (const uint8_t*)net->packed + kWBytes + 256;
   for (int i = 0; i < kTcLayers; ++i) a.winv[i] = f8 ? net->h_winv8[i] : 1.0f;
   a.err = (int*)((uint8_t*)net->packed + kWBytes);
