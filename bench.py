@@ -93,7 +93,7 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle samples every 200 ms during the timed region."""
+    """nvidia-smi clock/throttle samples every 50 ms during the timed legs."""
 
     def __init__(self, index):
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
@@ -102,7 +102,7 @@ class ClockSampler:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + q,
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits", "-lms", "50"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
@@ -182,14 +182,18 @@ TRAINED = os.path.join(ROOT, "internship_b200", "data", "mrpnn_trained.npy")
 # k_tc32_head + k_tc32_tail),
 # per density fetch for the trace. A launch's traffic = this figure x the
 # launch's units.
-TRAFFIC_PER_UNIT = {"k_simt": 3356.7, "k_mlp_tc": 2542.6, "k_gather_fm_exact": 2490.3,
-                    "k_gather_fm_texture": 2447.0, "k_nn_trace": 137.2}
+TRAFFIC_PER_UNIT = {"k_simt": 3356.7, "k_simt_trunk": 2092.4, "k_mlp_tc": 2456.3, "k_gather_fm_exact": 2490.3,
+                    "k_gather_fm_texture": 2447.0, "k_nn_trace": 52.56}
+# k_nn_trace: dram__bytes_read + write of one launch of the 1080p bench frame
+# (759.9 MB for 14.46 M density fetches); the others at 960x540 per active pixel.
 SIMT_KERNELS = ("k_simt_trunk + k_light_trunk + k_tc32_head + k_tc32_tail (fp32 network: CUDA-core trunks, "
                 "tcgen05 head with fp32-accurate three-term TF32 products, CUDA-core tail)")
 # The library's kernels of one fp32 / exact-sampler frame, in launch order
 # (as an ncu launch list of this command shows them).
 FP32_FRAME_KERNELS = ("k_sphere_h0", "k_nn_trace", "k_gather_fm", "k_simt_trunk", "k_light_trunk", "k_tc32_head",
                       "k_tc32_tail")
+# algorithmic FLOPs per active pixel of the fp32 main-trunk kernel (blocks 0..7 and L81)
+TRUNK_FLOP_PER_PIXEL = 32.9e3
 # fp32 FMA rate of the CUDA cores (148 SMs x 128 lanes x 2 FLOP x 1.965 GHz), nominal
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
@@ -382,7 +386,7 @@ def batched_serving(replays=10, seed=11):
             "frame_latency_ms": {"p50": float(np.percentile(np.concatenate(frame_ms), 50)),
                                  "p99": float(np.percentile(np.concatenate(frame_ms), 99)),
                                  "definition": "from the batch frame's start to the completion of the wave holding "
-                                               "the frame's last pixel (events in the captured graph)"}
+                                               "the frame's last pixel (device-timer stamps in the captured graph)"}
             if frame_ms else {"unavailable": frame_err},
             "autotuned": {"wave_pixels": int(wave.value), "trace_block": int(tb.value), "gather_block": int(gb.value)},
             "replays": replays, "graph": "one CUDA graph per batch frame", "setup_s": t_setup}
@@ -641,9 +645,10 @@ def main():
                 "active": int(cnt[3]), "fetches": int(cnt[0])}
 
     # fp32 network, exact sampler: the headline configuration
+    # clocks sampled over all the timed legs below (nvidia-smi needs a moment to start)
     clocks = ClockSampler(torch.cuda.current_device())
+    time.sleep(0.5)
     head = leg(_lib.PREC_FP32, _lib.SAMPLER_EXACT, 0)
-    clk = clocks.stop()
     ms, active, fetches = head["ms"], head["active"], head["fetches"]
     fps = replicas.throughput(args.steps, world, ms)
     # the same frames with texture-unit sampling and with the BF16 tensor-core network
@@ -652,6 +657,7 @@ def main():
             "bf16_texture": leg(_lib.PREC_BF16, _lib.SAMPLER_TEXTURE, 3000),
             "fp8_texture": leg(_lib.PREC_FP8, _lib.SAMPLER_TEXTURE, 4000)}
     p.precision, p.sampler = _lib.PREC_FP32, _lib.SAMPLER_EXACT
+    clk = clocks.stop()
 
     # -- end to end through the public API, frames delivered to pinned host
     # memory: mr_render_host_async renders frame k+1 while frame k's copy runs
@@ -715,8 +721,25 @@ def main():
     stages["nn_network"]["frac_of_fp32_fma_peak"] = stages["nn_network"]["achieved"] / FP32_PEAK_TFLOPS
     for s_ in stages.values():
         s_["traffic_source"] = "ncu dram__bytes_read+write per unit at 960x540, scaled by this launch's units"
-    dom = max(stages, key=lambda k: stages[k]["ms"])
-    roofline = dict(stages[dom], stage=dom)
+    stages["nn_trace"]["traffic_source"] = ("ncu dram__bytes_read+write of one 1080p launch (52.56 B per fetch), "
+                                            "scaled by this launch's fetches")
+    # the dominant single kernel of the frame: the trace, the gather, or the
+    # largest of the network's four kernels (the main trunk, timed on its own
+    # as library stage 7)
+    trunk_ms = head["stage"][7]
+    kernels = {"k_nn_trace": dict(stages["nn_trace"], stage="nn_trace"),
+               "k_gather_fm": dict(stages["nn_gather"], stage="nn_gather"),
+               "k_simt_trunk": {"bound": "fp32", "kernel": "k_simt_trunk (fp32 main trunk on the CUDA cores)",
+                                "ms": trunk_ms,
+                                "achieved": TRUNK_FLOP_PER_PIXEL * active / (trunk_ms / 1e3) / 1e12,
+                                "peak": FP32_PEAK_TFLOPS, "unit": "TFLOP/s",
+                                "peak_source": "nominal fp32 FMA rate (148 SMs x 128 lanes x 2 x 1.965 GHz)",
+                                "stage": "nn_network"}}
+    kernels["k_simt_trunk"]["frac"] = kernels["k_simt_trunk"]["achieved"] / FP32_PEAK_TFLOPS
+    kernels["k_simt_trunk"]["traffic"] = TRAFFIC_PER_UNIT["k_simt_trunk"] * active
+    dom = max(kernels, key=lambda k: kernels[k]["ms"])
+    roofline = kernels[dom]
+    stages["nn_network"]["largest_kernel"] = {"kernel": "k_simt_trunk", "ms": trunk_ms}
     variants = {}
     for name, lg in legs.items():
         g_ms, m_ms = lg["stage"][2], lg["stage"][6]

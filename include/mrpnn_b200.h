@@ -436,7 +436,8 @@ int mr_sync(void* stream, int32_t timeout_ms);
 
 /* Per-stage CUDA-event timing of this volume's kernels (off by default).
  * Stages: 0 delta tracking, 1 neural trace, 2 neural descriptor gather,
- * 3 TR build, 4 HG table build, 5 pyramid build, 6 neural network (MLP).
+ * 3 TR build, 4 HG table build, 5 pyramid build, 6 neural network (MLP),
+ * 7 the fp32 network's main-trunk kernel alone (part of stage 6).
  * mr_volume_stage_times waits
  * for the device, returns the summed milliseconds and launch counts of the
  * first n stages since the last query, and resets them. */

@@ -21,7 +21,9 @@ constexpr int kCounters = 8;
 
 // Optional per-stage CUDA-event timing (mr_volume_set_timing).
 enum Stage {
-  ST_PT = 0, ST_NN_TRACE = 1, ST_NN_PREDICT = 2, ST_TR = 3, ST_LUT = 4, ST_MIPS = 5, ST_NN_MLP = 6, ST_COUNT = 8
+  ST_PT = 0, ST_NN_TRACE = 1, ST_NN_PREDICT = 2, ST_TR = 3, ST_LUT = 4, ST_MIPS = 5, ST_NN_MLP = 6,
+  ST_NN_TRUNK = 7,  // the fp32 network's main-trunk kernel alone (inside ST_NN_MLP)
+  ST_COUNT = 8
 };
 struct StageTimer {
   bool on = false;

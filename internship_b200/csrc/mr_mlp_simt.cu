@@ -1142,7 +1142,7 @@ int launch_mlp_simt(const Network* net, const float* desc, const float* aux, lon
                     long long ars, long long afs, int n, const unsigned* count, float* out, const int* pix,
                     const float* trph, F3 light_color, F3 scatter, cudaStream_t s, const int* job,
                     const BatchOut* bout, float* tout, long long trs, long long tcs, float* stg, long long srs,
-                    long long scs) {
+                    long long scs, StageTimer* timer) {
   if (!tout || !stg) return set_error(MR_ERR_ARG, "fp32 network: no buffer for the trunk or LC2 outputs");
   if (net->h_tail.size() != (size_t)kTailFloats || net->h_light.size() * sizeof(float) != sizeof(LightParams))
     return set_error(MR_ERR_STATE, "network not packed");
@@ -1164,7 +1164,9 @@ int launch_mlp_simt(const Network* net, const float* desc, const float* aux, lon
   a.afs = afs;
   a.n = n;
   a.count = count;
+  if (timer) timer->mark(ST_NN_TRUNK, s);
   k_simt_trunk<<<(unsigned)((n + kTile - 1) / kTile), kTile, kTrunkSmem, s>>>(a, TrunkOut{tout, trs, tcs});
+  if (timer) timer->mark(ST_NN_TRUNK, s);
   MR_CUDA(cudaGetLastError());
   {
     LightParams LP;

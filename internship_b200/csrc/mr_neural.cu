@@ -677,7 +677,8 @@ int launch_mlp_tc(const Network* net, const float* desc, const float* aux, long 
 int launch_mlp_simt(const Network* net, const float* desc, const float* aux, long long rs, long long cs,
                     long long ars, long long afs, int n, const unsigned* count, float* out, const int* pix,
                     const float* trph, F3 light_color, F3 scatter, cudaStream_t s, const int* job, const BatchOut* bout,
-                    float* tout, long long trs, long long tcs, float* stg, long long srs, long long scs);
+                    float* tout, long long trs, long long tcs, float* stg, long long srs, long long scs,
+                    StageTimer* timer = nullptr);
 int mlp_tc_error(const Network* net, bool reset);
 
 extern int check_params(const mr_render_params* p);
@@ -902,7 +903,7 @@ static int neural_passes(Volume* v, const Network* net, const mr_render_params* 
     // outputs over chunks 48..71 (all consumed by the trunk)
     rc = launch_mlp_simt(net, desc, aux, 4, 4 * cap, 1, cap, (int)npx, rec.count, dev_rgb, rec.pix, rec.trph,
                          to_f3(p->light_color), out_scale, s, nullptr, nullptr, desc, 4, 4 * cap,
-                         desc + 48 * 4 * cap, 4, 4 * cap);
+                         desc + 48 * 4 * cap, 4, 4 * cap, timed ? &v->timer : nullptr);
   mark(ST_NN_MLP);
   if (rc == MR_OK && marching) {
     k_march_compose<<<(unsigned)((npx + 127) / 128), 128, 0, s>>>(rec.count, rec.pix, madd, dev_rgb);

@@ -25,40 +25,86 @@ struct DTArgs {
   double* sumsq64;                  // W*H*3 (nullable)
 };
 
+// Per-pixel sums of one finished path's radiance (clamped at 0).
+__device__ __forceinline__ void add_path(const DTArgs& a, unsigned pix, F3 L) {
+  L = vmax(L, f3(0, 0, 0));
+  size_t o = (size_t)pix * 3;
+  if (a.sum32) {
+    atomicAdd(a.sum32 + o, L.x);
+    atomicAdd(a.sum32 + o + 1, L.y);
+    atomicAdd(a.sum32 + o + 2, L.z);
+  }
+  if (a.sum64) {
+    atomicAdd(a.sum64 + o, (double)L.x);
+    atomicAdd(a.sum64 + o + 1, (double)L.y);
+    atomicAdd(a.sum64 + o + 2, (double)L.z);
+  }
+  if (a.sumsq64) {
+    atomicAdd(a.sumsq64 + o, (double)L.x * L.x);
+    atomicAdd(a.sumsq64 + o + 1, (double)L.y * L.y);
+    atomicAdd(a.sumsq64 + o + 2, (double)L.z * L.z);
+  }
+}
+
+// CalculateRadiance regenerated per bounce: each iteration of the loop is one
+// bounce (free flight to the next vertex, then NEE towards the light) of
+// every lane's path, and a lane whose path ended takes its next work item at
+// the top of the next iteration instead of idling until the warp's longest
+// path ends. Path lengths are heavy-tailed (up to max_bounces vertices in an
+// optically thick medium against none for a ray that misses the volume), so
+// whole-path lockstep leaves most lanes idle. A path draws the same random
+// numbers in the same order as path_radiance, so its radiance is the same.
 __global__ void __launch_bounds__(128) k_delta_track(DTArgs a) {
   TrackStats st{0, 0};
   unsigned paths = 0;
   const unsigned long long P = (unsigned long long)a.cam.width * a.cam.height;
+  Rng rng;
+  F3 pos = f3(0, 0, 0), rd = f3(0, 0, 0), rate = f3(0, 0, 0), res = f3(0, 0, 0);
+  unsigned pix = 0;
+  int bounce = 0;
+  bool live = false, done = false;
   for (;;) {
-    unsigned long long w = claim_work(a.queue);
-    if (w >= a.total) break;
-    // sample-major order: concurrently traced paths are neighbouring pixels.
-    unsigned s = (unsigned)(w / P);
-    unsigned pix = (unsigned)(w - (unsigned long long)s * P);
-    int row = pix / a.cam.width, col = pix - row * a.cam.width;
-    Rng rng;
-    rng.init(a.seed, pix, a.sample_offset + s, TAG_PT);
-    float jx = rng.next(), jy = rng.next();
-    F3 dir = camera_dir(a.cam, row, col, jx, jy);
-    float t;
-    F3 L = path_radiance(a.m, a.sc, rng, a.cam.ori, dir, &t, st);
-    L = vmax(L, f3(0, 0, 0));
-    ++paths;
-    size_t o = (size_t)pix * 3;
-    if (a.sum32) {
-      atomicAdd(a.sum32 + o, L.x);
-      atomicAdd(a.sum32 + o + 1, L.y);
-      atomicAdd(a.sum32 + o + 2, L.z);
+    // lanes without a path claim work items until one enters the volume
+    while (!live) {
+      unsigned long long w = claim_work(a.queue);
+      if (w >= a.total) { done = true; break; }
+      // sample-major order: concurrently traced paths are neighbouring pixels.
+      unsigned s = (unsigned)(w / P);
+      pix = (unsigned)(w - (unsigned long long)s * P);
+      int row = pix / a.cam.width, col = pix - row * a.cam.width;
+      rng.init(a.seed, pix, a.sample_offset + s, TAG_PT);
+      float jx = rng.next(), jy = rng.next();
+      F3 dir = normalize(camera_dir(a.cam, row, col, jx, jy));
+      float dis = ray_box_offset(a.cam.ori, dir);
+      ++paths;
+      if (dis < 0) { add_path(a, pix, sky(a.sc, dir)); continue; }
+      if (a.sc.max_bounces <= 0) { add_path(a, pix, f3(0, 0, 0)); continue; }
+      pos = a.cam.ori + dir * dis;
+      rd = dir;
+      rate = f3(1, 1, 1);
+      res = f3(0, 0, 0);
+      bounce = 0;
+      live = true;
     }
-    if (a.sum64) {
-      atomicAdd(a.sum64 + o, (double)L.x);
-      atomicAdd(a.sum64 + o + 1, (double)L.y);
-      atomicAdd(a.sum64 + o + 2, (double)L.z);
+    if (done) break;
+    // one bounce (the body of CalculateRadiance's loop, core/render.cuh:219-254)
+    F3 np, nd;
+    float maxd = ray_box_distance(pos, rd);
+    if (!next_vertex(a.m, rng, a.sc.alpha, a.sc.g, pos, rd, maxd, np, nd, st)) {
+      res = res + sky(a.sc, rd) * rate;
+      add_path(a, pix, res);
+      live = false;
+      continue;
     }
-    if (a.sumsq64) {
-      atomicAdd(a.sumsq64 + o, (double)L.x * L.x);
-      atomicAdd(a.sumsq64 + o + 1, (double)L.y * L.y);
-      atomicAdd(a.sumsq64 + o + 2, (double)L.z * L.z);
+    pos = np;
+    rate = rate * a.sc.scatter;
+    maxd = ray_box_distance(pos, a.sc.L);
+    float ph = hg_phase(dot(rd, a.sc.L), a.sc.g);
+    res = res + (a.sc.light_color * rate) * (transmittance(a.m, rng, pos, a.sc.L, maxd, a.sc.alpha, st) * ph);
+    rd = nd;
+    if (++bounce >= a.sc.max_bounces) {
+      add_path(a, pix, res);
+      live = false;
     }
   }
   // one atomic per warp for the statistics
