@@ -518,9 +518,11 @@ def denoise_leg(hbm_gbs, steps=10, W=1920, H=1080):
 def training_leg(configs=8, samples=400_000, spp=1024, epochs=20):
     """Reduced configuration-4 run of the learned part: labels from the
     project's delta tracker on seeded fBm clouds (FP64 sums), training with
-    the hand-written kernels, held-out error with and without the network."""
+    the hand-written kernels (BF16 tensor-core head, FP32 master weights and
+    Adam), held-out error with and without the network."""
     from internship_b200 import train
-    _, rep = train.run(configs=configs, samples=samples, spp=spp, bounces=512, epochs=epochs, batch=65536, lr=1e-3)
+    _, rep = train.run(configs=configs, samples=samples, spp=spp, bounces=512, epochs=epochs, batch=65536, lr=1e-3,
+                       precision="bf16")
     rep["workload"] = ("%d seeded fBm clouds (128^3 / 256^3 / 512^3), alpha 16-256, albedo 0.9-1.0, g 0.7-0.9, "
                        "%d rows, %d spp per label, %d epochs (configuration 4 reduced: 32 clouds, 5 M rows, "
                        "4096 spp)" % (configs, samples, spp, epochs))

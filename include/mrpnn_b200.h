@@ -272,6 +272,13 @@ int mr_sampler_selftest(int32_t n, const float* host_table, const float* host_uv
  * memory. Returns MR_ERR_TIMEOUT (the expected outcome) with the time the wait
  * took in *host_waited_ns (may be NULL); the device stays usable. */
 int mr_tc_wait_selftest(int32_t limit_us, int64_t* host_waited_ns);
+/* BF16 tile product D[128 x n] = A[128 x k] B[n x k]^T (row-major inputs)
+ * with A (a_mn = 1) and / or B (b_mn = 1) read MN-major: stored in the
+ * canonical K-major layout of the transpose, as the BF16 training reads its
+ * forward tiles and weights in the backward products. Shapes (n, k):
+ * (64, 32), (128, 64), (128, 128), (64, 128). */
+int mr_tc_selftest_mn(int32_t n, int32_t k, int32_t a_mn, int32_t b_mn, const uint16_t* host_a,
+                      const uint16_t* host_b, float* host_d);
 /* Memory-path probe (no reference counterpart): reads dev_buf (`bytes`, a
  * multiple of 16, 16-byte aligned) `passes` times with 16-byte loads that
  * bypass L1, from a resident grid; dev_sink is one device word. Time it with
@@ -430,6 +437,12 @@ int mr_trainer_gradient(mr_trainer* t, const float* dev_desc, const float* dev_a
 int mr_trainer_step(mr_trainer* t, const float* dev_desc, const float* dev_aux, const float* dev_label, int32_t n,
                     float lr, float* host_loss, void* stream);
 int mr_trainer_weights(const mr_trainer* t, float* host_out, size_t count);
+/* Arithmetic of the training step: MR_PREC_FP32 (default; every layer on the
+ * CUDA cores, one row per thread) or MR_PREC_BF16: the head's LC0 / LC1 / LC2
+ * forward, input-gradient and weight-gradient products as tcgen05 MMAs with
+ * BF16 operands and FP32 accumulation, the rest in FP32; Adam keeps the FP32
+ * master weights either way. */
+int mr_trainer_set_precision(mr_trainer* t, int32_t precision);
 
 /* Wait for `stream` with a watchdog: MR_ERR_TIMEOUT after timeout_ms. */
 int mr_sync(void* stream, int32_t timeout_ms);

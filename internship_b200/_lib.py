@@ -31,7 +31,7 @@ EXPORTS = [
     "mr_batch_autotune", "mr_batch_render", "mr_batch_capture", "mr_batch_launch", "mr_batch_counters",
     "mr_tc_selftest_fp8", "mr_sampler_selftest", "mr_tc_selftest_tf32", "mr_render_host_async",
     "mr_render_host_wait", "mr_spiral_stencil", "mr_stream_read_probe", "mr_volume_load", "mr_volume_file_read",
-    "mr_tc_wait_selftest", "mr_volume_set_hdri", "mr_volume_load_hdri", "mr_volume_clear_hdri", "mr_hdr_read",
+    "mr_tc_wait_selftest", "mr_tc_selftest_mn", "mr_trainer_set_precision", "mr_volume_set_hdri", "mr_volume_load_hdri", "mr_volume_clear_hdri", "mr_hdr_read",
     "mr_batch_set_timing", "mr_batch_frame_times", "mr_volume_set_surface_ior",
 ]
 NOALLOC_MAX_PIXELS = 16384
@@ -108,6 +108,8 @@ def load():
     L.mr_stream_read_probe.argtypes = [vp, sz, i32, vp, vp]
     L.mr_volume_load.argtypes = [C.c_char_p, i32, C.POINTER(vp), vp]
     L.mr_tc_wait_selftest.argtypes = [i32, C.POINTER(C.c_int64)]
+    L.mr_tc_selftest_mn.argtypes = [i32, i32, i32, i32, vp, vp, vp]
+    L.mr_trainer_set_precision.argtypes = [vp, i32]
     L.mr_volume_set_hdri.argtypes = [vp, vp, i32, i32]
     L.mr_batch_set_timing.argtypes = [vp, i32]
     L.mr_volume_set_surface_ior.argtypes = [vp, fp]

@@ -140,10 +140,6 @@ constexpr int kTmemCols = 512;  // 128 per group (power of two allocation)
 static_assert(128 * kGroups <= kTmemCols, "tensor memory budget");
 static_assert(kSmemBytes <= 232448, "shared memory budget");
 
-// Byte offset of element (row, k) of a K-major tile with KP columns.
-__host__ __device__ constexpr int canon_off(int row, int k, int kp) {
-  return ((row >> 3) * (kp >> 3) + (k >> 3)) * 128 + (row & 7) * 16 + (k & 7) * 2;
-}
 
 __device__ __forceinline__ void group_bar(int g) { asm volatile("bar.sync %0, 128;" ::"r"(g + 1) : "memory"); }
 

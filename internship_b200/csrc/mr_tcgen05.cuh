@@ -18,6 +18,12 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t 
   d |= (uint64_t)1 << 46;
   return d;
 }
+// Byte offset of element (row, k) of a BF16 tile with KP columns in the
+// canonical K-major no-swizzle layout: core matrices of 8 rows x 16 B
+// (8 elements), adjacent along K 128 B apart, 8-row groups (KP/8)*128 B apart.
+__host__ __device__ constexpr int canon_off(int row, int k, int kp) {
+  return ((row >> 3) * (kp >> 3) + (k >> 3)) * 128 + (row & 7) * 16 + (k & 7) * 2;
+}
 // Instruction descriptor: BF16 x BF16 -> FP32, A and B K-major, M x N.
 __host__ __device__ constexpr uint32_t idesc_bf16(int m, int n) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);

@@ -25,6 +25,7 @@
 #include "mr_internal.h"
 #include "mr_net_layout.cuh"
 #include "mr_track.cuh"
+#include "mr_train.cuh"
 
 namespace mr {
 
@@ -179,104 +180,6 @@ __global__ void k_train_frames(const float* dir, int n, F3 L, uint32_t seed, flo
 // then the light-direction trunk (:424-437). Per block: width S, mode (0 SE +
 // ADD3, 1 SERES + ADD3, 2 SERES + REP3), descriptor offset, pool index, SE
 // weights and the three branch layers (density, transmittance, phase).
-struct TrainTables {
-  int S[12], mode[12], from[12], pid[12], se0[12], se1[12], w[12][3], b[12][3];
-  int l81w[3], l81b[3], ld41w[3], ld41b[3];
-  int f1, f2, ggw, ggb, lc0w, lc0b, lc1w, lc1b, lc2w, lc2b, lxw, lxb, lxrw[12], lxrb[12], lx12w, lx12b;
-};
-constexpr TrainTables make_train_tables() {
-  TrainTables t{};
-  const WeightTable wt = make_weight_table();
-  const int S[12] = {8, 8, 16, 16, 16, 32, 32, 32, 8, 8, 8, 8};
-  const int mode[12] = {0, 2, 1, 1, 2, 1, 1, 1, 0, 1, 1, 1};
-  const int from[12] = {0, 8, 16, 32, 48, 64, 96, 128, 160, 168, 176, 184};
-  const int se0[12] = {MR_W_LSE01W, MR_W_LSE11W, MR_W_LSE21W, MR_W_LSE31W, MR_W_LSE41W, MR_W_LSE51W,
-                       MR_W_LSE61W, MR_W_LSE71W, MR_W_LDSE01W, MR_W_LDSE11W, MR_W_LDSE21W, MR_W_LDSE31W};
-  const int se1[12] = {MR_W_LSE02W, MR_W_LSE12W, MR_W_LSE22W, MR_W_LSE32W, MR_W_LSE42W, MR_W_LSE52W,
-                       MR_W_LSE62W, MR_W_LSE72W, MR_W_LDSE02W, MR_W_LDSE12W, MR_W_LDSE22W, MR_W_LDSE32W};
-  const int lw[12][3] = {{MR_W_L01W, MR_W_L_Tr01W, MR_W_L_Hg01W}, {MR_W_L11W, MR_W_L_Tr11W, MR_W_L_Hg11W},
-                         {MR_W_L21W, MR_W_L_Tr21W, MR_W_L_Hg21W}, {MR_W_L31W, MR_W_L_Tr31W, MR_W_L_Hg31W},
-                         {MR_W_L41W, MR_W_L_Tr41W, MR_W_L_Hg41W}, {MR_W_L51W, MR_W_L_Tr51W, MR_W_L_Hg51W},
-                         {MR_W_L61W, MR_W_L_Tr61W, MR_W_L_Hg61W}, {MR_W_L71W, MR_W_L_Tr71W, MR_W_L_Hg71W},
-                         {MR_W_LD01W, MR_W_LD_Tr01W, MR_W_LD_Hg01W}, {MR_W_LD11W, MR_W_LD_Tr11W, MR_W_LD_Hg11W},
-                         {MR_W_LD21W, MR_W_LD_Tr21W, MR_W_LD_Hg21W}, {MR_W_LD31W, MR_W_LD_Tr31W, MR_W_LD_Hg31W}};
-  const int lb[12][3] = {{MR_W_L01B, MR_W_L_Tr01B, MR_W_L_Hg01B}, {MR_W_L11B, MR_W_L_Tr11B, MR_W_L_Hg11B},
-                         {MR_W_L21B, MR_W_L_Tr21B, MR_W_L_Hg21B}, {MR_W_L31B, MR_W_L_Tr31B, MR_W_L_Hg31B},
-                         {MR_W_L41B, MR_W_L_Tr41B, MR_W_L_Hg41B}, {MR_W_L51B, MR_W_L_Tr51B, MR_W_L_Hg51B},
-                         {MR_W_L61B, MR_W_L_Tr61B, MR_W_L_Hg61B}, {MR_W_L71B, MR_W_L_Tr71B, MR_W_L_Hg71B},
-                         {MR_W_LD01B, MR_W_LD_Tr01B, MR_W_LD_Hg01B}, {MR_W_LD11B, MR_W_LD_Tr11B, MR_W_LD_Hg11B},
-                         {MR_W_LD21B, MR_W_LD_Tr21B, MR_W_LD_Hg21B}, {MR_W_LD31B, MR_W_LD_Tr31B, MR_W_LD_Hg31B}};
-  for (int i = 0; i < 12; ++i) {
-    t.S[i] = S[i]; t.mode[i] = mode[i]; t.from[i] = from[i]; t.pid[i] = 3 * i;
-    t.se0[i] = wt.off[se0[i]]; t.se1[i] = wt.off[se1[i]];
-    for (int br = 0; br < 3; ++br) { t.w[i][br] = wt.off[lw[i][br]]; t.b[i][br] = wt.off[lb[i][br]]; }
-  }
-  const int l81w[3] = {MR_W_L81W, MR_W_L_Tr81W, MR_W_L_Hg81W}, l81b[3] = {MR_W_L81B, MR_W_L_Tr81B, MR_W_L_Hg81B};
-  const int ld41w[3] = {MR_W_LD41W, MR_W_LD_Tr41W, MR_W_LD_Hg41W};
-  const int ld41b[3] = {MR_W_LD41B, MR_W_LD_Tr41B, MR_W_LD_Hg41B};
-  for (int br = 0; br < 3; ++br) {
-    t.l81w[br] = wt.off[l81w[br]]; t.l81b[br] = wt.off[l81b[br]];
-    t.ld41w[br] = wt.off[ld41w[br]]; t.ld41b[br] = wt.off[ld41b[br]];
-  }
-  t.f1 = wt.off[MR_W_LSEFin1W]; t.f2 = wt.off[MR_W_LSEFin2W];
-  t.ggw = wt.off[MR_W_LGGSW]; t.ggb = wt.off[MR_W_LGGSB];
-  t.lc0w = wt.off[MR_W_LC0W]; t.lc0b = wt.off[MR_W_LC0B]; t.lc1w = wt.off[MR_W_LC1W]; t.lc1b = wt.off[MR_W_LC1B];
-  t.lc2w = wt.off[MR_W_LC2W]; t.lc2b = wt.off[MR_W_LC2B]; t.lxw = wt.off[MR_W_LXW]; t.lxb = wt.off[MR_W_LXB];
-  const int rw[12] = {MR_W_LX0W, MR_W_LX1W, MR_W_LX2W, MR_W_LX3W, MR_W_LX4W, MR_W_LX5W,
-                      MR_W_LX6W, MR_W_LX7W, MR_W_LX8W, MR_W_LX9W, MR_W_LX10W, MR_W_LX11W};
-  const int rb[12] = {MR_W_LX0B, MR_W_LX1B, MR_W_LX2B, MR_W_LX3B, MR_W_LX4B, MR_W_LX5B,
-                      MR_W_LX6B, MR_W_LX7B, MR_W_LX8B, MR_W_LX9B, MR_W_LX10B, MR_W_LX11B};
-  for (int i = 0; i < 12; ++i) { t.lxrw[i] = wt.off[rw[i]]; t.lxrb[i] = wt.off[rb[i]]; }
-  t.lx12w = wt.off[MR_W_LX12W]; t.lx12b = wt.off[MR_W_LX12B];
-  return t;
-}
-__constant__ TrainTables c_tt = make_train_tables();
-
-__device__ __forceinline__ float relu(float x) { return x > 0.0f ? x : 0.0f; }
-__device__ __forceinline__ float sigmoid(float x) { return 1.0f / (1.0f + expf(-x)); }
-
-// Warp sum of v, added to G[idx] by lane 0. Every lane of the warp calls it
-// with the same idx.
-__device__ __forceinline__ void gacc(float* G, int idx, float v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0 && v != 0.0f) atomicAdd(G + idx, v);
-}
-
-// ypre[o] = b[o] + sum_i W[o*K + i] x[i]
-__device__ __forceinline__ void dense_fwd(const float* __restrict__ W, const float* __restrict__ B, const float* x,
-                                          int K, int N, float* ypre) {
-#pragma unroll 1
-  for (int o = 0; o < N; ++o) {
-    float a = 0.0f;
-#pragma unroll 4
-    for (int i = 0; i < K; ++i) a += x[i] * __ldg(W + o * K + i);
-    ypre[o] = a + (B ? __ldg(B + o) : 0.0f);
-  }
-}
-// Given dpre (N), input x (K): gradients of W (GW) and B (GB), and dx += W^T dpre
-// (dx may be null).
-__device__ __forceinline__ void dense_bwd(const float* __restrict__ W, float* GW, float* GB, const float* x,
-                                          const float* dpre, float* dx, int K, int N) {
-#pragma unroll 1
-  for (int o = 0; o < N; ++o) {
-    const float d = dpre[o];
-    if (!__any_sync(0xffffffffu, d != 0.0f)) continue;  // dead unit for the whole warp
-    if (GB) gacc(GB, o, d);
-#pragma unroll 4
-    for (int i = 0; i < K; ++i) gacc(GW, o * K + i, d * x[i]);
-  }
-  if (dx) {
-#pragma unroll 1
-    for (int i = 0; i < K; ++i) {
-      float a = 0.0f;
-#pragma unroll 4
-      for (int o = 0; o < N; ++o) a += __ldg(W + o * K + i) * dpre[o];
-      dx[i] += a;
-    }
-  }
-}
-
 struct TrainArgs {
   const float* w;       // fp32 master weights (blob layout)
   float* grad;          // fp32 gradient accumulator (blob layout)
@@ -286,8 +189,17 @@ struct TrainArgs {
   int n;
   float inv_batch;      // loss weight 1/n
   float* loss;          // summed (X - T)^2 / n
+  float* h0;            // TR_TRUNK_FWD: the head input per row (n x 128), written
+  const float* dh0;     // TR_TRUNK_BWD: its gradient per row (n x 128), read
 };
 
+// Parts of the training step the kernel runs: the whole network (fp32), or
+// the two halves around the tensor-core head of the BF16 step (the trunks'
+// forward up to the head input, and the trunks' backward from its gradient,
+// the forward recomputed).
+enum { TR_FULL = 0, TR_TRUNK_FWD = 1, TR_TRUNK_BWD = 2 };
+
+template <int MODE>
 __global__ void __launch_bounds__(128) k_train_fwd_bwd(TrainArgs a) {
   const int k0 = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = k0 < a.n;
@@ -376,60 +288,39 @@ __global__ void __launch_bounds__(128) k_train_fwd_bwd(TrainArgs a) {
   for (int br = 0; br < 3; ++br)
     for (int i = 0; i < 8; ++i) H0[96 + 8 * br + i] = relu(CLP[br][i]) * SP[3 + br];
   for (int i = 0; i < 8; ++i) H0[120 + i] = relu(X8P[i]);
-  float A1P[128], A1[128], A2P[64], A2[64], A3P[32], A3[32], AXP[16];
-  dense_fwd(W + T.lc0w, W + T.lc0b, H0, 128, 128, A1P);
-  for (int i = 0; i < 128; ++i) A1[i] = relu(A1P[i]);
-  dense_fwd(W + T.lc1w, W + T.lc1b, A1, 128, 64, A2P);
-  for (int i = 0; i < 64; ++i) A2[i] = relu(A2P[i]);
-  dense_fwd(W + T.lc2w, W + T.lc2b, A2, 64, 32, A3P);
-  for (int i = 0; i < 32; ++i) A3[i] = relu(A3P[i]);
-  dense_fwd(W + T.lxw, W + T.lxb, A3, 32, 16, AXP);
-  float AR[7][16], TP[6][16], TT[6][16], UP[6][16];
-  for (int i = 0; i < 16; ++i) AR[0][i] = relu(AXP[i]);
-#pragma unroll 1
-  for (int r = 0; r < 6; ++r) {
-    dense_fwd(W + T.lxrw[2 * r], W + T.lxrb[2 * r], AR[r], 16, 16, TP[r]);
-    for (int i = 0; i < 16; ++i) TT[r][i] = relu(TP[r][i]);
-    dense_fwd(W + T.lxrw[2 * r + 1], W + T.lxrb[2 * r + 1], TT[r], 16, 16, UP[r]);
-    for (int i = 0; i < 16; ++i) AR[r + 1][i] = AR[r][i] + relu(UP[r][i]);
+  if constexpr (MODE == TR_TRUNK_FWD) {
+    if (valid) {
+      float4* o = reinterpret_cast<float4*>(a.h0 + (size_t)k * 128);
+      for (int i = 0; i < 32; ++i) o[i] = make_float4(H0[4 * i], H0[4 * i + 1], H0[4 * i + 2], H0[4 * i + 3]);
+    }
+    return;
   }
-  float OP;
-  dense_fwd(W + T.lx12w, W + T.lx12b, AR[6], 16, 1, &OP);
-  const float Xo = relu(OP);
-  const float target = log1pf(fmaxf(a.label[k], 0.0f) / srp);
-  const float err = valid ? Xo - target : 0.0f;
-  {
-    float l = err * err * a.inv_batch;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
-    if ((threadIdx.x & 31) == 0) atomicAdd(a.loss, l);
+  float dH0[128];
+  if constexpr (MODE == TR_TRUNK_BWD) {
+    const float4* gi = reinterpret_cast<const float4*>(a.dh0 + (size_t)k * 128);
+    for (int i = 0; i < 32; ++i) {
+      const float4 q = valid ? gi[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      dH0[4 * i] = q.x; dH0[4 * i + 1] = q.y; dH0[4 * i + 2] = q.z; dH0[4 * i + 3] = q.w;
+    }
+  } else {
+    float A1P[128], A1[128], A2P[64], A2[64], A3P[32], A3[32];
+    dense_fwd(W + T.lc0w, W + T.lc0b, H0, 128, 128, A1P);
+    for (int i = 0; i < 128; ++i) A1[i] = relu(A1P[i]);
+    dense_fwd(W + T.lc1w, W + T.lc1b, A1, 128, 64, A2P);
+    for (int i = 0; i < 64; ++i) A2[i] = relu(A2P[i]);
+    dense_fwd(W + T.lc2w, W + T.lc2b, A2, 64, 32, A3P);
+    for (int i = 0; i < 32; ++i) A3[i] = relu(A3P[i]);
+    float d3[32], dA3[32], d2[64], dA2[64], d1[128], dA1[128];
+    tail_fwd_bwd(W, G, T, A3, a.label[k], srp, valid, a.inv_batch, a.loss, d3);
+    for (int i = 0; i < 32; ++i) dA3[i] = A3P[i] > 0.0f ? d3[i] : 0.0f;
+    for (int i = 0; i < 64; ++i) d2[i] = 0.0f;
+    dense_bwd(W + T.lc2w, G + T.lc2w, G + T.lc2b, A2, dA3, d2, 64, 32);
+    for (int i = 0; i < 64; ++i) dA2[i] = A2P[i] > 0.0f ? d2[i] : 0.0f;
+    for (int i = 0; i < 128; ++i) d1[i] = 0.0f;
+    dense_bwd(W + T.lc1w, G + T.lc1w, G + T.lc1b, A1, dA2, d1, 128, 64);
+    for (int i = 0; i < 128; ++i) { dA1[i] = A1P[i] > 0.0f ? d1[i] : 0.0f; dH0[i] = 0.0f; }
+    dense_bwd(W + T.lc0w, G + T.lc0w, G + T.lc0b, H0, dA1, dH0, 128, 128);
   }
-
-  // ---- backward
-  float dOP = 2.0f * err * a.inv_batch * (OP > 0.0f ? 1.0f : 0.0f);
-  float da[16];
-  for (int i = 0; i < 16; ++i) da[i] = 0.0f;
-  dense_bwd(W + T.lx12w, G + T.lx12w, G + T.lx12b, AR[6], &dOP, da, 16, 1);
-#pragma unroll 1
-  for (int r = 5; r >= 0; --r) {
-    float du[16], dt[16], dtp[16];
-    for (int i = 0; i < 16; ++i) { du[i] = UP[r][i] > 0.0f ? da[i] : 0.0f; dt[i] = 0.0f; }
-    dense_bwd(W + T.lxrw[2 * r + 1], G + T.lxrw[2 * r + 1], G + T.lxrb[2 * r + 1], TT[r], du, dt, 16, 16);
-    for (int i = 0; i < 16; ++i) dtp[i] = TP[r][i] > 0.0f ? dt[i] : 0.0f;
-    dense_bwd(W + T.lxrw[2 * r], G + T.lxrw[2 * r], G + T.lxrb[2 * r], AR[r], dtp, da, 16, 16);  // da += W^T dtp
-  }
-  float dAX[16], d3[32], dA3[32], d2[64], dA2[64], d1[128], dA1[128], dH0[128];
-  for (int i = 0; i < 16; ++i) dAX[i] = AXP[i] > 0.0f ? da[i] : 0.0f;
-  for (int i = 0; i < 32; ++i) d3[i] = 0.0f;
-  dense_bwd(W + T.lxw, G + T.lxw, G + T.lxb, A3, dAX, d3, 32, 16);
-  for (int i = 0; i < 32; ++i) dA3[i] = A3P[i] > 0.0f ? d3[i] : 0.0f;
-  for (int i = 0; i < 64; ++i) d2[i] = 0.0f;
-  dense_bwd(W + T.lc2w, G + T.lc2w, G + T.lc2b, A2, dA3, d2, 64, 32);
-  for (int i = 0; i < 64; ++i) dA2[i] = A2P[i] > 0.0f ? d2[i] : 0.0f;
-  for (int i = 0; i < 128; ++i) d1[i] = 0.0f;
-  dense_bwd(W + T.lc1w, G + T.lc1w, G + T.lc1b, A1, dA2, d1, 128, 64);
-  for (int i = 0; i < 128; ++i) { dA1[i] = A1P[i] > 0.0f ? d1[i] : 0.0f; dH0[i] = 0.0f; }
-  dense_bwd(W + T.lc0w, G + T.lc0w, G + T.lc0b, H0, dA1, dH0, 128, 128);
   // head input: gated combs and LGGS
   float dSP[6] = {0, 0, 0, 0, 0, 0};
   float dCM[3][32], dCL[3][8];
@@ -512,7 +403,20 @@ struct Trainer {
   float* loss = nullptr;
   int step = 0;
   float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  // MR_PREC_BF16: the head on the tensor cores (mr_train_tc.cu) between the
+  // trunks' forward and backward halves, which exchange the head input and
+  // its gradient per row through h0 / dh0 (cap rows each).
+  int precision = MR_PREC_FP32;
+  float* h0 = nullptr;
+  float* dh0 = nullptr;
+  size_t cap = 0;
+  uint8_t* img = nullptr;  // BF16 head weights, rebuilt from w every step
+  int* err = nullptr;      // set when a bounded wait of the head kernel gives up
 };
+
+int launch_head_tc(const float* w, float* grad, uint8_t* img, const float* h0, float* dh0, const float* aux,
+                   const float* label, int n, float inv_batch, float* loss, int* err, cudaStream_t s);
+size_t head_image_bytes();
 
 }  // namespace mr
 
@@ -633,8 +537,37 @@ extern "C" int mr_trainer_destroy(mr_trainer* h) {
   cudaFree(h->t.v);
   cudaFree(h->t.grad);
   cudaFree(h->t.loss);
+  cudaFree(h->t.h0);
+  cudaFree(h->t.dh0);
+  cudaFree(h->t.img);
+  cudaFree(h->t.err);
   delete h;
   return MR_OK;
+}
+
+extern "C" int mr_trainer_set_precision(mr_trainer* h, int32_t precision) {
+  clear_error();
+  if (!h) return set_error(MR_ERR_ARG, "mr_trainer_set_precision: NULL trainer");
+  if (precision != MR_PREC_FP32 && precision != MR_PREC_BF16)
+    return set_error(MR_ERR_ARG, "training precision must be MR_PREC_FP32 or MR_PREC_BF16 (got %d)", precision);
+  Trainer& t = h->t;
+  if (precision == MR_PREC_BF16 && !t.img) {
+    MR_CUDA(cudaMalloc(&t.img, head_image_bytes()));
+    MR_CUDA(cudaMalloc(&t.err, sizeof(int)));
+    MR_CUDA(cudaMemset(t.err, 0, sizeof(int)));
+  }
+  t.precision = precision;
+  return MR_OK;
+}
+
+// MR_ERR_TIMEOUT (and a reset) when a bounded wait of the BF16 head gave up.
+static int head_error(Trainer& t) {
+  if (!t.err) return MR_OK;
+  int e = 0;
+  MR_CUDA(cudaMemcpy(&e, t.err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (!e) return MR_OK;
+  MR_CUDA(cudaMemset(t.err, 0, sizeof(int)));
+  return set_error(MR_ERR_TIMEOUT, "BF16 training head: an mbarrier wait timed out");
 }
 
 static int fwd_bwd(Trainer& t, const float* desc, const float* aux, const float* label, int n, cudaStream_t s) {
@@ -648,7 +581,30 @@ static int fwd_bwd(Trainer& t, const float* desc, const float* aux, const float*
   a.n = n;
   a.inv_batch = 1.0f / (float)n;
   a.loss = t.loss;
-  k_train_fwd_bwd<<<(n + 127) / 128, 128, 0, s>>>(a);
+  a.h0 = nullptr;
+  a.dh0 = nullptr;
+  const unsigned grid = (unsigned)((n + 127) / 128);
+  if (t.precision != MR_PREC_BF16) {
+    k_train_fwd_bwd<TR_FULL><<<grid, 128, 0, s>>>(a);
+    MR_CUDA(cudaGetLastError());
+    return MR_OK;
+  }
+  if ((size_t)n > t.cap) {
+    cudaFree(t.h0);
+    cudaFree(t.dh0);
+    t.h0 = t.dh0 = nullptr;
+    t.cap = 0;
+    MR_CUDA(cudaMalloc(&t.h0, (size_t)n * 128 * sizeof(float)));
+    MR_CUDA(cudaMalloc(&t.dh0, (size_t)n * 128 * sizeof(float)));
+    t.cap = (size_t)n;
+  }
+  a.h0 = t.h0;
+  a.dh0 = t.dh0;
+  k_train_fwd_bwd<TR_TRUNK_FWD><<<grid, 128, 0, s>>>(a);
+  MR_CUDA(cudaGetLastError());
+  int rc = launch_head_tc(t.w, t.grad, t.img, t.h0, t.dh0, aux, label, n, a.inv_batch, t.loss, t.err, s);
+  if (rc) return rc;
+  k_train_fwd_bwd<TR_TRUNK_BWD><<<grid, 128, 0, s>>>(a);
   MR_CUDA(cudaGetLastError());
   return MR_OK;
 }
@@ -669,7 +625,7 @@ extern "C" int mr_trainer_gradient(mr_trainer* h, const float* dev_desc, const f
   MR_CUDA(cudaMemsetAsync(t.grad, 0, MR_WEIGHT_TOTAL * sizeof(float), s));
   MR_CUDA(cudaStreamSynchronize(s));
   if (host_loss) *host_loss = l;
-  return MR_OK;
+  return head_error(t);
 }
 
 extern "C" int mr_trainer_step(mr_trainer* h, const float* dev_desc, const float* dev_aux, const float* dev_label,
@@ -691,6 +647,7 @@ extern "C" int mr_trainer_step(mr_trainer* h, const float* dev_desc, const float
     MR_CUDA(cudaMemcpyAsync(&l, t.loss, sizeof(float), cudaMemcpyDeviceToHost, s));
     MR_CUDA(cudaStreamSynchronize(s));
     *host_loss = l;
+    return head_error(t);
   }
   return MR_OK;
 }

@@ -116,13 +116,17 @@ def initial_weights(seed=1):
 
 
 class Trainer:
-    """fp32 master weights + Adam on the device (mr_trainer_*)."""
+    """fp32 master weights + Adam on the device (mr_trainer_*). precision
+    "fp32" runs every layer on the CUDA cores; "bf16" runs the head's GEMMs
+    (forward, input and weight gradients) on the tensor cores."""
 
-    def __init__(self, weights):
+    def __init__(self, weights, precision="fp32"):
         w = np.ascontiguousarray(weights, np.float32)
         h = C.c_void_p()
         check(_lib.load().mr_trainer_create(w.ctypes.data, w.size, C.byref(h)))
         self.handle = h
+        if precision != "fp32":
+            check(_lib.load().mr_trainer_set_precision(h, {"bf16": _lib.PREC_BF16}[precision]))
 
     def step(self, desc, aux, label, lr):
         loss = C.c_float()
@@ -154,11 +158,11 @@ class Trainer:
             pass
 
 
-def fit(desc, aux, label, weights, epochs, batch, lr, seed=0, log=None):
+def fit(desc, aux, label, weights, epochs, batch, lr, seed=0, log=None, precision="fp32"):
     """Adam over shuffled mini-batches; returns (weights, per-epoch mean
     losses)."""
     import torch
-    tr = Trainer(weights)
+    tr = Trainer(weights, precision)
     n = len(label)
     gen = torch.Generator(device="cuda")
     gen.manual_seed(seed)
@@ -199,7 +203,7 @@ def targets(aux, label):
 
 
 def run(configs=32, samples=5_000_000, spp=4096, bounces=512, epochs=20, batch=65536, lr=1e-3, holdout=0.05,
-        seed=0, log=None):
+        seed=0, log=None, precision="fp32"):
     """The whole learned part: generate the rows, train from initial_weights(1)
     and evaluate on a held-out share. Returns (weights, report); the report
     holds the row count, the held-out RMSE of X = log(1 + L / srp) with the
@@ -218,7 +222,7 @@ def run(configs=32, samples=5_000_000, spp=4096, bounces=512, epochs=20, batch=6
     nh = max(1, int(n * holdout))
     hold, trn = perm[:nh], perm[nh:]
     w0 = initial_weights(1)
-    w, hist = fit(desc[trn], aux[trn], label[trn], w0, epochs, batch, lr, seed, log=log)
+    w, hist = fit(desc[trn], aux[trn], label[trn], w0, epochs, batch, lr, seed, log=log, precision=precision)
     torch.cuda.synchronize()
     t2 = time.time()
     T = targets(aux[hold], label[hold])
@@ -228,7 +232,7 @@ def run(configs=32, samples=5_000_000, spp=4096, bounces=512, epochs=20, batch=6
     rmse0 = float(torch.sqrt(torch.mean(T ** 2)))
     rows_trained = (n - nh) * epochs
     return w, {"rows": n, "configs": configs, "spp": spp, "bounces": bounces, "epochs": epochs, "batch": batch,
-               "lr": lr, "holdout_rmse_log": rmse, "untrained_rmse_log": rmse_init, "no_network_rmse_log": rmse0,
+               "lr": lr, "precision": precision, "holdout_rmse_log": rmse, "untrained_rmse_log": rmse_init, "no_network_rmse_log": rmse0,
                "generate_s": t1 - t0, "train_s": t2 - t1, "labels_per_s": n / (t1 - t0),
                "label_paths_per_s": n * spp / (t1 - t0), "train_rows_per_s": rows_trained / (t2 - t1),
                "loss_history": hist}
@@ -246,9 +250,11 @@ def main():
     ap.add_argument("--holdout", type=float, default=0.05)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default="mrpnn_trained.npy")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16"],
+                    help="bf16: the head's GEMMs on the tensor cores (BF16 operands, FP32 accumulation)")
     args = ap.parse_args()
     w, rep = run(args.configs, args.samples, args.spp, args.bounces, args.epochs, args.batch, args.lr, args.holdout,
-                 args.seed, log=print)
+                 args.seed, log=print, precision=args.precision)
     np.save(args.out, w)
     print(json.dumps(rep))
 

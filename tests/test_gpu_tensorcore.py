@@ -275,3 +275,19 @@ def test_tf32_split_tile_product_is_fp32_accurate(n, k):
     assert e1.max() < 2e-3  # one TF32 product per element
     assert e3.max() < 1e-6  # fp32-level
     assert e3.max() < e1.max() / 100
+
+
+@pytest.mark.parametrize("n,k", [(64, 32), (128, 64), (128, 128), (64, 128)])
+@pytest.mark.parametrize("a_mn,b_mn", [(0, 1), (1, 0), (1, 1)])
+def test_mn_major_tile_product_matches_matmul(n, k, a_mn, b_mn):
+    """The BF16 training's backward products read forward tiles transposed
+    (MN-major operands): D = A B^T through those descriptors equals the fp32
+    product of the BF16 inputs."""
+    from internship_b200 import _lib
+    rng = np.random.default_rng(n * 7 + k + 3 * a_mn + b_mn)
+    a = _bf16_bits(rng.standard_normal((128, k)).astype(np.float32))
+    b = _bf16_bits(rng.standard_normal((n, k)).astype(np.float32))
+    d = np.zeros((128, n), np.float32)
+    _lib.check(_lib.load().mr_tc_selftest_mn(n, k, a_mn, b_mn, a.ctypes.data, b.ctypes.data, d.ctypes.data))
+    ref = _bf16_value(a).astype(np.float64) @ _bf16_value(b).astype(np.float64).T
+    np.testing.assert_allclose(d, ref, rtol=1e-5, atol=1e-4)

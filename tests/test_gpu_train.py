@@ -156,3 +156,49 @@ def test_training_gain_over_no_network(torch):
     assert hist[-1] < 0.5 * hist[0]
     assert rmse < 0.5 * rmse_none, (rmse, rmse_none)
     assert rmse < 0.5 * rmse_init, (rmse, rmse_init)
+
+
+def test_bf16_gradient_close_to_fp32(torch):
+    """MR_PREC_BF16 training: the head's products on the tensor cores with BF16
+    operands. Its gradient, against the fp32 kernel's on the same rows (which
+    the finite-difference test pins), differs by BF16 rounding only."""
+    from internship_b200.train import Trainer
+    from internship_b200.weights import active_random_weights, layout
+    w = active_random_weights(1)
+    desc, aux, label = _rows(4096, 7)
+    dd, da, dl = (torch.from_numpy(x).cuda() for x in (desc, aux, label))
+    res = {}
+    for prec in ("fp32", "bf16"):
+        tr = Trainer(w, prec)
+        res[prec] = tr.gradient(dd, da, dl)
+        tr.close()
+    (g32, l32), (g16, l16) = res["fp32"], res["bf16"]
+    assert l16 == pytest.approx(l32, rel=5e-3)
+    cos = float(np.dot(g32, g16) / (np.linalg.norm(g32) * np.linalg.norm(g16)))
+    assert cos > 0.9999, cos
+    assert np.linalg.norm(g32 - g16) < 0.01 * np.linalg.norm(g32)
+    off = 0
+    for name, n in layout():
+        a, b = g32[off:off + n], g16[off:off + n]
+        if np.linalg.norm(a) > 1e-3 * np.linalg.norm(g32):
+            assert np.linalg.norm(a - b) < 0.03 * np.linalg.norm(a), name
+        off += n
+
+
+def test_bf16_training_gain_over_no_network(torch):
+    """The same gain test as for fp32 training, with the BF16 tensor-core head."""
+    from internship_b200 import train
+    cfgs = train.scene_configs(2, seed=3, resolutions=(64,), alpha_range=(16.0, 48.0))
+    desc, aux, label = train.generate(cfgs, 6000, spp=128, max_bounces=128, seed=1)
+    n = len(label)
+    perm = torch.randperm(n, device="cuda", generator=torch.Generator(device="cuda").manual_seed(0))
+    hold, trn = perm[:1500], perm[1500:]
+    w0 = train.initial_weights(1)
+    w, hist = train.fit(desc[trn], aux[trn], label[trn], w0, epochs=25, batch=1024, lr=1e-3, precision="bf16")
+    T = train.targets(aux[hold], label[hold])
+    dh, ah = desc[hold].contiguous(), aux[hold].contiguous()
+    rmse = float(torch.sqrt(torch.mean((train.predict_x(w, dh, ah) - T) ** 2)))
+    rmse_none = float(torch.sqrt(torch.mean(T ** 2)))
+    print("BF16 training, held-out rmse: trained %.4f, no network %.4f" % (rmse, rmse_none))
+    assert hist[-1] < 0.5 * hist[0]
+    assert rmse < 0.5 * rmse_none, (rmse, rmse_none)
