@@ -89,9 +89,11 @@ typedef struct {
 
 /* How the neural gather samples the mip / transmittance / HG tables.
  * EXACT: fp32 trilinear in software (bit-stable, the oracle's arithmetic).
- * TEXTURE: the texture units' linear filter, as the reference samples its
- * texture references (core/volume.cu:1289-1298): 8-bit interpolation
- * weights, several times fewer instructions per sample. */
+ * TEXTURE: the texture units' trilinear filter for the mip and transmittance
+ * tables, as the reference samples its texture references
+ * (core/volume.cu:1289-1298): 8-bit interpolation weights, several times fewer
+ * instructions per sample; the HG table keeps the fp32 bilinear filter (its
+ * lookups go through the load path, off the busy texture path). */
 typedef enum { MR_SAMPLER_EXACT = 0, MR_SAMPLER_TEXTURE = 1 } mr_sampler;
 
 /* Library version string. */
