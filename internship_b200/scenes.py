@@ -134,3 +134,18 @@ def cloud_permutation(seed):
 def cloud_scene_params(width=1920, height=1080, **kw):
     kw.setdefault("rt", RT_MRPNN)
     return make_params(width, height, 1, **kw)
+
+
+def ray_box_offset_np(p, d):
+    """RayBoxOffset (core/vector.cu:41-58) on the host: entry distance of the
+    ray p + t d into the box +-0.4999, -1 on a miss (float32 arithmetic)."""
+    p = np.asarray(p, np.float32)
+    d = np.asarray(d, np.float32)
+    with np.errstate(divide="ignore"):
+        inv = np.where(d == 0, np.float32(999999999.0), np.float32(1.0) / np.where(d == 0, 1, d)).astype(np.float32)
+    to_axis = (-p) * inv
+    to_face = np.float32(0.4999) * inv
+    d0, d1 = to_axis + to_face, to_axis - to_face
+    tmi = float(np.max(np.minimum(d0, d1)))
+    tma = float(np.min(np.maximum(d0, d1)))
+    return max(tmi, 0.0) if tma >= tmi else -1.0

@@ -131,6 +131,7 @@ class VolumeRender:
         self.env_color = (0.0, 0.0, 0.0)
         self.network = None
         self.seed = 0
+        self.checkerboard = False
 
     # -- data -------------------------------------------------------------
     def SetData(self, x, y, z, value):
@@ -152,6 +153,7 @@ class VolumeRender:
             self.datas = a.reshape(r, r, r).copy()
 
     def Update(self):
+        self.__dict__.pop("_levels", None)
         L = _lib.load()
         d = np.ascontiguousarray(self.datas, np.float32)
         check(L.mr_volume_set_data(self.handle, d.ctypes.data, d.size))
@@ -161,6 +163,7 @@ class VolumeRender:
         self.max_density = md.value
 
     def Update_TR(self, lightDir, alpha=64.0):
+        self.__dict__.pop("_levels", None)
         check(_lib.load().mr_volume_update_tr(self.handle, f3(lightDir), float(alpha), None))
 
     def UpdateHGLut(self, g):
@@ -207,6 +210,104 @@ class VolumeRender:
 
     def SetSeed(self, seed):
         self.seed = int(seed)
+
+    def SetSurfaceIOR(self, ior):
+        """SetSurfaceIOR (core/volume.cu:1490-1493): the dielectric surface of
+        MR_RT_MARCHING_MRPNN renders; <= 0 removes it."""
+        check(_lib.load().mr_volume_set_surface_ior(self.handle, float(ior)))
+
+    def SetCheckboard(self, on):
+        """SetCheckboard: interactive delta tracking renders half the pixels
+        per frame (RenderInteractive)."""
+        self.checkerboard = bool(on)
+
+    # -- host-side samplers of the tables (core/volume.cu:675-722,1495-1576) --
+    def _level(self, what, level):
+        key = (what, level)
+        cache = self.__dict__.setdefault("_levels", {})
+        if key not in cache:
+            r = (256 if what != _lib.READ_TR else 128) >> level
+            cache[key] = self.read(what, level).reshape(r, r, r)
+        return cache[key]
+
+    @staticmethod
+    def _trilinear(data, uv, clamp):
+        """Sample / SampleClamp (core/volume.cu:675-722): trilinear at
+        uv * res - 1/2 over texels max(0, v), zero outside (or clamped)."""
+        res = data.shape[0]
+        uv = np.asarray(uv, np.float32)
+        pos = uv * np.float32(res) - np.float32(0.5)
+        i0 = np.floor(pos).astype(np.int64)
+        w = (pos - i0).astype(np.float32)
+
+        def at(dx, dy, dz):
+            ix, iy, iz = i0[..., 0] + dx, i0[..., 1] + dy, i0[..., 2] + dz
+            if clamp:
+                ix, iy, iz = (np.clip(a, 0, res - 1) for a in (ix, iy, iz))
+                ok = np.ones(ix.shape, bool)
+            else:
+                ok = (ix >= 0) & (iy >= 0) & (iz >= 0) & (ix < res) & (iy < res) & (iz < res)
+            v = data[np.clip(ix, 0, res - 1), np.clip(iy, 0, res - 1), np.clip(iz, 0, res - 1)]
+            return np.where(ok, np.maximum(v, 0.0), 0.0).astype(np.float32)
+
+        def lerp(a, b, t):
+            return a + (b - a) * t
+        wx, wy, wz = w[..., 0], w[..., 1], w[..., 2]
+        return lerp(lerp(lerp(at(0, 0, 0), at(0, 0, 1), wz), lerp(at(0, 1, 0), at(0, 1, 1), wz), wy),
+                    lerp(lerp(at(1, 0, 0), at(1, 0, 1), wz), lerp(at(1, 1, 0), at(1, 1, 1), wz), wy), wx)
+
+    def DensityAtUV(self, mip, uv):
+        """DensityAtUV(int | float mip, uv): the density pyramid at uv in
+        [0, 1]^3 (a fractional mip blends two levels)."""
+        if isinstance(mip, (float, np.floating)) and float(mip) != int(mip):
+            a = int(mip)
+            t = np.float32(mip - a)
+            return (self.DensityAtUV(a, uv) * (1 - t) + self.DensityAtUV(a + 1, uv) * t).astype(np.float32)
+        return self._trilinear(self._level(_lib.READ_MIP, int(mip)), uv, False)
+
+    def DensityAtPosition(self, mip, pos):
+        """DensityAtPosition: DensityAtUV at pos + 1/2 (pos in [-1/2, 1/2]^3)."""
+        return self.DensityAtUV(mip, np.asarray(pos, np.float32) + np.float32(0.5))
+
+    def TrAtPosition(self, mip, pos, lightDir):
+        """TrAtPosition: the transmittance pyramid at pos; outside the volume,
+        at the volume entry towards the light, or 1 where that ray misses."""
+        from .scenes import ray_box_offset_np
+        pos = np.atleast_2d(np.asarray(pos, np.float32))
+        data = self._level(_lib.READ_TR, int(mip))
+        out = np.ones(len(pos), np.float32)
+        inside = np.all((pos >= -0.5) & (pos <= 0.5), axis=1)
+        if inside.any():
+            out[inside] = self._trilinear(data, pos[inside] + np.float32(0.5), True)
+        L = np.asarray(lightDir, np.float32)
+        for k in np.nonzero(~inside)[0]:
+            o = ray_box_offset_np(pos[k], L)
+            if o >= 0:
+                out[k] = self._trilinear(data, (pos[k] + np.float32(0.5) + L * np.float32(o))[None], True)[0]
+        return out
+
+    def VarianceAtUV(self, mip, uv):
+        """VarianceAtUV (core/volume.cu:1533-1576), as the reference reads it:
+        texel (x, y, z) at uv * res (truncated), the level indexed
+        (z * res + y) * res + x, upper neighbours clamped, zero outside."""
+        if mip < 0 or mip >= 9:
+            return np.zeros(np.shape(uv)[:-1], np.float32)
+        flat = self._level(_lib.READ_VARIANCE, int(mip)).ravel()
+        res = 256 >> int(mip)
+        pos = np.asarray(uv, np.float32) * np.float32(res)
+        x0, y0, z0 = (pos[..., i].astype(np.int64) for i in range(3))
+        x1, y1, z1 = (np.minimum(a + 1, res - 1) for a in (x0, y0, z0))
+        fx, fy, fz = (pos[..., i] - p for i, p in enumerate((x0, y0, z0)))
+
+        def gv(x, y, z):
+            ok = (x >= 0) & (x < res) & (y >= 0) & (y < res) & (z >= 0) & (z < res)
+            i = (np.clip(z, 0, res - 1) * res + np.clip(y, 0, res - 1)) * res + np.clip(x, 0, res - 1)
+            return np.where(ok, flat[i], 0.0).astype(np.float32)
+        c00 = gv(x0, y0, z0) * (1 - fx) + gv(x1, y0, z0) * fx
+        c01 = gv(x0, y0, z1) * (1 - fx) + gv(x1, y0, z1) * fx
+        c10 = gv(x0, y1, z0) * (1 - fx) + gv(x1, y1, z0) * fx
+        c11 = gv(x0, y1, z1) * (1 - fx) + gv(x1, y1, z1) * fx
+        return ((c00 * (1 - fy) + c10 * fy) * (1 - fz) + (c01 * (1 - fy) + c11 * fy) * fz).astype(np.float32)
 
     # -- queries ------------------------------------------------------------
     def read(self, what, level=0):
@@ -258,6 +359,43 @@ class VolumeRender:
             check(L.mr_render_host(self.handle, net, C.byref(p), out.ctypes.data))
             acc += out
         return (acc / sampleNum).astype(np.float32)
+
+    def RenderInteractive(self, accum, hist, bgra, size, ori, up, right, lightDir, lightColor=(1, 1, 1), alpha=1.0,
+                          multiScatter=512, g=0.857, randseed=0, rt=PT, toneType=2, denoise=False, prev=None,
+                          stream=None):
+        """The interactive Render(float3* accum, Histogram* hist, unsigned*
+        bgra, ...) overload (core/volume.cu:469-547) into caller-owned device
+        buffers (torch CUDA tensors: accum W*H*3 float32, hist W*H*33 float32,
+        bgra W*H int32). randseed is the frame index (0 restarts the
+        accumulation); prev = (ori, up, right) of the previous frame for the
+        neural mode's reprojection. toneType 0 none, 1 gamma, 2 ACES."""
+        L = _lib.load()
+        p = self.params(size, ori, up, right, lightDir, rt, g, alpha, lightColor, multiScatter, 1,
+                        sample_offset=randseed)
+        it = _lib.Interactive()
+        po, pu, pr = prev if prev is not None else (ori, up, right)
+        it.prev_ori, it.prev_up, it.prev_right = f3(po), f3(pu), f3(pr)
+        it.frame_index, it.checkerboard = int(randseed), 1 if self.checkerboard else 0
+        it.tone, it.denoise, it.exposure = int(toneType), 1 if denoise else 0, float(self.exposure)
+        net = self.network.handle if self.network is not None else None
+        check(L.mr_render_interactive(self.handle, net, C.byref(p), C.byref(it), C.c_void_p(accum.data_ptr()),
+                                      C.c_void_p(hist.data_ptr()), C.c_void_p(bgra.data_ptr()),
+                                      None if stream is None else C.c_void_p(stream)))
+
+    def GetSamples(self, points, dirs, lightDir, alpha, g, scatter, multiScatter=512, spp=1024, seed=0):
+        """GetSamples (core/volume.cu:550-626, core/render.cuh:276-315): the
+        multiple-scattering radiance at each point along its view direction
+        (unit light, albedo `scatter`), the mean of `spp` paths accumulated in
+        FP64 on the GPU. points, dirs: (n, 3); returns (n,) float64."""
+        import torch
+        pos = torch.as_tensor(np.ascontiguousarray(points, np.float32), device="cuda")
+        dr = torch.as_tensor(np.ascontiguousarray(dirs, np.float32), device="cuda")
+        n = pos.shape[0]
+        acc = torch.zeros(n, dtype=torch.float64, device="cuda")
+        check(_lib.load().mr_train_labels(self.handle, C.c_void_p(pos.data_ptr()), C.c_void_p(dr.data_ptr()), n,
+                                          f3(lightDir), float(alpha), float(g), float(scatter), int(multiScatter),
+                                          int(spp), int(seed), C.c_void_p(acc.data_ptr()), None))
+        return (acc / spp).cpu().numpy()
 
     def close(self):
         if self.handle:
