@@ -97,7 +97,12 @@ def test_tr_at_position(vol):
     below, up = np.array([0.0, -0.9, 0.0], np.float32), np.array([0.0, 1.0, 0.0], np.float32)
     entry = below + up * np.float32(ray_box_offset_np(below, up)) + np.float32(0.5)
     assert float(v.TrAtPosition(1, below[None], up)[0]) == pytest.approx(_trilinear(lvl, entry, True), abs=1e-5)
-    assert float(v.TrAtPosition(1, np.array([[0.0, 0.9, 0.0]], np.float32), np.array([0, 1, 0], np.float32))[0]) == 1.0
+    # RayBoxOffset misses only when the ray's slab intervals do not overlap (a
+    # ray beside the box); one that starts above it and points away still
+    # gets offset 0, as in the reference
+    miss = np.array([[0.9, 0.9, 0.0]], np.float32)
+    assert ray_box_offset_np(miss[0], up) < 0
+    assert float(v.TrAtPosition(1, miss, up)[0]) == 1.0
 
 
 def test_get_samples_matches_oracle(vol):
