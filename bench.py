@@ -216,7 +216,7 @@ def matched_rmse(v, p, sp, oracle_spp=16384, small=None):
     if not os.path.exists(TRAINED):
         return {"unavailable": "no trained weights at internship_b200/data/mrpnn_trained.npy"}
     w_tr = np.load(TRAINED)
-    net = mr.Network(w_tr, mr.spiral_stencil())  # the shipped weights were trained on the spiral stencil
+    net = mr.Network(w_tr, mr.builtin_stencil())  # the shipped weights were trained on the reference stencil
     W, H = small if small else (p.width, p.height)
     q = _lib.RenderParams.from_buffer_copy(p)
     q.width, q.height = W, H
@@ -315,7 +315,7 @@ def batched_serving(replays=10, seed=11):
     rng = np.random.default_rng(seed)
     trained = os.path.exists(TRAINED)
     w = np.load(TRAINED) if trained else mr.xavier_weights(1)
-    net = mr.Network(w, mr.spiral_stencil() if trained else mr.builtin_stencil())
+    net = mr.Network(w, mr.builtin_stencil())
     vols, outs, frames = [], [], []
     b = C.c_void_p()
     _lib.check(L.mr_batch_create(C.byref(b)))
