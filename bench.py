@@ -182,7 +182,7 @@ TRAINED = os.path.join(ROOT, "internship_b200", "data", "mrpnn_trained.npy")
 # k_tc32_head + k_tc32_tail),
 # per density fetch for the trace. A launch's traffic = this figure x the
 # launch's units.
-TRAFFIC_PER_UNIT = {"k_simt": 3356.7, "k_simt_trunk": 2092.4, "k_mlp_tc": 2456.3, "k_gather_fm_exact": 2463.2,
+TRAFFIC_PER_UNIT = {"k_simt": 3377.8, "k_simt_trunk": 2103.4, "k_mlp_tc": 2456.3, "k_gather_fm_exact": 2463.2,
                     "k_gather_fm_texture": 2447.0, "k_nn_trace": 52.56}
 # k_nn_trace: dram__bytes_read + write of one launch of the 1080p bench frame
 # (759.9 MB for 14.46 M density fetches); the others at 960x540 per active pixel.
