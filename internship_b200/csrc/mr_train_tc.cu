@@ -434,16 +434,25 @@ extern "C" int mr_tc_selftest_mn(int32_t n, int32_t k, int32_t a_mn, int32_t b_m
   clear_error();
   if (!host_a || !host_b || !host_d) return set_error(MR_ERR_ARG, "mr_tc_selftest_mn: NULL argument");
   if ((a_mn | b_mn) & ~1) return set_error(MR_ERR_ARG, "mr_tc_selftest_mn: flags must be 0 or 1");
+  const bool built = (n == 64 && k == 32) || (n == 128 && k == 64) || (n == 128 && k == 128) || (n == 64 && k == 128);
+  if (!built) return set_error(MR_ERR_ARG, "mr_tc_selftest_mn: shape %dx%d not built", n, k);
   uint16_t *a = nullptr, *b = nullptr;
   float* d = nullptr;
   int* err = nullptr;
-  MR_CUDA(cudaMalloc(&a, 128 * k * 2));
-  MR_CUDA(cudaMalloc(&b, n * k * 2));
-  MR_CUDA(cudaMalloc(&d, 128 * n * 4));
-  MR_CUDA(cudaMalloc(&err, 4));
-  MR_CUDA(cudaMemset(err, 0, 4));
-  MR_CUDA(cudaMemcpy(a, host_a, 128 * k * 2, cudaMemcpyHostToDevice));
-  MR_CUDA(cudaMemcpy(b, host_b, n * k * 2, cudaMemcpyHostToDevice));
+  cudaError_t ce = cudaMalloc(&a, 128 * k * 2);
+  if (ce == cudaSuccess) ce = cudaMalloc(&b, n * k * 2);
+  if (ce == cudaSuccess) ce = cudaMalloc(&d, 128 * n * 4);
+  if (ce == cudaSuccess) ce = cudaMalloc(&err, 4);
+  if (ce == cudaSuccess) ce = cudaMemset(err, 0, 4);
+  if (ce == cudaSuccess) ce = cudaMemcpy(a, host_a, 128 * k * 2, cudaMemcpyHostToDevice);
+  if (ce == cudaSuccess) ce = cudaMemcpy(b, host_b, n * k * 2, cudaMemcpyHostToDevice);
+  if (ce != cudaSuccess) {
+    cudaFree(a);
+    cudaFree(b);
+    cudaFree(d);
+    cudaFree(err);
+    return cuda_error(ce, "mr_tc_selftest_mn buffers");
+  }
   int rc = MR_OK;
   const int sm = 131072 + 16;
 #define MR_SELFTEST(NN, KK)                                                                         \
