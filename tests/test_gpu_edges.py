@@ -1,6 +1,7 @@
 """Edge cases of the render path on the GPU: an empty volume, a one-pixel and
-a ragged odd-sized frame, paths with no bounce allowed, and a batch that
-mixes an empty volume with a full one."""
+a ragged odd-sized frame, paths with no bounce allowed, a batch that mixes an
+empty volume with a full one, and network row counts that end inside a
+128-row tile."""
 import ctypes as C
 
 import numpy as np
@@ -138,3 +139,43 @@ def test_batch_with_an_empty_volume(mr):
     net.close()
     ve.close()
     vs.close()
+
+
+@pytest.mark.parametrize("n", [1, 127, 129, 383])
+def test_predict_ragged_row_counts(mr, n):
+    """mr_radiance_predict on row counts that leave a partial 128-row tile:
+    fp32 against the oracle's network, BF16 and FP8 close to fp32, and no
+    write past row n."""
+    import torch
+    from internship_b200 import _lib
+    from internship_b200.weights import active_random_weights
+    rng = np.random.default_rng(n)
+    desc = np.zeros((n, 576), np.float32)
+    desc[:, :192] = rng.uniform(0.05, 3, (n, 192))
+    desc[:, 192:384] = rng.uniform(0, 1, (n, 192))
+    desc[:, 384:] = rng.uniform(0.05, 3, (n, 192))
+    aux = np.zeros((n, 5), np.float32)
+    aux[:, 0], aux[:, 1], aux[:, 2:5] = 0.857, rng.uniform(0, 3, n), 0.96
+    w = active_random_weights(1)
+    net = mr.Network(w, mr.builtin_stencil())
+    dd, da = torch.from_numpy(desc).cuda(), torch.from_numpy(aux).cuda()
+    ref = orc.predict(w, desc, aux)
+    outs = {}
+    for name, prec in (("fp32", _lib.PREC_FP32), ("bf16", _lib.PREC_BF16), ("fp8", _lib.PREC_FP8)):
+        out = torch.full((n + 64, 3), -7.0, device="cuda")  # sentinel rows after the last
+        _lib.check(_lib.load().mr_radiance_predict(net.handle, prec, C.c_void_p(dd.data_ptr()),
+                                                   C.c_void_p(da.data_ptr()), n, C.c_void_p(out.data_ptr()), None))
+        torch.cuda.synchronize()
+        o = out.cpu().numpy()
+        assert np.all(o[n:] == -7.0), name
+        outs[name] = o[:n]
+    np.testing.assert_allclose(outs["fp32"], ref, rtol=1e-4, atol=1e-6)
+    # on X = log(1 + L / srp), with the tensor-core tests' bounds (BF16: 8-bit
+    # mantissas through ~30 layers; E4M3: 3-bit)
+    x32 = np.log1p(outs["fp32"] / 0.96)
+    db = np.abs(np.log1p(outs["bf16"] / 0.96) - x32)
+    d8 = np.abs(np.log1p(outs["fp8"] / 0.96) - x32) / np.maximum(x32, 1e-3)
+    assert np.all(np.isfinite(outs["bf16"])) and np.all(np.isfinite(outs["fp8"]))
+    assert db.max() < 0.3 and (n < 10 or np.median(db) < 0.05)
+    assert n < 10 or np.median(d8) < 0.08
+    net.close()
