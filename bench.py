@@ -561,6 +561,8 @@ def main():
                     help="skip the L2 / HBM read probe (its 4 GiB buffer) and the delta-tracking leg: profiler runs")
     ap.add_argument("--frame", default=None,
                     help="WxH instead of 1920x1080: a smaller case for profiler captures, not a bench line")
+    ap.add_argument("--denoise-only", default=None, metavar="WxH",
+                    help="run only the histogram-denoiser leg at WxH and print its record: profiler runs")
     args = ap.parse_args()
     if args.frame:
         global WIDTH, HEIGHT
@@ -584,6 +586,10 @@ def main():
         return
 
     torch.cuda.set_device(local)
+    if args.denoise_only:
+        dw, dh = (int(x) for x in args.denoise_only.lower().split("x"))
+        print(json.dumps(denoise_leg(peaks()[0], steps=args.steps, W=dw, H=dh)), flush=True)
+        return
     import internship_b200 as mr
     from internship_b200 import _lib, replicas, scenes
     L = _lib.load()

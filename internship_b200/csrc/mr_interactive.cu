@@ -21,6 +21,7 @@
 //    with the previous frame's colour at the reprojected pixel, the result
 //    kept in the histogram's three scalar fields as the next frame's history.
 #include <algorithm>
+#include <cfloat>
 
 #include "mr_internal.h"
 #include "mr_track.cuh"
@@ -165,22 +166,42 @@ __global__ void __launch_bounds__(128) k_interactive_pt(InterArgs a) {
 
 constexpr int kTile = 16, kHalo = 5, kSpan = kTile + 2 * kHalo;  // 26
 constexpr int kHistFloats = 3 * kBins + 3;                       // 33
-constexpr int kDenoiseSmem = kSpan * kSpan * (kHistFloats + 3) * (int)sizeof(float);
+// One staged halo pixel: its histogram (bins, total, x2, x) then its colour,
+// 36 floats (144 bytes), so every record starts on a 16-byte boundary.
+constexpr int kRec = kHistFloats + 3;
+constexpr int kDenoiseSmem = kSpan * kSpan * (kRec + 1) * (int)sizeof(float);  // records + nonzero-bin masks
+
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
 
 // Compare (core/volume.cu:187-207): chi-square-like distance of two
-// histograms normalised by their sample counts, averaged over non-empty bins.
-__device__ __forceinline__ float compare(const float* cb, float cn, const float* nb, float nn) {
+// histograms normalised by their sample counts, averaged over the bins that
+// are nonzero in either. cb / cn / cm: the centre's bins, count and
+// nonzero-bin mask; nr / nm: a staged neighbour record and its mask. Bins are
+// sample counts (>= 0), so a bin that is zero in both histograms adds
+// t^2 / FLT_MIN with t = 0, exactly 0: the loop runs without a branch and adds
+// the same terms in the same order as the guarded loop of the reference, and
+// p is the popcount of the joint mask.
+__device__ __forceinline__ float compare(const float (&cb)[3 * kBins], float cn, uint32_t cm, const float* nr,
+                                         uint32_t nm) {
+  float hy[32];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const float4 v = reinterpret_cast<const float4*>(nr)[k];
+    hy[4 * k] = v.x; hy[4 * k + 1] = v.y; hy[4 * k + 2] = v.z; hy[4 * k + 3] = v.w;
+  }
+  const float nn = hy[3 * kBins];
   const float syx = sqrtf(nn / cn), sxy = sqrtf(cn / nn);
-  float p = 0.0f, res = 0.0f;
+  float res = 0.0f;
 #pragma unroll
   for (int i = 0; i < 3 * kBins; ++i) {
-    const float hx = cb[i], hy = nb[i];
-    if (hx != 0.0f || hy != 0.0f) {
-      p += 1.0f;
-      const float t = syx * hx - sxy * hy;
-      res += __fdividef(t * t, hx + hy);  // hx + hy > 0 here; 2-ulp division (121 x 30 per pixel)
-    }
+    const float hx = cb[i], h = hy[i];
+    const float t = syx * hx - sxy * h;
+    res += __fdividef(t * t, fmaxf(hx + h, FLT_MIN));  // 2-ulp division (121 x 30 per pixel)
   }
+  const float p = (float)__popc(cm | nm);
   return p == 0.0f ? 0.0f : res / p;
 }
 
@@ -194,45 +215,63 @@ struct DenoiseArgs {
   size_t npx;
 };
 
-__global__ void __launch_bounds__(256) k_denoise(DenoiseArgs a) {
-  extern __shared__ float sm[];
-  float* sh = sm;                                   // kSpan^2 x 33 (bins, total, x2, x)
-  float* sc = sm + kSpan * kSpan * kHistFloats;     // kSpan^2 x 3
+__global__ void __launch_bounds__(256, 2) k_denoise(DenoiseArgs a) {
+  extern __shared__ __align__(16) float sm[];
+  float* rec = sm;                                                           // kSpan^2 records
+  uint32_t* msk = reinterpret_cast<uint32_t*>(sm + kSpan * kSpan * kRec);  // nonzero bins of each record
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const int c0 = blockIdx.x * kTile - kHalo, r0 = blockIdx.y * kTile - kHalo;
   const bool filter = a.denoise && a.frame != 0;
-  // stage the clamped halo (UnRoll, core/volume.cu:181-185)
-  for (int i = threadIdx.x; i < kSpan * kSpan; i += blockDim.x) {
-    const int rr = min(max(r0 + i / kSpan, 0), a.H - 1), cc = min(max(c0 + i % kSpan, 0), a.W - 1);
-    const size_t p = (size_t)rr * a.W + cc;
-    sc[3 * i] = a.accum[3 * p];
-    sc[3 * i + 1] = a.accum[3 * p + 1];
-    sc[3 * i + 2] = a.accum[3 * p + 2];
+  // stage the clamped halo (UnRoll, core/volume.cu:181-185) by asynchronous
+  // 4-byte copies: every load is in flight at once
+  for (int i = threadIdx.x; i < kSpan * kSpan * 3; i += blockDim.x) {
+    const int q = i / 3, c = i - 3 * q;
+    const int rr = min(max(r0 + q / kSpan, 0), a.H - 1), cc = min(max(c0 + q % kSpan, 0), a.W - 1);
+    cp_async4(rec + q * kRec + kHistFloats + c, a.accum + 3 * ((size_t)rr * a.W + cc) + c);
   }
   if (filter) {
     for (int i = threadIdx.x; i < kSpan * kSpan * kHistFloats; i += blockDim.x) {
       const int q = i / kHistFloats, f = i - q * kHistFloats;
       const int rr = min(max(r0 + q / kSpan, 0), a.H - 1), cc = min(max(c0 + q % kSpan, 0), a.W - 1);
-      sh[i] = reinterpret_cast<const float*>(a.hist + (size_t)rr * a.W + cc)[f];
+      cp_async4(rec + q * kRec + f, reinterpret_cast<const float*>(a.hist + (size_t)rr * a.W + cc) + f);
     }
   }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
+  if (filter) {
+    for (int q = threadIdx.x; q < kSpan * kSpan; q += blockDim.x) {
+      const float4* r = reinterpret_cast<const float4*>(rec + q * kRec);
+      uint32_t m = 0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const float4 v = r[k];
+        const float e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (4 * k + j < 3 * kBins) m |= (e[j] != 0.0f ? 1u : 0u) << (4 * k + j);
+      }
+      msk[q] = m;
+    }
+    __syncthreads();
+  }
   const int row = blockIdx.y * kTile + ty, col = blockIdx.x * kTile + tx;
   if (row >= a.H || col >= a.W) return;
   const int li = (ty + kHalo) * kSpan + (tx + kHalo);
-  F3 res;
-  auto C = [&](int dr, int dc) { const int q = li + dr * kSpan + dc; return f3(sc[3 * q], sc[3 * q + 1], sc[3 * q + 2]); };
+  auto C = [&](int q) {
+    const float* r = rec + q * kRec + kHistFloats;
+    return f3(r[0], r[1], r[2]);
+  };
+  F3 res = C(li);
   if (a.frame == 0) {
     // checkerboard fill of the first frame (core/volume.cu:218-228)
-    if ((((row + a.flip) & 1) + col) % 2 == 0) {
-      res = C(0, 0);
-    } else {
+    if ((((row + a.flip) & 1) + col) % 2 != 0) {
       // neighbours clamped at the image border
-      const int up = row > 0 ? -1 : 0, dn = row < a.H - 1 ? 1 : 0, lf = col > 0 ? -1 : 0, rt = col < a.W - 1 ? 1 : 0;
-      res = (C(up, 0) + C(dn, 0) + C(0, lf) + C(0, rt)) / 4.0f;
+      const int up = row > 0 ? -kSpan : 0, dn = row < a.H - 1 ? kSpan : 0, lf = col > 0 ? -1 : 0,
+                rt = col < a.W - 1 ? 1 : 0;
+      res = (C(li + up) + C(li + dn) + C(li + lf) + C(li + rt)) / 4.0f;
     }
-  } else {
-    const float* ch = sh + li * kHistFloats;
+  } else if (filter) {
+    const float* ch = rec + li * kRec;
     float variance;
     if (a.mom) {
       // |E[l^2] - E[l]^2| from the FP64 sums over the pixel's samples
@@ -243,25 +282,34 @@ __global__ void __launch_bounds__(256) k_denoise(DenoiseArgs a) {
     } else {
       variance = fabsf(ch[3 * kBins + 1] - ch[3 * kBins + 2] * ch[3 * kBins + 2]);
     }
-    if (filter && variance > 0.01f) {
+    if (variance > 0.01f) {
       float cb[3 * kBins];
+      float cn;
 #pragma unroll
-      for (int i = 0; i < 3 * kBins; ++i) cb[i] = ch[i];
-      const float cn = ch[3 * kBins];
+      for (int k = 0; k < 8; ++k) {
+        const float4 v = reinterpret_cast<const float4*>(ch)[k];
+        const float e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          if (4 * k + j < 3 * kBins) cb[4 * k + j] = e[j];
+          else if (4 * k + j == 3 * kBins) cn = e[j];
+        }
+      }
+      const uint32_t cm = msk[li];
       res = f3(0, 0, 0);
       float ws = 0.0f;
       for (int dr = -kHalo; dr <= kHalo; ++dr)
 #pragma unroll
         for (int dc = -kHalo; dc <= kHalo; ++dc) {
           // the staged halo is already clamped, as UnRoll clamps
-          const float* nh = sh + (li + dr * kSpan + dc) * kHistFloats;
-          const float w = fmaxf(0.0f, 1.0f - 1.2f * compare(cb, cn, nh, nh[3 * kBins]));
-          res = res + C(dr, dc) * w;
+          const int q = li + dr * kSpan + dc;
+          const float* nr = rec + q * kRec;
+          const float w = fmaxf(0.0f, 1.0f - 1.2f * compare(cb, cn, cm, nr, msk[q]));
+          const float4 cv = *reinterpret_cast<const float4*>(nr + 32);  // x, then the colour
+          res = res + f3(cv.y, cv.z, cv.w) * w;
           ws += w;
         }
       res = res / ws;
-    } else {
-      res = C(0, 0);
     }
   }
   a.out[(size_t)row * a.W + col] = pack_bgra(res, a.exposure, a.tone);
