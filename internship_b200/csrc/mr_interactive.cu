@@ -176,6 +176,15 @@ __device__ __forceinline__ void cp_async4(float* dst, const float* src) {
                : "memory");
 }
 
+// x / y by the PTX approximate division (at most 2 ulp for y in
+// [2^-126, 2^126]) with subnormal inputs and results flushed to zero: a
+// subnormal bin term t^2 / (hx + hy) is below any weight's resolution.
+__device__ __forceinline__ float div_approx_ftz(float x, float y) {
+  float r;
+  asm("div.approx.ftz.f32 %0, %1, %2;" : "=f"(r) : "f"(x), "f"(y));
+  return r;
+}
+
 // Compare (core/volume.cu:187-207): chi-square-like distance of two
 // histograms normalised by their sample counts, averaged over the bins that
 // are nonzero in either. cb / cn / cm: the centre's bins, count and
@@ -199,7 +208,7 @@ __device__ __forceinline__ float compare(const float (&cb)[3 * kBins], float cn,
   for (int i = 0; i < 3 * kBins; ++i) {
     const float hx = cb[i], h = hy[i];
     const float t = syx * hx - sxy * h;
-    res += __fdividef(t * t, fmaxf(hx + h, FLT_MIN));  // 2-ulp division (121 x 30 per pixel)
+    res += div_approx_ftz(t * t, fmaxf(hx + h, FLT_MIN));
   }
   const float p = (float)__popc(cm | nm);
   return p == 0.0f ? 0.0f : res / p;

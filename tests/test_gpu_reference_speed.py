@@ -39,19 +39,26 @@ def _tables(v):
     return mips, tr, v.read(_lib.READ_HGLUT)
 
 
-def _ref_pass_ms(ref, mode, p, L, bounces, passes):
+def _ref_pass_ms(ref, mode, p, L, bounces, passes, repeats=3):
     """Device time of one reference pass: wall time of passes + 1 passes
     minus that of one pass (the harness's allocations, the host copies of
-    its FP64 sums and its final synchronisation cancel)."""
+    its FP64 sums and its final synchronisation cancel). Each wall time is
+    the least of `repeats` runs, so that host noise in a single run (which
+    once made the difference negative) does not enter."""
     ori, up, right = _camera(p)
     args = (p.width, p.height, ori, up, right, L, (1.0, 1.0, 1.0), p.alpha, bounces, p.g)
     ref.render(mode, *args, 1)  # warm-up
-    t0 = time.perf_counter()
-    ref.render(mode, *args, 1)
-    t1 = time.perf_counter()
-    ref.render(mode, *args, passes + 1)
-    t2 = time.perf_counter()
-    return ((t2 - t1) - (t1 - t0)) * 1e3 / passes
+    one, many = [], []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        ref.render(mode, *args, 1)
+        one.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        ref.render(mode, *args, passes + 1)
+        many.append(time.perf_counter() - t0)
+    ms = (min(many) - min(one)) * 1e3 / passes
+    assert ms > 0, "reference pass time not resolved: %r, %r" % (one, many)
+    return ms
 
 
 def _ours_ms(v, p, frames):
@@ -105,7 +112,7 @@ def test_neural_render_against_reference_kernel_same_gpu(mr):
     ref = ref_py.Ref()
     ref.load_weights(w)
     ref.setup(dens.cpu().numpy(), md.value, mips, tr, lut, scatter=(0.99, 0.99, 0.99))
-    ref_ms = _ref_pass_ms(ref, 1, p, L, 512, 3)
+    ref_ms = _ref_pass_ms(ref, 1, p, L, 512, 16)
     print("\nneural %dx%d, 512^3 cloud: reference NNPredict<MRPNN> %.2f ms per frame (%.1f frames/s); "
           "here fp32/exact %.3f ms (%.1f frames/s, %.1fx), BF16/texture %.3f ms (%.1f frames/s, %.1fx)"
           % (W, W, ref_ms, 1e3 / ref_ms, ours["fp32_exact"], 1e3 / ours["fp32_exact"], ref_ms / ours["fp32_exact"],
