@@ -511,6 +511,9 @@ def denoise_leg(hbm_gbs, steps=10, W=1920, H=1080):
     ach = n * 148.0 / (t / 1e3) / 1e9
     return {"workload": "mr_denoise at %dx%d, ACES, filter active on every pixel" % (W, H), "kernel": "k_denoise",
             "ms": t, "pixels_per_s": n / (t / 1e3),
+            "compare_bin_terms_per_s": n * 121 * 30 / (t / 1e3),
+            "bound": "instruction issue and the XU pipe (121 x 30 Compare bin terms per pixel, one approximate "
+                     "reciprocal each), not HBM",
             "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm_gbs, "unit": "GB/s", "frac": ach / hbm_gbs,
                          "algorithmic_bytes": "148 B per pixel (histogram 132 B + colour 12 B read, 4 B written)"}}
 

@@ -176,12 +176,37 @@ __device__ __forceinline__ void cp_async4(float* dst, const float* src) {
                : "memory");
 }
 
-// x / y by the PTX approximate division (at most 2 ulp for y in
-// [2^-126, 2^126]) with subnormal inputs and results flushed to zero: a
-// subnormal bin term t^2 / (hx + hy) is below any weight's resolution.
-__device__ __forceinline__ float div_approx_ftz(float x, float y) {
+// Packed fp32 pairs (the sm_100 .f32x2 forms of add, mul and fma: two
+// independent fp32 operations, each rounded as its scalar form).
+struct P2 { float x, y; };
+__device__ __forceinline__ P2 add2(P2 a, P2 b) {
+  P2 d;
+  asm("{\n\t.reg .b64 a, b, d;\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\t"
+      "add.rn.f32x2 d, a, b;\n\tmov.b64 {%0, %1}, d;\n\t}"
+      : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return d;
+}
+__device__ __forceinline__ P2 mul2(P2 a, P2 b) {
+  P2 d;
+  asm("{\n\t.reg .b64 a, b, d;\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\t"
+      "mul.rn.f32x2 d, a, b;\n\tmov.b64 {%0, %1}, d;\n\t}"
+      : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return d;
+}
+__device__ __forceinline__ P2 fma2(P2 a, P2 b, P2 c) {
+  P2 d;
+  asm("{\n\t.reg .b64 a, b, c, d;\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\tmov.b64 c, {%6, %7};\n\t"
+      "fma.rn.f32x2 d, a, b, c;\n\tmov.b64 {%0, %1}, d;\n\t}"
+      : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+  return d;
+}
+// 1 / y by the PTX approximate reciprocal, subnormals flushed to zero. A
+// quotient x / y is taken as x * (1 / y), the form the PTX ISA gives for its
+// approximate division (at most 2 ulp for y in [2^-126, 2^126]); a subnormal
+// bin term is far below any weight's resolution.
+__device__ __forceinline__ float rcp_approx_ftz(float y) {
   float r;
-  asm("div.approx.ftz.f32 %0, %1, %2;" : "=f"(r) : "f"(x), "f"(y));
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(y));
   return r;
 }
 
@@ -192,7 +217,8 @@ __device__ __forceinline__ float div_approx_ftz(float x, float y) {
 // sample counts (>= 0), so a bin that is zero in both histograms adds
 // t^2 / FLT_MIN with t = 0, exactly 0: the loop runs without a branch and adds
 // the same terms in the same order as the guarded loop of the reference, and
-// p is the popcount of the joint mask.
+// p is the popcount of the joint mask. Bins go in pairs through the packed
+// fp32 forms; the terms are still summed one by one in bin order.
 __device__ __forceinline__ float compare(const float (&cb)[3 * kBins], float cn, uint32_t cm, const float* nr,
                                          uint32_t nm) {
   float hy[32];
@@ -203,12 +229,16 @@ __device__ __forceinline__ float compare(const float (&cb)[3 * kBins], float cn,
   }
   const float nn = hy[3 * kBins];
   const float syx = sqrtf(nn / cn), sxy = sqrtf(cn / nn);
+  const P2 a2{syx, syx}, b2{-sxy, -sxy};
   float res = 0.0f;
 #pragma unroll
-  for (int i = 0; i < 3 * kBins; ++i) {
-    const float hx = cb[i], h = hy[i];
-    const float t = syx * hx - sxy * h;
-    res += div_approx_ftz(t * t, fmaxf(hx + h, FLT_MIN));
+  for (int i = 0; i < 3 * kBins; i += 2) {
+    const P2 hx{cb[i], cb[i + 1]}, h{hy[i], hy[i + 1]};
+    const P2 s = add2(hx, h);
+    const P2 t = fma2(a2, hx, mul2(b2, h));  // syx hx - sxy h
+    const P2 q = mul2(mul2(t, t), P2{rcp_approx_ftz(fmaxf(s.x, FLT_MIN)), rcp_approx_ftz(fmaxf(s.y, FLT_MIN))});
+    res += q.x;
+    res += q.y;
   }
   const float p = (float)__popc(cm | nm);
   return p == 0.0f ? 0.0f : res / p;
