@@ -169,7 +169,8 @@ constexpr int kHistFloats = 3 * kBins + 3;                       // 33
 // One staged halo pixel: its histogram (bins, total, x2, x) then its colour,
 // 36 floats (144 bytes), so every record starts on a 16-byte boundary.
 constexpr int kRec = kHistFloats + 3;
-constexpr int kDenoiseSmem = kSpan * kSpan * (kRec + 1) * (int)sizeof(float);  // records + nonzero-bin masks
+// records, nonzero-bin masks, (sqrt n, 1 / sqrt n) of each record's count
+constexpr int kDenoiseSmem = kSpan * kSpan * (kRec + 3) * (int)sizeof(float);
 
 __device__ __forceinline__ void cp_async4(float* dst, const float* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
@@ -216,19 +217,22 @@ __device__ __forceinline__ float rcp_approx_ftz(float y) {
 // nonzero-bin mask; nr / nm: a staged neighbour record and its mask. Bins are
 // sample counts (>= 0), so a bin that is zero in both histograms adds
 // t^2 / FLT_MIN with t = 0, exactly 0: the loop runs without a branch and adds
-// the same terms in the same order as the guarded loop of the reference, and
-// p is the popcount of the joint mask. Bins go in pairs through the packed
-// fp32 forms; the terms are still summed one by one in bin order.
-__device__ __forceinline__ float compare(const float (&cb)[3 * kBins], float cn, uint32_t cm, const float* nr,
-                                         uint32_t nm) {
+// a term for the same bins, in the same order, as the guarded loop of the
+// reference, and p is the popcount of the joint mask. Bins go in pairs through the packed
+// fp32 forms; the terms are still summed one by one in bin order. The count
+// ratios sqrt(nn / cn) and sqrt(cn / nn) are taken as products of each
+// count's staged sqrt(n) and 1 / sqrt(n) (cs: the centre's, ns: the
+// neighbour's), and the mean over the p bins by an approximate division:
+// each within a few ulp of the reference's divisions and roots.
+__device__ __forceinline__ float compare(const float (&cb)[3 * kBins], float2 cs, uint32_t cm, const float* nr,
+                                         float2 ns, uint32_t nm) {
   float hy[32];
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     const float4 v = reinterpret_cast<const float4*>(nr)[k];
     hy[4 * k] = v.x; hy[4 * k + 1] = v.y; hy[4 * k + 2] = v.z; hy[4 * k + 3] = v.w;
   }
-  const float nn = hy[3 * kBins];
-  const float syx = sqrtf(nn / cn), sxy = sqrtf(cn / nn);
+  const float syx = ns.x * cs.y, sxy = cs.x * ns.y;
   const P2 a2{syx, syx}, b2{-sxy, -sxy};
   float res = 0.0f;
 #pragma unroll
@@ -241,7 +245,7 @@ __device__ __forceinline__ float compare(const float (&cb)[3 * kBins], float cn,
     res += q.y;
   }
   const float p = (float)__popc(cm | nm);
-  return p == 0.0f ? 0.0f : res / p;
+  return p == 0.0f ? 0.0f : res * rcp_approx_ftz(p);
 }
 
 struct DenoiseArgs {
@@ -258,6 +262,7 @@ __global__ void __launch_bounds__(256, 2) k_denoise(DenoiseArgs a) {
   extern __shared__ __align__(16) float sm[];
   float* rec = sm;                                                           // kSpan^2 records
   uint32_t* msk = reinterpret_cast<uint32_t*>(sm + kSpan * kSpan * kRec);  // nonzero bins of each record
+  float2* rsq = reinterpret_cast<float2*>(sm + kSpan * kSpan * (kRec + 1));  // (sqrt n, 1 / sqrt n) per record
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const int c0 = blockIdx.x * kTile - kHalo, r0 = blockIdx.y * kTile - kHalo;
   const bool filter = a.denoise && a.frame != 0;
@@ -290,6 +295,8 @@ __global__ void __launch_bounds__(256, 2) k_denoise(DenoiseArgs a) {
           if (4 * k + j < 3 * kBins) m |= (e[j] != 0.0f ? 1u : 0u) << (4 * k + j);
       }
       msk[q] = m;
+      const float rn = sqrtf(rec[q * kRec + 3 * kBins]);
+      rsq[q] = make_float2(rn, 1.0f / rn);
     }
     __syncthreads();
   }
@@ -323,18 +330,16 @@ __global__ void __launch_bounds__(256, 2) k_denoise(DenoiseArgs a) {
     }
     if (variance > 0.01f) {
       float cb[3 * kBins];
-      float cn;
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         const float4 v = reinterpret_cast<const float4*>(ch)[k];
         const float e[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < 4; ++j)
           if (4 * k + j < 3 * kBins) cb[4 * k + j] = e[j];
-          else if (4 * k + j == 3 * kBins) cn = e[j];
-        }
       }
       const uint32_t cm = msk[li];
+      const float2 cs = rsq[li];
       res = f3(0, 0, 0);
       float ws = 0.0f;
       for (int dr = -kHalo; dr <= kHalo; ++dr)
@@ -343,7 +348,7 @@ __global__ void __launch_bounds__(256, 2) k_denoise(DenoiseArgs a) {
           // the staged halo is already clamped, as UnRoll clamps
           const int q = li + dr * kSpan + dc;
           const float* nr = rec + q * kRec;
-          const float w = fmaxf(0.0f, 1.0f - 1.2f * compare(cb, cn, cm, nr, msk[q]));
+          const float w = fmaxf(0.0f, 1.0f - 1.2f * compare(cb, cs, cm, nr, rsq[q], msk[q]));
           const float4 cv = *reinterpret_cast<const float4*>(nr + 32);  // x, then the colour
           res = res + f3(cv.y, cv.z, cv.w) * w;
           ws += w;
