@@ -174,9 +174,10 @@ int refv_fill_hg(float g, int randnum, float* lut_out, float* bn_out) {
 
 // Denoise<denoise> on caller buffers: accum w*h*3, hist w*h*33 (the
 // Histogram layout), frame (frameNum), flip, tone (0 none, 1 gamma, 2 ACES),
-// exposure; out w*h packed 0xAARRGGBB.
+// exposure; out w*h packed 0xAARRGGBB. kernel_ms (may be null) receives the
+// kernel's device time from CUDA events around its launch.
 int refv_denoise(const float* accum, const float* hist, int w, int h, int frame, int flip_, int tone, int denoise,
-                 float exp_, uint32_t* out) {
+                 float exp_, uint32_t* out, float* kernel_ms) {
   int n = w * h;
   float3* d_acc = nullptr;
   Histogram* d_hist = nullptr;
@@ -190,12 +191,20 @@ int refv_denoise(const float* accum, const float* hist, int w, int h, int frame,
   CK(cudaMemcpyToSymbol(flip, &flip_, sizeof(int)));
   CK(cudaMemcpyToSymbol(exposure, &exp_, sizeof(float)));
   int group = 32, groups = (n + group - 1) / group;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0));
   if (denoise)
     Denoise<true><<<groups, group>>>(d_acc, d_hist, d_out, int2{w, h}, tone);
   else
     Denoise<false><<<groups, group>>>(d_acc, d_hist, d_out, int2{w, h}, tone);
   CK(cudaGetLastError());
+  CK(cudaEventRecord(e1));
   CK(cudaDeviceSynchronize());
+  if (kernel_ms) CK(cudaEventElapsedTime(kernel_ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
   CK(cudaMemcpy(out, d_out, n * sizeof(unsigned int), cudaMemcpyDeviceToHost));
   cudaFree(d_acc);
   cudaFree(d_hist);

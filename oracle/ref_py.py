@@ -144,7 +144,8 @@ class RefVolume:
         L.refv_set_scalars.argtypes = [C.c_void_p, C.c_float, f32p, C.c_float, f32p]
         L.refv_fill_tr.argtypes = [f32p, C.c_float, f32p, f32p]
         L.refv_fill_hg.argtypes = [C.c_float, C.c_int, f32p, f32p]
-        L.refv_denoise.argtypes = [f32p, f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, u32p]
+        L.refv_denoise.argtypes = [f32p, f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, u32p,
+                                   C.POINTER(C.c_float)]
         L.refv_get_samples.argtypes = [C.c_void_p, C.c_int, f32p, f32p, f32p, C.c_float, C.c_float, C.c_float,
                                        C.c_int, C.c_int, C.c_int, f32p]
         L.refv_interactive.argtypes = [C.c_void_p, C.c_int, C.c_int, f32p, f32p, f32p, f32p, f32p, C.c_float, C.c_int,
@@ -186,11 +187,13 @@ class RefVolume:
         assert self.L.refv_fill_hg(float(g), int(randnum), lut, bn) == 0
         return lut, bn
 
-    def denoise(self, accum, hist, w, h, frame, flip, tone, denoise, exposure=1.0):
+    def denoise(self, accum, hist, w, h, frame, flip, tone, denoise, exposure=1.0, timed=False):
+        """Packed output; with timed=True also the kernel's device time in ms."""
         out = np.zeros(w * h, np.uint32)
+        ms = C.c_float(0.0)
         assert self.L.refv_denoise(_f(accum), _f(hist), w, h, int(frame), int(flip), int(tone), int(denoise),
-                                   float(exposure), out) == 0
-        return out
+                                   float(exposure), out, C.byref(ms)) == 0
+        return (out, ms.value) if timed else out
 
     def get_samples(self, pos, dirs, light, alpha, g, scatter, bounces, spp, randnum=0):
         n = len(pos)
